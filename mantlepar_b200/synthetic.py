@@ -1,0 +1,184 @@
+"""Seeded synthetic transport workloads (no datasets are involved).
+
+Builds the cell-average initial state and the face-normal velocity data of the
+MantlePar coupled transport workloads:
+
+* uniform ``nx x ny`` quads on ``[0, 0.5] x [0, 1]`` (src/core/mesh.cpp:27-55,
+  uniform family: x_i = x0 + i*L/nx with the far endpoint snapped);
+* cell averages ``H = (1 - y_c) + a_H * U_H``, ``C = 0.3 + 0.02 * U_C`` with
+  ``U`` from the reference's stateless SplitMix64 finaliser
+  (src/core/mesh.cpp:12-25) keyed ``seed + 2*cell + field``;
+* solid velocity ``v_s = (d psi/dy, -d psi/dx)`` of the streamfunction
+  ``psi = A sin(2 pi x) sin(pi y)`` and Darcy velocity ``u_d = (0, 0.01)``,
+  sampled at the 5 Gauss points of every edge.  Normal components are taken
+  against each edge's canonical right normal ``(dy, -dx)/len``
+  (src/core/integral.cpp:62-89) in the reference's edge-id order
+  (src/core/mesh_info.h:84: AlongI ids ``j*nx + i`` first, then AlongJ ids
+  ``nx*(ny+1) + j*(nx+1) + i``).  ``psi = 0`` on the walls, so the solid
+  normal velocity is set to exactly zero on boundary edges.
+
+The material set ("S") keeps the reference defaults except Te0=250 K,
+Tm0=1250 K, L=6e5, cp=1200, Xe=0.5, alpha0=0: with these the literal H, C
+formulas populate the two-solid, eutectic and solid+liquid regions (with the
+defaults C=0.3 exceeds Xe=0.25 and the reference rejects the state).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+GAUSS5_POINTS, GAUSS5_WEIGHTS = np.polynomial.legendre.leggauss(5)
+
+_M1 = np.uint64(0x9E3779B97F4A7C15)
+_M2 = np.uint64(0xBF58476D1CE4E5B9)
+_M3 = np.uint64(0x94D049BB133111EB)
+
+
+def mix64(v: np.ndarray) -> np.ndarray:
+    """SplitMix64 finaliser on uint64 arrays (src/core/mesh.cpp:12-18)."""
+    with np.errstate(over="ignore"):
+        v = v.astype(np.uint64) + _M1
+        v = (v ^ (v >> np.uint64(30))) * _M2
+        v = (v ^ (v >> np.uint64(27))) * _M3
+        return v ^ (v >> np.uint64(31))
+
+
+def unit_noise(seed: int, field: int, cells: np.ndarray) -> np.ndarray:
+    """Uniform [0,1) per cell: top 53 bits of SplitMix64(seed + 2*cell + field)."""
+    with np.errstate(over="ignore"):
+        key = np.uint64(seed) + np.uint64(2) * cells.astype(np.uint64) + np.uint64(field)
+    return (mix64(key) >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
+
+
+@dataclasses.dataclass
+class Material:
+    """Dimensional material inputs (src/phase/eutectic_rescaled.h:10-26)."""
+    Tm0: float = 2000.0
+    Te0: float = 1480.0
+    nu: float = 6.5e6
+    L: float = 5.0e5
+    cp: float = 1200.0
+    Xe: float = 0.25
+    rho: float = 3000.0
+    rhor: float = 500.0
+    mus: float = 1.0e19
+    mul: float = 1.0
+    k0: float = 1.0e-8
+    g: float = 10.0
+    alpha0: float = 3.0e-5
+
+    def astuple(self):
+        return dataclasses.astuple(self)
+
+
+def material_s() -> Material:
+    """Material set S used by every transport workload."""
+    return Material(Tm0=1250.0, Te0=250.0, L=6.0e5, cp=1200.0, Xe=0.5, alpha0=0.0)
+
+
+@dataclasses.dataclass
+class Workload:
+    nx: int
+    ny: int
+    x0: float = 0.0
+    x1: float = 0.5
+    y0: float = 0.0
+    y1: float = 1.0
+    noise_H: float = 0.05
+    noise_C: float = 0.02
+    psi_amplitude: float = 0.1
+    darcy: float = 0.01
+    seed: int = 1
+    cfl: float = 0.4
+    steps: int = 200
+    integrator: int = 3
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.ny
+
+    @property
+    def edges(self) -> int:
+        return self.nx * (self.ny + 1) + (self.nx + 1) * self.ny
+
+
+def vertex_coords(n: int, lo: float, hi: float) -> np.ndarray:
+    """Vertex coordinates of one axis as src/core/mesh.cpp VertexAt (uniform)."""
+    h = (hi - lo) / float(n)
+    v = lo + np.arange(n + 1, dtype=np.float64) * h
+    v[0] = lo
+    v[-1] = lo + (hi - lo)
+    return v
+
+
+def initial_state(w: Workload) -> tuple[np.ndarray, np.ndarray]:
+    """Seeded cell averages H, C (x fastest, id = j*nx + i)."""
+    ys = vertex_coords(w.ny, w.y0, w.y1)
+    yc = 0.5 * (ys[:-1] + ys[1:])
+    cells = np.arange(w.cells, dtype=np.uint64)
+    H = (1.0 - np.repeat(yc, w.nx)) + w.noise_H * unit_noise(w.seed, 0, cells)
+    C = 0.3 + w.noise_C * unit_noise(w.seed, 1, cells)
+    return np.ascontiguousarray(H), np.ascontiguousarray(C)
+
+
+def face_velocity(w: Workload) -> tuple[np.ndarray, np.ndarray]:
+    """Normal solid / Darcy velocity at edge Gauss points, shape (edges, 5).
+
+    Row e holds canonical edge id e; column q the q-th Gauss point along the
+    canonical direction (increasing x for AlongI edges, increasing y for
+    AlongJ edges).  Normals are the canonical right normals: (0,-1) for AlongI
+    edges and (1,0) for AlongJ edges.
+    """
+    xs = vertex_coords(w.nx, w.x0, w.x1)
+    ys = vertex_coords(w.ny, w.y0, w.y1)
+    A = w.psi_amplitude
+    t = 0.5 * (1.0 + GAUSS5_POINTS)
+    two_pi = 2.0 * math.pi
+    # AlongI edges: (i, j) for j in 0..ny, i in 0..nx-1; normal (0,-1).
+    xi = xs[:-1, None] + t[None, :] * (xs[1:] - xs[:-1])[:, None]          # (nx, 5)
+    yj = ys                                                               # (ny+1)
+    vy = -two_pi * A * np.cos(two_pi * xi)[None, :, :] * np.sin(math.pi * yj)[:, None, None]
+    vs_i = -vy                                                            # v_s . (0,-1)
+    vs_i[0] = 0.0
+    vs_i[-1] = 0.0
+    ud_i = np.full_like(vs_i, -w.darcy)                                   # u_d . (0,-1)
+    # AlongJ edges: (i, j) for j in 0..ny-1, i in 0..nx; normal (1,0).
+    yq = ys[:-1, None] + t[None, :] * (ys[1:] - ys[:-1])[:, None]          # (ny, 5)
+    vx = math.pi * A * np.sin(two_pi * xs)[None, :, None] * np.cos(math.pi * yq)[:, None, :]
+    vs_j = vx
+    vs_j[:, 0, :] = 0.0
+    vs_j[:, -1, :] = 0.0
+    ud_j = np.zeros_like(vs_j)
+    vs = np.concatenate([vs_i.reshape(-1, 5), vs_j.reshape(-1, 5)])
+    ud = np.concatenate([ud_i.reshape(-1, 5), ud_j.reshape(-1, 5)])
+    return np.ascontiguousarray(vs), np.ascontiguousarray(ud)
+
+
+# The BASELINE workloads, named by what they are.
+def plain_small() -> Workload:
+    """20x20 plain FP64 instance, 200 steps (the run.sh --grid 20 size)."""
+    return Workload(nx=20, ny=20, steps=200)
+
+
+def plain_large() -> Workload:
+    """1280x2560 plain FP64 single instance, 100 steps."""
+    return Workload(nx=1280, ny=2560, steps=100)
+
+
+def mixed_large() -> Workload:
+    """4096x4096 mixed-precision instance, H noise 0.1, 50 steps."""
+    return Workload(nx=4096, ny=4096, noise_H=0.1, steps=50)
+
+
+def batched_instances(count: int = 256, seed: int = 3) -> list[Workload]:
+    """Uneven meshes: nx, ny log-uniform on [40,640] and [40,960], step 20."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        nx = int(20 * round(math.exp(rng.uniform(math.log(40), math.log(640))) / 20))
+        ny = int(20 * round(math.exp(rng.uniform(math.log(40), math.log(960))) / 20))
+        amp = float(rng.uniform(0.05, 0.2))
+        out.append(Workload(nx=max(nx, 40), ny=max(ny, 40), psi_amplitude=amp, seed=1000 + i, steps=100))
+    return out

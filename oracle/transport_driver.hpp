@@ -1,0 +1,633 @@
+// CPU oracle: the coupled H/C transport stage and time loop.
+// TEST INFRASTRUCTURE ONLY -- the checker for the CUDA transport kernels.
+//
+// Restates, for one rank (no MPI), with the synthetic flow supplier:
+//   src/couple/evolve.cpp:36-52     PhaseTransportVelocities
+//   src/couple/evolve.cpp:221-268   Build (face table, diffusion sampling)
+//   src/couple/evolve.cpp:270-277   Phase (limited evaluation + admissibility)
+//   src/couple/evolve.cpp:279-384   RHS (faces, cell quadrature, totals)
+//   src/couple/evolve.cpp:386-393   Admissible
+//   src/couple/evolve.cpp:428-511   Run (SSPRK2 with CFL retry, balance check)
+//   src/couple/state_reconstruction.cpp:101-192  Update, Evaluate, Limit
+//   src/couple/initial_flow.cpp:94-117  edge porosity (harmonic mean, dry cells)
+// The flow supplier (Stokes-Darcy FEM, re-solved per stage in the reference)
+// is replaced by face-normal velocity data: solid velocity and Darcy velocity
+// normal components at each edge Gauss point, frozen for the run. The edge
+// porosity is recomputed from the current stage exactly as the reference's
+// porosity sampling does. Shu-Osher SSPRK3 is added beside SSPRK2.
+//
+// Backend B supplies the per-cell numerics: B::Recon (update/evaluate of one
+// field's reconstruction of one cell), B::phase, and the geometry primitives.
+#ifndef MP_ORACLE_TRANSPORT_DRIVER_HPP
+#define MP_ORACLE_TRANSPORT_DRIVER_HPP
+
+#include "oracle.h"
+#include "restated.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <thread>
+#include <vector>
+
+namespace orc {
+
+// Static-chunked parallel loop over [0, n) on std::threads (the image has no
+// OpenMP runtime). Records the first orc::Error by lowest index.
+inline int& oracle_threads() { static int t = 0; return t; }
+template <class F>
+void parallel_for(int n, F&& f) {
+    int nt = oracle_threads() > 0 ? oracle_threads() : (int)std::thread::hardware_concurrency();
+    nt = std::max(1, std::min(nt, n));
+    std::vector<int> codes(nt, 0);
+    std::vector<int> where(nt, n);
+    auto body = [&](int t) {
+        const int lo = (int)((long long)n * t / nt), hi = (int)((long long)n * (t + 1) / nt);
+        for (int k = lo; k < hi; ++k) {
+            try { f(k); } catch (const Error& e) { codes[t] = e.code; where[t] = k; return; }
+        }
+    };
+    if (nt == 1) body(0);
+    else {
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t) pool.emplace_back(body, t);
+        body(0);
+        for (auto& th : pool) th.join();
+    }
+    for (int t = 0; t < nt; ++t) if (codes[t]) throw Error{codes[t], "parallel loop failed"};
+}
+
+struct Face {
+    int left = 0, right = -1;        // cell ids (x fastest); right = -1 on a boundary
+    int edge = 0;                    // canonical edge id
+    bool boundary = false, reverse = false;
+    Pt a, b;                         // oriented vertices (left cell CCW)
+    double length = 0;
+    Pt normal;
+    double area[2] = {0, 0};
+    Sampling diffusion;
+};
+
+template <class B>
+struct Driver {
+    orc_material mat{};
+    orc_derived der{};
+    orc_transport_opts o{};
+    B backend;
+    int nx = 0, ny = 0, ncell = 0, nIedge = 0, nedge = 0;
+    std::vector<Pt> vert;                // (nx+1)*(ny+1)
+    std::vector<double> area;            // per cell
+    std::vector<double> gp, gw;          // 5-point Gauss rule (edges and cells)
+    std::vector<Face> faces;
+    std::vector<typename B::Recon> rh, rc;   // per-cell reconstructions of H and C
+    std::vector<double> H, C, T, phi, oldH, oldC;
+    std::vector<double> lim_h, lim_c;
+    std::vector<double> vsn, udn;        // per edge, per canonical q
+    std::vector<double> edge_phi;        // per edge, per canonical q
+    std::vector<unsigned char> wet;
+    std::vector<double> rhsH, rhsC, rate, divg;
+    double time = 0;
+    int accepted = 0;
+    int nq = 5;
+    int samples_n = 4;
+    double samples_frac = 0.9;
+
+    struct Rates { double boundaryH = 0, boundaryC = 0, sourceH = 0, maximumRate = 0, divergence = 0; };
+    Rates current;
+    bool have_current = false;
+
+    int cell_id(int i, int j) const { return j * nx + i; }
+    Quad corners(int i, int j) const {
+        const int M = nx + 1;
+        return Quad{{vert[(size_t)j * M + i], vert[(size_t)j * M + i + 1], vert[(size_t)(j + 1) * M + i + 1], vert[(size_t)(j + 1) * M + i]}};
+    }
+
+    // mesh.cpp:27-55 (uniform family), integral-based areas as MeshInfo::CacheAreas.
+    void build_mesh() {
+        const int M = nx + 1, N = ny + 1;
+        const double L = o.x1 - o.x0, Hh = o.y1 - o.y0;
+        const double hx = L / (double)(M - 1), hy = Hh / (double)(N - 1);
+        vert.resize((size_t)M * N);
+        for (int j = 0; j < N; ++j)
+            for (int i = 0; i < M; ++i) {
+                Pt p{o.x0 + (double)i * hx, o.y0 + (double)j * hy};
+                if (i == 0) p.x = o.x0;
+                if (i == M - 1) p.x = o.x0 + L;
+                if (j == 0) p.y = o.y0;
+                if (j == N - 1) p.y = o.y0 + Hh;
+                vert[(size_t)j * M + i] = p;
+            }
+        area.resize(ncell);
+        std::vector<double> p1, w1;
+        B::gauss_rule(1, p1, w1);
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i)
+                area[cell_id(i, j)] = B::cell_area(corners(i, j), p1, w1);
+    }
+
+    // evolve.cpp:221-268 for one rank: faces in sorted edge-id order.
+    void build_faces() {
+        faces.clear();
+        faces.reserve(nedge);
+        for (int id = 0; id < nedge; ++id) {
+            Face f;
+            f.edge = id;
+            int li, lj, ri, rj;
+            Pt v0, v1;
+            const int M = nx + 1;
+            if (id < nIedge) {
+                const int i = id % nx, j = id / nx;
+                v0 = vert[(size_t)j * M + i]; v1 = vert[(size_t)j * M + i + 1];
+                li = i; lj = j; ri = i; rj = j - 1;
+            } else {
+                const int k = id - nIedge, i = k % M, j = k / M;
+                v0 = vert[(size_t)j * M + i]; v1 = vert[(size_t)(j + 1) * M + i];
+                li = i - 1; lj = j; ri = i; rj = j;
+            }
+            const bool hasL = li >= 0 && li < nx && lj >= 0 && lj < ny;
+            const bool hasR = ri >= 0 && ri < nx && rj >= 0 && rj < ny;
+            f.boundary = !hasL || !hasR;
+            f.reverse = !hasL;
+            f.left = f.reverse ? cell_id(ri, rj) : cell_id(li, lj);
+            if (!f.boundary) f.right = cell_id(ri, rj);
+            f.a = v0; f.b = v1;
+            if (f.reverse) std::swap(f.a, f.b);
+            B::edge_geometry(f.a, f.b, f.length, f.normal);
+            f.area[0] = area[f.left];
+            const Quad lq = corners(f.left % nx, f.left / nx);
+            if (f.boundary) {
+                f.area[1] = f.area[0];
+                B::sampling(f.a, f.b, lq, nullptr, gp, gw, samples_n, samples_frac, f.diffusion);
+            } else {
+                f.area[1] = area[f.right];
+                const Quad rq = corners(f.right % nx, f.right / nx);
+                B::sampling(f.a, f.b, lq, &rq, gp, gw, samples_n, samples_frac, f.diffusion);
+            }
+            faces.push_back(std::move(f));
+        }
+    }
+
+    void init(const orc_material& m, const orc_transport_opts& opts) {
+        mat = m; o = opts;
+        require(B::derive(mat, der), E_OUTOFRANGE, "Invalid material parameters");
+        require(mat.alpha0 == 0.0, E_WRONG, "Adiabatic source needs cell-point velocities");
+        nx = o.nx; ny = o.ny;
+        require(nx >= 2 && ny >= 2, E_SIZ, "Transport requires at least 2x2 cells");
+        ncell = nx * ny;
+        nIedge = nx * (ny + 1);
+        nedge = nIedge + (nx + 1) * ny;
+        B::gauss_rule(nq, gp, gw);
+        build_mesh();
+        build_faces();
+        backend.setup(*this);
+        rh.resize(ncell); rc.resize(ncell);
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const int k = cell_id(i, j);
+                rh[k].init(backend, *this, i, j, std::sqrt(area[k]));
+                rc[k] = rh[k];
+            }
+        H.assign(ncell, 0); C.assign(ncell, 0); T.assign(ncell, 0); phi.assign(ncell, 0);
+        oldH.assign(ncell, 0); oldC.assign(ncell, 0);
+        lim_h.assign(ncell, 1); lim_c.assign(ncell, 1);
+        vsn.assign((size_t)nedge * nq, 0); udn.assign((size_t)nedge * nq, 0);
+        edge_phi.assign((size_t)nedge * nq, 0);
+        wet.assign(ncell, 0);
+        rhsH.assign(ncell, 0); rhsC.assign(ncell, 0); rate.assign(ncell, 0); divg.assign(ncell, 0);
+    }
+
+    // state_reconstruction.cpp:127-134 (limited evaluation)
+    void evaluate(int cell, Pt p, double& h, double& c) const {
+        h = rh[cell].evaluate(p);
+        h = H[cell] + lim_h[cell] * (h - H[cell]);
+        c = rc[cell].evaluate(p);
+        c = C[cell] + lim_c[cell] * (c - C[cell]);
+    }
+
+    // evolve.cpp:270-277
+    void phase_at(int cell, Pt p, orc_phase& s, double& h, double& c) const {
+        evaluate(cell, p, h, c);
+        int code = 0;
+        if (!B::phase(mat, der, h, c, o.pressure, s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
+        require(s.TDp >= 0 && s.phil < 1, E_OUTOFRANGE, "Coupled Darcy-Stokes requires nonnegative temperature and porosity < 1");
+    }
+
+    // state_reconstruction.cpp:101-120
+    void update() {
+        std::fill(lim_h.begin(), lim_h.end(), 1.0);
+        std::fill(lim_c.begin(), lim_c.end(), 1.0);
+        parallel_for(ncell, [&](int k) {
+            rh[k].update(H, nx, area[k]);
+            rc[k].update(C, nx, area[k]);
+        });
+    }
+
+    // Limiter point set of one cell (state_reconstruction.cpp:152-168).
+    void limiter_points(int i, int j, std::vector<Pt>& pts) const {
+        const Quad q = corners(i, j);
+        pts.clear();
+        pts.push_back(B::map_cell(Pt{0, 0}, q));
+        for (double a : gp) for (double b : gp) pts.push_back(B::map_cell(Pt{a, b}, q));
+        for (int e = 0; e < 4; ++e) {
+            const Pt a = q[e], b = q[(e + 1) % 4];
+            for (double r : gp) pts.push_back(B::map_edge(r, a, b));
+            int ni = i, nj = j;
+            if (e == 0) nj = j - 1; else if (e == 1) ni = i + 1; else if (e == 2) nj = j + 1; else ni = i - 1;
+            Sampling s;
+            if (ni < 0 || nj < 0 || ni >= nx || nj >= ny) B::sampling(a, b, q, nullptr, gp, gw, samples_n, samples_frac, s);
+            else { const Quad other = corners(ni, nj); B::sampling(a, b, q, &other, gp, gw, samples_n, samples_frac, s); }
+            for (size_t k = 0; k < s.samples.size(); ++k) if (s.sides[k] == 0) pts.push_back(s.samples[k]);
+        }
+    }
+
+    // state_reconstruction.cpp:136-192
+    void limit() {
+        parallel_for(ncell, [&](int k) {
+                    thread_local std::vector<Pt> pts;
+                    const int i = k % nx, j = k / nx;
+                    const double mean[2] = {H[k], C[k]};
+                    require(std::isfinite(mean[0]) && mean[0] >= 0 && std::isfinite(mean[1]) && mean[1] >= 0 && mean[1] <= mat.Xe,
+                            E_OUTOFRANGE, "Inadmissible cell average in coupled reconstruction");
+                    double lo[2] = {mean[0], mean[1]}, hi[2] = {mean[0], mean[1]};
+                    for (int y = std::max(0, j - 1); y < std::min(ny, j + 2); ++y)
+                        for (int x = std::max(0, i - 1); x < std::min(nx, i + 2); ++x) {
+                            const double v[2] = {H[cell_id(x, y)], C[cell_id(x, y)]};
+                            for (int z = 0; z < 2; ++z) { lo[z] = std::min(lo[z], v[z]); hi[z] = std::max(hi[z], v[z]); }
+                        }
+                    lo[0] = std::max(0.0, lo[0]); lo[1] = std::max(0.0, lo[1]);
+                    hi[1] = std::min(mat.Xe, hi[1]);
+                    limiter_points(i, j, pts);
+                    double th[2] = {1, 1};
+                    for (const Pt& p : pts) {
+                        const double v[2] = {rh[k].evaluate(p), rc[k].evaluate(p)};
+                        for (int z = 0; z < 2; ++z) {
+                            require(std::isfinite(v[z]), E_FP, "Nonfinite reconstructed state");
+                            const double delta = v[z] - mean[z];
+                            if (v[z] > hi[z]) th[z] = std::min(th[z], (hi[z] - mean[z]) / delta);
+                            if (v[z] < lo[z]) th[z] = std::min(th[z], (lo[z] - mean[z]) / delta);
+                        }
+                    }
+                    lim_h[k] = th[0] < 1 ? std::max(0.0, th[0] * (1 - 1e-13)) : 1;
+                    lim_c[k] = th[1] < 1 ? std::max(0.0, th[1] * (1 - 1e-13)) : 1;
+        });
+    }
+
+    // initial_flow.cpp:46-117 with the reconstruction present: wet cells and
+    // the edge porosity per (edge, canonical q); the last writer in cell order wins.
+    void sample_porosity() {
+        parallel_for(ncell, [&](int k) {
+                const int i = k % nx, j = k / nx;
+                const Quad q = corners(i, j);
+                bool w = false;
+                for (double x : gp) for (double y : gp) {
+                    const Pt p = B::map_cell(Pt{x, y}, q);
+                    double h, c; evaluate(k, p, h, c);
+                    orc_phase s; int code = 0;
+                    if (!B::phase(mat, der, h, c, o.pressure, s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
+                    w = w || s.phil > 0;
+                }
+                wet[k] = w;
+        });
+        // Edge samples: sequential in the reference's cell order so that the
+        // last writer of each shared edge is the same as in the reference.
+        std::vector<double> val((size_t)ncell * 4 * nq);
+        parallel_for(ncell, [&](int k) {
+                const int i = k % nx, j = k / nx;
+                const Quad q = corners(i, j);
+                for (int e = 0; e < 4; ++e) {
+                    int ni = i, nj = j;
+                    if (e == 0) nj = j - 1; else if (e == 1) ni = i + 1; else if (e == 2) nj = j + 1; else ni = i - 1;
+                    const bool bnd = ni < 0 || nj < 0 || ni >= nx || nj >= ny;
+                    for (int t = 0; t < nq; ++t) {
+                        const Pt p = B::map_edge(gp[t], q[e], q[(e + 1) % 4]);
+                        double h, c; evaluate(k, p, h, c);
+                        orc_phase s; int code = 0;
+                        if (!B::phase(mat, der, h, c, o.pressure, s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
+                        const double a = s.phil;
+                        double b = a;
+                        if (!bnd) {
+                            const int nk = cell_id(ni, nj);
+                            evaluate(nk, p, h, c);
+                            if (!B::phase(mat, der, h, c, o.pressure, s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
+                            b = s.phil;
+                        }
+                        double v = (a + b) > 0 ? 2 * a * b / (a + b) : 0;
+                        if (!wet[k]) v = 0;
+                        if (!bnd && !wet[cell_id(ni, nj)]) v = 0;
+                        val[((size_t)k * 4 + e) * nq + t] = v;
+                    }
+                }
+        });
+        for (int k = 0; k < ncell; ++k) {
+            const int i = k % nx, j = k / nx;
+            const int M = nx + 1;
+            const int ids[4] = {j * nx + i, nIedge + j * M + i + 1, (j + 1) * nx + i, nIedge + j * M + i};
+            const int dir[4] = {1, 1, -1, -1};
+            for (int e = 0; e < 4; ++e)
+                for (int t = 0; t < nq; ++t) {
+                    const int cq = dir[e] == 1 ? t : nq - 1 - t;
+                    edge_phi[(size_t)ids[e] * nq + cq] = val[((size_t)k * 4 + e) * nq + t];
+                }
+        }
+    }
+
+    // evolve.cpp:279-384
+    Rates rhs() {
+        update();
+        limit();
+        sample_porosity();
+        std::fill(rhsH.begin(), rhsH.end(), 0.0);
+        std::fill(rhsC.begin(), rhsC.end(), 0.0);
+        std::fill(rate.begin(), rate.end(), 0.0);
+        std::fill(divg.begin(), divg.end(), 0.0);
+        std::fill(T.begin(), T.end(), 0.0);
+        std::fill(phi.begin(), phi.end(), 0.0);
+        const double LD = der.LD;
+        const double theta = o.theta;
+        const size_t nf = faces.size();
+        std::vector<double> fH(nf), fC(nf), fR(nf), fM(nf);
+        parallel_for((int)nf, [&](int fi) {
+                const Face& f = faces[fi];
+                double fluxH = 0, fluxC = 0, fluxMix = 0, rt = 0;
+                for (int q = 0; q < nq; ++q) {
+                    const int cq = f.reverse ? nq - 1 - q : q;
+                    const double sgn = f.reverse ? -1.0 : 1.0;
+                    // Normal components against this face's oriented normal.
+                    const double vs = sgn * vsn[(size_t)f.edge * nq + cq];
+                    const double ud = sgn * udn[(size_t)f.edge * nq + cq];
+                    const double ephi = edge_phi[(size_t)f.edge * nq + cq];
+                    const Pt p = B::map_edge(gp[q], f.a, f.b);
+                    orc_phase a, b; double hL, cL, hR, cR;
+                    phase_at(f.left, p, a, hL, cL);
+                    if (f.boundary) { b = a; hR = hL; cR = cL; }
+                    else phase_at(f.right, p, b, hR, cR);
+                    // evolve.cpp:36-52 on normal components
+                    const double cl = .5 * (a.cl + b.cl), cs = .5 * (a.cs + b.cs);
+                    const double bulk = ephi * cl + (1 - ephi) * cs;
+                    const double factor = ephi == 0 ? 0 : std::pow(ephi, 1 + theta);
+                    const double flux = factor * ud;
+                    const double vn = vs + flux;
+                    const double ve = vs + (bulk > 0 ? cl / bulk * flux : 0);
+                    const double aH = o.lf_global ? o.lf_global_speed : std::fabs(vn);
+                    const double aC = o.lf_global ? o.lf_global_speed : std::fabs(ve);
+                    require(aH + 1e-14 >= std::fabs(vn) && aC + 1e-14 >= std::fabs(ve), E_OUTOFRANGE, "Global LF speed is below the stage flow speed");
+                    double fh = .5 * (vn * (a.TDp + b.TDp) - aH * (b.TDp - a.TDp)) - LD * (1 - ephi) * vs;
+                    double fc = .5 * (ve * (cL + cR) - aC * (cR - cL));
+                    if (f.boundary) {
+                        // initialization.cpp:469-489 per field policy
+                        auto kind = [&](int policy, double speed) {
+                            if (policy == 2 || speed == 0) return 2;          // zero flux
+                            if (speed < 0) { require(policy == 0, E_OUTOFRANGE, "Backflow encountered on an outflow-only boundary."); return 0; }
+                            return 1;                                         // extrapolated
+                        };
+                        const int kh = kind(o.H_policy, vn), kc = kind(o.C_policy, ve);
+                        const double inflowC = kc == 0 ? o.inflow_C : cL;
+                        double Tb = a.TDp;
+                        if (kh == 0) {
+                            orc_phase s; int code = 0;
+                            if (!B::phase(mat, der, o.inflow_H, inflowC, o.pressure, s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
+                            Tb = s.TDp;
+                        }
+                        fh = kh == 2 ? 0 : vn * Tb - LD * (1 - ephi) * vs;
+                        fc = kc == 2 ? 0 : ve * (kc == 0 ? o.inflow_C : cL);
+                    }
+                    const double weight = .5 * f.length * gw[q];
+                    fluxH += weight * fh; fluxC += weight * fc; fluxMix += weight * vn;
+                    const double sens = 1 + std::max(std::fabs(a.dTD_dCD), std::fabs(b.dTD_dCD));
+                    require(std::isfinite(sens), E_FP, "Singular phase derivative in CFL estimate");
+                    rt += weight * (aC + aH + 2 * std::fabs(vs)) * sens;
+                }
+                // Diffusion samples (zero diffusivity: admissibility checks only).
+                for (size_t s = 0; s < f.diffusion.samples.size(); ++s) {
+                    const int side = f.diffusion.sides[s];
+                    if (side == 2) continue;
+                    orc_phase ph; double h, c;
+                    phase_at(side == 0 ? f.left : f.right, f.diffusion.samples[s], ph, h, c);
+                }
+                fH[fi] = fluxH; fC[fi] = fluxC; fR[fi] = rt; fM[fi] = fluxMix;
+        });
+        Rates out;
+        for (size_t fi = 0; fi < nf; ++fi) {
+            const Face& f = faces[fi];
+            const double fluxH = fH[fi], fluxC = fC[fi];
+            rhsH[f.left] += -fluxH / f.area[0];
+            rhsC[f.left] += -fluxC / f.area[0];
+            rate[f.left] += fR[fi] / f.area[0];
+            divg[f.left] += fM[fi] / f.area[0];
+            if (!f.boundary) {
+                rhsH[f.right] += fluxH / f.area[1];
+                rhsC[f.right] += fluxC / f.area[1];
+                rate[f.right] += fR[fi] / f.area[1];
+                divg[f.right] += -fM[fi] / f.area[1];
+            } else {
+                out.boundaryH += fluxH; out.boundaryC += fluxC;
+            }
+        }
+        // evolve.cpp:359-376: cell quadrature of T and phi (zero adiabatic source).
+        parallel_for(ncell, [&](int k) {
+                const int i = k % nx, j = k / nx;
+                const Quad q = corners(i, j);
+                double t = 0, ph = 0;
+                for (int b = 0; b < nq; ++b)
+                    for (int a = 0; a < nq; ++a) {
+                        const Pt ref{gp[a], gp[b]};
+                        const Pt p = B::map_cell(ref, q);
+                        const double w = gw[a] * gw[b] * B::cell_jacobian(ref, q);
+                        orc_phase s; double h, c;
+                        phase_at(k, p, s, h, c);
+                        t += w / area[k] * s.TDp;
+                        ph += w / area[k] * s.phil;
+                    }
+                T[k] = t; phi[k] = ph;
+        });
+        double mx = -std::numeric_limits<double>::infinity(), dv = 0;
+        for (int k = 0; k < ncell; ++k) { mx = std::max(mx, rate[k]); dv = std::max(dv, std::fabs(divg[k])); }
+        out.maximumRate = mx;
+        out.divergence = dv;
+        require(std::isfinite(out.maximumRate), E_FP, "Nonfinite coupled stage rate");
+        return out;
+    }
+
+    // evolve.cpp:386-393
+    bool admissible() const {
+        double hmin = H[0], hmax = H[0], cmin = C[0], cmax = C[0];
+        bool fin = true;
+        for (int k = 0; k < ncell; ++k) {
+            fin = fin && std::isfinite(H[k]) && std::isfinite(C[k]);
+            hmin = std::min(hmin, H[k]); hmax = std::max(hmax, H[k]);
+            cmin = std::min(cmin, C[k]); cmax = std::max(cmax, C[k]);
+        }
+        return fin && hmin >= 0 && cmin >= 0 && cmax <= mat.Xe;
+    }
+
+    double integral(const std::vector<double>& f) const {
+        double s = 0;
+        for (int k = 0; k < ncell; ++k) s += f[k] * area[k];
+        return s;
+    }
+
+    // evolve.cpp:428-511 (SSPRK2) and the Shu-Osher SSPRK3 form of the same loop.
+    void step(orc_step_report& rep) {
+        if (!have_current) { oldH = H; oldC = C; current = rhs(); have_current = true; }
+        const double dt_cap = accepted == 0 ? o.dt_initial : o.dt_max;
+        const double start = time;
+        const double oldHI = integral(H), oldCI = integral(C);
+        const double limit = current.maximumRate > 0 ? o.cfl / current.maximumRate : o.dt_max;
+        double dt = std::min(dt_cap, limit);
+        const std::vector<double> firstH = rhsH, firstC = rhsC;
+        const Rates first = current;
+        Rates second, third;
+        int retries = 0;
+        double courant = 0;
+        std::vector<double> U1H, U1C;
+        for (;;) {
+            require(dt >= o.dt_min && retries < 40, E_NOT_CONVERGED, "Coupled step cannot satisfy admissibility/CFL above minimum step");
+            for (int k = 0; k < ncell; ++k) { H[k] = oldH[k] + dt * firstH[k]; C[k] = oldC[k] + dt * firstC[k]; }
+            time = start + dt;
+            bool valid = admissible();
+            if (valid) {
+                second = rhs();
+                courant = dt * std::max(first.maximumRate, second.maximumRate);
+                valid = courant <= o.cfl * (1 + 1e-12);
+            }
+            if (valid && o.integrator == 3) {
+                for (int k = 0; k < ncell; ++k) {
+                    H[k] = H[k] + dt * rhsH[k]; C[k] = C[k] + dt * rhsC[k];
+                    H[k] = .75 * oldH[k] + .25 * H[k]; C[k] = .75 * oldC[k] + .25 * C[k];
+                }
+                valid = admissible();
+                if (valid) {
+                    third = rhs();
+                    courant = dt * std::max(std::max(first.maximumRate, second.maximumRate), third.maximumRate);
+                    valid = courant <= o.cfl * (1 + 1e-12);
+                }
+                if (valid) {
+                    for (int k = 0; k < ncell; ++k) {
+                        H[k] = H[k] + dt * rhsH[k]; C[k] = C[k] + dt * rhsC[k];
+                        H[k] = (1.0 / 3.0) * oldH[k] + (2.0 / 3.0) * H[k];
+                        C[k] = (1.0 / 3.0) * oldC[k] + (2.0 / 3.0) * C[k];
+                    }
+                    valid = admissible();
+                }
+            } else if (valid) {
+                for (int k = 0; k < ncell; ++k) {
+                    H[k] = H[k] + dt * rhsH[k]; C[k] = C[k] + dt * rhsC[k];
+                    H[k] = .5 * oldH[k] + .5 * H[k]; C[k] = .5 * oldC[k] + .5 * C[k];
+                }
+                valid = admissible();
+            }
+            if (valid) break;
+            dt *= .5; ++retries;
+        }
+        const double HI = integral(H), CI = integral(C);
+        double bH, bC;
+        if (o.integrator == 3) {
+            bH = HI - oldHI + dt * ((first.boundaryH + second.boundaryH) / 6 + third.boundaryH * (2.0 / 3.0));
+            bC = CI - oldCI + dt * ((first.boundaryC + second.boundaryC) / 6 + third.boundaryC * (2.0 / 3.0));
+        } else {
+            bH = HI - oldHI + .5 * dt * (first.boundaryH + second.boundaryH - first.sourceH - second.sourceH);
+            bC = CI - oldCI + .5 * dt * (first.boundaryC + second.boundaryC);
+        }
+        require(std::fabs(bH) < 1e-10 * std::max(1.0, std::fabs(oldHI)) && std::fabs(bC) < 1e-10, E_PLIB,
+                "Coupled finite-volume conservation balance failed");
+        current = rhs();
+        ++accepted;
+        oldH = H; oldC = C;
+        rep.status = 0; rep.retries = retries; rep.dt = dt; rep.time = time; rep.courant = courant;
+        rep.boundaryH = o.integrator == 3 ? (first.boundaryH + second.boundaryH) / 6 + third.boundaryH * (2.0 / 3.0) : .5 * (first.boundaryH + second.boundaryH);
+        rep.boundaryC = o.integrator == 3 ? (first.boundaryC + second.boundaryC) / 6 + third.boundaryC * (2.0 / 3.0) : .5 * (first.boundaryC + second.boundaryC);
+        rep.sourceH = 0; rep.maxRate = current.maximumRate; rep.divergence = current.divergence;
+        rep.balanceH = bH; rep.balanceC = bC; rep.H_integral = HI; rep.C_integral = CI;
+    }
+};
+
+
+// Handle + C API bodies shared by the restated oracle (orc_*) and the
+// reference-backed oracle (ref_*); each library instantiates it once.
+template <class B>
+struct Handle {
+    Driver<B> d;
+};
+
+template <class B>
+struct Api {
+    static void* create(const orc_material* m, const orc_transport_opts* o) {
+        oracle_threads() = o->threads;
+        Handle<B>* t = new Handle<B>;
+        try { t->d.init(*m, *o); } catch (const Error&) { delete t; return nullptr; }
+        return t;
+    }
+    static void destroy(void* h) { delete static_cast<Handle<B>*>(h); }
+    static int set_face_velocity(void* h, const double* vs_n, const double* ud_n) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        const size_t n = (size_t)d.nedge * d.nq;
+        std::copy(vs_n, vs_n + n, d.vsn.begin());
+        std::copy(ud_n, ud_n + n, d.udn.begin());
+        d.have_current = false;
+        return 0;
+    }
+    static int set_state(void* h, const double* H, const double* C, double time) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        std::copy(H, H + d.ncell, d.H.begin());
+        std::copy(C, C + d.ncell, d.C.begin());
+        d.time = time; d.accepted = 0; d.have_current = false;
+        return 0;
+    }
+    static int get_state(const void* h, double* H, double* C, double* T, double* phi) {
+        const auto& d = static_cast<const Handle<B>*>(h)->d;
+        if (H) std::copy(d.H.begin(), d.H.end(), H);
+        if (C) std::copy(d.C.begin(), d.C.end(), C);
+        if (T) std::copy(d.T.begin(), d.T.end(), T);
+        if (phi) std::copy(d.phi.begin(), d.phi.end(), phi);
+        return 0;
+    }
+    static int rhs(void* h, double* rhsH, double* rhsC, double* T, double* phi, double* rate, orc_step_report* rep) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        try {
+            const auto r = d.rhs();
+            if (rhsH) std::copy(d.rhsH.begin(), d.rhsH.end(), rhsH);
+            if (rhsC) std::copy(d.rhsC.begin(), d.rhsC.end(), rhsC);
+            if (T) std::copy(d.T.begin(), d.T.end(), T);
+            if (phi) std::copy(d.phi.begin(), d.phi.end(), phi);
+            if (rate) std::copy(d.rate.begin(), d.rate.end(), rate);
+            if (rep) {
+                *rep = orc_step_report{};
+                rep->boundaryH = r.boundaryH; rep->boundaryC = r.boundaryC; rep->sourceH = r.sourceH;
+                rep->maxRate = r.maximumRate; rep->divergence = r.divergence;
+            }
+            return 0;
+        } catch (const Error& e) { return e.code; }
+    }
+    static int limiter(void* h, double* thetaH, double* thetaC) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        try {
+            d.update(); d.limit();
+            std::copy(d.lim_h.begin(), d.lim_h.end(), thetaH);
+            std::copy(d.lim_c.begin(), d.lim_c.end(), thetaC);
+            return 0;
+        } catch (const Error& e) { return e.code; }
+    }
+    static int step(void* h, int nsteps, orc_step_report* report) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        for (int s = 0; s < nsteps; ++s) {
+            const double t0 = d.time;
+            std::vector<double> h0 = d.H, c0 = d.C;
+            try {
+                orc_step_report r{};
+                d.step(r);
+                if (report) report[s] = r;
+            } catch (const Error& e) {
+                // evolve.cpp:493-499: roll back to the latest accepted state.
+                d.time = t0; d.H = h0; d.C = c0; d.have_current = false;
+                if (report) { report[s] = orc_step_report{}; report[s].status = e.code; }
+                return e.code;
+            }
+        }
+        return 0;
+    }
+};
+
+}  // namespace orc
+
+#endif
