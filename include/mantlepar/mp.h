@@ -1,0 +1,205 @@
+/*
+ * mantlepar_b200 C ABI: the drop-in boundary of the MantlePar ML-WENO H/C
+ * transport + eutectic phase hot path on NVIDIA B200 (sm_100a).
+ *
+ * Plain C: opaque handles, caller-owned buffers, status codes, no exceptions
+ * and no C++ or torch types cross this boundary. Every entry point returns an
+ * mp_status (0 = success) and assigns its outputs only on success unless
+ * stated otherwise; mp_last_error_string() describes the last failure of the
+ * calling thread. Handles are not thread-safe; use one handle per stream.
+ *
+ * Array layouts follow the reference:
+ *  - cell fields: natural order id = j*nx + i, x fastest
+ *    (src/couple/evolve.cpp:66, src/couple/initialization.h:137-139);
+ *  - edges: reference MeshInfo ids (src/core/mesh_info.h:84): AlongI edges
+ *    j*nx + i (j = 0..ny) first, then AlongJ edges nx*(ny+1) + j*(nx+1) + i;
+ *  - edge Gauss points: 5 per edge along the canonical direction (increasing
+ *    i or j, src/core/mesh_info.h:37), normal components against the
+ *    canonical right normal (dy,-dx)/length (src/core/integral.cpp:62-89).
+ * Pointers given to set/get calls may be host or device memory (UVA).
+ */
+#ifndef MANTLEPAR_MP_H
+#define MANTLEPAR_MP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* mp_stream_t; /* == cudaStream_t; NULL = default stream */
+
+/* Status classes mirror the PETSc error classes the reference raises on this
+ * path (numeric values are project-defined; PETSc's are not vendored), plus
+ * the three exception classes of src/phase/eutectic_rescaled.h:111-113. */
+typedef enum mp_status {
+    MP_OK = 0,
+    MP_ERR_ARG_SIZ = 60,          /* PETSC_ERR_ARG_SIZ */
+    MP_ERR_ARG_WRONG = 62,        /* PETSC_ERR_ARG_WRONG */
+    MP_ERR_ARG_OUTOFRANGE = 63,   /* PETSC_ERR_ARG_OUTOFRANGE */
+    MP_ERR_FP = 72,               /* PETSC_ERR_FP */
+    MP_ERR_ARG_WRONGSTATE = 73,   /* PETSC_ERR_ARG_WRONGSTATE */
+    MP_ERR_PLIB = 77,             /* PETSC_ERR_PLIB (conservation balance) */
+    MP_ERR_NOT_CONVERGED = 91,    /* PETSC_ERR_NOT_CONVERGED (step retries) */
+    MP_ERR_PHASE_INVALID = 101,   /* std::invalid_argument from EutecticModel */
+    MP_ERR_PHASE_OVERFLOW = 102,  /* std::overflow_error from EutecticModel */
+    MP_ERR_PHASE_RUNTIME = 103,   /* std::runtime_error from EutecticModel */
+    MP_ERR_TIMEOUT = 110,         /* a bounded device wait ran out */
+    MP_ERR_NOMEM = 111,           /* device memory exhausted / admission refused */
+    MP_ERR_CUDA = 112             /* CUDA runtime error */
+} mp_status;
+
+/* Last failure of the calling thread (static storage, never NULL). */
+const char* mp_last_error_string(void);
+
+/* ------------------------------------------------------------------ phase */
+
+/* Replaces mantle::phase::MaterialParameters (src/phase/eutectic_rescaled.h:10-26). */
+typedef struct mp_material {
+    double Tm0, Te0, nu, L, cp, Xe, rho, rhor, mus, mul, k0, g, alpha0;
+} mp_material;
+
+/* Replaces mantle::phase::DerivedParameters (src/phase/eutectic_rescaled.h:29-41). */
+typedef struct mp_derived {
+    double dT, h0, gamma, LD, TDm0, TDe0, invk0, l0, u0, p0, t0;
+} mp_derived;
+
+/* Replaces mantle::phase::PhaseBoundaries (src/phase/eutectic_rescaled.h:52-57). */
+typedef struct mp_phase_bounds {
+    double Tep, Tmp, H_eutectic_end, H_liquidus;
+} mp_phase_bounds;
+
+/* Structure-of-arrays output of a phase batch (device pointers). Any pointer
+ * may be NULL to skip that field. region holds mantle::phase::PhaseRegion
+ * values 1..6 (src/phase/eutectic_rescaled.h:43-50); flags bit 0 has_solid,
+ * bit 1 has_liquid, bit 2 finite_temperature_derivatives. */
+typedef struct mp_phase_soa {
+    double *phi1, *phi2, *phil, *cl, *cs, *TDp, *Tep, *dTD_dCD, *dTD_dHD;
+    int8_t* region;
+    uint8_t* flags;
+} mp_phase_soa;
+
+typedef struct mp_phase_model mp_phase_model;
+
+/* Replaces EutecticModel::EutecticModel / setParameters
+ * (src/phase/eutectic_rescaled.h:105,109; .cpp:42-86,137-141). Invalid
+ * parameters -> MP_ERR_PHASE_INVALID / MP_ERR_PHASE_OVERFLOW; a rejected
+ * update leaves the model unchanged. */
+mp_status mp_phase_create(const mp_material* params, mp_phase_model** model);
+mp_status mp_phase_set_params(mp_phase_model* model, const mp_material* params);
+mp_status mp_phase_get_params(const mp_phase_model* model, mp_material* params);
+mp_status mp_phase_get_derived(const mp_phase_model* model, mp_derived* derived);
+void mp_phase_destroy(mp_phase_model* model);
+
+/* Replaces EutecticModel::boundaries (src/phase/eutectic_rescaled.h:116,
+ * .cpp:163-185). Host computation with the same FP64 operations the kernels use. */
+mp_status mp_phase_boundaries(const mp_phase_model* model, double C, double P, mp_phase_bounds* out);
+
+/* Batched EutecticModel::evaluate (src/phase/eutectic_rescaled.h:114,
+ * .cpp:192-282) on the GPU. H, C, P are device arrays of length n; P may be
+ * NULL, then P_const applies to every point. Returns the status of the
+ * lowest failing index (written to *first_bad, -1 if none). Synchronous on
+ * `stream`. On failure the failing points hold NaN (region 0) and the other
+ * points hold their values. */
+mp_status mp_phase_evaluate_batch(const mp_phase_model* model, const double* H, const double* C,
+                                  const double* P, double P_const, size_t n,
+                                  const mp_phase_soa* out, long long* first_bad, mp_stream_t stream);
+
+/* ------------------------------------------------------------- transport */
+
+/* Uniform rectangular mesh (src/core/mesh.cpp:27-55, uniform family). */
+typedef struct mp_mesh_desc {
+    int nx, ny;            /* cells per axis, >= 2 each */
+    double x0, x1, y0, y1; /* domain */
+} mp_mesh_desc;
+
+enum { MP_BC_INFLOW_OUTFLOW = 0, MP_BC_OUTFLOW = 1, MP_BC_ZERO_FLUX = 2 };
+enum { MP_SSPRK2 = 2, MP_SSPRK3 = 3 };
+enum { MP_PRECISION_FP64 = 0, MP_PRECISION_MIXED = 1 };
+
+/* Subset of mantle::couple::Configuration used on this path
+ * (src/couple/initialization.cpp:132-164,236-244,266-279; input.h:154-159). */
+typedef struct mp_transport_opts {
+    mp_material material;
+    double pressure;          /* constant pressure model [Pa] */
+    double cfl;               /* time.step.cfl, in (0,1] */
+    double dt_initial, dt_max, dt_min;
+    double theta;             /* flow.material.theta (Darcy exponent) */
+    double inflow_H, inflow_C;/* inflow_outflow reservoir values */
+    int H_policy, C_policy;   /* MP_BC_* for enthalpy / composition */
+    int integrator;           /* MP_SSPRK2 (reference) or MP_SSPRK3 */
+    int lf_global;            /* 0 local Lax-Friedrichs, 1 global */
+    double lf_global_speed;
+    double diffusivity;       /* thermal diffusivity kappa; only 0 is supported */
+    int precision;            /* MP_PRECISION_FP64 or MP_PRECISION_MIXED */
+} mp_transport_opts;
+
+/* Per accepted step (history columns of src/couple/evolve.cpp:399-418,443). */
+typedef struct mp_step_report {
+    int status, retries;
+    double dt, time, courant;
+    double boundaryH, boundaryC, sourceH, maxRate, divergence;
+    double balanceH, balanceC, H_integral, C_integral;
+} mp_step_report;
+
+/* Totals of one stage evaluation (Rates in src/couple/evolve.cpp:156). */
+typedef struct mp_stage_totals {
+    double boundaryH, boundaryC, sourceH, maxRate, divergence;
+} mp_stage_totals;
+
+typedef struct mp_transport mp_transport;
+
+/* Replaces the setup half of mantle::couple::AdvancePhaseCoupled
+ * (src/couple/evolve.h:17; Build at evolve.cpp:221-268 and
+ * StateReconstruction::Initialize at state_reconstruction.cpp:35-96). */
+mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_transport_opts* opts,
+                              mp_stream_t stream, mp_transport** out);
+void mp_transport_destroy(mp_transport* t);
+
+/* Flow supplier output (stays on PETSc in a coupled run): normal solid and
+ * Darcy velocity at every edge Gauss point, arrays of edges*5 doubles.
+ * Replaces the samples of SampleInitialFlow (src/couple/flow_sampling.cpp:62-121). */
+mp_status mp_transport_set_face_velocity(mp_transport* t, const double* vs_n, const double* ud_n);
+
+/* Cell averages H, C (length nx*ny) and the clock; resets accepted steps
+ * (LoadPreheatState semantics, src/couple/evolve.cpp:54-125). */
+mp_status mp_transport_set_state(mp_transport* t, const double* H, const double* C, double time);
+/* Current H, C and the cell-averaged T, phi of the latest stage evaluation;
+ * any pointer may be NULL. */
+mp_status mp_transport_get_state(mp_transport* t, double* H, double* C, double* T, double* phi);
+
+/* One stage evaluation L(U) of the current state (RHS, src/couple/evolve.cpp:279-384).
+ * Outputs (length nx*ny, host or device) may be NULL. */
+mp_status mp_transport_rhs(mp_transport* t, double* rhsH, double* rhsC, double* T, double* phi,
+                           double* rate, mp_stage_totals* totals);
+
+/* Advance nsteps accepted steps (the time loop of src/couple/evolve.cpp:428-511);
+ * reports (may be NULL) receives one entry per step. On failure the state
+ * is rolled back to the last accepted step (evolve.cpp:493-499). */
+mp_status mp_transport_step(mp_transport* t, int nsteps, mp_step_report* reports);
+
+/* Limiter factors theta_H, theta_C of the current state
+ * (StateReconstruction::Limit, src/couple/state_reconstruction.cpp:136-192). */
+mp_status mp_transport_limiter(mp_transport* t, double* thetaH, double* thetaC);
+
+/* ------------------------------------------------------------ measurement */
+
+/* Number of this library's kernel launches issued so far (all handles). */
+unsigned long long mp_kernel_launches(void);
+
+/* Per-kernel CUDA-event timing of a handle's stage kernels (no counterpart in
+ * the reference, which has no timers on this path). enable resets the
+ * accumulators; kernel_times returns accumulated ms and launch counts for
+ * [0] cell kernel, [1] face kernel, [2] sum kernel, [3] axpy/reductions. */
+mp_status mp_transport_profile(mp_transport* t, int enable);
+mp_status mp_transport_kernel_times(mp_transport* t, double ms[4], unsigned long long launches[4]);
+
+/* Measured FP64 FMA throughput of this GPU (TFLOP/s), the compute roof of
+ * this FP64-bound path. */
+mp_status mp_probe_fp64_peak(mp_stream_t stream, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,134 @@
+"""ctypes binding of the mantlepar_b200 C ABI (include/mantlepar/mp.h).
+
+The CUDA library is loaded from the package directory; there is no CPU
+fallback: if it is missing, importing the bindings fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libmantlepar_b200.so")
+HEADER = os.path.join(ROOT, "include", "mantlepar", "mp.h")
+
+STATUS = {
+    0: "MP_OK", 60: "MP_ERR_ARG_SIZ", 62: "MP_ERR_ARG_WRONG", 63: "MP_ERR_ARG_OUTOFRANGE",
+    72: "MP_ERR_FP", 73: "MP_ERR_ARG_WRONGSTATE", 77: "MP_ERR_PLIB", 91: "MP_ERR_NOT_CONVERGED",
+    101: "MP_ERR_PHASE_INVALID", 102: "MP_ERR_PHASE_OVERFLOW", 103: "MP_ERR_PHASE_RUNTIME",
+    110: "MP_ERR_TIMEOUT", 111: "MP_ERR_NOMEM", 112: "MP_ERR_CUDA",
+}
+
+
+class MPError(RuntimeError):
+    """A failed mantlepar_b200 call; `code` is the mp_status value."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS.get(code, code)}: {message}")
+        self.code = code
+
+
+class Material(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ["Tm0", "Te0", "nu", "L", "cp", "Xe", "rho", "rhor", "mus", "mul", "k0", "g", "alpha0"]]
+
+
+class Derived(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ["dT", "h0", "gamma", "LD", "TDm0", "TDe0", "invk0", "l0", "u0", "p0", "t0"]]
+
+
+class Bounds(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ["Tep", "Tmp", "H_eutectic_end", "H_liquidus"]]
+
+
+class PhaseSoA(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in
+                ["phi1", "phi2", "phil", "cl", "cs", "TDp", "Tep", "dTD_dCD", "dTD_dHD", "region", "flags"]]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("x0", C.c_double), ("x1", C.c_double),
+                ("y0", C.c_double), ("y1", C.c_double)]
+
+
+class TransportOpts(C.Structure):
+    _fields_ = [("material", Material), ("pressure", C.c_double), ("cfl", C.c_double),
+                ("dt_initial", C.c_double), ("dt_max", C.c_double), ("dt_min", C.c_double),
+                ("theta", C.c_double), ("inflow_H", C.c_double), ("inflow_C", C.c_double),
+                ("H_policy", C.c_int), ("C_policy", C.c_int), ("integrator", C.c_int),
+                ("lf_global", C.c_int), ("lf_global_speed", C.c_double), ("diffusivity", C.c_double),
+                ("precision", C.c_int)]
+
+
+class StepReport(C.Structure):
+    _fields_ = [("status", C.c_int), ("retries", C.c_int), ("dt", C.c_double), ("time", C.c_double),
+                ("courant", C.c_double), ("boundaryH", C.c_double), ("boundaryC", C.c_double),
+                ("sourceH", C.c_double), ("maxRate", C.c_double), ("divergence", C.c_double),
+                ("balanceH", C.c_double), ("balanceC", C.c_double), ("H_integral", C.c_double),
+                ("C_integral", C.c_double)]
+
+
+class StageTotals(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ["boundaryH", "boundaryC", "sourceH", "maxRate", "divergence"]]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load (once) the CUDA library; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"mantlepar_b200 CUDA library missing: {LIB_PATH} "
+                           "(build it with `python -m mantlepar_b200.build`)")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, i, d, sz = C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_size_t
+    sig = {
+        "mp_last_error_string": (C.c_char_p, []),
+        "mp_kernel_launches": (C.c_ulonglong, []),
+        "mp_phase_create": (i, [C.POINTER(Material), C.POINTER(vp)]),
+        "mp_phase_set_params": (i, [vp, C.POINTER(Material)]),
+        "mp_phase_get_params": (i, [vp, C.POINTER(Material)]),
+        "mp_phase_get_derived": (i, [vp, C.POINTER(Derived)]),
+        "mp_phase_destroy": (None, [vp]),
+        "mp_phase_boundaries": (i, [vp, d, d, C.POINTER(Bounds)]),
+        "mp_phase_evaluate_batch": (i, [vp, vp, vp, vp, d, sz, C.POINTER(PhaseSoA), C.POINTER(C.c_longlong), vp]),
+        "mp_transport_create": (i, [C.POINTER(MeshDesc), C.POINTER(TransportOpts), vp, C.POINTER(vp)]),
+        "mp_transport_destroy": (None, [vp]),
+        "mp_transport_set_face_velocity": (i, [vp, vp, vp]),
+        "mp_transport_set_state": (i, [vp, vp, vp, d]),
+        "mp_transport_get_state": (i, [vp, vp, vp, vp, vp]),
+        "mp_transport_rhs": (i, [vp, vp, vp, vp, vp, vp, C.POINTER(StageTotals)]),
+        "mp_transport_step": (i, [vp, i, C.POINTER(StepReport)]),
+        "mp_transport_limiter": (i, [vp, vp, vp]),
+        "mp_transport_profile": (i, [vp, i]),
+        "mp_transport_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
+        "mp_probe_fp64_peak": (i, [vp, C.POINTER(C.c_double)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(code: int) -> None:
+    if code != 0:
+        raise MPError(code, lib().mp_last_error_string().decode())
+
+
+def header_functions() -> list[str]:
+    """Names of the functions declared in include/mantlepar/mp.h."""
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mp_[a-z0-9_]+)\s*\(", text)))
+
+
+def kernel_launches() -> int:
+    return int(lib().mp_kernel_launches())

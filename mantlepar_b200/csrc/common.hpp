@@ -1,0 +1,42 @@
+// Shared host-side plumbing of the mantlepar_b200 C ABI: status strings,
+// CUDA error mapping and the kernel launch counter.
+#ifndef MP_COMMON_HPP
+#define MP_COMMON_HPP
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+
+#include "../../include/mantlepar/mp.h"
+
+namespace mp {
+
+void set_error(const char* fmt, ...);
+extern std::atomic<unsigned long long> g_launches;
+
+inline void count_launch(unsigned long long n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Map a CUDA error to MP_ERR_CUDA (or MP_ERR_NOMEM) and record its text.
+inline mp_status cuda_status(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return MP_OK;
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? MP_ERR_NOMEM : MP_ERR_CUDA;
+}
+
+}  // namespace mp
+
+#define MP_CUDA(call)                                                        \
+    do {                                                                     \
+        cudaError_t mp_e_ = (call);                                          \
+        if (mp_e_ != cudaSuccess) return ::mp::cuda_status(mp_e_, #call);   \
+    } while (0)
+
+#define MP_TRY(call)                                                         \
+    do {                                                                     \
+        mp_status mp_s_ = (call);                                            \
+        if (mp_s_ != MP_OK) return mp_s_;                                    \
+    } while (0)
+
+#endif

@@ -1,0 +1,54 @@
+// Per-mesh tables of the uniform-mesh ML-WENO stage (host-built, read by
+// the kernels from global memory).
+//
+// On a uniform rectangular mesh every interior cell has the same stencil
+// geometry up to a translation, so the reference's per-cell setup
+// (TensorStencilPoly::Initialize, src/mlweno/tensorstencilpoly.cpp:146-231;
+// SetTargetSmoothness :383-398; Reconstruction::Initialize,
+// src/mlweno/reconstruction.cpp:109-210; the limiter point set,
+// src/couple/state_reconstruction.cpp:152-168; diffusion sample geometry,
+// src/mlweno/diffusiveflux.cpp:255-334) collapses to one table set per
+// mesh, with nine boundary classes (left/interior/right x bottom/interior/top)
+// for the candidate mask and the limiter points. All coordinates are in the
+// target cell's normalised frame xi = (x - x_c)/h, h = sqrt(cell area).
+#ifndef MP_TABLES_HPP
+#define MP_TABLES_HPP
+
+namespace mp {
+
+constexpr int kMaxPoints = 1024;   // limiter points over all 9 classes
+constexpr int kNQ = 5;             // Gauss points per edge / per cell axis
+
+struct StageTables {
+    // 3x3 candidate (order 2): basis coefficients C9[cell][monomial]
+    // (monomial m = j*3 + i for xi^i eta^j) and the reference-square
+    // smoothness matrix on the differences to stencil cell 0 (rows/cols 1..8).
+    double C9[9][9];
+    double S9[8][8];
+    // 2x2 candidates (order 1) in the stencil's own frame (centre = the shared
+    // vertex): coefficients and the target-cell smoothness matrix for target
+    // position t = tj*2 + ti (rows/cols 1..3 of the difference form).
+    double C4[4][4];
+    double S4[4][3][3];
+    double X, Y;            // half cell extents in the normalised frame
+    double epsA;            // epsilon * cell area of the weight regulariser
+    double area;            // cell area (1-point rule, as MeshInfo::CacheAreas)
+    double len_h, len_v;    // lengths of AlongI (horizontal) / AlongJ edges
+    double gq[kNQ];         // Gauss points on [-1,1]
+    double gw[kNQ];         // Gauss weights
+    double cw[kNQ * kNQ];   // cell-quadrature weight / area, q = b*5 + a
+    // Limiter points of class c in [pt_off[c], pt_off[c+1]); pt_kind 1 marks
+    // a diffusion sample point (checked for admissibility in the stage).
+    int pt_off[10];
+    double pt_x[kMaxPoints];
+    double pt_y[kMaxPoints];
+    unsigned char pt_kind[kMaxPoints];
+};
+
+// Build the tables of an nx x ny uniform mesh on [x0,x1] x [y0,y1].
+// Returns 0 or an mp_status code (stencil solve failure).
+int build_stage_tables(int nx, int ny, double x0, double x1, double y0, double y1, StageTables& t);
+
+}  // namespace mp
+
+#endif

@@ -1,0 +1,143 @@
+"""GPU parity of the FP64 transport stage and time loop against the reference.
+
+The golden arrays come from the reference's own classes (oracle/_ref); the
+per-cell relative error of a state field is |x - ref| / max(|ref|, 1e-3 *
+max|ref|) and the FP64 bar is 1e-12 per cell for one stage and for short
+runs. Stage right-hand sides are sums of face fluxes of both signs, so their
+error is measured against their infinity norm (same 1e-12 bar). Over 200
+steps the FP64 (GPU) and 80-bit (reference) roundings drift apart slowly;
+that bound (1e-10) is stated in the test.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from mantlepar_b200 import synthetic as sy
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = np.load(os.path.join(os.path.dirname(__file__), "golden", "transport_golden.npz"))
+CASES = {"w20": sy.Workload(nx=20, ny=20), "w2x2": sy.Workload(nx=2, ny=2),
+         "w3x5": sy.Workload(nx=3, ny=5, seed=7), "w7x4": sy.Workload(nx=7, ny=4, seed=9, noise_H=0.1)}
+RTOL_STAGE = 1e-12
+RTOL_RUN10 = 1e-12
+RTOL_RUN200 = 1e-10
+
+
+def rel(a, b):
+    b = np.asarray(b)
+    return np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-3 * max(np.max(np.abs(b)), 1e-300)))
+
+
+def rel_inf(a, b):
+    b = np.asarray(b)
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+def make(w, integrator=2):
+    from mantlepar_b200.transport import Transport, TransportConfig
+    t = Transport(w, TransportConfig(cfl=w.cfl, integrator=integrator))
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    t.set_face_velocity(vs, ud)
+    t.set_state(H, C)
+    return t
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_stage_rhs_matches_reference(cuda_lib, name):
+    t = make(CASES[name])
+    r = t.rhs()
+    for k in ["T", "phi", "rate"]:
+        e = rel(r[k], GOLDEN[f"{name}_rhs_{k}"])
+        assert e <= RTOL_STAGE, (k, e)
+    for k in ["rhsH", "rhsC"]:
+        e = rel_inf(r[k], GOLDEN[f"{name}_rhs_{k}"])
+        assert e <= RTOL_STAGE, (k, e)
+    tot = GOLDEN[f"{name}_rhs_totals"]
+    assert abs(r["maxRate"] - tot[2]) <= RTOL_STAGE * tot[2]
+    assert abs(r["boundaryH"] - tot[0]) <= 1e-12 * max(1.0, abs(tot[0]))
+    assert abs(r["boundaryC"] - tot[1]) <= 1e-12 * max(1.0, abs(tot[1]))
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_limiter_matches_reference(cuda_lib, name):
+    t = make(CASES[name])
+    a, b = t.limiter()
+    assert np.max(np.abs(a - GOLDEN[f"{name}_thetaH"])) <= 1e-12
+    assert np.max(np.abs(b - GOLDEN[f"{name}_thetaC"])) <= 1e-12
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("integ", [2, 3])
+def test_ten_steps_match_reference(cuda_lib, name, integ):
+    t = make(CASES[name], integ)
+    _, reps = t.step(10)
+    got = np.stack(t.get_state())
+    ref = GOLDEN[f"{name}_rk{integ}_10"]
+    for k, label in enumerate(["H", "C", "T", "phi"]):
+        assert rel(got[k], ref[k]) <= RTOL_RUN10, (label, rel(got[k], ref[k]))
+    assert [r["retries"] for r in reps] == list(GOLDEN[f"{name}_rk{integ}_10_retries"])
+    dt = np.array([r["dt"] for r in reps])
+    assert rel(dt, GOLDEN[f"{name}_rk{integ}_10_dt"]) <= RTOL_RUN10
+
+
+@pytest.mark.parametrize("integ", [2, 3])
+def test_200_steps_match_reference(cuda_lib, integ):
+    t = make(CASES["w20"], integ)
+    _, reps = t.step(200)
+    got = np.stack(t.get_state())
+    ref = GOLDEN[f"w20_rk{integ}_200"]
+    errs = {label: rel(got[k], ref[k]) for k, label in enumerate(["H", "C", "T", "phi"])}
+    assert max(errs.values()) <= RTOL_RUN200, errs
+    for r in reps:
+        assert abs(r["balanceH"]) < 1e-12 and abs(r["balanceC"]) < 1e-12
+        assert r["courant"] <= 0.4 * (1 + 1e-10)
+
+
+def test_deterministic(cuda_lib):
+    a, b = make(CASES["w20"], 3), make(CASES["w20"], 3)
+    a.step(7)
+    b.step(7)
+    for x, y in zip(a.get_state(), b.get_state()):
+        assert np.array_equal(x, y)
+
+
+def test_large_mesh_properties(cuda_lib):
+    """A 320x640 instance: conservation, admissibility and CFL every step."""
+    w = sy.Workload(nx=320, ny=640, seed=5)
+    t = make(w, 3)
+    _, reps = t.step(5)
+    H, C, T, phi = t.get_state()
+    assert H.min() >= 0 and C.min() >= 0 and C.max() <= 0.5
+    assert np.all((phi >= 0) & (phi < 1)) and np.all(T >= 0)
+    for r in reps:
+        assert abs(r["balanceH"]) < 1e-10 * max(1.0, abs(r["H_integral"])) and abs(r["balanceC"]) < 1e-10
+        assert r["courant"] <= w.cfl * (1 + 1e-12)
+
+
+def test_inadmissible_state_is_an_error_and_rolls_back(cuda_lib):
+    from mantlepar_b200._capi import MPError
+    w = CASES["w3x5"]
+    t = make(w)
+    H, C = sy.initial_state(w)
+    C = C.copy()
+    C[4] = 0.7
+    t.set_state(H, C)
+    with pytest.raises(MPError) as err:
+        t.step(1)
+    assert err.value.code == 63
+    H2, C2, _, _ = t.get_state()
+    assert np.array_equal(C2, C) and np.array_equal(H2, H)
+
+
+def test_invalid_configurations_are_rejected(cuda_lib):
+    from mantlepar_b200._capi import MPError
+    from mantlepar_b200.transport import Transport, TransportConfig
+    with pytest.raises(MPError):
+        Transport(sy.Workload(nx=1, ny=4))
+    with pytest.raises(MPError):
+        Transport(sy.Workload(nx=4, ny=4), TransportConfig(cfl=1.5))
+    with pytest.raises(MPError):
+        Transport(sy.Workload(nx=4, ny=4), TransportConfig(diffusivity=1e-3))

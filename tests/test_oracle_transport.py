@@ -1,0 +1,95 @@
+"""The transport oracle against the reference-backed build and the golden runs."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from mantlepar_b200 import synthetic as sy
+
+GOLDEN = np.load(os.path.join(os.path.dirname(__file__), "golden", "transport_golden.npz"))
+CASES = {"w20": sy.Workload(nx=20, ny=20), "w2x2": sy.Workload(nx=2, ny=2),
+         "w3x5": sy.Workload(nx=3, ny=5, seed=7), "w7x4": sy.Workload(nx=7, ny=4, seed=9, noise_H=0.1)}
+
+
+def _oracle(w, integrator=2, lib=None, **kw):
+    t = po.TransportOracle(sy.material_s(), w, lib=lib, integrator=integrator, **kw)
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    t.set_face_velocity(vs, ud)
+    t.set_state(H, C)
+    return t
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.int64)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_restated_rhs_equals_golden_bitwise(name):
+    t = _oracle(CASES[name])
+    code, r = t.rhs()
+    assert code == 0
+    for k in ["rhsH", "rhsC", "T", "phi", "rate"]:
+        assert np.array_equal(bits(r[k]), bits(GOLDEN[f"{name}_rhs_{k}"])), k
+    code, a, b = t.limiter()
+    assert code == 0
+    assert np.array_equal(bits(a), bits(GOLDEN[f"{name}_thetaH"]))
+    assert np.array_equal(bits(b), bits(GOLDEN[f"{name}_thetaC"]))
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("integ", [2, 3])
+def test_restated_steps_equal_golden_bitwise(name, integ):
+    t = _oracle(CASES[name], integ)
+    code, reps = t.step(10)
+    assert code == 0
+    st = np.stack(t.get_state())
+    assert np.array_equal(bits(st), bits(GOLDEN[f"{name}_rk{integ}_10"]))
+    assert np.array_equal(np.array([r["retries"] for r in reps]), GOLDEN[f"{name}_rk{integ}_10_retries"])
+
+
+def test_oracle_conservation_and_cfl():
+    """Per-step balance (evolve.cpp:486-490, integration-test bound 1e-12) and courant <= cfl."""
+    w = CASES["w20"]
+    t = _oracle(w, 2)
+    code, reps = t.step(25)
+    assert code == 0
+    for r in reps:
+        assert abs(r["balanceH"]) < 1e-12 and abs(r["balanceC"]) < 1e-12
+        assert r["courant"] <= w.cfl * (1 + 1e-10)
+    H, C, T, phi = t.get_state()
+    assert H.min() >= 0 and C.min() >= 0 and C.max() <= sy.material_s().Xe
+    assert np.all((phi >= 0) & (phi < 1))
+
+
+def test_uniform_tables_match_per_cell_tables():
+    """Sharing one table set per boundary class moves results only at roundoff."""
+    w = sy.Workload(nx=12, ny=16, seed=3)
+    a = _oracle(w, 3)
+    b = _oracle(w, 3, uniform_tables=True)
+    assert a.step(5)[0] == 0 and b.step(5)[0] == 0
+    for x, y in zip(a.get_state(), b.get_state()):
+        assert np.max(np.abs(x - y) / np.maximum(np.abs(y), 1e-3)) < 1e-13
+
+
+def test_inadmissible_state_rejected_and_rolled_back():
+    w = CASES["w3x5"]
+    t = _oracle(w)
+    H, C = sy.initial_state(w)
+    C = C.copy()
+    C[4] = 0.7          # above Xe = 0.5
+    t.set_state(H, C)
+    code, _ = t.step(1)
+    assert code != 0
+    H2, C2, _, _ = t.get_state()
+    assert np.array_equal(C2, C)   # state untouched
+
+
+@pytest.mark.skipif(not po.reference_available(), reason="reference build (oracle/_ref) not present")
+def test_restated_equals_reference_on_new_seed():
+    w = sy.Workload(nx=9, ny=11, seed=123, noise_H=0.08, psi_amplitude=0.15)
+    a = _oracle(w, 3)
+    b = _oracle(w, 3, lib=po.reference())
+    assert a.step(6)[0] == 0 and b.step(6)[0] == 0
+    assert np.array_equal(bits(np.stack(a.get_state())), bits(np.stack(b.get_state())))
