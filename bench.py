@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark of the MantlePar ML-WENO H/C transport + eutectic phase hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mantlepar_b200|reference]
+
+Metric: cell-updates/s (one cell advanced one accepted SSP-RK time step, all
+stages). Workload (N=1): the plain FP64 single large instance, 1280x2560 uniform
+quads on [0,0.5]x[0,1], seeded synthetic H/C/psi/Darcy data, SSPRK3 at CFL 0.4
+(the reference integrates with SSPRK2; both are built). A bench step is one
+accepted time step. The per-stage working set (~1.1 GB) exceeds the 126 MB L2,
+so no flush is needed between steps.
+
+value      device-timed (CUDA events) throughput with state resident in HBM;
+e2e        the same metric through the C ABI with host buffers: per step the
+           face velocities and H/C go host->device from pinned memory, the step
+           runs, and H/C/T/phi come back device->host;
+roofline   one stage evaluation (cell + face + sum kernels) counted as one launch
+           against the measured HBM copy bandwidth (algorithmic 144 B/cell/stage),
+           plus roofline_fp64 against a measured FP64 FMA peak (the binding roof);
+cpu_baseline  the reference's own phase/mlweno/core sources (oracle/_ref) or the
+           restated oracle, all host threads, on a bounded 160x320 sample.
+Under torchrun (N>1) every rank advances its own 1280x2560 instance (replicas;
+the instances are independent) and the max time over ranks is used.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(nx=1280, ny=2560)
+ALG_BYTES_PER_CELL_STAGE = 144          # read U^(k), U^n; write U^(k+1); 2 faces x 5 q x 8 B v_s.n; write T, phi
+# FP64 operations per cell per stage (executed DFMA counted as 2, DADD/DMUL as 1)
+# of the cell+face+sum kernels, from the ncu capture summarised in
+# profiles/transport_stage_fp64_1280x2560.md (None until measured).
+FP64_FLOPS_PER_CELL_STAGE = None
+# DRAM bytes per cell per stage of the three stage kernels from the same capture.
+DRAM_BYTES_PER_CELL_STAGE = None
+CPU_SAMPLE = dict(nx=160, ny=320)
+CPU_SECONDS = 12.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_run(nsteps_min: int, seconds: float, threads: int):
+    """Reference CPU implementation on the bounded sample: returns (value, cores, kind, sample, steps, time)."""
+    from oracle import pyoracle as po
+    from mantlepar_b200 import synthetic as sy
+    kind = "reference" if po.reference_available() else "port"
+    lib = po.reference() if kind == "reference" else po.restated()
+    w = sy.Workload(**CPU_SAMPLE)
+    t = po.TransportOracle(sy.material_s(), w, lib=lib, integrator=3, threads=threads)
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    t.set_face_velocity(vs, ud)
+    t.set_state(H, C)
+    code, _ = t.step(1)                 # first RHS + one step (not timed)
+    assert code == 0
+    steps, t0 = 0, time.perf_counter()
+    while steps < nsteps_min or time.perf_counter() - t0 < seconds:
+        code, _ = t.step(1)
+        assert code == 0
+        steps += 1
+        if steps >= max(nsteps_min, 1) and time.perf_counter() - t0 >= seconds:
+            break
+    el = time.perf_counter() - t0
+    t.close()
+    return w.cells * steps / el, threads, kind, f"{w.nx}x{w.ny} sub-instance of the same construction, {steps} SSPRK3 steps", steps, el
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    from oracle import pyoracle as po
+    from mantlepar_b200 import synthetic as sy
+    kind = "reference" if po.reference_available() else "port"
+    lib = po.reference() if kind == "reference" else po.restated()
+    w = sy.Workload(**CPU_SAMPLE)
+    t = po.TransportOracle(sy.material_s(), w, lib=lib, integrator=3, threads=threads)
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    t.set_face_velocity(vs, ud)
+    t.set_state(H, C)
+    code, _ = t.step(args.warmup)
+    assert code == 0
+    t0 = time.perf_counter()
+    code, reps = t.step(args.steps)
+    el = time.perf_counter() - t0
+    assert code == 0
+    value = w.cells * args.steps / el
+    line = {"impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_block(),
+            "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": kind,
+                             "sample": f"{w.nx}x{w.ny} sub-instance per step (bounded sample of the 1280x2560 workload), SSPRK3"},
+            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_block():
+    return {"workload": f"plain FP64 transport+phase, single {WORKLOAD['nx']}x{WORKLOAD['ny']} instance on [0,0.5]x[0,1], SSPRK3, CFL 0.4",
+            "nx": WORKLOAD["nx"], "ny": WORKLOAD["ny"], "integrator": "SSPRK3", "cfl": 0.4,
+            "material": "S (Te0=250K, Tm0=1250K, L=6e5, cp=1200, Xe=0.5, alpha0=0)",
+            "l2": "inputs larger than L2 (per-stage working set ~1.1 GB > 126 MB)"}
+
+
+def run_gpu(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        pg = dist
+    from mantlepar_b200 import _capi, synthetic as sy
+    from mantlepar_b200.transport import Transport, TransportConfig
+    import ctypes as C
+    lib = _capi.lib()
+    w = sy.Workload(**WORKLOAD, seed=1 + rank)
+    stream = torch.cuda.current_stream(dev)
+    t = Transport(w, TransportConfig(cfl=w.cfl, integrator=3), stream=stream.cuda_stream)
+    vs, ud = sy.face_velocity(w)
+    H, Cc = sy.initial_state(w)
+    t.set_face_velocity(vs, ud)
+    t.set_state(H, Cc)
+    t.step(max(args.warmup, 1))
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    # ---- resident throughput with per-kernel event timing
+    _capi.check(lib.mp_transport_profile(t._h, 1))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = _capi.kernel_launches()
+    barrier()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        _, reps = t.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = _capi.kernel_launches() - launches0
+    ms = e0.elapsed_time(e1)
+    kms = (C.c_double * 4)()
+    kn = (C.c_ulonglong * 4)()
+    _capi.check(lib.mp_transport_kernel_times(t._h, kms, kn))
+    _capi.check(lib.mp_transport_profile(t._h, 0))
+    ms_max = ms
+    if pg:
+        x = torch.tensor([ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(x, op=pg.ReduceOp.MAX)
+        ms_max = float(x.item())
+    cells = w.cells
+    value = world * cells * args.steps / (ms_max * 1e-3)
+    retries = sum(r["retries"] for r in reps)
+
+    # ---- end to end through the C ABI with pinned host buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    hv, hu, hH, hC = pin(vs), pin(ud), pin(H), pin(Cc)
+    oH, oC, oT, oP = (torch.empty(cells, dtype=torch.float64).pin_memory() for _ in range(4))
+    barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        t.set_face_velocity(hv, hu)
+        t.set_state(hH, hC)
+        t.step(1)
+        t.get_state_into(oH, oC, oT, oP)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    if pg:
+        x = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
+        pg.all_reduce(x, op=pg.ReduceOp.MAX)
+        ms_e2e = float(x.item())
+    e2e_value = world * cells * args.steps / (ms_e2e * 1e-3)
+    h2d = hv.numel() * 8 + hu.numel() * 8 + hH.numel() * 8 + hC.numel() * 8
+    d2h = 4 * cells * 8
+
+    # ---- roofline of one stage (cell + face + sum kernels)
+    stages = kn[0]
+    stage_ms = (kms[0] + kms[1] + kms[2]) / max(stages, 1)
+    hbm_peak, peak_kind = peaks()
+    achieved = ALG_BYTES_PER_CELL_STAGE * cells / (stage_ms * 1e-3) / 1e9
+    traffic = DRAM_BYTES_PER_CELL_STAGE * cells if DRAM_BYTES_PER_CELL_STAGE else None
+    fp64 = C.c_double(0)
+    _capi.check(lib.mp_probe_fp64_peak(stream.cuda_stream, C.byref(fp64)))
+    total_k = sum(kms[k] for k in range(4))
+    shares = {n: round(kms[k] / total_k, 4) if total_k else None for k, n in enumerate(["cell", "face", "sum", "axpy_reduce"])}
+    line = None
+    if rank == 0:
+        roof64 = {"bound": "fp64", "peak": fp64.value, "unit": "TFLOP/s", "peak_kind": "measured (FMA probe)"}
+        if FP64_FLOPS_PER_CELL_STAGE:
+            a64 = FP64_FLOPS_PER_CELL_STAGE * cells / (stage_ms * 1e-3) / 1e12
+            roof64.update(achieved=a64, frac=a64 / fp64.value, flops_per_cell_stage=FP64_FLOPS_PER_CELL_STAGE)
+        else:
+            roof64.update(achieved=None, frac=None)
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_block(),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": traffic,
+                         "peak_kind": peak_kind + " copy bandwidth",
+                         "kernel": "one stage = cell_kernel + face_kernel + sum_kernel",
+                         "stage_ms": stage_ms, "stages_timed": int(stages), "kernel_shares": shares},
+            "roofline_fp64": roof64,
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": ms_e2e / args.steps},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "retries": retries,
+        }
+    t.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, kind, sample, _, _ = cpu_run(2, CPU_SECONDS, os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": kind, "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mantlepar_b200", choices=["mantlepar_b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nx", type=int, default=WORKLOAD["nx"], help="cells in x (profiling of smaller cases)")
+    ap.add_argument("--ny", type=int, default=WORKLOAD["ny"], help="cells in y")
+    args = ap.parse_args()
+    WORKLOAD.update(nx=args.nx, ny=args.ny)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_gpu(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

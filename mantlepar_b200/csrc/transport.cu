@@ -56,8 +56,12 @@ struct Totals {
     double nonfinite;
 };
 
-__device__ __forceinline__ void record_error(unsigned long long* status, long long where, int code) {
-    atomicMin(status, ((unsigned long long)where << 8) | (unsigned long long)(code & 0xff));
+// Status word: the smallest key wins. The key orders failures as the
+// reference's RHS meets them (evolve.cpp:279-384): reconstruction update,
+// limiter, porosity sampling, face loop, cell quadrature; then by cell/edge.
+enum : int { PART_UPDATE = 0, PART_LIMIT = 1, PART_POROSITY = 2, PART_FACES = 3, PART_CELLS = 4 };
+__device__ __forceinline__ void record_error(unsigned long long* status, int part, long long where, int code) {
+    atomicMin(status, ((unsigned long long)part << 56) | ((unsigned long long)where << 8) | (unsigned long long)(code & 0xff));
 }
 
 __device__ __forceinline__ double ld_ro(const double* p) { return __ldg(p); }
@@ -87,7 +91,11 @@ __global__ void __launch_bounds__(128) cell_kernel(CellArgs a, Physics ph) {
     const size_t N = (size_t)nx * ny;
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1);
     const int cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
-    int st = 0;
+    int st = 0;          // reconstruction update (smoothness / weights)
+    int st_lim = 0;      // limiter: admissible means, finite reconstructed values
+    int st_por = 0;      // porosity sampling: phase at the cell points
+    int st_face = 0;     // face loop: diffusion-sample admissibility
+    int st_cell = 0;     // cell quadrature: T >= 0, porosity < 1
 
     double uh[3][3], uc[3][3];
     double loH, hiH, loC, hiC;
@@ -101,7 +109,7 @@ __global__ void __launch_bounds__(128) cell_kernel(CellArgs a, Physics ph) {
         }
     const double mH = uh[1][1], mC = uc[1][1];
     // state_reconstruction.cpp:187-188: admissible means.
-    if (!(isfinite(mH) && mH >= 0.0 && isfinite(mC) && mC >= 0.0 && mC <= ph.k.Xe)) st = E_OUTOFRANGE;
+    if (!(isfinite(mH) && mH >= 0.0 && isfinite(mC) && mC >= 0.0 && mC <= ph.k.Xe)) st_lim = E_OUTOFRANGE;
     // 3x3 neighbour bounds (state_reconstruction.cpp:189-196); the clamped
     // gather repeats in-domain values, which leaves min/max unchanged.
     loH = hiH = mH; loC = hiC = mC;
@@ -126,7 +134,7 @@ __global__ void __launch_bounds__(128) cell_kernel(CellArgs a, Physics ph) {
         const double x = t.pt_x[p], y = t.pt_y[p];
         const double vH = mH + q2(DH, x, y);
         const double vC = mC + q2(DC, x, y);
-        if (!isfinite(vH) || !isfinite(vC)) { st = st ? st : E_FP; continue; }
+        if (!isfinite(vH) || !isfinite(vC)) { st_lim = st_lim ? st_lim : E_FP; continue; }
         if (vH > hiH) thH = fmin(thH, (hiH - mH) / (vH - mH));
         if (vH < loH) thH = fmin(thH, (loH - mH) / (vH - mH));
         if (vC > hiC) thC = fmin(thC, (hiC - mC) / (vC - mC));
@@ -153,8 +161,8 @@ __global__ void __launch_bounds__(128) cell_kernel(CellArgs a, Physics ph) {
             PhaseLean pl;
             if (!s && !isfinite(h)) s = PH_INVALID;
             if (!s) s = phase_lean(ph.k, h, c, bd, pl);
-            if (s) { st = st ? st : s; continue; }
-            if (!(pl.T >= 0.0 && pl.phil < 1.0)) st = st ? st : E_OUTOFRANGE;
+            if (s) { st_por = st_por ? st_por : s; continue; }
+            if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_cell = st_cell ? st_cell : E_OUTOFRANGE;
             const double w = t.cw[b * kNQ + aq];
             Tsum += w * pl.T;
             Psum += w * pl.phil;
@@ -178,12 +186,16 @@ __global__ void __launch_bounds__(128) cell_kernel(CellArgs a, Physics ph) {
                 PhaseLean pl;
                 if (!s && !isfinite(h)) s = PH_INVALID;
                 if (!s) s = phase_lean(ph.k, h, c, bd, pl);
-                if (s) { st = st ? st : s; continue; }
-                if (!(pl.T >= 0.0 && pl.phil < 1.0)) st = st ? st : E_OUTOFRANGE;
+                if (s) { st_face = st_face ? st_face : s; continue; }
+                if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_face = st_face ? st_face : E_OUTOFRANGE;
             }
         }
     }
-    if (st) record_error(a.status, cell, st);
+    if (st) record_error(a.status, PART_UPDATE, cell, st);
+    if (st_lim) record_error(a.status, PART_LIMIT, cell, st_lim);
+    if (st_por) record_error(a.status, PART_POROSITY, cell, st_por);
+    if (st_face) record_error(a.status, PART_FACES, cell, st_face);
+    if (st_cell) record_error(a.status, PART_CELLS, cell, st_cell);
 #pragma unroll
     for (int m = 0; m < 9; ++m) {
         a.rec[(size_t)m * N + cell] = DH[m];
@@ -341,7 +353,7 @@ __global__ void __launch_bounds__(128) face_kernel(FaceArgs a, Physics ph) {
         if (!isfinite(sens)) st = st ? st : E_FP;
         rate += w * (aC + aH + 2.0 * fabs(vs)) * sens;
     }
-    if (st) record_error(a.status, L, st);
+    if (st) record_error(a.status, PART_FACES, L, st);
     a.face[e] = fluxH;
     a.face[nE + e] = fluxC;
     a.face[2 * nE + e] = rate;
@@ -588,7 +600,7 @@ void free_all(mp_transport* t) {
 mp_status check_status(mp_transport* t, const char* where) {
     const unsigned long long v = *t->h_status;
     if (v == ~0ULL) return MP_OK;
-    const long long cell = (long long)(v >> 8);
+    const long long cell = (long long)((v >> 8) & ((1ULL << 48) - 1));
     const int code = (int)(v & 0xff);
     const char* what = code == MP_ERR_ARG_OUTOFRANGE ? "inadmissible state (T < 0, porosity >= 1, C outside [0,Xe] or backflow)"
                      : code == MP_ERR_FP ? "non-finite value in reconstruction, smoothness or CFL rate"
