@@ -183,6 +183,23 @@ mp_status mp_transport_step(mp_transport* t, int nsteps, mp_step_report* reports
  * (StateReconstruction::Limit, src/couple/state_reconstruction.cpp:136-192). */
 mp_status mp_transport_limiter(mp_transport* t, double* thetaH, double* thetaC);
 
+/* One stage evaluation (as mp_transport_rhs) that allocates no device memory,
+ * for callers that cannot call cudaMalloc -- e.g. code inside a framework that
+ * owns all device memory through its own pool, or code that must not allocate
+ * once its latency-critical phase has begun. No counterpart in the reference
+ * (its CPU code allocates freely). All scratch lives in one fixed file-scope
+ * device array (about 7.4 MB per GPU that loads the library, held until the
+ * process exits); meshes above 32768 cells (nx*ny) are rejected with
+ * MP_ERR_ARG_SIZ. The first call on each device looks up that array's device
+ * address, so make it before any stream capture. Calls share the array and
+ * overwrite it; calls that overlap on the GPU race. All array arguments are
+ * device pointers (H, C, rhsH, rhsC, T, phi: nx*ny; vs_n, ud_n: edges*5);
+ * rate and totals may be NULL. Synchronous on `stream`. */
+mp_status mp_transport_rhs_noalloc(const mp_mesh_desc* mesh, const mp_transport_opts* opts,
+                                   const double* H, const double* C, const double* vs_n, const double* ud_n,
+                                   double* rhsH, double* rhsC, double* T, double* phi, double* rate,
+                                   mp_stage_totals* totals, mp_stream_t stream);
+
 /* ------------------------------------------------------------ measurement */
 
 /* Number of this library's kernel launches issued so far (all handles). */

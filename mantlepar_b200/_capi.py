@@ -109,6 +109,8 @@ def lib() -> C.CDLL:
         "mp_transport_profile": (i, [vp, i]),
         "mp_transport_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
         "mp_probe_fp64_peak": (i, [vp, C.POINTER(C.c_double)]),
+        "mp_transport_rhs_noalloc": (i, [C.POINTER(MeshDesc), C.POINTER(TransportOpts), vp, vp, vp, vp,
+                                         vp, vp, vp, vp, vp, C.POINTER(StageTotals), vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -978,3 +978,67 @@ extern "C" mp_status mp_probe_fp64_peak(mp_stream_t stream, double* tflops) {
     *tflops = 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3) / 1e12;
     return MP_OK;
 }
+
+// ------------------------------------------------ stage on caller buffers
+
+namespace mp {
+
+size_t raw_partial_bytes(size_t ncell) { return ((ncell + kRedBlock - 1) / kRedBlock) * sizeof(Partial); }
+size_t raw_totals_bytes() { return sizeof(Totals); }
+
+// One stage evaluation L(U) (STORE_L mode) on buffers the caller provides:
+// tab (device StageTables), rec (18*ncell doubles), wet (ncell bytes), face
+// (4*nedge doubles), partial (raw_partial_bytes), totals (raw_totals_bytes),
+// status (one unsigned long long). Used by entry points that cannot allocate.
+mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double* H, const double* C,
+                        const double* vsn, const double* udn, double* rhsH, double* rhsC, double* T, double* phi,
+                        double* rate, StageTables* tab, double* rec, unsigned char* wet, double* face, void* partial,
+                        void* totals, unsigned long long* status, mp_stage_totals* out, cudaStream_t s) {
+    mp_derived der;
+    MP_TRY(derive_checked(o.material, der));
+    Physics ph;
+    ph.k = phase_const(o.material, der);
+    if (eutectic_temperature(ph.k, o.pressure, ph.Tep)) { set_error("pressure must be finite"); return MP_ERR_ARG_OUTOFRANGE; }
+    ph.theta = o.theta; ph.inflowH = o.inflow_H; ph.inflowC = o.inflow_C;
+    ph.Hpol = o.H_policy; ph.Cpol = o.C_policy; ph.lf_global = o.lf_global; ph.lf_speed = o.lf_global_speed;
+    const size_t N = (size_t)nx * ny;
+    const size_t NE = (size_t)nx * (ny + 1) + (size_t)(nx + 1) * ny;
+    const int sum_blocks = (int)((N + kRedBlock - 1) / kRedBlock);
+    Partial* part = static_cast<Partial*>(partial);
+    Totals* tot = static_cast<Totals*>(totals);
+    MP_CUDA(cudaMemsetAsync(status, 0xff, sizeof(unsigned long long), s));
+    {
+        CellArgs a{nx, ny, tab, H, C, rec, wet, T, phi, status, nullptr};
+        dim3 blk(32, 4), grd((nx + 31) / 32, (ny + 3) / 4);
+        cell_kernel<<<grd, blk, 0, s>>>(a, ph);
+    }
+    {
+        FaceArgs a{nx, ny, tab, H, C, rec, wet, vsn, udn, face, status};
+        face_kernel<<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(a, ph);
+    }
+    {
+        SumArgs a{nx, ny, tab, face, H, C, H, C, rhsH, rhsC, rate, SUM_STORE_L, 0.0, 0.0, 0.0, part};
+        sum_kernel<<<sum_blocks, kRedBlock, 0, s>>>(a);
+    }
+    reduce_kernel<<<1, 1024, 0, s>>>(part, sum_blocks, tot);
+    count_launch(4);
+    MP_CUDA(cudaGetLastError());
+    Totals host_tot;
+    unsigned long long host_status = 0;
+    MP_CUDA(cudaMemcpyAsync(&host_tot, tot, sizeof(Totals), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaMemcpyAsync(&host_status, status, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    if (host_status != ~0ULL) {
+        const long long cell = (long long)((host_status >> 8) & ((1ULL << 48) - 1));
+        set_error("RHS: cell %lld: stage failure (class %d)", cell, (int)(host_status & 0xff));
+        return (mp_status)(host_status & 0xff);
+    }
+    if (!std::isfinite(host_tot.maxRate)) { set_error("RHS: nonfinite coupled stage rate"); return MP_ERR_FP; }
+    if (out) {
+        out->boundaryH = host_tot.bH; out->boundaryC = host_tot.bC; out->sourceH = 0.0;
+        out->maxRate = host_tot.maxRate; out->divergence = host_tot.divergence;
+    }
+    return MP_OK;
+}
+
+}  // namespace mp
