@@ -14,7 +14,7 @@ value      device-timed (CUDA events) throughput with state resident in HBM;
 e2e        the same metric through the C ABI with host buffers: per step the
            face velocities and H/C go host->device from pinned memory, the step
            runs, and H/C/T/phi come back device->host;
-roofline   one stage evaluation (cell + face + sum kernels) counted as one launch
+roofline   one stage evaluation (the four stage kernels) counted as one launch
            against the measured HBM copy bandwidth (algorithmic 144 B/cell/stage),
            plus roofline_fp64 against a measured FP64 FMA peak (the binding roof);
 cpu_baseline  the reference's own phase/mlweno/core sources (oracle/_ref) or the
@@ -40,12 +40,13 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(nx=1280, ny=2560)
 ALG_BYTES_PER_CELL_STAGE = 144          # read U^(k), U^n; write U^(k+1); 2 faces x 5 q x 8 B v_s.n; write T, phi
-# FP64 operations per cell per stage (executed DFMA counted as 2, DADD/DMUL as 1)
-# of the cell+face+sum kernels, from the ncu capture summarised in
-# profiles/transport_stage_fp64_1280x2560.md (None until measured).
-FP64_FLOPS_PER_CELL_STAGE = None
-# DRAM bytes per cell per stage of the three stage kernels from the same capture.
-DRAM_BYTES_PER_CELL_STAGE = None
+# Executed FP64 operations per cell per stage (DFMA counted as 2, DADD/DMUL
+# as 1) of the four stage kernels, from the ncu capture summarised in
+# profiles/transport_stage_full_640x1280.md (per-cell figures are size-independent).
+FP64_FLOPS_PER_CELL_STAGE = 6637
+# DRAM bytes per cell per stage of the four stage kernels from the same capture
+# (640x1280 keeps every stage array above L2 size; traffic scales with cells).
+DRAM_BYTES_PER_CELL_STAGE = 900
 CPU_SAMPLE = dict(nx=160, ny=320)
 CPU_SECONDS = 12.0
 
@@ -225,8 +226,8 @@ def run_gpu(args, world, rank, local):
         torch.cuda.synchronize()
     launches = _capi.kernel_launches() - launches0
     ms = e0.elapsed_time(e1)
-    kms = (C.c_double * 4)()
-    kn = (C.c_ulonglong * 4)()
+    kms = (C.c_double * 6)()
+    kn = (C.c_ulonglong * 6)()
     _capi.check(lib.mp_transport_kernel_times(t._h, kms, kn))
     _capi.check(lib.mp_transport_profile(t._h, 0))
     ms_max = ms
@@ -261,16 +262,18 @@ def run_gpu(args, world, rank, local):
     h2d = hv.numel() * 8 + hu.numel() * 8 + hH.numel() * 8 + hC.numel() * 8
     d2h = 4 * cells * 8
 
-    # ---- roofline of one stage (cell + face + sum kernels)
+    # ---- roofline of one stage (reconstruction + cell phase + face + sum kernels)
     stages = kn[0]
-    stage_ms = (kms[0] + kms[1] + kms[2]) / max(stages, 1)
+    stage_ms = (kms[0] + kms[1] + kms[2] + kms[3]) / max(stages, 1)
     hbm_peak, peak_kind = peaks()
     achieved = ALG_BYTES_PER_CELL_STAGE * cells / (stage_ms * 1e-3) / 1e9
     traffic = DRAM_BYTES_PER_CELL_STAGE * cells if DRAM_BYTES_PER_CELL_STAGE else None
     fp64 = C.c_double(0)
     _capi.check(lib.mp_probe_fp64_peak(stream.cuda_stream, C.byref(fp64)))
-    total_k = sum(kms[k] for k in range(4))
-    shares = {n: round(kms[k] / total_k, 4) if total_k else None for k, n in enumerate(["cell", "face", "sum", "axpy_reduce"])}
+    total_k = sum(kms[k] for k in range(5))
+    names = ["recon", "cellphase", "face", "sum", "axpy_reduce"]
+    shares = {n: round(kms[k] / total_k, 4) if total_k else None for k, n in enumerate(names)}
+    kernel_ms = {n: kms[k] / max(kn[k], 1) for k, n in enumerate(names)}
     line = None
     if rank == 0:
         roof64 = {"bound": "fp64", "peak": fp64.value, "unit": "TFLOP/s", "peak_kind": "measured (FMA probe)"}
@@ -287,8 +290,9 @@ def run_gpu(args, world, rank, local):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": traffic,
                          "peak_kind": peak_kind + " copy bandwidth",
-                         "kernel": "one stage = cell_kernel + face_kernel + sum_kernel",
-                         "stage_ms": stage_ms, "stages_timed": int(stages), "kernel_shares": shares},
+                         "kernel": "one stage = recon_kernel + cellphase_kernel + face_kernel + sum_kernel",
+                         "stage_ms": stage_ms, "stages_timed": int(stages), "kernel_shares": shares,
+                         "kernel_avg_ms": kernel_ms},
             "roofline_fp64": roof64,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": ms_e2e / args.steps},

@@ -208,9 +208,10 @@ unsigned long long mp_kernel_launches(void);
 /* Per-kernel CUDA-event timing of a handle's stage kernels (no counterpart in
  * the reference, which has no timers on this path). enable resets the
  * accumulators; kernel_times returns accumulated ms and launch counts for
- * [0] cell kernel, [1] face kernel, [2] sum kernel, [3] axpy/reductions. */
+ * [0] reconstruction/limiter, [1] cell phase quadrature, [2] faces,
+ * [3] accumulation/RK, [4] axpy and reductions, [5] unused. */
 mp_status mp_transport_profile(mp_transport* t, int enable);
-mp_status mp_transport_kernel_times(mp_transport* t, double ms[4], unsigned long long launches[4]);
+mp_status mp_transport_kernel_times(mp_transport* t, double ms[6], unsigned long long launches[6]);
 
 /* Measured FP64 FMA throughput of this GPU (TFLOP/s), the compute roof of
  * this FP64-bound path. */

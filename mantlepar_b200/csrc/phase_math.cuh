@@ -233,6 +233,75 @@ MP_HD int phase_lean(const PhaseConst& k, double H, double C, const Bounds& b, P
     return st;
 }
 
+// Constants of the stage kernels' phase evaluation (precomputed reciprocals).
+struct StageConst {
+    double Xe, LD, invXe, invLD, halfInvLD, fourLD, LDoverXe;
+};
+
+MP_HD StageConst stage_const(const PhaseConst& k) {
+    StageConst c;
+    c.Xe = k.Xe; c.LD = k.LD;
+    c.invXe = 1.0 / k.Xe; c.invLD = 1.0 / k.LD; c.halfInvLD = 0.5 / k.LD;
+    c.fourLD = 4.0 * k.LD; c.LDoverXe = k.LD / k.Xe;
+    return c;
+}
+
+// Phase evaluation for the transport stage (T, phil, cl, cs, dT/dC): the
+// same regions and closed forms as phase_eval, with the divisions by Xe and
+// LD replaced by precomputed reciprocals and one shared reciprocal for
+// 1/phil and 1/disc in the solid+liquid region. Agrees with phase_eval to a
+// few ulp; region selection uses interval ends formed the same way.
+MP_HD int phase_stage(const StageConst& k, double H, double C, double Tep, PhaseLean& s) {
+    if (!(C >= 0.0 && C <= k.Xe) || !mp_isfinite(H)) return PH_INVALID;
+    int st = PH_OK;
+    const double Tmp = Tep + 1.0;
+    const double r = C * k.invXe;
+    const double Hliq = C == 0.0 ? Tmp + k.LD : (Tep + (1.0 - r)) + k.LD;
+    const double Heut = Tep + k.LD * r;
+    double phi1 = 0.0, phi2 = 0.0;
+    s.phil = 0.0; s.cl = 0.0; s.dTdC = 0.0;
+    bool liquid_region = false;
+    if (C == 0.0) {
+        if (H <= Tmp) { phi1 = 1.0; s.T = H; }
+        else if (H < Hliq) {
+            s.phil = clip_fraction((H - Tmp) * k.invLD, st);
+            phi1 = 1.0 - s.phil;
+            s.T = Tmp;
+        } else { s.phil = 1.0; s.T = H - k.LD; liquid_region = true; }
+    } else if (H <= Tep) {
+        phi1 = 1.0 - C; phi2 = C; s.T = H;
+    } else if (H >= Hliq) {
+        s.phil = 1.0; s.cl = C; s.T = H - k.LD; liquid_region = true;
+    } else if (H <= Heut) {
+        const double melt = (H == Heut) ? r : fmin(r, (H - Tep) * k.invLD);
+        const double second = fmax(0.0, C - melt * k.Xe);
+        s.phil = clip_fraction(melt, st);
+        phi2 = clip_fraction(second, st);
+        phi1 = clip_fraction(1.0 - melt - second, st);
+        s.cl = k.Xe;
+        s.T = Tep;
+    } else {
+        const double a = H - Tmp;
+        const double disc = fabs(a) < 1e150 ? sqrt(a * a + k.fourLD * r) : hypot(a, 2.0 * sqrt(k.LD * r));
+        const double melt = a >= 0.0 ? (a + disc) * k.halfInvLD : 2.0 * r / (disc - a);
+        const double inv = 1.0 / (melt * disc);
+        const double inv_melt = disc * inv, inv_disc = melt * inv;
+        s.phil = clip_fraction(melt, st);
+        phi1 = clip_fraction(1.0 - melt, st);
+        s.cl = clip_fraction(C * inv_melt, st);
+        s.T = a >= 0.0 ? Tmp - r * inv_melt : H - k.LD * melt;
+        s.dTdC = minus_magnitude(k.LDoverXe * inv_disc);
+    }
+    if (C == 0.0 && H > Tep && !liquid_region) {
+        const double gap = fabs(H - Tmp);
+        s.dTdC = gap == 0.0 ? -INFINITY : minus_magnitude(k.LDoverXe / gap);
+    }
+    const double solid = phi1 + phi2;
+    s.cs = (solid > 0.0 && phi2 != 0.0) ? phi2 / solid : 0.0;
+    if (!(s.phil > 0.0)) s.cl = 0.0;
+    return st;
+}
+
 }  // namespace mp
 
 #endif

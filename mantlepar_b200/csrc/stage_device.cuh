@@ -1,4 +1,4 @@
-// Device building blocks of the ML-WENO H/C transport stage (FP64).
+// Device building blocks of the ML-WENO H/C transport stage.
 //
 // Per cell, the reference's reconstruction (Reconstruction::Update +
 // TensorStencilPoly::Smoothness, src/mlweno/reconstruction.cpp:275-355 and
@@ -7,7 +7,9 @@
 //   R(x) = u_t + sum_k w_k P_k(x)  ==  u_t + D(xi, eta),
 // the 2x2 candidates being re-expanded about the target centre. The limiter
 // (state_reconstruction.cpp:136-192) then scales D by theta, so each limited
-// evaluation at a point is one 9-term Horner form.
+// evaluation at a point is one 9-term polynomial. R is the arithmetic type of
+// the reconstruction (double for the FP64 path, float for the mixed path);
+// centred differences are formed in FP64 before the conversion.
 #ifndef MP_STAGE_DEVICE_CUH
 #define MP_STAGE_DEVICE_CUH
 
@@ -16,126 +18,230 @@
 
 namespace mp {
 
-// Evaluate a Q2 polynomial, coefficient m = j*3 + i of xi^i eta^j.
+// Table entries in the arithmetic type R (FP32 copies for the mixed path).
+struct StageTablesF {
+    float C9[9][9];
+    float S9[8][8];
+    float C4[4][4];
+    float S4[4][3][3];
+    float X, Y, epsA, logEpsA2;
+    float gx[kNQ], gy[kNQ];
+    float line_c[kMaxLines];
+};
+
+template <class R> struct Tab;
+template <> struct Tab<double> {
+    const StageTables* t;
+    __device__ double C9(int c, int m) const { return t->C9[c][m]; }
+    __device__ double S9(int r, int c) const { return t->S9[r][c]; }
+    __device__ double C4(int c, int m) const { return t->C4[c][m]; }
+    __device__ double S4(int k, int r, int c) const { return t->S4[k][r][c]; }
+    __device__ double X() const { return t->X; }
+    __device__ double Y() const { return t->Y; }
+    __device__ double epsA() const { return t->epsA; }
+    __device__ double gx(int q) const { return t->gx[q]; }
+    __device__ double gy(int q) const { return t->gy[q]; }
+    __device__ double line_c(int l) const { return t->line_c[l]; }
+};
+template <> struct Tab<float> {
+    const StageTables* t;
+    const StageTablesF* f;
+    __device__ float C9(int c, int m) const { return f->C9[c][m]; }
+    __device__ float S9(int r, int c) const { return f->S9[r][c]; }
+    __device__ float C4(int c, int m) const { return f->C4[c][m]; }
+    __device__ float S4(int k, int r, int c) const { return f->S4[k][r][c]; }
+    __device__ float X() const { return f->X; }
+    __device__ float Y() const { return f->Y; }
+    __device__ float epsA() const { return f->epsA; }
+    __device__ float gx(int q) const { return f->gx[q]; }
+    __device__ float gy(int q) const { return f->gy[q]; }
+    __device__ float line_c(int l) const { return f->line_c[l]; }
+};
+
+template <class R> __device__ __forceinline__ R eps_of();
+template <> __device__ __forceinline__ double eps_of<double>() { return 2.220446049250313e-16; }
+template <> __device__ __forceinline__ float eps_of<float>() { return 1.1920929e-07f; }
+
+// Row / column coefficients of a Q2 polynomial (coefficient m = j*3 + i of
+// xi^i eta^j): along the row eta = y, p(xi) = a0 + xi*(a1 + xi*a2).
 template <class R>
-__device__ __forceinline__ R q2(const R* D, R x, R y) {
-    const R r0 = D[0] + x * (D[1] + x * D[2]);
-    const R r1 = D[3] + x * (D[4] + x * D[5]);
-    const R r2 = D[6] + x * (D[7] + x * D[8]);
-    return r0 + y * (r1 + y * r2);
+__device__ __forceinline__ void q2_row(const R* D, R y, R& a0, R& a1, R& a2) {
+    a0 = D[0] + y * (D[3] + y * D[6]);
+    a1 = D[1] + y * (D[4] + y * D[7]);
+    a2 = D[2] + y * (D[5] + y * D[8]);
 }
+// Along the column xi = x, p(eta) = b0 + eta*(b1 + eta*b2).
+template <class R>
+__device__ __forceinline__ void q2_col(const R* D, R x, R& b0, R& b1, R& b2) {
+    b0 = D[0] + x * (D[1] + x * D[2]);
+    b1 = D[3] + x * (D[4] + x * D[5]);
+    b2 = D[6] + x * (D[7] + x * D[8]);
+}
+template <class R>
+__device__ __forceinline__ R quad(R c0, R c1, R c2, R s) { return c0 + s * (c1 + s * c2); }
 
 // sigma = d^T S d on differences to stencil cell 0 with the reference's
-// roundoff clip (tensorstencilpoly.cpp:424-430). S excludes row/col 0.
-template <int N>
-__device__ __forceinline__ double smoothness(const double (*S)[N], const double* diff, int& st) {
-    double sum = 0.0, mag = 0.0;
+// roundoff clip (tensorstencilpoly.cpp:424-430). Returns -1 on failure.
+template <class R, int N, class G>
+__device__ __forceinline__ R smoothness(G&& S, const R* diff) {
+    R sum = 0, mag = 0;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
-        const double sr = S[r][r] * diff[r] * diff[r];
+        const R sr = S(r, r) * diff[r] * diff[r];
         sum += sr; mag += fabs(sr);
 #pragma unroll
         for (int c = r + 1; c < N; ++c) {
-            const double term = 2.0 * (S[r][c] * diff[r]) * diff[c];
+            const R term = R(2) * (S(r, c) * diff[r]) * diff[c];
             sum += term; mag += fabs(term);
         }
     }
-    if (!isfinite(sum)) { st = 72; return 0.0; }
-    if (sum < -64.0 * 2.220446049250313e-16 * mag) { st = 72; return 0.0; }
-    return fmax(0.0, sum);
+    if (!isfinite(sum) || sum < -R(64) * eps_of<R>() * mag) return R(-1);
+    return sum > R(0) ? sum : R(0);
 }
 
-// Build D (9 coefficients) for one field from the 3x3 neighbourhood u[dj][di]
-// (index 1,1 = target). Candidate mask by boundary class (ci, cj):
-// reconstruction.cpp:150-153 drops stencils that leave the domain.
-__device__ __forceinline__ void reconstruct(const StageTables& t, int ci, int cj, const double (&u)[3][3],
-                                            double (&D)[9], int& st) {
-    const double ut = u[1][1];
+// Nonlinear weights alpha_k = (sigma_k + eps*A)^-(s*r_k + eta(r_k)): 7 for
+// the 3x3 order-2 candidate, 5 for the 2x2 order-1 candidates
+// (reconstruction.cpp:43-54,212-265). Written as ratios r = epsA/(sigma+epsA)
+// in (0,1] with the common factor (epsA)^-7 divided out, so nothing
+// overflows. In FP32 the powers would underflow, so each ratio is split into
+// mantissa and binary exponent and the exponents are summed as integers; the
+// weights are returned normalised in FP64 (sum exactly 1 to FP64 rounding).
+template <class R>
+__device__ __forceinline__ void weights(const R* sig, const bool* on, R eA, double* w) {
+    if constexpr (sizeof(R) == 8) {
+        double alpha[5];
+        const double scale = on[0] ? eA * eA : 1.0;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const double r = eA / (sig[k] + eA);
+            const double r2 = r * r;
+            alpha[k] = !on[k] ? 0.0 : (k == 0 ? r2 * r2 * r2 * r : scale * (r2 * r2 * r));
+        }
+        double sum = 0;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) sum += alpha[k];
+        const double inv = 1.0 / sum;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) w[k] = alpha[k] * inv;
+    } else {
+        int ea;
+        const float fa = frexpf(eA, &ea);
+        const float fa2 = fa * fa;
+        float mant[5];
+        int ex[5], emax = -1 << 30;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            int e;
+            const float f = frexpf(eA / (sig[k] + eA), &e);
+            const float f2 = f * f;
+            if (k == 0) { mant[k] = f2 * f2 * f2 * f; ex[k] = 7 * e; }
+            else { mant[k] = f2 * f2 * f * (on[0] ? fa2 : 1.0f); ex[k] = 5 * e + (on[0] ? 2 * ea : 0); }
+            if (on[k]) emax = max(emax, ex[k]);
+        }
+        double alpha[5], sum = 0;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            alpha[k] = on[k] ? (double)ldexpf(mant[k], max(ex[k] - emax, -200)) : 0.0;
+            sum += alpha[k];
+        }
+        const double inv = 1.0 / sum;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) w[k] = alpha[k] * inv;
+    }
+}
+
+// Build D (9 coefficients, FP64) for one field from the 3x3 neighbourhood
+// u[dj][di] (index 1,1 = target). The smoothness indicators and the weights
+// are computed in R (FP32 on the mixed path); the coefficients and D stay
+// FP64 because every limited value handed to the phase inversion is built
+// from them. Candidate mask by boundary class (ci, cj): stencils that leave
+// the domain are dropped (reconstruction.cpp:150-153). Returns a nonzero
+// PETSC_ERR_FP-class status when a smoothness form is negative beyond
+// roundoff or the weights cannot be normalised.
+template <class R>
+__device__ __forceinline__ int reconstruct(const Tab<R>& t, const StageTables& td, int ci, int cj,
+                                           const double (&u)[3][3], double (&D)[9]) {
     double d[3][3];
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int b = 0; b < 3; ++b) d[a][b] = u[a][b] - ut;
-#pragma unroll
-    for (int m = 0; m < 9; ++m) D[m] = 0.0;
-    const double eA = t.epsA;
-    double alpha[5];
-    double coef[5][9];
+        for (int b = 0; b < 3; ++b) d[a][b] = u[a][b] - u[1][1];
+    // Candidate order: 3x3 at (-1,-1); 2x2 at (0,-1), (0,0), (-1,-1), (-1,0).
+    const int offi[4] = {0, 0, -1, -1}, offj[4] = {-1, 0, -1, 0};
     bool on[5];
-    // Large 3x3 candidate, offset (-1,-1), order 2 (weight exponent s*r+eta = 3+4 = 7).
     on[0] = (ci == 1 && cj == 1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        on[k + 1] = !((offi[k] == 0 && ci == 2) || (offi[k] == -1 && ci == 0) || (offj[k] == 0 && cj == 2) ||
+                      (offj[k] == -1 && cj == 0));
+    R sig[5];
+    int st = 0;
+    // Pass 1: smoothness of every active candidate.
+    if (on[0]) {
+        R diff[8];
+#pragma unroll
+        for (int c = 1; c < 9; ++c) diff[c - 1] = (R)(d[c / 3][c % 3] - d[0][0]);
+        sig[0] = smoothness<R, 8>([&](int r, int c) { return t.S9(r, c); }, diff);
+        if (sig[0] < R(0)) st = MP_ERR_FP;
+    } else {
+        sig[0] = 0;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!on[k + 1]) { sig[k + 1] = 0; continue; }
+        const int oi = offi[k], oj = offj[k];
+        const double a0 = d[1 + oj][1 + oi];
+        R diff[3];
+#pragma unroll
+        for (int c = 1; c < 4; ++c) diff[c - 1] = (R)(d[1 + oj + c / 2][1 + oi + c % 2] - a0);
+        const int tpos = (-oj) * 2 + (-oi);
+        sig[k + 1] = smoothness<R, 3>([&](int r, int c) { return t.S4(tpos, r, c); }, diff);
+        if (sig[k + 1] < R(0)) st = MP_ERR_FP;
+    }
+    double w[5];
+    weights<R>(sig, on, t.epsA(), w);
+    if (!isfinite(w[0] + w[1] + w[2] + w[3] + w[4])) st = MP_ERR_FP;
+    // Pass 2: weighted coefficients accumulated into D (FP64).
+#pragma unroll
+    for (int m = 0; m < 9; ++m) D[m] = 0;
     if (on[0]) {
         double diff[8];
 #pragma unroll
         for (int c = 1; c < 9; ++c) diff[c - 1] = d[c / 3][c % 3] - d[0][0];
-        const double sig = smoothness<8>(t.S9, diff, st);
 #pragma unroll
         for (int m = 0; m < 9; ++m) {
             double v = m == 0 ? d[0][0] : 0.0;
 #pragma unroll
-            for (int c = 1; c < 9; ++c) v += diff[c - 1] * t.C9[c][m];
-            coef[0][m] = v;
+            for (int c = 1; c < 9; ++c) v += diff[c - 1] * td.C9[c][m];
+            D[m] = w[0] * v;
         }
-        const double r = eA / (sig + eA);
-        const double r2 = r * r, r3 = r2 * r;
-        alpha[0] = r3 * r3 * r;
-    } else {
-        alpha[0] = 0.0;
     }
-    // Small 2x2 candidates, order 1 (exponent 2+3 = 5), offsets (0,-1),(0,0),(-1,-1),(-1,0);
-    // target position in the stencil t = tj*2+ti with (ti,tj) = -offset.
-    const int offi[4] = {0, 0, -1, -1}, offj[4] = {-1, 0, -1, 0};
-    const double scale = on[0] ? eA * eA : 1.0;  // alpha_k * (eps A)^7 keeps all terms in range
+    const double X = td.X, Y = td.Y;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
+        if (!on[k + 1]) continue;
         const int oi = offi[k], oj = offj[k];
-        on[k + 1] = !((oi == 0 && ci == 2) || (oi == -1 && ci == 0) || (oj == 0 && cj == 2) || (oj == -1 && cj == 0));
-        if (!on[k + 1]) { alpha[k + 1] = 0.0; continue; }
-        double a4[4];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) a4[s] = d[1 + oj + s / 2][1 + oi + s % 2];
+        const double a0 = d[1 + oj][1 + oi];
         double diff[3];
 #pragma unroll
-        for (int c = 1; c < 4; ++c) diff[c - 1] = a4[c] - a4[0];
-        const int tpos = (-oj) * 2 + (-oi);
-        const double sig = smoothness<3>(t.S4[tpos], diff, st);
+        for (int c = 1; c < 4; ++c) diff[c - 1] = d[1 + oj + c / 2][1 + oi + c % 2] - a0;
         double b[4];
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            double v = m == 0 ? a4[0] : 0.0;
+            double v = m == 0 ? a0 : 0.0;
 #pragma unroll
-            for (int c = 1; c < 4; ++c) v += diff[c - 1] * t.C4[c][m];
+            for (int c = 1; c < 4; ++c) v += diff[c - 1] * td.C4[c][m];
             b[m] = v;
         }
         // Re-expand about the target centre: zeta = xi - delta, delta = ((2oi+1)X, (2oj+1)Y).
-        const double dx = (2 * oi + 1) * t.X, dy = (2 * oj + 1) * t.Y;
-        coef[k + 1][0] = b[0] - b[1] * dx - b[2] * dy + b[3] * dx * dy;
-        coef[k + 1][1] = b[1] - b[3] * dy;
-        coef[k + 1][3] = b[2] - b[3] * dx;
-        coef[k + 1][4] = b[3];
-        const double r = eA / (sig + eA);
-        const double r2 = r * r;
-        alpha[k + 1] = scale * (r2 * r2 * r);
+        const double dx = (double)(2 * oi + 1) * X, dy = (double)(2 * oj + 1) * Y;
+        const double wk = w[k + 1];
+        D[0] += wk * (b[0] - b[1] * dx - b[2] * dy + b[3] * dx * dy);
+        D[1] += wk * (b[1] - b[3] * dy);
+        D[3] += wk * (b[2] - b[3] * dx);
+        D[4] += wk * b[3];
     }
-    double sum = 0.0;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) sum += alpha[k];
-    if (!(sum > 0.0) || !isfinite(sum)) { st = 72; return; }
-    const double inv = 1.0 / sum;
-    if (on[0]) {
-        const double w = alpha[0] * inv;
-#pragma unroll
-        for (int m = 0; m < 9; ++m) D[m] = w * coef[0][m];
-    }
-#pragma unroll
-    for (int k = 1; k < 5; ++k) {
-        if (!on[k]) continue;
-        const double w = alpha[k] * inv;
-        D[0] += w * coef[k][0];
-        D[1] += w * coef[k][1];
-        D[3] += w * coef[k][3];
-        D[4] += w * coef[k][4];
-    }
+    return st;
 }
 
 }  // namespace mp

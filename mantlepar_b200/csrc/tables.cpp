@@ -267,8 +267,9 @@ int build_stage_tables(int nx, int ny, double x0, double x1, double y0, double y
             const V2 r{gp[a], gp[b]};
             t.cw[b * kNQ + a] = gw[a] * gw[b] * jacobian(r, target) / area;
         }
+    for (int q = 0; q < kNQ; ++q) { t.gx[q] = t.X * gp[q]; t.gy[q] = t.Y * gp[q]; }
     // Limiter points per class: class = cj*3 + ci, ci in {0: left wall, 1, 2: right wall}.
-    int at = 0;
+    int at = 0, nl = 0;
     for (int cls = 0; cls < 9; ++cls) {
         t.pt_off[cls] = at;
         const int ci = cls % 3, cj = cls / 3;
@@ -289,8 +290,42 @@ int build_stage_tables(int nx, int ny, double x0, double x1, double y0, double y
         }
         if (at + (int)pts.size() > kMaxPoints) return MP_ERR_ARG_SIZ;
         for (size_t k = 0; k < pts.size(); ++k) { t.pt_x[at] = pts[k].x; t.pt_y[at] = pts[k].y; t.pt_kind[at] = kind[k]; ++at; }
+        // Group the points after the centre into 5-point lines. Each group of
+        // 5 consecutive points (a Gauss row, an edge, or one sample depth of
+        // an edge) shares one normalised coordinate; its other coordinate is
+        // X*g_q or Y*g_q up to the rounding of the bilinear map.
+        t.line_off[cls] = nl;
+        std::vector<std::array<double, 3>> lines;  // dir, fixed coordinate, kind
+        // 5x5 Gauss points were added with a outer (x), b inner (y): regroup into rows.
+        for (int b = 0; b < kNQ; ++b) {
+            double eta = 0;
+            for (int a = 0; a < kNQ; ++a) eta += pts[1 + a * kNQ + b].y;
+            lines.push_back({0.0, eta / kNQ, 0.0});
+        }
+        size_t k = 1 + kNQ * kNQ;
+        for (int e = 0; e < 4; ++e) {
+            const bool row = (e == 0 || e == 2);
+            // edge points, then samples: for each Gauss point, the left-side
+            // samples (2 interior / 4 boundary) -- regroup by depth.
+            double fixed = 0;
+            for (int q = 0; q < kNQ; ++q) fixed += row ? pts[k + q].y : pts[k + q].x;
+            lines.push_back({row ? 0.0 : 1.0, fixed / kNQ, 0.0});
+            k += kNQ;
+            size_t ns = 0;
+            while (k + ns < pts.size() && kind[k + ns] == 1) ++ns;
+            const size_t per = ns / kNQ;   // samples per Gauss point
+            for (size_t d = 0; d < per; ++d) {
+                double f = 0;
+                for (int q = 0; q < kNQ; ++q) f += row ? pts[k + q * per + d].y : pts[k + q * per + d].x;
+                lines.push_back({row ? 0.0 : 1.0, f / kNQ, 1.0});
+            }
+            k += ns;
+        }
+        if (nl + (int)lines.size() > kMaxLines) return MP_ERR_ARG_SIZ;
+        for (const auto& l : lines) { t.line_dir[nl] = (unsigned char)l[0]; t.line_c[nl] = l[1]; t.line_kind[nl] = (unsigned char)l[2]; ++nl; }
     }
     t.pt_off[9] = at;
+    t.line_off[9] = nl;
     return MP_OK;
 }
 

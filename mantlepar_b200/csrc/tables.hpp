@@ -18,6 +18,7 @@ namespace mp {
 
 constexpr int kMaxPoints = 1024;   // limiter points over all 9 classes
 constexpr int kNQ = 5;             // Gauss points per edge / per cell axis
+constexpr int kMaxLines = 256;     // limiter point lines over all 9 classes
 
 struct StageTables {
     // 3x3 candidate (order 2): basis coefficients C9[cell][monomial]
@@ -43,6 +44,17 @@ struct StageTables {
     double pt_x[kMaxPoints];
     double pt_y[kMaxPoints];
     unsigned char pt_kind[kMaxPoints];
+    // The same points grouped into 5-point lines: apart from the cell centre,
+    // every limiter point lies on a row eta = line_c with xi = X*g_q, or on a
+    // column xi = line_c with eta = Y*g_q (q = 0..4). Class c owns lines
+    // [line_off[c], line_off[c+1]); line_dir 0 = row, 1 = column; line_kind
+    // 1 = diffusion samples.
+    int line_off[10];
+    double line_c[kMaxLines];
+    unsigned char line_dir[kMaxLines];
+    unsigned char line_kind[kMaxLines];
+    double gx[kNQ];         // X * g_q
+    double gy[kNQ];         // Y * g_q
 };
 
 // Build the tables of an nx x ny uniform mesh on [x0,x1] x [y0,y1].

@@ -38,6 +38,7 @@ enum : int {
 
 struct Physics {
     PhaseConst k;
+    StageConst sk;
     double Tep;            // pressure-corrected eutectic temperature (constant pressure)
     double theta;          // Darcy exponent
     double inflowH, inflowC;
@@ -64,214 +65,312 @@ __device__ __forceinline__ void record_error(unsigned long long* status, int par
     atomicMin(status, ((unsigned long long)part << 56) | ((unsigned long long)where << 8) | (unsigned long long)(code & 0xff));
 }
 
-__device__ __forceinline__ double ld_ro(const double* p) { return __ldg(p); }
 
-// ---------------------------------------------------------------- cell kernel
+// ------------------------------------------------------- reconstruction kernel
 
-struct CellArgs {
+// Cell flags byte: bit 0 wet (porosity sampling), bit 1 exact diffusion-sample
+// check needed (the cheap bound could not prove admissibility).
+enum : unsigned char { FLAG_WET = 1, FLAG_CHECK = 2 };
+
+template <class R>
+struct ReconArgs {
     int nx, ny;
-    const StageTables* tab;
+    Tab<R> tab;
     const double* H;
     const double* C;
-    double* rec;           // kRec * ncell, SoA
-    unsigned char* wet;
-    double* T;
-    double* phi;
+    double* rec;           // 18 * ncell, SoA: rec[m*N + cell], m < 9 for H
+    unsigned char* flags;
     unsigned long long* status;
     double* theta;         // optional (2 * ncell): limiter factors for H, C
 };
 
-__global__ void __launch_bounds__(128) cell_kernel(CellArgs a, Physics ph) {
+// Max/min of the deviation polynomial over the class's limiter points,
+// evaluated in R from D (FP64). For R = float the points attaining the
+// extremes are re-evaluated in FP64, so theta is formed from FP64 values.
+template <class R>
+__device__ __forceinline__ void scan_lines(const StageTables& t, const Tab<R>& tb, int l0, int l1, const double* Dd,
+                                           double& mx, double& mn, bool& bad) {
+    R D[9];
+#pragma unroll
+    for (int m = 0; m < 9; ++m) D[m] = (R)Dd[m];
+    R rmx = D[0], rmn = D[0];        // cell centre
+    int amx = -1, amn = -1;          // extreme point as line*8 + q (-1 = centre)
+    for (int l = l0; l < l1; ++l) {
+        const R c = tb.line_c(l);
+        R a0, a1, a2;
+        const bool row = t.line_dir[l] == 0;
+        if (row) q2_row(D, c, a0, a1, a2);
+        else q2_col(D, c, a0, a1, a2);
+#pragma unroll
+        for (int q = 0; q < kNQ; ++q) {
+            const R v = quad(a0, a1, a2, row ? tb.gx(q) : tb.gy(q));
+            if constexpr (sizeof(R) == 8) {
+                rmx = fmax(rmx, v); rmn = fmin(rmn, v);
+            } else {
+                if (v > rmx) { rmx = v; amx = l * 8 + q; }
+                if (v < rmn) { rmn = v; amn = l * 8 + q; }
+            }
+            bad = bad || !isfinite(v);
+        }
+    }
+    if constexpr (sizeof(R) == 8) {
+        mx = (double)rmx; mn = (double)rmn;
+    } else {
+        auto at = [&](int code) {
+            if (code < 0) return Dd[0];
+            const int l = code >> 3, q = code & 7;
+            double a0, a1, a2;
+            if (t.line_dir[l] == 0) { q2_row(Dd, t.line_c[l], a0, a1, a2); return quad(a0, a1, a2, t.gx[q]); }
+            q2_col(Dd, t.line_c[l], a0, a1, a2);
+            return quad(a0, a1, a2, t.gy[q]);
+        };
+        mx = at(amx); mn = at(amn);
+    }
+}
+
+// theta of one field: min over points of (bound - mean)/(v - mean) for v
+// outside [lo, hi] (state_reconstruction.cpp:216-224). With v = mean + D and
+// rounding monotone, the minimum is reached at the extreme D, so one
+// division per bound gives the reference's value.
+__device__ __forceinline__ double theta_of(double m, double lo, double hi, double dmax, double dmin) {
+    double th = 1.0;
+    const double vmax = m + dmax, vmin = m + dmin;
+    if (vmax > hi) th = fmin(th, (hi - m) / (vmax - m));
+    if (vmin < lo) th = fmin(th, (lo - m) / (vmin - m));
+    return th < 1.0 ? fmax(0.0, th * (1.0 - 1e-13)) : 1.0;
+}
+
+template <class R>
+__global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= a.nx || j >= a.ny) return;
-    const StageTables& t = *a.tab;
+    const StageTables& t = *a.tab.t;
     const int nx = a.nx, ny = a.ny;
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1);
     const int cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
-    int st = 0;          // reconstruction update (smoothness / weights)
-    int st_lim = 0;      // limiter: admissible means, finite reconstructed values
-    int st_por = 0;      // porosity sampling: phase at the cell points
-    int st_face = 0;     // face loop: diffusion-sample admissibility
-    int st_cell = 0;     // cell quadrature: T >= 0, porosity < 1
+    int st_lim = 0;
 
-    double uh[3][3], uc[3][3];
-    double loH, hiH, loC, hiC;
+    double u[3][3];
+    double DH[9], DC[9];
+    double mH, mC, loH, hiH, loC, hiC;
+    int st = 0;
+    // Enthalpy, then composition: one 3x3 gather at a time keeps registers low.
 #pragma unroll
-    for (int dj = 0; dj < 3; ++dj)
+    for (int f = 0; f < 2; ++f) {
+        const double* F = f ? a.C : a.H;
 #pragma unroll
-        for (int di = 0; di < 3; ++di) {
-            const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
-            uh[dj][di] = ld_ro(a.H + (size_t)jj * nx + ii);
-            uc[dj][di] = ld_ro(a.C + (size_t)jj * nx + ii);
+        for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+            for (int di = 0; di < 3; ++di) {
+                const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
+                u[dj][di] = __ldg(F + (size_t)jj * nx + ii);
+            }
+        // 3x3 neighbour bounds (state_reconstruction.cpp:189-196); the clamped
+        // gather repeats in-domain values, which leaves min/max unchanged.
+        double lo = u[1][1], hi = u[1][1];
+#pragma unroll
+        for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+            for (int di = 0; di < 3; ++di) { lo = fmin(lo, u[dj][di]); hi = fmax(hi, u[dj][di]); }
+        if (f == 0) {
+            mH = u[1][1]; loH = fmax(0.0, lo); hiH = hi;
+            const int s1 = reconstruct<R>(a.tab, t, ci, cj, u, DH);
+            st = st ? st : s1;
+        } else {
+            mC = u[1][1]; loC = fmax(0.0, lo); hiC = fmin(ph.k.Xe, hi);
+            const int s1 = reconstruct<R>(a.tab, t, ci, cj, u, DC);
+            st = st ? st : s1;
         }
-    const double mH = uh[1][1], mC = uc[1][1];
+    }
     // state_reconstruction.cpp:187-188: admissible means.
     if (!(isfinite(mH) && mH >= 0.0 && isfinite(mC) && mC >= 0.0 && mC <= ph.k.Xe)) st_lim = E_OUTOFRANGE;
-    // 3x3 neighbour bounds (state_reconstruction.cpp:189-196); the clamped
-    // gather repeats in-domain values, which leaves min/max unchanged.
-    loH = hiH = mH; loC = hiC = mC;
-#pragma unroll
-    for (int dj = 0; dj < 3; ++dj)
-#pragma unroll
-        for (int di = 0; di < 3; ++di) {
-            loH = fmin(loH, uh[dj][di]); hiH = fmax(hiH, uh[dj][di]);
-            loC = fmin(loC, uc[dj][di]); hiC = fmax(hiC, uc[dj][di]);
-        }
-    loH = fmax(0.0, loH); loC = fmax(0.0, loC); hiC = fmin(ph.k.Xe, hiC);
 
-    double DH[9], DC[9];
-    reconstruct(t, ci, cj, uh, DH, st);
-    reconstruct(t, ci, cj, uc, DC, st);
-
-    // Limiter (state_reconstruction.cpp:197-227): theta over the class's points.
+    // Limiter over the class's points, evaluated line by line.
     const int cls = cj * 3 + ci;
-    double thH = 1.0, thC = 1.0;
-    const int p0 = t.pt_off[cls], p1 = t.pt_off[cls + 1];
-    for (int p = p0; p < p1; ++p) {
-        const double x = t.pt_x[p], y = t.pt_y[p];
-        const double vH = mH + q2(DH, x, y);
-        const double vC = mC + q2(DC, x, y);
-        if (!isfinite(vH) || !isfinite(vC)) { st_lim = st_lim ? st_lim : E_FP; continue; }
-        if (vH > hiH) thH = fmin(thH, (hiH - mH) / (vH - mH));
-        if (vH < loH) thH = fmin(thH, (loH - mH) / (vH - mH));
-        if (vC > hiC) thC = fmin(thC, (hiC - mC) / (vC - mC));
-        if (vC < loC) thC = fmin(thC, (loC - mC) / (vC - mC));
-    }
-    thH = thH < 1.0 ? fmax(0.0, thH * (1.0 - 1e-13)) : 1.0;
-    thC = thC < 1.0 ? fmax(0.0, thC * (1.0 - 1e-13)) : 1.0;
+    const int l0 = t.line_off[cls], l1 = t.line_off[cls + 1];
+    double hmx, hmn, cmx, cmn;
+    bool bad = false;
+    scan_lines<R>(t, a.tab, l0, l1, DH, hmx, hmn, bad);
+    scan_lines<R>(t, a.tab, l0, l1, DC, cmx, cmn, bad);
+    if (bad) st_lim = st_lim ? st_lim : E_FP;
+    const double thH = theta_of(mH, loH, hiH, hmx, hmn);
+    const double thC = theta_of(mC, loC, hiC, cmx, cmn);
     if (a.theta) { a.theta[cell] = thH; a.theta[N + cell] = thC; }
+    // Diffusion samples (zero diffusivity: kept for their admissibility
+    // check). Limited values at limiter points stay in [lo, hi], so the
+    // samples are admissible when hi_H is below the liquidus at hi_C and
+    // Tep >= 0; otherwise the phase kernel checks each sample exactly.
+    const double Hliq = ph.Tep + (1.0 - hiC / ph.k.Xe) + ph.k.LD;
+    const bool safe = ph.Tep >= 0.0 && hiH + 1e-12 * (1.0 + fabs(hiH)) < Hliq;
 #pragma unroll
-    for (int m = 0; m < 9; ++m) { DH[m] *= thH; DC[m] *= thC; }
+    for (int m = 0; m < 9; ++m) {
+        a.rec[(size_t)m * N + cell] = DH[m] * thH;
+        a.rec[(size_t)(m + 9) * N + cell] = DC[m] * thC;
+    }
+    a.flags[cell] = safe ? 0 : FLAG_CHECK;
+    if (st) record_error(a.status, PART_UPDATE, cell, st);
+    if (st_lim) record_error(a.status, PART_LIMIT, cell, st_lim);
+}
 
-    // Cell quadrature of T and phi (evolve.cpp:359-376) and the wet flag of
-    // the porosity sampling (initial_flow.cpp:56-67): same 5x5 points.
+// ---------------------------------------------------------- cell phase kernel
+
+template <class R>
+struct CellPhaseArgs {
+    int nx, ny;
+    Tab<R> tab;
+    const double* H;
+    const double* C;
+    const double* rec;
+    unsigned char* flags;
+    double* T;
+    double* phi;
+    unsigned long long* status;
+};
+
+__device__ __forceinline__ void load_rec(const double* rec, size_t N, long long cell, double* DH, double* DC) {
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+        DH[m] = __ldg(rec + (size_t)m * N + cell);
+        DC[m] = __ldg(rec + (size_t)(m + 9) * N + cell);
+    }
+}
+
+// Cell quadrature of T and phi (evolve.cpp:359-376) and the wet flag of the
+// porosity sampling (initial_flow.cpp:56-67) on the same 5x5 points.
+template <class R>
+__global__ void __launch_bounds__(128) cellphase_kernel(CellPhaseArgs<R> a, Physics ph) {
+    const long long N = (long long)a.nx * a.ny;
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= N) return;
+    const StageTables& t = *a.tab.t;
+    const double mH = __ldg(a.H + cell), mC = __ldg(a.C + cell);
+    double DH[9], DC[9];
+    load_rec(a.rec, (size_t)N, cell, DH, DC);
+    int st_por = 0, st_cell = 0, st_face = 0;
     double Tsum = 0.0, Psum = 0.0;
     bool wet = false;
     for (int b = 0; b < kNQ; ++b) {
-        const double y = t.Y * t.gq[b];
-        for (int aq = 0; aq < kNQ; ++aq) {
-            const double x = t.X * t.gq[aq];
-            const double h = mH + q2(DH, x, y);
-            const double c = mC + q2(DC, x, y);
-            Bounds bd;
-            int s = bounds_at(ph.k, c, ph.Tep, bd);
+        double h0, h1, h2, c0, c1, c2;
+        const double y = t.gy[b];
+        q2_row(DH, y, h0, h1, h2);
+        q2_row(DC, y, c0, c1, c2);
+#pragma unroll
+        for (int q = 0; q < kNQ; ++q) {
+            const double x = t.gx[q];
+            const double h = mH + quad(h0, h1, h2, x);
+            const double c = mC + quad(c0, c1, c2, x);
             PhaseLean pl;
-            if (!s && !isfinite(h)) s = PH_INVALID;
-            if (!s) s = phase_lean(ph.k, h, c, bd, pl);
+            const int s = phase_stage(ph.sk, h, c, ph.Tep, pl);
             if (s) { st_por = st_por ? st_por : s; continue; }
             if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_cell = st_cell ? st_cell : E_OUTOFRANGE;
-            const double w = t.cw[b * kNQ + aq];
+            const double w = t.cw[b * kNQ + q];
             Tsum += w * pl.T;
             Psum += w * pl.phil;
             wet = wet || pl.phil > 0.0;
         }
     }
-    // Diffusion samples (kept for their admissibility check; zero diffusivity):
-    // every limited value at a limiter point lies in [lo, hi], so the samples
-    // are admissible when hi_H is below the liquidus at hi_C and Tep >= 0.
-    {
-        const double Hliq = ph.Tep + (1.0 - hiC / ph.k.Xe) + ph.k.LD;
-        const bool safe = ph.Tep >= 0.0 && hiH + 1e-12 * (1.0 + fabs(hiH)) < Hliq;
-        if (!safe) {
-            for (int p = p0; p < p1; ++p) {
-                if (!t.pt_kind[p]) continue;
-                const double x = t.pt_x[p], y = t.pt_y[p];
-                const double h = mH + q2(DH, x, y);
-                const double c = mC + q2(DC, x, y);
-                Bounds bd;
-                int s = bounds_at(ph.k, c, ph.Tep, bd);
+    const unsigned char fl = a.flags[cell];
+    if (fl & FLAG_CHECK) {
+        // Exact admissibility of the limited values at the diffusion samples.
+        const int i = (int)(cell % a.nx), j = (int)(cell / a.nx);
+        const int ci = i == 0 ? 0 : (i == a.nx - 1 ? 2 : 1);
+        const int cj = j == 0 ? 0 : (j == a.ny - 1 ? 2 : 1);
+        const int cls = cj * 3 + ci;
+        for (int l = t.line_off[cls]; l < t.line_off[cls + 1]; ++l) {
+            if (!t.line_kind[l]) continue;
+            double h0, h1, h2, c0, c1, c2;
+            const bool row = t.line_dir[l] == 0;
+            const double lc = t.line_c[l];
+            if (row) { q2_row(DH, lc, h0, h1, h2); q2_row(DC, lc, c0, c1, c2); }
+            else { q2_col(DH, lc, h0, h1, h2); q2_col(DC, lc, c0, c1, c2); }
+            for (int q = 0; q < kNQ; ++q) {
+                const double s_ = row ? t.gx[q] : t.gy[q];
+                const double h = mH + quad(h0, h1, h2, s_);
+                const double c = mC + quad(c0, c1, c2, s_);
                 PhaseLean pl;
-                if (!s && !isfinite(h)) s = PH_INVALID;
-                if (!s) s = phase_lean(ph.k, h, c, bd, pl);
+                const int s = phase_stage(ph.sk, h, c, ph.Tep, pl);
                 if (s) { st_face = st_face ? st_face : s; continue; }
                 if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_face = st_face ? st_face : E_OUTOFRANGE;
             }
         }
     }
-    if (st) record_error(a.status, PART_UPDATE, cell, st);
-    if (st_lim) record_error(a.status, PART_LIMIT, cell, st_lim);
     if (st_por) record_error(a.status, PART_POROSITY, cell, st_por);
     if (st_face) record_error(a.status, PART_FACES, cell, st_face);
     if (st_cell) record_error(a.status, PART_CELLS, cell, st_cell);
-#pragma unroll
-    for (int m = 0; m < 9; ++m) {
-        a.rec[(size_t)m * N + cell] = DH[m];
-        a.rec[(size_t)(m + 9) * N + cell] = DC[m];
-    }
-    a.wet[cell] = wet ? 1 : 0;
+    a.flags[cell] = (unsigned char)((fl & FLAG_CHECK) | (wet ? FLAG_WET : 0));
     a.T[cell] = Tsum;
     a.phi[cell] = Psum;
 }
 
 // ---------------------------------------------------------------- face kernel
 
+template <class R>
 struct FaceArgs {
     int nx, ny;
-    const StageTables* tab;
+    Tab<R> tab;
     const double* H;
     const double* C;
     const double* rec;
-    const unsigned char* wet;
+    const unsigned char* flags;
     const double* vsn;     // [edge*5 + q], canonical
     const double* udn;
     double* face;          // 4 * nedge SoA: fluxH, fluxC, rate, fluxMixture
     unsigned long long* status;
 };
 
-struct Side {
+// Limited H and C of one side along the edge line: v(s) = m + c0 + s*(c1 + s*c2).
+struct SideLine {
     double mH, mC;
-    double DH[9], DC[9];
+    double h0, h1, h2, c0, c1, c2;
 };
 
-__device__ __forceinline__ void load_side(const FaceArgs& a, size_t N, long long cell, Side& s) {
-    s.mH = ld_ro(a.H + cell);
-    s.mC = ld_ro(a.C + cell);
-#pragma unroll
-    for (int m = 0; m < 9; ++m) {
-        s.DH[m] = ld_ro(a.rec + (size_t)m * N + cell);
-        s.DC[m] = ld_ro(a.rec + (size_t)(m + 9) * N + cell);
-    }
+template <class R>
+__device__ __forceinline__ void side_line(const FaceArgs<R>& a, size_t N, long long cell, bool row, double fixed,
+                                          SideLine& s) {
+    double DH[9], DC[9];
+    load_rec(a.rec, N, cell, DH, DC);
+    s.mH = __ldg(a.H + cell);
+    s.mC = __ldg(a.C + cell);
+    if (row) { q2_row(DH, fixed, s.h0, s.h1, s.h2); q2_row(DC, fixed, s.c0, s.c1, s.c2); }
+    else { q2_col(DH, fixed, s.h0, s.h1, s.h2); q2_col(DC, fixed, s.c0, s.c1, s.c2); }
 }
 
 // Limited evaluation + phase + Phase()'s admissibility (evolve.cpp:270-277).
-__device__ __forceinline__ int side_phase(const Physics& ph, const Side& s, double x, double y, double& h, double& c,
+__device__ __forceinline__ int side_phase(const Physics& ph, const SideLine& s, double at, double& h, double& c,
                                           PhaseLean& pl) {
-    h = s.mH + q2(s.DH, x, y);
-    c = s.mC + q2(s.DC, x, y);
-    Bounds bd;
-    int st = bounds_at(ph.k, c, ph.Tep, bd);
-    if (!st && !isfinite(h)) st = PH_INVALID;
-    if (!st) st = phase_lean(ph.k, h, c, bd, pl);
+    h = s.mH + quad(s.h0, s.h1, s.h2, at);
+    c = s.mC + quad(s.c0, s.c1, s.c2, at);
+    int st = phase_stage(ph.sk, h, c, ph.Tep, pl);
     if (!st && !(pl.T >= 0.0 && pl.phil < 1.0)) st = E_OUTOFRANGE;
     return st;
 }
 
-__global__ void __launch_bounds__(128) face_kernel(FaceArgs a, Physics ph) {
+template <class R>
+__global__ void __launch_bounds__(128) face_kernel(FaceArgs<R> a, Physics ph) {
     const int nx = a.nx, ny = a.ny;
     const long long nI = (long long)nx * (ny + 1);
     const long long nE = nI + (long long)(nx + 1) * ny;
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nE) return;
-    const StageTables& t = *a.tab;
+    const StageTables& t = *a.tab.t;
     const size_t N = (size_t)nx * ny;
     bool boundary, reverse, horizontal;
-    long long L, R = -1;
+    long long L, Rc = -1;
     double len;
-    // Left/right cells and frames as the reference's Build (evolve.cpp:230-251).
-    double lx, ly, rx, ry;       // edge position in the left/right cell frame: fixed coordinate
+    double lfix, rfix;   // the edge's fixed normalised coordinate in the left / right cell frame
+    // Left/right cells and orientation as the reference's Build (evolve.cpp:230-251).
     if (e < nI) {
         horizontal = true;
         const int i = (int)(e % nx), j = (int)(e / nx);
         boundary = (j == 0 || j == ny);
         reverse = (j == ny);
         L = reverse ? (long long)(ny - 1) * nx + i : (long long)j * nx + i;
-        if (!boundary) R = (long long)(j - 1) * nx + i;
-        ly = reverse ? t.Y : -t.Y;   // edge row in the left cell's frame
-        ry = t.Y;
-        lx = rx = 0.0;
+        if (!boundary) Rc = (long long)(j - 1) * nx + i;
+        lfix = reverse ? t.Y : -t.Y;
+        rfix = t.Y;
         len = t.len_h;
     } else {
         horizontal = false;
@@ -280,33 +379,30 @@ __global__ void __launch_bounds__(128) face_kernel(FaceArgs a, Physics ph) {
         boundary = (i == 0 || i == nx);
         reverse = (i == 0);
         L = reverse ? (long long)j * nx : (long long)j * nx + (i - 1);
-        if (!boundary) R = (long long)j * nx + i;
-        lx = reverse ? -t.X : t.X;
-        rx = -t.X;
-        ly = ry = 0.0;
+        if (!boundary) Rc = (long long)j * nx + i;
+        lfix = reverse ? -t.X : t.X;
+        rfix = -t.X;
         len = t.len_v;
     }
-    Side sl, sr;
-    load_side(a, N, L, sl);
-    if (!boundary) load_side(a, N, R, sr);
-    const bool wetL = a.wet[L] != 0, wetR = boundary ? true : a.wet[R] != 0;
+    SideLine sl, sr;
+    side_line(a, N, L, horizontal, lfix, sl);
+    if (!boundary) side_line(a, N, Rc, horizontal, rfix, sr);
+    const bool wetL = (a.flags[L] & FLAG_WET) != 0, wetR = boundary ? true : (a.flags[Rc] & FLAG_WET) != 0;
     const double sgn = reverse ? -1.0 : 1.0;
     const double LD = ph.k.LD;
     double fluxH = 0.0, fluxC = 0.0, fluxMix = 0.0, rate = 0.0;
     int st = 0;
     for (int q = 0; q < kNQ; ++q) {
         const int cq = reverse ? kNQ - 1 - q : q;
-        const double g = t.gq[cq];
-        const double vs = sgn * ld_ro(a.vsn + e * kNQ + cq);
-        const double ud = sgn * ld_ro(a.udn + e * kNQ + cq);
-        const double xl = horizontal ? t.X * g : lx, yl = horizontal ? ly : t.Y * g;
+        const double at = horizontal ? t.gx[cq] : t.gy[cq];
+        const double vs = sgn * __ldg(a.vsn + e * kNQ + cq);
+        const double ud = sgn * __ldg(a.udn + e * kNQ + cq);
         double hL, cL, hR, cR;
         PhaseLean A, B;
-        int s = side_phase(ph, sl, xl, yl, hL, cL, A);
+        int s = side_phase(ph, sl, at, hL, cL, A);
         if (boundary) { B = A; hR = hL; cR = cL; }
         else {
-            const double xr = horizontal ? t.X * g : rx, yr = horizontal ? ry : t.Y * g;
-            const int s2 = side_phase(ph, sr, xr, yr, hR, cR, B);
+            const int s2 = side_phase(ph, sr, at, hR, cR, B);
             s = s ? s : s2;
         }
         if (s) { st = st ? st : s; continue; }
@@ -328,17 +424,15 @@ __global__ void __launch_bounds__(128) face_kernel(FaceArgs a, Physics ph) {
         double fc = 0.5 * (ve * (cL + cR) - aC * (cR - cL));
         if (boundary) {
             // EvaluateAdvectionBoundary (initialization.cpp:469-489) per field.
-            int kh = (ph.Hpol == MP_BC_ZERO_FLUX || vn == 0.0) ? 2 : (vn < 0.0 ? 0 : 1);
-            int kc = (ph.Cpol == MP_BC_ZERO_FLUX || ve == 0.0) ? 2 : (ve < 0.0 ? 0 : 1);
+            const int kh = (ph.Hpol == MP_BC_ZERO_FLUX || vn == 0.0) ? 2 : (vn < 0.0 ? 0 : 1);
+            const int kc = (ph.Cpol == MP_BC_ZERO_FLUX || ve == 0.0) ? 2 : (ve < 0.0 ? 0 : 1);
             if ((kh == 0 && ph.Hpol != MP_BC_INFLOW_OUTFLOW) || (kc == 0 && ph.Cpol != MP_BC_INFLOW_OUTFLOW))
                 st = st ? st : E_OUTOFRANGE;
             const double inC = kc == 0 ? ph.inflowC : cL;
             double Tb = A.T;
             if (kh == 0) {
-                Bounds bd;
                 PhaseLean pin;
-                int s3 = bounds_at(ph.k, inC, ph.Tep, bd);
-                if (!s3) s3 = phase_lean(ph.k, ph.inflowH, inC, bd, pin);
+                const int s3 = phase_stage(ph.sk, ph.inflowH, inC, ph.Tep, pin);
                 if (s3) st = st ? st : s3;
                 Tb = pin.T;
             }
@@ -531,8 +625,10 @@ struct mp_transport {
     double *S2H = nullptr, *S2C = nullptr;
     double *LH = nullptr, *LC = nullptr;    // L(U^n)
     double *T = nullptr, *phi = nullptr;
-    double* rec = nullptr;
-    unsigned char* wet = nullptr;
+    void* rec = nullptr;                    // 18 * N doubles (limited deviation polynomials)
+    unsigned char* flags = nullptr;         // wet | exact-check flags per cell
+    mp::StageTablesF* tabF = nullptr;       // FP32 tables (mixed precision)
+    bool mixed = false;
     double *vsn = nullptr, *udn = nullptr;
     double* face = nullptr;
     double* rate = nullptr;
@@ -551,14 +647,25 @@ struct mp_transport {
     std::vector<cudaEvent_t> ev_pool;
     std::vector<int> ev_kind;              // pending pairs: kind of kernel
     size_t ev_used = 0;
-    double kern_ms[4] = {0, 0, 0, 0};
-    unsigned long long kern_n[4] = {0, 0, 0, 0};
+    double kern_ms[6] = {0, 0, 0, 0, 0, 0};
+    unsigned long long kern_n[6] = {0, 0, 0, 0, 0, 0};
 };
 
 namespace mp {
 namespace {
 
-// Event pair around one kernel when profiling (kind: 0 cell, 1 face, 2 sum, 3 other).
+void tables_to_float(const StageTables& t, StageTablesF& f) {
+    for (int a = 0; a < 9; ++a) for (int b = 0; b < 9; ++b) f.C9[a][b] = (float)t.C9[a][b];
+    for (int a = 0; a < 8; ++a) for (int b = 0; b < 8; ++b) f.S9[a][b] = (float)t.S9[a][b];
+    for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) f.C4[a][b] = (float)t.C4[a][b];
+    for (int k = 0; k < 4; ++k) for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) f.S4[k][a][b] = (float)t.S4[k][a][b];
+    f.X = (float)t.X; f.Y = (float)t.Y; f.epsA = (float)t.epsA; f.logEpsA2 = (float)(2.0 * std::log(t.epsA));
+    for (int q = 0; q < kNQ; ++q) { f.gx[q] = (float)t.gx[q]; f.gy[q] = (float)t.gy[q]; }
+    for (int l = 0; l < kMaxLines; ++l) f.line_c[l] = (float)t.line_c[l];
+}
+
+// Event pair around one kernel when profiling
+// (kind: 0 reconstruction/limiter, 1 cell phase, 2 face, 3 sum, 4 axpy/reductions).
 cudaEvent_t prof_event(mp_transport* t) {
     if (t->ev_used == t->ev_pool.size()) {
         cudaEvent_t e;
@@ -590,8 +697,8 @@ void harvest(mp_transport* t) {
 
 void free_all(mp_transport* t) {
     for (cudaEvent_t e : t->ev_pool) cudaEventDestroy(e);
-    void* bufs[] = {t->tab, t->H, t->C, t->S1H, t->S1C, t->S2H, t->S2C, t->LH, t->LC, t->T, t->phi, t->rec,
-                    t->wet, t->vsn, t->udn, t->face, t->rate, t->partial, t->d_tot, t->d_status};
+    void* bufs[] = {t->tab, t->tabF, t->H, t->C, t->S1H, t->S1C, t->S2H, t->S2C, t->LH, t->LC, t->T, t->phi,
+                    t->rec, t->flags, t->vsn, t->udn, t->face, t->rate, t->partial, t->d_tot, t->d_status};
     for (void* b : bufs) if (b) cudaFree(b);
     if (t->h_tot) cudaFreeHost(t->h_tot);
     if (t->h_status) cudaFreeHost(t->h_status);
@@ -611,26 +718,51 @@ mp_status check_status(mp_transport* t, const char* where) {
     return (mp_status)code;
 }
 
+// Launch the stage kernels of state (H, C) in arithmetic type R.
+template <class R>
+void launch_stage_kernels(int nx, int ny, Tab<R> tb, const Physics& ph, const double* H, const double* C, double* rec,
+                          unsigned char* flags, double* T, double* phi, const double* vsn, const double* udn,
+                          double* face, unsigned long long* status, double* theta, cudaStream_t s,
+                          mp_transport* prof) {
+    const size_t N = (size_t)nx * ny;
+    const size_t NE = (size_t)nx * (ny + 1) + (size_t)(nx + 1) * ny;
+    auto run = [&](int kind, auto&& f) { if (prof) timed(prof, kind, f); else f(); };
+    {
+        ReconArgs<R> a{nx, ny, tb, H, C, rec, flags, status, theta};
+        dim3 blk(32, 4), grd((nx + 31) / 32, (ny + 3) / 4);
+        run(0, [&] { recon_kernel<R><<<grd, blk, 0, s>>>(a, ph); });
+    }
+    {
+        CellPhaseArgs<R> a{nx, ny, tb, H, C, rec, flags, T, phi, status};
+        run(1, [&] { cellphase_kernel<R><<<(unsigned)((N + 127) / 128), 128, 0, s>>>(a, ph); });
+    }
+    {
+        FaceArgs<R> a{nx, ny, tb, H, C, rec, flags, vsn, udn, face, status};
+        run(2, [&] { face_kernel<R><<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(a, ph); });
+    }
+}
+
 // Launch one stage evaluation of state (H, C). mode SUM_STORE_L writes L to
 // (outH, outC); SUM_RK writes a0*U^n + a1*(U + dt*L). Totals land in *d_tot.
 mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mode, double a0, double a1, double dt,
                        double* outH, double* outC, double* theta = nullptr) {
     cudaStream_t s = t->stream;
-    {
-        CellArgs a{t->nx, t->ny, t->tab, H, C, t->rec, t->wet, t->T, t->phi, t->d_status, theta};
-        dim3 blk(32, 4), grd((t->nx + 31) / 32, (t->ny + 3) / 4);
-        timed(t, 0, [&] { cell_kernel<<<grd, blk, 0, s>>>(a, t->ph); });
-    }
-    {
-        FaceArgs a{t->nx, t->ny, t->tab, H, C, t->rec, t->wet, t->vsn, t->udn, t->face, t->d_status};
-        timed(t, 1, [&] { face_kernel<<<(unsigned)((t->NE + 127) / 128), 128, 0, s>>>(a, t->ph); });
+    mp_transport* prof = t->profile ? t : nullptr;
+    if (t->mixed) {
+        Tab<float> tb{t->tab, t->tabF};
+        launch_stage_kernels<float>(t->nx, t->ny, tb, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
+                                    t->vsn, t->udn, t->face, t->d_status, theta, s, prof);
+    } else {
+        Tab<double> tb{t->tab};
+        launch_stage_kernels<double>(t->nx, t->ny, tb, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T,
+                                     t->phi, t->vsn, t->udn, t->face, t->d_status, theta, s, prof);
     }
     {
         SumArgs a{t->nx, t->ny, t->tab, t->face, H, C, t->H, t->C, outH, outC, t->rate, mode, a0, a1, dt, t->partial};
-        timed(t, 2, [&] { sum_kernel<<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
+        timed(t, 3, [&] { sum_kernel<<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
     }
-    timed(t, 3, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, t->sum_blocks, t->d_tot); });
-    count_launch(4);
+    timed(t, 4, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, t->sum_blocks, t->d_tot); });
+    count_launch(5);
     MP_CUDA(cudaGetLastError());
     return MP_OK;
 }
@@ -693,11 +825,11 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
         }
         bool valid, failed;
         Totals adm;
-        timed(t, 3, [&] {
+        timed(t, 4, [&] {
             axpy_kernel<<<nblk_axpy, kRedBlock, 0, s>>>((int)t->N, t->H, t->C, t->LH, t->LC, dt, t->host_tab.area,
                                                          t->S1H, t->S1C, t->partial);
         });
-        timed(t, 3, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, nblk_axpy, t->d_tot); });
+        timed(t, 4, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, nblk_axpy, t->d_tot); });
         count_launch(2);
         MP_CUDA(cudaGetLastError());
         MP_TRY(read_totals(t, adm, failed, "stage 1"));
@@ -781,7 +913,7 @@ extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_tran
     if (opts->integrator != MP_SSPRK2 && opts->integrator != MP_SSPRK3) { set_error("integrator must be 2 or 3"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->diffusivity != 0.0) { set_error("thermal diffusion (kappa > 0) is not supported by this build"); return MP_ERR_ARG_WRONG; }
     if (opts->material.alpha0 != 0.0) { set_error("adiabatic source (alpha0 != 0) needs cell-point velocities; not supported by this build"); return MP_ERR_ARG_WRONG; }
-    if (opts->precision != MP_PRECISION_FP64) { set_error("mixed precision is served by the batched path"); return MP_ERR_ARG_WRONG; }
+    if (opts->precision != MP_PRECISION_FP64 && opts->precision != MP_PRECISION_MIXED) { set_error("unknown precision"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->H_policy < 0 || opts->H_policy > 2 || opts->C_policy < 0 || opts->C_policy > 2) { set_error("unknown boundary policy"); return MP_ERR_ARG_OUTOFRANGE; }
     mp_derived der;
     MP_TRY(derive_checked(opts->material, der));
@@ -793,6 +925,8 @@ extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_tran
     t->N = (size_t)t->nx * t->ny;
     t->NE = (size_t)t->nx * (t->ny + 1) + (size_t)(t->nx + 1) * t->ny;
     t->ph.k = phase_const(opts->material, der);
+    t->ph.sk = stage_const(t->ph.k);
+    t->mixed = opts->precision == MP_PRECISION_MIXED;
     double Tep;
     if (eutectic_temperature(t->ph.k, opts->pressure, Tep)) { delete t; set_error("pressure must be finite"); return MP_ERR_ARG_OUTOFRANGE; }
     t->ph.Tep = Tep; t->ph.theta = opts->theta;
@@ -809,7 +943,8 @@ extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_tran
     for (double** p : {&t->H, &t->C, &t->S1H, &t->S1C, &t->S2H, &t->S2C, &t->LH, &t->LC, &t->T, &t->phi, &t->rate})
         alloc((void**)p, N * sizeof(double));
     alloc((void**)&t->rec, (size_t)kRec * N * sizeof(double));
-    alloc((void**)&t->wet, N);
+    alloc((void**)&t->flags, N);
+    if (t->mixed) alloc((void**)&t->tabF, sizeof(StageTablesF));
     alloc((void**)&t->vsn, NE * kNQ * sizeof(double));
     alloc((void**)&t->udn, NE * kNQ * sizeof(double));
     alloc((void**)&t->face, 4 * NE * sizeof(double));
@@ -819,6 +954,11 @@ extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_tran
     if (e == cudaSuccess) e = cudaMallocHost((void**)&t->h_tot, sizeof(Totals));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&t->h_status, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemcpyAsync(t->tab, &t->host_tab, sizeof(StageTables), cudaMemcpyHostToDevice, t->stream);
+    StageTablesF tf;
+    if (t->mixed) {
+        tables_to_float(t->host_tab, tf);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(t->tabF, &tf, sizeof(StageTablesF), cudaMemcpyHostToDevice, t->stream);
+    }
     if (e == cudaSuccess) e = cudaMemsetAsync(t->vsn, 0, NE * kNQ * sizeof(double), t->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(t->udn, 0, NE * kNQ * sizeof(double), t->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
@@ -923,7 +1063,7 @@ extern "C" mp_status mp_transport_profile(mp_transport* t, int enable) {
     MP_CUDA(cudaStreamSynchronize(t->stream));
     mp::harvest(t);
     t->profile = enable != 0;
-    for (int k = 0; k < 4; ++k) { t->kern_ms[k] = 0; t->kern_n[k] = 0; }
+    for (int k = 0; k < 6; ++k) { t->kern_ms[k] = 0; t->kern_n[k] = 0; }
     return MP_OK;
 }
 
@@ -931,7 +1071,7 @@ extern "C" mp_status mp_transport_kernel_times(mp_transport* t, double* ms, unsi
     if (!t || !ms || !launches) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
     MP_CUDA(cudaStreamSynchronize(t->stream));
     mp::harvest(t);
-    for (int k = 0; k < 4; ++k) { ms[k] = t->kern_ms[k]; launches[k] = t->kern_n[k]; }
+    for (int k = 0; k < 6; ++k) { ms[k] = t->kern_ms[k]; launches[k] = t->kern_n[k]; }
     return MP_OK;
 }
 
@@ -998,6 +1138,7 @@ mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double
     MP_TRY(derive_checked(o.material, der));
     Physics ph;
     ph.k = phase_const(o.material, der);
+    ph.sk = stage_const(ph.k);
     if (eutectic_temperature(ph.k, o.pressure, ph.Tep)) { set_error("pressure must be finite"); return MP_ERR_ARG_OUTOFRANGE; }
     ph.theta = o.theta; ph.inflowH = o.inflow_H; ph.inflowC = o.inflow_C;
     ph.Hpol = o.H_policy; ph.Cpol = o.C_policy; ph.lf_global = o.lf_global; ph.lf_speed = o.lf_global_speed;
@@ -1007,21 +1148,15 @@ mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double
     Partial* part = static_cast<Partial*>(partial);
     Totals* tot = static_cast<Totals*>(totals);
     MP_CUDA(cudaMemsetAsync(status, 0xff, sizeof(unsigned long long), s));
-    {
-        CellArgs a{nx, ny, tab, H, C, rec, wet, T, phi, status, nullptr};
-        dim3 blk(32, 4), grd((nx + 31) / 32, (ny + 3) / 4);
-        cell_kernel<<<grd, blk, 0, s>>>(a, ph);
-    }
-    {
-        FaceArgs a{nx, ny, tab, H, C, rec, wet, vsn, udn, face, status};
-        face_kernel<<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(a, ph);
-    }
+    (void)NE;
+    launch_stage_kernels<double>(nx, ny, Tab<double>{tab}, ph, H, C, rec, wet, T, phi, vsn, udn, face, status, nullptr,
+                                 s, nullptr);
     {
         SumArgs a{nx, ny, tab, face, H, C, H, C, rhsH, rhsC, rate, SUM_STORE_L, 0.0, 0.0, 0.0, part};
         sum_kernel<<<sum_blocks, kRedBlock, 0, s>>>(a);
     }
     reduce_kernel<<<1, 1024, 0, s>>>(part, sum_blocks, tot);
-    count_launch(4);
+    count_launch(5);
     MP_CUDA(cudaGetLastError());
     Totals host_tot;
     unsigned long long host_status = 0;
