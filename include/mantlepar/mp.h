@@ -183,6 +183,41 @@ mp_status mp_transport_step(mp_transport* t, int nsteps, mp_step_report* reports
  * (StateReconstruction::Limit, src/couple/state_reconstruction.cpp:136-192). */
 mp_status mp_transport_limiter(mp_transport* t, double* thetaH, double* thetaC);
 
+/* --------------------------------------------------------------- batched */
+
+/* Many independent transport instances of uneven size advanced together
+ * (no counterpart in the reference, which runs one mesh per MPI job). Each
+ * instance keeps the reference's semantics on its own: own dt from its CFL
+ * rate, stage admissibility and courant retries, balance check, rollback on
+ * failure (src/couple/evolve.cpp:449-507); one launch per stage kernel covers
+ * all instances. Results are bitwise those of a single-instance run. */
+typedef struct mp_batch mp_batch;
+mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, const mp_transport_opts* opts,
+                          mp_stream_t stream, mp_batch** out);
+void mp_batch_destroy(mp_batch* b);
+/* Add an instance in a free slot (or a new one); remove frees its memory. */
+mp_status mp_batch_add(mp_batch* b, const mp_mesh_desc* mesh, int* instance);
+mp_status mp_batch_remove(mp_batch* b, int instance);
+/* Device bytes one instance of this mesh holds (memory admission). */
+size_t mp_batch_instance_bytes(const mp_mesh_desc* mesh);
+size_t mp_batch_bytes_in_use(const mp_batch* b);
+int mp_batch_slots(const mp_batch* b);
+mp_status mp_batch_set_face_velocity(mp_batch* b, int instance, const double* vs_n, const double* ud_n);
+mp_status mp_batch_set_state(mp_batch* b, int instance, const double* H, const double* C, double time);
+/* Any output pointer may be NULL; status is the instance's sticky failure
+ * status (0 = healthy). */
+mp_status mp_batch_get_state(mp_batch* b, int instance, double* H, double* C, double* T, double* phi,
+                             double* time, int* accepted, int* status);
+/* nsteps accepted steps of every healthy instance; reports (may be NULL)
+ * holds nsteps * slots entries, step-major; an instance that fails stops
+ * (its status is reported) while the others continue. */
+mp_status mp_batch_step(mp_batch* b, int nsteps, mp_step_report* reports);
+/* Project autotuner: times the candidate reconstruction tile shapes and
+ * cells-per-thread on this batch and keeps the fastest; tile = {bx, by, cpt}. */
+mp_status mp_batch_autotune(mp_batch* b, int reps, int tile[3], double* best_ms);
+mp_status mp_batch_profile(mp_batch* b, int enable);
+mp_status mp_batch_kernel_times(mp_batch* b, double ms[6], unsigned long long launches[6]);
+
 /* One stage evaluation (as mp_transport_rhs) that allocates no device memory,
  * for callers that cannot call cudaMalloc -- e.g. code inside a framework that
  * owns all device memory through its own pool, or code that must not allocate

@@ -111,6 +111,20 @@ def lib() -> C.CDLL:
         "mp_probe_fp64_peak": (i, [vp, C.POINTER(C.c_double)]),
         "mp_transport_rhs_noalloc": (i, [C.POINTER(MeshDesc), C.POINTER(TransportOpts), vp, vp, vp, vp,
                                          vp, vp, vp, vp, vp, C.POINTER(StageTotals), vp]),
+        "mp_batch_create": (i, [C.POINTER(MeshDesc), i, C.POINTER(TransportOpts), vp, C.POINTER(vp)]),
+        "mp_batch_destroy": (None, [vp]),
+        "mp_batch_add": (i, [vp, C.POINTER(MeshDesc), C.POINTER(C.c_int)]),
+        "mp_batch_remove": (i, [vp, i]),
+        "mp_batch_instance_bytes": (sz, [C.POINTER(MeshDesc)]),
+        "mp_batch_bytes_in_use": (sz, [vp]),
+        "mp_batch_slots": (i, [vp]),
+        "mp_batch_set_face_velocity": (i, [vp, i, vp, vp]),
+        "mp_batch_set_state": (i, [vp, i, vp, vp, d]),
+        "mp_batch_get_state": (i, [vp, i, vp, vp, vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "mp_batch_step": (i, [vp, i, C.POINTER(StepReport)]),
+        "mp_batch_autotune": (i, [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+        "mp_batch_profile": (i, [vp, i]),
+        "mp_batch_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

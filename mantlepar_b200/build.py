@@ -21,7 +21,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmantlepar_b200.so")
 
-SOURCES = ["phase_api.cu", "transport.cu", "tables.cpp", "mp_noalloc.cu"]
+SOURCES = ["phase_api.cu", "transport.cu", "tables.cpp", "mp_noalloc.cu", "batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
          "-I", os.path.join(ROOT, "include")]

@@ -1,0 +1,790 @@
+// Batched transport: many independent meshes of uneven size advanced
+// together, each with its own dt, CFL retries, balance check and status.
+//
+// Every stage is one launch per kernel over ALL active instances: a device
+// work map sends each thread block to (instance, tile) and the block's
+// instance record holds that instance's buffers and tables. The per-element
+// arithmetic is the single-instance path's (stage_kernels.cuh), and the
+// block grouping of the reductions is per instance, so each instance's
+// result is bitwise the same alone and in a batch.
+//
+// The step logic is the reference's Run loop (src/couple/evolve.cpp:449-507)
+// applied per instance: dt = min(cap, cfl/rate), stage-1 admissibility,
+// courant check over the stage rates, admissibility of the combined state,
+// halve-and-retry (<= 40), balance check, rollback on failure. Instances that
+// need a retry run the next attempt while finished instances wait.
+#include "common.hpp"
+#include "phase_math.cuh"
+#include "stage_device.cuh"
+#include "stage_kernels.cuh"
+#include "tables.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace mp {
+
+PhaseConst phase_const(const mp_material& p, const mp_derived& d);
+mp_status derive_checked(const mp_material& p, mp_derived& d);
+
+namespace {
+
+void tables_to_float_b(const StageTables& t, StageTablesF& f) {
+    for (int a = 0; a < 9; ++a) for (int b = 0; b < 9; ++b) f.C9[a][b] = (float)t.C9[a][b];
+    for (int a = 0; a < 8; ++a) for (int b = 0; b < 8; ++b) f.S9[a][b] = (float)t.S9[a][b];
+    for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) f.C4[a][b] = (float)t.C4[a][b];
+    for (int k = 0; k < 4; ++k) for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) f.S4[k][a][b] = (float)t.S4[k][a][b];
+    f.X = (float)t.X; f.Y = (float)t.Y; f.epsA = (float)t.epsA; f.logEpsA2 = (float)(2.0 * std::log(t.epsA));
+    for (int q = 0; q < kNQ; ++q) { f.gx[q] = (float)t.gx[q]; f.gy[q] = (float)t.gy[q]; }
+    for (int l = 0; l < kMaxLines; ++l) f.line_c[l] = (float)t.line_c[l];
+}
+
+// Stage kinds: P evaluates L(U^n) (store L), B the second stage (RK combine
+// into S2), C the third stage of SSPRK3 (RK combine into S1).
+enum : int { KIND_P = 0, KIND_B = 1, KIND_C = 2, NKIND = 3 };
+
+// Per-instance records of one stage kind, read by the batched kernels.
+template <class R>
+struct InstArgs {
+    ReconArgs<R> recon;
+    CellPhaseArgs<R> phase;
+    FaceArgs<R> face;
+    SumArgs sum;
+};
+
+struct AxpyArgs {
+    int n;
+    const double *H0, *C0, *LH, *LC;
+    double *H1, *C1;
+    const double* dtp;
+    double area;
+    Partial* partial;
+};
+
+// Work items: block -> instance and the first element of its tile.
+struct Work { int inst, a, b, part; };
+
+struct Tuning { int bx = 32, by = 4, cpt = 1; };
+
+// ------------------------------------------------------------ batched kernels
+
+template <class R>
+__global__ void __launch_bounds__(128) batch_recon_kernel(const InstArgs<R>* args, const Work* work, const int* active,
+                                                          Physics ph, int cpt) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    const ReconArgs<R>& a = args[w.inst].recon;
+    const int j = w.b + threadIdx.y;
+    for (int c = 0; c < cpt; ++c) recon_cell(a, ph, w.a + c * blockDim.x + threadIdx.x, j);
+}
+
+template <class R>
+__global__ void __launch_bounds__(128) batch_phase_kernel(const InstArgs<R>* args, const Work* work, const int* active,
+                                                          Physics ph) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    cellphase_cell(args[w.inst].phase, ph, (long long)w.a + threadIdx.x);
+}
+
+template <class R>
+__global__ void __launch_bounds__(128) batch_face_kernel(const InstArgs<R>* args, const Work* work, const int* active,
+                                                         Physics ph) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    face_edge(args[w.inst].face, ph, (long long)w.a + threadIdx.x);
+}
+
+template <class R>
+__global__ void __launch_bounds__(kRedBlock) batch_sum_kernel(const InstArgs<R>* args, const Work* work, const int* active) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    const SumArgs& a = args[w.inst].sum;
+    const Partial v = sum_cell(a, (long long)w.a + threadIdx.x);
+    block_reduce_write(v, a.partial + w.part);
+}
+
+__global__ void __launch_bounds__(kRedBlock) batch_axpy_kernel(const AxpyArgs* args, const Work* work, const int* active) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    const AxpyArgs& a = args[w.inst];
+    const long long k = (long long)w.a + threadIdx.x;
+    Partial v{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
+    if (k < a.n) {
+        const double dt = *a.dtp;
+        const double h = __dadd_rn(a.H0[k], __dmul_rn(dt, a.LH[k]));
+        const double c = __dadd_rn(a.C0[k], __dmul_rn(dt, a.LC[k]));
+        a.H1[k] = h; a.C1[k] = c;
+        v.HI = h * a.area; v.CI = c * a.area;
+        v.Hmin = h; v.Cmin = c; v.Cmax = c;
+        v.nonfinite = (isfinite(h) && isfinite(c)) ? 0.0 : 1.0;
+    }
+    block_reduce_write(v, a.partial + w.part);
+}
+
+// One block per instance: fixed-order reduction of its block partials (the
+// same thread/tree shape as the single-instance reduction, so totals agree
+// bit for bit).
+__global__ void __launch_bounds__(1024) batch_reduce_kernel(const Partial* partial, const int* part_off,
+                                                           const int* part_cnt, const int* active, Totals* out) {
+    const int inst = blockIdx.x;
+    if (!active[inst]) return;
+    const int off = part_off[inst], cnt = part_cnt[inst];
+    Partial v{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
+    for (int b = threadIdx.x; b < cnt; b += blockDim.x) {
+        const Partial p = partial[off + b];
+        v.maxRate = fmax(v.maxRate, p.maxRate); v.divergence = fmax(v.divergence, p.divergence);
+        v.bH += p.bH; v.bC += p.bC; v.HI += p.HI; v.CI += p.CI;
+        v.Hmin = fmin(v.Hmin, p.Hmin); v.Cmin = fmin(v.Cmin, p.Cmin); v.Cmax = fmax(v.Cmax, p.Cmax);
+        v.nonfinite = fmax(v.nonfinite, p.nonfinite);
+    }
+    __shared__ Partial result;
+    block_reduce_write(v, &result);
+    __syncthreads();
+    if (threadIdx.x == 0)
+        out[inst] = Totals{result.maxRate, result.divergence, result.bH, result.bC, result.HI, result.CI,
+                           result.Hmin, result.Cmin, result.Cmax, result.nonfinite};
+}
+
+}  // namespace
+}  // namespace mp
+
+// ----------------------------------------------------------------- instance
+
+struct MPInstance {
+    bool used = false;
+    mp_mesh_desc mesh{};
+    int nx = 0, ny = 0;
+    size_t N = 0, NE = 0, bytes = 0;
+    void* arena = nullptr;            // one allocation per instance
+    double *H, *C, *S1H, *S1C, *S2H, *S2C, *LH, *LC, *T, *phi, *rec, *rate, *vsn, *udn, *face;
+    unsigned char* flags;
+    mp::StageTables* tab;
+    mp::StageTablesF* tabF;
+    mp::StageTables host_tab;
+    double time = 0.0;
+    int accepted = 0;
+    bool have_L = false;
+    mp::Totals cur{};
+    int status = 0;                   // sticky failure status
+};
+
+struct mp_batch {
+    mp_transport_opts opts;
+    mp_derived der;
+    mp::Physics ph;
+    cudaStream_t stream = nullptr;
+    bool mixed = false;
+    std::vector<MPInstance> inst;
+    // device tables rebuilt when the set changes
+    bool dirty = true;
+    int slots = 0;                     // capacity of the per-instance device arrays
+    void* d_args[mp::NKIND] = {nullptr, nullptr, nullptr};
+    mp::AxpyArgs* d_axpy = nullptr;
+    mp::Work *d_wrecon = nullptr, *d_wphase = nullptr, *d_wface = nullptr, *d_wsum = nullptr;
+    int n_wrecon = 0, n_wphase = 0, n_wface = 0, n_wsum = 0;
+    int *d_active = nullptr, *d_part_off = nullptr, *d_part_cnt = nullptr;
+    mp::Partial* d_partial = nullptr;
+    int partial_cap = 0;
+    mp::Totals* d_tot = nullptr;
+    mp::Totals* h_tot = nullptr;
+    unsigned long long* d_status = nullptr;
+    unsigned long long* h_status = nullptr;
+    double* d_dt = nullptr;
+    double* h_dt = nullptr;
+    int* h_active = nullptr;
+    mp::Tuning tune;
+    size_t bytes_in_use = 0;
+    // profiling
+    bool profile = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<int> ev_kind;
+    size_t ev_used = 0;
+    double kern_ms[6] = {0, 0, 0, 0, 0, 0};
+    unsigned long long kern_n[6] = {0, 0, 0, 0, 0, 0};
+};
+
+namespace mp {
+namespace {
+
+size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+size_t instance_bytes(int nx, int ny) {
+    const size_t N = (size_t)nx * ny, NE = (size_t)nx * (ny + 1) + (size_t)(nx + 1) * ny;
+    size_t b = 0;
+    b += 11 * align256(N * sizeof(double));      // H C S1H S1C S2H S2C LH LC T phi rate
+    b += align256(18 * N * sizeof(double));      // rec
+    b += align256(N);                            // flags
+    b += 2 * align256(NE * kNQ * sizeof(double));// vsn udn
+    b += align256(4 * NE * sizeof(double));      // face
+    b += align256(sizeof(StageTables)) + align256(sizeof(StageTablesF));
+    return b;
+}
+
+cudaEvent_t prof_event(mp_batch* b) {
+    if (b->ev_used == b->ev_pool.size()) { cudaEvent_t e; cudaEventCreate(&e); b->ev_pool.push_back(e); }
+    return b->ev_pool[b->ev_used++];
+}
+template <class F>
+void timed(mp_batch* b, int kind, F&& f) {
+    if (!b->profile) { f(); return; }
+    cudaEventRecord(prof_event(b), b->stream);
+    f();
+    cudaEventRecord(prof_event(b), b->stream);
+    b->ev_kind.push_back(kind);
+}
+void harvest(mp_batch* b) {
+    for (size_t k = 0; k < b->ev_kind.size(); ++k) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, b->ev_pool[2 * k], b->ev_pool[2 * k + 1]) == cudaSuccess) {
+            b->kern_ms[b->ev_kind[k]] += ms;
+            b->kern_n[b->ev_kind[k]] += 1;
+        }
+    }
+    b->ev_kind.clear();
+    b->ev_used = 0;
+}
+
+mp_status alloc_instance(mp_batch* b, MPInstance& in, const mp_mesh_desc& m) {
+    in.mesh = m; in.nx = m.nx; in.ny = m.ny;
+    in.N = (size_t)m.nx * m.ny;
+    in.NE = (size_t)m.nx * (m.ny + 1) + (size_t)(m.nx + 1) * m.ny;
+    const int tb = build_stage_tables(m.nx, m.ny, m.x0, m.x1, m.y0, m.y1, in.host_tab);
+    if (tb) { set_error("stencil table construction failed"); return (mp_status)tb; }
+    in.bytes = instance_bytes(m.nx, m.ny);
+    MP_CUDA(cudaMallocAsync(&in.arena, in.bytes, b->stream));
+    unsigned char* p = static_cast<unsigned char*>(in.arena);
+    auto take = [&](size_t bytes) { void* r = p; p += align256(bytes); return r; };
+    const size_t N = in.N, NE = in.NE;
+    double** dbl[] = {&in.H, &in.C, &in.S1H, &in.S1C, &in.S2H, &in.S2C, &in.LH, &in.LC, &in.T, &in.phi, &in.rate};
+    for (double** q : dbl) *q = static_cast<double*>(take(N * sizeof(double)));
+    in.rec = static_cast<double*>(take(18 * N * sizeof(double)));
+    in.flags = static_cast<unsigned char*>(take(N));
+    in.vsn = static_cast<double*>(take(NE * kNQ * sizeof(double)));
+    in.udn = static_cast<double*>(take(NE * kNQ * sizeof(double)));
+    in.face = static_cast<double*>(take(4 * NE * sizeof(double)));
+    in.tab = static_cast<StageTables*>(take(sizeof(StageTables)));
+    in.tabF = static_cast<StageTablesF*>(take(sizeof(StageTablesF)));
+    StageTablesF tf;
+    tables_to_float_b(in.host_tab, tf);
+    MP_CUDA(cudaMemcpyAsync(in.tab, &in.host_tab, sizeof(StageTables), cudaMemcpyHostToDevice, b->stream));
+    MP_CUDA(cudaMemcpyAsync(in.tabF, &tf, sizeof(StageTablesF), cudaMemcpyHostToDevice, b->stream));
+    MP_CUDA(cudaMemsetAsync(in.vsn, 0, NE * kNQ * sizeof(double), b->stream));
+    MP_CUDA(cudaMemsetAsync(in.udn, 0, NE * kNQ * sizeof(double), b->stream));
+    MP_CUDA(cudaStreamSynchronize(b->stream));   // tf lives on this stack frame
+    in.used = true;
+    in.time = 0.0; in.accepted = 0; in.have_L = false; in.status = 0;
+    b->bytes_in_use += in.bytes;
+    b->dirty = true;
+    return MP_OK;
+}
+
+void free_instance(mp_batch* b, MPInstance& in) {
+    if (in.arena) cudaFreeAsync(in.arena, b->stream);
+    b->bytes_in_use -= in.bytes;
+    in = MPInstance{};
+    b->dirty = true;
+}
+
+template <class T>
+mp_status ensure(T** p, size_t count, size_t& cap_bytes_tracker, cudaStream_t s) {
+    (void)cap_bytes_tracker;
+    if (*p) cudaFreeAsync(*p, s);
+    *p = nullptr;
+    if (count == 0) count = 1;
+    MP_CUDA(cudaMallocAsync((void**)p, count * sizeof(T), s));
+    return MP_OK;
+}
+
+// Rebuild per-instance argument records, work maps and partial offsets.
+template <class R>
+mp_status rebuild_args(mp_batch* b, int slots) {
+    std::vector<InstArgs<R>> args[NKIND];
+    for (int k = 0; k < NKIND; ++k) args[k].resize(slots);
+    std::vector<AxpyArgs> ax(slots);
+    std::vector<int> part_off(slots, 0), part_cnt(slots, 0);
+    std::vector<Work> wr, wp, wf, ws;
+    int parts = 0;
+    const Tuning tu = b->tune;
+    for (int i = 0; i < slots; ++i) {
+        MPInstance& in = b->inst[i];
+        if (!in.used) continue;
+        Tab<R> tb;
+        tb.t = in.tab;
+        if constexpr (sizeof(R) == 4) tb.f = in.tabF;
+        const int nsum = (int)((in.N + kRedBlock - 1) / kRedBlock);
+        part_off[i] = parts; part_cnt[i] = nsum;
+        Partial* pp = nullptr;  // fixed below once the partial array exists
+        (void)pp;
+        for (int k = 0; k < NKIND; ++k) {
+            const double* inH = k == KIND_P ? in.H : (k == KIND_B ? in.S1H : in.S2H);
+            const double* inC = k == KIND_P ? in.C : (k == KIND_B ? in.S1C : in.S2C);
+            double* outH = k == KIND_P ? in.LH : (k == KIND_B ? in.S2H : in.S1H);
+            double* outC = k == KIND_P ? in.LC : (k == KIND_B ? in.S2C : in.S1C);
+            InstArgs<R>& a = args[k][i];
+            a.recon = ReconArgs<R>{in.nx, in.ny, tb, inH, inC, in.rec, in.flags, b->d_status + i, nullptr};
+            a.phase = CellPhaseArgs<R>{in.nx, in.ny, tb, inH, inC, in.rec, in.flags, in.T, in.phi, b->d_status + i};
+            a.face = FaceArgs<R>{in.nx, in.ny, tb, inH, inC, in.rec, in.flags, in.vsn, in.udn, in.face, b->d_status + i};
+            const bool rk3 = b->opts.integrator == MP_SSPRK3;
+            const double a0 = k == KIND_B ? (rk3 ? 0.75 : 0.5) : (1.0 / 3.0);
+            const double a1 = k == KIND_B ? (rk3 ? 0.25 : 0.5) : (2.0 / 3.0);
+            a.sum = SumArgs{in.nx, in.ny, in.tab, in.face, inH, inC, in.H, in.C, outH, outC, in.rate,
+                            k == KIND_P ? (int)SUM_STORE_L : (int)SUM_RK, a0, a1, 0.0, b->d_partial + parts,
+                            b->d_dt + i};
+        }
+        ax[i] = AxpyArgs{(int)in.N, in.H, in.C, in.LH, in.LC, in.S1H, in.S1C, b->d_dt + i, in.host_tab.area,
+                         b->d_partial + parts};
+        for (int ty = 0; ty < in.ny; ty += tu.by)
+            for (int tx = 0; tx < in.nx; tx += tu.bx * tu.cpt) wr.push_back(Work{i, tx, ty, 0});
+        for (size_t c = 0; c < in.N; c += 128) wp.push_back(Work{i, (int)c, 0, 0});
+        for (size_t e = 0; e < in.NE; e += 128) wf.push_back(Work{i, (int)e, 0, 0});
+        for (int s = 0; s < nsum; ++s) ws.push_back(Work{i, s * kRedBlock, 0, s});
+        parts += nsum;
+    }
+    (void)parts;
+    cudaStream_t s = b->stream;
+    for (int k = 0; k < NKIND; ++k) {
+        if (b->d_args[k]) cudaFreeAsync(b->d_args[k], s);
+        MP_CUDA(cudaMallocAsync(&b->d_args[k], std::max<size_t>(1, slots) * sizeof(InstArgs<R>), s));
+        MP_CUDA(cudaMemcpyAsync(b->d_args[k], args[k].data(), slots * sizeof(InstArgs<R>), cudaMemcpyHostToDevice, s));
+    }
+    size_t dummy = 0;
+    MP_TRY(ensure(&b->d_axpy, slots, dummy, s));
+    MP_CUDA(cudaMemcpyAsync(b->d_axpy, ax.data(), slots * sizeof(AxpyArgs), cudaMemcpyHostToDevice, s));
+    MP_TRY(ensure(&b->d_wrecon, wr.size(), dummy, s));
+    MP_TRY(ensure(&b->d_wphase, wp.size(), dummy, s));
+    MP_TRY(ensure(&b->d_wface, wf.size(), dummy, s));
+    MP_TRY(ensure(&b->d_wsum, ws.size(), dummy, s));
+    if (!wr.empty()) MP_CUDA(cudaMemcpyAsync(b->d_wrecon, wr.data(), wr.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+    if (!wp.empty()) MP_CUDA(cudaMemcpyAsync(b->d_wphase, wp.data(), wp.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+    if (!wf.empty()) MP_CUDA(cudaMemcpyAsync(b->d_wface, wf.data(), wf.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+    if (!ws.empty()) MP_CUDA(cudaMemcpyAsync(b->d_wsum, ws.data(), ws.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+    b->n_wrecon = (int)wr.size(); b->n_wphase = (int)wp.size(); b->n_wface = (int)wf.size(); b->n_wsum = (int)ws.size();
+    MP_CUDA(cudaMemcpyAsync(b->d_part_off, part_off.data(), slots * sizeof(int), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaMemcpyAsync(b->d_part_cnt, part_cnt.data(), slots * sizeof(int), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaStreamSynchronize(s));   // host vectors go out of scope
+    return MP_OK;
+}
+
+mp_status rebuild(mp_batch* b) {
+    if (!b->dirty) return MP_OK;
+    cudaStream_t s = b->stream;
+    const int slots = (int)b->inst.size();
+    // per-slot arrays
+    if (slots > b->slots) {
+        for (void* p : {(void*)b->d_active, (void*)b->d_part_off, (void*)b->d_part_cnt, (void*)b->d_tot,
+                        (void*)b->d_status, (void*)b->d_dt})
+            if (p) cudaFreeAsync(p, s);
+        if (b->h_tot) cudaFreeHost(b->h_tot);
+        if (b->h_status) cudaFreeHost(b->h_status);
+        if (b->h_dt) cudaFreeHost(b->h_dt);
+        if (b->h_active) cudaFreeHost(b->h_active);
+        const int cap = std::max(slots, 8);
+        MP_CUDA(cudaMallocAsync((void**)&b->d_active, cap * sizeof(int), s));
+        MP_CUDA(cudaMallocAsync((void**)&b->d_part_off, cap * sizeof(int), s));
+        MP_CUDA(cudaMallocAsync((void**)&b->d_part_cnt, cap * sizeof(int), s));
+        MP_CUDA(cudaMallocAsync((void**)&b->d_tot, cap * sizeof(Totals), s));
+        MP_CUDA(cudaMallocAsync((void**)&b->d_status, cap * sizeof(unsigned long long), s));
+        MP_CUDA(cudaMallocAsync((void**)&b->d_dt, cap * sizeof(double), s));
+        MP_CUDA(cudaMallocHost((void**)&b->h_tot, cap * sizeof(Totals)));
+        MP_CUDA(cudaMallocHost((void**)&b->h_status, cap * sizeof(unsigned long long)));
+        MP_CUDA(cudaMallocHost((void**)&b->h_dt, cap * sizeof(double)));
+        MP_CUDA(cudaMallocHost((void**)&b->h_active, cap * sizeof(int)));
+        b->slots = cap;
+    }
+    int parts = 0;
+    for (const MPInstance& in : b->inst) if (in.used) parts += (int)((in.N + kRedBlock - 1) / kRedBlock);
+    if (parts > b->partial_cap) {
+        if (b->d_partial) cudaFreeAsync(b->d_partial, s);
+        MP_CUDA(cudaMallocAsync((void**)&b->d_partial, std::max(parts, 1) * sizeof(Partial), s));
+        b->partial_cap = parts;
+    }
+    if (b->mixed) MP_TRY(rebuild_args<float>(b, slots));
+    else MP_TRY(rebuild_args<double>(b, slots));
+    b->dirty = false;
+    return MP_OK;
+}
+
+mp_status set_active(mp_batch* b, const std::vector<int>& act) {
+    const int slots = (int)b->inst.size();
+    for (int i = 0; i < slots; ++i) b->h_active[i] = act[i];
+    MP_CUDA(cudaMemcpyAsync(b->d_active, b->h_active, slots * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    return MP_OK;
+}
+
+template <class R>
+void launch_kind(mp_batch* b, int kind) {
+    cudaStream_t s = b->stream;
+    const InstArgs<R>* args = static_cast<const InstArgs<R>*>(b->d_args[kind]);
+    const Tuning tu = b->tune;
+    if (b->n_wrecon) timed(b, 0, [&] { batch_recon_kernel<R><<<b->n_wrecon, dim3(tu.bx, tu.by), 0, s>>>(args, b->d_wrecon, b->d_active, b->ph, tu.cpt); });
+    if (b->n_wphase) timed(b, 1, [&] { batch_phase_kernel<R><<<b->n_wphase, 128, 0, s>>>(args, b->d_wphase, b->d_active, b->ph); });
+    if (b->n_wface) timed(b, 2, [&] { batch_face_kernel<R><<<b->n_wface, 128, 0, s>>>(args, b->d_wface, b->d_active, b->ph); });
+    if (b->n_wsum) timed(b, 3, [&] { batch_sum_kernel<R><<<b->n_wsum, kRedBlock, 0, s>>>(args, b->d_wsum, b->d_active); });
+    timed(b, 4, [&] { batch_reduce_kernel<<<(int)b->inst.size(), 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot); });
+    count_launch(5);
+}
+
+// Stage of one kind on the active instances; totals and status to the host.
+mp_status run_stage(mp_batch* b, int kind, const std::vector<int>& act) {
+    MP_TRY(set_active(b, act));
+    const int slots = (int)b->inst.size();
+    MP_CUDA(cudaMemsetAsync(b->d_status, 0xff, slots * sizeof(unsigned long long), b->stream));
+    if (b->mixed) launch_kind<float>(b, kind);
+    else launch_kind<double>(b, kind);
+    MP_CUDA(cudaGetLastError());
+    MP_CUDA(cudaMemcpyAsync(b->h_tot, b->d_tot, slots * sizeof(Totals), cudaMemcpyDeviceToHost, b->stream));
+    MP_CUDA(cudaMemcpyAsync(b->h_status, b->d_status, slots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->stream));
+    MP_CUDA(cudaStreamSynchronize(b->stream));
+    harvest(b);
+    return MP_OK;
+}
+
+mp_status run_axpy(mp_batch* b, const std::vector<int>& act) {
+    MP_TRY(set_active(b, act));
+    const int slots = (int)b->inst.size();
+    cudaStream_t s = b->stream;
+    MP_CUDA(cudaMemcpyAsync(b->d_dt, b->h_dt, slots * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (b->n_wsum) timed(b, 4, [&] { batch_axpy_kernel<<<b->n_wsum, kRedBlock, 0, s>>>(b->d_axpy, b->d_wsum, b->d_active); });
+    timed(b, 4, [&] { batch_reduce_kernel<<<slots, 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot); });
+    count_launch(2);
+    MP_CUDA(cudaGetLastError());
+    MP_CUDA(cudaMemcpyAsync(b->h_tot, b->d_tot, slots * sizeof(Totals), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    harvest(b);
+    return MP_OK;
+}
+
+int status_code(unsigned long long v) { return v == ~0ULL ? 0 : (int)(v & 0xff); }
+
+bool admissible_tot(const Totals& t, double Xe) {
+    return t.nonfinite == 0.0 && t.Hmin >= 0.0 && t.Cmin >= 0.0 && t.Cmax <= Xe;
+}
+
+// L(U^n) for instances that lack it.
+mp_status eval_missing(mp_batch* b) {
+    const int slots = (int)b->inst.size();
+    std::vector<int> act(slots, 0);
+    bool any = false;
+    for (int i = 0; i < slots; ++i) {
+        const MPInstance& in = b->inst[i];
+        if (in.used && !in.status && !in.have_L) { act[i] = 1; any = true; }
+    }
+    if (!any) return MP_OK;
+    MP_TRY(run_stage(b, KIND_P, act));
+    for (int i = 0; i < slots; ++i) {
+        if (!act[i]) continue;
+        MPInstance& in = b->inst[i];
+        const int st = status_code(b->h_status[i]);
+        if (st) { in.status = st; continue; }
+        if (!std::isfinite(b->h_tot[i].maxRate)) { in.status = MP_ERR_FP; continue; }
+        in.cur = b->h_tot[i];
+        in.have_L = true;
+    }
+    return MP_OK;
+}
+
+// One accepted step of every healthy instance (the reference's loop per instance).
+mp_status step_all(mp_batch* b, std::vector<mp_step_report>& reps) {
+    MP_TRY(rebuild(b));
+    MP_TRY(eval_missing(b));
+    const int slots = (int)b->inst.size();
+    const mp_transport_opts& o = b->opts;
+    const double Xe = o.material.Xe;
+    const bool rk3 = o.integrator == MP_SSPRK3;
+    reps.assign(slots, mp_step_report{});
+    std::vector<double> dt(slots, 0.0), start(slots, 0.0), courant(slots, 0.0);
+    std::vector<int> retries(slots, 0), pending(slots, 0), done(slots, 0);
+    std::vector<Totals> first(slots), second(slots), third(slots);
+    for (int i = 0; i < slots; ++i) {
+        MPInstance& in = b->inst[i];
+        if (!in.used || in.status) continue;
+        first[i] = in.cur;
+        const double cap = in.accepted == 0 ? o.dt_initial : o.dt_max;
+        const double limit = in.cur.maxRate > 0 ? o.cfl / in.cur.maxRate : o.dt_max;
+        dt[i] = std::min(cap, limit);
+        start[i] = in.time;
+        pending[i] = 1;
+    }
+    for (;;) {
+        bool any = false;
+        for (int i = 0; i < slots; ++i) {
+            if (!pending[i]) continue;
+            if (!(dt[i] >= o.dt_min && retries[i] < 40)) { b->inst[i].status = MP_ERR_NOT_CONVERGED; pending[i] = 0; continue; }
+            b->h_dt[i] = dt[i];
+            any = true;
+        }
+        if (!any) break;
+        MP_TRY(run_axpy(b, pending));
+        std::vector<int> valid(slots, 0);
+        for (int i = 0; i < slots; ++i) if (pending[i]) valid[i] = admissible_tot(b->h_tot[i], Xe);
+        MP_TRY(run_stage(b, KIND_B, valid));
+        for (int i = 0; i < slots; ++i) {
+            if (!valid[i]) continue;
+            const int st = status_code(b->h_status[i]);
+            if (st || !std::isfinite(b->h_tot[i].maxRate)) { b->inst[i].status = st ? st : MP_ERR_FP; valid[i] = 0; pending[i] = 0; continue; }
+            second[i] = b->h_tot[i];
+            courant[i] = dt[i] * std::max(first[i].maxRate, second[i].maxRate);
+            valid[i] = courant[i] <= o.cfl * (1 + 1e-12) && admissible_tot(second[i], Xe);
+        }
+        if (rk3) {
+            MP_TRY(run_stage(b, KIND_C, valid));
+            for (int i = 0; i < slots; ++i) {
+                if (!valid[i]) continue;
+                const int st = status_code(b->h_status[i]);
+                if (st || !std::isfinite(b->h_tot[i].maxRate)) { b->inst[i].status = st ? st : MP_ERR_FP; valid[i] = 0; pending[i] = 0; continue; }
+                third[i] = b->h_tot[i];
+                courant[i] = dt[i] * std::max(std::max(first[i].maxRate, second[i].maxRate), third[i].maxRate);
+                valid[i] = courant[i] <= o.cfl * (1 + 1e-12) && admissible_tot(third[i], Xe);
+            }
+        }
+        for (int i = 0; i < slots; ++i) {
+            if (!pending[i]) continue;
+            if (valid[i]) { done[i] = 1; pending[i] = 0; }
+            else { dt[i] *= 0.5; ++retries[i]; }
+        }
+    }
+    // Balance check and commit (evolve.cpp:486-499).
+    cudaStream_t s = b->stream;
+    for (int i = 0; i < slots; ++i) {
+        if (!done[i]) continue;
+        MPInstance& in = b->inst[i];
+        const Totals fin = rk3 ? third[i] : second[i];
+        double repH, repC, bH, bC;
+        if (rk3) {
+            repH = (first[i].bH + second[i].bH) / 6 + third[i].bH * (2.0 / 3.0);
+            repC = (first[i].bC + second[i].bC) / 6 + third[i].bC * (2.0 / 3.0);
+            bH = fin.HI - first[i].HI + dt[i] * repH;
+            bC = fin.CI - first[i].CI + dt[i] * repC;
+        } else {
+            repH = .5 * (first[i].bH + second[i].bH);
+            repC = .5 * (first[i].bC + second[i].bC);
+            bH = fin.HI - first[i].HI + .5 * dt[i] * (first[i].bH + second[i].bH);
+            bC = fin.CI - first[i].CI + .5 * dt[i] * (first[i].bC + second[i].bC);
+        }
+        if (!(std::fabs(bH) < 1e-10 * std::max(1.0, std::fabs(first[i].HI)) && std::fabs(bC) < 1e-10)) {
+            in.status = MP_ERR_PLIB;
+            done[i] = 0;
+            continue;
+        }
+        double* nH = rk3 ? in.S1H : in.S2H;
+        double* nC = rk3 ? in.S1C : in.S2C;
+        MP_CUDA(cudaMemcpyAsync(in.H, nH, in.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        MP_CUDA(cudaMemcpyAsync(in.C, nC, in.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        in.time = start[i] + dt[i];
+        in.have_L = false;
+        mp_step_report& r = reps[i];
+        r.retries = retries[i]; r.dt = dt[i]; r.time = in.time; r.courant = courant[i];
+        r.boundaryH = repH; r.boundaryC = repC; r.balanceH = bH; r.balanceC = bC;
+        r.H_integral = fin.HI; r.C_integral = fin.CI;
+    }
+    MP_TRY(eval_missing(b));
+    for (int i = 0; i < slots; ++i) {
+        MPInstance& in = b->inst[i];
+        if (!in.used) continue;
+        if (done[i] && !in.status) {
+            ++in.accepted;
+            reps[i].maxRate = in.cur.maxRate;
+            reps[i].divergence = in.cur.divergence;
+        }
+        reps[i].status = in.status;
+    }
+    return MP_OK;
+}
+
+// Autotuner: time one P-stage over the whole batch for each candidate tile
+// shape / cells-per-thread of the reconstruction kernel; keep the fastest.
+mp_status autotune(mp_batch* b, int reps, double* best_ms) {
+    const Tuning cands[] = {{32, 4, 1}, {32, 2, 1}, {64, 2, 1}, {16, 8, 1}, {128, 1, 1}, {32, 4, 2}, {32, 2, 2}, {64, 1, 2}};
+    const int slots = (int)b->inst.size();
+    std::vector<int> act(slots, 0);
+    for (int i = 0; i < slots; ++i) act[i] = b->inst[i].used && !b->inst[i].status;
+    double best = 1e300;
+    Tuning pick = b->tune;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    for (const Tuning& c : cands) {
+        b->tune = c;
+        b->dirty = true;
+        MP_TRY(rebuild(b));
+        MP_TRY(set_active(b, act));
+        if (b->mixed) launch_kind<float>(b, KIND_P); else launch_kind<double>(b, KIND_P);   // warm-up
+        cudaEventRecord(e0, b->stream);
+        for (int r = 0; r < reps; ++r) { if (b->mixed) launch_kind<float>(b, KIND_P); else launch_kind<double>(b, KIND_P); }
+        cudaEventRecord(e1, b->stream);
+        MP_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) { best = ms; pick = c; }
+    }
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    b->tune = pick;
+    b->dirty = true;
+    MP_TRY(rebuild(b));
+    // the timing runs overwrote L and T/phi of every instance: recompute L(U^n)
+    for (MPInstance& in : b->inst) in.have_L = false;
+    if (best_ms) *best_ms = best / reps;
+    return MP_OK;
+}
+
+}  // namespace
+}  // namespace mp
+
+// -------------------------------------------------------------------- C ABI
+
+extern "C" mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, const mp_transport_opts* opts,
+                                     mp_stream_t stream, mp_batch** out) {
+    using namespace mp;
+    if (!opts || !out || count < 0 || (count > 0 && !meshes)) { set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (!(opts->cfl > 0 && opts->cfl <= 1)) { set_error("Coupled CFL must be in (0,1]"); return MP_ERR_ARG_OUTOFRANGE; }
+    if (opts->integrator != MP_SSPRK2 && opts->integrator != MP_SSPRK3) { set_error("integrator must be 2 or 3"); return MP_ERR_ARG_OUTOFRANGE; }
+    if (opts->diffusivity != 0.0) { set_error("thermal diffusion (kappa > 0) is not supported by this build"); return MP_ERR_ARG_WRONG; }
+    if (opts->material.alpha0 != 0.0) { set_error("adiabatic source (alpha0 != 0) is not supported by this build"); return MP_ERR_ARG_WRONG; }
+    if (opts->precision != MP_PRECISION_FP64 && opts->precision != MP_PRECISION_MIXED) { set_error("unknown precision"); return MP_ERR_ARG_OUTOFRANGE; }
+    mp_derived der;
+    MP_TRY(derive_checked(opts->material, der));
+    mp_batch* b = new mp_batch;
+    b->opts = *opts; b->der = der;
+    b->stream = (cudaStream_t)stream;
+    b->mixed = opts->precision == MP_PRECISION_MIXED;
+    b->ph.k = phase_const(opts->material, der);
+    b->ph.sk = stage_const(b->ph.k);
+    if (eutectic_temperature(b->ph.k, opts->pressure, b->ph.Tep)) { delete b; set_error("pressure must be finite"); return MP_ERR_ARG_OUTOFRANGE; }
+    b->ph.theta = opts->theta; b->ph.inflowH = opts->inflow_H; b->ph.inflowC = opts->inflow_C;
+    b->ph.Hpol = opts->H_policy; b->ph.Cpol = opts->C_policy; b->ph.lf_global = opts->lf_global;
+    b->ph.lf_speed = opts->lf_global_speed;
+    b->inst.resize(count);
+    for (int i = 0; i < count; ++i) {
+        if (meshes[i].nx < 2 || meshes[i].ny < 2) { set_error("instance %d: at least 2x2 cells", i); mp_batch_destroy(b); return MP_ERR_ARG_SIZ; }
+        const mp_status s = alloc_instance(b, b->inst[i], meshes[i]);
+        if (s != MP_OK) { mp_batch_destroy(b); return s; }
+    }
+    *out = b;
+    return MP_OK;
+}
+
+extern "C" void mp_batch_destroy(mp_batch* b) {
+    if (!b) return;
+    cudaStreamSynchronize(b->stream);
+    for (MPInstance& in : b->inst) if (in.used && in.arena) cudaFreeAsync(in.arena, b->stream);
+    for (int k = 0; k < mp::NKIND; ++k) if (b->d_args[k]) cudaFreeAsync(b->d_args[k], b->stream);
+    for (void* p : {(void*)b->d_axpy, (void*)b->d_wrecon, (void*)b->d_wphase, (void*)b->d_wface, (void*)b->d_wsum,
+                    (void*)b->d_active, (void*)b->d_part_off, (void*)b->d_part_cnt, (void*)b->d_partial,
+                    (void*)b->d_tot, (void*)b->d_status, (void*)b->d_dt})
+        if (p) cudaFreeAsync(p, b->stream);
+    cudaStreamSynchronize(b->stream);
+    if (b->h_tot) cudaFreeHost(b->h_tot);
+    if (b->h_status) cudaFreeHost(b->h_status);
+    if (b->h_dt) cudaFreeHost(b->h_dt);
+    if (b->h_active) cudaFreeHost(b->h_active);
+    for (cudaEvent_t e : b->ev_pool) cudaEventDestroy(e);
+    delete b;
+}
+
+static mp_status batch_slot(mp_batch* b, int i, MPInstance** out) {
+    if (!b) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (i < 0 || i >= (int)b->inst.size() || !b->inst[i].used) { mp::set_error("no instance %d", i); return MP_ERR_ARG_OUTOFRANGE; }
+    *out = &b->inst[i];
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_add(mp_batch* b, const mp_mesh_desc* mesh, int* instance) {
+    if (!b || !mesh || !instance) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (mesh->nx < 2 || mesh->ny < 2) { mp::set_error("Transport requires at least 2x2 cells"); return MP_ERR_ARG_SIZ; }
+    int slot = -1;
+    for (int i = 0; i < (int)b->inst.size(); ++i) if (!b->inst[i].used) { slot = i; break; }
+    if (slot < 0) { slot = (int)b->inst.size(); b->inst.emplace_back(); }
+    MP_TRY(mp::alloc_instance(b, b->inst[slot], *mesh));
+    *instance = slot;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_remove(mp_batch* b, int i) {
+    MPInstance* in;
+    MP_TRY(batch_slot(b, i, &in));
+    mp::free_instance(b, *in);
+    return MP_OK;
+}
+
+extern "C" size_t mp_batch_instance_bytes(const mp_mesh_desc* mesh) {
+    return mesh ? mp::instance_bytes(mesh->nx, mesh->ny) : 0;
+}
+
+extern "C" mp_status mp_batch_set_face_velocity(mp_batch* b, int i, const double* vs_n, const double* ud_n) {
+    MPInstance* in;
+    MP_TRY(batch_slot(b, i, &in));
+    if (!vs_n || !ud_n) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    MP_CUDA(cudaMemcpyAsync(in->vsn, vs_n, in->NE * mp::kNQ * sizeof(double), cudaMemcpyDefault, b->stream));
+    MP_CUDA(cudaMemcpyAsync(in->udn, ud_n, in->NE * mp::kNQ * sizeof(double), cudaMemcpyDefault, b->stream));
+    MP_CUDA(cudaStreamSynchronize(b->stream));
+    in->have_L = false;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_set_state(mp_batch* b, int i, const double* H, const double* C, double time) {
+    MPInstance* in;
+    MP_TRY(batch_slot(b, i, &in));
+    if (!H || !C) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    MP_CUDA(cudaMemcpyAsync(in->H, H, in->N * sizeof(double), cudaMemcpyDefault, b->stream));
+    MP_CUDA(cudaMemcpyAsync(in->C, C, in->N * sizeof(double), cudaMemcpyDefault, b->stream));
+    MP_CUDA(cudaStreamSynchronize(b->stream));
+    in->time = time; in->accepted = 0; in->have_L = false; in->status = 0;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_get_state(mp_batch* b, int i, double* H, double* C, double* T, double* phi,
+                                        double* time, int* accepted, int* status) {
+    MPInstance* in;
+    MP_TRY(batch_slot(b, i, &in));
+    const size_t by = in->N * sizeof(double);
+    if (H) MP_CUDA(cudaMemcpyAsync(H, in->H, by, cudaMemcpyDefault, b->stream));
+    if (C) MP_CUDA(cudaMemcpyAsync(C, in->C, by, cudaMemcpyDefault, b->stream));
+    if (T) MP_CUDA(cudaMemcpyAsync(T, in->T, by, cudaMemcpyDefault, b->stream));
+    if (phi) MP_CUDA(cudaMemcpyAsync(phi, in->phi, by, cudaMemcpyDefault, b->stream));
+    MP_CUDA(cudaStreamSynchronize(b->stream));
+    if (time) *time = in->time;
+    if (accepted) *accepted = in->accepted;
+    if (status) *status = in->status;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_step(mp_batch* b, int nsteps, mp_step_report* reports) {
+    if (!b) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    std::vector<mp_step_report> reps;
+    const int slots = (int)b->inst.size();
+    for (int k = 0; k < nsteps; ++k) {
+        MP_TRY(mp::step_all(b, reps));
+        if (reports)
+            for (int i = 0; i < slots; ++i) reports[(size_t)k * slots + i] = reps[i];
+    }
+    return MP_OK;
+}
+
+extern "C" int mp_batch_slots(const mp_batch* b) { return b ? (int)b->inst.size() : 0; }
+
+extern "C" size_t mp_batch_bytes_in_use(const mp_batch* b) { return b ? b->bytes_in_use : 0; }
+
+extern "C" mp_status mp_batch_autotune(mp_batch* b, int reps, int* tile, double* best_ms) {
+    if (!b) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    MP_TRY(mp::autotune(b, reps > 0 ? reps : 2, best_ms));
+    if (tile) { tile[0] = b->tune.bx; tile[1] = b->tune.by; tile[2] = b->tune.cpt; }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_profile(mp_batch* b, int enable) {
+    if (!b) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    MP_CUDA(cudaStreamSynchronize(b->stream));
+    mp::harvest(b);
+    b->profile = enable != 0;
+    for (int k = 0; k < 6; ++k) { b->kern_ms[k] = 0; b->kern_n[k] = 0; }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_kernel_times(mp_batch* b, double ms[6], unsigned long long launches[6]) {
+    if (!b || !ms || !launches) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    MP_CUDA(cudaStreamSynchronize(b->stream));
+    mp::harvest(b);
+    for (int k = 0; k < 6; ++k) { ms[k] = b->kern_ms[k]; launches[k] = b->kern_n[k]; }
+    return MP_OK;
+}

@@ -15,6 +15,7 @@
 #include "common.hpp"
 #include "phase_math.cuh"
 #include "stage_device.cuh"
+#include "stage_kernels.cuh"
 #include "tables.hpp"
 
 #include <algorithm>
@@ -29,542 +30,21 @@ mp_status derive_checked(const mp_material& p, mp_derived& d);
 
 namespace {
 
-constexpr int kRec = 18;          // limited deviation coefficients: 9 for H, 9 for C
-constexpr int kRedBlock = 256;
-
-enum : int {
-    E_OUTOFRANGE = MP_ERR_ARG_OUTOFRANGE, E_FP = MP_ERR_FP, E_WRONG = MP_ERR_ARG_WRONG
-};
-
-struct Physics {
-    PhaseConst k;
-    StageConst sk;
-    double Tep;            // pressure-corrected eutectic temperature (constant pressure)
-    double theta;          // Darcy exponent
-    double inflowH, inflowC;
-    int Hpol, Cpol, lf_global;
-    double lf_speed;
-};
-
-// Block partials of one stage (sum_kernel) or state check (axpy_kernel).
-struct Partial {
-    double maxRate, divergence, bH, bC, HI, CI, Hmin, Cmin, Cmax;
-    double nonfinite;
-};
-
-struct Totals {
-    double maxRate, divergence, bH, bC, HI, CI, Hmin, Cmin, Cmax;
-    double nonfinite;
-};
-
-// Status word: the smallest key wins. The key orders failures as the
-// reference's RHS meets them (evolve.cpp:279-384): reconstruction update,
-// limiter, porosity sampling, face loop, cell quadrature; then by cell/edge.
-enum : int { PART_UPDATE = 0, PART_LIMIT = 1, PART_POROSITY = 2, PART_FACES = 3, PART_CELLS = 4 };
-__device__ __forceinline__ void record_error(unsigned long long* status, int part, long long where, int code) {
-    atomicMin(status, ((unsigned long long)part << 56) | ((unsigned long long)where << 8) | (unsigned long long)(code & 0xff));
-}
-
-
-// ------------------------------------------------------- reconstruction kernel
-
-// Cell flags byte: bit 0 wet (porosity sampling), bit 1 exact diffusion-sample
-// check needed (the cheap bound could not prove admissibility).
-enum : unsigned char { FLAG_WET = 1, FLAG_CHECK = 2 };
-
-template <class R>
-struct ReconArgs {
-    int nx, ny;
-    Tab<R> tab;
-    const double* H;
-    const double* C;
-    double* rec;           // 18 * ncell, SoA: rec[m*N + cell], m < 9 for H
-    unsigned char* flags;
-    unsigned long long* status;
-    double* theta;         // optional (2 * ncell): limiter factors for H, C
-};
-
-// Max/min of the deviation polynomial over the class's limiter points,
-// evaluated in R from D (FP64). For R = float the points attaining the
-// extremes are re-evaluated in FP64, so theta is formed from FP64 values.
-template <class R>
-__device__ __forceinline__ void scan_lines(const StageTables& t, const Tab<R>& tb, int l0, int l1, const double* Dd,
-                                           double& mx, double& mn, bool& bad) {
-    R D[9];
-#pragma unroll
-    for (int m = 0; m < 9; ++m) D[m] = (R)Dd[m];
-    R rmx = D[0], rmn = D[0];        // cell centre
-    int amx = -1, amn = -1;          // extreme point as line*8 + q (-1 = centre)
-    for (int l = l0; l < l1; ++l) {
-        const R c = tb.line_c(l);
-        R a0, a1, a2;
-        const bool row = t.line_dir[l] == 0;
-        if (row) q2_row(D, c, a0, a1, a2);
-        else q2_col(D, c, a0, a1, a2);
-#pragma unroll
-        for (int q = 0; q < kNQ; ++q) {
-            const R v = quad(a0, a1, a2, row ? tb.gx(q) : tb.gy(q));
-            if constexpr (sizeof(R) == 8) {
-                rmx = fmax(rmx, v); rmn = fmin(rmn, v);
-            } else {
-                if (v > rmx) { rmx = v; amx = l * 8 + q; }
-                if (v < rmn) { rmn = v; amn = l * 8 + q; }
-            }
-            bad = bad || !isfinite(v);
-        }
-    }
-    if constexpr (sizeof(R) == 8) {
-        mx = (double)rmx; mn = (double)rmn;
-    } else {
-        auto at = [&](int code) {
-            if (code < 0) return Dd[0];
-            const int l = code >> 3, q = code & 7;
-            double a0, a1, a2;
-            if (t.line_dir[l] == 0) { q2_row(Dd, t.line_c[l], a0, a1, a2); return quad(a0, a1, a2, t.gx[q]); }
-            q2_col(Dd, t.line_c[l], a0, a1, a2);
-            return quad(a0, a1, a2, t.gy[q]);
-        };
-        mx = at(amx); mn = at(amn);
-    }
-}
-
-// theta of one field: min over points of (bound - mean)/(v - mean) for v
-// outside [lo, hi] (state_reconstruction.cpp:216-224). With v = mean + D and
-// rounding monotone, the minimum is reached at the extreme D, so one
-// division per bound gives the reference's value.
-__device__ __forceinline__ double theta_of(double m, double lo, double hi, double dmax, double dmin) {
-    double th = 1.0;
-    const double vmax = m + dmax, vmin = m + dmin;
-    if (vmax > hi) th = fmin(th, (hi - m) / (vmax - m));
-    if (vmin < lo) th = fmin(th, (lo - m) / (vmin - m));
-    return th < 1.0 ? fmax(0.0, th * (1.0 - 1e-13)) : 1.0;
-}
-
+// Single-instance kernels: one thread per cell / edge.
 template <class R>
 __global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= a.nx || j >= a.ny) return;
-    const StageTables& t = *a.tab.t;
-    const int nx = a.nx, ny = a.ny;
-    const long long cell = (long long)j * nx + i;
-    const size_t N = (size_t)nx * ny;
-    const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1);
-    const int cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
-    int st_lim = 0;
-
-    double u[3][3];
-    double DH[9], DC[9];
-    double mH, mC, loH, hiH, loC, hiC;
-    int st = 0;
-    // Enthalpy, then composition: one 3x3 gather at a time keeps registers low.
-#pragma unroll
-    for (int f = 0; f < 2; ++f) {
-        const double* F = f ? a.C : a.H;
-#pragma unroll
-        for (int dj = 0; dj < 3; ++dj)
-#pragma unroll
-            for (int di = 0; di < 3; ++di) {
-                const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
-                u[dj][di] = __ldg(F + (size_t)jj * nx + ii);
-            }
-        // 3x3 neighbour bounds (state_reconstruction.cpp:189-196); the clamped
-        // gather repeats in-domain values, which leaves min/max unchanged.
-        double lo = u[1][1], hi = u[1][1];
-#pragma unroll
-        for (int dj = 0; dj < 3; ++dj)
-#pragma unroll
-            for (int di = 0; di < 3; ++di) { lo = fmin(lo, u[dj][di]); hi = fmax(hi, u[dj][di]); }
-        if (f == 0) {
-            mH = u[1][1]; loH = fmax(0.0, lo); hiH = hi;
-            const int s1 = reconstruct<R>(a.tab, t, ci, cj, u, DH);
-            st = st ? st : s1;
-        } else {
-            mC = u[1][1]; loC = fmax(0.0, lo); hiC = fmin(ph.k.Xe, hi);
-            const int s1 = reconstruct<R>(a.tab, t, ci, cj, u, DC);
-            st = st ? st : s1;
-        }
-    }
-    // state_reconstruction.cpp:187-188: admissible means.
-    if (!(isfinite(mH) && mH >= 0.0 && isfinite(mC) && mC >= 0.0 && mC <= ph.k.Xe)) st_lim = E_OUTOFRANGE;
-
-    // Limiter over the class's points, evaluated line by line.
-    const int cls = cj * 3 + ci;
-    const int l0 = t.line_off[cls], l1 = t.line_off[cls + 1];
-    double hmx, hmn, cmx, cmn;
-    bool bad = false;
-    scan_lines<R>(t, a.tab, l0, l1, DH, hmx, hmn, bad);
-    scan_lines<R>(t, a.tab, l0, l1, DC, cmx, cmn, bad);
-    if (bad) st_lim = st_lim ? st_lim : E_FP;
-    const double thH = theta_of(mH, loH, hiH, hmx, hmn);
-    const double thC = theta_of(mC, loC, hiC, cmx, cmn);
-    if (a.theta) { a.theta[cell] = thH; a.theta[N + cell] = thC; }
-    // Diffusion samples (zero diffusivity: kept for their admissibility
-    // check). Limited values at limiter points stay in [lo, hi], so the
-    // samples are admissible when hi_H is below the liquidus at hi_C and
-    // Tep >= 0; otherwise the phase kernel checks each sample exactly.
-    const double Hliq = ph.Tep + (1.0 - hiC / ph.k.Xe) + ph.k.LD;
-    const bool safe = ph.Tep >= 0.0 && hiH + 1e-12 * (1.0 + fabs(hiH)) < Hliq;
-#pragma unroll
-    for (int m = 0; m < 9; ++m) {
-        a.rec[(size_t)m * N + cell] = DH[m] * thH;
-        a.rec[(size_t)(m + 9) * N + cell] = DC[m] * thC;
-    }
-    a.flags[cell] = safe ? 0 : FLAG_CHECK;
-    if (st) record_error(a.status, PART_UPDATE, cell, st);
-    if (st_lim) record_error(a.status, PART_LIMIT, cell, st_lim);
+    recon_cell(a, ph, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
 }
-
-// ---------------------------------------------------------- cell phase kernel
-
-template <class R>
-struct CellPhaseArgs {
-    int nx, ny;
-    Tab<R> tab;
-    const double* H;
-    const double* C;
-    const double* rec;
-    unsigned char* flags;
-    double* T;
-    double* phi;
-    unsigned long long* status;
-};
-
-__device__ __forceinline__ void load_rec(const double* rec, size_t N, long long cell, double* DH, double* DC) {
-#pragma unroll
-    for (int m = 0; m < 9; ++m) {
-        DH[m] = __ldg(rec + (size_t)m * N + cell);
-        DC[m] = __ldg(rec + (size_t)(m + 9) * N + cell);
-    }
-}
-
-// Cell quadrature of T and phi (evolve.cpp:359-376) and the wet flag of the
-// porosity sampling (initial_flow.cpp:56-67) on the same 5x5 points.
 template <class R>
 __global__ void __launch_bounds__(128) cellphase_kernel(CellPhaseArgs<R> a, Physics ph) {
-    const long long N = (long long)a.nx * a.ny;
-    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= N) return;
-    const StageTables& t = *a.tab.t;
-    const double mH = __ldg(a.H + cell), mC = __ldg(a.C + cell);
-    double DH[9], DC[9];
-    load_rec(a.rec, (size_t)N, cell, DH, DC);
-    int st_por = 0, st_cell = 0, st_face = 0;
-    double Tsum = 0.0, Psum = 0.0;
-    bool wet = false;
-    for (int b = 0; b < kNQ; ++b) {
-        double h0, h1, h2, c0, c1, c2;
-        const double y = t.gy[b];
-        q2_row(DH, y, h0, h1, h2);
-        q2_row(DC, y, c0, c1, c2);
-#pragma unroll
-        for (int q = 0; q < kNQ; ++q) {
-            const double x = t.gx[q];
-            const double h = mH + quad(h0, h1, h2, x);
-            const double c = mC + quad(c0, c1, c2, x);
-            PhaseLean pl;
-            const int s = phase_stage(ph.sk, h, c, ph.Tep, pl);
-            if (s) { st_por = st_por ? st_por : s; continue; }
-            if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_cell = st_cell ? st_cell : E_OUTOFRANGE;
-            const double w = t.cw[b * kNQ + q];
-            Tsum += w * pl.T;
-            Psum += w * pl.phil;
-            wet = wet || pl.phil > 0.0;
-        }
-    }
-    const unsigned char fl = a.flags[cell];
-    if (fl & FLAG_CHECK) {
-        // Exact admissibility of the limited values at the diffusion samples.
-        const int i = (int)(cell % a.nx), j = (int)(cell / a.nx);
-        const int ci = i == 0 ? 0 : (i == a.nx - 1 ? 2 : 1);
-        const int cj = j == 0 ? 0 : (j == a.ny - 1 ? 2 : 1);
-        const int cls = cj * 3 + ci;
-        for (int l = t.line_off[cls]; l < t.line_off[cls + 1]; ++l) {
-            if (!t.line_kind[l]) continue;
-            double h0, h1, h2, c0, c1, c2;
-            const bool row = t.line_dir[l] == 0;
-            const double lc = t.line_c[l];
-            if (row) { q2_row(DH, lc, h0, h1, h2); q2_row(DC, lc, c0, c1, c2); }
-            else { q2_col(DH, lc, h0, h1, h2); q2_col(DC, lc, c0, c1, c2); }
-            for (int q = 0; q < kNQ; ++q) {
-                const double s_ = row ? t.gx[q] : t.gy[q];
-                const double h = mH + quad(h0, h1, h2, s_);
-                const double c = mC + quad(c0, c1, c2, s_);
-                PhaseLean pl;
-                const int s = phase_stage(ph.sk, h, c, ph.Tep, pl);
-                if (s) { st_face = st_face ? st_face : s; continue; }
-                if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_face = st_face ? st_face : E_OUTOFRANGE;
-            }
-        }
-    }
-    if (st_por) record_error(a.status, PART_POROSITY, cell, st_por);
-    if (st_face) record_error(a.status, PART_FACES, cell, st_face);
-    if (st_cell) record_error(a.status, PART_CELLS, cell, st_cell);
-    a.flags[cell] = (unsigned char)((fl & FLAG_CHECK) | (wet ? FLAG_WET : 0));
-    a.T[cell] = Tsum;
-    a.phi[cell] = Psum;
+    cellphase_cell(a, ph, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
-
-// ---------------------------------------------------------------- face kernel
-
-template <class R>
-struct FaceArgs {
-    int nx, ny;
-    Tab<R> tab;
-    const double* H;
-    const double* C;
-    const double* rec;
-    const unsigned char* flags;
-    const double* vsn;     // [edge*5 + q], canonical
-    const double* udn;
-    double* face;          // 4 * nedge SoA: fluxH, fluxC, rate, fluxMixture
-    unsigned long long* status;
-};
-
-// Limited H and C of one side along the edge line: v(s) = m + c0 + s*(c1 + s*c2).
-struct SideLine {
-    double mH, mC;
-    double h0, h1, h2, c0, c1, c2;
-};
-
-template <class R>
-__device__ __forceinline__ void side_line(const FaceArgs<R>& a, size_t N, long long cell, bool row, double fixed,
-                                          SideLine& s) {
-    double DH[9], DC[9];
-    load_rec(a.rec, N, cell, DH, DC);
-    s.mH = __ldg(a.H + cell);
-    s.mC = __ldg(a.C + cell);
-    if (row) { q2_row(DH, fixed, s.h0, s.h1, s.h2); q2_row(DC, fixed, s.c0, s.c1, s.c2); }
-    else { q2_col(DH, fixed, s.h0, s.h1, s.h2); q2_col(DC, fixed, s.c0, s.c1, s.c2); }
-}
-
-// Limited evaluation + phase + Phase()'s admissibility (evolve.cpp:270-277).
-__device__ __forceinline__ int side_phase(const Physics& ph, const SideLine& s, double at, double& h, double& c,
-                                          PhaseLean& pl) {
-    h = s.mH + quad(s.h0, s.h1, s.h2, at);
-    c = s.mC + quad(s.c0, s.c1, s.c2, at);
-    int st = phase_stage(ph.sk, h, c, ph.Tep, pl);
-    if (!st && !(pl.T >= 0.0 && pl.phil < 1.0)) st = E_OUTOFRANGE;
-    return st;
-}
-
 template <class R>
 __global__ void __launch_bounds__(128) face_kernel(FaceArgs<R> a, Physics ph) {
-    const int nx = a.nx, ny = a.ny;
-    const long long nI = (long long)nx * (ny + 1);
-    const long long nE = nI + (long long)(nx + 1) * ny;
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nE) return;
-    const StageTables& t = *a.tab.t;
-    const size_t N = (size_t)nx * ny;
-    bool boundary, reverse, horizontal;
-    long long L, Rc = -1;
-    double len;
-    double lfix, rfix;   // the edge's fixed normalised coordinate in the left / right cell frame
-    // Left/right cells and orientation as the reference's Build (evolve.cpp:230-251).
-    if (e < nI) {
-        horizontal = true;
-        const int i = (int)(e % nx), j = (int)(e / nx);
-        boundary = (j == 0 || j == ny);
-        reverse = (j == ny);
-        L = reverse ? (long long)(ny - 1) * nx + i : (long long)j * nx + i;
-        if (!boundary) Rc = (long long)(j - 1) * nx + i;
-        lfix = reverse ? t.Y : -t.Y;
-        rfix = t.Y;
-        len = t.len_h;
-    } else {
-        horizontal = false;
-        const long long k = e - nI;
-        const int i = (int)(k % (nx + 1)), j = (int)(k / (nx + 1));
-        boundary = (i == 0 || i == nx);
-        reverse = (i == 0);
-        L = reverse ? (long long)j * nx : (long long)j * nx + (i - 1);
-        if (!boundary) Rc = (long long)j * nx + i;
-        lfix = reverse ? -t.X : t.X;
-        rfix = -t.X;
-        len = t.len_v;
-    }
-    SideLine sl, sr;
-    side_line(a, N, L, horizontal, lfix, sl);
-    if (!boundary) side_line(a, N, Rc, horizontal, rfix, sr);
-    const bool wetL = (a.flags[L] & FLAG_WET) != 0, wetR = boundary ? true : (a.flags[Rc] & FLAG_WET) != 0;
-    const double sgn = reverse ? -1.0 : 1.0;
-    const double LD = ph.k.LD;
-    double fluxH = 0.0, fluxC = 0.0, fluxMix = 0.0, rate = 0.0;
-    int st = 0;
-    for (int q = 0; q < kNQ; ++q) {
-        const int cq = reverse ? kNQ - 1 - q : q;
-        const double at = horizontal ? t.gx[cq] : t.gy[cq];
-        const double vs = sgn * __ldg(a.vsn + e * kNQ + cq);
-        const double ud = sgn * __ldg(a.udn + e * kNQ + cq);
-        double hL, cL, hR, cR;
-        PhaseLean A, B;
-        int s = side_phase(ph, sl, at, hL, cL, A);
-        if (boundary) { B = A; hR = hL; cR = cL; }
-        else {
-            const int s2 = side_phase(ph, sr, at, hR, cR, B);
-            s = s ? s : s2;
-        }
-        if (s) { st = st ? st : s; continue; }
-        // Edge porosity: harmonic mean of both sides, zero next to a dry cell
-        // (initial_flow.cpp:94-117).
-        double ephi = (A.phil + B.phil) > 0.0 ? 2.0 * A.phil * B.phil / (A.phil + B.phil) : 0.0;
-        if (!wetL || !wetR) ephi = 0.0;
-        // PhaseTransportVelocities (evolve.cpp:36-52) on normal components.
-        const double cl = 0.5 * (A.cl + B.cl), cs = 0.5 * (A.cs + B.cs);
-        const double bulk = ephi * cl + (1.0 - ephi) * cs;
-        const double factor = ephi == 0.0 ? 0.0 : (ph.theta == 0.0 ? ephi : pow(ephi, 1.0 + ph.theta));
-        const double flux = factor * ud;
-        const double vn = vs + flux;
-        const double ve = vs + (bulk > 0.0 ? cl / bulk * flux : 0.0);
-        const double aH = ph.lf_global ? ph.lf_speed : fabs(vn);
-        const double aC = ph.lf_global ? ph.lf_speed : fabs(ve);
-        if (ph.lf_global && !(aH + 1e-14 >= fabs(vn) && aC + 1e-14 >= fabs(ve))) st = st ? st : E_OUTOFRANGE;
-        double fh = 0.5 * (vn * (A.T + B.T) - aH * (B.T - A.T)) - LD * (1.0 - ephi) * vs;
-        double fc = 0.5 * (ve * (cL + cR) - aC * (cR - cL));
-        if (boundary) {
-            // EvaluateAdvectionBoundary (initialization.cpp:469-489) per field.
-            const int kh = (ph.Hpol == MP_BC_ZERO_FLUX || vn == 0.0) ? 2 : (vn < 0.0 ? 0 : 1);
-            const int kc = (ph.Cpol == MP_BC_ZERO_FLUX || ve == 0.0) ? 2 : (ve < 0.0 ? 0 : 1);
-            if ((kh == 0 && ph.Hpol != MP_BC_INFLOW_OUTFLOW) || (kc == 0 && ph.Cpol != MP_BC_INFLOW_OUTFLOW))
-                st = st ? st : E_OUTOFRANGE;
-            const double inC = kc == 0 ? ph.inflowC : cL;
-            double Tb = A.T;
-            if (kh == 0) {
-                PhaseLean pin;
-                const int s3 = phase_stage(ph.sk, ph.inflowH, inC, ph.Tep, pin);
-                if (s3) st = st ? st : s3;
-                Tb = pin.T;
-            }
-            fh = kh == 2 ? 0.0 : vn * Tb - LD * (1.0 - ephi) * vs;
-            fc = kc == 2 ? 0.0 : ve * (kc == 0 ? ph.inflowC : cL);
-        }
-        const double w = 0.5 * len * t.gw[q];
-        fluxH += w * fh;
-        fluxC += w * fc;
-        fluxMix += w * vn;
-        const double sens = 1.0 + fmax(fabs(A.dTdC), fabs(B.dTdC));
-        if (!isfinite(sens)) st = st ? st : E_FP;
-        rate += w * (aC + aH + 2.0 * fabs(vs)) * sens;
-    }
-    if (st) record_error(a.status, PART_FACES, L, st);
-    a.face[e] = fluxH;
-    a.face[nE + e] = fluxC;
-    a.face[2 * nE + e] = rate;
-    a.face[3 * nE + e] = fluxMix;
+    face_edge(a, ph, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
-
-// ----------------------------------------------------------------- sum kernel
-
-enum SumMode : int { SUM_STORE_L = 0, SUM_RK = 1 };
-
-struct SumArgs {
-    int nx, ny;
-    const StageTables* tab;
-    const double* face;
-    const double* H;       // stage state
-    const double* C;
-    const double* H0;      // U^n
-    const double* C0;
-    double* outH;          // RK: next state; STORE_L: rhs
-    double* outC;
-    double* rate;          // optional per-cell rate
-    int mode;
-    double a0, a1, dt;     // next = a0*U^n + a1*(U + dt*L)
-    Partial* partial;
-};
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-__device__ __forceinline__ double warp_max(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    return v;
-}
-__device__ __forceinline__ double warp_min(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
-    return v;
-}
-
-// Deterministic block reduction of a Partial (fixed shuffle tree per block).
-__device__ void block_reduce_write(Partial v, Partial* out) {
-    __shared__ double sh[32][10];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double r[10] = {v.maxRate, v.divergence, v.bH, v.bC, v.HI, v.CI, v.Hmin, v.Cmin, v.Cmax, v.nonfinite};
-    r[0] = warp_max(r[0]); r[1] = warp_max(r[1]);
-    r[2] = warp_sum(r[2]); r[3] = warp_sum(r[3]); r[4] = warp_sum(r[4]); r[5] = warp_sum(r[5]);
-    r[6] = warp_min(r[6]); r[7] = warp_min(r[7]); r[8] = warp_max(r[8]); r[9] = warp_max(r[9]);
-    if (lane == 0)
-        for (int k = 0; k < 10; ++k) sh[warp][k] = r[k];
-    __syncthreads();
-    if (warp == 0) {
-        const int nw = (blockDim.x + 31) >> 5;
-        const Partial id{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
-        double s[10] = {id.maxRate, id.divergence, 0, 0, 0, 0, id.Hmin, id.Cmin, id.Cmax, 0};
-        if (lane < nw) for (int k = 0; k < 10; ++k) s[k] = sh[lane][k];
-        s[0] = warp_max(s[0]); s[1] = warp_max(s[1]);
-        s[2] = warp_sum(s[2]); s[3] = warp_sum(s[3]); s[4] = warp_sum(s[4]); s[5] = warp_sum(s[5]);
-        s[6] = warp_min(s[6]); s[7] = warp_min(s[7]); s[8] = warp_max(s[8]); s[9] = warp_max(s[9]);
-        if (lane == 0) *out = Partial{s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], s[8], s[9]};
-    }
-}
-
 __global__ void __launch_bounds__(kRedBlock) sum_kernel(SumArgs a) {
-    const int nx = a.nx, ny = a.ny;
-    const long long N = (long long)nx * ny;
-    const long long nI = (long long)nx * (ny + 1);
-    const long long nE = nI + (long long)(nx + 1) * ny;
-    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    Partial v{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
-    if (cell < N) {
-        const StageTables& t = *a.tab;
-        const int i = (int)(cell % nx), j = (int)(cell / nx);
-        const double A = t.area;
-        // Faces of this cell in the reference's id order: bottom, top, left, right,
-        // each with the sign of its side (evolve.cpp:350-354).
-        const long long eb = (long long)j * nx + i, et = (long long)(j + 1) * nx + i;
-        const long long el = nI + (long long)j * (nx + 1) + i, er = el + 1;
-        const double sb = -1.0, stp = (j == ny - 1) ? -1.0 : 1.0, sl = (i == 0) ? -1.0 : 1.0, sr = -1.0;
-        const long long ids[4] = {eb, et, el, er};
-        const double sg[4] = {sb, stp, sl, sr};
-        double rH = 0.0, rC = 0.0, rr = 0.0, dv = 0.0, bH = 0.0, bC = 0.0;
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            const double FH = a.face[ids[f]], FC = a.face[nE + ids[f]];
-            const double FR = a.face[2 * nE + ids[f]], FM = a.face[3 * nE + ids[f]];
-            rH += sg[f] * FH / A;
-            rC += sg[f] * FC / A;
-            rr += FR / A;
-            dv += -sg[f] * FM / A;
-        }
-        if (j == 0) { bH += a.face[eb]; bC += a.face[nE + eb]; }
-        if (j == ny - 1) { bH += a.face[et]; bC += a.face[nE + et]; }
-        if (i == 0) { bH += a.face[el]; bC += a.face[nE + el]; }
-        if (i == nx - 1) { bH += a.face[er]; bC += a.face[nE + er]; }
-        double nh, nc;
-        if (a.mode == SUM_RK) {
-            const double h = a.H[cell], c = a.C[cell];
-            const double sh_ = __dadd_rn(h, __dmul_rn(a.dt, rH));
-            const double sc_ = __dadd_rn(c, __dmul_rn(a.dt, rC));
-            nh = __dadd_rn(__dmul_rn(a.a0, a.H0[cell]), __dmul_rn(a.a1, sh_));
-            nc = __dadd_rn(__dmul_rn(a.a0, a.C0[cell]), __dmul_rn(a.a1, sc_));
-        } else {
-            nh = a.H[cell]; nc = a.C[cell];
-        }
-        a.outH[cell] = a.mode == SUM_RK ? nh : rH;
-        a.outC[cell] = a.mode == SUM_RK ? nc : rC;
-        if (a.rate) a.rate[cell] = rr;
-        v.maxRate = rr;
-        v.divergence = fabs(dv);
-        v.bH = bH; v.bC = bC;
-        v.HI = nh * A; v.CI = nc * A;
-        v.Hmin = nh; v.Cmin = nc; v.Cmax = nc;
-        v.nonfinite = (isfinite(nh) && isfinite(nc) && isfinite(rr)) ? 0.0 : 1.0;
-    }
+    const Partial v = sum_cell(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);
     block_reduce_write(v, a.partial + blockIdx.x);
 }
 

@@ -1,0 +1,93 @@
+"""Batched transport: each instance equals its single-instance run bit for bit."""
+import numpy as np
+import pytest
+
+from mantlepar_b200 import synthetic as sy
+
+pytestmark = pytest.mark.gpu
+
+WORKLOADS = [sy.Workload(nx=20, ny=20, seed=1), sy.Workload(nx=40, ny=60, seed=5, psi_amplitude=0.15),
+             sy.Workload(nx=3, ny=5, seed=7), sy.Workload(nx=64, ny=32, seed=9, noise_H=0.1),
+             sy.Workload(nx=2, ny=2, seed=11, psi_amplitude=0.05)]
+
+
+def solo(w, cfg, steps):
+    from mantlepar_b200.transport import Transport
+    t = Transport(w, cfg)
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    t.set_face_velocity(vs, ud)
+    t.set_state(H, C)
+    _, reps = t.step(steps)
+    return t.get_state(), reps
+
+
+def batch_of(ws, cfg):
+    from mantlepar_b200.batch import Batch
+    b = Batch(ws, cfg)
+    for i, w in enumerate(ws):
+        vs, ud = sy.face_velocity(w)
+        H, C = sy.initial_state(w)
+        b.set_face_velocity(i, vs, ud)
+        b.set_state(i, H, C)
+    return b
+
+
+@pytest.mark.parametrize("precision,integ", [(0, 3), (0, 2), (1, 3)])
+def test_batch_equals_solo_bitwise(cuda_lib, precision, integ):
+    from mantlepar_b200.transport import TransportConfig
+    cfg = TransportConfig(cfl=0.4, integrator=integ, precision=precision)
+    b = batch_of(WORKLOADS, cfg)
+    reps = b.step(8)
+    for i, w in enumerate(WORKLOADS):
+        (H, C, T, phi), sreps = solo(w, cfg, 8)
+        got = b.get_state(i)
+        assert got["status"] == 0 and got["accepted"] == 8
+        for a, x in ((got["H"], H), (got["C"], C), (got["T"], T), (got["phi"], phi)):
+            assert np.array_equal(a, x)
+        assert [r[i]["retries"] for r in reps] == [r["retries"] for r in sreps]
+        assert [r[i]["dt"] for r in reps] == [r["dt"] for r in sreps]
+        assert [r[i]["balanceH"] for r in reps] == [r["balanceH"] for r in sreps]
+
+
+def test_failing_instance_is_isolated(cuda_lib):
+    from mantlepar_b200.transport import TransportConfig
+    cfg = TransportConfig(cfl=0.4, integrator=3)
+    b = batch_of(WORKLOADS[:3], cfg)
+    w = WORKLOADS[1]
+    H, C = sy.initial_state(w)
+    C = C.copy()
+    C[17] = 0.9
+    b.set_state(1, H, C)
+    b.step(3)
+    bad = b.get_state(1)
+    assert bad["status"] == 63 and bad["accepted"] == 0
+    assert np.array_equal(bad["C"], C)
+    for i in (0, 2):
+        (Hs, Cs, _, _), _ = solo(WORKLOADS[i], cfg, 3)
+        got = b.get_state(i)
+        assert got["status"] == 0 and np.array_equal(got["H"], Hs) and np.array_equal(got["C"], Cs)
+
+
+def test_add_remove_and_autotune_keep_results(cuda_lib):
+    from mantlepar_b200.transport import TransportConfig
+    cfg = TransportConfig(cfl=0.4, integrator=3)
+    b = batch_of(WORKLOADS[:2], cfg)
+    tile, ms = b.autotune(reps=1)
+    assert len(tile) == 3 and ms > 0
+    b.step(2)
+    b.remove(0)
+    k = b.add(WORKLOADS[3])
+    assert k == 0                       # the freed slot is reused
+    vs, ud = sy.face_velocity(WORKLOADS[3])
+    H, C = sy.initial_state(WORKLOADS[3])
+    b.set_face_velocity(k, vs, ud)
+    b.set_state(k, H, C)
+    b.step(3)
+    (H1, C1, _, _), _ = solo(WORKLOADS[1], cfg, 5)
+    got = b.get_state(1)
+    assert np.array_equal(got["H"], H1) and np.array_equal(got["C"], C1)
+    (H3, C3, _, _), _ = solo(WORKLOADS[3], cfg, 3)
+    got = b.get_state(k)
+    assert np.array_equal(got["H"], H3) and np.array_equal(got["C"], C3)
+    assert b.bytes_in_use() == sum(b.instance_bytes(w) for w in (WORKLOADS[1], WORKLOADS[3]))
