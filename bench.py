@@ -185,6 +185,73 @@ def config_block():
             "l2": "inputs larger than L2 (per-stage working set ~1.1 GB > 126 MB)"}
 
 
+def rel_errors(got, ref):
+    """Per-cell |x-ref|/max(|ref|, 1e-3*max|ref|) (max, L2) and normwise error."""
+    scale = np.maximum(np.abs(ref), 1e-3 * np.max(np.abs(ref)))
+    e = np.abs(got - ref) / scale
+    return {"max": float(np.max(e)), "l2": float(np.sqrt(np.mean(e * e))),
+            "normwise": float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))}
+
+
+def timed_steps(obj, steps, stream):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    out = obj.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+def run_forms(args, stream):
+    """The mixed-precision large instance and the batched uneven meshes."""
+    from mantlepar_b200 import synthetic as sy
+    from mantlepar_b200.batch import Batch
+    from mantlepar_b200.transport import Transport, TransportConfig
+    forms = {}
+    # Mixed precision: 4096x4096, H noise 0.1, SSPRK3; errors against the FP64 path
+    # (which matches the FP64 oracle to 1e-12 at the small sizes the oracle runs).
+    w = sy.mixed_large()
+    H, Cc = sy.initial_state(w)
+    vs, ud = sy.face_velocity(w)
+    res = {}
+    for prec in (1, 0):
+        t = Transport(w, TransportConfig(cfl=w.cfl, integrator=3, precision=prec), stream=stream.cuda_stream)
+        t.set_face_velocity(vs, ud)
+        t.set_state(H, Cc)
+        t.step(1)
+        ms, _ = timed_steps(t, args.form_steps, stream)
+        res[prec] = (ms, t.get_state())
+        t.close()
+    errs = {name: rel_errors(a, b) for name, a, b in zip(["H", "C", "T", "phi"], res[1][1], res[0][1])}
+    forms["mixed_4096x4096"] = {
+        "value": w.cells * args.form_steps / (res[1][0] * 1e-3), "unit": "cell-updates/s",
+        "fp64_value": w.cells * args.form_steps / (res[0][0] * 1e-3),
+        "steps": args.form_steps, "errors_vs_fp64_path": errs,
+        "precision": "FP32 smoothness/weights/limiter scan; FP64 coefficients, phase, fluxes"}
+    del res
+    # Batched: 256 uneven meshes (seed 3), mixed and FP64, autotuned tiles.
+    ws = sy.batched_instances(256, seed=3)
+    cells = sum(x.cells for x in ws)
+    for prec, name in ((1, "batched_mixed_256"), (0, "batched_fp64_256")):
+        b = Batch(ws, TransportConfig(cfl=0.4, integrator=3, precision=prec), stream=stream.cuda_stream)
+        for i, x in enumerate(ws):
+            vs_i, ud_i = sy.face_velocity(x)
+            H_i, C_i = sy.initial_state(x)
+            b.set_face_velocity(i, vs_i, ud_i)
+            b.set_state(i, H_i, C_i)
+        tile, _ = b.autotune(reps=1)
+        b.step(1)
+        ms, reps = timed_steps(b, args.form_steps, stream)
+        ok = all(r[i]["status"] == 0 for r in reps for i in range(len(ws)))
+        forms[name] = {"value": cells * args.form_steps / (ms * 1e-3), "unit": "cell-updates/s",
+                       "instances": len(ws), "cells": cells, "steps": args.form_steps,
+                       "autotuned_tile": list(tile), "all_instances_healthy": ok}
+        b.close()
+    return forms
+
+
 def run_gpu(args, world, rank, local):
     import torch
     torch.cuda.set_device(local)
@@ -304,6 +371,11 @@ def run_gpu(args, world, rank, local):
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+    if rank == 0 and world == 1 and not args.no_forms:
+        forms = run_forms(args, torch.cuda.current_stream(dev))
+        forms["plain_fp64_1280x2560"] = {"value": value, "unit": "cell-updates/s"}
+        forms["batched_mixed_over_plain_fp64"] = forms["batched_mixed_256"]["value"] / value
+        line["forms"] = forms
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, kind, sample, _, _ = cpu_run(2, CPU_SECONDS, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": kind, "sample": sample}
@@ -318,6 +390,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mantlepar_b200", choices=["mantlepar_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the mixed / batched forms")
+    ap.add_argument("--form-steps", type=int, default=5, help="timed steps of each extra form")
     ap.add_argument("--nx", type=int, default=WORKLOAD["nx"], help="cells in x (profiling of smaller cases)")
     ap.add_argument("--ny", type=int, default=WORKLOAD["ny"], help="cells in y")
     args = ap.parse_args()
