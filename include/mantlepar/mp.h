@@ -212,11 +212,41 @@ mp_status mp_batch_get_state(mp_batch* b, int instance, double* H, double* C, do
  * holds nsteps * slots entries, step-major; an instance that fails stops
  * (its status is reported) while the others continue. */
 mp_status mp_batch_step(mp_batch* b, int nsteps, mp_step_report* reports);
+/* Final time of an instance (time.end, src/couple/input.h:155): its steps
+ * are limited to the remaining time and it stops there; finished() reports
+ * it (within 32 eps, as src/couple/evolve.cpp:450-451). */
+mp_status mp_batch_set_end_time(mp_batch* b, int instance, double t_end);
+int mp_batch_finished(const mp_batch* b, int instance);
 /* Project autotuner: times the candidate reconstruction tile shapes and
  * cells-per-thread on this batch and keeps the fastest; tile = {bx, by, cpt}. */
 mp_status mp_batch_autotune(mp_batch* b, int reps, int tile[3], double* best_ms);
 mp_status mp_batch_profile(mp_batch* b, int enable);
 mp_status mp_batch_kernel_times(mp_batch* b, double ms[6], unsigned long long launches[6]);
+
+/* --------------------------------------------------------------- serving */
+
+/* A request loop for transport solves of different sizes (no counterpart in
+ * the reference): requests are admitted in arrival order while their device
+ * bytes fit the budget, advanced together one step at a time (continuous
+ * batching: work that arrives while others run joins at the next step), and
+ * released at their final time. Inputs are host arrays, copied on submit. */
+typedef struct mp_server mp_server;
+typedef struct mp_request_info {
+    int status, accepted;       /* final status, accepted steps */
+    double time;                /* reached time (= t_final on success) */
+    double queue_s, latency_s;  /* submit -> admit, submit -> result */
+    double cells;
+} mp_request_info;
+mp_status mp_serve_create(const mp_transport_opts* opts, size_t memory_budget, mp_server** out);
+void mp_serve_destroy(mp_server* s);
+mp_status mp_serve_submit(mp_server* s, const mp_mesh_desc* mesh, const double* H, const double* C,
+                          const double* vs_n, const double* ud_n, double t_final, long long* id);
+/* Block until request id finishes (timeout_s < 0: no limit; on expiry
+ * MP_ERR_TIMEOUT and the request stays queued/running). */
+mp_status mp_serve_wait(mp_server* s, long long id, double timeout_s, double* H, double* C, double* T,
+                        double* phi, mp_request_info* info);
+mp_status mp_serve_stats(mp_server* s, double* cell_updates, double* busy_s, long long* steps,
+                         int* resident, int* queued);
 
 /* One stage evaluation (as mp_transport_rhs) that allocates no device memory,
  * for callers that cannot call cudaMalloc -- e.g. code inside a framework that

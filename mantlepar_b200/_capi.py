@@ -71,6 +71,11 @@ class StepReport(C.Structure):
                 ("C_integral", C.c_double)]
 
 
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("accepted", C.c_int), ("time", C.c_double), ("queue_s", C.c_double),
+                ("latency_s", C.c_double), ("cells", C.c_double)]
+
+
 class StageTotals(C.Structure):
     _fields_ = [(n, C.c_double) for n in ["boundaryH", "boundaryC", "sourceH", "maxRate", "divergence"]]
 
@@ -124,6 +129,14 @@ def lib() -> C.CDLL:
         "mp_batch_step": (i, [vp, i, C.POINTER(StepReport)]),
         "mp_batch_autotune": (i, [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
         "mp_batch_profile": (i, [vp, i]),
+        "mp_batch_set_end_time": (i, [vp, i, d]),
+        "mp_batch_finished": (i, [vp, i]),
+        "mp_serve_create": (i, [C.POINTER(TransportOpts), sz, C.POINTER(vp)]),
+        "mp_serve_destroy": (None, [vp]),
+        "mp_serve_submit": (i, [vp, C.POINTER(MeshDesc), vp, vp, vp, vp, d, C.POINTER(C.c_longlong)]),
+        "mp_serve_wait": (i, [vp, C.c_longlong, d, vp, vp, vp, vp, C.POINTER(RequestInfo)]),
+        "mp_serve_stats": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                               C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "mp_batch_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
     }
     for name, (res, args) in sig.items():

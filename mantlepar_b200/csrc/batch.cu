@@ -164,11 +164,19 @@ struct MPInstance {
     mp::StageTablesF* tabF;
     mp::StageTables host_tab;
     double time = 0.0;
+    double t_end = INFINITY;          // time.end of this instance
     int accepted = 0;
     bool have_L = false;
     mp::Totals cur{};
     int status = 0;                   // sticky failure status
 };
+
+// time.end reached (src/couple/evolve.cpp:450-451: within 32 eps of the end).
+static bool finished(const MPInstance& in) {
+    if (!std::isfinite(in.t_end)) return false;
+    const double remaining = in.t_end - in.time;
+    return remaining <= 32 * 2.220446049250313e-16 * std::max(1.0, std::fabs(in.t_end));
+}
 
 struct mp_batch {
     mp_transport_opts opts;
@@ -497,13 +505,16 @@ mp_status step_all(mp_batch* b, std::vector<mp_step_report>& reps) {
     std::vector<double> dt(slots, 0.0), start(slots, 0.0), courant(slots, 0.0);
     std::vector<int> retries(slots, 0), pending(slots, 0), done(slots, 0);
     std::vector<Totals> first(slots), second(slots), third(slots);
+    std::vector<double> remaining(slots, INFINITY);
     for (int i = 0; i < slots; ++i) {
         MPInstance& in = b->inst[i];
         if (!in.used || in.status) continue;
+        if (finished(in)) { in.time = in.t_end; continue; }
         first[i] = in.cur;
+        remaining[i] = in.t_end - in.time;
         const double cap = in.accepted == 0 ? o.dt_initial : o.dt_max;
         const double limit = in.cur.maxRate > 0 ? o.cfl / in.cur.maxRate : o.dt_max;
-        dt[i] = std::min(cap, limit);
+        dt[i] = std::min(std::min(remaining[i], cap), limit);
         start[i] = in.time;
         pending[i] = 1;
     }
@@ -511,7 +522,7 @@ mp_status step_all(mp_batch* b, std::vector<mp_step_report>& reps) {
         bool any = false;
         for (int i = 0; i < slots; ++i) {
             if (!pending[i]) continue;
-            if (!(dt[i] >= o.dt_min && retries[i] < 40)) { b->inst[i].status = MP_ERR_NOT_CONVERGED; pending[i] = 0; continue; }
+            if (!(dt[i] >= std::min(remaining[i], o.dt_min) && retries[i] < 40)) { b->inst[i].status = MP_ERR_NOT_CONVERGED; pending[i] = 0; continue; }
             b->h_dt[i] = dt[i];
             any = true;
         }
@@ -573,6 +584,8 @@ mp_status step_all(mp_batch* b, std::vector<mp_step_report>& reps) {
         MP_CUDA(cudaMemcpyAsync(in.H, nH, in.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
         MP_CUDA(cudaMemcpyAsync(in.C, nC, in.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
         in.time = start[i] + dt[i];
+        if (std::isfinite(in.t_end) && in.t_end - in.time <= 32 * 2.220446049250313e-16 * std::max(1.0, std::fabs(in.t_end)))
+            in.time = in.t_end;
         in.have_L = false;
         mp_step_report& r = reps[i];
         r.retries = retries[i]; r.dt = dt[i]; r.time = in.time; r.courant = courant[i];
@@ -762,6 +775,19 @@ extern "C" mp_status mp_batch_step(mp_batch* b, int nsteps, mp_step_report* repo
 }
 
 extern "C" int mp_batch_slots(const mp_batch* b) { return b ? (int)b->inst.size() : 0; }
+
+extern "C" mp_status mp_batch_set_end_time(mp_batch* b, int i, double t_end) {
+    MPInstance* in;
+    MP_TRY(batch_slot(b, i, &in));
+    if (std::isnan(t_end)) { mp::set_error("end time must not be NaN"); return MP_ERR_ARG_OUTOFRANGE; }
+    in->t_end = t_end;
+    return MP_OK;
+}
+
+extern "C" int mp_batch_finished(const mp_batch* b, int i) {
+    if (!b || i < 0 || i >= (int)b->inst.size() || !b->inst[i].used) return 0;
+    return finished(b->inst[i]) ? 1 : 0;
+}
 
 extern "C" size_t mp_batch_bytes_in_use(const mp_batch* b) { return b ? b->bytes_in_use : 0; }
 

@@ -1,0 +1,117 @@
+"""Serving: a request loop for transport solves of different sizes.
+
+`Server` wraps mp_serve_* (C++ loop thread, memory admission, continuous
+batching). `poisson_requests` draws the served workload: Poisson arrivals
+(mean 200 req/s), nx in {20..1280 step 20}, ny = nx * U{1,2}, final time
+U[0.01, 0.1], initial H/C as the 20x20 workload's construction.
+`run_stream` submits each request at its arrival time from a client thread
+and returns per-request latencies and the aggregate throughput.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import threading
+import time
+
+import numpy as np
+
+from . import _capi
+from .synthetic import Workload, face_velocity, initial_state
+from .transport import TransportConfig
+
+
+@dataclasses.dataclass
+class Request:
+    arrival: float
+    workload: Workload
+    t_final: float
+
+
+def poisson_requests(n: int, rate: float = 200.0, seed: int = 4, max_nx: int = 1280) -> list[Request]:
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(n):
+        t += rng.exponential(1.0 / rate)
+        nx = int(rng.integers(1, max_nx // 20 + 1)) * 20
+        ny = nx * int(rng.integers(1, 3))
+        tf = float(rng.uniform(0.01, 0.1))
+        out.append(Request(t, Workload(nx=nx, ny=ny, seed=100 + k), tf))
+    return out
+
+
+class Server:
+    def __init__(self, config: TransportConfig | None = None, memory_budget: int = 16 << 30):
+        self._lib = _capi.lib()
+        self.config = config or TransportConfig()
+        opts = self.config.to_c()
+        h = C.c_void_p()
+        _capi.check(self._lib.mp_serve_create(C.byref(opts), C.c_size_t(memory_budget), C.byref(h)))
+        self._h = h
+        self._cells = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mp_serve_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, w: Workload, t_final: float, H=None, Cc=None, vs=None, ud=None) -> int:
+        if H is None:
+            H, Cc = initial_state(w)
+        if vs is None:
+            vs, ud = face_velocity(w)
+        m = _capi.MeshDesc(w.nx, w.ny, w.x0, w.x1, w.y0, w.y1)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (H, Cc, vs, ud)]
+        rid = C.c_longlong(0)
+        _capi.check(self._lib.mp_serve_submit(self._h, C.byref(m), *[a.ctypes.data for a in arrs],
+                                              float(t_final), C.byref(rid)))
+        self._cells[rid.value] = w.cells
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = -1.0):
+        n = self._cells.pop(rid)
+        H, Cc, T, phi = (np.zeros(n) for _ in range(4))
+        info = _capi.RequestInfo()
+        _capi.check(self._lib.mp_serve_wait(self._h, C.c_longlong(rid), float(timeout), H.ctypes.data,
+                                            Cc.ctypes.data, T.ctypes.data, phi.ctypes.data, C.byref(info)))
+        return dict(H=H, C=Cc, T=T, phi=phi, **{k: getattr(info, k) for k, _ in _capi.RequestInfo._fields_})
+
+    def stats(self):
+        cu, busy, steps, res, q = C.c_double(0), C.c_double(0), C.c_longlong(0), C.c_int(0), C.c_int(0)
+        _capi.check(self._lib.mp_serve_stats(self._h, C.byref(cu), C.byref(busy), C.byref(steps), C.byref(res), C.byref(q)))
+        return dict(cell_updates=cu.value, busy_s=busy.value, steps=steps.value, resident=res.value, queued=q.value)
+
+
+def run_stream(server: Server, requests: list[Request]) -> dict:
+    """Submit each request at its arrival time; wait for all; latencies in ms."""
+    inputs = [(initial_state(r.workload), face_velocity(r.workload)) for r in requests]
+    ids = [None] * len(requests)
+    t0 = time.perf_counter()
+
+    def client():
+        for k, r in enumerate(requests):
+            delay = r.arrival - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            (H, Cc), (vs, ud) = inputs[k]
+            ids[k] = server.submit(r.workload, r.t_final, H, Cc, vs, ud)
+
+    th = threading.Thread(target=client)
+    th.start()
+    th.join()
+    results = [server.wait(rid) for rid in ids]
+    wall = time.perf_counter() - t0
+    lat = np.array([r["latency_s"] for r in results]) * 1e3
+    stats = server.stats()
+    return dict(requests=len(requests), wall_s=wall, p50_ms=float(np.percentile(lat, 50)),
+                p99_ms=float(np.percentile(lat, 99)), mean_ms=float(lat.mean()),
+                cell_updates=stats["cell_updates"], value=stats["cell_updates"] / wall,
+                gpu_busy_value=stats["cell_updates"] / max(stats["busy_s"], 1e-12),
+                all_ok=all(r["status"] == 0 for r in results), results=results)

@@ -1,0 +1,58 @@
+"""Serving: continuous batching with memory admission; every served result is
+bitwise the result of the same solve run alone."""
+import numpy as np
+import pytest
+
+from mantlepar_b200 import synthetic as sy
+
+pytestmark = pytest.mark.gpu
+
+
+def alone(w, tf, cfg):
+    from mantlepar_b200.batch import Batch
+    b = Batch([w], cfg)
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    b.set_face_velocity(0, vs, ud)
+    b.set_state(0, H, C)
+    b._lib.mp_batch_set_end_time(b._h, 0, tf)
+    for _ in range(10000):
+        if b._lib.mp_batch_finished(b._h, 0):
+            break
+        b.step(1)
+    return b.get_state(0)
+
+
+def test_served_results_equal_solo_runs(cuda_lib):
+    from mantlepar_b200.batch import Batch
+    from mantlepar_b200.serve import Server
+    from mantlepar_b200.transport import TransportConfig
+    cfg = TransportConfig(cfl=0.4, integrator=3)
+    reqs = [(sy.Workload(nx=20, ny=20, seed=21), 0.02), (sy.Workload(nx=40, ny=80, seed=22), 0.004),
+            (sy.Workload(nx=60, ny=60, seed=23), 0.003), (sy.Workload(nx=20, ny=40, seed=24), 0.03),
+            (sy.Workload(nx=80, ny=80, seed=25), 0.002), (sy.Workload(nx=40, ny=40, seed=26), 0.01)]
+    # A budget for about two of the larger requests at once forces queueing.
+    budget = 2 * Batch.instance_bytes(sy.Workload(nx=80, ny=80)) + Batch.instance_bytes(sy.Workload(nx=20, ny=20))
+    srv = Server(cfg, memory_budget=budget)
+    ids = [srv.submit(w, tf) for w, tf in reqs]
+    got = [srv.wait(i, timeout=120.0) for i in ids]
+    st = srv.stats()
+    srv.close()
+    assert st["cell_updates"] > 0 and st["steps"] > 0
+    assert any(g["queue_s"] > 0 for g in got)
+    for (w, tf), g in zip(reqs, got):
+        assert g["status"] == 0 and g["time"] == tf
+        ref = alone(w, tf, cfg)
+        assert g["accepted"] == ref["accepted"]
+        for k in ("H", "C", "T", "phi"):
+            assert np.array_equal(g[k], ref[k]), k
+
+
+def test_oversized_request_is_refused(cuda_lib):
+    from mantlepar_b200._capi import MPError
+    from mantlepar_b200.serve import Server
+    srv = Server(memory_budget=1 << 20)
+    with pytest.raises(MPError) as err:
+        srv.submit(sy.Workload(nx=200, ny=200), 0.01)
+    assert err.value.code == 111
+    srv.close()
