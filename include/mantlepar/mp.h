@@ -226,8 +226,8 @@ mp_status mp_batch_kernel_times(mp_batch* b, double ms[6], unsigned long long la
 /* --------------------------------------------------------------- serving */
 
 /* A request loop for transport solves of different sizes (no counterpart in
- * the reference): requests are admitted in arrival order while their device
- * bytes fit the budget, advanced together one step at a time (continuous
+ * the reference): requests are admitted while their device bytes fit the
+ * budget and the resident cells are below a target, advanced together one step at a time (continuous
  * batching: work that arrives while others run joins at the next step), and
  * released at their final time. Inputs are host arrays, copied on submit. */
 typedef struct mp_server mp_server;
@@ -247,13 +247,18 @@ mp_status mp_serve_wait(mp_server* s, long long id, double timeout_s, double* H,
                         double* phi, mp_request_info* info);
 mp_status mp_serve_stats(mp_server* s, double* cell_updates, double* busy_s, long long* steps,
                          int* resident, int* queued);
+/* Admission order and resident-cell target (0 = admit while memory fits).
+ * Default: smallest estimated work (cells * t_final * cells per unit length)
+ * first, 4e6 cells. */
+enum { MP_SERVE_FIFO = 0, MP_SERVE_SMALLEST_WORK = 1 };
+mp_status mp_serve_set_policy(mp_server* s, int order, double resident_cells_target);
 
 /* One stage evaluation (as mp_transport_rhs) that allocates no device memory,
  * for callers that cannot call cudaMalloc -- e.g. code inside a framework that
  * owns all device memory through its own pool, or code that must not allocate
  * once its latency-critical phase has begun. No counterpart in the reference
  * (its CPU code allocates freely). All scratch lives in one fixed file-scope
- * device array (about 7.4 MB per GPU that loads the library, held until the
+ * device array (about 7.3 MB per GPU that loads the library, held until the
  * process exits); meshes above 32768 cells (nx*ny) are rejected with
  * MP_ERR_ARG_SIZ. The first call on each device looks up that array's device
  * address, so make it before any stream capture. Calls share the array and

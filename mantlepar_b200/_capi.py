@@ -137,6 +137,7 @@ def lib() -> C.CDLL:
         "mp_serve_wait": (i, [vp, C.c_longlong, d, vp, vp, vp, vp, C.POINTER(RequestInfo)]),
         "mp_serve_stats": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "mp_serve_set_policy": (i, [vp, i, d]),
         "mp_batch_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
     }
     for name, (res, args) in sig.items():

@@ -31,15 +31,6 @@ mp_status derive_checked(const mp_material& p, mp_derived& d);
 
 namespace {
 
-void tables_to_float_b(const StageTables& t, StageTablesF& f) {
-    for (int a = 0; a < 9; ++a) for (int b = 0; b < 9; ++b) f.C9[a][b] = (float)t.C9[a][b];
-    for (int a = 0; a < 8; ++a) for (int b = 0; b < 8; ++b) f.S9[a][b] = (float)t.S9[a][b];
-    for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) f.C4[a][b] = (float)t.C4[a][b];
-    for (int k = 0; k < 4; ++k) for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) f.S4[k][a][b] = (float)t.S4[k][a][b];
-    f.X = (float)t.X; f.Y = (float)t.Y; f.epsA = (float)t.epsA; f.logEpsA2 = (float)(2.0 * std::log(t.epsA));
-    for (int q = 0; q < kNQ; ++q) { f.gx[q] = (float)t.gx[q]; f.gy[q] = (float)t.gy[q]; }
-    for (int l = 0; l < kMaxLines; ++l) f.line_c[l] = (float)t.line_c[l];
-}
 
 // Stage kinds: P evaluates L(U^n) (store L), B the second stage (RK combine
 // into S2), C the third stage of SSPRK3 (RK combine into S1).
@@ -275,7 +266,7 @@ mp_status alloc_instance(mp_batch* b, MPInstance& in, const mp_mesh_desc& m) {
     in.tab = static_cast<StageTables*>(take(sizeof(StageTables)));
     in.tabF = static_cast<StageTablesF*>(take(sizeof(StageTablesF)));
     StageTablesF tf;
-    tables_to_float_b(in.host_tab, tf);
+    tables_to_float(in.host_tab, tf);
     MP_CUDA(cudaMemcpyAsync(in.tab, &in.host_tab, sizeof(StageTables), cudaMemcpyHostToDevice, b->stream));
     MP_CUDA(cudaMemcpyAsync(in.tabF, &tf, sizeof(StageTablesF), cudaMemcpyHostToDevice, b->stream));
     MP_CUDA(cudaMemsetAsync(in.vsn, 0, NE * kNQ * sizeof(double), b->stream));
@@ -337,7 +328,7 @@ mp_status rebuild_args(mp_batch* b, int slots) {
             const bool rk3 = b->opts.integrator == MP_SSPRK3;
             const double a0 = k == KIND_B ? (rk3 ? 0.75 : 0.5) : (1.0 / 3.0);
             const double a1 = k == KIND_B ? (rk3 ? 0.25 : 0.5) : (2.0 / 3.0);
-            a.sum = SumArgs{in.nx, in.ny, in.tab, in.face, inH, inC, in.H, in.C, outH, outC, in.rate,
+            a.sum = SumArgs{in.nx, in.ny, in.host_tab.area, in.face, inH, inC, in.H, in.C, outH, outC, in.rate,
                             k == KIND_P ? (int)SUM_STORE_L : (int)SUM_RK, a0, a1, 0.0, b->d_partial + parts,
                             b->d_dt + i};
         }

@@ -4,14 +4,15 @@
 // that owns all device memory through its own pool (and forbids or cannot
 // reach the CUDA allocator), or code whose every allocation must happen
 // before a latency-critical phase. For them this entry point evaluates one
-// transport stage with every piece of scratch memory (stencil tables,
-// per-cell reconstruction records, face fluxes, reduction partials, status
-// word) taken from one file-scope device array of fixed size. The caller
+// transport stage with every piece of scratch memory (per-cell
+// reconstruction records, face fluxes, reduction partials, status word)
+// taken from one file-scope device array of fixed size; the stencil tables
+// travel as kernel parameters. The caller
 // still provides the inputs and outputs (device memory).
 //
 // Limits and behaviour:
 //  - at most kMaxCells cells (nx*ny <= 32768); larger meshes are rejected
-//    with MP_ERR_ARG_SIZ; the array holds about 7.4 MB on every GPU that
+//    with MP_ERR_ARG_SIZ; the array holds about 7.3 MB on every GPU that
 //    loads this library, until the process exits;
 //  - the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current, so make the first
@@ -28,7 +29,7 @@ namespace mp {
 
 mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double* H, const double* C,
                         const double* vsn, const double* udn, double* rhsH, double* rhsC, double* T, double* phi,
-                        double* rate, StageTables* tab, double* rec, unsigned char* wet, double* face, void* partial,
+                        double* rate, const StageTables& tab, double* rec, unsigned char* wet, double* face, void* partial,
                         void* totals, unsigned long long* status, mp_stage_totals* out, cudaStream_t s);
 size_t raw_partial_bytes(size_t ncell);
 size_t raw_totals_bytes();
@@ -39,8 +40,7 @@ constexpr size_t kMaxCells = 32768;
 // nedges = 2*ncells + nx + ny <= 2.5*ncells + 2 for nx, ny >= 2.
 constexpr size_t kMaxEdges = kMaxCells * 5 / 2 + 2;
 constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
-constexpr size_t kTabOff = 0;
-constexpr size_t kRecOff = kTabOff + align256(sizeof(StageTables));
+constexpr size_t kRecOff = 0;
 constexpr size_t kWetOff = kRecOff + align256(18 * sizeof(double) * kMaxCells);
 constexpr size_t kFaceOff = kWetOff + align256(kMaxCells);
 constexpr size_t kPartOff = kFaceOff + align256(4 * sizeof(double) * kMaxEdges);
@@ -97,9 +97,7 @@ extern "C" mp_status mp_transport_rhs_noalloc(const mp_mesh_desc* mesh, const mp
     unsigned char* base = nullptr;
     MP_TRY(scratch_address(&base));
     cudaStream_t s = (cudaStream_t)stream;
-    StageTables* dtab = reinterpret_cast<StageTables*>(base + kTabOff);
-    MP_CUDA(cudaMemcpyAsync(dtab, &tab, sizeof(StageTables), cudaMemcpyHostToDevice, s));
-    return stage_rhs_raw(mesh->nx, mesh->ny, *opts, H, C, vs_n, ud_n, rhsH, rhsC, T, phi, rate, dtab,
+    return stage_rhs_raw(mesh->nx, mesh->ny, *opts, H, C, vs_n, ud_n, rhsH, rhsC, T, phi, rate, tab,
                          reinterpret_cast<double*>(base + kRecOff), base + kWetOff,
                          reinterpret_cast<double*>(base + kFaceOff), base + kPartOff, base + kTotOff,
                          reinterpret_cast<unsigned long long*>(base + kStatOff), totals, s);

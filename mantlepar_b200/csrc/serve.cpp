@@ -5,15 +5,21 @@
 // velocities, final time) -- what AdvancePhaseCoupled does for one
 // configuration (src/couple/evolve.cpp:513-519). Requests are queued on
 // submit; a loop thread owns a batch (batch.cu) and, before every step,
-// admits queued requests in arrival order while their device bytes fit the
-// budget. Every step advances all resident requests at once (one launch per
+// admits queued requests while their device bytes fit the budget and the
+// resident cells are below a target. The order is arrival (FIFO) or smallest
+// estimated work first: work ~ cells * t_final * (cells per unit length),
+// the step count of a CFL-limited solve scaling with the mesh resolution.
+// The resident target keeps enough cells on the GPU to fill it while short
+// requests pass long ones. Every step advances all resident requests at once (one launch per
 // stage kernel for all of them), so work that arrives while others are on the
 // GPU joins at the next step. A request leaves when it reaches its final time
 // or fails; its result is copied out and its memory freed for the queue.
 // State stays resident on the device between steps.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <deque>
 #include <map>
@@ -54,6 +60,7 @@ struct Request {
     std::vector<double> H, C, vs, ud;      // inputs (host copies)
     std::vector<double> oH, oC, oT, oP;    // results
     double t_final = 0;
+    double work = 0;                       // admission-order estimate
     Clock::time_point submitted, admitted, finished;
     int slot = -1;
     int status = 0;
@@ -77,6 +84,9 @@ struct mp_server {
     std::map<long long, std::shared_ptr<Request>> requests;
     std::vector<std::shared_ptr<Request>> active;
     long long next_id = 1;
+    int order = MP_SERVE_SMALLEST_WORK;
+    double resident_target = 4.0e6;        // cells; 0 = no limit
+    double resident_cells = 0;
     bool stop = false;
     mp_status fatal = MP_OK;
     std::string fatal_msg;
@@ -91,16 +101,23 @@ namespace {
 
 double seconds(Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double>(b - a).count(); }
 
-// Admit queued requests in arrival order while they fit the memory budget.
+// Admit queued requests (FIFO or smallest estimated work first) while they
+// fit the memory budget and the resident cells are below the target. A
+// request that does not fit waits; under FIFO nothing passes it.
 void admit(mp_server* s) {
     for (;;) {
         std::shared_ptr<Request> r;
         {
             std::lock_guard<std::mutex> g(s->m);
             if (s->queue.empty()) return;
-            r = s->queue.front();
+            if (s->resident_target > 0 && !s->active.empty() && s->resident_cells >= s->resident_target) return;
+            auto pick = s->queue.begin();
+            if (s->order == MP_SERVE_SMALLEST_WORK)
+                for (auto it = s->queue.begin(); it != s->queue.end(); ++it)
+                    if ((*it)->work < (*pick)->work) pick = it;
+            r = *pick;
             if (mp_batch_bytes_in_use(s->batch) + r->bytes > s->budget) return;
-            s->queue.pop_front();
+            s->queue.erase(pick);
         }
         int slot = -1;
         mp_status st = mp_batch_add(s->batch, &r->mesh, &slot);
@@ -116,6 +133,7 @@ void admit(mp_server* s) {
             continue;
         }
         r->slot = slot;
+        s->resident_cells += (double)r->cells;
         r->H.clear(); r->H.shrink_to_fit(); r->C.clear(); r->C.shrink_to_fit();
         r->vs.clear(); r->vs.shrink_to_fit(); r->ud.clear(); r->ud.shrink_to_fit();
         std::lock_guard<std::mutex> g(s->m);
@@ -136,6 +154,7 @@ void retire(mp_server* s) {
                            &r->accepted, &r->status);
         mp_batch_remove(s->batch, r->slot);
         std::lock_guard<std::mutex> g(s->m);
+        s->resident_cells -= (double)r->cells;
         r->finished = Clock::now();
         r->done = true;
         s->cv_done.notify_all();
@@ -234,6 +253,8 @@ extern "C" mp_status mp_serve_submit(mp_server* s, const mp_mesh_desc* mesh, con
     r->vs.assign(vs_n, vs_n + edges * 5);
     r->ud.assign(ud_n, ud_n + edges * 5);
     r->t_final = t_final;
+    const double res = std::max(mesh->nx / std::fabs(mesh->x1 - mesh->x0), mesh->ny / std::fabs(mesh->y1 - mesh->y0));
+    r->work = (double)r->cells * t_final * res;
     r->submitted = Clock::now();
     {
         std::lock_guard<std::mutex> g(s->m);
@@ -281,6 +302,19 @@ extern "C" mp_status mp_serve_wait(mp_server* s, long long id, double timeout_s,
         info->latency_s = seconds(r->submitted, r->finished);
         info->cells = (double)r->cells;
     }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_serve_set_policy(mp_server* s, int order, double resident_cells_target) {
+    if (!s) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (order != MP_SERVE_FIFO && order != MP_SERVE_SMALLEST_WORK) { mp::set_error("unknown admission order %d", order); return MP_ERR_ARG_OUTOFRANGE; }
+    if (!(resident_cells_target >= 0)) { mp::set_error("resident target must be >= 0"); return MP_ERR_ARG_OUTOFRANGE; }
+    {
+        std::lock_guard<std::mutex> g(s->m);
+        s->order = order;
+        s->resident_target = resident_cells_target;
+    }
+    s->cv_work.notify_all();
     return MP_OK;
 }
 

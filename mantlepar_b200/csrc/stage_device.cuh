@@ -13,6 +13,8 @@
 #ifndef MP_STAGE_DEVICE_CUH
 #define MP_STAGE_DEVICE_CUH
 
+#include <cmath>
+
 #include "phase_math.cuh"
 #include "tables.hpp"
 
@@ -29,9 +31,34 @@ struct StageTablesF {
     float line_c[kMaxLines];
 };
 
+// The tables a single-instance launch passes by value (__grid_constant__):
+// FP64 set and its FP32 copy.
+struct ParamTables {
+    StageHot d;
+    StageTablesF f;
+};
+
+inline void tables_to_float(const StageHot& t, StageTablesF& f) {
+    for (int a = 0; a < 9; ++a) for (int b = 0; b < 9; ++b) f.C9[a][b] = (float)t.C9[a][b];
+    for (int a = 0; a < 8; ++a) for (int b = 0; b < 8; ++b) f.S9[a][b] = (float)t.S9[a][b];
+    for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) f.C4[a][b] = (float)t.C4[a][b];
+    for (int k = 0; k < 4; ++k) for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) f.S4[k][a][b] = (float)t.S4[k][a][b];
+    f.X = (float)t.X; f.Y = (float)t.Y; f.epsA = (float)t.epsA; f.logEpsA2 = (float)(2.0 * std::log(t.epsA));
+    for (int q = 0; q < kNQ; ++q) { f.gx[q] = (float)t.gx[q]; f.gy[q] = (float)t.gy[q]; }
+    for (int l = 0; l < kMaxLines; ++l) f.line_c[l] = (float)t.line_c[l];
+}
+
+inline void make_param_tables(const StageTables& t, ParamTables& p) {
+    p.d = static_cast<const StageHot&>(t);
+    tables_to_float(t, p.f);
+}
+
 template <class R> struct Tab;
+// Tab pointing at the parameter-space copy (inside a kernel taking a
+// __grid_constant__ ParamTables).
+template <class R> __device__ __forceinline__ Tab<R> param_tab(const ParamTables& p);
 template <> struct Tab<double> {
-    const StageTables* t;
+    const StageHot* t;
     __device__ double C9(int c, int m) const { return t->C9[c][m]; }
     __device__ double S9(int r, int c) const { return t->S9[r][c]; }
     __device__ double C4(int c, int m) const { return t->C4[c][m]; }
@@ -44,7 +71,7 @@ template <> struct Tab<double> {
     __device__ double line_c(int l) const { return t->line_c[l]; }
 };
 template <> struct Tab<float> {
-    const StageTables* t;
+    const StageHot* t;
     const StageTablesF* f;
     __device__ float C9(int c, int m) const { return f->C9[c][m]; }
     __device__ float S9(int r, int c) const { return f->S9[r][c]; }
@@ -57,6 +84,9 @@ template <> struct Tab<float> {
     __device__ float gy(int q) const { return f->gy[q]; }
     __device__ float line_c(int l) const { return f->line_c[l]; }
 };
+
+template <> __device__ __forceinline__ Tab<double> param_tab<double>(const ParamTables& p) { return Tab<double>{&p.d}; }
+template <> __device__ __forceinline__ Tab<float> param_tab<float>(const ParamTables& p) { return Tab<float>{&p.d, &p.f}; }
 
 template <class R> __device__ __forceinline__ R eps_of();
 template <> __device__ __forceinline__ double eps_of<double>() { return 2.220446049250313e-16; }
@@ -159,7 +189,7 @@ __device__ __forceinline__ void weights(const R* sig, const bool* on, R eA, doub
 // PETSC_ERR_FP-class status when a smoothness form is negative beyond
 // roundoff or the weights cannot be normalised.
 template <class R>
-__device__ __forceinline__ int reconstruct(const Tab<R>& t, const StageTables& td, int ci, int cj,
+__device__ __forceinline__ int reconstruct(const Tab<R>& t, const StageHot& td, int ci, int cj,
                                            const double (&u)[3][3], double (&D)[9]) {
     double d[3][3];
 #pragma unroll

@@ -75,7 +75,7 @@ struct ReconArgs {
 // evaluated in R from D (FP64). For R = float the points attaining the
 // extremes are re-evaluated in FP64, so theta is formed from FP64 values.
 template <class R>
-__device__ __forceinline__ void scan_lines(const StageTables& t, const Tab<R>& tb, int l0, int l1, const double* Dd,
+__device__ __forceinline__ void scan_lines(const StageHot& t, const Tab<R>& tb, int l0, int l1, const double* Dd,
                                            double& mx, double& mn, bool& bad) {
     R D[9];
 #pragma unroll
@@ -130,7 +130,7 @@ __device__ __forceinline__ double theta_of(double m, double lo, double hi, doubl
 template <class R>
 __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics& ph, int i, int j) {
     if (i >= a.nx || j >= a.ny) return;
-    const StageTables& t = *a.tab.t;
+    const StageHot& t = *a.tab.t;
     const int nx = a.nx, ny = a.ny;
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
@@ -229,7 +229,7 @@ template <class R>
 __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const Physics& ph, long long cell) {
     const long long N = (long long)a.nx * a.ny;
     if (cell >= N) return;
-    const StageTables& t = *a.tab.t;
+    const StageHot& t = *a.tab.t;
     const double mH = __ldg(a.H + cell), mC = __ldg(a.C + cell);
     double DH[9], DC[9];
     load_rec(a.rec, (size_t)N, cell, DH, DC);
@@ -338,7 +338,7 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
     const long long nI = (long long)nx * (ny + 1);
     const long long nE = nI + (long long)(nx + 1) * ny;
     if (e >= nE) return;
-    const StageTables& t = *a.tab.t;
+    const StageHot& t = *a.tab.t;
     const size_t N = (size_t)nx * ny;
     bool boundary, reverse, horizontal;
     long long L, Rc = -1;
@@ -443,7 +443,7 @@ enum SumMode : int { SUM_STORE_L = 0, SUM_RK = 1 };
 
 struct SumArgs {
     int nx, ny;
-    const StageTables* tab;
+    double area;           // cell area
     const double* face;
     const double* H;       // stage state
     const double* C;
@@ -506,9 +506,8 @@ __device__ __forceinline__ Partial sum_cell(const SumArgs& a, long long cell) {
     const long long nE = nI + (long long)(nx + 1) * ny;
     Partial v{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
     if (cell < N) {
-        const StageTables& t = *a.tab;
         const int i = (int)(cell % nx), j = (int)(cell / nx);
-        const double A = t.area;
+        const double A = a.area;
         // Faces of this cell in the reference's id order: bottom, top, left, right,
         // each with the sign of its side (evolve.cpp:350-354).
         const long long eb = (long long)j * nx + i, et = (long long)(j + 1) * nx + i;

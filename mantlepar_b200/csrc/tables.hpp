@@ -1,5 +1,5 @@
-// Per-mesh tables of the uniform-mesh ML-WENO stage (host-built, read by
-// the kernels from global memory).
+// Per-mesh tables of the uniform-mesh ML-WENO stage (host-built; the
+// kernels read them as a kernel parameter or from global memory).
 //
 // On a uniform rectangular mesh every interior cell has the same stencil
 // geometry up to a translation, so the reference's per-cell setup
@@ -20,7 +20,10 @@ constexpr int kMaxPoints = 1024;   // limiter points over all 9 classes
 constexpr int kNQ = 5;             // Gauss points per edge / per cell axis
 constexpr int kMaxLines = 256;     // limiter point lines over all 9 classes
 
-struct StageTables {
+// The fields the stage kernels read. Small enough (~4.5 KB) to travel as a
+// kernel parameter, so that table coefficients become constant-bank operands
+// of the FP64 instructions instead of loads.
+struct StageHot {
     // 3x3 candidate (order 2): basis coefficients C9[cell][monomial]
     // (monomial m = j*3 + i for xi^i eta^j) and the reference-square
     // smoothness matrix on the differences to stencil cell 0 (rows/cols 1..8).
@@ -35,16 +38,11 @@ struct StageTables {
     double epsA;            // epsilon * cell area of the weight regulariser
     double area;            // cell area (1-point rule, as MeshInfo::CacheAreas)
     double len_h, len_v;    // lengths of AlongI (horizontal) / AlongJ edges
-    double gq[kNQ];         // Gauss points on [-1,1]
     double gw[kNQ];         // Gauss weights
     double cw[kNQ * kNQ];   // cell-quadrature weight / area, q = b*5 + a
-    // Limiter points of class c in [pt_off[c], pt_off[c+1]); pt_kind 1 marks
-    // a diffusion sample point (checked for admissibility in the stage).
-    int pt_off[10];
-    double pt_x[kMaxPoints];
-    double pt_y[kMaxPoints];
-    unsigned char pt_kind[kMaxPoints];
-    // The same points grouped into 5-point lines: apart from the cell centre,
+    double gx[kNQ];         // X * g_q
+    double gy[kNQ];         // Y * g_q
+    // Limiter points grouped into 5-point lines: apart from the cell centre,
     // every limiter point lies on a row eta = line_c with xi = X*g_q, or on a
     // column xi = line_c with eta = Y*g_q (q = 0..4). Class c owns lines
     // [line_off[c], line_off[c+1]); line_dir 0 = row, 1 = column; line_kind
@@ -53,8 +51,16 @@ struct StageTables {
     double line_c[kMaxLines];
     unsigned char line_dir[kMaxLines];
     unsigned char line_kind[kMaxLines];
-    double gx[kNQ];         // X * g_q
-    double gy[kNQ];         // Y * g_q
+};
+
+struct StageTables : StageHot {
+    double gq[kNQ];         // Gauss points on [-1,1]
+    // Limiter points of class c in [pt_off[c], pt_off[c+1]); pt_kind 1 marks
+    // a diffusion sample point (checked for admissibility in the stage).
+    int pt_off[10];
+    double pt_x[kMaxPoints];
+    double pt_y[kMaxPoints];
+    unsigned char pt_kind[kMaxPoints];
 };
 
 // Build the tables of an nx x ny uniform mesh on [x0,x1] x [y0,y1].

@@ -31,17 +31,26 @@ mp_status derive_checked(const mp_material& p, mp_derived& d);
 namespace {
 
 // Single-instance kernels: one thread per cell / edge.
+// The stage tables arrive by value as a __grid_constant__ parameter, so the
+// unrolled table coefficients are constant-bank operands.
 template <class R>
-__global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph) {
-    recon_cell(a, ph, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+__global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph, const __grid_constant__ ParamTables p) {
+    ReconArgs<R> b = a;
+    b.tab = param_tab<R>(p);
+    recon_cell(b, ph, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
 }
 template <class R>
-__global__ void __launch_bounds__(128) cellphase_kernel(CellPhaseArgs<R> a, Physics ph) {
-    cellphase_cell(a, ph, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+__global__ void __launch_bounds__(128) cellphase_kernel(CellPhaseArgs<R> a, Physics ph,
+                                                        const __grid_constant__ ParamTables p) {
+    CellPhaseArgs<R> b = a;
+    b.tab = param_tab<R>(p);
+    cellphase_cell(b, ph, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 template <class R>
-__global__ void __launch_bounds__(128) face_kernel(FaceArgs<R> a, Physics ph) {
-    face_edge(a, ph, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+__global__ void __launch_bounds__(128) face_kernel(FaceArgs<R> a, Physics ph, const __grid_constant__ ParamTables p) {
+    FaceArgs<R> b = a;
+    b.tab = param_tab<R>(p);
+    face_edge(b, ph, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 __global__ void __launch_bounds__(kRedBlock) sum_kernel(SumArgs a) {
     const Partial v = sum_cell(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);
@@ -98,7 +107,7 @@ struct mp_transport {
     int nx = 0, ny = 0;
     size_t N = 0, NE = 0;
     mp::StageTables host_tab;
-    mp::StageTables* tab = nullptr;
+    mp::ParamTables ptab;                   // kernel-parameter copy of the tables
     // State and stage buffers (device).
     double *H = nullptr, *C = nullptr;      // accepted state U^n
     double *S1H = nullptr, *S1C = nullptr;  // stage states
@@ -107,7 +116,6 @@ struct mp_transport {
     double *T = nullptr, *phi = nullptr;
     void* rec = nullptr;                    // 18 * N doubles (limited deviation polynomials)
     unsigned char* flags = nullptr;         // wet | exact-check flags per cell
-    mp::StageTablesF* tabF = nullptr;       // FP32 tables (mixed precision)
     bool mixed = false;
     double *vsn = nullptr, *udn = nullptr;
     double* face = nullptr;
@@ -134,15 +142,6 @@ struct mp_transport {
 namespace mp {
 namespace {
 
-void tables_to_float(const StageTables& t, StageTablesF& f) {
-    for (int a = 0; a < 9; ++a) for (int b = 0; b < 9; ++b) f.C9[a][b] = (float)t.C9[a][b];
-    for (int a = 0; a < 8; ++a) for (int b = 0; b < 8; ++b) f.S9[a][b] = (float)t.S9[a][b];
-    for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) f.C4[a][b] = (float)t.C4[a][b];
-    for (int k = 0; k < 4; ++k) for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) f.S4[k][a][b] = (float)t.S4[k][a][b];
-    f.X = (float)t.X; f.Y = (float)t.Y; f.epsA = (float)t.epsA; f.logEpsA2 = (float)(2.0 * std::log(t.epsA));
-    for (int q = 0; q < kNQ; ++q) { f.gx[q] = (float)t.gx[q]; f.gy[q] = (float)t.gy[q]; }
-    for (int l = 0; l < kMaxLines; ++l) f.line_c[l] = (float)t.line_c[l];
-}
 
 // Event pair around one kernel when profiling
 // (kind: 0 reconstruction/limiter, 1 cell phase, 2 face, 3 sum, 4 axpy/reductions).
@@ -177,7 +176,7 @@ void harvest(mp_transport* t) {
 
 void free_all(mp_transport* t) {
     for (cudaEvent_t e : t->ev_pool) cudaEventDestroy(e);
-    void* bufs[] = {t->tab, t->tabF, t->H, t->C, t->S1H, t->S1C, t->S2H, t->S2C, t->LH, t->LC, t->T, t->phi,
+    void* bufs[] = {t->H, t->C, t->S1H, t->S1C, t->S2H, t->S2C, t->LH, t->LC, t->T, t->phi,
                     t->rec, t->flags, t->vsn, t->udn, t->face, t->rate, t->partial, t->d_tot, t->d_status};
     for (void* b : bufs) if (b) cudaFree(b);
     if (t->h_tot) cudaFreeHost(t->h_tot);
@@ -200,7 +199,7 @@ mp_status check_status(mp_transport* t, const char* where) {
 
 // Launch the stage kernels of state (H, C) in arithmetic type R.
 template <class R>
-void launch_stage_kernels(int nx, int ny, Tab<R> tb, const Physics& ph, const double* H, const double* C, double* rec,
+void launch_stage_kernels(int nx, int ny, const ParamTables& pt, const Physics& ph, const double* H, const double* C, double* rec,
                           unsigned char* flags, double* T, double* phi, const double* vsn, const double* udn,
                           double* face, unsigned long long* status, double* theta, cudaStream_t s,
                           mp_transport* prof) {
@@ -208,17 +207,17 @@ void launch_stage_kernels(int nx, int ny, Tab<R> tb, const Physics& ph, const do
     const size_t NE = (size_t)nx * (ny + 1) + (size_t)(nx + 1) * ny;
     auto run = [&](int kind, auto&& f) { if (prof) timed(prof, kind, f); else f(); };
     {
-        ReconArgs<R> a{nx, ny, tb, H, C, rec, flags, status, theta};
+        ReconArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, status, theta};
         dim3 blk(32, 4), grd((nx + 31) / 32, (ny + 3) / 4);
-        run(0, [&] { recon_kernel<R><<<grd, blk, 0, s>>>(a, ph); });
+        run(0, [&] { recon_kernel<R><<<grd, blk, 0, s>>>(a, ph, pt); });
     }
     {
-        CellPhaseArgs<R> a{nx, ny, tb, H, C, rec, flags, T, phi, status};
-        run(1, [&] { cellphase_kernel<R><<<(unsigned)((N + 127) / 128), 128, 0, s>>>(a, ph); });
+        CellPhaseArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, T, phi, status};
+        run(1, [&] { cellphase_kernel<R><<<(unsigned)((N + 127) / 128), 128, 0, s>>>(a, ph, pt); });
     }
     {
-        FaceArgs<R> a{nx, ny, tb, H, C, rec, flags, vsn, udn, face, status};
-        run(2, [&] { face_kernel<R><<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(a, ph); });
+        FaceArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, vsn, udn, face, status};
+        run(2, [&] { face_kernel<R><<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(a, ph, pt); });
     }
 }
 
@@ -229,16 +228,15 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
     cudaStream_t s = t->stream;
     mp_transport* prof = t->profile ? t : nullptr;
     if (t->mixed) {
-        Tab<float> tb{t->tab, t->tabF};
-        launch_stage_kernels<float>(t->nx, t->ny, tb, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
+        launch_stage_kernels<float>(t->nx, t->ny, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
                                     t->vsn, t->udn, t->face, t->d_status, theta, s, prof);
     } else {
-        Tab<double> tb{t->tab};
-        launch_stage_kernels<double>(t->nx, t->ny, tb, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T,
+        launch_stage_kernels<double>(t->nx, t->ny, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T,
                                      t->phi, t->vsn, t->udn, t->face, t->d_status, theta, s, prof);
     }
     {
-        SumArgs a{t->nx, t->ny, t->tab, t->face, H, C, t->H, t->C, outH, outC, t->rate, mode, a0, a1, dt, t->partial};
+        SumArgs a{t->nx, t->ny, t->host_tab.area, t->face, H, C, t->H, t->C, outH, outC, t->rate, mode, a0, a1, dt,
+                  t->partial};
         timed(t, 3, [&] { sum_kernel<<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
     }
     timed(t, 4, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, t->sum_blocks, t->d_tot); });
@@ -415,16 +413,15 @@ extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_tran
     t->ph.lf_global = opts->lf_global; t->ph.lf_speed = opts->lf_global_speed;
     const int tb = build_stage_tables(t->nx, t->ny, mesh->x0, mesh->x1, mesh->y0, mesh->y1, t->host_tab);
     if (tb) { delete t; set_error("stencil table construction failed"); return (mp_status)tb; }
+    make_param_tables(t->host_tab, t->ptab);
     t->sum_blocks = (int)((t->N + kRedBlock - 1) / kRedBlock);
     const size_t N = t->N, NE = t->NE;
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes); };
-    alloc((void**)&t->tab, sizeof(StageTables));
     for (double** p : {&t->H, &t->C, &t->S1H, &t->S1C, &t->S2H, &t->S2C, &t->LH, &t->LC, &t->T, &t->phi, &t->rate})
         alloc((void**)p, N * sizeof(double));
     alloc((void**)&t->rec, (size_t)kRec * N * sizeof(double));
     alloc((void**)&t->flags, N);
-    if (t->mixed) alloc((void**)&t->tabF, sizeof(StageTablesF));
     alloc((void**)&t->vsn, NE * kNQ * sizeof(double));
     alloc((void**)&t->udn, NE * kNQ * sizeof(double));
     alloc((void**)&t->face, 4 * NE * sizeof(double));
@@ -433,12 +430,6 @@ extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_tran
     alloc((void**)&t->d_status, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&t->h_tot, sizeof(Totals));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&t->h_status, sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(t->tab, &t->host_tab, sizeof(StageTables), cudaMemcpyHostToDevice, t->stream);
-    StageTablesF tf;
-    if (t->mixed) {
-        tables_to_float(t->host_tab, tf);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(t->tabF, &tf, sizeof(StageTablesF), cudaMemcpyHostToDevice, t->stream);
-    }
     if (e == cudaSuccess) e = cudaMemsetAsync(t->vsn, 0, NE * kNQ * sizeof(double), t->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(t->udn, 0, NE * kNQ * sizeof(double), t->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
@@ -607,12 +598,12 @@ size_t raw_partial_bytes(size_t ncell) { return ((ncell + kRedBlock - 1) / kRedB
 size_t raw_totals_bytes() { return sizeof(Totals); }
 
 // One stage evaluation L(U) (STORE_L mode) on buffers the caller provides:
-// tab (device StageTables), rec (18*ncell doubles), wet (ncell bytes), face
+// tab (host StageTables, passed to the kernels by value), rec (18*ncell doubles), wet (ncell bytes), face
 // (4*nedge doubles), partial (raw_partial_bytes), totals (raw_totals_bytes),
 // status (one unsigned long long). Used by entry points that cannot allocate.
 mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double* H, const double* C,
                         const double* vsn, const double* udn, double* rhsH, double* rhsC, double* T, double* phi,
-                        double* rate, StageTables* tab, double* rec, unsigned char* wet, double* face, void* partial,
+                        double* rate, const StageTables& tab, double* rec, unsigned char* wet, double* face, void* partial,
                         void* totals, unsigned long long* status, mp_stage_totals* out, cudaStream_t s) {
     mp_derived der;
     MP_TRY(derive_checked(o.material, der));
@@ -629,10 +620,11 @@ mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double
     Totals* tot = static_cast<Totals*>(totals);
     MP_CUDA(cudaMemsetAsync(status, 0xff, sizeof(unsigned long long), s));
     (void)NE;
-    launch_stage_kernels<double>(nx, ny, Tab<double>{tab}, ph, H, C, rec, wet, T, phi, vsn, udn, face, status, nullptr,
-                                 s, nullptr);
+    ParamTables pt;
+    make_param_tables(tab, pt);
+    launch_stage_kernels<double>(nx, ny, pt, ph, H, C, rec, wet, T, phi, vsn, udn, face, status, nullptr, s, nullptr);
     {
-        SumArgs a{nx, ny, tab, face, H, C, H, C, rhsH, rhsC, rate, SUM_STORE_L, 0.0, 0.0, 0.0, part};
+        SumArgs a{nx, ny, tab.area, face, H, C, H, C, rhsH, rhsC, rate, SUM_STORE_L, 0.0, 0.0, 0.0, part};
         sum_kernel<<<sum_blocks, kRedBlock, 0, s>>>(a);
     }
     reduce_kernel<<<1, 1024, 0, s>>>(part, sum_blocks, tot);

@@ -83,6 +83,11 @@ class Server:
                                             Cc.ctypes.data, T.ctypes.data, phi.ctypes.data, C.byref(info)))
         return dict(H=H, C=Cc, T=T, phi=phi, **{k: getattr(info, k) for k, _ in _capi.RequestInfo._fields_})
 
+    FIFO, SMALLEST_WORK = 0, 1
+
+    def set_policy(self, order: int, resident_cells_target: float):
+        _capi.check(self._lib.mp_serve_set_policy(self._h, int(order), float(resident_cells_target)))
+
     def stats(self):
         cu, busy, steps, res, q = C.c_double(0), C.c_double(0), C.c_longlong(0), C.c_int(0), C.c_int(0)
         _capi.check(self._lib.mp_serve_stats(self._h, C.byref(cu), C.byref(busy), C.byref(steps), C.byref(res), C.byref(q)))

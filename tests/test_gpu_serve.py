@@ -23,7 +23,8 @@ def alone(w, tf, cfg):
     return b.get_state(0)
 
 
-def test_served_results_equal_solo_runs(cuda_lib):
+@pytest.mark.parametrize("order", [0, 1], ids=["fifo", "smallest_work"])
+def test_served_results_equal_solo_runs(cuda_lib, order):
     from mantlepar_b200.batch import Batch
     from mantlepar_b200.serve import Server
     from mantlepar_b200.transport import TransportConfig
@@ -34,12 +35,17 @@ def test_served_results_equal_solo_runs(cuda_lib):
     # A budget for about two of the larger requests at once forces queueing.
     budget = 2 * Batch.instance_bytes(sy.Workload(nx=80, ny=80)) + Batch.instance_bytes(sy.Workload(nx=20, ny=20))
     srv = Server(cfg, memory_budget=budget)
+    # A resident target below the total forces the order to matter.
+    srv.set_policy(order, 6000)
     ids = [srv.submit(w, tf) for w, tf in reqs]
     got = [srv.wait(i, timeout=120.0) for i in ids]
     st = srv.stats()
     srv.close()
     assert st["cell_updates"] > 0 and st["steps"] > 0
     assert any(g["queue_s"] > 0 for g in got)
+    if order == Server.SMALLEST_WORK:
+        work = [w.cells * tf * max(w.nx, w.ny) for w, tf in reqs]
+        assert got[int(np.argmin(work))]["latency_s"] <= got[int(np.argmax(work))]["latency_s"]
     for (w, tf), g in zip(reqs, got):
         assert g["status"] == 0 and g["time"] == tf
         ref = alone(w, tf, cfg)
@@ -55,4 +61,8 @@ def test_oversized_request_is_refused(cuda_lib):
     with pytest.raises(MPError) as err:
         srv.submit(sy.Workload(nx=200, ny=200), 0.01)
     assert err.value.code == 111
+    with pytest.raises(MPError):
+        srv.set_policy(7, 0)
+    with pytest.raises(MPError):
+        srv.set_policy(0, -1)
     srv.close()
