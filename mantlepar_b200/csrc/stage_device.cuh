@@ -26,6 +26,8 @@ struct StageTablesF {
     float S9[8][8];
     float C4[4][4];
     float S4[4][3][3];
+    float SF9[36];
+    float SF4[4][6];
     float X, Y, epsA, logEpsA2;
     float gx[kNQ], gy[kNQ];
     float line_c[kMaxLines];
@@ -43,6 +45,8 @@ inline void tables_to_float(const StageHot& t, StageTablesF& f) {
     for (int a = 0; a < 8; ++a) for (int b = 0; b < 8; ++b) f.S9[a][b] = (float)t.S9[a][b];
     for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) f.C4[a][b] = (float)t.C4[a][b];
     for (int k = 0; k < 4; ++k) for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) f.S4[k][a][b] = (float)t.S4[k][a][b];
+    for (int k = 0; k < 36; ++k) f.SF9[k] = (float)t.SF9[k];
+    for (int k = 0; k < 4; ++k) for (int a = 0; a < 6; ++a) f.SF4[k][a] = (float)t.SF4[k][a];
     f.X = (float)t.X; f.Y = (float)t.Y; f.epsA = (float)t.epsA; f.logEpsA2 = (float)(2.0 * std::log(t.epsA));
     for (int q = 0; q < kNQ; ++q) { f.gx[q] = (float)t.gx[q]; f.gy[q] = (float)t.gy[q]; }
     for (int l = 0; l < kMaxLines; ++l) f.line_c[l] = (float)t.line_c[l];
@@ -63,6 +67,8 @@ template <> struct Tab<double> {
     __device__ double S9(int r, int c) const { return t->S9[r][c]; }
     __device__ double C4(int c, int m) const { return t->C4[c][m]; }
     __device__ double S4(int k, int r, int c) const { return t->S4[k][r][c]; }
+    __device__ double SF9(int k) const { return t->SF9[k]; }
+    __device__ double SF4(int p, int k) const { return t->SF4[p][k]; }
     __device__ double X() const { return t->X; }
     __device__ double Y() const { return t->Y; }
     __device__ double epsA() const { return t->epsA; }
@@ -77,6 +83,8 @@ template <> struct Tab<float> {
     __device__ float S9(int r, int c) const { return f->S9[r][c]; }
     __device__ float C4(int c, int m) const { return f->C4[c][m]; }
     __device__ float S4(int k, int r, int c) const { return f->S4[k][r][c]; }
+    __device__ float SF9(int k) const { return f->SF9[k]; }
+    __device__ float SF4(int p, int k) const { return f->SF4[p][k]; }
     __device__ float X() const { return f->X; }
     __device__ float Y() const { return f->Y; }
     __device__ float epsA() const { return f->epsA; }
@@ -110,23 +118,36 @@ __device__ __forceinline__ void q2_col(const R* D, R x, R& b0, R& b1, R& b2) {
 template <class R>
 __device__ __forceinline__ R quad(R c0, R c1, R c2, R s) { return c0 + s * (c1 + s * c2); }
 
-// sigma = d^T S d on differences to stencil cell 0 with the reference's
-// roundoff clip (tensorstencilpoly.cpp:424-430). Returns -1 on failure.
-template <class R, int N, class G>
-__device__ __forceinline__ R smoothness(G&& S, const R* diff) {
-    R sum = 0, mag = 0;
+// sigma = d^T S d on differences to stencil cell 0, formed as one FMA chain
+// per row of the folded upper triangle SF. A negative or non-finite chain
+// (roundoff at sigma ~ 0, or bad data) is decided as the reference does:
+// the term-by-term sum with its roundoff clip (tensorstencilpoly.cpp:424-430).
+// Returns -1 on failure.
+template <class R, int N, class GF, class G>
+__device__ __forceinline__ R smoothness(GF&& SF, G&& S, const R* diff) {
+    R sum = 0;
+    int k = 0;
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+        R tr = SF(k++) * diff[r];
+#pragma unroll
+        for (int c = r + 1; c < N; ++c) tr = fma(SF(k++), diff[c], tr);
+        sum = fma(diff[r], tr, sum);
+    }
+    if (sum >= R(0) && sum < R(INFINITY)) return sum;
+    R exact = 0, mag = 0;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
         const R sr = S(r, r) * diff[r] * diff[r];
-        sum += sr; mag += fabs(sr);
+        exact += sr; mag += fabs(sr);
 #pragma unroll
         for (int c = r + 1; c < N; ++c) {
             const R term = R(2) * (S(r, c) * diff[r]) * diff[c];
-            sum += term; mag += fabs(term);
+            exact += term; mag += fabs(term);
         }
     }
-    if (!isfinite(sum) || sum < -R(64) * eps_of<R>() * mag) return R(-1);
-    return sum > R(0) ? sum : R(0);
+    if (!isfinite(exact) || exact < -R(64) * eps_of<R>() * mag) return R(-1);
+    return exact > R(0) ? exact : R(0);
 }
 
 // Nonlinear weights alpha_k = (sigma_k + eps*A)^-(s*r_k + eta(r_k)): 7 for
@@ -139,11 +160,32 @@ __device__ __forceinline__ R smoothness(G&& S, const R* diff) {
 template <class R>
 __device__ __forceinline__ void weights(const R* sig, const bool* on, R eA, double* w) {
     if constexpr (sizeof(R) == 8) {
+        // The five reciprocals 1/(sigma_k + epsA) from one division: prefix
+        // and suffix products of s_k = sigma_k + epsA (s_k >= epsA > 0).
+        double sk[5], pre[5], suf[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) sk[k] = sig[k] + eA;
+        pre[0] = 1.0;
+#pragma unroll
+        for (int k = 1; k < 5; ++k) pre[k] = pre[k - 1] * sk[k - 1];
+        suf[4] = 1.0;
+#pragma unroll
+        for (int k = 3; k >= 0; --k) suf[k] = suf[k + 1] * sk[k + 1];
+        const double P = pre[4] * sk[4];
+        double inv_s[5];
+        if (P > 1e-290 && P < 1e290) {
+            const double invP = 1.0 / P;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) inv_s[k] = (pre[k] * suf[k]) * invP;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 5; ++k) inv_s[k] = 1.0 / sk[k];
+        }
         double alpha[5];
         const double scale = on[0] ? eA * eA : 1.0;
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-            const double r = eA / (sig[k] + eA);
+            const double r = eA * inv_s[k];
             const double r2 = r * r;
             alpha[k] = !on[k] ? 0.0 : (k == 0 ? r2 * r2 * r2 * r : scale * (r2 * r2 * r));
         }
@@ -198,6 +240,7 @@ __device__ __forceinline__ int reconstruct(const Tab<R>& t, const StageHot& td, 
         for (int b = 0; b < 3; ++b) d[a][b] = u[a][b] - u[1][1];
     // Candidate order: 3x3 at (-1,-1); 2x2 at (0,-1), (0,0), (-1,-1), (-1,0).
     const int offi[4] = {0, 0, -1, -1}, offj[4] = {-1, 0, -1, 0};
+    static_assert(sizeof(R) == 4 || sizeof(R) == 8, "R is float or double");
     bool on[5];
     on[0] = (ci == 1 && cj == 1);
 #pragma unroll
@@ -211,7 +254,7 @@ __device__ __forceinline__ int reconstruct(const Tab<R>& t, const StageHot& td, 
         R diff[8];
 #pragma unroll
         for (int c = 1; c < 9; ++c) diff[c - 1] = (R)(d[c / 3][c % 3] - d[0][0]);
-        sig[0] = smoothness<R, 8>([&](int r, int c) { return t.S9(r, c); }, diff);
+        sig[0] = smoothness<R, 8>([&](int k) { return t.SF9(k); }, [&](int r, int c) { return t.S9(r, c); }, diff);
         if (sig[0] < R(0)) st = MP_ERR_FP;
     } else {
         sig[0] = 0;
@@ -225,7 +268,8 @@ __device__ __forceinline__ int reconstruct(const Tab<R>& t, const StageHot& td, 
 #pragma unroll
         for (int c = 1; c < 4; ++c) diff[c - 1] = (R)(d[1 + oj + c / 2][1 + oi + c % 2] - a0);
         const int tpos = (-oj) * 2 + (-oi);
-        sig[k + 1] = smoothness<R, 3>([&](int r, int c) { return t.S4(tpos, r, c); }, diff);
+        sig[k + 1] = smoothness<R, 3>([&](int q) { return t.SF4(tpos, q); }, [&](int r, int c) { return t.S4(tpos, r, c); },
+                                      diff);
         if (sig[k + 1] < R(0)) st = MP_ERR_FP;
     }
     double w[5];

@@ -71,33 +71,72 @@ struct ReconArgs {
     double* theta;         // optional (2 * ncell): limiter factors for H, C
 };
 
-// Max/min of the deviation polynomial over the class's limiter points,
-// evaluated in R from D (FP64). For R = float the points attaining the
+// Max/min of the deviation polynomial over the class's limiter points by
+// exact per-point evaluation in FP64, with the finiteness check of every
+// value. Used when the coefficients are too large for the fast scan's bound.
+__device__ __noinline__ void scan_lines_exact(const StageHot& t, int l0, int l1, const double* D, double& mx,
+                                              double& mn, bool& bad) {
+    double rmx = D[0], rmn = D[0];
+    bad = bad || !isfinite(D[0]);
+    for (int l = l0; l < l1; ++l) {
+        double a0, a1, a2;
+        const bool row = t.line_dir[l] == 0;
+        if (row) q2_row(D, t.line_c[l], a0, a1, a2);
+        else q2_col(D, t.line_c[l], a0, a1, a2);
+        for (int q = 0; q < kNQ; ++q) {
+            const double v = quad(a0, a1, a2, row ? t.gx[q] : t.gy[q]);
+            rmx = fmax(rmx, v); rmn = fmin(rmn, v);
+            bad = bad || !isfinite(v);
+        }
+    }
+    mx = rmx; mn = rmn;
+}
+
+// Max/min of the deviation polynomial over the class's limiter points. Each
+// line holds its centre (s = 0) and the symmetric Gauss pairs s = +-s_k
+// (g = 0, +-g1, +-g2), so along a line v(+-s_k) = (a0 + a2 s_k^2) +- a1 s_k
+// and the larger of a pair is e_k + |a1| s_k: three candidates per line for
+// the maximum and three for the minimum. With every |D_m| below scan_guard
+// no value can overflow, so no per-point finiteness test is needed;
+// otherwise the exact scan runs. For R = float the candidates attaining the
 // extremes are re-evaluated in FP64, so theta is formed from FP64 values.
 template <class R>
 __device__ __forceinline__ void scan_lines(const StageHot& t, const Tab<R>& tb, int l0, int l1, const double* Dd,
                                            double& mx, double& mn, bool& bad) {
+    bool small = true;
+#pragma unroll
+    for (int m = 0; m < 9; ++m) small = small && fabs(Dd[m]) < t.scan_guard;
+    if (!small) { scan_lines_exact(t, l0, l1, Dd, mx, mn, bad); return; }
     R D[9];
 #pragma unroll
     for (int m = 0; m < 9; ++m) D[m] = (R)Dd[m];
+    const R sx1 = tb.gx(3), sx2 = tb.gx(4), sy1 = tb.gy(3), sy2 = tb.gy(4);
+    const R qx1 = sx1 * sx1, qx2 = sx2 * sx2, qy1 = sy1 * sy1, qy2 = sy2 * sy2;
     R rmx = D[0], rmn = D[0];        // cell centre
-    int amx = -1, amn = -1;          // extreme point as line*8 + q (-1 = centre)
+    int amx = -1, amn = -1;          // FP32: extreme point as line*8 + q (-1 = centre)
     for (int l = l0; l < l1; ++l) {
         const R c = tb.line_c(l);
         R a0, a1, a2;
         const bool row = t.line_dir[l] == 0;
         if (row) q2_row(D, c, a0, a1, a2);
         else q2_col(D, c, a0, a1, a2);
-#pragma unroll
-        for (int q = 0; q < kNQ; ++q) {
-            const R v = quad(a0, a1, a2, row ? tb.gx(q) : tb.gy(q));
-            if constexpr (sizeof(R) == 8) {
-                rmx = fmax(rmx, v); rmn = fmin(rmn, v);
-            } else {
-                if (v > rmx) { rmx = v; amx = l * 8 + q; }
-                if (v < rmn) { rmn = v; amn = l * 8 + q; }
-            }
-            bad = bad || !isfinite(v);
+        const R s1 = row ? sx1 : sy1, s2 = row ? sx2 : sy2;
+        const R e1 = fma(a2, row ? qx1 : qy1, a0), e2 = fma(a2, row ? qx2 : qy2, a0);
+        const R b = fabs(a1);
+        const R d1 = b * s1, d2 = b * s2;
+        const R p1 = e1 + d1, p2 = e2 + d2, m1 = e1 - d1, m2 = e2 - d2;
+        if constexpr (sizeof(R) == 8) {
+            rmx = a0 > rmx ? a0 : rmx; rmx = p1 > rmx ? p1 : rmx; rmx = p2 > rmx ? p2 : rmx;
+            rmn = a0 < rmn ? a0 : rmn; rmn = m1 < rmn ? m1 : rmn; rmn = m2 < rmn ? m2 : rmn;
+        } else {
+            // Gauss index of +s_k is 2 + k, of -s_k is 2 - k.
+            const bool up = a1 >= R(0);
+            if (a0 > rmx) { rmx = a0; amx = l * 8 + 2; }
+            if (p1 > rmx) { rmx = p1; amx = l * 8 + (up ? 3 : 1); }
+            if (p2 > rmx) { rmx = p2; amx = l * 8 + (up ? 4 : 0); }
+            if (a0 < rmn) { rmn = a0; amn = l * 8 + 2; }
+            if (m1 < rmn) { rmn = m1; amn = l * 8 + (up ? 1 : 3); }
+            if (m2 < rmn) { rmn = m2; amn = l * 8 + (up ? 0 : 4); }
         }
     }
     if constexpr (sizeof(R) == 8) {

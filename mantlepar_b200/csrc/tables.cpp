@@ -255,8 +255,19 @@ int build_stage_tables(int nx, int ny, double x0, double x1, double y0, double y
         if (tpos == 0) for (int r = 0; r < 4; ++r) for (int m = 0; m < 4; ++m) t.C4[r][m] = small.coef[(size_t)r * 4 + m];
         for (int r = 1; r < 4; ++r) for (int s = 1; s < 4; ++s) t.S4[tpos][r - 1][s - 1] = small.target[(size_t)r * 4 + s];
     }
+    {
+        int k = 0;
+        for (int r = 0; r < 8; ++r)
+            for (int c = r; c < 8; ++c) t.SF9[k++] = c == r ? t.S9[r][r] : 2.0 * t.S9[r][c];
+        for (int tpos = 0; tpos < 4; ++tpos) {
+            k = 0;
+            for (int r = 0; r < 3; ++r)
+                for (int c = r; c < 3; ++c) t.SF4[tpos][k++] = c == r ? t.S4[tpos][r][r] : 2.0 * t.S4[tpos][r][c];
+        }
+    }
     t.X = 0.5 * dx / h;
     t.Y = 0.5 * dy / h;
+    t.scan_guard = 1e36 / (16.0 * std::max(1.0, t.X * t.X) * std::max(1.0, t.Y * t.Y));
     t.epsA = 1e-2 * area;
     t.area = area;
     t.len_h = dx;

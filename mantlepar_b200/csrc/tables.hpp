@@ -34,6 +34,11 @@ struct StageHot {
     // position t = tj*2 + ti (rows/cols 1..3 of the difference form).
     double C4[4][4];
     double S4[4][3][3];
+    // The same forms folded to their upper triangles, row by row: entry
+    // (r, r) is S_rr, entry (r, c > r) is 2 S_rc, so d^T S d is one FMA
+    // chain per row.
+    double SF9[36];
+    double SF4[4][6];
     double X, Y;            // half cell extents in the normalised frame
     double epsA;            // epsilon * cell area of the weight regulariser
     double area;            // cell area (1-point rule, as MeshInfo::CacheAreas)
@@ -42,6 +47,10 @@ struct StageHot {
     double cw[kNQ * kNQ];   // cell-quadrature weight / area, q = b*5 + a
     double gx[kNQ];         // X * g_q
     double gy[kNQ];         // Y * g_q
+    // With every deviation coefficient below this magnitude, every limiter
+    // value is finite (in FP32 too): 1e36 / (16 max(1, X^2) max(1, Y^2)),
+    // the points lying within |xi| <= X, |eta| <= Y.
+    double scan_guard;
     // Limiter points grouped into 5-point lines: apart from the cell centre,
     // every limiter point lies on a row eta = line_c with xi = X*g_q, or on a
     // column xi = line_c with eta = Y*g_q (q = 0..4). Class c owns lines
