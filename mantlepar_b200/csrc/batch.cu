@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kRedBlock) batch_sum_kernel(const InstArgs<R>*
     const Work w = work[blockIdx.x];
     if (!active[w.inst]) return;
     const SumArgs& a = args[w.inst].sum;
-    const Partial v = sum_cell(a, (long long)w.a + threadIdx.x);
+    const Partial v = sum_cells(a, w.a);
     block_reduce_write(v, a.partial + w.part);
 }
 
@@ -100,17 +100,7 @@ __global__ void __launch_bounds__(kRedBlock) batch_axpy_kernel(const AxpyArgs* a
     const Work w = work[blockIdx.x];
     if (!active[w.inst]) return;
     const AxpyArgs& a = args[w.inst];
-    const long long k = (long long)w.a + threadIdx.x;
-    Partial v{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
-    if (k < a.n) {
-        const double dt = *a.dtp;
-        const double h = __dadd_rn(a.H0[k], __dmul_rn(dt, a.LH[k]));
-        const double c = __dadd_rn(a.C0[k], __dmul_rn(dt, a.LC[k]));
-        a.H1[k] = h; a.C1[k] = c;
-        v.HI = h * a.area; v.CI = c * a.area;
-        v.Hmin = h; v.Cmin = c; v.Cmax = c;
-        v.nonfinite = (isfinite(h) && isfinite(c)) ? 0.0 : 1.0;
-    }
+    const Partial v = axpy_cells(a.n, a.H0, a.C0, a.LH, a.LC, *a.dtp, a.area, a.H1, a.C1, w.a);
     block_reduce_write(v, a.partial + w.part);
 }
 
@@ -312,7 +302,7 @@ mp_status rebuild_args(mp_batch* b, int slots) {
         Tab<R> tb;
         tb.t = in.tab;
         if constexpr (sizeof(R) == 4) tb.f = in.tabF;
-        const int nsum = (int)((in.N + kRedBlock - 1) / kRedBlock);
+        const int nsum = (int)((in.N + kSumCells - 1) / kSumCells);
         part_off[i] = parts; part_cnt[i] = nsum;
         Partial* pp = nullptr;  // fixed below once the partial array exists
         (void)pp;
@@ -338,7 +328,7 @@ mp_status rebuild_args(mp_batch* b, int slots) {
             for (int tx = 0; tx < in.nx; tx += tu.bx * tu.cpt) wr.push_back(Work{i, tx, ty, 0});
         for (size_t c = 0; c < in.N; c += 128) wp.push_back(Work{i, (int)c, 0, 0});
         for (size_t e = 0; e < in.NE; e += 128) wf.push_back(Work{i, (int)e, 0, 0});
-        for (int s = 0; s < nsum; ++s) ws.push_back(Work{i, s * kRedBlock, 0, s});
+        for (int s = 0; s < nsum; ++s) ws.push_back(Work{i, s * kSumCells, 0, s});
         parts += nsum;
     }
     (void)parts;
@@ -393,7 +383,7 @@ mp_status rebuild(mp_batch* b) {
         b->slots = cap;
     }
     int parts = 0;
-    for (const MPInstance& in : b->inst) if (in.used) parts += (int)((in.N + kRedBlock - 1) / kRedBlock);
+    for (const MPInstance& in : b->inst) if (in.used) parts += (int)((in.N + kSumCells - 1) / kSumCells);
     if (parts > b->partial_cap) {
         if (b->d_partial) cudaFreeAsync(b->d_partial, s);
         MP_CUDA(cudaMallocAsync((void**)&b->d_partial, std::max(parts, 1) * sizeof(Partial), s));
@@ -661,6 +651,7 @@ extern "C" mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, cons
     b->inst.resize(count);
     for (int i = 0; i < count; ++i) {
         if (meshes[i].nx < 2 || meshes[i].ny < 2) { set_error("instance %d: at least 2x2 cells", i); mp_batch_destroy(b); return MP_ERR_ARG_SIZ; }
+        if (mesh_too_large(meshes[i].nx, meshes[i].ny)) { set_error("instance %d: mesh has 2^31 edges or more", i); mp_batch_destroy(b); return MP_ERR_ARG_SIZ; }
         const mp_status s = alloc_instance(b, b->inst[i], meshes[i]);
         if (s != MP_OK) { mp_batch_destroy(b); return s; }
     }
@@ -696,6 +687,7 @@ static mp_status batch_slot(mp_batch* b, int i, MPInstance** out) {
 extern "C" mp_status mp_batch_add(mp_batch* b, const mp_mesh_desc* mesh, int* instance) {
     if (!b || !mesh || !instance) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (mesh->nx < 2 || mesh->ny < 2) { mp::set_error("Transport requires at least 2x2 cells"); return MP_ERR_ARG_SIZ; }
+    if (mp::mesh_too_large(mesh->nx, mesh->ny)) { mp::set_error("mesh has 2^31 edges or more"); return MP_ERR_ARG_SIZ; }
     int slot = -1;
     for (int i = 0; i < (int)b->inst.size(); ++i) if (!b->inst[i].used) { slot = i; break; }
     if (slot < 0) { slot = (int)b->inst.size(); b->inst.emplace_back(); }

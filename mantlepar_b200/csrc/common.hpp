@@ -25,6 +25,13 @@ inline mp_status cuda_status(cudaError_t e, const char* what) {
     return e == cudaErrorMemoryAllocation ? MP_ERR_NOMEM : MP_ERR_CUDA;
 }
 
+// Kernels index cells and edges of one mesh with 32-bit unsigned arithmetic:
+// meshes with 2^31 edges or more are rejected.
+inline bool mesh_too_large(int nx, int ny) {
+    const long long edges = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
+    return edges >= (1LL << 31);
+}
+
 }  // namespace mp
 
 #define MP_CUDA(call)                                                        \

@@ -246,12 +246,22 @@ MP_HD StageConst stage_const(const PhaseConst& k) {
     return c;
 }
 
-// Phase evaluation for the transport stage (T, phil, cl, cs, dT/dC): the
-// same regions and closed forms as phase_eval, with the divisions by Xe and
-// LD replaced by precomputed reciprocals and one shared reciprocal for
-// 1/phil and 1/disc in the solid+liquid region. Agrees with phase_eval to a
-// few ulp; region selection uses interval ends formed the same way.
-MP_HD int phase_stage(const StageConst& k, double H, double C, double Tep, PhaseLean& s) {
+// Phase evaluation for the transport stage: the same regions and closed
+// forms as phase_eval, with the divisions by Xe and LD replaced by
+// precomputed reciprocals. kFull = false evaluates T and phil only (the cell
+// quadrature), still applying every admissibility check of the full
+// evaluation; kFull = true adds cl, cs and dT/dC (the face points).
+//  - solid + liquid: T = Tmp - (disc - a)/2 is the reference's
+//    Tmp - r/melt (a >= 0) and H - LD*melt (a < 0) on the quadratic
+//    melt^2 LD - a melt - r = 0; its rounding error is bounded by that of
+//    disc, far below T >= Tep. 1/g (g = disc - a) and 1/(r disc) come from
+//    one division where that product is in range.
+//  - two solids: (1 - C) + C rounds to exactly 1 for 0 <= C <= 1, so
+//    cs = phi2/solid = C.
+// Agrees with phase_eval to a few ulp; region selection uses interval ends
+// formed the same way.
+template <bool kFull>
+MP_HD int phase_stage_t(const StageConst& k, double H, double C, double Tep, PhaseLean& s) {
     if (!(C >= 0.0 && C <= k.Xe) || !mp_isfinite(H)) return PH_INVALID;
     int st = PH_OK;
     const double Tmp = Tep + 1.0;
@@ -259,8 +269,8 @@ MP_HD int phase_stage(const StageConst& k, double H, double C, double Tep, Phase
     const double Hliq = C == 0.0 ? Tmp + k.LD : (Tep + (1.0 - r)) + k.LD;
     const double Heut = Tep + k.LD * r;
     double phi1 = 0.0, phi2 = 0.0;
-    s.phil = 0.0; s.cl = 0.0; s.dTdC = 0.0;
-    bool liquid_region = false;
+    s.phil = 0.0; s.cl = 0.0; s.cs = 0.0; s.dTdC = 0.0;
+    bool liquid_region = false, general_cs = false;
     if (C == 0.0) {
         if (H <= Tmp) { phi1 = 1.0; s.T = H; }
         else if (H < Hliq) {
@@ -270,6 +280,10 @@ MP_HD int phase_stage(const StageConst& k, double H, double C, double Tep, Phase
         } else { s.phil = 1.0; s.T = H - k.LD; liquid_region = true; }
     } else if (H <= Tep) {
         phi1 = 1.0 - C; phi2 = C; s.T = H;
+        if (kFull) {
+            if (phi1 + phi2 == 1.0) s.cs = C;
+            else general_cs = true;
+        }
     } else if (H >= Hliq) {
         s.phil = 1.0; s.cl = C; s.T = H - k.LD; liquid_region = true;
     } else if (H <= Heut) {
@@ -280,26 +294,61 @@ MP_HD int phase_stage(const StageConst& k, double H, double C, double Tep, Phase
         phi1 = clip_fraction(1.0 - melt - second, st);
         s.cl = k.Xe;
         s.T = Tep;
+        general_cs = kFull;
     } else {
         const double a = H - Tmp;
         const double disc = fabs(a) < 1e150 ? sqrt(a * a + k.fourLD * r) : hypot(a, 2.0 * sqrt(k.LD * r));
-        const double melt = a >= 0.0 ? (a + disc) * k.halfInvLD : 2.0 * r / (disc - a);
-        const double inv = 1.0 / (melt * disc);
-        const double inv_melt = disc * inv, inv_disc = melt * inv;
+        double melt;
+        if (kFull) {
+            double inv_melt, inv_disc;
+            if (a >= 0.0) {
+                melt = (a + disc) * k.halfInvLD;
+                const double inv = 1.0 / (melt * disc);
+                inv_melt = disc * inv; inv_disc = melt * inv;
+            } else {
+                const double g = disc - a, rd = r * disc, p = g * rd;
+                if (p > 1e-290 && p < 1e290) {
+                    const double x = 1.0 / p;
+                    const double inv_rd = g * x;
+                    melt = 2.0 * r * (rd * x);
+                    inv_melt = 0.5 * g * (disc * inv_rd);
+                    inv_disc = r * inv_rd;
+                } else {
+                    melt = 2.0 * r / g;
+                    const double inv = 1.0 / (melt * disc);
+                    inv_melt = disc * inv; inv_disc = melt * inv;
+                }
+            }
+            s.cl = clip_fraction(C * inv_melt, st);
+            s.dTdC = minus_magnitude(k.LDoverXe * inv_disc);
+        } else {
+            melt = a >= 0.0 ? (a + disc) * k.halfInvLD : 2.0 * r / (disc - a);
+            // cl = C/melt in [-tol, 1 + tol] (C, melt > 0), as the full evaluation checks.
+            if (!(C <= (1.0 + 64.0 * 2.220446049250313e-16) * melt)) st = PH_RUNTIME;
+        }
         s.phil = clip_fraction(melt, st);
         phi1 = clip_fraction(1.0 - melt, st);
-        s.cl = clip_fraction(C * inv_melt, st);
-        s.T = a >= 0.0 ? Tmp - r * inv_melt : H - k.LD * melt;
-        s.dTdC = minus_magnitude(k.LDoverXe * inv_disc);
+        s.T = Tmp - 0.5 * (disc - a);
     }
-    if (C == 0.0 && H > Tep && !liquid_region) {
-        const double gap = fabs(H - Tmp);
-        s.dTdC = gap == 0.0 ? -INFINITY : minus_magnitude(k.LDoverXe / gap);
+    if (kFull) {
+        if (C == 0.0 && H > Tep && !liquid_region) {
+            const double gap = fabs(H - Tmp);
+            s.dTdC = gap == 0.0 ? -INFINITY : minus_magnitude(k.LDoverXe / gap);
+        }
+        if (general_cs) {
+            const double solid = phi1 + phi2;
+            s.cs = (solid > 0.0 && phi2 != 0.0) ? phi2 / solid : 0.0;
+        }
+        if (!(s.phil > 0.0)) s.cl = 0.0;
     }
-    const double solid = phi1 + phi2;
-    s.cs = (solid > 0.0 && phi2 != 0.0) ? phi2 / solid : 0.0;
-    if (!(s.phil > 0.0)) s.cl = 0.0;
     return st;
+}
+
+MP_HD int phase_stage(const StageConst& k, double H, double C, double Tep, PhaseLean& s) {
+    return phase_stage_t<true>(k, H, C, Tep, s);
+}
+MP_HD int phase_stage_lean(const StageConst& k, double H, double C, double Tep, PhaseLean& s) {
+    return phase_stage_t<false>(k, H, C, Tep, s);
 }
 
 }  // namespace mp

@@ -238,6 +238,7 @@ extern "C" mp_status mp_serve_submit(mp_server* s, const mp_mesh_desc* mesh, con
                                      const double* vs_n, const double* ud_n, double t_final, long long* id) {
     if (!s || !mesh || !H || !C || !vs_n || !ud_n || !id) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (mesh->nx < 2 || mesh->ny < 2) { mp::set_error("Transport requires at least 2x2 cells"); return MP_ERR_ARG_SIZ; }
+    if (mp::mesh_too_large(mesh->nx, mesh->ny)) { mp::set_error("mesh has 2^31 edges or more"); return MP_ERR_ARG_SIZ; }
     if (!(t_final > 0)) { mp::set_error("final time must be positive"); return MP_ERR_ARG_OUTOFRANGE; }
     auto r = std::make_shared<Request>();
     r->mesh = *mesh;

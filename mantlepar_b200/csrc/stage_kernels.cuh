@@ -18,6 +18,10 @@ namespace {
 
 constexpr int kRec = 18;          // limited deviation coefficients: 9 for H, 9 for C
 constexpr int kRedBlock = 256;
+// The accumulation and axpy kernels give each thread kSumPer cells (strided
+// by the block size, so loads stay coalesced) before one block reduction.
+constexpr int kSumPer = 4;
+constexpr int kSumCells = kRedBlock * kSumPer;
 
 enum : int {
     E_OUTOFRANGE = MP_ERR_ARG_OUTOFRANGE, E_FP = MP_ERR_FP, E_WRONG = MP_ERR_ARG_WRONG
@@ -38,6 +42,10 @@ struct Partial {
     double maxRate, divergence, bH, bC, HI, CI, Hmin, Cmin, Cmax;
     double nonfinite;
 };
+
+__device__ __forceinline__ Partial partial_identity() {
+    return Partial{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
+}
 
 struct Totals {
     double maxRate, divergence, bH, bC, HI, CI, Hmin, Cmin, Cmax;
@@ -286,7 +294,7 @@ __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const 
             const double h = mH + quad(h0, h1, h2, x);
             const double c = mC + quad(c0, c1, c2, x);
             PhaseLean pl;
-            const int s = phase_stage(ph.sk, h, c, ph.Tep, pl);
+            const int s = phase_stage_lean(ph.sk, h, c, ph.Tep, pl);
             if (s) { st_por = st_por ? st_por : s; continue; }
             if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_cell = st_cell ? st_cell : E_OUTOFRANGE;
             const double w = t.cw[b * kNQ + q];
@@ -314,7 +322,7 @@ __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const 
                 const double h = mH + quad(h0, h1, h2, s_);
                 const double c = mC + quad(c0, c1, c2, s_);
                 PhaseLean pl;
-                const int s = phase_stage(ph.sk, h, c, ph.Tep, pl);
+                const int s = phase_stage_lean(ph.sk, h, c, ph.Tep, pl);
                 if (s) { st_face = st_face ? st_face : s; continue; }
                 if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_face = st_face ? st_face : E_OUTOFRANGE;
             }
@@ -386,7 +394,8 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
     // Left/right cells and orientation as the reference's Build (evolve.cpp:230-251).
     if (e < nI) {
         horizontal = true;
-        const int i = (int)(e % nx), j = (int)(e / nx);
+        const unsigned ue = (unsigned)e;   // edge counts stay below 2^31 (checked on create)
+        const int i = (int)(ue % (unsigned)nx), j = (int)(ue / (unsigned)nx);
         boundary = (j == 0 || j == ny);
         reverse = (j == ny);
         L = reverse ? (long long)(ny - 1) * nx + i : (long long)j * nx + i;
@@ -396,8 +405,8 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
         len = t.len_h;
     } else {
         horizontal = false;
-        const long long k = e - nI;
-        const int i = (int)(k % (nx + 1)), j = (int)(k / (nx + 1));
+        const unsigned k = (unsigned)(e - nI);
+        const int i = (int)(k % (unsigned)(nx + 1)), j = (int)(k / (unsigned)(nx + 1));
         boundary = (i == 0 || i == nx);
         reverse = (i == 0);
         L = reverse ? (long long)j * nx : (long long)j * nx + (i - 1);
@@ -536,58 +545,85 @@ __device__ void block_reduce_write(Partial v, Partial* out) {
     }
 }
 
-// Per-cell accumulation + RK combination; returns the cell's contribution to
-// the stage reductions (identity values for cell >= N).
-__device__ __forceinline__ Partial sum_cell(const SumArgs& a, long long cell) {
+// Per-cell accumulation + RK combination; folds the cell's contribution to
+// the stage reductions into v.
+__device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partial& v) {
     const int nx = a.nx, ny = a.ny;
-    const long long N = (long long)nx * ny;
     const long long nI = (long long)nx * (ny + 1);
     const long long nE = nI + (long long)(nx + 1) * ny;
-    Partial v{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
-    if (cell < N) {
-        const int i = (int)(cell % nx), j = (int)(cell / nx);
-        const double A = a.area;
-        // Faces of this cell in the reference's id order: bottom, top, left, right,
-        // each with the sign of its side (evolve.cpp:350-354).
-        const long long eb = (long long)j * nx + i, et = (long long)(j + 1) * nx + i;
-        const long long el = nI + (long long)j * (nx + 1) + i, er = el + 1;
-        const double sb = -1.0, stp = (j == ny - 1) ? -1.0 : 1.0, sl = (i == 0) ? -1.0 : 1.0, sr = -1.0;
-        const long long ids[4] = {eb, et, el, er};
-        const double sg[4] = {sb, stp, sl, sr};
-        double rH = 0.0, rC = 0.0, rr = 0.0, dv = 0.0, bH = 0.0, bC = 0.0;
+    const int i = (int)(cell % (unsigned)nx), j = (int)(cell / (unsigned)nx);
+    const double A = a.area;
+    // Faces of this cell in the reference's id order: bottom, top, left, right,
+    // each with the sign of its side (evolve.cpp:350-354).
+    const long long eb = (long long)j * nx + i, et = (long long)(j + 1) * nx + i;
+    const long long el = nI + (long long)j * (nx + 1) + i, er = el + 1;
+    const double sb = -1.0, stp = (j == ny - 1) ? -1.0 : 1.0, sl = (i == 0) ? -1.0 : 1.0, sr = -1.0;
+    const long long ids[4] = {eb, et, el, er};
+    const double sg[4] = {sb, stp, sl, sr};
+    double rH = 0.0, rC = 0.0, rr = 0.0, dv = 0.0, bH = 0.0, bC = 0.0;
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            const double FH = a.face[ids[f]], FC = a.face[nE + ids[f]];
-            const double FR = a.face[2 * nE + ids[f]], FM = a.face[3 * nE + ids[f]];
-            rH += sg[f] * FH / A;
-            rC += sg[f] * FC / A;
-            rr += FR / A;
-            dv += -sg[f] * FM / A;
-        }
-        if (j == 0) { bH += a.face[eb]; bC += a.face[nE + eb]; }
-        if (j == ny - 1) { bH += a.face[et]; bC += a.face[nE + et]; }
-        if (i == 0) { bH += a.face[el]; bC += a.face[nE + el]; }
-        if (i == nx - 1) { bH += a.face[er]; bC += a.face[nE + er]; }
-        double nh, nc;
-        if (a.mode == SUM_RK) {
-            const double dt_ = a.dtp ? *a.dtp : a.dt;
-            const double h = a.H[cell], c = a.C[cell];
-            const double sh_ = __dadd_rn(h, __dmul_rn(dt_, rH));
-            const double sc_ = __dadd_rn(c, __dmul_rn(dt_, rC));
-            nh = __dadd_rn(__dmul_rn(a.a0, a.H0[cell]), __dmul_rn(a.a1, sh_));
-            nc = __dadd_rn(__dmul_rn(a.a0, a.C0[cell]), __dmul_rn(a.a1, sc_));
-        } else {
-            nh = a.H[cell]; nc = a.C[cell];
-        }
-        a.outH[cell] = a.mode == SUM_RK ? nh : rH;
-        a.outC[cell] = a.mode == SUM_RK ? nc : rC;
-        if (a.rate) a.rate[cell] = rr;
-        v.maxRate = rr;
-        v.divergence = fabs(dv);
-        v.bH = bH; v.bC = bC;
-        v.HI = nh * A; v.CI = nc * A;
-        v.Hmin = nh; v.Cmin = nc; v.Cmax = nc;
-        v.nonfinite = (isfinite(nh) && isfinite(nc) && isfinite(rr)) ? 0.0 : 1.0;
+    for (int f = 0; f < 4; ++f) {
+        const double FH = a.face[ids[f]], FC = a.face[nE + ids[f]];
+        const double FR = a.face[2 * nE + ids[f]], FM = a.face[3 * nE + ids[f]];
+        rH += sg[f] * FH / A;
+        rC += sg[f] * FC / A;
+        rr += FR / A;
+        dv += -sg[f] * FM / A;
+    }
+    if (j == 0) { bH += a.face[eb]; bC += a.face[nE + eb]; }
+    if (j == ny - 1) { bH += a.face[et]; bC += a.face[nE + et]; }
+    if (i == 0) { bH += a.face[el]; bC += a.face[nE + el]; }
+    if (i == nx - 1) { bH += a.face[er]; bC += a.face[nE + er]; }
+    double nh, nc;
+    if (a.mode == SUM_RK) {
+        const double dt_ = a.dtp ? *a.dtp : a.dt;
+        const double h = a.H[cell], c = a.C[cell];
+        const double sh_ = __dadd_rn(h, __dmul_rn(dt_, rH));
+        const double sc_ = __dadd_rn(c, __dmul_rn(dt_, rC));
+        nh = __dadd_rn(__dmul_rn(a.a0, a.H0[cell]), __dmul_rn(a.a1, sh_));
+        nc = __dadd_rn(__dmul_rn(a.a0, a.C0[cell]), __dmul_rn(a.a1, sc_));
+    } else {
+        nh = a.H[cell]; nc = a.C[cell];
+    }
+    a.outH[cell] = a.mode == SUM_RK ? nh : rH;
+    a.outC[cell] = a.mode == SUM_RK ? nc : rC;
+    if (a.rate) a.rate[cell] = rr;
+    v.maxRate = fmax(v.maxRate, rr);
+    v.divergence = fmax(v.divergence, fabs(dv));
+    v.bH += bH; v.bC += bC;
+    v.HI += nh * A; v.CI += nc * A;
+    v.Hmin = fmin(v.Hmin, nh); v.Cmin = fmin(v.Cmin, nc); v.Cmax = fmax(v.Cmax, nc);
+    v.nonfinite = fmax(v.nonfinite, (isfinite(nh) && isfinite(nc) && isfinite(rr)) ? 0.0 : 1.0);
+}
+
+// The kSumPer cells of this thread in the sum block starting at first.
+__device__ __forceinline__ Partial sum_cells(const SumArgs& a, long long first) {
+    const long long N = (long long)a.nx * a.ny;
+    Partial v = partial_identity();
+#pragma unroll
+    for (int k = 0; k < kSumPer; ++k) {
+        const long long c = first + k * kRedBlock + threadIdx.x;
+        if (c < N) sum_cell(a, (unsigned)c, v);
+    }
+    return v;
+}
+
+// U1 = U^n + dt*L^n over the kSumPer cells of this thread, with the
+// admissibility/integral partials of U1.
+__device__ __forceinline__ Partial axpy_cells(long long n, const double* H0, const double* C0, const double* LH,
+                                              const double* LC, double dt, double area, double* H1, double* C1,
+                                              long long first) {
+    Partial v = partial_identity();
+#pragma unroll
+    for (int q = 0; q < kSumPer; ++q) {
+        const long long k = first + q * kRedBlock + threadIdx.x;
+        if (k >= n) continue;
+        const double h = __dadd_rn(H0[k], __dmul_rn(dt, LH[k]));
+        const double c = __dadd_rn(C0[k], __dmul_rn(dt, LC[k]));
+        H1[k] = h; C1[k] = c;
+        v.HI += h * area; v.CI += c * area;
+        v.Hmin = fmin(v.Hmin, h); v.Cmin = fmin(v.Cmin, c); v.Cmax = fmax(v.Cmax, c);
+        v.nonfinite = fmax(v.nonfinite, (isfinite(h) && isfinite(c)) ? 0.0 : 1.0);
     }
     return v;
 }

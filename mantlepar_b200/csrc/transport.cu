@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(128) face_kernel(FaceArgs<R> a, Physics ph, co
     face_edge(b, ph, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 __global__ void __launch_bounds__(kRedBlock) sum_kernel(SumArgs a) {
-    const Partial v = sum_cell(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+    const Partial v = sum_cells(a, (long long)blockIdx.x * kSumCells);
     block_reduce_write(v, a.partial + blockIdx.x);
 }
 
@@ -61,16 +61,7 @@ __global__ void __launch_bounds__(kRedBlock) sum_kernel(SumArgs a) {
 __global__ void __launch_bounds__(kRedBlock) axpy_kernel(int n, const double* H0, const double* C0, const double* LH,
                                                          const double* LC, double dt, double area, double* H1,
                                                          double* C1, Partial* partial) {
-    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    Partial v{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
-    if (k < n) {
-        const double h = __dadd_rn(H0[k], __dmul_rn(dt, LH[k]));
-        const double c = __dadd_rn(C0[k], __dmul_rn(dt, LC[k]));
-        H1[k] = h; C1[k] = c;
-        v.HI = h * area; v.CI = c * area;
-        v.Hmin = h; v.Cmin = c; v.Cmax = c;
-        v.nonfinite = (isfinite(h) && isfinite(c)) ? 0.0 : 1.0;
-    }
+    const Partial v = axpy_cells(n, H0, C0, LH, LC, dt, area, H1, C1, (long long)blockIdx.x * kSumCells);
     block_reduce_write(v, partial + blockIdx.x);
 }
 
@@ -295,7 +286,7 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
     int retries = 0;
     double courant = 0.0;
     Totals second{}, third{}, fin{};
-    const int nblk_axpy = (int)((t->N + kRedBlock - 1) / kRedBlock);
+    const int nblk_axpy = (int)((t->N + kSumCells - 1) / kSumCells);
     for (;;) {
         if (!(dt >= o.dt_min && retries < 40)) {
             set_error("Coupled step cannot satisfy admissibility/CFL above minimum step");
@@ -387,6 +378,7 @@ extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_tran
     using namespace mp;
     if (!mesh || !opts || !out) { set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (mesh->nx < 2 || mesh->ny < 2) { set_error("Transport requires at least 2x2 cells"); return MP_ERR_ARG_SIZ; }
+    if (mesh_too_large(mesh->nx, mesh->ny)) { set_error("mesh has 2^31 edges or more"); return MP_ERR_ARG_SIZ; }
     if (!(opts->cfl > 0 && opts->cfl <= 1)) { set_error("Coupled CFL must be in (0,1]"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->integrator != MP_SSPRK2 && opts->integrator != MP_SSPRK3) { set_error("integrator must be 2 or 3"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->diffusivity != 0.0) { set_error("thermal diffusion (kappa > 0) is not supported by this build"); return MP_ERR_ARG_WRONG; }
@@ -414,7 +406,7 @@ extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_tran
     const int tb = build_stage_tables(t->nx, t->ny, mesh->x0, mesh->x1, mesh->y0, mesh->y1, t->host_tab);
     if (tb) { delete t; set_error("stencil table construction failed"); return (mp_status)tb; }
     make_param_tables(t->host_tab, t->ptab);
-    t->sum_blocks = (int)((t->N + kRedBlock - 1) / kRedBlock);
+    t->sum_blocks = (int)((t->N + kSumCells - 1) / kSumCells);
     const size_t N = t->N, NE = t->NE;
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes); };
@@ -594,7 +586,7 @@ extern "C" mp_status mp_probe_fp64_peak(mp_stream_t stream, double* tflops) {
 
 namespace mp {
 
-size_t raw_partial_bytes(size_t ncell) { return ((ncell + kRedBlock - 1) / kRedBlock) * sizeof(Partial); }
+size_t raw_partial_bytes(size_t ncell) { return ((ncell + kSumCells - 1) / kSumCells) * sizeof(Partial); }
 size_t raw_totals_bytes() { return sizeof(Totals); }
 
 // One stage evaluation L(U) (STORE_L mode) on buffers the caller provides:
@@ -615,7 +607,7 @@ mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double
     ph.Hpol = o.H_policy; ph.Cpol = o.C_policy; ph.lf_global = o.lf_global; ph.lf_speed = o.lf_global_speed;
     const size_t N = (size_t)nx * ny;
     const size_t NE = (size_t)nx * (ny + 1) + (size_t)(nx + 1) * ny;
-    const int sum_blocks = (int)((N + kRedBlock - 1) / kRedBlock);
+    const int sum_blocks = (int)((N + kSumCells - 1) / kSumCells);
     Partial* part = static_cast<Partial*>(partial);
     Totals* tot = static_cast<Totals*>(totals);
     MP_CUDA(cudaMemsetAsync(status, 0xff, sizeof(unsigned long long), s));
