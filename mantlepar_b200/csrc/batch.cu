@@ -54,7 +54,8 @@ struct AxpyArgs {
     Partial* partial;
 };
 
-// Work items: block -> instance and the first element of its tile.
+// Work items: block -> instance and the first element of its tile (faces:
+// edges [a, b); reconstruction: columns from a, row b).
 struct Work { int inst, a, b, part; };
 
 struct Tuning { int bx = 32, by = 4, cpt = 1; };
@@ -84,7 +85,8 @@ __global__ void __launch_bounds__(128) batch_face_kernel(const InstArgs<R>* args
                                                          Physics ph) {
     const Work w = work[blockIdx.x];
     if (!active[w.inst]) return;
-    face_edge(args[w.inst].face, ph, (long long)w.a + threadIdx.x);
+    const long long e = (long long)w.a + threadIdx.x;
+    if (e < w.b) face_edge(args[w.inst].face, ph, e);
 }
 
 template <class R>
@@ -318,7 +320,7 @@ mp_status rebuild_args(mp_batch* b, int slots) {
             const bool rk3 = b->opts.integrator == MP_SSPRK3;
             const double a0 = k == KIND_B ? (rk3 ? 0.75 : 0.5) : (1.0 / 3.0);
             const double a1 = k == KIND_B ? (rk3 ? 0.25 : 0.5) : (2.0 / 3.0);
-            a.sum = SumArgs{in.nx, in.ny, in.host_tab.area, in.face, inH, inC, in.H, in.C, outH, outC, in.rate,
+            a.sum = SumArgs{in.nx, in.ny, in.host_tab.area, 1.0 / in.host_tab.area, in.face, inH, inC, in.H, in.C, outH, outC, in.rate,
                             k == KIND_P ? (int)SUM_STORE_L : (int)SUM_RK, a0, a1, 0.0, b->d_partial + parts,
                             b->d_dt + i};
         }
@@ -327,7 +329,7 @@ mp_status rebuild_args(mp_batch* b, int slots) {
         for (int ty = 0; ty < in.ny; ty += tu.by)
             for (int tx = 0; tx < in.nx; tx += tu.bx * tu.cpt) wr.push_back(Work{i, tx, ty, 0});
         for (size_t c = 0; c < in.N; c += 128) wp.push_back(Work{i, (int)c, 0, 0});
-        for (size_t e = 0; e < in.NE; e += 128) wf.push_back(Work{i, (int)e, 0, 0});
+        for (size_t e = 0; e < in.NE; e += 128) wf.push_back(Work{i, (int)e, (int)std::min(in.NE, e + 128), 0});
         for (int s = 0; s < nsum; ++s) ws.push_back(Work{i, s * kSumCells, 0, s});
         parts += nsum;
     }

@@ -100,14 +100,32 @@ __device__ __noinline__ void scan_lines_exact(const StageHot& t, int l0, int l1,
     mx = rmx; mn = rmn;
 }
 
+// Candidates of one limiter line: its centre p0 = a0 and the larger (p1, p2)
+// and smaller (m1, m2) value of each Gauss pair, v(+-s_k) = e_k +- a1 s_k.
+template <class R>
+__device__ __forceinline__ void line_candidates(const StageHot& t, const Tab<R>& tb, int l, const R* D, R sx1, R sx2,
+                                                R sy1, R sy2, R qx1, R qx2, R qy1, R qy2, R& p0, R& p1, R& p2, R& m1,
+                                                R& m2) {
+    const R c = tb.line_c(l);
+    R a0, a1, a2;
+    const bool row = t.line_dir[l] == 0;
+    if (row) q2_row(D, c, a0, a1, a2);
+    else q2_col(D, c, a0, a1, a2);
+    const R s1 = row ? sx1 : sy1, s2 = row ? sx2 : sy2;
+    const R e1 = fma(a2, row ? qx1 : qy1, a0), e2 = fma(a2, row ? qx2 : qy2, a0);
+    const R b = fabs(a1);
+    const R d1 = b * s1, d2 = b * s2;
+    p0 = a0; p1 = e1 + d1; p2 = e2 + d2; m1 = e1 - d1; m2 = e2 - d2;
+}
+
 // Max/min of the deviation polynomial over the class's limiter points. Each
 // line holds its centre (s = 0) and the symmetric Gauss pairs s = +-s_k
 // (g = 0, +-g1, +-g2), so along a line v(+-s_k) = (a0 + a2 s_k^2) +- a1 s_k
 // and the larger of a pair is e_k + |a1| s_k: three candidates per line for
 // the maximum and three for the minimum. With every |D_m| below scan_guard
 // no value can overflow, so no per-point finiteness test is needed;
-// otherwise the exact scan runs. For R = float the candidates attaining the
-// extremes are re-evaluated in FP64, so theta is formed from FP64 values.
+// otherwise the exact scan runs. For R = float the lines holding the
+// extremes are evaluated again in FP64, so theta is formed from FP64 values.
 template <class R>
 __device__ __forceinline__ void scan_lines(const StageHot& t, const Tab<R>& tb, int l0, int l1, const double* Dd,
                                            double& mx, double& mn, bool& bad) {
@@ -120,45 +138,40 @@ __device__ __forceinline__ void scan_lines(const StageHot& t, const Tab<R>& tb, 
     for (int m = 0; m < 9; ++m) D[m] = (R)Dd[m];
     const R sx1 = tb.gx(3), sx2 = tb.gx(4), sy1 = tb.gy(3), sy2 = tb.gy(4);
     const R qx1 = sx1 * sx1, qx2 = sx2 * sx2, qy1 = sy1 * sy1, qy2 = sy2 * sy2;
-    R rmx = D[0], rmn = D[0];        // cell centre
-    int amx = -1, amn = -1;          // FP32: extreme point as line*8 + q (-1 = centre)
-    for (int l = l0; l < l1; ++l) {
-        const R c = tb.line_c(l);
-        R a0, a1, a2;
-        const bool row = t.line_dir[l] == 0;
-        if (row) q2_row(D, c, a0, a1, a2);
-        else q2_col(D, c, a0, a1, a2);
-        const R s1 = row ? sx1 : sy1, s2 = row ? sx2 : sy2;
-        const R e1 = fma(a2, row ? qx1 : qy1, a0), e2 = fma(a2, row ? qx2 : qy2, a0);
-        const R b = fabs(a1);
-        const R d1 = b * s1, d2 = b * s2;
-        const R p1 = e1 + d1, p2 = e2 + d2, m1 = e1 - d1, m2 = e2 - d2;
-        if constexpr (sizeof(R) == 8) {
-            rmx = a0 > rmx ? a0 : rmx; rmx = p1 > rmx ? p1 : rmx; rmx = p2 > rmx ? p2 : rmx;
-            rmn = a0 < rmn ? a0 : rmn; rmn = m1 < rmn ? m1 : rmn; rmn = m2 < rmn ? m2 : rmn;
-        } else {
-            // Gauss index of +s_k is 2 + k, of -s_k is 2 - k.
-            const bool up = a1 >= R(0);
-            if (a0 > rmx) { rmx = a0; amx = l * 8 + 2; }
-            if (p1 > rmx) { rmx = p1; amx = l * 8 + (up ? 3 : 1); }
-            if (p2 > rmx) { rmx = p2; amx = l * 8 + (up ? 4 : 0); }
-            if (a0 < rmn) { rmn = a0; amn = l * 8 + 2; }
-            if (m1 < rmn) { rmn = m1; amn = l * 8 + (up ? 1 : 3); }
-            if (m2 < rmn) { rmn = m2; amn = l * 8 + (up ? 0 : 4); }
-        }
-    }
     if constexpr (sizeof(R) == 8) {
-        mx = (double)rmx; mn = (double)rmn;
+        double rmx = D[0], rmn = D[0];   // cell centre
+        for (int l = l0; l < l1; ++l) {
+            double p0, p1, p2, m1, m2;
+            line_candidates<double>(t, tb, l, D, sx1, sx2, sy1, sy2, qx1, qx2, qy1, qy2, p0, p1, p2, m1, m2);
+            rmx = p0 > rmx ? p0 : rmx; rmx = p1 > rmx ? p1 : rmx; rmx = p2 > rmx ? p2 : rmx;
+            rmn = p0 < rmn ? p0 : rmn; rmn = m1 < rmn ? m1 : rmn; rmn = m2 < rmn ? m2 : rmn;
+        }
+        mx = rmx; mn = rmn;
     } else {
-        auto at = [&](int code) {
-            if (code < 0) return Dd[0];
-            const int l = code >> 3, q = code & 7;
-            double a0, a1, a2;
-            if (t.line_dir[l] == 0) { q2_row(Dd, t.line_c[l], a0, a1, a2); return quad(a0, a1, a2, t.gx[q]); }
-            q2_col(Dd, t.line_c[l], a0, a1, a2);
-            return quad(a0, a1, a2, t.gy[q]);
-        };
-        mx = at(amx); mn = at(amn);
+        // FP32: keep the line holding each extreme; its candidates are then
+        // evaluated again in FP64.
+        float rmx = D[0], rmn = D[0];
+        int lmx = -1, lmn = -1;          // -1 = centre
+        for (int l = l0; l < l1; ++l) {
+            float p0, p1, p2, m1, m2;
+            line_candidates<float>(t, tb, l, D, sx1, sx2, sy1, sy2, qx1, qx2, qy1, qy2, p0, p1, p2, m1, m2);
+            const float lx = fmaxf(p0, fmaxf(p1, p2)), ln = fminf(p0, fminf(m1, m2));
+            if (lx > rmx) { rmx = lx; lmx = l; }
+            if (ln < rmn) { rmn = ln; lmn = l; }
+        }
+        const Tab<double> td{&t};
+        const double gx1 = t.gx[3], gx2 = t.gx[4], gy1 = t.gy[3], gy2 = t.gy[4];
+        const double hx1 = gx1 * gx1, hx2 = gx2 * gx2, hy1 = gy1 * gy1, hy2 = gy2 * gy2;
+        mx = Dd[0]; mn = Dd[0];
+        double p0, p1, p2, m1, m2;
+        if (lmx >= 0) {
+            line_candidates<double>(t, td, lmx, Dd, gx1, gx2, gy1, gy2, hx1, hx2, hy1, hy2, p0, p1, p2, m1, m2);
+            mx = fmax(p0, fmax(p1, p2));
+        }
+        if (lmn >= 0) {
+            line_candidates<double>(t, td, lmn, Dd, gx1, gx2, gy1, gy2, hx1, hx2, hy1, hy2, p0, p1, p2, m1, m2);
+            mn = fmin(p0, fmin(m1, m2));
+        }
     }
 }
 
@@ -438,16 +451,32 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
         }
         if (s) { st = st ? st : s; continue; }
         // Edge porosity: harmonic mean of both sides, zero next to a dry cell
-        // (initial_flow.cpp:94-117).
-        double ephi = (A.phil + B.phil) > 0.0 ? 2.0 * A.phil * B.phil / (A.phil + B.phil) : 0.0;
-        if (!wetL || !wetR) ephi = 0.0;
-        // PhaseTransportVelocities (evolve.cpp:36-52) on normal components.
+        // (initial_flow.cpp:94-117). PhaseTransportVelocities (evolve.cpp:36-52)
+        // on normal components: bulk = ephi cl + (1 - ephi) cs, and the
+        // composition velocity adds cl/bulk times the Darcy flux. With
+        // S = phil_A + phil_B and Q = S bulk, ephi = 2 phil_A phil_B / S and
+        // cl/bulk = cl S / Q come from one division 1/(S Q) where it is in range.
         const double cl = 0.5 * (A.cl + B.cl), cs = 0.5 * (A.cs + B.cs);
-        const double bulk = ephi * cl + (1.0 - ephi) * cs;
+        const double S = A.phil + B.phil;
+        double ephi = 0.0, clb = 0.0;   // clb = cl/bulk where bulk > 0, else 0
+        if (wetL && wetR && S > 0.0) {
+            const double P2 = 2.0 * A.phil * B.phil;
+            const double Q = P2 * (cl - cs) + cs * S;
+            const double SQ = S * Q;
+            if (SQ > 1e-290 && SQ < 1e290) {
+                const double x = 1.0 / SQ;
+                ephi = P2 * (Q * x);
+                clb = cl * (S * (S * x));
+            } else {
+                ephi = P2 / S;
+                const double bulk = ephi * cl + (1.0 - ephi) * cs;
+                clb = bulk > 0.0 ? cl / bulk : 0.0;
+            }
+        }
         const double factor = ephi == 0.0 ? 0.0 : (ph.theta == 0.0 ? ephi : pow(ephi, 1.0 + ph.theta));
         const double flux = factor * ud;
         const double vn = vs + flux;
-        const double ve = vs + (bulk > 0.0 ? cl / bulk * flux : 0.0);
+        const double ve = vs + clb * flux;
         const double aH = ph.lf_global ? ph.lf_speed : fabs(vn);
         const double aC = ph.lf_global ? ph.lf_speed : fabs(ve);
         if (ph.lf_global && !(aH + 1e-14 >= fabs(vn) && aC + 1e-14 >= fabs(ve))) st = st ? st : E_OUTOFRANGE;
@@ -492,6 +521,7 @@ enum SumMode : int { SUM_STORE_L = 0, SUM_RK = 1 };
 struct SumArgs {
     int nx, ny;
     double area;           // cell area
+    double inv_area;       // 1 / area
     const double* face;
     const double* H;       // stage state
     const double* C;
@@ -552,7 +582,7 @@ __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partia
     const long long nI = (long long)nx * (ny + 1);
     const long long nE = nI + (long long)(nx + 1) * ny;
     const int i = (int)(cell % (unsigned)nx), j = (int)(cell / (unsigned)nx);
-    const double A = a.area;
+    const double A = a.area, invA = a.inv_area;
     // Faces of this cell in the reference's id order: bottom, top, left, right,
     // each with the sign of its side (evolve.cpp:350-354).
     const long long eb = (long long)j * nx + i, et = (long long)(j + 1) * nx + i;
@@ -560,30 +590,33 @@ __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partia
     const double sb = -1.0, stp = (j == ny - 1) ? -1.0 : 1.0, sl = (i == 0) ? -1.0 : 1.0, sr = -1.0;
     const long long ids[4] = {eb, et, el, er};
     const double sg[4] = {sb, stp, sl, sr};
+    // The reference divides each face term by the area; here the signed sums
+    // are scaled once by 1/A (a few ulp apart).
     double rH = 0.0, rC = 0.0, rr = 0.0, dv = 0.0, bH = 0.0, bC = 0.0;
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-        const double FH = a.face[ids[f]], FC = a.face[nE + ids[f]];
-        const double FR = a.face[2 * nE + ids[f]], FM = a.face[3 * nE + ids[f]];
-        rH += sg[f] * FH / A;
-        rC += sg[f] * FC / A;
-        rr += FR / A;
-        dv += -sg[f] * FM / A;
+        const double FH = __ldg(a.face + ids[f]), FC = __ldg(a.face + nE + ids[f]);
+        const double FR = __ldg(a.face + 2 * nE + ids[f]), FM = __ldg(a.face + 3 * nE + ids[f]);
+        rH += sg[f] * FH;
+        rC += sg[f] * FC;
+        rr += FR;
+        dv -= sg[f] * FM;
     }
-    if (j == 0) { bH += a.face[eb]; bC += a.face[nE + eb]; }
-    if (j == ny - 1) { bH += a.face[et]; bC += a.face[nE + et]; }
-    if (i == 0) { bH += a.face[el]; bC += a.face[nE + el]; }
-    if (i == nx - 1) { bH += a.face[er]; bC += a.face[nE + er]; }
+    rH *= invA; rC *= invA; rr *= invA; dv *= invA;
+    if (j == 0) { bH += __ldg(a.face + eb); bC += __ldg(a.face + nE + eb); }
+    if (j == ny - 1) { bH += __ldg(a.face + et); bC += __ldg(a.face + nE + et); }
+    if (i == 0) { bH += __ldg(a.face + el); bC += __ldg(a.face + nE + el); }
+    if (i == nx - 1) { bH += __ldg(a.face + er); bC += __ldg(a.face + nE + er); }
     double nh, nc;
     if (a.mode == SUM_RK) {
         const double dt_ = a.dtp ? *a.dtp : a.dt;
-        const double h = a.H[cell], c = a.C[cell];
+        const double h = __ldg(a.H + cell), c = __ldg(a.C + cell);
         const double sh_ = __dadd_rn(h, __dmul_rn(dt_, rH));
         const double sc_ = __dadd_rn(c, __dmul_rn(dt_, rC));
-        nh = __dadd_rn(__dmul_rn(a.a0, a.H0[cell]), __dmul_rn(a.a1, sh_));
-        nc = __dadd_rn(__dmul_rn(a.a0, a.C0[cell]), __dmul_rn(a.a1, sc_));
+        nh = __dadd_rn(__dmul_rn(a.a0, __ldg(a.H0 + cell)), __dmul_rn(a.a1, sh_));
+        nc = __dadd_rn(__dmul_rn(a.a0, __ldg(a.C0 + cell)), __dmul_rn(a.a1, sc_));
     } else {
-        nh = a.H[cell]; nc = a.C[cell];
+        nh = __ldg(a.H + cell); nc = __ldg(a.C + cell);
     }
     a.outH[cell] = a.mode == SUM_RK ? nh : rH;
     a.outC[cell] = a.mode == SUM_RK ? nc : rC;

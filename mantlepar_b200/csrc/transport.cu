@@ -226,7 +226,7 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
                                      t->phi, t->vsn, t->udn, t->face, t->d_status, theta, s, prof);
     }
     {
-        SumArgs a{t->nx, t->ny, t->host_tab.area, t->face, H, C, t->H, t->C, outH, outC, t->rate, mode, a0, a1, dt,
+        SumArgs a{t->nx, t->ny, t->host_tab.area, 1.0 / t->host_tab.area, t->face, H, C, t->H, t->C, outH, outC, t->rate, mode, a0, a1, dt,
                   t->partial};
         timed(t, 3, [&] { sum_kernel<<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
     }
@@ -616,7 +616,7 @@ mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double
     make_param_tables(tab, pt);
     launch_stage_kernels<double>(nx, ny, pt, ph, H, C, rec, wet, T, phi, vsn, udn, face, status, nullptr, s, nullptr);
     {
-        SumArgs a{nx, ny, tab.area, face, H, C, H, C, rhsH, rhsC, rate, SUM_STORE_L, 0.0, 0.0, 0.0, part};
+        SumArgs a{nx, ny, tab.area, 1.0 / tab.area, face, H, C, H, C, rhsH, rhsC, rate, SUM_STORE_L, 0.0, 0.0, 0.0, part};
         sum_kernel<<<sum_blocks, kRedBlock, 0, s>>>(a);
     }
     reduce_kernel<<<1, 1024, 0, s>>>(part, sum_blocks, tot);
