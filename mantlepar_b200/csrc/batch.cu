@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(128) batch_recon_kernel(const InstArgs<R>* arg
 }
 
 template <class R>
-__global__ void __launch_bounds__(128) batch_phase_kernel(const InstArgs<R>* args, const Work* work, const int* active,
+__global__ void __launch_bounds__(128, 8) batch_phase_kernel(const InstArgs<R>* args, const Work* work, const int* active,
                                                           Physics ph) {
     const Work w = work[blockIdx.x];
     if (!active[w.inst]) return;
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(128) batch_phase_kernel(const InstArgs<R>* arg
 }
 
 template <class R>
-__global__ void __launch_bounds__(128) batch_face_kernel(const InstArgs<R>* args, const Work* work, const int* active,
+__global__ void __launch_bounds__(128, 5) batch_face_kernel(const InstArgs<R>* args, const Work* work, const int* active,
                                                          Physics ph) {
     const Work w = work[blockIdx.x];
     if (!active[w.inst]) return;

@@ -32,7 +32,9 @@ namespace {
 
 // Single-instance kernels: one thread per cell / edge.
 // The stage tables arrive by value as a __grid_constant__ parameter, so the
-// unrolled table coefficients are constant-bank operands.
+// unrolled table coefficients are constant-bank operands. Minimum resident
+// blocks per SM (register caps) as measured fastest on B200: cell phase 8,
+// faces 5; the reconstruction keeps its natural register count.
 template <class R>
 __global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph, const __grid_constant__ ParamTables p) {
     ReconArgs<R> b = a;
@@ -40,14 +42,14 @@ __global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph, 
     recon_cell(b, ph, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
 }
 template <class R>
-__global__ void __launch_bounds__(128) cellphase_kernel(CellPhaseArgs<R> a, Physics ph,
+__global__ void __launch_bounds__(128, 8) cellphase_kernel(CellPhaseArgs<R> a, Physics ph,
                                                         const __grid_constant__ ParamTables p) {
     CellPhaseArgs<R> b = a;
     b.tab = param_tab<R>(p);
     cellphase_cell(b, ph, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 template <class R>
-__global__ void __launch_bounds__(128) face_kernel(FaceArgs<R> a, Physics ph, const __grid_constant__ ParamTables p) {
+__global__ void __launch_bounds__(128, 5) face_kernel(FaceArgs<R> a, Physics ph, const __grid_constant__ ParamTables p) {
     FaceArgs<R> b = a;
     b.tab = param_tab<R>(p);
     face_edge(b, ph, (long long)blockIdx.x * blockDim.x + threadIdx.x);
