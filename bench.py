@@ -41,12 +41,13 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(nx=1280, ny=2560)
 ALG_BYTES_PER_CELL_STAGE = 144          # read U^(k), U^n; write U^(k+1); 2 faces x 5 q x 8 B v_s.n; write T, phi
 # Executed FP64 operations per cell per stage (DFMA counted as 2, DADD/DMUL
-# as 1) of the four stage kernels, from the ncu capture summarised in
-# profiles/transport_stage_full_640x1280.md (per-cell figures are size-independent).
-FP64_FLOPS_PER_CELL_STAGE = 6637
+# as 1) of the stage kernels, from the ncu capture summarised in
+# profiles/transport_stage_full_640x1280.md: reconstruction 2073, cell phase
+# 1188, faces 1703, accumulation ~48 (per-cell figures are size-independent).
+FP64_FLOPS_PER_CELL_STAGE = 5012
 # DRAM bytes per cell per stage of the four stage kernels from the same capture
 # (640x1280 keeps every stage array above L2 size; traffic scales with cells).
-DRAM_BYTES_PER_CELL_STAGE = 900
+DRAM_BYTES_PER_CELL_STAGE = 924
 CPU_SAMPLE = dict(nx=160, ny=320)
 CPU_SECONDS = 12.0
 
@@ -61,12 +62,18 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks/throttle reasons sampled every 20 ms.
+
+    The sampler starts before the timed region and waits for its first
+    sample; each line is timestamped on arrival, and `summary` keeps the
+    samples that arrived between `mark_start` and `mark_end`.
+    """
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.lines = []
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -74,17 +81,26 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.monotonic() + 5.0
+            while not self.lines and time.monotonic() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def mark_start(self):
+        self.t0 = time.monotonic()
+
+    def mark_end(self):
+        self.t1 = time.monotonic()
 
     def __exit__(self, *a):
         if self.proc:
@@ -97,7 +113,11 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        lo = self.t0 if self.t0 is not None else -float("inf")
+        hi = (self.t1 + 0.025) if self.t1 is not None else float("inf")
+        for ts, line in self.lines:
+            if not (lo <= ts <= hi):
+                continue
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -304,10 +324,13 @@ def run_gpu(args, world, rank, local):
     launches0 = _capi.kernel_launches()
     barrier()
     with ClockSampler(local) as clk:
+        barrier()
+        clk.mark_start()
         e0.record(stream)
         _, reps = t.step(args.steps)
         e1.record(stream)
         torch.cuda.synchronize()
+        clk.mark_end()
     launches = _capi.kernel_launches() - launches0
     ms = e0.elapsed_time(e1)
     kms = (C.c_double * 6)()
@@ -403,7 +426,7 @@ def run_gpu(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mantlepar_b200", choices=["mantlepar_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
