@@ -285,7 +285,7 @@ def run_forms(args, stream):
             "requests": out["requests"], "arrival_span_s": reqs[-1].arrival, "wall_s": out["wall_s"],
             "gpu_busy_value": out["gpu_busy_value"], "all_ok": out["all_ok"],
             "admission": "smallest estimated work first, 4e6 resident cells, 64 GiB budget",
-            "note": "latency = completion - submission; the first requests of the stream; 200 req/s offers about 2000x one GPU's capacity, so queueing dominates p99"}
+            "note": "latency = completion - submission; the first requests of the stream; 200 req/s offers about 500x one GPU's capacity, so queueing dominates"}
     return forms
 
 
