@@ -100,11 +100,34 @@ mp_status mp_phase_boundaries(const mp_phase_model* model, double C, double P, m
  * .cpp:192-282) on the GPU. H, C, P are device arrays of length n; P may be
  * NULL, then P_const applies to every point. Returns the status of the
  * lowest failing index (written to *first_bad, -1 if none). Synchronous on
- * `stream`. On failure the failing points hold NaN (region 0) and the other
- * points hold their values. */
+ * `stream`. On failure the failing points hold NaN and the other points
+ * hold their values; a failing point's region is the selected region when
+ * the failure came after region selection (fractions or temperatures of the
+ * evaluation itself), else 0 (invalid input, unresolvable intervals). */
 mp_status mp_phase_evaluate_batch(const mp_phase_model* model, const double* H, const double* C,
                                   const double* P, double P_const, size_t n,
                                   const mp_phase_soa* out, long long* first_bad, mp_stream_t stream);
+
+/* mp_phase_evaluate_batch for callers holding host memory only (the
+ * reference's C++ code has no CUDA): H, C, P and every non-NULL field of
+ * `out` are HOST arrays of length n; inputs are staged through device memory
+ * owned by the model. Same statuses and failure semantics as the batch call.
+ * Calls on one model are serialised. Replaces EutecticModel::evaluate /
+ * classify (src/phase/eutectic_rescaled.h:114-115) for host callers. */
+mp_status mp_phase_evaluate_host(const mp_phase_model* model, const double* H, const double* C,
+                                 const double* P, double P_const, size_t n,
+                                 const mp_phase_soa* out, long long* first_bad);
+
+/* Replaces EutecticModel::pressureCorrectedTemperature
+ * (src/phase/eutectic_rescaled.h:128, .cpp:143-149): TD + P/nu/dT with long
+ * double intermediates. Non-finite input -> MP_ERR_PHASE_INVALID; an
+ * unrepresentable result -> MP_ERR_PHASE_OVERFLOW. */
+mp_status mp_phase_pressure_corrected_temperature(const mp_phase_model* model, double TD, double P, double* out);
+
+/* Replaces EutecticModel::staticPressure (src/phase/eutectic_rescaled.h:129-130,
+ * .cpp:151-161): rho*g*zD*length_scale; the one-argument reference form is
+ * length_scale = derived l0. length_scale must be finite and positive. */
+mp_status mp_phase_static_pressure(const mp_phase_model* model, double zD, double length_scale, double* out);
 
 /* ------------------------------------------------------------- transport */
 

@@ -103,6 +103,9 @@ def lib() -> C.CDLL:
         "mp_phase_destroy": (None, [vp]),
         "mp_phase_boundaries": (i, [vp, d, d, C.POINTER(Bounds)]),
         "mp_phase_evaluate_batch": (i, [vp, vp, vp, vp, d, sz, C.POINTER(PhaseSoA), C.POINTER(C.c_longlong), vp]),
+        "mp_phase_evaluate_host": (i, [vp, vp, vp, vp, d, sz, C.POINTER(PhaseSoA), C.POINTER(C.c_longlong)]),
+        "mp_phase_pressure_corrected_temperature": (i, [vp, d, d, dp]),
+        "mp_phase_static_pressure": (i, [vp, d, d, dp]),
         "mp_transport_create": (i, [C.POINTER(MeshDesc), C.POINTER(TransportOpts), vp, C.POINTER(vp)]),
         "mp_transport_destroy": (None, [vp]),
         "mp_transport_set_face_velocity": (i, [vp, vp, vp]),

@@ -1,11 +1,14 @@
 """Build the mantlepar_b200 CUDA library in-tree for sm_100a.
 
     python -m mantlepar_b200.build        # -> mantlepar_b200/libmantlepar_b200.so
+                                          #    mantlepar_b200/libmantle_b200_host.so
 
 Every translation unit is compiled by nvcc with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` and linked into one
 shared library (static CUDA runtime) that exports the C ABI of
-include/mantlepar/mp.h.
+include/mantlepar/mp.h. The C++ host layer (include/mantle/phase/
+eutectic_rescaled.h, mantlepar_b200/host/) is compiled by g++ into a second
+library linked against the first.
 """
 from __future__ import annotations
 
@@ -20,6 +23,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmantlepar_b200.so")
+# C++ host layer (mantle::phase::EutecticModel over the C ABI), linked to LIB.
+HOST_LIB = os.path.join(HERE, "libmantle_b200_host.so")
+HOST_SOURCES = [os.path.join(HERE, "host", "eutectic_model.cpp")]
 
 SOURCES = ["phase_api.cu", "transport.cu", "tables.cpp", "mp_noalloc.cu", "batch.cu", "serve.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -51,6 +57,9 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "mantlepar", "mp.h")]
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
+        hdeps = HOST_SOURCES + [LIB, os.path.join(ROOT, "include", "mantle", "phase", "eutectic_rescaled.h")]
+        if not os.path.exists(HOST_LIB) or os.path.getmtime(HOST_LIB) < max(os.path.getmtime(d) for d in hdeps):
+            build_host()
         return LIB
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
@@ -58,7 +67,19 @@ def build(verbose: bool = False, force: bool = False) -> str:
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_host()
     return LIB
+
+
+def build_host() -> str:
+    """Compile the C++ host layer (g++, C++17) against the CUDA library."""
+    cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall",
+           "-I", os.path.join(ROOT, "include"), *HOST_SOURCES, "-o", HOST_LIB,
+           "-L", HERE, "-l:libmantlepar_b200.so", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host layer build failed:\n{r.stdout}\n{r.stderr}")
+    return HOST_LIB
 
 
 if __name__ == "__main__":

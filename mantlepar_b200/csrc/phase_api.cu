@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <string>
 
 namespace mp {
@@ -104,10 +105,12 @@ __global__ void phase_batch_kernel(PhaseConst k, const double* __restrict__ H, c
         int st = st0;
         if (P) st = eutectic_temperature(k, P[i], Tep);
         PhaseOut s;
+        s.region = 0;   // set by phase_eval once the region is selected
         if (!st) st = phase_eval(k, H[i], C[i], Tep, s);
         if (st) {
+            // The region stays when the failure came after its selection.
             s.phi1 = s.phi2 = s.phil = s.cl = s.cs = s.T = s.Tep = s.dTdC = s.dTdH = nan;
-            s.region = 0; s.flags = 0;
+            s.flags = 0;
             atomicMin(first_bad, ((unsigned long long)i << 8) | (unsigned long long)st);
         }
         if (out.phi1) out.phi1[i] = s.phi1;
@@ -145,6 +148,12 @@ struct mp_phase_model {
     mp::PhaseConst k;
     unsigned long long* d_bad = nullptr;   // device word for the first failing index
     unsigned long long* h_bad = nullptr;   // pinned mirror
+    // mp_phase_evaluate_host: device staging of host inputs/outputs, grown on
+    // demand and serialised per model (evaluate() is const and may be called
+    // from several threads).
+    std::mutex host_lock;
+    unsigned char* d_stage = nullptr;
+    size_t stage_bytes = 0;
 };
 
 extern "C" const char* mp_last_error_string(void) { return mp::g_error.c_str(); }
@@ -188,6 +197,7 @@ extern "C" void mp_phase_destroy(mp_phase_model* m) {
     if (!m) return;
     if (m->d_bad) cudaFree(m->d_bad);
     if (m->h_bad) cudaFreeHost(m->h_bad);
+    if (m->d_stage) cudaFree(m->d_stage);
     delete m;
 }
 
@@ -230,4 +240,85 @@ extern "C" mp_status mp_phase_evaluate_batch(const mp_phase_model* m, const doub
     if (first_bad) *first_bad = idx;
     mp::set_error("point %lld: %s", idx, mp::phase_message(code));
     return (mp_status)code;
+}
+
+extern "C" mp_status mp_phase_evaluate_host(const mp_phase_model* mc, const double* H, const double* C, const double* P,
+                                            double P_const, size_t n, const mp_phase_soa* out, long long* first_bad) {
+    if (!mc || !out || (n && (!H || !C))) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (first_bad) *first_bad = -1;
+    if (n == 0) return MP_OK;
+    mp_phase_model* m = const_cast<mp_phase_model*>(mc);
+    std::lock_guard<std::mutex> g(m->host_lock);
+    // Staging: H, C, P, then the nine double fields, then region and flags.
+    const size_t dbl = n * sizeof(double);
+    const size_t need = 12 * dbl + 2 * n;
+    if (m->stage_bytes < need) {
+        if (m->d_stage) cudaFree(m->d_stage);
+        m->d_stage = nullptr;
+        m->stage_bytes = 0;
+        MP_CUDA(cudaMalloc(&m->d_stage, need));
+        m->stage_bytes = need;
+    }
+    double* dH = reinterpret_cast<double*>(m->d_stage);
+    double* dC = dH + n;
+    double* dP = dC + n;
+    double* fields = dP + n;
+    int8_t* dregion = reinterpret_cast<int8_t*>(fields + 9 * n);
+    uint8_t* dflags = reinterpret_cast<uint8_t*>(dregion + n);
+    MP_CUDA(cudaMemcpy(dH, H, dbl, cudaMemcpyHostToDevice));
+    MP_CUDA(cudaMemcpy(dC, C, dbl, cudaMemcpyHostToDevice));
+    if (P) MP_CUDA(cudaMemcpy(dP, P, dbl, cudaMemcpyHostToDevice));
+    double* const* hsrc[9] = {&out->phi1, &out->phi2, &out->phil, &out->cl, &out->cs,
+                              &out->TDp, &out->Tep, &out->dTD_dCD, &out->dTD_dHD};
+    mp_phase_soa d{};
+    double** dst[9] = {&d.phi1, &d.phi2, &d.phil, &d.cl, &d.cs, &d.TDp, &d.Tep, &d.dTD_dCD, &d.dTD_dHD};
+    for (int k = 0; k < 9; ++k) *dst[k] = *hsrc[k] ? fields + k * n : nullptr;
+    d.region = out->region ? dregion : nullptr;
+    d.flags = out->flags ? dflags : nullptr;
+    long long bad = -1;
+    const mp_status st = mp_phase_evaluate_batch(m, dH, dC, P ? dP : nullptr, P_const, n, &d, &bad, nullptr);
+    if (st != MP_OK && bad < 0) return st;   // launch/runtime failure: nothing was evaluated
+    const std::string msg = st != MP_OK ? mp_last_error_string() : std::string();
+    for (int k = 0; k < 9; ++k)
+        if (*hsrc[k]) MP_CUDA(cudaMemcpy(*hsrc[k], fields + k * n, dbl, cudaMemcpyDeviceToHost));
+    if (out->region) MP_CUDA(cudaMemcpy(out->region, dregion, n, cudaMemcpyDeviceToHost));
+    if (out->flags) MP_CUDA(cudaMemcpy(out->flags, dflags, n, cudaMemcpyDeviceToHost));
+    if (first_bad) *first_bad = bad;
+    if (st != MP_OK) mp::set_error("%s", msg.c_str());
+    return st;
+}
+
+namespace {
+// The reference's requireFinite / requirePositive / checkedDouble
+// (eutectic_rescaled.cpp:13-32) as status codes.
+mp_status need_finite(double v, const char* name) {
+    if (std::isfinite(v)) return MP_OK;
+    mp::set_error("%s must be finite", name);
+    return MP_ERR_PHASE_INVALID;
+}
+mp_status checked_out(long double v, const char* name, double* out) {
+    if (!std::isfinite(v) || std::fabs(v) > (long double)std::numeric_limits<double>::max()) {
+        mp::set_error("%s is not representable", name);
+        return MP_ERR_PHASE_OVERFLOW;
+    }
+    *out = (double)v;
+    return MP_OK;
+}
+}  // namespace
+
+extern "C" mp_status mp_phase_pressure_corrected_temperature(const mp_phase_model* m, double TD, double P,
+                                                             double* out) {
+    if (!m || !out) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    MP_TRY(need_finite(TD, "TD"));
+    MP_TRY(need_finite(P, "P"));
+    const long double shift = (long double)P / m->params.nu / m->derived.dT;
+    return checked_out((long double)TD + shift, "pressure-corrected temperature", out);
+}
+
+extern "C" mp_status mp_phase_static_pressure(const mp_phase_model* m, double zD, double length_scale, double* out) {
+    if (!m || !out) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    MP_TRY(need_finite(zD, "zD"));
+    MP_TRY(need_finite(length_scale, "length_scale"));
+    if (length_scale <= 0.0) { mp::set_error("length_scale must be positive"); return MP_ERR_PHASE_INVALID; }
+    return checked_out((long double)m->params.rho * m->params.g * zD * length_scale, "static pressure", out);
 }

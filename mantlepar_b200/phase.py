@@ -146,5 +146,22 @@ class EutecticModel:
                           has_liquid=bool(flags & 2), finite_temperature_derivatives=bool(flags & 4))
 
     def classify(self, HD: float, CD: float, P: float) -> int:
-        out, _, _ = self.evaluate_batch(np.array([HD]), np.array([CD]), np.array([P]), fields=["region"])
-        return int(out["region"].cpu().numpy()[0])
+        """Region only (eutectic_rescaled.cpp:187-190): a failure of the
+        evaluation after the region was selected still returns the region."""
+        out, code, _ = self.evaluate_batch(np.array([HD]), np.array([CD]), np.array([P]), fields=["region"],
+                                           raise_on_error=False)
+        region = int(out["region"].cpu().numpy()[0])
+        if code and not (region and code in (102, 103)):
+            _raise(code)
+        return region
+
+    def pressureCorrectedTemperature(self, TD: float, P: float) -> float:
+        v = C.c_double(0.0)
+        _raise(self._lib.mp_phase_pressure_corrected_temperature(self._h, float(TD), float(P), C.byref(v)))
+        return v.value
+
+    def staticPressure(self, zD: float, length_scale: float | None = None) -> float:
+        ls = self.derived()["l0"] if length_scale is None else float(length_scale)
+        v = C.c_double(0.0)
+        _raise(self._lib.mp_phase_static_pressure(self._h, float(zD), ls, C.byref(v)))
+        return v.value

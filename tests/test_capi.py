@@ -27,3 +27,22 @@ def test_build_targets_sm100a_only():
     from mantlepar_b200 import build
     assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
     assert "-lineinfo" in build.FLAGS
+
+
+def test_host_layer_exports_the_phase_model_interface(cuda_lib):
+    """The C++ host layer exports mantle::phase::EutecticModel's members and
+    links against the CUDA library (no evaluation without a GPU)."""
+    from mantlepar_b200 import build
+    assert os.path.exists(build.HOST_LIB)
+    out = subprocess.run(["nm", "-DC", "--defined-only", build.HOST_LIB], capture_output=True, text=True).stdout
+    for member in ["EutecticModel::EutecticModel(mantle::phase::MaterialParameters const&)",
+                   "EutecticModel::evaluate(double, double, double) const",
+                   "EutecticModel::classify(double, double, double) const",
+                   "EutecticModel::boundaries(double, double) const",
+                   "EutecticModel::setParameters(mantle::phase::MaterialParameters const&)",
+                   "EutecticModel::pressureCorrectedTemperature(double, double) const",
+                   "EutecticModel::staticPressure(double, double) const",
+                   "EutecticModel::printInfo(std::ostream&) const"]:
+        assert "mantle::phase::" + member in out, member
+    deps = subprocess.run(["ldd", build.HOST_LIB], capture_output=True, text=True).stdout
+    assert "libmantlepar_b200.so" in deps

@@ -150,3 +150,26 @@ def test_large_batch_against_oracle(models):
     assert code == 0
     for f in ["phil", "TDp", "cl", "cs"]:
         assert np.max(rel_err(g[f][idx], ref[f])) <= RTOL, f
+
+
+def test_scalar_helpers_and_classify(models):
+    """pressureCorrectedTemperature / staticPressure (eutectic_rescaled.cpp:143-161)
+    and classify's region-only semantics (:187-190)."""
+    m = models[0]
+    p, d = m.parameters(), m.derived()
+    for P in ka.PRESSURES:
+        assert math.isclose(m.pressureCorrectedTemperature(2.0, P), 2.0 + P / p.nu / d["dT"], rel_tol=1e-15)
+    assert m.staticPressure(0.0) == 0.0
+    assert math.isclose(m.staticPressure(0.5), p.rho * p.g * 0.5 * d["l0"], rel_tol=1e-15)
+    assert math.isclose(m.staticPressure(0.5, 1000.0), p.rho * p.g * 500.0, rel_tol=1e-15)
+    with pytest.raises(ValueError):
+        m.pressureCorrectedTemperature(math.nan, 0.0)
+    with pytest.raises(ValueError):
+        m.staticPressure(0.5, 0.0)
+    with pytest.raises(OverflowError):
+        m.staticPressure(1e300, 1e300)
+    b = m.boundaries(0.4 * p.Xe, 0.0)
+    assert m.classify(b.Tep, 0.4 * p.Xe, 0.0) == 2
+    assert m.classify(math.nextafter(b.Tep, math.inf), 0.4 * p.Xe, 0.0) == 3
+    with pytest.raises(ValueError):
+        m.classify(0.5, 2.0, 0.0)
