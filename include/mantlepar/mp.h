@@ -202,6 +202,20 @@ mp_status mp_transport_rhs(mp_transport* t, double* rhsH, double* rhsC, double* 
  * is rolled back to the last accepted step (evolve.cpp:493-499). */
 mp_status mp_transport_step(mp_transport* t, int nsteps, mp_step_report* reports);
 
+/* Time controls of the coupled loop (src/couple/evolve.cpp:449-457,483;
+ * TimeInput in src/input/input.h:154-158). MP_TIME_CFL (default): dt =
+ * min(remaining, first step ? dt_initial : dt_max, cfl / stage rate), halved
+ * on a failed stage (<= 40 retries). MP_TIME_FIXED: dt = min(remaining,
+ * dt_initial); MP_ERR_ARG_OUTOFRANGE when that exceeds the CFL bound or a
+ * stage fails. t_end (INFINITY = none): the last step is shortened to land
+ * on it and mp_transport_step stops there (report entries of steps not taken
+ * have dt = 0 and time = t_end). */
+enum { MP_TIME_CFL = 0, MP_TIME_FIXED = 1 };
+mp_status mp_transport_set_time_control(mp_transport* t, int control, double t_end);
+
+/* Current time and accepted steps (InitialState::time, acceptedSteps). */
+mp_status mp_transport_get_time(const mp_transport* t, double* time, int* accepted);
+
 /* Limiter factors theta_H, theta_C of the current state
  * (StateReconstruction::Limit, src/couple/state_reconstruction.cpp:136-192). */
 mp_status mp_transport_limiter(mp_transport* t, double* thetaH, double* thetaC);

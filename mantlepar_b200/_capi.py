@@ -141,6 +141,8 @@ def lib() -> C.CDLL:
         "mp_serve_stats": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "mp_serve_set_policy": (i, [vp, i, d]),
+        "mp_transport_set_time_control": (i, [vp, i, d]),
+        "mp_transport_get_time": (i, [vp, dp, C.POINTER(C.c_int)]),
         "mp_batch_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
     }
     for name, (res, args) in sig.items():

@@ -25,7 +25,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmantlepar_b200.so")
 # C++ host layer (mantle::phase::EutecticModel over the C ABI), linked to LIB.
 HOST_LIB = os.path.join(HERE, "libmantle_b200_host.so")
-HOST_SOURCES = [os.path.join(HERE, "host", "eutectic_model.cpp")]
+HOST_SOURCES = [os.path.join(HERE, "host", "eutectic_model.cpp"), os.path.join(HERE, "host", "coupled_transport.cpp")]
 
 SOURCES = ["phase_api.cu", "transport.cu", "tables.cpp", "mp_noalloc.cu", "batch.cu", "serve.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -57,7 +57,8 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "mantlepar", "mp.h")]
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
-        hdeps = HOST_SOURCES + [LIB, os.path.join(ROOT, "include", "mantle", "phase", "eutectic_rescaled.h")]
+        hdeps = HOST_SOURCES + [LIB, os.path.join(ROOT, "include", "mantle", "phase", "eutectic_rescaled.h"),
+                                os.path.join(ROOT, "include", "mantle", "couple", "coupled_transport.h")]
         if not os.path.exists(HOST_LIB) or os.path.getmtime(HOST_LIB) < max(os.path.getmtime(d) for d in hdeps):
             build_host()
         return LIB

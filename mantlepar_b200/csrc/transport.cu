@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 namespace mp {
@@ -122,6 +123,10 @@ struct mp_transport {
     double time = 0.0;
     int accepted = 0;
     bool have_L = false;
+    // Time controls (evolve.cpp:449-457, input TimeInput): end time the last
+    // step is shortened to land on, and the "fixed" control.
+    double t_end = INFINITY;
+    bool fixed = false;
     mp::Totals curTot{};                   // totals of L(U^n)
     // Optional per-kernel timing (CUDA events on this handle's stream).
     bool profile = false;
@@ -281,16 +286,22 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
     const double Xe = o.material.Xe;
     const Totals first = t->curTot;
     const double oldHI = first.HI, oldCI = first.CI;
-    const double cap = t->accepted == 0 ? o.dt_initial : o.dt_max;
+    const double remaining = t->t_end - t->time;
+    const double cap = t->fixed ? o.dt_initial : (t->accepted == 0 ? o.dt_initial : o.dt_max);
     const double limit = first.maxRate > 0 ? o.cfl / first.maxRate : o.dt_max;
-    double dt = std::min(cap, limit);
+    double dt = std::min(remaining, cap);
+    if (t->fixed && !(dt <= limit * (1 + 1e-12))) {
+        set_error("Fixed time step exceeds the phase-coupled CFL bound; use control: cfl");
+        return MP_ERR_ARG_OUTOFRANGE;
+    }
+    if (!t->fixed) dt = std::min(dt, limit);
     const double start = t->time;
     int retries = 0;
     double courant = 0.0;
     Totals second{}, third{}, fin{};
     const int nblk_axpy = (int)((t->N + kSumCells - 1) / kSumCells);
     for (;;) {
-        if (!(dt >= o.dt_min && retries < 40)) {
+        if (!(dt >= std::min(remaining, o.dt_min) && retries < 40)) {
             set_error("Coupled step cannot satisfy admissibility/CFL above minimum step");
             return MP_ERR_NOT_CONVERGED;
         }
@@ -332,6 +343,10 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
             fin = second;
         }
         if (valid) break;
+        if (t->fixed) {
+            set_error("Fixed coupled step failed stage admissibility/CFL");
+            return MP_ERR_ARG_OUTOFRANGE;
+        }
         dt *= 0.5;
         ++retries;
     }
@@ -494,6 +509,15 @@ extern "C" mp_status mp_transport_step(mp_transport* t, int nsteps, mp_step_repo
     if (!t) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (nsteps < 0) { mp::set_error("nsteps must be nonnegative"); return MP_ERR_ARG_OUTOFRANGE; }
     for (int k = 0; k < nsteps; ++k) {
+        // At the end time (within 32 ulp of it, evolve.cpp:450-451) stepping stops;
+        // the remaining reports keep dt = 0 and the end time.
+        if (std::isfinite(t->t_end) &&
+            t->t_end - t->time <= 32 * std::numeric_limits<double>::epsilon() * std::max(1.0, std::fabs(t->t_end))) {
+            t->time = t->t_end;
+            if (reports)
+                for (int r = k; r < nsteps; ++r) { reports[r] = mp_step_report{}; reports[r].time = t->time; }
+            return MP_OK;
+        }
         mp_step_report rep{};
         const double t0 = t->time;
         const mp_status s = mp::do_step(t, rep);
@@ -506,6 +530,26 @@ extern "C" mp_status mp_transport_step(mp_transport* t, int nsteps, mp_step_repo
         }
         if (reports) reports[k] = rep;
     }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_transport_set_time_control(mp_transport* t, int control, double t_end) {
+    if (!t) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (control != MP_TIME_CFL && control != MP_TIME_FIXED) { mp::set_error("unknown time control %d", control); return MP_ERR_ARG_OUTOFRANGE; }
+    if (std::isnan(t_end)) { mp::set_error("end time must not be NaN"); return MP_ERR_ARG_OUTOFRANGE; }
+    if (control == MP_TIME_FIXED && !(t->opts.dt_initial > 0 && std::isfinite(t->opts.dt_initial))) {
+        mp::set_error("fixed control needs a positive finite dt_initial");
+        return MP_ERR_ARG_OUTOFRANGE;
+    }
+    t->fixed = control == MP_TIME_FIXED;
+    t->t_end = t_end;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_transport_get_time(const mp_transport* t, double* time, int* accepted) {
+    if (!t) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (time) *time = t->time;
+    if (accepted) *accepted = t->accepted;
     return MP_OK;
 }
 

@@ -118,6 +118,17 @@ class Transport:
         _capi.check(self._lib.mp_transport_limiter(self._h, _ptr(a), _ptr(b)))
         return a, b
 
+    CFL, FIXED = 0, 1
+
+    def set_time_control(self, control: int, t_end: float = float("inf")):
+        """time.control ("cfl" = CFL, "fixed" = FIXED) and time.end of the coupled loop."""
+        _capi.check(self._lib.mp_transport_set_time_control(self._h, int(control), float(t_end)))
+
+    def get_time(self):
+        t, n = C.c_double(0.0), C.c_int(0)
+        _capi.check(self._lib.mp_transport_get_time(self._h, C.byref(t), C.byref(n)))
+        return t.value, n.value
+
     def step(self, nsteps: int, raise_on_error: bool = True):
         reps = (_capi.StepReport * max(1, nsteps))()
         code = self._lib.mp_transport_step(self._h, int(nsteps), reps)

@@ -106,6 +106,9 @@ int orc_transport_rhs(orc_transport* t, double* rhsH, double* rhsC, double* T, d
                       double* rate, orc_step_report* rates);
 /* Advance nsteps accepted steps. */
 int orc_transport_step(orc_transport* t, int nsteps, orc_step_report* report);
+/* Time controls of evolve.cpp:449-457,483: control 0 = cfl, 1 = fixed (dt =
+ * dt_initial); t_end = INFINITY for none (the last step lands on t_end). */
+int orc_transport_set_time_control(orc_transport* t, int control, double t_end);
 int orc_transport_limiter(orc_transport* t, double* thetaH, double* thetaC);
 
 /* Synthetic input builders shared by tests and bench (SplitMix64 noise as in

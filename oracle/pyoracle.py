@@ -84,8 +84,9 @@ class _Lib:
         t("create").restype = C.c_void_p
         t("create").argtypes = [C.POINTER(Material), C.POINTER(TransportOpts)]
         t("destroy").argtypes = [C.c_void_p]
-        for n in ["set_face_velocity", "set_state", "get_state", "rhs", "limiter", "step"]:
+        for n in ["set_face_velocity", "set_state", "get_state", "rhs", "limiter", "step", "set_time_control"]:
             t(n).restype = C.c_int
+        t("set_time_control").argtypes = [C.c_void_p, C.c_int, C.c_double]
         t("set_face_velocity").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         t("set_state").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double]
         t("get_state").argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 4
@@ -227,6 +228,9 @@ class TransportOracle:
         a, b = np.zeros(n), np.zeros(n)
         code = self.lib.f("transport_limiter")(self.h, _dptr(a), _dptr(b))
         return code, a, b
+
+    def set_time_control(self, control: int, t_end: float = float("inf")):
+        return self.lib.f("transport_set_time_control")(self.h, int(control), float(t_end))
 
     def step(self, nsteps: int):
         reps = (StepReport * max(1, nsteps))()

@@ -205,5 +205,6 @@ int ref_transport_rhs(void* t, double* a, double* b, double* T, double* phi, dou
 }
 int ref_transport_limiter(void* t, double* a, double* b) { return RefApi::limiter(t, a, b); }
 int ref_transport_step(void* t, int n, orc_step_report* r) { return RefApi::step(t, n, r); }
+int ref_transport_set_time_control(void* t, int control, double t_end) { return RefApi::set_time_control(t, control, t_end); }
 
 }  // extern "C"

@@ -29,6 +29,7 @@
 #include <cstring>
 #include <memory>
 #include <thread>
+#include <limits>
 #include <vector>
 
 namespace orc {
@@ -89,6 +90,9 @@ struct Driver {
     std::vector<double> rhsH, rhsC, rate, divg;
     double time = 0;
     int accepted = 0;
+    // Time controls (evolve.cpp:449-457,483): end time and the "fixed" control.
+    double t_end = INFINITY;
+    bool fixed = false;
     int nq = 5;
     int samples_n = 4;
     double samples_frac = 0.9;
@@ -470,11 +474,15 @@ struct Driver {
     // evolve.cpp:428-511 (SSPRK2) and the Shu-Osher SSPRK3 form of the same loop.
     void step(orc_step_report& rep) {
         if (!have_current) { oldH = H; oldC = C; current = rhs(); have_current = true; }
-        const double dt_cap = accepted == 0 ? o.dt_initial : o.dt_max;
+        const double remaining = t_end - time;
         const double start = time;
         const double oldHI = integral(H), oldCI = integral(C);
+        // evolve.cpp:454-457
+        double dt = std::min(remaining, fixed ? o.dt_initial : (accepted == 0 ? o.dt_initial : o.dt_max));
         const double limit = current.maximumRate > 0 ? o.cfl / current.maximumRate : o.dt_max;
-        double dt = std::min(dt_cap, limit);
+        require(!fixed || dt <= limit * (1 + 1e-12), E_OUTOFRANGE,
+                "Fixed time step exceeds the phase-coupled CFL bound; use control: cfl");
+        if (!fixed) dt = std::min(dt, limit);
         const std::vector<double> firstH = rhsH, firstC = rhsC;
         const Rates first = current;
         Rates second, third;
@@ -482,7 +490,8 @@ struct Driver {
         double courant = 0;
         std::vector<double> U1H, U1C;
         for (;;) {
-            require(dt >= o.dt_min && retries < 40, E_NOT_CONVERGED, "Coupled step cannot satisfy admissibility/CFL above minimum step");
+            require(dt >= std::min(remaining, o.dt_min) && retries < 40, E_NOT_CONVERGED,
+                    "Coupled step cannot satisfy admissibility/CFL above minimum step");
             for (int k = 0; k < ncell; ++k) { H[k] = oldH[k] + dt * firstH[k]; C[k] = oldC[k] + dt * firstC[k]; }
             time = start + dt;
             bool valid = admissible();
@@ -518,6 +527,7 @@ struct Driver {
                 valid = admissible();
             }
             if (valid) break;
+            require(!fixed, E_OUTOFRANGE, "Fixed coupled step failed stage admissibility/CFL");
             dt *= .5; ++retries;
         }
         const double HI = integral(H), CI = integral(C);
@@ -608,9 +618,25 @@ struct Api {
             return 0;
         } catch (const Error& e) { return e.code; }
     }
+    static int set_time_control(void* h, int control, double t_end) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        if (control != 0 && control != 1) return E_OUTOFRANGE;
+        d.fixed = control == 1;
+        d.t_end = t_end;
+        return 0;
+    }
+
     static int step(void* h, int nsteps, orc_step_report* report) {
         auto& d = static_cast<Handle<B>*>(h)->d;
         for (int s = 0; s < nsteps; ++s) {
+            // evolve.cpp:450-451: at the end time (within 32 ulp) the loop stops.
+            if (std::isfinite(d.t_end) &&
+                d.t_end - d.time <= 32 * std::numeric_limits<double>::epsilon() * std::max(1.0, std::fabs(d.t_end))) {
+                d.time = d.t_end;
+                if (report)
+                    for (int r = s; r < nsteps; ++r) { report[r] = orc_step_report{}; report[r].time = d.time; }
+                return 0;
+            }
             const double t0 = d.time;
             std::vector<double> h0 = d.H, c0 = d.C;
             try {

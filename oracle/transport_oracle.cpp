@@ -125,6 +125,9 @@ extern "C" int orc_transport_limiter(orc_transport* t, double* thetaH, double* t
 extern "C" int orc_transport_step(orc_transport* t, int nsteps, orc_step_report* report) {
     return RestatedApi::step(t, nsteps, report);
 }
+extern "C" int orc_transport_set_time_control(orc_transport* t, int control, double t_end) {
+    return RestatedApi::set_time_control(t, control, t_end);
+}
 
 // Synthetic-input noise: SplitMix64 keyed like src/core/mesh.cpp:40-44
 // (seed + 2*index + component), here index = cell id, component = field.

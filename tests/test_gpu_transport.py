@@ -141,3 +141,50 @@ def test_invalid_configurations_are_rejected(cuda_lib):
         Transport(sy.Workload(nx=4, ny=4), TransportConfig(cfl=1.5))
     with pytest.raises(MPError):
         Transport(sy.Workload(nx=4, ny=4), TransportConfig(diffusivity=1e-3))
+
+
+@pytest.mark.parametrize("control", [0, 1], ids=["cfl", "fixed"])
+def test_time_controls_match_oracle(cuda_lib, control):
+    """time.end and time.control (evolve.cpp:449-457,483) against the oracle:
+    the same dt sequence, the last step landing on the end time, the same state."""
+    from oracle import pyoracle as po
+    from mantlepar_b200.transport import Transport, TransportConfig
+    w = CASES["w20"]
+    dt0 = 2e-4 if control == 1 else 1e30
+    t = Transport(w, TransportConfig(cfl=w.cfl, integrator=3, dt_initial=dt0))
+    o = po.TransportOracle(sy.material_s(), w, integrator=3, dt_initial=dt0)
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    for x in (t, o):
+        x.set_face_velocity(vs, ud)
+        x.set_state(H, C)
+    t_end = 0.0071
+    t.set_time_control(control, t_end)
+    assert o.set_time_control(control, t_end) == 0
+    _, got = t.step(80)
+    code, ref = o.step(80)
+    assert code == 0
+    assert [r["retries"] for r in got] == [r["retries"] for r in ref]
+    assert rel(np.array([r["dt"] for r in got]) + 1e-300, np.array([r["dt"] for r in ref]) + 1e-300) <= RTOL_RUN10
+    time, accepted = t.get_time()
+    assert time == t_end and accepted == sum(1 for r in ref if r["dt"] > 0)
+    a, b = np.stack(t.get_state()), np.stack(o.get_state())
+    for k in range(4):
+        assert rel(a[k], b[k]) <= 1e-11, k
+
+
+def test_fixed_step_above_cfl_bound_is_rejected(cuda_lib):
+    from mantlepar_b200._capi import MPError
+    from mantlepar_b200.transport import Transport, TransportConfig
+    w = CASES["w20"]
+    t = Transport(w, TransportConfig(cfl=w.cfl, integrator=2, dt_initial=1.0))
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    t.set_face_velocity(vs, ud)
+    t.set_state(H, C)
+    t.set_time_control(t.FIXED)
+    with pytest.raises(MPError) as err:
+        t.step(1)
+    assert err.value.code == 63
+    assert t.get_time() == (0.0, 0)
+    assert np.array_equal(t.get_state()[0], H)

@@ -93,3 +93,34 @@ def test_restated_equals_reference_on_new_seed():
     b = _oracle(w, 3, lib=po.reference())
     assert a.step(6)[0] == 0 and b.step(6)[0] == 0
     assert np.array_equal(bits(np.stack(a.get_state())), bits(np.stack(b.get_state())))
+
+
+def test_oracle_time_controls():
+    """evolve.cpp:449-457,483: the last step lands on time.end; the fixed
+    control keeps dt = initialStep with no retries and rejects a step above the
+    CFL bound."""
+    w = CASES["w20"]
+    t = _oracle(w, integrator=3)
+    t_end = 0.0123
+    assert t.set_time_control(0, t_end) == 0
+    code, reps = t.step(60)
+    assert code == 0
+    taken = [r for r in reps if r["dt"] > 0]
+    assert taken and taken[-1]["time"] == t_end and reps[-1]["time"] == t_end
+    assert all(r["dt"] == 0 for r in reps[len(taken):])
+    assert taken[-1]["dt"] < max(r["dt"] for r in taken)       # shortened last step
+    # fixed control below the CFL bound: constant dt, no retries
+    f = _oracle(w, integrator=2, dt_initial=2e-4)
+    assert f.set_time_control(1, 1e-3) == 0
+    code, reps = f.step(10)
+    assert code == 0
+    taken = [r for r in reps if r["dt"] > 0]
+    assert len(taken) == 5 and all(abs(r["dt"] - 2e-4) < 1e-18 for r in taken) and all(r["retries"] == 0 for r in taken)
+    # fixed control above the CFL bound: PETSC_ERR_ARG_OUTOFRANGE, state kept
+    g = _oracle(w, integrator=2, dt_initial=1.0)
+    g.set_time_control(1)
+    H0, C0, _, _ = g.get_state()
+    code, _ = g.step(1)
+    assert code == 63
+    H1, C1, _, _ = g.get_state()
+    assert np.array_equal(H0, H1) and np.array_equal(C0, C1)
