@@ -216,6 +216,39 @@ mp_status mp_transport_set_time_control(mp_transport* t, int control, double t_e
 /* Current time and accepted steps (InitialState::time, acceptedSteps). */
 mp_status mp_transport_get_time(const mp_transport* t, double* time, int* accepted);
 
+/* ------------------------------------------------------ row-slab domains */
+
+/* One row slab of a mesh decomposed across GPUs or processes (the reference
+ * partitions the cell DMDA, src/couple/state_reconstruction.cpp:40-58): the
+ * slab owns global rows [row_begin, row_end) and keeps up to two halo rows
+ * below and above (where the global mesh has them). Tables, boundary classes,
+ * physical walls and error keys use the global mesh, so a decomposed run
+ * reproduces the single-domain run cell by cell. Entry points on a slab:
+ *  - set_state / get_state / rhs / limiter take and return the OWNED rows
+ *    ((row_end - row_begin) * nx values);
+ *  - set_face_velocity takes the edges of the LOCAL mesh: nx x local_rows
+ *    cells starting at global row `row0` (mp_transport_slab_layout), in the
+ *    edge order of mantlepar/mp.h;
+ *  - before every stage the halo hook must fill the stage input's halo rows
+ *    from the neighbours' owned rows, and after every reduction the combine
+ *    hook must combine the totals and the status word across all slabs
+ *    (maxRate, divergence, Cmax, nonfinite: max; Hmin, Cmin: min; the others:
+ *    sum; status: min). Every slab must call the same entry points in the
+ *    same order. */
+typedef struct mp_stage_partials {
+    double maxRate, divergence, boundaryH, boundaryC, H_integral, C_integral, Hmin, Cmin, Cmax, nonfinite;
+} mp_stage_partials;
+/* H, C: the stage input (device, local rows); return 0 or a status. */
+typedef int (*mp_halo_fn)(void* user, double* H, double* C);
+typedef int (*mp_combine_fn)(void* user, mp_stage_partials* totals, unsigned long long* status);
+
+mp_status mp_transport_create_slab(const mp_mesh_desc* global_mesh, int row_begin, int row_end,
+                                   const mp_transport_opts* opts, mp_stream_t stream, mp_transport** out);
+/* local_rows: rows held (owned + halos); row0: global row of local row 0;
+ * own_begin/own_end: local rows owned. */
+mp_status mp_transport_slab_layout(const mp_transport* t, int* local_rows, int* row0, int* own_begin, int* own_end);
+mp_status mp_transport_set_hooks(mp_transport* t, mp_halo_fn halo, mp_combine_fn combine, void* user);
+
 /* Limiter factors theta_H, theta_C of the current state
  * (StateReconstruction::Limit, src/couple/state_reconstruction.cpp:136-192). */
 mp_status mp_transport_limiter(mp_transport* t, double* thetaH, double* thetaC);

@@ -52,6 +52,12 @@ struct Totals {
     double nonfinite;
 };
 
+// Row slabs of a decomposed mesh: the local arrays hold rows gj0 .. of a
+// global mesh of gny rows (gny = 0: the local mesh is the whole mesh).
+// Physical-boundary tests and error keys use global rows.
+template <class A>
+__device__ __forceinline__ int global_ny(const A& a) { return a.gny > 0 ? a.gny : a.ny; }
+
 // Status word: the smallest key wins. The key orders failures as the
 // reference's RHS meets them (evolve.cpp:279-384): reconstruction update,
 // limiter, porosity sampling, face loop, cell quadrature; then by cell/edge.
@@ -77,6 +83,7 @@ struct ReconArgs {
     unsigned char* flags;
     unsigned long long* status;
     double* theta;         // optional (2 * ncell): limiter factors for H, C
+    int gj0 = 0, gny = 0;  // slab: global row of local row 0, global rows
 };
 
 // Max/min of the deviation polynomial over the class's limiter points by
@@ -195,7 +202,9 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1);
-    const int cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
+    const int gj = a.gj0 + j, gny = global_ny(a);
+    const int cj = gj == 0 ? 0 : (gj == gny - 1 ? 2 : 1);
+    const long long key = cell + (long long)a.gj0 * nx;
     int st_lim = 0;
 
     double u[3][3];
@@ -256,8 +265,8 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
         a.rec[(size_t)(m + 9) * N + cell] = DC[m] * thC;
     }
     a.flags[cell] = safe ? 0 : FLAG_CHECK;
-    if (st) record_error(a.status, PART_UPDATE, cell, st);
-    if (st_lim) record_error(a.status, PART_LIMIT, cell, st_lim);
+    if (st) record_error(a.status, PART_UPDATE, key, st);
+    if (st_lim) record_error(a.status, PART_LIMIT, key, st_lim);
 }
 
 // ---------------------------------------------------------- cell phase kernel
@@ -273,6 +282,7 @@ struct CellPhaseArgs {
     double* T;
     double* phi;
     unsigned long long* status;
+    int gj0 = 0, gny = 0;  // slab: global row of local row 0, global rows
 };
 
 __device__ __forceinline__ void load_rec(const double* rec, size_t N, long long cell, double* DH, double* DC) {
@@ -319,9 +329,9 @@ __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const 
     const unsigned char fl = a.flags[cell];
     if (fl & FLAG_CHECK) {
         // Exact admissibility of the limited values at the diffusion samples.
-        const int i = (int)(cell % a.nx), j = (int)(cell / a.nx);
+        const int i = (int)(cell % a.nx), j = a.gj0 + (int)(cell / a.nx);
         const int ci = i == 0 ? 0 : (i == a.nx - 1 ? 2 : 1);
-        const int cj = j == 0 ? 0 : (j == a.ny - 1 ? 2 : 1);
+        const int cj = j == 0 ? 0 : (j == global_ny(a) - 1 ? 2 : 1);
         const int cls = cj * 3 + ci;
         for (int l = t.line_off[cls]; l < t.line_off[cls + 1]; ++l) {
             if (!t.line_kind[l]) continue;
@@ -341,9 +351,10 @@ __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const 
             }
         }
     }
-    if (st_por) record_error(a.status, PART_POROSITY, cell, st_por);
-    if (st_face) record_error(a.status, PART_FACES, cell, st_face);
-    if (st_cell) record_error(a.status, PART_CELLS, cell, st_cell);
+    const long long key = cell + (long long)a.gj0 * a.nx;
+    if (st_por) record_error(a.status, PART_POROSITY, key, st_por);
+    if (st_face) record_error(a.status, PART_FACES, key, st_face);
+    if (st_cell) record_error(a.status, PART_CELLS, key, st_cell);
     a.flags[cell] = (unsigned char)((fl & FLAG_CHECK) | (wet ? FLAG_WET : 0));
     a.T[cell] = Tsum;
     a.phi[cell] = Psum;
@@ -363,6 +374,7 @@ struct FaceArgs {
     const double* udn;
     double* face;          // 4 * nedge SoA: fluxH, fluxC, rate, fluxMixture
     unsigned long long* status;
+    int gj0 = 0, gny = 0;  // slab: global row of local row 0, global rows
 };
 
 // Limited H and C of one side along the edge line: v(s) = m + c0 + s*(c1 + s*c2).
@@ -409,9 +421,10 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
         horizontal = true;
         const unsigned ue = (unsigned)e;   // edge counts stay below 2^31 (checked on create)
         const int i = (int)(ue % (unsigned)nx), j = (int)(ue / (unsigned)nx);
-        boundary = (j == 0 || j == ny);
-        reverse = (j == ny);
-        L = reverse ? (long long)(ny - 1) * nx + i : (long long)j * nx + i;
+        const int gj = a.gj0 + j, gny = global_ny(a);
+        boundary = (gj == 0 || gj == gny);
+        reverse = (gj == gny);
+        L = reverse ? (long long)(j - 1) * nx + i : (long long)j * nx + i;
         if (!boundary) Rc = (long long)(j - 1) * nx + i;
         lfix = reverse ? t.Y : -t.Y;
         rfix = t.Y;
@@ -507,7 +520,7 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
         if (!isfinite(sens)) st = st ? st : E_FP;
         rate += w * (aC + aH + 2.0 * fabs(vs)) * sens;
     }
-    if (st) record_error(a.status, PART_FACES, L, st);
+    if (st) record_error(a.status, PART_FACES, L + (long long)a.gj0 * nx, st);
     a.face[e] = fluxH;
     a.face[nE + e] = fluxC;
     a.face[2 * nE + e] = rate;
@@ -534,6 +547,9 @@ struct SumArgs {
     double a0, a1, dt;     // next = a0*U^n + a1*(U + dt*L)
     Partial* partial;
     const double* dtp;     // when set, dt is read from device memory (batched instances)
+    int gj0 = 0, gny = 0;  // slab: global row of local row 0, global rows
+    long long cbeg = 0;    // cells [cbeg, cend) are accumulated (cend < 0: all)
+    long long cend = -1;
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -587,7 +603,8 @@ __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partia
     // each with the sign of its side (evolve.cpp:350-354).
     const long long eb = (long long)j * nx + i, et = (long long)(j + 1) * nx + i;
     const long long el = nI + (long long)j * (nx + 1) + i, er = el + 1;
-    const double sb = -1.0, stp = (j == ny - 1) ? -1.0 : 1.0, sl = (i == 0) ? -1.0 : 1.0, sr = -1.0;
+    const int gj = a.gj0 + j, gny = global_ny(a);
+    const double sb = -1.0, stp = (gj == gny - 1) ? -1.0 : 1.0, sl = (i == 0) ? -1.0 : 1.0, sr = -1.0;
     const long long ids[4] = {eb, et, el, er};
     const double sg[4] = {sb, stp, sl, sr};
     // The reference divides each face term by the area; here the signed sums
@@ -603,8 +620,8 @@ __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partia
         dv -= sg[f] * FM;
     }
     rH *= invA; rC *= invA; rr *= invA; dv *= invA;
-    if (j == 0) { bH += __ldg(a.face + eb); bC += __ldg(a.face + nE + eb); }
-    if (j == ny - 1) { bH += __ldg(a.face + et); bC += __ldg(a.face + nE + et); }
+    if (gj == 0) { bH += __ldg(a.face + eb); bC += __ldg(a.face + nE + eb); }
+    if (gj == gny - 1) { bH += __ldg(a.face + et); bC += __ldg(a.face + nE + et); }
     if (i == 0) { bH += __ldg(a.face + el); bC += __ldg(a.face + nE + el); }
     if (i == nx - 1) { bH += __ldg(a.face + er); bC += __ldg(a.face + nE + er); }
     double nh, nc;
@@ -630,13 +647,14 @@ __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partia
 }
 
 // The kSumPer cells of this thread in the sum block starting at first.
+// `first` counts from the start of the accumulated range [cbeg, cend).
 __device__ __forceinline__ Partial sum_cells(const SumArgs& a, long long first) {
-    const long long N = (long long)a.nx * a.ny;
+    const long long end = a.cend >= 0 ? a.cend : (long long)a.nx * a.ny;
     Partial v = partial_identity();
 #pragma unroll
     for (int k = 0; k < kSumPer; ++k) {
-        const long long c = first + k * kRedBlock + threadIdx.x;
-        if (c < N) sum_cell(a, (unsigned)c, v);
+        const long long c = a.cbeg + first + k * kRedBlock + threadIdx.x;
+        if (c < end) sum_cell(a, (unsigned)c, v);
     }
     return v;
 }

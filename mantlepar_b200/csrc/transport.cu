@@ -31,29 +31,48 @@ mp_status derive_checked(const mp_material& p, mp_derived& d);
 
 namespace {
 
+// Rows of one launch: global position of the local rows and the ranges the
+// kernels cover (a whole mesh: gj0 = gny = 0, rec and own = [0, ny)).
+struct StageRange {
+    int gj0 = 0, gny = 0;
+    int rec0 = 0, rec1 = 0;    // reconstruction and cell phase rows
+    int own0 = 0, own1 = 0;    // rows advanced (faces of their cells, accumulation)
+};
+
+StageRange whole(int ny) { StageRange r; r.rec1 = r.own1 = ny; return r; }
+
 // Single-instance kernels: one thread per cell / edge.
 // The stage tables arrive by value as a __grid_constant__ parameter, so the
 // unrolled table coefficients are constant-bank operands. Minimum resident
 // blocks per SM (register caps) as measured fastest on B200: cell phase 8,
 // faces 5; the reconstruction keeps its natural register count.
+// Rows [jlo, jhi) are reconstructed (all rows, or a slab's owned rows +- 1).
 template <class R>
-__global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph, const __grid_constant__ ParamTables p) {
+__global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
+                                                    int jlo, int jhi) {
     ReconArgs<R> b = a;
     b.tab = param_tab<R>(p);
-    recon_cell(b, ph, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+    const int j = jlo + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    if (j < jhi) recon_cell(b, ph, blockIdx.x * blockDim.x + threadIdx.x, j);
 }
 template <class R>
 __global__ void __launch_bounds__(128, 8) cellphase_kernel(CellPhaseArgs<R> a, Physics ph,
-                                                        const __grid_constant__ ParamTables p) {
+                                                        const __grid_constant__ ParamTables p, long long c0, long long c1) {
     CellPhaseArgs<R> b = a;
     b.tab = param_tab<R>(p);
-    cellphase_cell(b, ph, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+    const long long cell = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell < c1) cellphase_cell(b, ph, cell);
 }
+// Edges [h0, h0 + nh) (horizontal) then [v0, v0 + nv) (vertical): every edge
+// of the mesh, or of a slab's owned cells.
 template <class R>
-__global__ void __launch_bounds__(128, 5) face_kernel(FaceArgs<R> a, Physics ph, const __grid_constant__ ParamTables p) {
+__global__ void __launch_bounds__(128, 5) face_kernel(FaceArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
+                                                      long long h0, long long nh, long long v0, long long nv) {
     FaceArgs<R> b = a;
     b.tab = param_tab<R>(p);
-    face_edge(b, ph, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nh) face_edge(b, ph, h0 + k);
+    else if (k < nh + nv) face_edge(b, ph, v0 + (k - nh));
 }
 __global__ void __launch_bounds__(kRedBlock) sum_kernel(SumArgs a) {
     const Partial v = sum_cells(a, (long long)blockIdx.x * kSumCells);
@@ -127,6 +146,14 @@ struct mp_transport {
     // step is shortened to land on, and the "fixed" control.
     double t_end = INFINITY;
     bool fixed = false;
+    // Row slab of a decomposed mesh (mp_transport_create_slab): local rows
+    // hold global rows range.gj0.. of range.gny; rows [own0, own1) are
+    // advanced. A whole mesh has range = whole(ny). Between stages the hooks
+    // fill the halo rows and combine the stage totals across slabs.
+    mp::StageRange range;
+    mp_halo_fn halo = nullptr;
+    mp_combine_fn combine = nullptr;
+    void* hook_user = nullptr;
     mp::Totals curTot{};                   // totals of L(U^n)
     // Optional per-kernel timing (CUDA events on this handle's stream).
     bool profile = false;
@@ -197,25 +224,29 @@ mp_status check_status(mp_transport* t, const char* where) {
 
 // Launch the stage kernels of state (H, C) in arithmetic type R.
 template <class R>
-void launch_stage_kernels(int nx, int ny, const ParamTables& pt, const Physics& ph, const double* H, const double* C, double* rec,
+void launch_stage_kernels(int nx, int ny, const StageRange& rg, const ParamTables& pt, const Physics& ph, const double* H, const double* C, double* rec,
                           unsigned char* flags, double* T, double* phi, const double* vsn, const double* udn,
                           double* face, unsigned long long* status, double* theta, cudaStream_t s,
                           mp_transport* prof) {
-    const size_t N = (size_t)nx * ny;
     const size_t NE = (size_t)nx * (ny + 1) + (size_t)(nx + 1) * ny;
     auto run = [&](int kind, auto&& f) { if (prof) timed(prof, kind, f); else f(); };
     {
-        ReconArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, status, theta};
-        dim3 blk(32, 4), grd((nx + 31) / 32, (ny + 3) / 4);
-        run(0, [&] { recon_kernel<R><<<grd, blk, 0, s>>>(a, ph, pt); });
+        ReconArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, status, theta, rg.gj0, rg.gny};
+        dim3 blk(32, 4), grd((nx + 31) / 32, (rg.rec1 - rg.rec0 + 3) / 4);
+        run(0, [&] { recon_kernel<R><<<grd, blk, 0, s>>>(a, ph, pt, rg.rec0, rg.rec1); });
     }
     {
-        CellPhaseArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, T, phi, status};
-        run(1, [&] { cellphase_kernel<R><<<(unsigned)((N + 127) / 128), 128, 0, s>>>(a, ph, pt); });
+        CellPhaseArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, T, phi, status, rg.gj0, rg.gny};
+        const long long c0 = (long long)rg.rec0 * nx, c1 = (long long)rg.rec1 * nx;
+        run(1, [&] { cellphase_kernel<R><<<(unsigned)((c1 - c0 + 127) / 128), 128, 0, s>>>(a, ph, pt, c0, c1); });
     }
     {
-        FaceArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, vsn, udn, face, status};
-        run(2, [&] { face_kernel<R><<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(a, ph, pt); });
+        FaceArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, vsn, udn, face, status, rg.gj0, rg.gny};
+        const long long nI = (long long)nx * (ny + 1);
+        const long long h0 = (long long)rg.own0 * nx, nh = (long long)(rg.own1 - rg.own0 + 1) * nx;
+        const long long v0 = nI + (long long)rg.own0 * (nx + 1), nv = (long long)(rg.own1 - rg.own0) * (nx + 1);
+        (void)NE;
+        run(2, [&] { face_kernel<R><<<(unsigned)((nh + nv + 127) / 128), 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
     }
 }
 
@@ -224,17 +255,24 @@ void launch_stage_kernels(int nx, int ny, const ParamTables& pt, const Physics& 
 mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mode, double a0, double a1, double dt,
                        double* outH, double* outC, double* theta = nullptr) {
     cudaStream_t s = t->stream;
+    if (t->halo) {
+        // A slab: its neighbours' owned rows into this stage input's halo rows.
+        MP_CUDA(cudaStreamSynchronize(s));
+        const int rc = t->halo(t->hook_user, const_cast<double*>(H), const_cast<double*>(C));
+        if (rc) { set_error("halo exchange failed (%d)", rc); return rc > 0 ? (mp_status)rc : MP_ERR_CUDA; }
+    }
     mp_transport* prof = t->profile ? t : nullptr;
     if (t->mixed) {
-        launch_stage_kernels<float>(t->nx, t->ny, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
+        launch_stage_kernels<float>(t->nx, t->ny, t->range, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
                                     t->vsn, t->udn, t->face, t->d_status, theta, s, prof);
     } else {
-        launch_stage_kernels<double>(t->nx, t->ny, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T,
+        launch_stage_kernels<double>(t->nx, t->ny, t->range, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T,
                                      t->phi, t->vsn, t->udn, t->face, t->d_status, theta, s, prof);
     }
     {
         SumArgs a{t->nx, t->ny, t->host_tab.area, 1.0 / t->host_tab.area, t->face, H, C, t->H, t->C, outH, outC, t->rate, mode, a0, a1, dt,
-                  t->partial};
+                  t->partial, nullptr, t->range.gj0, t->range.gny, (long long)t->range.own0 * t->nx,
+                  (long long)t->range.own1 * t->nx};
         timed(t, 3, [&] { sum_kernel<<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
     }
     timed(t, 4, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, t->sum_blocks, t->d_tot); });
@@ -249,6 +287,12 @@ mp_status read_totals(mp_transport* t, Totals& out, bool& failed, const char* wh
     MP_CUDA(cudaMemcpyAsync(t->h_status, t->d_status, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     MP_CUDA(cudaStreamSynchronize(s));
     harvest(t);
+    if (t->combine) {
+        // A slab: totals and the first failure across all slabs.
+        static_assert(sizeof(Totals) == sizeof(mp_stage_partials), "Totals layout");
+        const int rc = t->combine(t->hook_user, reinterpret_cast<mp_stage_partials*>(t->h_tot), t->h_status);
+        if (rc) { set_error("%s: totals combine failed (%d)", where, rc); return rc > 0 ? (mp_status)rc : MP_ERR_CUDA; }
+    }
     out = *t->h_tot;
     failed = *t->h_status != ~0ULL;
     (void)where;
@@ -273,6 +317,9 @@ mp_status eval_current(mp_transport* t, double* theta = nullptr) {
     t->have_L = true;
     return MP_OK;
 }
+
+size_t own_begin(const mp_transport* t) { return (size_t)t->range.own0 * t->nx; }
+size_t own_count(const mp_transport* t) { return (size_t)(t->range.own1 - t->range.own0) * t->nx; }
 
 bool admissible(const Totals& tot, double Xe) {
     return tot.nonfinite == 0.0 && tot.Hmin >= 0.0 && tot.Cmin >= 0.0 && tot.Cmax <= Xe;
@@ -299,7 +346,8 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
     int retries = 0;
     double courant = 0.0;
     Totals second{}, third{}, fin{};
-    const int nblk_axpy = (int)((t->N + kSumCells - 1) / kSumCells);
+    const size_t o0 = own_begin(t), on = own_count(t);
+    const int nblk_axpy = (int)((on + kSumCells - 1) / kSumCells);
     for (;;) {
         if (!(dt >= std::min(remaining, o.dt_min) && retries < 40)) {
             set_error("Coupled step cannot satisfy admissibility/CFL above minimum step");
@@ -308,8 +356,9 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
         bool valid, failed;
         Totals adm;
         timed(t, 4, [&] {
-            axpy_kernel<<<nblk_axpy, kRedBlock, 0, s>>>((int)t->N, t->H, t->C, t->LH, t->LC, dt, t->host_tab.area,
-                                                         t->S1H, t->S1C, t->partial);
+            axpy_kernel<<<nblk_axpy, kRedBlock, 0, s>>>((int)on, t->H + o0, t->C + o0, t->LH + o0, t->LC + o0, dt,
+                                                         t->host_tab.area,
+                                                         t->S1H + o0, t->S1C + o0, t->partial);
         });
         timed(t, 4, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, nblk_axpy, t->d_tot); });
         count_launch(2);
@@ -390,8 +439,10 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
 
 // -------------------------------------------------------------------- C ABI
 
-extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_transport_opts* opts, mp_stream_t stream,
-                                         mp_transport** out) {
+namespace {
+// A whole mesh (slab = false) or the row slab [row_begin, row_end) of `mesh`.
+mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int row_end, const mp_transport_opts* opts,
+                      mp_stream_t stream, mp_transport** out) {
     using namespace mp;
     if (!mesh || !opts || !out) { set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (mesh->nx < 2 || mesh->ny < 2) { set_error("Transport requires at least 2x2 cells"); return MP_ERR_ARG_SIZ; }
@@ -405,10 +456,28 @@ extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_tran
     mp_derived der;
     MP_TRY(derive_checked(opts->material, der));
     if (!(opts->inflow_C >= 0 && opts->inflow_C <= opts->material.Xe)) { set_error("Composition must lie in [0, phase.parameters.Xe]"); return MP_ERR_ARG_OUTOFRANGE; }
+    if (slab && !(row_begin >= 0 && row_begin < row_end && row_end <= mesh->ny)) {
+        set_error("slab rows [%d, %d) outside [0, %d)", row_begin, row_end, mesh->ny);
+        return MP_ERR_ARG_OUTOFRANGE;
+    }
     mp_transport* t = new mp_transport;
     t->mesh = *mesh; t->opts = *opts; t->der = der;
     t->stream = (cudaStream_t)stream;
     t->nx = mesh->nx; t->ny = mesh->ny;
+    if (slab) {
+        // Two halo rows where the global mesh continues (3x3 gathers of the
+        // reconstructed halo row reach the second one).
+        const int hb = std::min(2, row_begin), ht = std::min(2, mesh->ny - row_end);
+        t->ny = (row_end - row_begin) + hb + ht;
+        t->range.gj0 = row_begin - hb;
+        t->range.gny = mesh->ny;
+        t->range.own0 = hb;
+        t->range.own1 = hb + (row_end - row_begin);
+        t->range.rec0 = hb > 0 ? hb - 1 : 0;
+        t->range.rec1 = ht > 0 ? t->range.own1 + 1 : t->range.own1;
+    } else {
+        t->range = whole(mesh->ny);
+    }
     t->N = (size_t)t->nx * t->ny;
     t->NE = (size_t)t->nx * (t->ny + 1) + (size_t)(t->nx + 1) * t->ny;
     t->ph.k = phase_const(opts->material, der);
@@ -420,10 +489,10 @@ extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_tran
     t->ph.inflowH = opts->inflow_H; t->ph.inflowC = opts->inflow_C;
     t->ph.Hpol = opts->H_policy; t->ph.Cpol = opts->C_policy;
     t->ph.lf_global = opts->lf_global; t->ph.lf_speed = opts->lf_global_speed;
-    const int tb = build_stage_tables(t->nx, t->ny, mesh->x0, mesh->x1, mesh->y0, mesh->y1, t->host_tab);
+    const int tb = build_stage_tables(mesh->nx, mesh->ny, mesh->x0, mesh->x1, mesh->y0, mesh->y1, t->host_tab);
     if (tb) { delete t; set_error("stencil table construction failed"); return (mp_status)tb; }
     make_param_tables(t->host_tab, t->ptab);
-    t->sum_blocks = (int)((t->N + kSumCells - 1) / kSumCells);
+    t->sum_blocks = (int)((own_count(t) + kSumCells - 1) / kSumCells);
     const size_t N = t->N, NE = t->NE;
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes); };
@@ -444,6 +513,36 @@ extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_tran
     if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
     if (e != cudaSuccess) { free_all(t); delete t; return cuda_status(e, "mp_transport_create"); }
     *out = t;
+    return MP_OK;
+}
+}  // namespace
+
+extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_transport_opts* opts, mp_stream_t stream,
+                                         mp_transport** out) {
+    return create_impl(mesh, false, 0, 0, opts, stream, out);
+}
+
+extern "C" mp_status mp_transport_create_slab(const mp_mesh_desc* global_mesh, int row_begin, int row_end,
+                                              const mp_transport_opts* opts, mp_stream_t stream, mp_transport** out) {
+    return create_impl(global_mesh, true, row_begin, row_end, opts, stream, out);
+}
+
+extern "C" mp_status mp_transport_slab_layout(const mp_transport* t, int* local_rows, int* row0, int* own_begin,
+                                              int* own_end) {
+    if (!t) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (local_rows) *local_rows = t->ny;
+    if (row0) *row0 = t->range.gj0;
+    if (own_begin) *own_begin = t->range.own0;
+    if (own_end) *own_end = t->range.own1;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_transport_set_hooks(mp_transport* t, mp_halo_fn halo, mp_combine_fn combine, void* user) {
+    if (!t) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    t->halo = halo;
+    t->combine = combine;
+    t->hook_user = user;
+    t->have_L = false;
     return MP_OK;
 }
 
@@ -467,8 +566,9 @@ extern "C" mp_status mp_transport_set_face_velocity(mp_transport* t, const doubl
 extern "C" mp_status mp_transport_set_state(mp_transport* t, const double* H, const double* C, double time) {
     if (!t || !H || !C) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (!std::isfinite(time)) { mp::set_error("Nonfinite source time"); return MP_ERR_ARG_OUTOFRANGE; }
-    MP_CUDA(cudaMemcpyAsync(t->H, H, t->N * sizeof(double), cudaMemcpyDefault, t->stream));
-    MP_CUDA(cudaMemcpyAsync(t->C, C, t->N * sizeof(double), cudaMemcpyDefault, t->stream));
+    const size_t o0 = mp::own_begin(t), ob = mp::own_count(t) * sizeof(double);
+    MP_CUDA(cudaMemcpyAsync(t->H + o0, H, ob, cudaMemcpyDefault, t->stream));
+    MP_CUDA(cudaMemcpyAsync(t->C + o0, C, ob, cudaMemcpyDefault, t->stream));
     MP_CUDA(cudaStreamSynchronize(t->stream));
     t->time = time;
     t->accepted = 0;
@@ -478,11 +578,11 @@ extern "C" mp_status mp_transport_set_state(mp_transport* t, const double* H, co
 
 extern "C" mp_status mp_transport_get_state(mp_transport* t, double* H, double* C, double* T, double* phi) {
     if (!t) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
-    const size_t b = t->N * sizeof(double);
-    if (H) MP_CUDA(cudaMemcpyAsync(H, t->H, b, cudaMemcpyDefault, t->stream));
-    if (C) MP_CUDA(cudaMemcpyAsync(C, t->C, b, cudaMemcpyDefault, t->stream));
-    if (T) MP_CUDA(cudaMemcpyAsync(T, t->T, b, cudaMemcpyDefault, t->stream));
-    if (phi) MP_CUDA(cudaMemcpyAsync(phi, t->phi, b, cudaMemcpyDefault, t->stream));
+    const size_t o0 = mp::own_begin(t), b = mp::own_count(t) * sizeof(double);
+    if (H) MP_CUDA(cudaMemcpyAsync(H, t->H + o0, b, cudaMemcpyDefault, t->stream));
+    if (C) MP_CUDA(cudaMemcpyAsync(C, t->C + o0, b, cudaMemcpyDefault, t->stream));
+    if (T) MP_CUDA(cudaMemcpyAsync(T, t->T + o0, b, cudaMemcpyDefault, t->stream));
+    if (phi) MP_CUDA(cudaMemcpyAsync(phi, t->phi + o0, b, cudaMemcpyDefault, t->stream));
     MP_CUDA(cudaStreamSynchronize(t->stream));
     return MP_OK;
 }
@@ -491,12 +591,12 @@ extern "C" mp_status mp_transport_rhs(mp_transport* t, double* rhsH, double* rhs
                                       mp_stage_totals* totals) {
     if (!t) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
     MP_TRY(mp::eval_current(t));
-    const size_t b = t->N * sizeof(double);
-    if (rhsH) MP_CUDA(cudaMemcpyAsync(rhsH, t->LH, b, cudaMemcpyDefault, t->stream));
-    if (rhsC) MP_CUDA(cudaMemcpyAsync(rhsC, t->LC, b, cudaMemcpyDefault, t->stream));
-    if (T) MP_CUDA(cudaMemcpyAsync(T, t->T, b, cudaMemcpyDefault, t->stream));
-    if (phi) MP_CUDA(cudaMemcpyAsync(phi, t->phi, b, cudaMemcpyDefault, t->stream));
-    if (rate) MP_CUDA(cudaMemcpyAsync(rate, t->rate, b, cudaMemcpyDefault, t->stream));
+    const size_t o0 = mp::own_begin(t), b = mp::own_count(t) * sizeof(double);
+    if (rhsH) MP_CUDA(cudaMemcpyAsync(rhsH, t->LH + o0, b, cudaMemcpyDefault, t->stream));
+    if (rhsC) MP_CUDA(cudaMemcpyAsync(rhsC, t->LC + o0, b, cudaMemcpyDefault, t->stream));
+    if (T) MP_CUDA(cudaMemcpyAsync(T, t->T + o0, b, cudaMemcpyDefault, t->stream));
+    if (phi) MP_CUDA(cudaMemcpyAsync(phi, t->phi + o0, b, cudaMemcpyDefault, t->stream));
+    if (rate) MP_CUDA(cudaMemcpyAsync(rate, t->rate + o0, b, cudaMemcpyDefault, t->stream));
     MP_CUDA(cudaStreamSynchronize(t->stream));
     if (totals) {
         totals->boundaryH = t->curTot.bH; totals->boundaryC = t->curTot.bC; totals->sourceH = 0.0;
@@ -559,8 +659,9 @@ extern "C" mp_status mp_transport_limiter(mp_transport* t, double* thetaH, doubl
     MP_CUDA(cudaMalloc(&theta, 2 * t->N * sizeof(double)));
     const mp_status s = mp::eval_current(t, theta);
     cudaError_t e = cudaSuccess;
-    if (s == MP_OK) e = cudaMemcpyAsync(thetaH, theta, t->N * sizeof(double), cudaMemcpyDefault, t->stream);
-    if (s == MP_OK && e == cudaSuccess) e = cudaMemcpyAsync(thetaC, theta + t->N, t->N * sizeof(double), cudaMemcpyDefault, t->stream);
+    const size_t o0 = mp::own_begin(t), ob = mp::own_count(t) * sizeof(double);
+    if (s == MP_OK) e = cudaMemcpyAsync(thetaH, theta + o0, ob, cudaMemcpyDefault, t->stream);
+    if (s == MP_OK && e == cudaSuccess) e = cudaMemcpyAsync(thetaC, theta + t->N + o0, ob, cudaMemcpyDefault, t->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
     cudaFree(theta);
     if (s != MP_OK) return s;
@@ -660,7 +761,8 @@ mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double
     (void)NE;
     ParamTables pt;
     make_param_tables(tab, pt);
-    launch_stage_kernels<double>(nx, ny, pt, ph, H, C, rec, wet, T, phi, vsn, udn, face, status, nullptr, s, nullptr);
+    launch_stage_kernels<double>(nx, ny, whole(ny), pt, ph, H, C, rec, wet, T, phi, vsn, udn, face, status, nullptr, s,
+                                 nullptr);
     {
         SumArgs a{nx, ny, tab.area, 1.0 / tab.area, face, H, C, H, C, rhsH, rhsC, rate, SUM_STORE_L, 0.0, 0.0, 0.0, part};
         sum_kernel<<<sum_blocks, kRedBlock, 0, s>>>(a);
