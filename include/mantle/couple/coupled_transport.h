@@ -5,8 +5,8 @@
 // The reference's Configuration / InitialState carry PETSc, MPI, MFEM and
 // YAML types; here they are plain structs holding the subset the transport
 // reads, with the reference's member names: phase model, phase-law pressure,
-// advection boundary rules, Lax-Friedrichs options, thermal diffusivity
-// (0 in this build), time controls (TimeInput), and the cell fields H, C, T,
+// advection and thermal boundary rules (one per wall), Lax-Friedrichs
+// options, thermal diffusivity, time controls (TimeInput), and the cell fields H, C, T,
 // phi with time and acceptedSteps. Cell order is j*nx + i; edge data uses the
 // reference's edge ids and canonical Gauss-point order (see mantlepar/mp.h).
 //
@@ -36,8 +36,19 @@ struct AdvectionCondition {
     AdvectionPolicy policy = AdvectionPolicy::ZeroFlux;
     double inflow = 0.0;
 };
+enum class ThermalPolicy { Temperature, OutwardFlux, ZeroFlux };
+
+// value: dimensionless temperature, or physical outward diffusive flux per length.
+struct ThermalCondition {
+    ThermalPolicy policy = ThermalPolicy::ZeroFlux;
+    double value = 0.0;
+};
+
+enum Wall { Bottom = 0, Top = 1, Left = 2, Right = 3 };
+
 struct TransportBoundarySpecification {
     AdvectionCondition enthalpy, composition;
+    ThermalCondition temperature[4];     // per Wall
 };
 
 enum class LaxFriedrichsMode { Local, Global };
@@ -61,7 +72,7 @@ struct Configuration {
     double pressure = 0.0;               // phase-law pressure [Pa], constant
     TransportBoundarySpecification boundary;
     LaxFriedrichsOptions stabilizer;
-    double thermalDiffusivity = 0.0;     // must be 0 in this build
+    double thermalDiffusivity = 0.0;     // kappa >= 0 (normal-line sampled diffusion of T)
     double darcyExponent = 0.0;          // theta of phi^(1+theta) u_d
     TimeInput time;
     Integrator integrator = Integrator::SSPRK2;

@@ -154,7 +154,7 @@ typedef struct mp_transport_opts {
     int integrator;           /* MP_SSPRK2 (reference) or MP_SSPRK3 */
     int lf_global;            /* 0 local Lax-Friedrichs, 1 global */
     double lf_global_speed;
-    double diffusivity;       /* thermal diffusivity kappa; only 0 is supported */
+    double diffusivity;       /* thermal diffusivity kappa >= 0 (evolve.cpp:330-349) */
     int precision;            /* MP_PRECISION_FP64 or MP_PRECISION_MIXED */
 } mp_transport_opts;
 
@@ -212,6 +212,15 @@ mp_status mp_transport_step(mp_transport* t, int nsteps, mp_step_report* reports
  * have dt = 0 and time = t_end). */
 enum { MP_TIME_CFL = 0, MP_TIME_FIXED = 1 };
 mp_status mp_transport_set_time_control(mp_transport* t, int control, double t_end);
+
+/* Thermal conditions of the diffusion, one per wall: [0] bottom (y0), [1] top
+ * (y1), [2] left (x0), [3] right (x1) (TransportBoundarySpecification
+ * ::temperature, EvaluateThermalBoundary, src/couple/initialization.cpp:490-506):
+ * MP_THERMAL_ZERO_FLUX (default), MP_THERMAL_TEMPERATURE (prescribed
+ * dimensionless temperature), MP_THERMAL_FLUX (prescribed physical outward
+ * diffusive flux per unit length; applies even with kappa = 0). */
+enum { MP_THERMAL_ZERO_FLUX = 0, MP_THERMAL_TEMPERATURE = 1, MP_THERMAL_FLUX = 2 };
+mp_status mp_transport_set_thermal_bc(mp_transport* t, const int* type, const double* value);
 
 /* Current time and accepted steps (InitialState::time, acceptedSteps). */
 mp_status mp_transport_get_time(const mp_transport* t, double* time, int* accepted);
@@ -286,6 +295,8 @@ mp_status mp_batch_step(mp_batch* b, int nsteps, mp_step_report* reports);
  * are limited to the remaining time and it stops there; finished() reports
  * it (within 32 eps, as src/couple/evolve.cpp:450-451). */
 mp_status mp_batch_set_end_time(mp_batch* b, int instance, double t_end);
+/* mp_transport_set_thermal_bc for every instance of the batch. */
+mp_status mp_batch_set_thermal_bc(mp_batch* b, const int* type, const double* value);
 int mp_batch_finished(const mp_batch* b, int instance);
 /* Project autotuner: times the candidate reconstruction tile shapes and
  * cells-per-thread on this batch and keeps the fastest; tile = {bx, by, cpt}. */

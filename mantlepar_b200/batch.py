@@ -88,6 +88,11 @@ class Batch:
                                                  C.byref(t), C.byref(acc), C.byref(st)))
         return dict(time=t.value, accepted=acc.value, status=st.value)
 
+    def set_thermal_bc(self, types=(0, 0, 0, 0), values=(0.0, 0.0, 0.0, 0.0)):
+        ti = (C.c_int * 4)(*[int(x) for x in types])
+        tv = (C.c_double * 4)(*[float(x) for x in values])
+        _capi.check(self._lib.mp_batch_set_thermal_bc(self._h, ti, tv))
+
     def step(self, nsteps: int = 1):
         slots = self.slots
         reps = (_capi.StepReport * max(1, nsteps * slots))()

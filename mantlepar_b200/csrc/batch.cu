@@ -90,6 +90,15 @@ __global__ void __launch_bounds__(128, 5) batch_face_kernel(const InstArgs<R>* a
 }
 
 template <class R>
+__global__ void __launch_bounds__(128) batch_diffusion_kernel(const InstArgs<R>* args, const Work* work, const int* active,
+                                                              Physics ph) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    const long long e = (long long)w.a + threadIdx.x;
+    if (e < w.b) diffusion_edge(args[w.inst].face, ph, e);
+}
+
+template <class R>
 __global__ void __launch_bounds__(kRedBlock) batch_sum_kernel(const InstArgs<R>* args, const Work* work, const int* active) {
     const Work w = work[blockIdx.x];
     if (!active[w.inst]) return;
@@ -412,6 +421,8 @@ void launch_kind(mp_batch* b, int kind) {
     if (b->n_wrecon) timed(b, 0, [&] { batch_recon_kernel<R><<<b->n_wrecon, dim3(tu.bx, tu.by), 0, s>>>(args, b->d_wrecon, b->d_active, b->ph, tu.cpt); });
     if (b->n_wphase) timed(b, 1, [&] { batch_phase_kernel<R><<<b->n_wphase, 128, 0, s>>>(args, b->d_wphase, b->d_active, b->ph); });
     if (b->n_wface) timed(b, 2, [&] { batch_face_kernel<R><<<b->n_wface, 128, 0, s>>>(args, b->d_wface, b->d_active, b->ph); });
+    if (b->n_wface && b->ph.diffusion)
+        timed(b, 2, [&] { batch_diffusion_kernel<R><<<b->n_wface, 128, 0, s>>>(args, b->d_wface, b->d_active, b->ph); });
     if (b->n_wsum) timed(b, 3, [&] { batch_sum_kernel<R><<<b->n_wsum, kRedBlock, 0, s>>>(args, b->d_wsum, b->d_active); });
     timed(b, 4, [&] { batch_reduce_kernel<<<(int)b->inst.size(), 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot); });
     count_launch(5);
@@ -635,7 +646,7 @@ extern "C" mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, cons
     if (!opts || !out || count < 0 || (count > 0 && !meshes)) { set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (!(opts->cfl > 0 && opts->cfl <= 1)) { set_error("Coupled CFL must be in (0,1]"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->integrator != MP_SSPRK2 && opts->integrator != MP_SSPRK3) { set_error("integrator must be 2 or 3"); return MP_ERR_ARG_OUTOFRANGE; }
-    if (opts->diffusivity != 0.0) { set_error("thermal diffusion (kappa > 0) is not supported by this build"); return MP_ERR_ARG_WRONG; }
+    if (!(std::isfinite(opts->diffusivity) && opts->diffusivity >= 0.0)) { set_error("Diffusivity must be finite and nonnegative"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->material.alpha0 != 0.0) { set_error("adiabatic source (alpha0 != 0) is not supported by this build"); return MP_ERR_ARG_WRONG; }
     if (opts->precision != MP_PRECISION_FP64 && opts->precision != MP_PRECISION_MIXED) { set_error("unknown precision"); return MP_ERR_ARG_OUTOFRANGE; }
     mp_derived der;
@@ -650,6 +661,9 @@ extern "C" mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, cons
     b->ph.theta = opts->theta; b->ph.inflowH = opts->inflow_H; b->ph.inflowC = opts->inflow_C;
     b->ph.Hpol = opts->H_policy; b->ph.Cpol = opts->C_policy; b->ph.lf_global = opts->lf_global;
     b->ph.lf_speed = opts->lf_global_speed;
+    b->ph.kappa = opts->diffusivity;
+    for (int w = 0; w < 4; ++w) { b->ph.wall_type[w] = 0; b->ph.wall_value[w] = 0.0; }
+    b->ph.diffusion = opts->diffusivity > 0.0;
     b->inst.resize(count);
     for (int i = 0; i < count; ++i) {
         if (meshes[i].nx < 2 || meshes[i].ny < 2) { set_error("instance %d: at least 2x2 cells", i); mp_batch_destroy(b); return MP_ERR_ARG_SIZ; }
@@ -797,5 +811,22 @@ extern "C" mp_status mp_batch_kernel_times(mp_batch* b, double ms[6], unsigned l
     MP_CUDA(cudaStreamSynchronize(b->stream));
     mp::harvest(b);
     for (int k = 0; k < 6; ++k) { ms[k] = b->kern_ms[k]; launches[k] = b->kern_n[k]; }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_set_thermal_bc(mp_batch* b, const int* type, const double* value) {
+    if (!b || !type || !value) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    for (int w = 0; w < 4; ++w) {
+        if (type[w] < MP_THERMAL_ZERO_FLUX || type[w] > MP_THERMAL_FLUX) { mp::set_error("unknown thermal condition %d", type[w]); return MP_ERR_ARG_WRONG; }
+        if (type[w] != MP_THERMAL_ZERO_FLUX && !std::isfinite(value[w])) { mp::set_error("Boundary data must be finite"); return MP_ERR_ARG_OUTOFRANGE; }
+    }
+    bool flux = false;
+    for (int w = 0; w < 4; ++w) {
+        b->ph.wall_type[w] = type[w];
+        b->ph.wall_value[w] = type[w] == MP_THERMAL_ZERO_FLUX ? 0.0 : value[w];
+        flux = flux || type[w] == MP_THERMAL_FLUX;
+    }
+    b->ph.diffusion = b->ph.kappa > 0.0 || flux;
+    for (auto& in : b->inst) in.have_L = false;
     return MP_OK;
 }

@@ -35,6 +35,13 @@ struct Physics {
     double inflowH, inflowC;
     int Hpol, Cpol, lf_global;
     double lf_speed;
+    // Thermal diffusion: on when kappa > 0 or a wall prescribes a flux.
+    // Walls 0 bottom, 1 top, 2 left, 3 right: 0 zero flux, 1 prescribed
+    // temperature, 2 prescribed outward flux (per unit length).
+    int diffusion;
+    double kappa;
+    int wall_type[4];
+    double wall_value[4];
 };
 
 // Block partials of one stage (sum_kernel) or state check (axpy_kernel).
@@ -525,6 +532,110 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
     a.face[nE + e] = fluxC;
     a.face[2 * nE + e] = rate;
     a.face[3 * nE + e] = fluxMix;
+}
+
+// ------------------------------------------------------------- diffusion
+
+// The diffusive part of one edge's H flux and rate (evolve.cpp:330-347 with
+// IntegrateDiffusive(Boundary)FluxWithDerivatives, diffusiveflux.cpp:105-200,
+// identity law): temperatures of the limited states at 4 samples per Gauss
+// point on the line normal to the edge (2 per side; at a wall 4 inside and the
+// wall value), gradient sum_k c_k (T_k - T_last) / ds, flux -= w kappa grad,
+// and |d flux / d T_k| added to the rate sample by sample. Added to the face
+// results after the advective part, as the reference adds them.
+template <class R>
+__device__ __forceinline__ void diffusion_edge(const FaceArgs<R>& a, const Physics& ph, long long e) {
+    const int nx = a.nx, ny = a.ny;
+    const long long nI = (long long)nx * (ny + 1);
+    const long long nE = nI + (long long)(nx + 1) * ny;
+    if (e >= nE) return;
+    const StageHot& t = *a.tab.t;
+    const size_t N = (size_t)nx * ny;
+    bool boundary, reverse, horizontal;
+    long long L, Rc = -1;
+    int wall = -1;
+    if (e < nI) {
+        horizontal = true;
+        const unsigned ue = (unsigned)e;
+        const int i = (int)(ue % (unsigned)nx), j = (int)(ue / (unsigned)nx);
+        const int gj = a.gj0 + j, gny = global_ny(a);
+        boundary = (gj == 0 || gj == gny);
+        reverse = (gj == gny);
+        L = reverse ? (long long)(j - 1) * nx + i : (long long)j * nx + i;
+        if (!boundary) Rc = (long long)(j - 1) * nx + i;
+        else wall = gj == 0 ? 0 : 1;
+    } else {
+        horizontal = false;
+        const unsigned k = (unsigned)(e - nI);
+        const int i = (int)(k % (unsigned)(nx + 1)), j = (int)(k / (unsigned)(nx + 1));
+        boundary = (i == 0 || i == nx);
+        reverse = (i == 0);
+        L = reverse ? (long long)j * nx : (long long)j * nx + (i - 1);
+        if (!boundary) Rc = (long long)j * nx + i;
+        else wall = i == 0 ? 2 : 3;
+    }
+    const int type = boundary ? ph.wall_type[wall] : 1;
+    if (boundary && type == 0) return;             // zero flux: nothing added
+    const int o = horizontal ? 0 : 1;
+    double DL[9], CL[9], DR[9], CR[9];
+    double mHL = 0, mCL = 0, mHR = 0, mCR = 0;
+    if (type == 1) {
+        load_rec(a.rec, N, L, DL, CL);
+        mHL = __ldg(a.H + L); mCL = __ldg(a.C + L);
+        if (!boundary) {
+            load_rec(a.rec, N, Rc, DR, CR);
+            mHR = __ldg(a.H + Rc); mCR = __ldg(a.C + Rc);
+        }
+    }
+    double integral = 0.0, rate = a.face[2 * nE + e];
+    const double kappa = ph.kappa;
+    int st = 0;
+    for (int q = 0; q < kNQ; ++q) {
+        const double w = t.dif_w[o][q];
+        if (boundary && type == 2) { integral += w * ph.wall_value[wall]; continue; }
+        const int cq = reverse ? kNQ - 1 - q : q;
+        const double at = horizontal ? t.gx[cq] : t.gy[cq];
+        const int count = boundary ? 5 : 4;
+        double v[5];
+        // Temperatures at the samples: limited H, C on the line across the edge
+        // through this Gauss point, in the frame of the sample's cell.
+        double lh0, lh1, lh2, lc0, lc1, lc2, rh0 = 0, rh1 = 0, rh2 = 0, rc0 = 0, rc1 = 0, rc2 = 0;
+        if (horizontal) { q2_col(DL, at, lh0, lh1, lh2); q2_col(CL, at, lc0, lc1, lc2); }
+        else { q2_row(DL, at, lh0, lh1, lh2); q2_row(CL, at, lc0, lc1, lc2); }
+        if (!boundary) {
+            if (horizontal) { q2_col(DR, at, rh0, rh1, rh2); q2_col(CR, at, rc0, rc1, rc2); }
+            else { q2_row(DR, at, rh0, rh1, rh2); q2_row(CR, at, rc0, rc1, rc2); }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const bool left = boundary || k < 2;
+            const double s = boundary ? t.dif_pos_bnd[wall][k] : t.dif_pos_int[o][k];
+            const double h = left ? mHL + quad(lh0, lh1, lh2, s) : mHR + quad(rh0, rh1, rh2, s);
+            const double c = left ? mCL + quad(lc0, lc1, lc2, s) : mCR + quad(rc0, rc1, rc2, s);
+            PhaseLean pl;
+            int s1 = phase_stage_lean(ph.sk, h, c, ph.Tep, pl);
+            if (!s1 && !(pl.T >= 0.0 && pl.phil < 1.0)) s1 = E_OUTOFRANGE;
+            if (s1) st = st ? st : s1;
+            v[k] = s1 ? 0.0 : pl.T;
+        }
+        if (boundary) v[4] = ph.wall_value[wall];
+        const double* c = boundary ? t.dif_c_bnd : t.dif_c_int;
+        const double last = v[count - 1];
+        double grad = 0.0, clast = 0.0;
+        for (int k = 0; k + 1 < count; ++k) { grad += c[k] * (v[k] - last); clast -= c[k]; }
+        const double ds = t.dif_ds[o][boundary ? 1 : 0];
+        grad /= ds;
+        if (!isfinite(grad)) st = st ? st : E_FP;
+        integral -= w * kappa * grad;
+        const double scale = -w * kappa / ds;
+        for (int k = 0; k < count; ++k) {
+            if (boundary && k + 1 == count) continue;     // the wall value: not a sample
+            rate += fabs(scale * (k + 1 == count ? clast : c[k]));
+        }
+    }
+    if (st) record_error(a.status, PART_FACES, L + (long long)a.gj0 * nx, st);
+    a.face[e] += integral;
+    a.face[2 * nE + e] = rate;
 }
 
 // ----------------------------------------------------------------- sum kernel

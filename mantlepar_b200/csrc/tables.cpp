@@ -232,6 +232,76 @@ void left_samples(V2 a, V2 b, const Quad& left, const Quad* right, const std::ve
 
 }  // namespace
 
+namespace {
+
+// diffusiveflux.cpp:203-253: first-derivative weights on uniform nodes 0..n
+// at n/2 (middle) or n (end), long double intermediates.
+void derivative_weights(int count, bool middle, double* w) {
+    typedef long double ld;
+    const int n = count - 1;
+    if (middle) {
+        ld factor = std::exp2(1.0L - n);
+        for (int k = 3; k <= n; k += 2) factor *= (ld)k / (k - 1);
+        if ((count / 2) % 2) factor = -factor;
+        ld choose = 1;
+        for (int i = 0; i < count / 2; ++i) {
+            const ld den = (ld)n - 2.0L * i;
+            w[i] = (double)(factor * choose / (den * den));
+            w[n - i] = -w[i];
+            choose *= (ld)(n - i) / (i + 1);
+            factor = -factor;
+        }
+    } else {
+        ld harmonic = 0;
+        for (int j = 1; j <= n; ++j) harmonic += 1.0L / j;
+        w[n] = (double)harmonic;
+        ld choose = 1, sign = n % 2 ? -1 : 1;
+        for (int i = 0; i < n; ++i) {
+            w[i] = (double)(sign * choose / (n - i));
+            choose *= (ld)(n - i) / (i + 1);
+            sign = -sign;
+        }
+    }
+}
+
+// Normal-line samples of a uniform rectangular mesh (diffusiveflux.cpp:255-334,
+// numberOfSamples 4, extentFraction 0.9): the available ray distance across
+// an edge is the cell size normal to it.
+void fill_diffusion(StageHot& t, double dx, double dy, double h, const std::vector<double>& gw) {
+    typedef long double ld;
+    const int N = 4;
+    const ld frac = 0.9L;
+    derivative_weights(N, true, t.dif_c_int);
+    derivative_weights(N + 1, false, t.dif_c_bnd);
+    const double size[2] = {dy, dx};      // across horizontal / vertical edges
+    const double len[2] = {dx, dy};
+    for (int o = 0; o < 2; ++o) {
+        t.dif_ds[o][0] = (double)(frac * size[o] * (2.0L / (N - 1)));
+        t.dif_ds[o][1] = (double)(frac * size[o] * (1.0L / N));
+        for (int q = 0; q < kNQ; ++q) t.dif_w[o][q] = (double)((ld)len[o] * gw[q] / 2);
+    }
+    const double Y = t.Y, X = t.X;
+    // Interior: offsets (k - 1.5) ds along the edge normal, which points from
+    // the left cell into the right one: down for horizontal edges (left cell
+    // above), +x for vertical edges (left cell at smaller x).
+    for (int k = 0; k < N; ++k) {
+        const ld off = (ld)k - (N - 1) / 2.0L;
+        const double sh = (double)(off * t.dif_ds[0][0] / h), sv = (double)(off * t.dif_ds[1][0] / h);
+        t.dif_pos_int[0][k] = k < N / 2 ? -Y - sh : Y - sh;
+        t.dif_pos_int[1][k] = k < N / 2 ? X + sv : -X + sv;
+    }
+    // Walls: interior samples at (N - k) ds inside, farthest first.
+    for (int k = 0; k < N; ++k) {
+        const double dh = (double)((ld)(N - k) * t.dif_ds[0][1] / h), dv = (double)((ld)(N - k) * t.dif_ds[1][1] / h);
+        t.dif_pos_bnd[0][k] = -Y + dh;   // bottom wall: the cell above it
+        t.dif_pos_bnd[1][k] = Y - dh;    // top wall: the cell below it
+        t.dif_pos_bnd[2][k] = -X + dv;   // left wall
+        t.dif_pos_bnd[3][k] = X - dv;    // right wall
+    }
+}
+
+}  // namespace
+
 int build_stage_tables(int nx, int ny, double x0, double x1, double y0, double y1, StageTables& t) {
     if (nx < 2 || ny < 2) return MP_ERR_ARG_SIZ;
     const double dx = (x1 - x0) / (double)nx, dy = (y1 - y0) / (double)ny;
@@ -268,6 +338,7 @@ int build_stage_tables(int nx, int ny, double x0, double x1, double y0, double y
     t.X = 0.5 * dx / h;
     t.Y = 0.5 * dy / h;
     t.scan_guard = 1e36 / (16.0 * std::max(1.0, t.X * t.X) * std::max(1.0, t.Y * t.Y));
+    fill_diffusion(t, dx, dy, h, gw);
     t.epsA = 1e-2 * area;
     t.area = area;
     t.len_h = dx;

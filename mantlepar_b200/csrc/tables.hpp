@@ -47,6 +47,21 @@ struct StageHot {
     double cw[kNQ * kNQ];   // cell-quadrature weight / area, q = b*5 + a
     double gx[kNQ];         // X * g_q
     double gy[kNQ];         // Y * g_q
+    // Thermal diffusion by normal-line sampling (diffusiveflux.cpp:203-334)
+    // with 4 samples per Gauss point and extent fraction 0.9, for this mesh:
+    // derivative weights (interior: middle of 4 nodes; wall: end of 5 nodes),
+    // physical spacing [horizontal/vertical edges][interior/wall], physical
+    // Gauss weights len*w_q/2 [horizontal/vertical][q], and the coordinate
+    // across the edge of each sample in its cell's normalised frame: interior
+    // samples k = 0, 1 lie in the left cell, 2, 3 in the right one
+    // [horizontal/vertical][k]; wall samples k = 0..3 lie in the wall cell,
+    // farthest first [wall: bottom, top, left, right][k].
+    double dif_c_int[4];
+    double dif_c_bnd[5];
+    double dif_ds[2][2];
+    double dif_w[2][kNQ];
+    double dif_pos_int[2][4];
+    double dif_pos_bnd[4][4];
     // With every deviation coefficient below this magnitude, every limiter
     // value is finite (in FP32 too): 1e36 / (16 max(1, X^2) max(1, Y^2)),
     // the points lying within |xi| <= X, |eta| <= Y.

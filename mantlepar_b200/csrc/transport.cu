@@ -74,6 +74,17 @@ __global__ void __launch_bounds__(128, 5) face_kernel(FaceArgs<R> a, Physics ph,
     if (k < nh) face_edge(b, ph, h0 + k);
     else if (k < nh + nv) face_edge(b, ph, v0 + (k - nh));
 }
+// The diffusive part of the same edges (only launched when diffusion is on).
+template <class R>
+__global__ void __launch_bounds__(128) diffusion_kernel(FaceArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
+                                                        long long h0, long long nh, long long v0, long long nv) {
+    FaceArgs<R> b = a;
+    b.tab = param_tab<R>(p);
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nh) diffusion_edge(b, ph, h0 + k);
+    else if (k < nh + nv) diffusion_edge(b, ph, v0 + (k - nh));
+}
+
 __global__ void __launch_bounds__(kRedBlock) sum_kernel(SumArgs a) {
     const Partial v = sum_cells(a, (long long)blockIdx.x * kSumCells);
     block_reduce_write(v, a.partial + blockIdx.x);
@@ -247,6 +258,8 @@ void launch_stage_kernels(int nx, int ny, const StageRange& rg, const ParamTable
         const long long v0 = nI + (long long)rg.own0 * (nx + 1), nv = (long long)(rg.own1 - rg.own0) * (nx + 1);
         (void)NE;
         run(2, [&] { face_kernel<R><<<(unsigned)((nh + nv + 127) / 128), 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
+        if (ph.diffusion)
+            run(2, [&] { diffusion_kernel<R><<<(unsigned)((nh + nv + 127) / 128), 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
     }
 }
 
@@ -449,7 +462,7 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
     if (mesh_too_large(mesh->nx, mesh->ny)) { set_error("mesh has 2^31 edges or more"); return MP_ERR_ARG_SIZ; }
     if (!(opts->cfl > 0 && opts->cfl <= 1)) { set_error("Coupled CFL must be in (0,1]"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->integrator != MP_SSPRK2 && opts->integrator != MP_SSPRK3) { set_error("integrator must be 2 or 3"); return MP_ERR_ARG_OUTOFRANGE; }
-    if (opts->diffusivity != 0.0) { set_error("thermal diffusion (kappa > 0) is not supported by this build"); return MP_ERR_ARG_WRONG; }
+    if (!(std::isfinite(opts->diffusivity) && opts->diffusivity >= 0.0)) { set_error("Diffusivity must be finite and nonnegative"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->material.alpha0 != 0.0) { set_error("adiabatic source (alpha0 != 0) needs cell-point velocities; not supported by this build"); return MP_ERR_ARG_WRONG; }
     if (opts->precision != MP_PRECISION_FP64 && opts->precision != MP_PRECISION_MIXED) { set_error("unknown precision"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->H_policy < 0 || opts->H_policy > 2 || opts->C_policy < 0 || opts->C_policy > 2) { set_error("unknown boundary policy"); return MP_ERR_ARG_OUTOFRANGE; }
@@ -489,6 +502,9 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
     t->ph.inflowH = opts->inflow_H; t->ph.inflowC = opts->inflow_C;
     t->ph.Hpol = opts->H_policy; t->ph.Cpol = opts->C_policy;
     t->ph.lf_global = opts->lf_global; t->ph.lf_speed = opts->lf_global_speed;
+    t->ph.kappa = opts->diffusivity;
+    for (int w = 0; w < 4; ++w) { t->ph.wall_type[w] = 0; t->ph.wall_value[w] = 0.0; }
+    t->ph.diffusion = opts->diffusivity > 0.0;
     const int tb = build_stage_tables(mesh->nx, mesh->ny, mesh->x0, mesh->x1, mesh->y0, mesh->y1, t->host_tab);
     if (tb) { delete t; set_error("stencil table construction failed"); return (mp_status)tb; }
     make_param_tables(t->host_tab, t->ptab);
@@ -646,6 +662,23 @@ extern "C" mp_status mp_transport_set_time_control(mp_transport* t, int control,
     return MP_OK;
 }
 
+extern "C" mp_status mp_transport_set_thermal_bc(mp_transport* t, const int* type, const double* value) {
+    if (!t || !type || !value) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    for (int w = 0; w < 4; ++w) {
+        if (type[w] < MP_THERMAL_ZERO_FLUX || type[w] > MP_THERMAL_FLUX) { mp::set_error("unknown thermal condition %d", type[w]); return MP_ERR_ARG_WRONG; }
+        if (type[w] != MP_THERMAL_ZERO_FLUX && !std::isfinite(value[w])) { mp::set_error("Boundary data must be finite"); return MP_ERR_ARG_OUTOFRANGE; }
+    }
+    bool flux = false;
+    for (int w = 0; w < 4; ++w) {
+        t->ph.wall_type[w] = type[w];
+        t->ph.wall_value[w] = type[w] == MP_THERMAL_ZERO_FLUX ? 0.0 : value[w];
+        flux = flux || type[w] == MP_THERMAL_FLUX;
+    }
+    t->ph.diffusion = t->ph.kappa > 0.0 || flux;
+    t->have_L = false;
+    return MP_OK;
+}
+
 extern "C" mp_status mp_transport_get_time(const mp_transport* t, double* time, int* accepted) {
     if (!t) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (time) *time = t->time;
@@ -752,6 +785,8 @@ mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double
     if (eutectic_temperature(ph.k, o.pressure, ph.Tep)) { set_error("pressure must be finite"); return MP_ERR_ARG_OUTOFRANGE; }
     ph.theta = o.theta; ph.inflowH = o.inflow_H; ph.inflowC = o.inflow_C;
     ph.Hpol = o.H_policy; ph.Cpol = o.C_policy; ph.lf_global = o.lf_global; ph.lf_speed = o.lf_global_speed;
+    ph.diffusion = 0; ph.kappa = 0.0;
+    for (int w = 0; w < 4; ++w) { ph.wall_type[w] = 0; ph.wall_value[w] = 0.0; }
     const size_t N = (size_t)nx * ny;
     const size_t NE = (size_t)nx * (ny + 1) + (size_t)(nx + 1) * ny;
     const int sum_blocks = (int)((N + kSumCells - 1) / kSumCells);

@@ -137,6 +137,12 @@ class Slab:
         _capi.check(self._lib.mp_transport_get_state(self._h, _ptr(H), _ptr(Cc), _ptr(T), _ptr(phi)))
         return H, Cc, T, phi
 
+    def set_thermal_bc(self, types=(0, 0, 0, 0), values=(0.0, 0.0, 0.0, 0.0)):
+        """Thermal conditions per wall (bottom, top, left, right) of the GLOBAL mesh."""
+        ti = (C.c_int * 4)(*[int(x) for x in types])
+        tv = (C.c_double * 4)(*[float(x) for x in values])
+        _capi.check(self._lib.mp_transport_set_thermal_bc(self._h, ti, tv))
+
     def set_hooks(self, halo, combine):
         """halo(H_ptr, C_ptr) -> int, combine(totals: ndarray[10] view, status: list[int]) -> int."""
         def _halo(user, H, Cc):

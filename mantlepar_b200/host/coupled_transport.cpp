@@ -67,6 +67,17 @@ mp_transport* create(const Configuration& c, const Mesh& m, bool continuing) {
     mp_status st = mp_transport_create(&d, &o, nullptr, &h);
     if (st != MP_OK) throw_status(st);
     st = mp_transport_set_time_control(h, control, c.time.end);
+    if (st == MP_OK) {
+        int type[4];
+        double value[4];
+        for (int w = 0; w < 4; ++w) {
+            const auto& tc = c.boundary.temperature[w];
+            type[w] = tc.policy == ThermalPolicy::Temperature ? MP_THERMAL_TEMPERATURE
+                    : (tc.policy == ThermalPolicy::OutwardFlux ? MP_THERMAL_FLUX : MP_THERMAL_ZERO_FLUX);
+            value[w] = tc.value;
+        }
+        st = mp_transport_set_thermal_bc(h, type, value);
+    }
     if (st != MP_OK) { mp_transport_destroy(h); throw_status(st); }
     return h;
 }

@@ -119,6 +119,14 @@ class Transport:
         return a, b
 
     CFL, FIXED = 0, 1
+    ZERO_FLUX, TEMPERATURE, FLUX = 0, 1, 2
+
+    def set_thermal_bc(self, types=(0, 0, 0, 0), values=(0.0, 0.0, 0.0, 0.0)):
+        """Thermal conditions per wall (bottom, top, left, right): ZERO_FLUX,
+        TEMPERATURE (dimensionless T) or FLUX (outward diffusive flux per length)."""
+        ti = (C.c_int * 4)(*[int(x) for x in types])
+        tv = (C.c_double * 4)(*[float(x) for x in values])
+        _capi.check(self._lib.mp_transport_set_thermal_bc(self._h, ti, tv))
 
     def set_time_control(self, control: int, t_end: float = float("inf")):
         """time.control ("cfl" = CFL, "fixed" = FIXED) and time.end of the coupled loop."""

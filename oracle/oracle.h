@@ -109,6 +109,10 @@ int orc_transport_step(orc_transport* t, int nsteps, orc_step_report* report);
 /* Time controls of evolve.cpp:449-457,483: control 0 = cfl, 1 = fixed (dt =
  * dt_initial); t_end = INFINITY for none (the last step lands on t_end). */
 int orc_transport_set_time_control(orc_transport* t, int control, double t_end);
+/* Thermal diffusion (evolve.cpp:330-349): diffusivity kappa >= 0 and, per wall
+ * (0 bottom y0, 1 top y1, 2 left x0, 3 right x1), type 0 zero flux, 1
+ * prescribed temperature, 2 prescribed outward flux, with its value. */
+int orc_transport_set_diffusion(orc_transport* t, double kappa, const int* types, const double* values);
 int orc_transport_limiter(orc_transport* t, double* thetaH, double* thetaC);
 
 /* Synthetic input builders shared by tests and bench (SplitMix64 noise as in

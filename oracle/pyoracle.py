@@ -84,8 +84,10 @@ class _Lib:
         t("create").restype = C.c_void_p
         t("create").argtypes = [C.POINTER(Material), C.POINTER(TransportOpts)]
         t("destroy").argtypes = [C.c_void_p]
-        for n in ["set_face_velocity", "set_state", "get_state", "rhs", "limiter", "step", "set_time_control"]:
+        for n in ["set_face_velocity", "set_state", "get_state", "rhs", "limiter", "step", "set_time_control",
+                  "set_diffusion"]:
             t(n).restype = C.c_int
+        t("set_diffusion").argtypes = [C.c_void_p, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         t("set_time_control").argtypes = [C.c_void_p, C.c_int, C.c_double]
         t("set_face_velocity").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         t("set_state").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double]
@@ -228,6 +230,13 @@ class TransportOracle:
         a, b = np.zeros(n), np.zeros(n)
         code = self.lib.f("transport_limiter")(self.h, _dptr(a), _dptr(b))
         return code, a, b
+
+    def set_diffusion(self, kappa: float, types=(0, 0, 0, 0), values=(0.0, 0.0, 0.0, 0.0)):
+        """kappa and per-wall thermal conditions (bottom, top, left, right):
+        0 zero flux, 1 prescribed temperature, 2 prescribed outward flux."""
+        ti = (C.c_int * 4)(*[int(x) for x in types])
+        tv = (C.c_double * 4)(*[float(x) for x in values])
+        return self.lib.f("transport_set_diffusion")(self.h, float(kappa), ti, tv)
 
     def set_time_control(self, control: int, t_end: float = float("inf")):
         return self.lib.f("transport_set_time_control")(self.h, int(control), float(t_end))

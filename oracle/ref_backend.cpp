@@ -127,6 +127,30 @@ struct RefBackend {
             s.sides.push_back(side == DiffusiveSampleSide::Left ? 0 : (side == DiffusiveSampleSide::Right ? 1 : 2));
         s.boundary = ds.IsBoundary();
         s.normal = O(ds.Normal());
+        s.spacing = ds.Spacing();
+        s.weights = ds.QuadratureWeights();
+        s.coefficients = ds.Coefficients();
+        s.native = std::make_shared<DiffusiveSampling>(ds);
+    }
+    // The reference's own IntegrateDiffusive(Boundary)FluxWithDerivatives
+    // (diffusiveflux.h:150-193) on its own sampling object.
+    static void diffuse(const orc::Sampling& s, const std::vector<double>& samples, double kappa,
+                        const orc::ThermalBC* bc, double& flux, std::vector<double>& deriv) {
+        const auto& ds = *static_cast<const DiffusiveSampling*>(s.native.get());
+        const std::vector<PetscReal> kap(ds.QuadraturePoints().size(), kappa);
+        DiffusiveEdgeFluxResult r;
+        if (bc) {
+            DiffusiveBoundaryValue v;
+            v.type = bc->type == 0 ? DiffusiveBoundaryType::ZeroFlux
+                   : (bc->type == 1 ? DiffusiveBoundaryType::PrescribedQuantity : DiffusiveBoundaryType::PrescribedFlux);
+            v.value = bc->type == 0 ? 0.0 : bc->value;
+            const std::vector<DiffusiveBoundaryValue> data(ds.QuadraturePoints().size(), v);
+            check(IntegrateDiffusiveBoundaryFluxWithDerivatives(ds, samples, kap, data, 0.0, {}, r));
+        } else {
+            check(IntegrateDiffusiveFluxWithDerivatives(ds, samples, kap, 0.0, {}, r));
+        }
+        flux = r.flux;
+        deriv = r.derivativeSamples;
     }
     static bool phase(const orc_material&, const orc_derived&, double H, double C, double Pp, orc_phase& s, int& code) {
         const EutecticModel* m = shared_model();
@@ -206,5 +230,8 @@ int ref_transport_rhs(void* t, double* a, double* b, double* T, double* phi, dou
 int ref_transport_limiter(void* t, double* a, double* b) { return RefApi::limiter(t, a, b); }
 int ref_transport_step(void* t, int n, orc_step_report* r) { return RefApi::step(t, n, r); }
 int ref_transport_set_time_control(void* t, int control, double t_end) { return RefApi::set_time_control(t, control, t_end); }
+int ref_transport_set_diffusion(void* t, double kappa, const int* types, const double* values) {
+    return RefApi::set_diffusion(t, kappa, types, values);
+}
 
 }  // extern "C"

@@ -21,6 +21,7 @@
 #include <cstdint>
 #include <limits>
 #include <stdexcept>
+#include <memory>
 #include <vector>
 
 namespace orc {
@@ -411,7 +412,94 @@ struct Sampling {
     std::vector<Pt> points;
     Pt normal;
     bool boundary = false;
+    std::shared_ptr<const void> native;   // the reference's own sampling object (reference-backed build)
 };
+
+// diffusiveflux.cpp:203-253: first-derivative weights on the uniform nodes
+// 0..n (n = count - 1), at n/2 (middle, count even) or at n (end).
+inline std::vector<double> lagrange_derivative_weights(int count, bool middle) {
+    const int n = count - 1;
+    std::vector<double> w((size_t)count);
+    auto real = [](ld v) {
+        require(std::isfinite(v) && std::fabs(v) <= (ld)std::numeric_limits<double>::max(), E_FP,
+                "Diffusion geometry, flux or derivative is not representable");
+        return (double)v;
+    };
+    if (middle) {
+        ld factor = std::exp2(1.0L - n);
+        for (int k = 3; k <= n; k += 2) factor *= (ld)k / (k - 1);
+        if ((count / 2) % 2) factor = -factor;
+        ld choose = 1;
+        for (int i = 0; i < count / 2; ++i) {
+            const ld den = (ld)n - 2.0L * i;
+            w[i] = real(factor * choose / (den * den));
+            w[n - i] = -w[i];
+            choose *= (ld)(n - i) / (i + 1);
+            factor = -factor;
+        }
+    } else {
+        ld harmonic = 0;
+        for (int j = 1; j <= n; ++j) harmonic += 1.0L / j;
+        w[n] = real(harmonic);
+        ld choose = 1, sign = n % 2 ? -1 : 1;
+        for (int i = 0; i < n; ++i) {
+            w[i] = real(sign * choose / (n - i));
+            choose *= (ld)(n - i) / (i + 1);
+            sign = -sign;
+        }
+    }
+    return w;
+}
+
+// Thermal boundary data at one Gauss point (EvaluateThermalBoundary,
+// initialization.cpp:490-506): 0 zero flux, 1 prescribed temperature,
+// 2 prescribed outward flux per unit length.
+struct ThermalBC { int type = 0; double value = 0; };
+
+// diffusiveflux.cpp:105-200 with the identity law (psi = T): the edge's
+// diffusive flux and d flux / d sample per sample (zero at boundary slots).
+inline void integrate_diffusion(const Sampling& s, const std::vector<double>& samples, double kappa,
+                                const ThermalBC* bc, double& flux, std::vector<double>& deriv) {
+    const size_t nq = s.points.size(), count = s.coefficients.size();
+    auto real = [](ld v) {
+        require(std::isfinite(v) && std::fabs(v) <= (ld)std::numeric_limits<double>::max(), E_FP,
+                "Diffusion geometry, flux or derivative is not representable");
+        return (double)v;
+    };
+    ld last_coef = 0;
+    for (size_t k = 0; k + 1 < count; ++k) last_coef -= s.coefficients[k];
+    ld integral = 0;
+    deriv.assign(samples.size(), 0.0);
+    std::vector<double> v(count);
+    for (size_t q = 0; q < nq; ++q) {
+        const double weight = s.weights[q];
+        const int type = bc ? bc->type : -1;
+        if (bc) {
+            if (type == 0) continue;
+            require(std::isfinite(bc->value), E_OUTOFRANGE, "Boundary data must be finite");
+            if (type == 2) { integral += (ld)weight * bc->value; continue; }
+        }
+        require(std::isfinite(kappa) && kappa >= 0, E_OUTOFRANGE, "Diffusivity must be finite and nonnegative");
+        for (size_t k = 0; k < count; ++k) {
+            const size_t a = q * count + k;
+            const double u = (bc && k + 1 == count) ? bc->value : samples[a];
+            require(std::isfinite(u), E_OUTOFRANGE, "Diffusion sample state must be finite");
+            v[k] = u;
+        }
+        ld gradient = 0;
+        for (size_t k = 0; k + 1 < count; ++k) gradient += (ld)s.coefficients[k] * ((ld)v[k] - v.back());
+        gradient /= s.spacing[q];
+        require(std::isfinite(gradient), E_FP, "Sampled normal derivative overflowed");
+        integral -= (ld)weight * kappa * gradient;
+        const ld scale = -(ld)weight * kappa / s.spacing[q];
+        for (size_t k = 0; k < count; ++k) {
+            const ld coef = k + 1 == count ? last_coef : (ld)s.coefficients[k];
+            const double partial = real(scale * coef * 1.0);
+            if (!(bc && k + 1 == count)) deriv[q * count + k] = partial;
+        }
+    }
+    flux = real(integral);
+}
 
 // diffusiveflux.cpp:255-334 with numberOfSamples N and extentFraction f.
 inline void build_sampling(Pt a, Pt b, const Quad& left, const Quad* right,
@@ -423,6 +511,7 @@ inline void build_sampling(Pt a, Pt b, const Quad& left, const Quad* right,
     const int rf = right ? find_face(*right, a, b, true) : 0;
     s.boundary = right == nullptr;
     const int count = s.boundary ? N + 1 : N;
+    s.coefficients = lagrange_derivative_weights(count, !s.boundary);
     const size_t nq = rp.size();
     s.points.resize(nq); s.spacing.resize(nq); s.weights.resize(nq);
     s.samples.resize(nq * count); s.sides.resize(nq * count);

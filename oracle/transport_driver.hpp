@@ -93,6 +93,19 @@ struct Driver {
     // Time controls (evolve.cpp:449-457,483): end time and the "fixed" control.
     double t_end = INFINITY;
     bool fixed = false;
+    // Thermal diffusion (evolve.cpp:330-349): constant diffusivity and one
+    // thermal condition per wall (0 bottom y0, 1 top y1, 2 left x0, 3 right x1).
+    double kappa = 0;
+    ThermalBC wall_bc[4];
+    bool diffusion_active() const {
+        if (kappa > 0) return true;
+        for (const auto& b : wall_bc) if (b.type == 2) return true;
+        return false;
+    }
+    int wall_of(const Face& f) const {
+        if (f.edge < nIedge) return f.edge / nx == 0 ? 0 : 1;
+        return (f.edge - nIedge) % (nx + 1) == 0 ? 2 : 3;
+    }
     int nq = 5;
     int samples_n = 4;
     double samples_frac = 0.9;
@@ -402,12 +415,22 @@ struct Driver {
                     require(std::isfinite(sens), E_FP, "Singular phase derivative in CFL estimate");
                     rt += weight * (aC + aH + 2 * std::fabs(vs)) * sens;
                 }
-                // Diffusion samples (zero diffusivity: admissibility checks only).
+                // Diffusion samples: temperatures of the limited states
+                // (evolve.cpp:332-338), then the normal-line flux (:339-347).
+                std::vector<double> Ts(f.diffusion.samples.size(), 0.0);
                 for (size_t s = 0; s < f.diffusion.samples.size(); ++s) {
                     const int side = f.diffusion.sides[s];
                     if (side == 2) continue;
                     orc_phase ph; double h, c;
                     phase_at(side == 0 ? f.left : f.right, f.diffusion.samples[s], ph, h, c);
+                    Ts[s] = ph.TDp;
+                }
+                if (diffusion_active()) {
+                    double dflux = 0;
+                    std::vector<double> deriv;
+                    B::diffuse(f.diffusion, Ts, kappa, f.boundary ? &wall_bc[wall_of(f)] : nullptr, dflux, deriv);
+                    fluxH += dflux;
+                    for (double d : deriv) rt += std::fabs(d);   // evolve.cpp:346
                 }
                 fH[fi] = fluxH; fC[fi] = fluxC; fR[fi] = rt; fM[fi] = fluxMix;
         });
@@ -618,6 +641,18 @@ struct Api {
             return 0;
         } catch (const Error& e) { return e.code; }
     }
+    static int set_diffusion(void* h, double kappa, const int* types, const double* values) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        if (!(std::isfinite(kappa) && kappa >= 0)) return E_OUTOFRANGE;
+        for (int w = 0; w < 4; ++w) {
+            if (types[w] < 0 || types[w] > 2 || !std::isfinite(values[w])) return E_OUTOFRANGE;
+            d.wall_bc[w] = ThermalBC{types[w], values[w]};
+        }
+        d.kappa = kappa;
+        d.have_current = false;
+        return 0;
+    }
+
     static int set_time_control(void* h, int control, double t_end) {
         auto& d = static_cast<Handle<B>*>(h)->d;
         if (control != 0 && control != 1) return E_OUTOFRANGE;

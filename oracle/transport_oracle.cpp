@@ -95,6 +95,10 @@ struct Restated {
     static bool phase(const orc_material& m, const orc_derived& d, double H, double C, double P, orc_phase& s, int& code) {
         return orc_internal::phase_eval(m, d, H, C, P, s, code);
     }
+    static void diffuse(const Sampling& s, const std::vector<double>& samples, double kappa, const ThermalBC* bc,
+                        double& flux, std::vector<double>& deriv) {
+        integrate_diffusion(s, samples, kappa, bc, flux, deriv);
+    }
     static bool derive(const orc_material& m, orc_derived& d) { return orc_internal::derive(m, d); }
 };
 
@@ -124,6 +128,9 @@ extern "C" int orc_transport_limiter(orc_transport* t, double* thetaH, double* t
 }
 extern "C" int orc_transport_step(orc_transport* t, int nsteps, orc_step_report* report) {
     return RestatedApi::step(t, nsteps, report);
+}
+extern "C" int orc_transport_set_diffusion(orc_transport* t, double kappa, const int* types, const double* values) {
+    return RestatedApi::set_diffusion(t, kappa, types, values);
 }
 extern "C" int orc_transport_set_time_control(orc_transport* t, int control, double t_end) {
     return RestatedApi::set_time_control(t, control, t_end);

@@ -140,7 +140,7 @@ def test_invalid_configurations_are_rejected(cuda_lib):
     with pytest.raises(MPError):
         Transport(sy.Workload(nx=4, ny=4), TransportConfig(cfl=1.5))
     with pytest.raises(MPError):
-        Transport(sy.Workload(nx=4, ny=4), TransportConfig(diffusivity=1e-3))
+        Transport(sy.Workload(nx=4, ny=4), TransportConfig(diffusivity=-1e-3))
 
 
 @pytest.mark.parametrize("control", [0, 1], ids=["cfl", "fixed"])
@@ -188,3 +188,85 @@ def test_fixed_step_above_cfl_bound_is_rejected(cuda_lib):
     assert err.value.code == 63
     assert t.get_time() == (0.0, 0)
     assert np.array_equal(t.get_state()[0], H)
+
+
+DIFFUSION_BCS = {"T_top_flux_bottom": ((1, 2, 0, 0), (0.9, -0.02, 0.0, 0.0)),
+                 "T_sides": ((0, 0, 1, 1), (0.0, 0.0, 0.5, 0.6)),
+                 "insulated": ((0, 0, 0, 0), (0.0, 0.0, 0.0, 0.0))}
+
+
+@pytest.mark.parametrize("bc", list(DIFFUSION_BCS))
+def test_diffusion_matches_oracle(cuda_lib, bc):
+    """Thermal diffusion (evolve.cpp:330-349; the oracle equals the reference's
+    own diffusiveflux.cpp bit for bit): stage RHS and rate to 1e-12, 10 SSPRK3
+    steps to 1e-12 with the same retry sequence."""
+    from oracle import pyoracle as po
+    from mantlepar_b200.transport import Transport, TransportConfig
+    w = sy.Workload(nx=12, ny=14, seed=6)
+    types, values = DIFFUSION_BCS[bc]
+    t = Transport(w, TransportConfig(cfl=w.cfl, integrator=3, diffusivity=0.02))
+    t.set_thermal_bc(types, values)
+    o = po.TransportOracle(sy.material_s(), w, integrator=3)
+    assert o.set_diffusion(0.02, types, values) == 0
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    for x in (t, o):
+        x.set_face_velocity(vs, ud)
+        x.set_state(H, C)
+    r = t.rhs()
+    code, ref = o.rhs()
+    assert code == 0
+    for k in ["T", "phi", "rate"]:
+        assert rel(r[k], ref[k]) <= RTOL_STAGE, k
+    for k in ["rhsH", "rhsC"]:
+        assert rel_inf(r[k], ref[k]) <= RTOL_STAGE, k
+    assert abs(r["boundaryH"] - ref["boundaryH"]) <= 1e-12 * max(1.0, abs(ref["boundaryH"]))
+    _, got = t.step(10)
+    code, want = o.step(10)
+    assert code == 0
+    assert [x["retries"] for x in got] == [x["retries"] for x in want]
+    a, b = np.stack(t.get_state()), np.stack(o.get_state())
+    for k in range(4):
+        assert rel(a[k], b[k]) <= RTOL_RUN10, k
+
+
+def test_diffusion_batched_and_slabs_equal_single(cuda_lib):
+    """With diffusion on, a batched instance and a decomposed mesh reproduce the
+    single instance bit for bit."""
+    import torch
+    from mantlepar_b200.batch import Batch
+    from mantlepar_b200.domain import Slab, ThreadExchange, partition
+    from mantlepar_b200.transport import Transport, TransportConfig
+    w = sy.Workload(nx=16, ny=20, seed=8)
+    cfg = TransportConfig(cfl=0.4, integrator=3, diffusivity=0.01)
+    types, values = DIFFUSION_BCS["T_top_flux_bottom"]
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    t = Transport(w, cfg)
+    t.set_thermal_bc(types, values)
+    t.set_face_velocity(vs, ud)
+    t.set_state(H, C)
+    _, reps = t.step(6)
+    ref = np.stack(t.get_state())
+    b = Batch([w, sy.Workload(nx=8, ny=10, seed=2)], cfg)
+    b.set_thermal_bc(types, values)
+    b.set_face_velocity(0, vs, ud)
+    b.set_state(0, H, C)
+    v2, u2 = sy.face_velocity(sy.Workload(nx=8, ny=10, seed=2))
+    H2, C2 = sy.initial_state(sy.Workload(nx=8, ny=10, seed=2))
+    b.set_face_velocity(1, v2, u2)
+    b.set_state(1, H2, C2)
+    for _ in range(6):
+        b.step(1)
+    g = b.get_state(0)
+    assert np.array_equal(np.stack([g["H"], g["C"], g["T"], g["phi"]]), ref)
+    slabs = [Slab(w, r, cfg, stream=torch.cuda.Stream()) for r in partition(w.ny, 3)]
+    for s in slabs:
+        s.set_thermal_bc(types, values)
+        s.set_face_velocity(vs, ud)
+        s.set_state(H, C)
+    outs = ThreadExchange(slabs).step(6)
+    for code, r in outs:
+        assert code == 0 and [x["dt"] for x in r] == [x["dt"] for x in reps]
+    got = np.concatenate([np.stack(s.get_state()) for s in slabs], axis=1)
+    assert np.array_equal(got, ref)

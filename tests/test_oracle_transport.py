@@ -124,3 +124,47 @@ def test_oracle_time_controls():
     assert code == 63
     H1, C1, _, _ = g.get_state()
     assert np.array_equal(H0, H1) and np.array_equal(C0, C1)
+
+
+@pytest.mark.skipif(not po.reference_available(), reason="reference-backed oracle not built")
+@pytest.mark.parametrize("bc", [((1, 2, 0, 0), (0.9, -0.02, 0.0, 0.0)), ((0, 0, 1, 1), (0.0, 0.0, 0.5, 0.6)),
+                                ((0, 0, 0, 0), (0.0, 0.0, 0.0, 0.0))], ids=["T_top_flux_bottom", "T_sides", "insulated"])
+def test_diffusion_restatement_equals_reference_bitwise(bc):
+    """Thermal diffusion (diffusiveflux.cpp:105-334 through evolve.cpp:330-349):
+    the restated integration and derivative weights equal the reference's own
+    functions bit for bit, for the RHS and for 10 SSPRK3 steps."""
+    w = sy.Workload(nx=12, ny=14, seed=6)
+    out = []
+    for lib in (po.restated(), po.reference()):
+        t = _oracle(w, integrator=3, lib=lib)
+        assert t.set_diffusion(0.02, *bc) == 0
+        code, r = t.rhs()
+        assert code == 0
+        code, reps = t.step(10)
+        assert code == 0
+        out.append((r, t.get_state(), reps))
+    (ra, sa, pa), (rb, sb, pb) = out
+    for k in ["rhsH", "rhsC", "T", "phi", "rate"]:
+        assert np.array_equal(bits(ra[k]), bits(rb[k])), k
+    for x, y in zip(sa, sb):
+        assert np.array_equal(bits(x), bits(y))
+    assert [r["dt"] for r in pa] == [r["dt"] for r in pb]
+
+
+def test_diffusion_changes_the_solution_as_expected():
+    """Diffusion moves heat down the temperature gradient: with an insulated
+    box the H integral is conserved; with a hot top wall heat flows in."""
+    w = sy.Workload(nx=12, ny=14, seed=6)
+    base = _oracle(w, integrator=3)
+    _, r0 = base.rhs()
+    ins = _oracle(w, integrator=3)
+    ins.set_diffusion(0.02)
+    _, r1 = ins.rhs()
+    hot = _oracle(w, integrator=3)
+    hot.set_diffusion(0.02, (0, 1, 0, 0), (0.0, 3.0, 0.0, 0.0))
+    _, r2 = hot.rhs()
+    assert not np.array_equal(r0["rhsH"], r1["rhsH"])
+    assert np.array_equal(r0["rhsC"], r1["rhsC"])                     # C does not diffuse
+    assert abs(r1["boundaryH"] - r0["boundaryH"]) < 1e-15              # insulated: no extra boundary flux
+    assert r2["boundaryH"] < r1["boundaryH"]                           # hot top wall: heat flows in
+    assert r1["maxRate"] > r0["maxRate"]                               # diffusion enters the CFL rate
