@@ -67,9 +67,15 @@ struct TimeInput {
 
 enum class Integrator { SSPRK2 = 2, SSPRK3 = 3 };
 
+// Phase-law pressure (the reference's pressure model "constant" or
+// "lithostatic"): constant `pressure` Pa, or rho g l0 (surfaceY - y).
+enum class PressureModel { Constant, Lithostatic };
+
 struct Configuration {
     phase::EutecticModel phase;
-    double pressure = 0.0;               // phase-law pressure [Pa], constant
+    double pressure = 0.0;               // constant model: phase-law pressure [Pa]
+    PressureModel pressureModel = PressureModel::Constant;
+    double surfaceY = 0.0;               // lithostatic model: surface height (>= mesh top)
     TransportBoundarySpecification boundary;
     LaxFriedrichsOptions stabilizer;
     double thermalDiffusivity = 0.0;     // kappa >= 0 (normal-line sampled diffusion of T)
@@ -91,9 +97,12 @@ struct InitialState {
     long acceptedSteps = 0;
 };
 
-// Normal components at [edge*5 + q] against the canonical right normal.
+// Normal components at [edge*5 + q] against the canonical right normal, and
+// (needed when phase.parameters().alpha0 != 0: the adiabatic source) the
+// vertical components at the cell quadrature points [cell*25 + b*5 + a].
 struct EdgeVelocities {
     std::vector<double> solid, darcy;
+    std::vector<double> cellSolidY, cellDarcyY;
 };
 
 struct Rates {

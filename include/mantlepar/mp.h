@@ -222,6 +222,21 @@ mp_status mp_transport_set_time_control(mp_transport* t, int control, double t_e
 enum { MP_THERMAL_ZERO_FLUX = 0, MP_THERMAL_TEMPERATURE = 1, MP_THERMAL_FLUX = 2 };
 mp_status mp_transport_set_thermal_bc(mp_transport* t, const int* type, const double* value);
 
+/* Phase-law pressure (initialization.cpp:148-163): MP_PRESSURE_CONSTANT with
+ * value = pressure in Pa (>= 0; the create-time opts.pressure), or
+ * MP_PRESSURE_LITHOSTATIC with value = surface_y (>= the mesh top): P(y) =
+ * rho g l0 (surface_y - y) (EutecticModel::staticPressure), so the eutectic
+ * temperature of every evaluation point depends on its height. */
+enum { MP_PRESSURE_CONSTANT = 0, MP_PRESSURE_LITHOSTATIC = 1 };
+mp_status mp_transport_set_pressure_model(mp_transport* t, int model, double value);
+
+/* Vertical solid and Darcy velocity components at the 5x5 cell quadrature
+ * points, [cell*25 + b*5 + a] (point (g_a, g_b) of the cell's Gauss rule), from
+ * the flow supplier (flow_sampling.cpp:93-101). Required when alpha0 != 0:
+ * the adiabatic source -alpha0 l0 g / cp * T * v_mix,y (evolve.cpp:359-369).
+ * On a slab: the cells of the local mesh. */
+mp_status mp_transport_set_cell_velocity(mp_transport* t, const double* vs_y, const double* ud_y);
+
 /* Current time and accepted steps (InitialState::time, acceptedSteps). */
 mp_status mp_transport_get_time(const mp_transport* t, double* time, int* accepted);
 
@@ -246,6 +261,7 @@ mp_status mp_transport_get_time(const mp_transport* t, double* time, int* accept
  *    same order. */
 typedef struct mp_stage_partials {
     double maxRate, divergence, boundaryH, boundaryC, H_integral, C_integral, Hmin, Cmin, Cmax, nonfinite;
+    double sourceH;   /* adiabatic source integral: sum */
 } mp_stage_partials;
 /* H, C: the stage input (device, local rows); return 0 or a status. */
 typedef int (*mp_halo_fn)(void* user, double* H, double* C);

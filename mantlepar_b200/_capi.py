@@ -143,6 +143,8 @@ def lib() -> C.CDLL:
         "mp_serve_set_policy": (i, [vp, i, d]),
         "mp_transport_set_time_control": (i, [vp, i, d]),
         "mp_transport_set_thermal_bc": (i, [vp, C.POINTER(C.c_int), dp]),
+        "mp_transport_set_pressure_model": (i, [vp, i, d]),
+        "mp_transport_set_cell_velocity": (i, [vp, vp, vp]),
         "mp_batch_set_thermal_bc": (i, [vp, C.POINTER(C.c_int), dp]),
         "mp_transport_create_slab": (i, [C.POINTER(MeshDesc), i, i, C.POINTER(TransportOpts), vp, C.POINTER(vp)]),
         "mp_transport_slab_layout": (i, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),

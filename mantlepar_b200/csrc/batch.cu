@@ -123,20 +123,14 @@ __global__ void __launch_bounds__(1024) batch_reduce_kernel(const Partial* parti
     const int inst = blockIdx.x;
     if (!active[inst]) return;
     const int off = part_off[inst], cnt = part_cnt[inst];
-    Partial v{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
-    for (int b = threadIdx.x; b < cnt; b += blockDim.x) {
-        const Partial p = partial[off + b];
-        v.maxRate = fmax(v.maxRate, p.maxRate); v.divergence = fmax(v.divergence, p.divergence);
-        v.bH += p.bH; v.bC += p.bC; v.HI += p.HI; v.CI += p.CI;
-        v.Hmin = fmin(v.Hmin, p.Hmin); v.Cmin = fmin(v.Cmin, p.Cmin); v.Cmax = fmax(v.Cmax, p.Cmax);
-        v.nonfinite = fmax(v.nonfinite, p.nonfinite);
-    }
+    Partial v = partial_identity();
+    for (int b = threadIdx.x; b < cnt; b += blockDim.x) fold_partial(v, partial[off + b]);
     __shared__ Partial result;
     block_reduce_write(v, &result);
     __syncthreads();
     if (threadIdx.x == 0)
         out[inst] = Totals{result.maxRate, result.divergence, result.bH, result.bC, result.HI, result.CI,
-                           result.Hmin, result.Cmin, result.Cmax, result.nonfinite};
+                           result.Hmin, result.Cmin, result.Cmax, result.nonfinite, result.sH};
 }
 
 }  // namespace
@@ -647,7 +641,7 @@ extern "C" mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, cons
     if (!(opts->cfl > 0 && opts->cfl <= 1)) { set_error("Coupled CFL must be in (0,1]"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->integrator != MP_SSPRK2 && opts->integrator != MP_SSPRK3) { set_error("integrator must be 2 or 3"); return MP_ERR_ARG_OUTOFRANGE; }
     if (!(std::isfinite(opts->diffusivity) && opts->diffusivity >= 0.0)) { set_error("Diffusivity must be finite and nonnegative"); return MP_ERR_ARG_OUTOFRANGE; }
-    if (opts->material.alpha0 != 0.0) { set_error("adiabatic source (alpha0 != 0) is not supported by this build"); return MP_ERR_ARG_WRONG; }
+    if (opts->material.alpha0 != 0.0) { set_error("the batched engine does not take cell-point velocities: adiabatic source (alpha0 != 0) needs the single-instance path"); return MP_ERR_ARG_WRONG; }
     if (opts->precision != MP_PRECISION_FP64 && opts->precision != MP_PRECISION_MIXED) { set_error("unknown precision"); return MP_ERR_ARG_OUTOFRANGE; }
     mp_derived der;
     MP_TRY(derive_checked(opts->material, der));
@@ -664,6 +658,8 @@ extern "C" mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, cons
     b->ph.kappa = opts->diffusivity;
     for (int w = 0; w < 4; ++w) { b->ph.wall_type[w] = 0; b->ph.wall_value[w] = 0.0; }
     b->ph.diffusion = opts->diffusivity > 0.0;
+    b->ph.litho = 0; b->ph.tep_a = b->ph.tep_b = b->ph.surface = 0.0;
+    b->ph.source = 0; b->ph.cooling = 0.0;
     b->inst.resize(count);
     for (int i = 0; i < count; ++i) {
         if (meshes[i].nx < 2 || meshes[i].ny < 2) { set_error("instance %d: at least 2x2 cells", i); mp_batch_destroy(b); return MP_ERR_ARG_SIZ; }

@@ -42,22 +42,52 @@ struct Physics {
     double kappa;
     int wall_type[4];
     double wall_value[4];
+    // Phase-law pressure: constant (litho = 0, Tep above), or lithostatic
+    // rho g l0 (surface - y): Tep(y) = tep_a + tep_b (surface - y).
+    int litho;
+    double tep_a, tep_b, surface;
+    // Adiabatic source -cooling T v_mix,y (evolve.cpp:359-369), cooling =
+    // alpha0 l0 g / cp; on when alpha0 != 0.
+    int source;
+    double cooling;
 };
+
+// Pressure-corrected eutectic temperature at height y (one FMA for the
+// lithostatic model; the constant model returns the stored value exactly).
+__device__ __forceinline__ double tep_at(const Physics& ph, double y) {
+    return ph.litho ? fma(ph.tep_b, ph.surface - y, ph.tep_a) : ph.Tep;
+}
+
+// Height of a point at normalised eta in the cell of global row gj.
+__device__ __forceinline__ double height(const StageHot& t, int gj, double eta) {
+    return t.y0 + (gj + 0.5) * t.dy + eta * t.hn;
+}
 
 // Block partials of one stage (sum_kernel) or state check (axpy_kernel).
 struct Partial {
     double maxRate, divergence, bH, bC, HI, CI, Hmin, Cmin, Cmax;
     double nonfinite;
+    double sH;             // adiabatic source integral
 };
 
 __device__ __forceinline__ Partial partial_identity() {
-    return Partial{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
+    return Partial{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0, 0.0};
 }
 
 struct Totals {
     double maxRate, divergence, bH, bC, HI, CI, Hmin, Cmin, Cmax;
     double nonfinite;
+    double sH;
 };
+
+// Fold one block partial into a running partial (fixed field rules).
+__device__ __forceinline__ void fold_partial(Partial& v, const Partial& p) {
+    v.maxRate = fmax(v.maxRate, p.maxRate); v.divergence = fmax(v.divergence, p.divergence);
+    v.bH += p.bH; v.bC += p.bC; v.HI += p.HI; v.CI += p.CI;
+    v.Hmin = fmin(v.Hmin, p.Hmin); v.Cmin = fmin(v.Cmin, p.Cmin); v.Cmax = fmax(v.Cmax, p.Cmax);
+    v.nonfinite = fmax(v.nonfinite, p.nonfinite);
+    v.sH += p.sH;
+}
 
 // Row slabs of a decomposed mesh: the local arrays hold rows gj0 .. of a
 // global mesh of gny rows (gny = 0: the local mesh is the whole mesh).
@@ -264,8 +294,10 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
     // check). Limited values at limiter points stay in [lo, hi], so the
     // samples are admissible when hi_H is below the liquidus at hi_C and
     // Tep >= 0; otherwise the phase kernel checks each sample exactly.
-    const double Hliq = ph.Tep + (1.0 - hiC / ph.k.Xe) + ph.k.LD;
-    const bool safe = ph.Tep >= 0.0 && hiH + 1e-12 * (1.0 + fabs(hiH)) < Hliq;
+    // (With a lithostatic pressure the lower Tep over the cell's height bounds it.)
+    const double tep = ph.litho ? fmin(tep_at(ph, t.y0 + gj * t.dy), tep_at(ph, t.y0 + (gj + 1) * t.dy)) : ph.Tep;
+    const double Hliq = tep + (1.0 - hiC / ph.k.Xe) + ph.k.LD;
+    const bool safe = tep >= 0.0 && hiH + 1e-12 * (1.0 + fabs(hiH)) < Hliq;
 #pragma unroll
     for (int m = 0; m < 9; ++m) {
         a.rec[(size_t)m * N + cell] = DH[m] * thH;
@@ -290,6 +322,14 @@ struct CellPhaseArgs {
     double* phi;
     unsigned long long* status;
     int gj0 = 0, gny = 0;  // slab: global row of local row 0, global rows
+    // Adiabatic source (when Physics::source): vertical solid and Darcy
+    // velocities at the cell points [cell*25 + b*5 + a]; per cell the heat
+    // sum w/A * source, the rate sum w/A * cooling |v_y| and sum w * source.
+    const double* cvs_y = nullptr;
+    const double* cud_y = nullptr;
+    double* srcH = nullptr;
+    double* srcR = nullptr;
+    double* srcS = nullptr;
 };
 
 __device__ __forceinline__ void load_rec(const double* rec, size_t N, long long cell, double* DH, double* DC) {
@@ -311,26 +351,38 @@ __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const 
     double DH[9], DC[9];
     load_rec(a.rec, (size_t)N, cell, DH, DC);
     int st_por = 0, st_cell = 0, st_face = 0;
-    double Tsum = 0.0, Psum = 0.0;
+    double Tsum = 0.0, Psum = 0.0, Ssum = 0.0, Rsum = 0.0, Wsum = 0.0;
     bool wet = false;
+    const int gjc = a.gj0 + (int)(cell / a.nx);
     for (int b = 0; b < kNQ; ++b) {
         double h0, h1, h2, c0, c1, c2;
         const double y = t.gy[b];
         q2_row(DH, y, h0, h1, h2);
         q2_row(DC, y, c0, c1, c2);
+        const double tep = ph.litho ? tep_at(ph, height(t, gjc, y)) : ph.Tep;
 #pragma unroll
         for (int q = 0; q < kNQ; ++q) {
             const double x = t.gx[q];
             const double h = mH + quad(h0, h1, h2, x);
             const double c = mC + quad(c0, c1, c2, x);
             PhaseLean pl;
-            const int s = phase_stage_lean(ph.sk, h, c, ph.Tep, pl);
+            const int s = phase_stage_lean(ph.sk, h, c, tep, pl);
             if (s) { st_por = st_por ? st_por : s; continue; }
             if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_cell = st_cell ? st_cell : E_OUTOFRANGE;
             const double w = t.cw[b * kNQ + q];
             Tsum += w * pl.T;
             Psum += w * pl.phil;
             wet = wet || pl.phil > 0.0;
+            if (ph.source) {
+                // evolve.cpp:359-369 with PhaseTransportVelocities at this point's porosity.
+                const long long at = cell * (kNQ * kNQ) + b * kNQ + q;
+                const double factor = pl.phil == 0.0 ? 0.0 : (ph.theta == 0.0 ? pl.phil : pow(pl.phil, 1.0 + ph.theta));
+                const double vy = __ldg(a.cvs_y + at) + factor * __ldg(a.cud_y + at);
+                const double src = -ph.cooling * pl.T * vy;
+                Ssum += w * src;
+                Rsum += w * ph.cooling * fabs(vy);
+                Wsum += t.cwp[b * kNQ + q] * src;
+            }
         }
     }
     const unsigned char fl = a.flags[cell];
@@ -351,8 +403,9 @@ __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const 
                 const double s_ = row ? t.gx[q] : t.gy[q];
                 const double h = mH + quad(h0, h1, h2, s_);
                 const double c = mC + quad(c0, c1, c2, s_);
+                const double tep = ph.litho ? tep_at(ph, height(t, j, row ? lc : t.gy[q])) : ph.Tep;
                 PhaseLean pl;
-                const int s = phase_stage_lean(ph.sk, h, c, ph.Tep, pl);
+                const int s = phase_stage_lean(ph.sk, h, c, tep, pl);
                 if (s) { st_face = st_face ? st_face : s; continue; }
                 if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_face = st_face ? st_face : E_OUTOFRANGE;
             }
@@ -365,6 +418,7 @@ __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const 
     a.flags[cell] = (unsigned char)((fl & FLAG_CHECK) | (wet ? FLAG_WET : 0));
     a.T[cell] = Tsum;
     a.phi[cell] = Psum;
+    if (ph.source) { a.srcH[cell] = Ssum; a.srcR[cell] = Rsum; a.srcS[cell] = Wsum; }
 }
 
 // ---------------------------------------------------------------- face kernel
@@ -402,11 +456,11 @@ __device__ __forceinline__ void side_line(const FaceArgs<R>& a, size_t N, long l
 }
 
 // Limited evaluation + phase + Phase()'s admissibility (evolve.cpp:270-277).
-__device__ __forceinline__ int side_phase(const Physics& ph, const SideLine& s, double at, double& h, double& c,
-                                          PhaseLean& pl) {
+__device__ __forceinline__ int side_phase(const Physics& ph, const SideLine& s, double at, double tep, double& h,
+                                          double& c, PhaseLean& pl) {
     h = s.mH + quad(s.h0, s.h1, s.h2, at);
     c = s.mC + quad(s.c0, s.c1, s.c2, at);
-    int st = phase_stage(ph.sk, h, c, ph.Tep, pl);
+    int st = phase_stage(ph.sk, h, c, tep, pl);
     if (!st && !(pl.T >= 0.0 && pl.phil < 1.0)) st = E_OUTOFRANGE;
     return st;
 }
@@ -420,6 +474,7 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
     const StageHot& t = *a.tab.t;
     const size_t N = (size_t)nx * ny;
     bool boundary, reverse, horizontal;
+    int erow;                // local row of the edge (horizontal) or of its cells (vertical)
     long long L, Rc = -1;
     double len;
     double lfix, rfix;   // the edge's fixed normalised coordinate in the left / right cell frame
@@ -429,6 +484,7 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
         const unsigned ue = (unsigned)e;   // edge counts stay below 2^31 (checked on create)
         const int i = (int)(ue % (unsigned)nx), j = (int)(ue / (unsigned)nx);
         const int gj = a.gj0 + j, gny = global_ny(a);
+        erow = j;
         boundary = (gj == 0 || gj == gny);
         reverse = (gj == gny);
         L = reverse ? (long long)(j - 1) * nx + i : (long long)j * nx + i;
@@ -440,6 +496,7 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
         horizontal = false;
         const unsigned k = (unsigned)(e - nI);
         const int i = (int)(k % (unsigned)(nx + 1)), j = (int)(k / (unsigned)(nx + 1));
+        erow = j;
         boundary = (i == 0 || i == nx);
         reverse = (i == 0);
         L = reverse ? (long long)j * nx : (long long)j * nx + (i - 1);
@@ -463,10 +520,13 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
         const double ud = sgn * __ldg(a.udn + e * kNQ + cq);
         double hL, cL, hR, cR;
         PhaseLean A, B;
-        int s = side_phase(ph, sl, at, hL, cL, A);
+        // Height of this Gauss point: the edge row for horizontal edges.
+        const double tep = !ph.litho ? ph.Tep
+                         : tep_at(ph, horizontal ? t.y0 + (a.gj0 + erow) * t.dy : height(t, a.gj0 + erow, at));
+        int s = side_phase(ph, sl, at, tep, hL, cL, A);
         if (boundary) { B = A; hR = hL; cR = cL; }
         else {
-            const int s2 = side_phase(ph, sr, at, hR, cR, B);
+            const int s2 = side_phase(ph, sr, at, tep, hR, cR, B);
             s = s ? s : s2;
         }
         if (s) { st = st ? st : s; continue; }
@@ -512,7 +572,7 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
             double Tb = A.T;
             if (kh == 0) {
                 PhaseLean pin;
-                const int s3 = phase_stage(ph.sk, ph.inflowH, inC, ph.Tep, pin);
+                const int s3 = phase_stage(ph.sk, ph.inflowH, inC, tep, pin);
                 if (s3) st = st ? st : s3;
                 Tb = pin.T;
             }
@@ -612,8 +672,11 @@ __device__ __forceinline__ void diffusion_edge(const FaceArgs<R>& a, const Physi
             const double s = boundary ? t.dif_pos_bnd[wall][k] : t.dif_pos_int[o][k];
             const double h = left ? mHL + quad(lh0, lh1, lh2, s) : mHR + quad(rh0, rh1, rh2, s);
             const double c = left ? mCL + quad(lc0, lc1, lc2, s) : mCR + quad(rc0, rc1, rc2, s);
+            const long long cellk = left ? L : Rc;
+            const double tep = !ph.litho ? ph.Tep
+                             : tep_at(ph, height(t, a.gj0 + (int)(cellk / nx), horizontal ? s : at));
             PhaseLean pl;
-            int s1 = phase_stage_lean(ph.sk, h, c, ph.Tep, pl);
+            int s1 = phase_stage_lean(ph.sk, h, c, tep, pl);
             if (!s1 && !(pl.T >= 0.0 && pl.phil < 1.0)) s1 = E_OUTOFRANGE;
             if (s1) st = st ? st : s1;
             v[k] = s1 ? 0.0 : pl.T;
@@ -661,6 +724,10 @@ struct SumArgs {
     int gj0 = 0, gny = 0;  // slab: global row of local row 0, global rows
     long long cbeg = 0;    // cells [cbeg, cend) are accumulated (cend < 0: all)
     long long cend = -1;
+    // Adiabatic source per cell (cell phase kernel): heat, rate, integral.
+    const double* srcH = nullptr;
+    const double* srcR = nullptr;
+    const double* srcS = nullptr;
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -681,24 +748,26 @@ __device__ __forceinline__ double warp_min(double v) {
 
 // Deterministic block reduction of a Partial (fixed shuffle tree per block).
 __device__ void block_reduce_write(Partial v, Partial* out) {
-    __shared__ double sh[32][10];
+    __shared__ double sh[32][11];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double r[10] = {v.maxRate, v.divergence, v.bH, v.bC, v.HI, v.CI, v.Hmin, v.Cmin, v.Cmax, v.nonfinite};
+    double r[11] = {v.maxRate, v.divergence, v.bH, v.bC, v.HI, v.CI, v.Hmin, v.Cmin, v.Cmax, v.nonfinite, v.sH};
     r[0] = warp_max(r[0]); r[1] = warp_max(r[1]);
     r[2] = warp_sum(r[2]); r[3] = warp_sum(r[3]); r[4] = warp_sum(r[4]); r[5] = warp_sum(r[5]);
     r[6] = warp_min(r[6]); r[7] = warp_min(r[7]); r[8] = warp_max(r[8]); r[9] = warp_max(r[9]);
+    r[10] = warp_sum(r[10]);
     if (lane == 0)
-        for (int k = 0; k < 10; ++k) sh[warp][k] = r[k];
+        for (int k = 0; k < 11; ++k) sh[warp][k] = r[k];
     __syncthreads();
     if (warp == 0) {
         const int nw = (blockDim.x + 31) >> 5;
-        const Partial id{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
-        double s[10] = {id.maxRate, id.divergence, 0, 0, 0, 0, id.Hmin, id.Cmin, id.Cmax, 0};
-        if (lane < nw) for (int k = 0; k < 10; ++k) s[k] = sh[lane][k];
+        const Partial id = partial_identity();
+        double s[11] = {id.maxRate, id.divergence, 0, 0, 0, 0, id.Hmin, id.Cmin, id.Cmax, 0, 0};
+        if (lane < nw) for (int k = 0; k < 11; ++k) s[k] = sh[lane][k];
         s[0] = warp_max(s[0]); s[1] = warp_max(s[1]);
         s[2] = warp_sum(s[2]); s[3] = warp_sum(s[3]); s[4] = warp_sum(s[4]); s[5] = warp_sum(s[5]);
         s[6] = warp_min(s[6]); s[7] = warp_min(s[7]); s[8] = warp_max(s[8]); s[9] = warp_max(s[9]);
-        if (lane == 0) *out = Partial{s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], s[8], s[9]};
+        s[10] = warp_sum(s[10]);
+        if (lane == 0) *out = Partial{s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], s[8], s[9], s[10]};
     }
 }
 
@@ -731,6 +800,11 @@ __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partia
         dv -= sg[f] * FM;
     }
     rH *= invA; rC *= invA; rr *= invA; dv *= invA;
+    double sH = 0.0;
+    if (a.srcH) {
+        // The source terms follow the face terms, as the reference adds them.
+        rH += __ldg(a.srcH + cell); rr += __ldg(a.srcR + cell); sH = __ldg(a.srcS + cell);
+    }
     if (gj == 0) { bH += __ldg(a.face + eb); bC += __ldg(a.face + nE + eb); }
     if (gj == gny - 1) { bH += __ldg(a.face + et); bC += __ldg(a.face + nE + et); }
     if (i == 0) { bH += __ldg(a.face + el); bC += __ldg(a.face + nE + el); }
@@ -755,6 +829,7 @@ __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partia
     v.HI += nh * A; v.CI += nc * A;
     v.Hmin = fmin(v.Hmin, nh); v.Cmin = fmin(v.Cmin, nc); v.Cmax = fmax(v.Cmax, nc);
     v.nonfinite = fmax(v.nonfinite, (isfinite(nh) && isfinite(nc) && isfinite(rr)) ? 0.0 : 1.0);
+    v.sH += sH;
 }
 
 // The kSumPer cells of this thread in the sum block starting at first.

@@ -339,6 +339,7 @@ int build_stage_tables(int nx, int ny, double x0, double x1, double y0, double y
     t.Y = 0.5 * dy / h;
     t.scan_guard = 1e36 / (16.0 * std::max(1.0, t.X * t.X) * std::max(1.0, t.Y * t.Y));
     fill_diffusion(t, dx, dy, h, gw);
+    t.y0 = y0; t.dy = dy; t.hn = h;
     t.epsA = 1e-2 * area;
     t.area = area;
     t.len_h = dx;
@@ -348,6 +349,7 @@ int build_stage_tables(int nx, int ny, double x0, double x1, double y0, double y
         for (int a = 0; a < kNQ; ++a) {
             const V2 r{gp[a], gp[b]};
             t.cw[b * kNQ + a] = gw[a] * gw[b] * jacobian(r, target) / area;
+            t.cwp[b * kNQ + a] = gw[a] * gw[b] * jacobian(r, target);
         }
     for (int q = 0; q < kNQ; ++q) { t.gx[q] = t.X * gp[q]; t.gy[q] = t.Y * gp[q]; }
     // Limiter points per class: class = cj*3 + ci, ci in {0: left wall, 1, 2: right wall}.

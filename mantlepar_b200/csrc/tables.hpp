@@ -62,6 +62,11 @@ struct StageHot {
     double dif_w[2][kNQ];
     double dif_pos_int[2][4];
     double dif_pos_bnd[4][4];
+    // Physical height of a point: y = y0 + (row + 0.5) * dy + eta * hn (global
+    // row; hn = sqrt(cell area) normalises the reconstruction frame), and the
+    // physical cell-quadrature weights w_a w_b |J| (q = b*5 + a).
+    double y0, dy, hn;
+    double cwp[kNQ * kNQ];
     // With every deviation coefficient below this magnitude, every limiter
     // value is finite (in FP32 too): 1e36 / (16 max(1, X^2) max(1, Y^2)),
     // the points lying within |xi| <= X, |eta| <= Y.

@@ -41,6 +41,15 @@ struct StageRange {
 
 StageRange whole(int ny) { StageRange r; r.rec1 = r.own1 = ny; return r; }
 
+// Adiabatic-source buffers of one transport (all null when alpha0 = 0).
+struct SourceBufs {
+    const double* cvs_y = nullptr;
+    const double* cud_y = nullptr;
+    double* srcH = nullptr;
+    double* srcR = nullptr;
+    double* srcS = nullptr;
+};
+
 // Single-instance kernels: one thread per cell / edge.
 // The stage tables arrive by value as a __grid_constant__ parameter, so the
 // unrolled table coefficients are constant-bank operands. Minimum resident
@@ -100,20 +109,14 @@ __global__ void __launch_bounds__(kRedBlock) axpy_kernel(int n, const double* H0
 
 // Fixed-order reduction of the block partials into one Totals.
 __global__ void __launch_bounds__(1024) reduce_kernel(const Partial* partial, int nblocks, Totals* out) {
-    Partial v{-INFINITY, 0.0, 0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, -INFINITY, 0.0};
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-        const Partial p = partial[b];
-        v.maxRate = fmax(v.maxRate, p.maxRate); v.divergence = fmax(v.divergence, p.divergence);
-        v.bH += p.bH; v.bC += p.bC; v.HI += p.HI; v.CI += p.CI;
-        v.Hmin = fmin(v.Hmin, p.Hmin); v.Cmin = fmin(v.Cmin, p.Cmin); v.Cmax = fmax(v.Cmax, p.Cmax);
-        v.nonfinite = fmax(v.nonfinite, p.nonfinite);
-    }
+    Partial v = partial_identity();
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) fold_partial(v, partial[b]);
     __shared__ Partial result;
     block_reduce_write(v, &result);
     __syncthreads();
     if (threadIdx.x == 0) {
         *out = Totals{result.maxRate, result.divergence, result.bH, result.bC, result.HI, result.CI,
-                      result.Hmin, result.Cmin, result.Cmax, result.nonfinite};
+                      result.Hmin, result.Cmin, result.Cmax, result.nonfinite, result.sH};
     }
 }
 
@@ -165,6 +168,9 @@ struct mp_transport {
     mp_halo_fn halo = nullptr;
     mp_combine_fn combine = nullptr;
     void* hook_user = nullptr;
+    // Adiabatic source: cell-point vertical velocities (25 per cell) and the
+    // per-cell source sums of a stage.
+    double *cvs_y = nullptr, *cud_y = nullptr, *srcH = nullptr, *srcR = nullptr, *srcS = nullptr;
     mp::Totals curTot{};                   // totals of L(U^n)
     // Optional per-kernel timing (CUDA events on this handle's stream).
     bool profile = false;
@@ -213,7 +219,8 @@ void harvest(mp_transport* t) {
 void free_all(mp_transport* t) {
     for (cudaEvent_t e : t->ev_pool) cudaEventDestroy(e);
     void* bufs[] = {t->H, t->C, t->S1H, t->S1C, t->S2H, t->S2C, t->LH, t->LC, t->T, t->phi,
-                    t->rec, t->flags, t->vsn, t->udn, t->face, t->rate, t->partial, t->d_tot, t->d_status};
+                    t->rec, t->flags, t->vsn, t->udn, t->face, t->rate, t->partial, t->d_tot, t->d_status,
+                    t->cvs_y, t->cud_y, t->srcH, t->srcR, t->srcS};
     for (void* b : bufs) if (b) cudaFree(b);
     if (t->h_tot) cudaFreeHost(t->h_tot);
     if (t->h_status) cudaFreeHost(t->h_status);
@@ -238,7 +245,7 @@ template <class R>
 void launch_stage_kernels(int nx, int ny, const StageRange& rg, const ParamTables& pt, const Physics& ph, const double* H, const double* C, double* rec,
                           unsigned char* flags, double* T, double* phi, const double* vsn, const double* udn,
                           double* face, unsigned long long* status, double* theta, cudaStream_t s,
-                          mp_transport* prof) {
+                          mp_transport* prof, const SourceBufs& src = SourceBufs{}) {
     const size_t NE = (size_t)nx * (ny + 1) + (size_t)(nx + 1) * ny;
     auto run = [&](int kind, auto&& f) { if (prof) timed(prof, kind, f); else f(); };
     {
@@ -247,7 +254,8 @@ void launch_stage_kernels(int nx, int ny, const StageRange& rg, const ParamTable
         run(0, [&] { recon_kernel<R><<<grd, blk, 0, s>>>(a, ph, pt, rg.rec0, rg.rec1); });
     }
     {
-        CellPhaseArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, T, phi, status, rg.gj0, rg.gny};
+        CellPhaseArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, T, phi, status, rg.gj0, rg.gny,
+                           src.cvs_y, src.cud_y, src.srcH, src.srcR, src.srcS};
         const long long c0 = (long long)rg.rec0 * nx, c1 = (long long)rg.rec1 * nx;
         run(1, [&] { cellphase_kernel<R><<<(unsigned)((c1 - c0 + 127) / 128), 128, 0, s>>>(a, ph, pt, c0, c1); });
     }
@@ -275,17 +283,26 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
         if (rc) { set_error("halo exchange failed (%d)", rc); return rc > 0 ? (mp_status)rc : MP_ERR_CUDA; }
     }
     mp_transport* prof = t->profile ? t : nullptr;
+    SourceBufs sb;
+    if (t->ph.source) {
+        if (!t->cvs_y) {
+            set_error("the adiabatic source (alpha0 != 0) needs the flow velocities at the cell quadrature points "
+                      "(mp_transport_set_cell_velocity)");
+            return MP_ERR_ARG_WRONGSTATE;
+        }
+        sb = SourceBufs{t->cvs_y, t->cud_y, t->srcH, t->srcR, t->srcS};
+    }
     if (t->mixed) {
         launch_stage_kernels<float>(t->nx, t->ny, t->range, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
-                                    t->vsn, t->udn, t->face, t->d_status, theta, s, prof);
+                                    t->vsn, t->udn, t->face, t->d_status, theta, s, prof, sb);
     } else {
         launch_stage_kernels<double>(t->nx, t->ny, t->range, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T,
-                                     t->phi, t->vsn, t->udn, t->face, t->d_status, theta, s, prof);
+                                     t->phi, t->vsn, t->udn, t->face, t->d_status, theta, s, prof, sb);
     }
     {
         SumArgs a{t->nx, t->ny, t->host_tab.area, 1.0 / t->host_tab.area, t->face, H, C, t->H, t->C, outH, outC, t->rate, mode, a0, a1, dt,
                   t->partial, nullptr, t->range.gj0, t->range.gny, (long long)t->range.own0 * t->nx,
-                  (long long)t->range.own1 * t->nx};
+                  (long long)t->range.own1 * t->nx, sb.srcH, sb.srcR, sb.srcS};
         timed(t, 3, [&] { sum_kernel<<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
     }
     timed(t, 4, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, t->sum_blocks, t->d_tot); });
@@ -415,15 +432,18 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
     // Balance (evolve.cpp:486-490) from the integrals of the new state.
     const double HI = fin.HI, CI = fin.CI;
     double bH, bC, repH, repC;
+    double repS;
     if (o.integrator == MP_SSPRK3) {
         repH = (first.bH + second.bH) / 6 + third.bH * (2.0 / 3.0);
         repC = (first.bC + second.bC) / 6 + third.bC * (2.0 / 3.0);
-        bH = HI - oldHI + dt * repH;
+        repS = (first.sH + second.sH) / 6 + third.sH * (2.0 / 3.0);
+        bH = HI - oldHI + dt * (repH - repS);
         bC = CI - oldCI + dt * repC;
     } else {
         repH = .5 * (first.bH + second.bH);
         repC = .5 * (first.bC + second.bC);
-        bH = HI - oldHI + .5 * dt * (first.bH + second.bH);
+        repS = .5 * (first.sH + second.sH);
+        bH = HI - oldHI + .5 * dt * (first.bH + second.bH - first.sH - second.sH);
         bC = CI - oldCI + .5 * dt * (first.bC + second.bC);
     }
     if (!(std::fabs(bH) < 1e-10 * std::max(1.0, std::fabs(oldHI)) && std::fabs(bC) < 1e-10)) {
@@ -441,7 +461,7 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
     ++t->accepted;
     rep = mp_step_report{};
     rep.status = 0; rep.retries = retries; rep.dt = dt; rep.time = t->time; rep.courant = courant;
-    rep.boundaryH = repH; rep.boundaryC = repC; rep.sourceH = 0.0;
+    rep.boundaryH = repH; rep.boundaryC = repC; rep.sourceH = repS;
     rep.maxRate = t->curTot.maxRate; rep.divergence = t->curTot.divergence;
     rep.balanceH = bH; rep.balanceC = bC; rep.H_integral = HI; rep.C_integral = CI;
     return MP_OK;
@@ -463,7 +483,6 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
     if (!(opts->cfl > 0 && opts->cfl <= 1)) { set_error("Coupled CFL must be in (0,1]"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->integrator != MP_SSPRK2 && opts->integrator != MP_SSPRK3) { set_error("integrator must be 2 or 3"); return MP_ERR_ARG_OUTOFRANGE; }
     if (!(std::isfinite(opts->diffusivity) && opts->diffusivity >= 0.0)) { set_error("Diffusivity must be finite and nonnegative"); return MP_ERR_ARG_OUTOFRANGE; }
-    if (opts->material.alpha0 != 0.0) { set_error("adiabatic source (alpha0 != 0) needs cell-point velocities; not supported by this build"); return MP_ERR_ARG_WRONG; }
     if (opts->precision != MP_PRECISION_FP64 && opts->precision != MP_PRECISION_MIXED) { set_error("unknown precision"); return MP_ERR_ARG_OUTOFRANGE; }
     if (opts->H_policy < 0 || opts->H_policy > 2 || opts->C_policy < 0 || opts->C_policy > 2) { set_error("unknown boundary policy"); return MP_ERR_ARG_OUTOFRANGE; }
     mp_derived der;
@@ -505,6 +524,9 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
     t->ph.kappa = opts->diffusivity;
     for (int w = 0; w < 4; ++w) { t->ph.wall_type[w] = 0; t->ph.wall_value[w] = 0.0; }
     t->ph.diffusion = opts->diffusivity > 0.0;
+    t->ph.litho = 0; t->ph.tep_a = t->ph.tep_b = t->ph.surface = 0.0;
+    t->ph.source = opts->material.alpha0 != 0.0;
+    t->ph.cooling = opts->material.alpha0 * der.l0 * opts->material.g / opts->material.cp;
     const int tb = build_stage_tables(mesh->nx, mesh->ny, mesh->x0, mesh->x1, mesh->y0, mesh->y1, t->host_tab);
     if (tb) { delete t; set_error("stencil table construction failed"); return (mp_status)tb; }
     make_param_tables(t->host_tab, t->ptab);
@@ -615,7 +637,7 @@ extern "C" mp_status mp_transport_rhs(mp_transport* t, double* rhsH, double* rhs
     if (rate) MP_CUDA(cudaMemcpyAsync(rate, t->rate + o0, b, cudaMemcpyDefault, t->stream));
     MP_CUDA(cudaStreamSynchronize(t->stream));
     if (totals) {
-        totals->boundaryH = t->curTot.bH; totals->boundaryC = t->curTot.bC; totals->sourceH = 0.0;
+        totals->boundaryH = t->curTot.bH; totals->boundaryC = t->curTot.bC; totals->sourceH = t->curTot.sH;
         totals->maxRate = t->curTot.maxRate; totals->divergence = t->curTot.divergence;
     }
     return MP_OK;
@@ -675,6 +697,53 @@ extern "C" mp_status mp_transport_set_thermal_bc(mp_transport* t, const int* typ
         flux = flux || type[w] == MP_THERMAL_FLUX;
     }
     t->ph.diffusion = t->ph.kappa > 0.0 || flux;
+    t->have_L = false;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_transport_set_pressure_model(mp_transport* t, int model, double value) {
+    if (!t) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (!std::isfinite(value)) { mp::set_error("pressure model value must be finite"); return MP_ERR_ARG_OUTOFRANGE; }
+    if (model == MP_PRESSURE_CONSTANT) {
+        if (value < 0) { mp::set_error("pressure must be nonnegative Pa"); return MP_ERR_ARG_OUTOFRANGE; }
+        double Tep;
+        if (mp::eutectic_temperature(t->ph.k, value, Tep)) { mp::set_error("pressure-corrected temperature is not representable"); return MP_ERR_PHASE_OVERFLOW; }
+        t->opts.pressure = value;
+        t->ph.Tep = Tep;
+        t->ph.litho = 0;
+    } else if (model == MP_PRESSURE_LITHOSTATIC) {
+        const double top = t->range.gny > 0 ? t->mesh.y1 : t->mesh.y1;
+        if (value < top) { mp::set_error("surface_y must be at or above the mesh top"); return MP_ERR_ARG_OUTOFRANGE; }
+        // Tep(y) = TDe0 + rho g l0 (surface - y) / nu / dT (eutectic_rescaled.cpp:143-161).
+        const long double b = (long double)t->opts.material.rho * t->opts.material.g * t->der.l0 /
+                              t->opts.material.nu / t->der.dT;
+        t->ph.litho = 1;
+        t->ph.tep_a = t->der.TDe0;
+        t->ph.tep_b = (double)b;
+        t->ph.surface = value;
+    } else {
+        mp::set_error("unknown pressure model %d", model);
+        return MP_ERR_ARG_OUTOFRANGE;
+    }
+    t->have_L = false;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_transport_set_cell_velocity(mp_transport* t, const double* vs_y, const double* ud_y) {
+    if (!t || !vs_y || !ud_y) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    const size_t n = t->N * mp::kNQ * mp::kNQ;
+    cudaError_t e = cudaSuccess;
+    for (double** p : {&t->cvs_y, &t->cud_y})
+        if (!*p && e == cudaSuccess) e = cudaMalloc(p, n * sizeof(double));
+    for (double** p : {&t->srcH, &t->srcR, &t->srcS})
+        if (!*p && e == cudaSuccess) e = cudaMalloc(p, t->N * sizeof(double));
+    if (e != cudaSuccess) return mp::cuda_status(e, "mp_transport_set_cell_velocity");
+    MP_CUDA(cudaMemcpyAsync(t->cvs_y, vs_y, n * sizeof(double), cudaMemcpyDefault, t->stream));
+    MP_CUDA(cudaMemcpyAsync(t->cud_y, ud_y, n * sizeof(double), cudaMemcpyDefault, t->stream));
+    MP_CUDA(cudaMemsetAsync(t->srcH, 0, t->N * sizeof(double), t->stream));
+    MP_CUDA(cudaMemsetAsync(t->srcR, 0, t->N * sizeof(double), t->stream));
+    MP_CUDA(cudaMemsetAsync(t->srcS, 0, t->N * sizeof(double), t->stream));
+    MP_CUDA(cudaStreamSynchronize(t->stream));
     t->have_L = false;
     return MP_OK;
 }
@@ -786,6 +855,8 @@ mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double
     ph.theta = o.theta; ph.inflowH = o.inflow_H; ph.inflowC = o.inflow_C;
     ph.Hpol = o.H_policy; ph.Cpol = o.C_policy; ph.lf_global = o.lf_global; ph.lf_speed = o.lf_global_speed;
     ph.diffusion = 0; ph.kappa = 0.0;
+    ph.litho = 0; ph.tep_a = ph.tep_b = ph.surface = 0.0;
+    ph.source = 0; ph.cooling = 0.0;
     for (int w = 0; w < 4; ++w) { ph.wall_type[w] = 0; ph.wall_value[w] = 0.0; }
     const size_t N = (size_t)nx * ny;
     const size_t NE = (size_t)nx * (ny + 1) + (size_t)(nx + 1) * ny;

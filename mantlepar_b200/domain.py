@@ -37,7 +37,8 @@ from .transport import REPORT_FIELDS, TransportConfig, _host, _ptr
 NONE_KEY = (1 << 63) - 1          # "no failure" status key as int64
 MAX_FIELDS = (0, 1, 8, 9)         # maxRate, divergence, Cmax, nonfinite
 MIN_FIELDS = (6, 7)               # Hmin, Cmin
-SUM_FIELDS = (2, 3, 4, 5)         # boundaryH, boundaryC, H_integral, C_integral
+SUM_FIELDS = (2, 3, 4, 5, 10)     # boundaryH, boundaryC, H_integral, C_integral, sourceH
+NFIELDS = 11
 
 
 def partition(ny: int, parts: int) -> list[tuple[int, int]]:
@@ -137,6 +138,17 @@ class Slab:
         _capi.check(self._lib.mp_transport_get_state(self._h, _ptr(H), _ptr(Cc), _ptr(T), _ptr(phi)))
         return H, Cc, T, phi
 
+    def set_pressure_model(self, model: int, value: float):
+        _capi.check(self._lib.mp_transport_set_pressure_model(self._h, int(model), float(value)))
+
+    def set_cell_velocity(self, vs_y_global, ud_y_global):
+        """Cell-point vertical velocities of the global mesh, sliced to the local cells."""
+        nx, q = self.w.nx, 25
+        lo, hi = self.row0 * nx * q, (self.row0 + self.local_rows) * nx * q
+        a = np.ascontiguousarray(np.asarray(vs_y_global)[lo:hi])
+        b = np.ascontiguousarray(np.asarray(ud_y_global)[lo:hi])
+        _capi.check(self._lib.mp_transport_set_cell_velocity(self._h, _ptr(a), _ptr(b)))
+
     def set_thermal_bc(self, types=(0, 0, 0, 0), values=(0.0, 0.0, 0.0, 0.0)):
         """Thermal conditions per wall (bottom, top, left, right) of the GLOBAL mesh."""
         ti = (C.c_int * 4)(*[int(x) for x in types])
@@ -153,7 +165,7 @@ class Slab:
 
         def _combine(user, tot, status):
             try:
-                arr = np.ctypeslib.as_array(C.cast(tot, C.POINTER(C.c_double)), shape=(10,))
+                arr = np.ctypeslib.as_array(C.cast(tot, C.POINTER(C.c_double)), shape=(NFIELDS,))
                 st = [int(status[0])]
                 rc = int(combine(arr, st))
                 status[0] = st[0]
@@ -297,15 +309,15 @@ class DistExchange:
         each rank then combines them in slab order, as ThreadExchange does, so
         the sums are deterministic."""
         dist = self.dist
-        mine = np.empty(11, dtype=np.int64)
-        mine[:10] = np.asarray(tot, dtype=np.float64).view(np.int64)
-        mine[10] = _status_in(st[0])
+        mine = np.empty(NFIELDS + 1, dtype=np.int64)
+        mine[:NFIELDS] = np.asarray(tot, dtype=np.float64).view(np.int64)
+        mine[NFIELDS] = _status_in(st[0])
         t = torch.from_numpy(mine).to(self.device)
-        out = torch.empty(self.world * 11, dtype=torch.int64, device=self.device)
+        out = torch.empty(self.world * (NFIELDS + 1), dtype=torch.int64, device=self.device)
         dist.all_gather_into_tensor(out, t, group=self.group)
-        rows = out.cpu().numpy().reshape(self.world, 11)
-        parts = [r[:10].view(np.float64) for r in rows]
-        res, key = combine_totals(parts, [int(r[10]) for r in rows])
+        rows = out.cpu().numpy().reshape(self.world, NFIELDS + 1)
+        parts = [r[:NFIELDS].view(np.float64) for r in rows]
+        res, key = combine_totals(parts, [int(r[NFIELDS]) for r in rows])
         tot[:] = res
         st[0] = _status_out(key)
         return 0

@@ -78,6 +78,8 @@ mp_transport* create(const Configuration& c, const Mesh& m, bool continuing) {
         }
         st = mp_transport_set_thermal_bc(h, type, value);
     }
+    if (st == MP_OK && c.pressureModel == PressureModel::Lithostatic)
+        st = mp_transport_set_pressure_model(h, MP_PRESSURE_LITHOSTATIC, c.surfaceY);
     if (st != MP_OK) { mp_transport_destroy(h); throw_status(st); }
     return h;
 }
@@ -89,11 +91,20 @@ CoupledTransport::CoupledTransport(const Configuration& configuration, const Mes
 
 CoupledTransport::~CoupledTransport() { mp_transport_destroy(handle_); }
 
-int CoupledTransport::setVelocities(const EdgeVelocities& v) {
-    const size_t n = (size_t)EdgeCount(mesh_) * 5;
+namespace {
+mp_status set_velocities(mp_transport* h, const Mesh& m, const EdgeVelocities& v) {
+    const size_t n = (size_t)EdgeCount(m) * 5, nc = (size_t)m.nx * m.ny * 25;
     if (v.solid.size() != n || v.darcy.size() != n) return MP_ERR_ARG_SIZ;
-    return mp_transport_set_face_velocity(handle_, v.solid.data(), v.darcy.data());
+    mp_status st = mp_transport_set_face_velocity(h, v.solid.data(), v.darcy.data());
+    if (st == MP_OK && !v.cellSolidY.empty()) {
+        if (v.cellSolidY.size() != nc || v.cellDarcyY.size() != nc) return MP_ERR_ARG_SIZ;
+        st = mp_transport_set_cell_velocity(h, v.cellSolidY.data(), v.cellDarcyY.data());
+    }
+    return st;
 }
+}  // namespace
+
+int CoupledTransport::setVelocities(const EdgeVelocities& v) { return set_velocities(handle_, mesh_, v); }
 
 int CoupledTransport::setState(const InitialState& s) {
     const size_t n = (size_t)mesh_.nx * mesh_.ny;
@@ -233,9 +244,7 @@ int AdvancePhaseCoupled(const Configuration& c, InitialState& state, const FlowS
         if (st != MP_OK) return finish(st);
         const int fs = flow(cur, v);
         if (fs != 0) { state = cur; return finish(fs); }
-        const size_t ne = (size_t)EdgeCount(mesh) * 5;
-        if (v.solid.size() != ne || v.darcy.size() != ne) { state = cur; return finish(MP_ERR_ARG_SIZ); }
-        st = mp_transport_set_face_velocity(h, v.solid.data(), v.darcy.data());
+        st = set_velocities(h, mesh, v);
         if (st != MP_OK) { state = cur; return finish(st); }
         mp_step_report r{};
         st = mp_transport_step(h, 1, &r);

@@ -156,6 +156,23 @@ def face_velocity(w: Workload) -> tuple[np.ndarray, np.ndarray]:
     return np.ascontiguousarray(vs), np.ascontiguousarray(ud)
 
 
+def cell_velocity(w: Workload) -> tuple[np.ndarray, np.ndarray]:
+    """Vertical solid / Darcy velocity at the 5x5 Gauss points of every cell,
+    [cell*25 + b*5 + a] for the point (g_a, g_b), from the same streamfunction
+    (v_s,y = -dpsi/dx) and u_d = (0, darcy)."""
+    xs = vertex_coords(w.nx, w.x0, w.x1)
+    ys = vertex_coords(w.ny, w.y0, w.y1)
+    t = 0.5 * (1.0 + GAUSS5_POINTS)
+    xq = xs[:-1, None] + t[None, :] * (xs[1:] - xs[:-1])[:, None]          # (nx, 5)
+    yq = ys[:-1, None] + t[None, :] * (ys[1:] - ys[:-1])[:, None]          # (ny, 5)
+    two_pi = 2.0 * math.pi
+    A = w.psi_amplitude
+    # (j, i, b, a)
+    vy = -two_pi * A * np.cos(two_pi * xq)[None, :, None, :] * np.sin(math.pi * yq)[:, None, :, None]
+    vs_y = np.ascontiguousarray(vy.reshape(-1))
+    return vs_y, np.full_like(vs_y, w.darcy)
+
+
 # The BASELINE workloads, named by what they are.
 def plain_small() -> Workload:
     """20x20 plain FP64 instance, 200 steps (the run.sh --grid 20 size)."""

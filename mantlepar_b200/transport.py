@@ -121,6 +121,17 @@ class Transport:
     CFL, FIXED = 0, 1
     ZERO_FLUX, TEMPERATURE, FLUX = 0, 1, 2
 
+    CONSTANT, LITHOSTATIC = 0, 1
+
+    def set_pressure_model(self, model: int, value: float):
+        """CONSTANT (value: pressure in Pa) or LITHOSTATIC (value: surface_y)."""
+        _capi.check(self._lib.mp_transport_set_pressure_model(self._h, int(model), float(value)))
+
+    def set_cell_velocity(self, vs_y, ud_y):
+        """Vertical solid / Darcy velocity at the cell quadrature points [cell*25 + b*5 + a]."""
+        a, b = _host(vs_y), _host(ud_y)
+        _capi.check(self._lib.mp_transport_set_cell_velocity(self._h, _ptr(a), _ptr(b)))
+
     def set_thermal_bc(self, types=(0, 0, 0, 0), values=(0.0, 0.0, 0.0, 0.0)):
         """Thermal conditions per wall (bottom, top, left, right): ZERO_FLUX,
         TEMPERATURE (dimensionless T) or FLUX (outward diffusive flux per length)."""

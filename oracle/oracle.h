@@ -113,6 +113,12 @@ int orc_transport_set_time_control(orc_transport* t, int control, double t_end);
  * (0 bottom y0, 1 top y1, 2 left x0, 3 right x1), type 0 zero flux, 1
  * prescribed temperature, 2 prescribed outward flux, with its value. */
 int orc_transport_set_diffusion(orc_transport* t, double kappa, const int* types, const double* values);
+/* Phase-law pressure (initialization.cpp:148-163): model 0 constant (value in
+ * Pa), 1 lithostatic with the surface at y = value. */
+int orc_transport_set_pressure_model(orc_transport* t, int model, double value);
+/* Vertical flow velocities (solid, Darcy) at the cell quadrature points
+ * [cell*25 + b*5 + a], for the adiabatic source (evolve.cpp:359-369). */
+int orc_transport_set_cell_velocity(orc_transport* t, const double* vs_y, const double* ud_y);
 int orc_transport_limiter(orc_transport* t, double* thetaH, double* thetaC);
 
 /* Synthetic input builders shared by tests and bench (SplitMix64 noise as in

@@ -85,8 +85,10 @@ class _Lib:
         t("create").argtypes = [C.POINTER(Material), C.POINTER(TransportOpts)]
         t("destroy").argtypes = [C.c_void_p]
         for n in ["set_face_velocity", "set_state", "get_state", "rhs", "limiter", "step", "set_time_control",
-                  "set_diffusion"]:
+                  "set_diffusion", "set_pressure_model", "set_cell_velocity"]:
             t(n).restype = C.c_int
+        t("set_pressure_model").argtypes = [C.c_void_p, C.c_int, C.c_double]
+        t("set_cell_velocity").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         t("set_diffusion").argtypes = [C.c_void_p, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         t("set_time_control").argtypes = [C.c_void_p, C.c_int, C.c_double]
         t("set_face_velocity").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -237,6 +239,16 @@ class TransportOracle:
         ti = (C.c_int * 4)(*[int(x) for x in types])
         tv = (C.c_double * 4)(*[float(x) for x in values])
         return self.lib.f("transport_set_diffusion")(self.h, float(kappa), ti, tv)
+
+    def set_pressure_model(self, model: int, value: float):
+        """0: constant pressure `value` Pa; 1: lithostatic with the surface at y = value."""
+        return self.lib.f("transport_set_pressure_model")(self.h, int(model), float(value))
+
+    def set_cell_velocity(self, vs_y, ud_y):
+        a = np.ascontiguousarray(vs_y, dtype=np.float64)
+        b = np.ascontiguousarray(ud_y, dtype=np.float64)
+        self._cellv = (a, b)
+        return self.lib.f("transport_set_cell_velocity")(self.h, _dptr(a), _dptr(b))
 
     def set_time_control(self, control: int, t_end: float = float("inf")):
         return self.lib.f("transport_set_time_control")(self.h, int(control), float(t_end))

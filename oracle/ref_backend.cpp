@@ -132,6 +132,12 @@ struct RefBackend {
         s.coefficients = ds.Coefficients();
         s.native = std::make_shared<DiffusiveSampling>(ds);
     }
+    static double static_pressure(const orc_material&, const orc_derived&, double zD) {
+        double v = 0;
+        const int code = classify_exceptions([&] { v = shared_model()->staticPressure(zD); });
+        if (code != ORC_OK) throw orc::Error{orc::E_PHASE + code, "staticPressure failed"};
+        return v;
+    }
     // The reference's own IntegrateDiffusive(Boundary)FluxWithDerivatives
     // (diffusiveflux.h:150-193) on its own sampling object.
     static void diffuse(const orc::Sampling& s, const std::vector<double>& samples, double kappa,
@@ -230,6 +236,8 @@ int ref_transport_rhs(void* t, double* a, double* b, double* T, double* phi, dou
 int ref_transport_limiter(void* t, double* a, double* b) { return RefApi::limiter(t, a, b); }
 int ref_transport_step(void* t, int n, orc_step_report* r) { return RefApi::step(t, n, r); }
 int ref_transport_set_time_control(void* t, int control, double t_end) { return RefApi::set_time_control(t, control, t_end); }
+int ref_transport_set_pressure_model(void* t, int model, double value) { return RefApi::set_pressure_model(t, model, value); }
+int ref_transport_set_cell_velocity(void* t, const double* a, const double* b) { return RefApi::set_cell_velocity(t, a, b); }
 int ref_transport_set_diffusion(void* t, double kappa, const int* types, const double* values) {
     return RefApi::set_diffusion(t, kappa, types, values);
 }

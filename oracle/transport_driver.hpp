@@ -97,6 +97,14 @@ struct Driver {
     // thermal condition per wall (0 bottom y0, 1 top y1, 2 left x0, 3 right x1).
     double kappa = 0;
     ThermalBC wall_bc[4];
+    // Phase-law pressure (initialization.cpp:148-163): constant o.pressure, or
+    // lithostatic rho*g*l0*(surface_y - y).
+    bool lithostatic = false;
+    double surface_y = 0;
+    double pressure_at(Pt p) const { return lithostatic ? B::static_pressure(mat, der, surface_y - p.y) : o.pressure; }
+    // Flow velocities at the cell quadrature points, vertical components
+    // [cell*nq*nq + b*nq + a], for the adiabatic source (evolve.cpp:359-369).
+    std::vector<double> cell_vs_y, cell_ud_y;
     bool diffusion_active() const {
         if (kappa > 0) return true;
         for (const auto& b : wall_bc) if (b.type == 2) return true;
@@ -188,7 +196,6 @@ struct Driver {
     void init(const orc_material& m, const orc_transport_opts& opts) {
         mat = m; o = opts;
         require(B::derive(mat, der), E_OUTOFRANGE, "Invalid material parameters");
-        require(mat.alpha0 == 0.0, E_WRONG, "Adiabatic source needs cell-point velocities");
         nx = o.nx; ny = o.ny;
         require(nx >= 2 && ny >= 2, E_SIZ, "Transport requires at least 2x2 cells");
         ncell = nx * ny;
@@ -226,7 +233,7 @@ struct Driver {
     void phase_at(int cell, Pt p, orc_phase& s, double& h, double& c) const {
         evaluate(cell, p, h, c);
         int code = 0;
-        if (!B::phase(mat, der, h, c, o.pressure, s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
+        if (!B::phase(mat, der, h, c, pressure_at(p), s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
         require(s.TDp >= 0 && s.phil < 1, E_OUTOFRANGE, "Coupled Darcy-Stokes requires nonnegative temperature and porosity < 1");
     }
 
@@ -301,7 +308,7 @@ struct Driver {
                     const Pt p = B::map_cell(Pt{x, y}, q);
                     double h, c; evaluate(k, p, h, c);
                     orc_phase s; int code = 0;
-                    if (!B::phase(mat, der, h, c, o.pressure, s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
+                    if (!B::phase(mat, der, h, c, pressure_at(p), s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
                     w = w || s.phil > 0;
                 }
                 wet[k] = w;
@@ -320,13 +327,13 @@ struct Driver {
                         const Pt p = B::map_edge(gp[t], q[e], q[(e + 1) % 4]);
                         double h, c; evaluate(k, p, h, c);
                         orc_phase s; int code = 0;
-                        if (!B::phase(mat, der, h, c, o.pressure, s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
+                        if (!B::phase(mat, der, h, c, pressure_at(p), s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
                         const double a = s.phil;
                         double b = a;
                         if (!bnd) {
                             const int nk = cell_id(ni, nj);
                             evaluate(nk, p, h, c);
-                            if (!B::phase(mat, der, h, c, o.pressure, s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
+                            if (!B::phase(mat, der, h, c, pressure_at(p), s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
                             b = s.phil;
                         }
                         double v = (a + b) > 0 ? 2 * a * b / (a + b) : 0;
@@ -403,7 +410,7 @@ struct Driver {
                         double Tb = a.TDp;
                         if (kh == 0) {
                             orc_phase s; int code = 0;
-                            if (!B::phase(mat, der, o.inflow_H, inflowC, o.pressure, s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
+                            if (!B::phase(mat, der, o.inflow_H, inflowC, pressure_at(p), s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
                             Tb = s.TDp;
                         }
                         fh = kh == 2 ? 0 : vn * Tb - LD * (1 - ephi) * vs;
@@ -451,7 +458,16 @@ struct Driver {
                 out.boundaryH += fluxH; out.boundaryC += fluxC;
             }
         }
-        // evolve.cpp:359-376: cell quadrature of T and phi (zero adiabatic source).
+        // evolve.cpp:359-376: cell quadrature of T and phi, and the adiabatic
+        // source -cooling*T*v_mix,y with v_mix from PhaseTransportVelocities
+        // (evolve.cpp:36-52) at the point's porosity; each point's heat and rate
+        // are added after the face terms, and sourceH sums w*source in the
+        // reference's cell and point order.
+        const double cooling = mat.alpha0 * der.l0 * mat.g / mat.cp;
+        const bool source = mat.alpha0 != 0;
+        require(!source || cell_vs_y.size() == (size_t)ncell * nq * nq, E_WRONGSTATE,
+                "The adiabatic source needs the flow velocities at the cell quadrature points");
+        std::vector<double> wsrc(source ? (size_t)ncell * nq * nq : 0);
         parallel_for(ncell, [&](int k) {
                 const int i = k % nx, j = k / nx;
                 const Quad q = corners(i, j);
@@ -465,9 +481,19 @@ struct Driver {
                         phase_at(k, p, s, h, c);
                         t += w / area[k] * s.TDp;
                         ph += w / area[k] * s.phil;
+                        if (source) {
+                            const size_t at = ((size_t)k * nq + b) * nq + a;
+                            const double factor = s.phil == 0 ? 0 : std::pow(s.phil, 1 + theta);
+                            const double vy = cell_vs_y[at] + factor * cell_ud_y[at];
+                            const double src = -cooling * s.TDp * vy;
+                            rhsH[k] += w / area[k] * src;
+                            rate[k] += w / area[k] * cooling * std::fabs(vy);
+                            wsrc[at] = w * src;
+                        }
                     }
                 T[k] = t; phi[k] = ph;
         });
+        for (double v : wsrc) out.sourceH += v;
         double mx = -std::numeric_limits<double>::infinity(), dv = 0;
         for (int k = 0; k < ncell; ++k) { mx = std::max(mx, rate[k]); dv = std::max(dv, std::fabs(divg[k])); }
         out.maximumRate = mx;
@@ -556,7 +582,8 @@ struct Driver {
         const double HI = integral(H), CI = integral(C);
         double bH, bC;
         if (o.integrator == 3) {
-            bH = HI - oldHI + dt * ((first.boundaryH + second.boundaryH) / 6 + third.boundaryH * (2.0 / 3.0));
+            bH = HI - oldHI + dt * ((first.boundaryH + second.boundaryH) / 6 + third.boundaryH * (2.0 / 3.0) -
+                                    ((first.sourceH + second.sourceH) / 6 + third.sourceH * (2.0 / 3.0)));
             bC = CI - oldCI + dt * ((first.boundaryC + second.boundaryC) / 6 + third.boundaryC * (2.0 / 3.0));
         } else {
             bH = HI - oldHI + .5 * dt * (first.boundaryH + second.boundaryH - first.sourceH - second.sourceH);
@@ -570,7 +597,9 @@ struct Driver {
         rep.status = 0; rep.retries = retries; rep.dt = dt; rep.time = time; rep.courant = courant;
         rep.boundaryH = o.integrator == 3 ? (first.boundaryH + second.boundaryH) / 6 + third.boundaryH * (2.0 / 3.0) : .5 * (first.boundaryH + second.boundaryH);
         rep.boundaryC = o.integrator == 3 ? (first.boundaryC + second.boundaryC) / 6 + third.boundaryC * (2.0 / 3.0) : .5 * (first.boundaryC + second.boundaryC);
-        rep.sourceH = 0; rep.maxRate = current.maximumRate; rep.divergence = current.divergence;
+        rep.sourceH = o.integrator == 3 ? (first.sourceH + second.sourceH) / 6 + third.sourceH * (2.0 / 3.0)
+                                        : .5 * (first.sourceH + second.sourceH);
+        rep.maxRate = current.maximumRate; rep.divergence = current.divergence;
         rep.balanceH = bH; rep.balanceC = bC; rep.H_integral = HI; rep.C_integral = CI;
     }
 };
@@ -649,6 +678,24 @@ struct Api {
             d.wall_bc[w] = ThermalBC{types[w], values[w]};
         }
         d.kappa = kappa;
+        d.have_current = false;
+        return 0;
+    }
+
+    static int set_pressure_model(void* h, int model, double value) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        if ((model != 0 && model != 1) || !std::isfinite(value)) return E_OUTOFRANGE;
+        d.lithostatic = model == 1;
+        if (model == 1) d.surface_y = value; else d.o.pressure = value;
+        d.have_current = false;
+        return 0;
+    }
+
+    static int set_cell_velocity(void* h, const double* vs_y, const double* ud_y) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        const size_t n = (size_t)d.ncell * d.nq * d.nq;
+        d.cell_vs_y.assign(vs_y, vs_y + n);
+        d.cell_ud_y.assign(ud_y, ud_y + n);
         d.have_current = false;
         return 0;
     }

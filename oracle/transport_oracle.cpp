@@ -7,6 +7,8 @@
 // first cell of each boundary class are shared by all cells of that class
 // (exact only up to the rounding of the per-cell vertex coordinates).
 #include "oracle.h"
+
+#include <limits>
 #include "transport_driver.hpp"
 
 #include <map>
@@ -95,6 +97,14 @@ struct Restated {
     static bool phase(const orc_material& m, const orc_derived& d, double H, double C, double P, orc_phase& s, int& code) {
         return orc_internal::phase_eval(m, d, H, C, P, s, code);
     }
+    // EutecticModel::staticPressure(zD) (eutectic_rescaled.cpp:151-161).
+    static double static_pressure(const orc_material& m, const orc_derived& d, double zD) {
+        require(std::isfinite(zD), E_PHASE + 1, "zD must be finite");
+        const long double v = (long double)m.rho * m.g * zD * d.l0;
+        require(std::isfinite(v) && std::fabs(v) <= (long double)std::numeric_limits<double>::max(), E_PHASE + 2,
+                "static pressure is not representable");
+        return (double)v;
+    }
     static void diffuse(const Sampling& s, const std::vector<double>& samples, double kappa, const ThermalBC* bc,
                         double& flux, std::vector<double>& deriv) {
         integrate_diffusion(s, samples, kappa, bc, flux, deriv);
@@ -128,6 +138,12 @@ extern "C" int orc_transport_limiter(orc_transport* t, double* thetaH, double* t
 }
 extern "C" int orc_transport_step(orc_transport* t, int nsteps, orc_step_report* report) {
     return RestatedApi::step(t, nsteps, report);
+}
+extern "C" int orc_transport_set_pressure_model(orc_transport* t, int model, double value) {
+    return RestatedApi::set_pressure_model(t, model, value);
+}
+extern "C" int orc_transport_set_cell_velocity(orc_transport* t, const double* vs_y, const double* ud_y) {
+    return RestatedApi::set_cell_velocity(t, vs_y, ud_y);
 }
 extern "C" int orc_transport_set_diffusion(orc_transport* t, double kappa, const int* types, const double* values) {
     return RestatedApi::set_diffusion(t, kappa, types, values);

@@ -43,7 +43,7 @@ def _worker(rank, world, port, q):
         okH = np.array_equal(H.numpy().reshape(lr, NX), g[row0:row0 + lr])
         okC = np.array_equal(C.numpy().reshape(lr, NX), -g[row0:row0 + lr])
         # totals: maxRate, divergence, bH, bC, HI, CI, Hmin, Cmin, Cmax, nonfinite
-        tot = np.array([rank + 1.0, 0.5 * rank, 1.0, 2.0, 10.0 * (rank + 1), 3.0, -rank, 5.0 - rank, rank, 0.0])
+        tot = np.array([rank + 1.0, 0.5 * rank, 1.0, 2.0, 10.0 * (rank + 1), 3.0, -rank, 5.0 - rank, rank, 0.0, 0.25 * rank])
         st = [(rank << 8) | 63 if rank == world - 1 else (1 << 64) - 1]
         ex.combine(tot, st)
         q.put((rank, okH, okC, tot.tolist(), st[0]))
@@ -63,7 +63,7 @@ def test_dist_exchange_gloo(world):
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    parts = [np.array([r + 1.0, 0.5 * r, 1.0, 2.0, 10.0 * (r + 1), 3.0, -r, 5.0 - r, r, 0.0]) for r in range(world)]
+    parts = [np.array([r + 1.0, 0.5 * r, 1.0, 2.0, 10.0 * (r + 1), 3.0, -r, 5.0 - r, r, 0.0, 0.25 * r]) for r in range(world)]
     want, _ = combine_totals(parts, [0] * world)
     for rank, okH, okC, tot, st in res:
         assert okH and okC, rank
@@ -76,7 +76,7 @@ def test_partition_and_combine():
     assert all(e - b >= 2 for b, e in partition(2560, 8))
     with pytest.raises(ValueError):
         partition(5, 3)
-    a = np.array([1.0, 2, 3, 4, 5, 6, 7, 8, 9, 0])
-    b = np.array([2.0, 1, 3, 4, 5, 6, 6, 9, 8, 1])
+    a = np.array([1.0, 2, 3, 4, 5, 6, 7, 8, 9, 0, 0.5])
+    b = np.array([2.0, 1, 3, 4, 5, 6, 6, 9, 8, 1, 0.25])
     tot, st = combine_totals([a, b], [5, 3])
-    assert tot.tolist() == [2, 2, 6, 8, 10, 12, 6, 8, 9, 1] and st == 3
+    assert tot.tolist() == [2, 2, 6, 8, 10, 12, 6, 8, 9, 1, 0.75] and st == 3

@@ -270,3 +270,71 @@ def test_diffusion_batched_and_slabs_equal_single(cuda_lib):
         assert code == 0 and [x["dt"] for x in r] == [x["dt"] for x in reps]
     got = np.concatenate([np.stack(s.get_state()) for s in slabs], axis=1)
     assert np.array_equal(got, ref)
+
+
+def _product_like_gpu(w, mat):
+    from mantlepar_b200.transport import Transport, TransportConfig
+    t = Transport(w, TransportConfig(material=mat, cfl=w.cfl, integrator=3, diffusivity=0.01))
+    t.set_thermal_bc((1, 1, 0, 0), (0.9, 0.2, 0.0, 0.0))
+    t.set_pressure_model(t.LITHOSTATIC, 1.1)
+    t.set_cell_velocity(*sy.cell_velocity(w))
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    t.set_face_velocity(vs, ud)
+    t.set_state(H, C)
+    return t
+
+
+def test_product_features_match_oracle(cuda_lib):
+    """Diffusion, lithostatic pressure and the adiabatic source together (the
+    reference's product-input features; the oracle equals the reference build
+    bit for bit): stage to 1e-12, 8 steps to 1e-12 with the same retries."""
+    from test_oracle_transport import product_like
+    w = sy.Workload(nx=10, ny=12, seed=3)
+    o, mat = product_like(w)
+    t = _product_like_gpu(w, mat)
+    r = t.rhs()
+    code, ref = o.rhs()
+    assert code == 0
+    for k in ["T", "phi", "rate"]:
+        assert rel(r[k], ref[k]) <= RTOL_STAGE, k
+    for k in ["rhsH", "rhsC"]:
+        assert rel_inf(r[k], ref[k]) <= RTOL_STAGE, k
+    assert abs(r["sourceH"] - ref["sourceH"]) <= 1e-12 * abs(ref["sourceH"])
+    _, got = t.step(8)
+    code, want = o.step(8)
+    assert code == 0
+    assert [x["retries"] for x in got] == [x["retries"] for x in want]
+    for g, x in zip(got, want):
+        assert abs(g["sourceH"] - x["sourceH"]) <= 1e-12 * max(1e-30, abs(x["sourceH"]))
+    a, b = np.stack(t.get_state()), np.stack(o.get_state())
+    for k in range(4):
+        assert rel(a[k], b[k]) <= RTOL_RUN10, k
+
+
+def test_product_features_on_slabs_equal_single(cuda_lib):
+    import dataclasses
+    import torch
+    from mantlepar_b200.domain import Slab, ThreadExchange, partition
+    from mantlepar_b200.transport import TransportConfig
+    w = sy.Workload(nx=12, ny=16, seed=4)
+    mat = dataclasses.replace(sy.material_s(), rho=100.0, alpha0=3e-5)
+    t = _product_like_gpu(w, mat)
+    _, reps = t.step(5)
+    ref = np.stack(t.get_state())
+    cfg = TransportConfig(material=mat, cfl=w.cfl, integrator=3, diffusivity=0.01)
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    cv = sy.cell_velocity(w)
+    slabs = [Slab(w, r, cfg, stream=torch.cuda.Stream()) for r in partition(w.ny, 3)]
+    for s in slabs:
+        s.set_thermal_bc((1, 1, 0, 0), (0.9, 0.2, 0.0, 0.0))
+        s.set_pressure_model(1, 1.1)
+        s.set_cell_velocity(*cv)
+        s.set_face_velocity(vs, ud)
+        s.set_state(H, C)
+    outs = ThreadExchange(slabs).step(5)
+    for code, r in outs:
+        assert code == 0 and [x["dt"] for x in r] == [x["dt"] for x in reps]
+    got = np.concatenate([np.stack(s.get_state()) for s in slabs], axis=1)
+    assert np.array_equal(got, ref)

@@ -168,3 +168,53 @@ def test_diffusion_changes_the_solution_as_expected():
     assert abs(r1["boundaryH"] - r0["boundaryH"]) < 1e-15              # insulated: no extra boundary flux
     assert r2["boundaryH"] < r1["boundaryH"]                           # hot top wall: heat flows in
     assert r1["maxRate"] > r0["maxRate"]                               # diffusion enters the CFL rate
+
+
+def product_like(w, lib=None):
+    """Thermal diffusion, lithostatic pressure and the adiabatic source together
+    (the features of the reference's product input), on material S with a
+    lighter density so the eutectic temperature varies mildly with depth."""
+    import dataclasses
+    mat = dataclasses.replace(sy.material_s(), rho=100.0, alpha0=3e-5)
+    t = po.TransportOracle(mat, w, lib=lib, integrator=3)
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    t.set_face_velocity(vs, ud)
+    t.set_state(H, C)
+    assert t.set_diffusion(0.01, (1, 1, 0, 0), (0.9, 0.2, 0.0, 0.0)) == 0
+    assert t.set_pressure_model(1, 1.1) == 0
+    assert t.set_cell_velocity(*sy.cell_velocity(w)) == 0
+    return t, mat
+
+
+@pytest.mark.skipif(not po.reference_available(), reason="reference-backed oracle not built")
+def test_product_features_restatement_equals_reference_bitwise():
+    w = sy.Workload(nx=10, ny=12, seed=3)
+    out = []
+    for lib in (po.restated(), po.reference()):
+        t, _ = product_like(w, lib)
+        code, r = t.rhs()
+        assert code == 0
+        code, reps = t.step(8)
+        assert code == 0
+        out.append((r, t.get_state(), reps))
+    (ra, sa, pa), (rb, sb, pb) = out
+    for k in ["rhsH", "rhsC", "T", "phi", "rate"]:
+        assert np.array_equal(bits(ra[k]), bits(rb[k])), k
+    assert ra["sourceH"] == rb["sourceH"] and ra["sourceH"] != 0.0
+    for x, y in zip(sa, sb):
+        assert np.array_equal(bits(x), bits(y))
+    assert [r["dt"] for r in pa] == [r["dt"] for r in pb]
+    assert all(abs(r["balanceH"]) < 1e-12 for r in pa)
+
+
+def test_source_requires_cell_velocities():
+    import dataclasses
+    w = sy.Workload(nx=6, ny=6)
+    t = po.TransportOracle(dataclasses.replace(sy.material_s(), alpha0=3e-5), w, integrator=3)
+    vs, ud = sy.face_velocity(w)
+    H, C = sy.initial_state(w)
+    t.set_face_velocity(vs, ud)
+    t.set_state(H, C)
+    code, _ = t.rhs()
+    assert code == 73
