@@ -269,6 +269,27 @@ def run_forms(args, stream):
                        "instances": len(ws), "cells": cells, "steps": args.form_steps,
                        "autotuned_tile": list(tile), "all_instances_healthy": ok}
         b.close()
+    # Product-input features on the plain workload: thermal diffusion, a
+    # lithostatic pressure and the adiabatic source (FP64).
+    import dataclasses
+    wp = sy.Workload(**WORKLOAD)
+    mat = dataclasses.replace(sy.material_s(), rho=100.0, alpha0=3e-5)
+    tp = Transport(wp, TransportConfig(material=mat, cfl=wp.cfl, integrator=3, diffusivity=1e-4),
+                   stream=stream.cuda_stream)
+    tp.set_thermal_bc((1, 1, 0, 0), (0.9, 0.2, 0.0, 0.0))
+    tp.set_pressure_model(tp.LITHOSTATIC, 1.1)
+    tp.set_cell_velocity(*sy.cell_velocity(wp))
+    vs_p, ud_p = sy.face_velocity(wp)
+    H_p, C_p = sy.initial_state(wp)
+    tp.set_face_velocity(vs_p, ud_p)
+    tp.set_state(H_p, C_p)
+    tp.step(1)
+    ms, (_, reps) = timed_steps(tp, args.form_steps, stream)
+    forms["product_features_1280x2560"] = {
+        "value": wp.cells * args.form_steps / (ms * 1e-3), "unit": "cell-updates/s", "steps": args.form_steps,
+        "features": "kappa=1e-4 with wall temperatures, lithostatic pressure, adiabatic source (alpha0=3e-5)",
+        "retries": sum(r["retries"] for r in reps)}
+    tp.close()
     # Served: a seeded Poisson stream (200 req/s) of uneven solves, mixed
     # precision, submitted in real time; memory admission against a 64 GiB budget.
     if args.serve_requests > 0:

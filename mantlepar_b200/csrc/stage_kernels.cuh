@@ -342,7 +342,9 @@ __device__ __forceinline__ void load_rec(const double* rec, size_t N, long long 
 
 // Cell quadrature of T and phi (evolve.cpp:359-376) and the wet flag of the
 // porosity sampling (initial_flow.cpp:56-67) on the same 5x5 points.
-template <class R>
+// kExt: the lithostatic pressure and the adiabatic source are compiled in
+// (a launch picks the variant; the default path carries none of their code).
+template <class R, bool kExt = false>
 __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const Physics& ph, long long cell) {
     const long long N = (long long)a.nx * a.ny;
     if (cell >= N) return;
@@ -359,7 +361,7 @@ __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const 
         const double y = t.gy[b];
         q2_row(DH, y, h0, h1, h2);
         q2_row(DC, y, c0, c1, c2);
-        const double tep = ph.litho ? tep_at(ph, height(t, gjc, y)) : ph.Tep;
+        const double tep = (kExt && ph.litho) ? tep_at(ph, height(t, gjc, y)) : ph.Tep;
 #pragma unroll
         for (int q = 0; q < kNQ; ++q) {
             const double x = t.gx[q];
@@ -373,7 +375,7 @@ __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const 
             Tsum += w * pl.T;
             Psum += w * pl.phil;
             wet = wet || pl.phil > 0.0;
-            if (ph.source) {
+            if (kExt && ph.source) {
                 // evolve.cpp:359-369 with PhaseTransportVelocities at this point's porosity.
                 const long long at = cell * (kNQ * kNQ) + b * kNQ + q;
                 const double factor = pl.phil == 0.0 ? 0.0 : (ph.theta == 0.0 ? pl.phil : pow(pl.phil, 1.0 + ph.theta));
@@ -403,7 +405,7 @@ __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const 
                 const double s_ = row ? t.gx[q] : t.gy[q];
                 const double h = mH + quad(h0, h1, h2, s_);
                 const double c = mC + quad(c0, c1, c2, s_);
-                const double tep = ph.litho ? tep_at(ph, height(t, j, row ? lc : t.gy[q])) : ph.Tep;
+                const double tep = (kExt && ph.litho) ? tep_at(ph, height(t, j, row ? lc : t.gy[q])) : ph.Tep;
                 PhaseLean pl;
                 const int s = phase_stage_lean(ph.sk, h, c, tep, pl);
                 if (s) { st_face = st_face ? st_face : s; continue; }
@@ -418,7 +420,7 @@ __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const 
     a.flags[cell] = (unsigned char)((fl & FLAG_CHECK) | (wet ? FLAG_WET : 0));
     a.T[cell] = Tsum;
     a.phi[cell] = Psum;
-    if (ph.source) { a.srcH[cell] = Ssum; a.srcR[cell] = Rsum; a.srcS[cell] = Wsum; }
+    if (kExt && ph.source) { a.srcH[cell] = Ssum; a.srcR[cell] = Rsum; a.srcS[cell] = Wsum; }
 }
 
 // ---------------------------------------------------------------- face kernel
@@ -465,7 +467,8 @@ __device__ __forceinline__ int side_phase(const Physics& ph, const SideLine& s, 
     return st;
 }
 
-template <class R>
+// kExt: the lithostatic pressure is compiled in.
+template <class R, bool kExt = false>
 __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& ph, long long e) {
     const int nx = a.nx, ny = a.ny;
     const long long nI = (long long)nx * (ny + 1);
@@ -521,7 +524,7 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
         double hL, cL, hR, cR;
         PhaseLean A, B;
         // Height of this Gauss point: the edge row for horizontal edges.
-        const double tep = !ph.litho ? ph.Tep
+        const double tep = !(kExt && ph.litho) ? ph.Tep
                          : tep_at(ph, horizontal ? t.y0 + (a.gj0 + erow) * t.dy : height(t, a.gj0 + erow, at));
         int s = side_phase(ph, sl, at, tep, hL, cL, A);
         if (boundary) { B = A; hR = hL; cR = cL; }
@@ -773,6 +776,8 @@ __device__ void block_reduce_write(Partial v, Partial* out) {
 
 // Per-cell accumulation + RK combination; folds the cell's contribution to
 // the stage reductions into v.
+// kSrc: the adiabatic source terms are added.
+template <bool kSrc = false>
 __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partial& v) {
     const int nx = a.nx, ny = a.ny;
     const long long nI = (long long)nx * (ny + 1);
@@ -801,7 +806,7 @@ __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partia
     }
     rH *= invA; rC *= invA; rr *= invA; dv *= invA;
     double sH = 0.0;
-    if (a.srcH) {
+    if (kSrc) {
         // The source terms follow the face terms, as the reference adds them.
         rH += __ldg(a.srcH + cell); rr += __ldg(a.srcR + cell); sH = __ldg(a.srcS + cell);
     }
@@ -834,13 +839,14 @@ __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partia
 
 // The kSumPer cells of this thread in the sum block starting at first.
 // `first` counts from the start of the accumulated range [cbeg, cend).
+template <bool kSrc = false>
 __device__ __forceinline__ Partial sum_cells(const SumArgs& a, long long first) {
     const long long end = a.cend >= 0 ? a.cend : (long long)a.nx * a.ny;
     Partial v = partial_identity();
 #pragma unroll
     for (int k = 0; k < kSumPer; ++k) {
         const long long c = a.cbeg + first + k * kRedBlock + threadIdx.x;
-        if (c < end) sum_cell(a, (unsigned)c, v);
+        if (c < end) sum_cell<kSrc>(a, (unsigned)c, v);
     }
     return v;
 }

@@ -64,24 +64,30 @@ __global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph, 
     const int j = jlo + (int)(blockIdx.y * blockDim.y + threadIdx.y);
     if (j < jhi) recon_cell(b, ph, blockIdx.x * blockDim.x + threadIdx.x, j);
 }
-template <class R>
+template <class R, bool kExt>
 __global__ void __launch_bounds__(128, 8) cellphase_kernel(CellPhaseArgs<R> a, Physics ph,
                                                         const __grid_constant__ ParamTables p, long long c0, long long c1) {
     CellPhaseArgs<R> b = a;
     b.tab = param_tab<R>(p);
     const long long cell = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell < c1) cellphase_cell(b, ph, cell);
+    if (cell < c1) cellphase_cell<R, kExt>(b, ph, cell);
 }
 // Edges [h0, h0 + nh) (horizontal) then [v0, v0 + nv) (vertical): every edge
 // of the mesh, or of a slab's owned cells.
-template <class R>
+// kRange: the edges of a slab's owned rows (two ranges); otherwise every
+// edge of the mesh with the plain linear mapping (measurably faster).
+template <class R, bool kExt, bool kRange>
 __global__ void __launch_bounds__(128, 5) face_kernel(FaceArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
                                                       long long h0, long long nh, long long v0, long long nv) {
     FaceArgs<R> b = a;
     b.tab = param_tab<R>(p);
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < nh) face_edge(b, ph, h0 + k);
-    else if (k < nh + nv) face_edge(b, ph, v0 + (k - nh));
+    if constexpr (kRange) {
+        // One call site: the edge body is inlined once.
+        if (k < nh + nv) face_edge<R, kExt>(b, ph, k < nh ? h0 + k : v0 + (k - nh));
+    } else {
+        face_edge<R, kExt>(b, ph, k);
+    }
 }
 // The diffusive part of the same edges (only launched when diffusion is on).
 template <class R>
@@ -90,12 +96,12 @@ __global__ void __launch_bounds__(128) diffusion_kernel(FaceArgs<R> a, Physics p
     FaceArgs<R> b = a;
     b.tab = param_tab<R>(p);
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < nh) diffusion_edge(b, ph, h0 + k);
-    else if (k < nh + nv) diffusion_edge(b, ph, v0 + (k - nh));
+    if (k < nh + nv) diffusion_edge(b, ph, k < nh ? h0 + k : v0 + (k - nh));
 }
 
+template <bool kSrc>
 __global__ void __launch_bounds__(kRedBlock) sum_kernel(SumArgs a) {
-    const Partial v = sum_cells(a, (long long)blockIdx.x * kSumCells);
+    const Partial v = sum_cells<kSrc>(a, (long long)blockIdx.x * kSumCells);
     block_reduce_write(v, a.partial + blockIdx.x);
 }
 
@@ -257,7 +263,9 @@ void launch_stage_kernels(int nx, int ny, const StageRange& rg, const ParamTable
         CellPhaseArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, T, phi, status, rg.gj0, rg.gny,
                            src.cvs_y, src.cud_y, src.srcH, src.srcR, src.srcS};
         const long long c0 = (long long)rg.rec0 * nx, c1 = (long long)rg.rec1 * nx;
-        run(1, [&] { cellphase_kernel<R><<<(unsigned)((c1 - c0 + 127) / 128), 128, 0, s>>>(a, ph, pt, c0, c1); });
+        const unsigned g = (unsigned)((c1 - c0 + 127) / 128);
+        if (ph.litho || ph.source) run(1, [&] { cellphase_kernel<R, true><<<g, 128, 0, s>>>(a, ph, pt, c0, c1); });
+        else run(1, [&] { cellphase_kernel<R, false><<<g, 128, 0, s>>>(a, ph, pt, c0, c1); });
     }
     {
         FaceArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, vsn, udn, face, status, rg.gj0, rg.gny};
@@ -265,7 +273,15 @@ void launch_stage_kernels(int nx, int ny, const StageRange& rg, const ParamTable
         const long long h0 = (long long)rg.own0 * nx, nh = (long long)(rg.own1 - rg.own0 + 1) * nx;
         const long long v0 = nI + (long long)rg.own0 * (nx + 1), nv = (long long)(rg.own1 - rg.own0) * (nx + 1);
         (void)NE;
-        run(2, [&] { face_kernel<R><<<(unsigned)((nh + nv + 127) / 128), 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
+        const unsigned g = (unsigned)((nh + nv + 127) / 128);
+        const bool ranged = !(rg.own0 == 0 && rg.own1 == ny);
+        if (ranged) {
+            if (ph.litho) run(2, [&] { face_kernel<R, true, true><<<g, 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
+            else run(2, [&] { face_kernel<R, false, true><<<g, 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
+        } else {
+            if (ph.litho) run(2, [&] { face_kernel<R, true, false><<<g, 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
+            else run(2, [&] { face_kernel<R, false, false><<<g, 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
+        }
         if (ph.diffusion)
             run(2, [&] { diffusion_kernel<R><<<(unsigned)((nh + nv + 127) / 128), 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
     }
@@ -303,7 +319,8 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
         SumArgs a{t->nx, t->ny, t->host_tab.area, 1.0 / t->host_tab.area, t->face, H, C, t->H, t->C, outH, outC, t->rate, mode, a0, a1, dt,
                   t->partial, nullptr, t->range.gj0, t->range.gny, (long long)t->range.own0 * t->nx,
                   (long long)t->range.own1 * t->nx, sb.srcH, sb.srcR, sb.srcS};
-        timed(t, 3, [&] { sum_kernel<<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
+        if (sb.srcH) timed(t, 3, [&] { sum_kernel<true><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
+        else timed(t, 3, [&] { sum_kernel<false><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
     }
     timed(t, 4, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, t->sum_blocks, t->d_tot); });
     count_launch(5);
@@ -871,7 +888,7 @@ mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double
                                  nullptr);
     {
         SumArgs a{nx, ny, tab.area, 1.0 / tab.area, face, H, C, H, C, rhsH, rhsC, rate, SUM_STORE_L, 0.0, 0.0, 0.0, part};
-        sum_kernel<<<sum_blocks, kRedBlock, 0, s>>>(a);
+        sum_kernel<false><<<sum_blocks, kRedBlock, 0, s>>>(a);
     }
     reduce_kernel<<<1, 1024, 0, s>>>(part, sum_blocks, tot);
     count_launch(5);
