@@ -278,6 +278,88 @@ mp_status mp_transport_set_hooks(mp_transport* t, mp_halo_fn halo, mp_combine_fn
  * (StateReconstruction::Limit, src/couple/state_reconstruction.cpp:136-192). */
 mp_status mp_transport_limiter(mp_transport* t, double* thetaH, double* thetaC);
 
+/* ---------------------------------------------------------------- preheat */
+
+/* The legacy dry preheat (mantle::couple::AdvanceLegacyPreheat,
+ * src/couple/preheat.h:26, preheat.cpp:65-287): H_t + div(us H - kappa grad H)
+ * = 0 with C held fixed and the Stokes velocity us frozen; forward Euler with
+ * the UNLIMITED ML-WENO reconstruction of H at the edge Gauss points, the
+ * linear-law Lax-Friedrichs flux (IntegrateAdvectiveFlux,
+ * src/mlweno/advectiveflux.cpp:327-338; boundary faces
+ * IntegrateAdvectiveBoundaryFlux :426-437), and the normal-line diffusion of
+ * H evaluated on constant cell-average samples. The per-cell rate, and so
+ * the step limit cfl / max rate, is fixed at begin (Build). */
+typedef struct mp_preheat_opts {
+    mp_material material;      /* phase model of the final diagnostics */
+    int pressure_model;        /* MP_PRESSURE_CONSTANT / MP_PRESSURE_LITHOSTATIC */
+    double pressure;           /* constant model: Pa; lithostatic: surface_y */
+    double end;                /* time.end */
+    long long max_steps;       /* time.maximumSteps */
+    int control;               /* MP_TIME_CFL or MP_TIME_FIXED */
+    double dt_initial, dt_min, dt_max;
+    double cfl;                /* time.step.cfl, in (0, 1] */
+    double diffusivity;        /* kappa >= 0 */
+    int thermal_type[4];       /* MP_THERMAL_*, walls bottom, top, left, right */
+    double thermal_value[4];
+    int H_policy;              /* MP_BC_* advection boundary of H */
+    double inflow_H;
+    int lf_global;             /* 0 local Lax-Friedrichs, 1 global */
+    double lf_global_speed;
+} mp_preheat_opts;
+
+/* PreheatStep (src/couple/preheat.h:6-11): one accepted step, or the
+ * initial state (dt = courant = boundaryFlux = balanceError = 0). */
+typedef struct mp_preheat_step {
+    long long step;
+    double time, dt, courant, integral, minimum, maximum, boundaryFlux, balanceError;
+} mp_preheat_step;
+
+/* PreheatReport (src/couple/preheat.h:13-17) without the history. */
+typedef struct mp_preheat_report {
+    double initialTime, finalTime, stepLimit;
+    double initialIntegral, finalIntegral, boundaryIntegral;
+} mp_preheat_report;
+
+typedef struct mp_preheat mp_preheat;
+
+mp_status mp_preheat_create(const mp_mesh_desc* mesh, const mp_preheat_opts* opts, mp_stream_t stream,
+                            mp_preheat** out);
+void mp_preheat_destroy(mp_preheat* p);
+/* Stokes velocity at the edge Gauss points: normal components [edge*5 + q]
+ * in the canonical order of this header (the x component on AlongJ edges,
+ * minus the y component on AlongI edges). */
+mp_status mp_preheat_set_velocity(mp_preheat* p, const double* vn);
+/* Cell averages H, C (nx*ny), the clock and InitialState::acceptedSteps. */
+mp_status mp_preheat_set_state(mp_preheat* p, const double* H, const double* C, double time, long long accepted);
+mp_status mp_preheat_get_state(mp_preheat* p, double* H, double* time, long long* accepted);
+/* Build (preheat.cpp:65-159) and the start of Run (:235-253): the per-cell
+ * rate (nx*ns, may be NULL), the step limit and the first history row;
+ * resets the run's step counter. MP_ERR_ARG_OUTOFRANGE when the state time
+ * exceeds time.end or a global LF speed is below a flow normal speed. */
+mp_status mp_preheat_begin(mp_preheat* p, double* rate, double* limit, mp_preheat_step* first);
+/* RHS (preheat.cpp:160-200) of the current H: dH/dt (may be NULL) and the
+ * outward boundary flux. */
+mp_status mp_preheat_rhs(mp_preheat* p, double* rhs, double* boundary_flux);
+/* Up to nsteps forward-Euler steps of Run (preheat.cpp:254-282), fewer when
+ * time.end is reached; rows (may be NULL) receives one entry per accepted
+ * step, *taken their number. Steps are issued in batches without a host
+ * round trip per step: the step sizes are fixed by the controls, and each
+ * step's finiteness and heat-balance checks run on the device, a failed
+ * step stopping the ones queued after it. On failure the state is the last
+ * accepted one (preheat.h:24-25) and the status says why:
+ * MP_ERR_FP (non-finite candidate), MP_ERR_PLIB (heat balance),
+ * MP_ERR_ARG_OUTOFRANGE (step above the limit or below time.step.minimum,
+ * backflow on an outflow-only wall), MP_ERR_NOT_CONVERGED (maximumSteps). */
+mp_status mp_preheat_advance(mp_preheat* p, long long nsteps, mp_preheat_step* rows, long long* taken);
+/* Diagnostics (preheat.cpp:202-233): cell T and phi from the 5x5 phase
+ * quadrature of the unlimited reconstruction of H and C. */
+mp_status mp_preheat_diagnostics(mp_preheat* p, double* T, double* phi);
+/* AdvanceLegacyPreheat: begin, advance to time.end, diagnostics. history
+ * (may be NULL) receives up to `capacity` rows (the initial row first);
+ * *rows = rows produced; T, phi may be NULL. */
+mp_status mp_preheat_run(mp_preheat* p, mp_preheat_report* report, mp_preheat_step* history,
+                         long long capacity, long long* rows, double* T, double* phi);
+
 /* --------------------------------------------------------------- batched */
 
 /* Many independent transport instances of uneven size advanced together

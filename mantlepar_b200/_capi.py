@@ -80,6 +80,26 @@ class StageTotals(C.Structure):
     _fields_ = [(n, C.c_double) for n in ["boundaryH", "boundaryC", "sourceH", "maxRate", "divergence"]]
 
 
+class PreheatOpts(C.Structure):
+    _fields_ = [("material", Material), ("pressure_model", C.c_int), ("pressure", C.c_double),
+                ("end", C.c_double), ("max_steps", C.c_longlong), ("control", C.c_int),
+                ("dt_initial", C.c_double), ("dt_min", C.c_double), ("dt_max", C.c_double), ("cfl", C.c_double),
+                ("diffusivity", C.c_double), ("thermal_type", C.c_int * 4), ("thermal_value", C.c_double * 4),
+                ("H_policy", C.c_int), ("inflow_H", C.c_double), ("lf_global", C.c_int),
+                ("lf_global_speed", C.c_double)]
+
+
+class PreheatStep(C.Structure):
+    _fields_ = [("step", C.c_longlong), ("time", C.c_double), ("dt", C.c_double), ("courant", C.c_double),
+                ("integral", C.c_double), ("minimum", C.c_double), ("maximum", C.c_double),
+                ("boundaryFlux", C.c_double), ("balanceError", C.c_double)]
+
+
+class PreheatReport(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ["initialTime", "finalTime", "stepLimit", "initialIntegral",
+                                          "finalIntegral", "boundaryIntegral"]]
+
+
 _lib = None
 
 
@@ -152,6 +172,17 @@ def lib() -> C.CDLL:
         "mp_transport_set_hooks": (i, [vp, vp, vp, vp]),
         "mp_transport_get_time": (i, [vp, dp, C.POINTER(C.c_int)]),
         "mp_batch_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
+        "mp_preheat_create": (i, [C.POINTER(MeshDesc), C.POINTER(PreheatOpts), vp, C.POINTER(vp)]),
+        "mp_preheat_destroy": (None, [vp]),
+        "mp_preheat_set_velocity": (i, [vp, vp]),
+        "mp_preheat_set_state": (i, [vp, vp, vp, d, C.c_longlong]),
+        "mp_preheat_get_state": (i, [vp, vp, dp, C.POINTER(C.c_longlong)]),
+        "mp_preheat_begin": (i, [vp, vp, dp, C.POINTER(PreheatStep)]),
+        "mp_preheat_rhs": (i, [vp, vp, dp]),
+        "mp_preheat_advance": (i, [vp, C.c_longlong, C.POINTER(PreheatStep), C.POINTER(C.c_longlong)]),
+        "mp_preheat_diagnostics": (i, [vp, vp, vp]),
+        "mp_preheat_run": (i, [vp, C.POINTER(PreheatReport), C.POINTER(PreheatStep), C.c_longlong,
+                               C.POINTER(C.c_longlong), vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -14,6 +14,8 @@
  *   src/couple/evolve.cpp                     (RHS, Admissible, SSPRK2 loop)
  *   src/couple/initial_flow.cpp               (edge porosity sampling)
  *   src/mlweno/diffusiveflux.cpp              (normal-line sample geometry)
+ *   src/mlweno/advectiveflux.cpp              (Lax-Friedrichs edge fluxes)
+ *   src/couple/preheat.cpp                    (legacy dry preheat)
  *   src/core/integral.cpp, src/core/mesh.cpp  (geometry, SplitMix64 noise)
  * keeping the reference's long double internals, so that it can be pinned
  * against the reference compiled from its own sources (oracle/_ref).
@@ -120,6 +122,28 @@ int orc_transport_set_pressure_model(orc_transport* t, int model, double value);
  * [cell*25 + b*5 + a], for the adiabatic source (evolve.cpp:359-369). */
 int orc_transport_set_cell_velocity(orc_transport* t, const double* vs_y, const double* ud_y);
 int orc_transport_limiter(orc_transport* t, double* thetaH, double* thetaC);
+
+/* Legacy dry preheat (src/couple/preheat.cpp:65-287) on a transport handle:
+ * the Stokes velocity is vs_n of set_face_velocity (ud_n unused), H is
+ * advected and diffused with the diffusivity and wall conditions of
+ * set_diffusion, C stays fixed; set_time_control gives the control and
+ * time.end, the opts dt_initial/dt_min/dt_max/cfl the step controls.
+ * One row per accepted step (PreheatStep, src/couple/preheat.h:6-11). */
+typedef struct orc_preheat_step {
+    long long step;
+    double time, dt, courant, integral, minimum, maximum, boundaryFlux, balanceError;
+} orc_preheat_step;
+/* Build (preheat.cpp:65-159) + the start of Run: per-cell rate, step limit,
+ * first history row; resets the run's step counter. */
+int orc_preheat_begin(orc_transport* t, double* rate, double* limit, orc_preheat_step* first);
+/* RHS (preheat.cpp:160-200) of the current H: dH/dt and the boundary flux. */
+int orc_preheat_rhs(orc_transport* t, double* rhs, double* boundary_flux);
+/* Up to nsteps forward-Euler steps of Run (preheat.cpp:254-282), stopping at
+ * time.end; *taken rows written. max_steps = time.maximumSteps. */
+int orc_preheat_advance(orc_transport* t, long long max_steps, long long nsteps, orc_preheat_step* rows,
+                        long long* taken);
+/* Diagnostics (preheat.cpp:202-233): cell T and phi. */
+int orc_preheat_diagnostics(orc_transport* t, double* T, double* phi);
 
 /* Synthetic input builders shared by tests and bench (SplitMix64 noise as in
  * src/core/mesh.cpp:12-25). */

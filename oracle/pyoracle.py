@@ -68,6 +68,16 @@ class StepReport(C.Structure):
                 ("C_integral", C.c_double)]
 
 
+class PreheatStep(C.Structure):
+    _fields_ = [("step", C.c_longlong), ("time", C.c_double), ("dt", C.c_double), ("courant", C.c_double),
+                ("integral", C.c_double), ("minimum", C.c_double), ("maximum", C.c_double),
+                ("boundaryFlux", C.c_double), ("balanceError", C.c_double)]
+
+
+def _row(r) -> dict:
+    return {n: getattr(r, n) for n, _ in PreheatStep._fields_}
+
+
 def _dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
 
@@ -97,6 +107,14 @@ class _Lib:
         t("rhs").argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 5 + [C.POINTER(StepReport)]
         t("limiter").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         t("step").argtypes = [C.c_void_p, C.c_int, C.POINTER(StepReport)]
+        p = lambda n: getattr(L, f"{prefix}_preheat_{n}")
+        for n in ["begin", "rhs", "advance", "diagnostics"]:
+            p(n).restype = C.c_int
+        p("begin").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(PreheatStep)]
+        p("rhs").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        p("advance").argtypes = [C.c_void_p, C.c_longlong, C.c_longlong, C.POINTER(PreheatStep),
+                                 C.POINTER(C.c_longlong)]
+        p("diagnostics").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
 
     def f(self, name):
         return getattr(self.lib, f"{self.prefix}_{name}")
@@ -171,13 +189,14 @@ class PhaseOracle:
 
 
 def transport_opts(w, *, uniform_tables=False, threads=0, integrator=None, pressure=0.0,
-                   dt_initial=1e30, dt_max=1e30, dt_min=1e-14) -> TransportOpts:
+                   dt_initial=1e30, dt_max=1e30, dt_min=1e-14, cfl=None, inflow_H=1.0, H_policy=0,
+                   lf_global=0, lf_global_speed=0.0) -> TransportOpts:
     return TransportOpts(nx=w.nx, ny=w.ny, x0=w.x0, x1=w.x1, y0=w.y0, y1=w.y1, pressure=pressure,
-                         cfl=w.cfl, dt_initial=dt_initial, dt_max=dt_max, dt_min=dt_min, theta=0.0,
-                         inflow_H=1.0, inflow_C=0.3, H_policy=0, C_policy=0,
-                         integrator=int(integrator if integrator is not None else w.integrator),
-                         lf_global=0, lf_global_speed=0.0, uniform_tables=int(uniform_tables),
-                         threads=int(threads))
+                         cfl=w.cfl if cfl is None else cfl, dt_initial=dt_initial, dt_max=dt_max,
+                         dt_min=dt_min, theta=0.0, inflow_H=inflow_H, inflow_C=0.3, H_policy=int(H_policy),
+                         C_policy=0, integrator=int(integrator if integrator is not None else w.integrator),
+                         lf_global=int(lf_global), lf_global_speed=float(lf_global_speed),
+                         uniform_tables=int(uniform_tables), threads=int(threads))
 
 
 class TransportOracle:
@@ -257,3 +276,31 @@ class TransportOracle:
         reps = (StepReport * max(1, nsteps))()
         code = self.lib.f("transport_step")(self.h, C.c_int(nsteps), reps)
         return code, [{n: getattr(r, n) for n, _ in StepReport._fields_} for r in reps[:nsteps]]
+
+    # Legacy dry preheat (src/couple/preheat.cpp) on this instance: velocity =
+    # vs of set_face_velocity, kappa and walls of set_diffusion, control and
+    # time.end of set_time_control.
+    def preheat_begin(self):
+        rate = np.zeros(self.w.cells)
+        limit = C.c_double()
+        first = PreheatStep()
+        code = self.lib.f("preheat_begin")(self.h, _dptr(rate), C.byref(limit), C.byref(first))
+        return code, rate, limit.value, _row(first)
+
+    def preheat_rhs(self):
+        rhs = np.zeros(self.w.cells)
+        b = C.c_double()
+        code = self.lib.f("preheat_rhs")(self.h, _dptr(rhs), C.byref(b))
+        return code, rhs, b.value
+
+    def preheat_advance(self, nsteps: int, max_steps: int = 1 << 62):
+        rows = (PreheatStep * max(1, nsteps))()
+        taken = C.c_longlong()
+        code = self.lib.f("preheat_advance")(self.h, C.c_longlong(max_steps), C.c_longlong(nsteps), rows,
+                                             C.byref(taken))
+        return code, [_row(r) for r in rows[:taken.value]]
+
+    def preheat_diagnostics(self):
+        T, phi = np.zeros(self.w.cells), np.zeros(self.w.cells)
+        code = self.lib.f("preheat_diagnostics")(self.h, _dptr(T), _dptr(phi))
+        return code, T, phi

@@ -1,11 +1,13 @@
 // Reference-backed oracle: the transport driver over the reference's OWN
 // compiled classes (src/mlweno Reconstruction/TensorStencilPoly, src/core
-// geometry, src/mlweno diffusion sampling, src/phase EutecticModel), built by
+// geometry, src/mlweno diffusion sampling and advective flux, src/phase
+// EutecticModel), built by
 // oracle/Makefile from the sources where they lie into oracle/_ref.
 // TEST INFRASTRUCTURE ONLY: used to pin the restated oracle and as the
 // CPU baseline ("kind": "reference"); never part of the product library.
 #include "reconstruction.h"
 #include "diffusiveflux.h"
+#include "advectiveflux.h"
 #include "integral.h"
 #include "eutectic_rescaled.h"
 
@@ -158,6 +160,37 @@ struct RefBackend {
         flux = r.flux;
         deriv = r.derivativeSamples;
     }
+    // The reference's own IntegrateAdvectiveFlux / IntegrateAdvectiveBoundaryFlux
+    // (advectiveflux.h:111-116,182-186) with the default linear law.
+    static double advect(orc::Pt a, orc::Pt b, const std::vector<double>& p, const std::vector<double>& w,
+                         const std::vector<orc::Pt>& vel, const std::vector<double>& left,
+                         const std::vector<double>& right, bool global, double speed) {
+        GaussRule1D rule; rule.points = p; rule.weights = w;
+        std::vector<Point> v;
+        for (const auto& x : vel) v.push_back(P(x));
+        LaxFriedrichsOptions opt;
+        opt.mode = global ? LaxFriedrichsMode::Global : LaxFriedrichsMode::Local;
+        opt.globalSpeed = speed;
+        PetscReal flux = 0;
+        check(IntegrateAdvectiveFlux(EdgeVertices{{P(a), P(b)}}, rule, v, left, right, 0.0, {}, opt, flux));
+        return flux;
+    }
+    static double advect_boundary(orc::Pt a, orc::Pt b, const std::vector<double>& p, const std::vector<double>& w,
+                                  const std::vector<orc::Pt>& vel, const std::vector<double>& interior,
+                                  const std::vector<orc::AdvectBC>& data) {
+        GaussRule1D rule; rule.points = p; rule.weights = w;
+        std::vector<Point> v;
+        for (const auto& x : vel) v.push_back(P(x));
+        std::vector<AdvectiveBoundaryValue> d(data.size());
+        for (size_t q = 0; q < data.size(); ++q) {
+            d[q].type = data[q].type == 0 ? AdvectiveBoundaryType::PrescribedState
+                      : (data[q].type == 1 ? AdvectiveBoundaryType::ExtrapolatedState : AdvectiveBoundaryType::ZeroFlux);
+            d[q].value = data[q].value;
+        }
+        PetscReal flux = 0;
+        check(IntegrateAdvectiveBoundaryFlux(EdgeVertices{{P(a), P(b)}}, rule, v, interior, d, 0.0, {}, flux));
+        return flux;
+    }
     static bool phase(const orc_material&, const orc_derived&, double H, double C, double Pp, orc_phase& s, int& code) {
         const EutecticModel* m = shared_model();
         code = classify_exceptions([&] { to_state(m->evaluate(H, C, Pp), s); });
@@ -241,5 +274,14 @@ int ref_transport_set_cell_velocity(void* t, const double* a, const double* b) {
 int ref_transport_set_diffusion(void* t, double kappa, const int* types, const double* values) {
     return RefApi::set_diffusion(t, kappa, types, values);
 }
+
+int ref_preheat_begin(void* t, double* rate, double* limit, orc_preheat_step* first) {
+    return RefApi::preheat_begin(t, rate, limit, first);
+}
+int ref_preheat_rhs(void* t, double* rhs, double* boundary_flux) { return RefApi::preheat_rhs(t, rhs, boundary_flux); }
+int ref_preheat_advance(void* t, long long max_steps, long long nsteps, orc_preheat_step* rows, long long* taken) {
+    return RefApi::preheat_advance(t, max_steps, nsteps, rows, taken);
+}
+int ref_preheat_diagnostics(void* t, double* T, double* phi) { return RefApi::preheat_diagnostics(t, T, phi); }
 
 }  // extern "C"

@@ -9,6 +9,8 @@
 //   src/mlweno/reconstruction.cpp     candidate filtering and log-space
 //                                     nonlinear weights (:109-355,:477-502)
 //   src/mlweno/diffusiveflux.cpp      normal-line sample geometry (:23-84,:255-334)
+//   src/mlweno/advectiveflux.cpp      linear-law Lax-Friedrichs edge and
+//                                     boundary flux integrals (:8-267)
 // The Gauss-Legendre rule stands in for PETSc's PetscDTGaussQuadrature
 // (PETSc 3.23+, not vendored): Newton iteration on P_n in long double, the
 // published Golub-Welsch-free method; nodes agree with PETSc to ~1 ulp.
@@ -532,6 +534,96 @@ inline void build_sampling(Pt a, Pt b, const Quad& left, const Quad* right,
             s.sides[at] = s.boundary ? (k + 1 == count ? 2 : 0) : (k < count / 2 ? 0 : 1);
         }
     }
+}
+
+// ------------------------------------------------------- advective flux
+
+// Advection boundary data of one edge point (AdvectiveBoundaryType):
+// 0 prescribed state, 1 extrapolated state, 2 zero flux.
+struct AdvectBC { int type = 1; double value = 0; };
+
+// advectiveflux.cpp:8-18 (RealValue) and :41-48 (NormalVelocity).
+inline double real_value(ld v) {
+    require(std::isfinite(v) && std::fabs(v) <= (ld)std::numeric_limits<double>::max(), E_FP,
+            "Advective flux or derivative is not representable");
+    return (double)v;
+}
+inline double normal_velocity(Pt v, Pt n) { return real_value((ld)v.x * n.x + (ld)v.y * n.y); }
+
+// advectiveflux.cpp:20-39 (CheckPoint) for the point fields the flux reads.
+inline void check_point(Pt p, Pt v, Pt n) {
+    require(std::isfinite(p.x) && std::isfinite(p.y) && std::isfinite(v.x) && std::isfinite(v.y) &&
+            std::isfinite(n.x) && std::isfinite(n.y), E_OUTOFRANGE, "Flux position, velocity and normal must be finite");
+    const double norm = std::hypot(n.x, n.y);
+    require(std::isfinite(norm) && std::fabs(norm - 1) <= 128 * std::numeric_limits<double>::epsilon(), E_WRONG,
+            "Advective flux requires a unit normal");
+}
+
+// LinearAdvectiveFlux (advectiveflux.cpp:272-285) through PhysicalFlux
+// (:64-80): value (v.n) u, derivative v.n.
+inline void linear_flux(double u, Pt v, Pt n, double& value, double& derivative) {
+    require(std::isfinite(u), E_OUTOFRANGE, "Advective trace must be finite");
+    derivative = normal_velocity(v, n);
+    value = real_value((ld)derivative * u);
+}
+
+// advectiveflux.cpp:82-87 (relative roundoff allowance of a speed bound).
+inline bool speed_bounds(double bound, double required) {
+    return bound >= required || required - bound <= 64 * std::numeric_limits<double>::epsilon() * std::max(bound, required);
+}
+
+// IntegrateAdvectiveFlux (advectiveflux.cpp:327-338 via EdgeImpl :180-225 and
+// FluxImpl :127-162) for the linear law: sum_q (w_q L / 2) Fhat_q with
+// Fhat = (F(uL) + F(uR) - alpha (uR - uL)) / 2 in long double, alpha = the
+// endpoint speed max(|F'(uL)|, |F'(uR)|) (local) or the supplied global speed.
+inline double integrate_advective_flux(Pt a, Pt b, const std::vector<double>& rp, const std::vector<double>& rw,
+                                       const std::vector<Pt>& vel, const std::vector<double>& left,
+                                       const std::vector<double>& right, bool global, double global_speed) {
+    double length; Pt normal;
+    edge_geometry(a, b, length, normal);
+    for (const Pt& v : vel) require(std::isfinite(v.x) && std::isfinite(v.y), E_OUTOFRANGE, "Edge velocity must be finite");
+    if (global) require(std::isfinite(global_speed) && global_speed >= 0, E_OUTOFRANGE, "Global LF speed must be finite and nonnegative");
+    ld sum = 0;
+    for (size_t q = 0; q < rp.size(); ++q) {
+        const Pt p = map_edge(rp[q], a, b);
+        check_point(p, vel[q], normal);
+        double fl, dl, fr, dr;
+        linear_flux(left[q], vel[q], normal, fl, dl);
+        linear_flux(right[q], vel[q], normal, fr, dr);
+        const double speed = std::max(std::fabs(dl), std::fabs(dr));
+        const double alpha = global ? global_speed : speed;
+        require(speed_bounds(alpha, speed), E_OUTOFRANGE, "Supplied global LF speed is smaller than the current local bound");
+        const ld jump = (ld)right[q] - left[q];
+        const double flux = real_value(((ld)fl + fr - (ld)alpha * jump) / 2);
+        const ld weight = (ld)rw[q] * length / 2;
+        sum += weight * flux;
+    }
+    return real_value(sum);
+}
+
+// IntegrateAdvectiveBoundaryFlux (advectiveflux.cpp:426-437 via BoundaryImpl
+// :227-267): the physical flux of the prescribed state (inflow) or of the
+// interior trace (outflow), exactly zero at zero-flux points.
+inline double integrate_advective_boundary_flux(Pt a, Pt b, const std::vector<double>& rp, const std::vector<double>& rw,
+                                                const std::vector<Pt>& vel, const std::vector<double>& interior,
+                                                const std::vector<AdvectBC>& data) {
+    double length; Pt normal;
+    edge_geometry(a, b, length, normal);
+    for (const Pt& v : vel) require(std::isfinite(v.x) && std::isfinite(v.y), E_OUTOFRANGE, "Edge velocity must be finite");
+    ld sum = 0;
+    for (size_t q = 0; q < rp.size(); ++q) {
+        require(data[q].type >= 0 && data[q].type <= 2, E_WRONG, "Unknown advection boundary policy");
+        require(std::isfinite(interior[q]), E_OUTOFRANGE, "Interior boundary trace must be finite");
+        const Pt p = map_edge(rp[q], a, b);
+        check_point(p, vel[q], normal);
+        if (data[q].type == 2) continue;
+        const bool outflow = data[q].type == 1;
+        double f, d;
+        linear_flux(outflow ? interior[q] : data[q].value, vel[q], normal, f, d);
+        const ld weight = (ld)rw[q] * length / 2;
+        sum += weight * f;
+    }
+    return real_value(sum);
 }
 
 }  // namespace orc

@@ -1,6 +1,6 @@
 /* Serial stand-in for the subset of PETSc's petscsys.h used by the
  * reference's src/core/integral.*, src/mlweno/{tensorstencilpoly,
- * reconstruction,diffusiveflux}.* (TEST INFRASTRUCTURE: lets the oracle
+ * reconstruction,diffusiveflux,advectiveflux}.* (TEST INFRASTRUCTURE: lets the oracle
  * compile those reference sources unmodified into oracle/_ref). Error
  * macros return the PETSc error class; no messages, no MPI. */
 #ifndef MP_SHIM_PETSCSYS_H
@@ -41,4 +41,19 @@ typedef int MPI_Comm;
 #define PetscSqrtReal(x) std::sqrt(x)
 #define PetscSinReal(x) std::sin(x)
 #define PetscRealPart(x) (x)
+/* One rank: an all-reduce of local values returns them unchanged (used by
+ * ReduceGlobalLaxFriedrichsSpeed in src/mlweno/advectiveflux.cpp). */
+typedef int MPI_Datatype;
+typedef int MPI_Op;
+#define MPI_INT 1
+#define MPIU_REAL 2
+#define MPI_MAX 1
+inline int MPI_Allreduce(const void* in, void* out, int count, MPI_Datatype type, MPI_Op, MPI_Comm) {
+    const unsigned char* a = static_cast<const unsigned char*>(in);
+    unsigned char* b = static_cast<unsigned char*>(out);
+    const int size = type == MPI_INT ? (int)sizeof(int) : (int)sizeof(double);
+    for (int k = 0; k < count * size; ++k) b[k] = a[k];
+    return 0;
+}
+#define PetscCallMPI(x) do { if ((x) != 0) return PETSC_ERR_LIB; } while (0)
 #endif

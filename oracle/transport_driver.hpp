@@ -10,6 +10,8 @@
 //   src/couple/evolve.cpp:428-511   Run (SSPRK2 with CFL retry, balance check)
 //   src/couple/state_reconstruction.cpp:101-192  Update, Evaluate, Limit
 //   src/couple/initial_flow.cpp:94-117  edge porosity (harmonic mean, dry cells)
+//   src/couple/preheat.cpp:65-287   legacy dry preheat (Build, RHS, Run,
+//                                   Diagnostics)
 // The flow supplier (Stokes-Darcy FEM, re-solved per stage in the reference)
 // is replaced by face-normal velocity data: solid velocity and Darcy velocity
 // normal components at each edge Gauss point, frozen for the run. The edge
@@ -602,6 +604,193 @@ struct Driver {
         rep.maxRate = current.maximumRate; rep.divergence = current.divergence;
         rep.balanceH = bH; rep.balanceC = bC; rep.H_integral = HI; rep.C_integral = CI;
     }
+
+    // ------------------------------------------------ legacy dry preheat
+    // src/couple/preheat.cpp: H_t + div(us H - kappa grad H) = 0 with C fixed
+    // and the Stokes velocity frozen (vsn, the solid normal components; ud
+    // unused). Forward Euler with the unlimited reconstruction of H, the
+    // linear-law Lax-Friedrichs edge flux, and the normal-line diffusion of
+    // H on constant cell-average samples. The time controls of
+    // set_time_control apply (t_end = time.end) with o.dt_initial/min/max.
+    std::vector<double> pre_rate;        // constant per-cell rate (Build)
+    double pre_rate_max = 0, pre_limit = 0;
+    long long pre_steps = 0;             // steps of this run (Run's counter)
+    double pre_integral = 0;             // report.finalIntegral
+    bool pre_ready = false;
+
+    // Velocity vectors of a face's points in its oriented order: the normal
+    // component along the face normal (the tangential part enters neither
+    // the flux nor the rate, and on this mesh v.n reproduces it exactly).
+    void face_velocity(const Face& f, std::vector<Pt>& vel) const {
+        vel.resize(nq);
+        for (int q = 0; q < nq; ++q) {
+            const int cq = f.reverse ? nq - 1 - q : q;
+            const double vn = (f.reverse ? -1.0 : 1.0) * vsn[(size_t)f.edge * nq + cq];
+            vel[q] = Pt{vn * f.normal.x, vn * f.normal.y};
+        }
+    }
+
+    // preheat.cpp:65-159 (Build): per face the LF speed sum_q L w_q alpha / 2
+    // and the diffusion derivatives at zero samples summed per side; each
+    // side's cell gets (speed + |derivative|) / area, faces in edge order.
+    void preheat_build() {
+        const size_t nf = faces.size();
+        std::vector<double> r0(nf), r1(nf);
+        parallel_for((int)nf, [&](int fi) {
+            const Face& f = faces[fi];
+            std::vector<Pt> vel;
+            face_velocity(f, vel);
+            double speed = 0;
+            for (int q = 0; q < nq; ++q) {
+                const double ns = std::fabs(vel[q].x * f.normal.x + vel[q].y * f.normal.y);
+                const double alpha = o.lf_global ? o.lf_global_speed : ns;
+                require(alpha + 1e-14 >= ns, E_OUTOFRANGE, "Global LF speed is smaller than the flow normal speed");
+                speed += .5 * f.length * gw[q] * alpha;
+            }
+            const std::vector<double> u(f.diffusion.samples.size(), 0.0);
+            double dflux;
+            std::vector<double> deriv;
+            B::diffuse(f.diffusion, u, kappa, f.boundary ? &wall_bc[wall_of(f)] : nullptr, dflux, deriv);
+            double d[2] = {0, 0};
+            for (size_t q = 0; q < u.size(); ++q)
+                if (f.diffusion.sides[q] != 2) d[f.diffusion.sides[q]] += deriv[q];
+            r0[fi] = (speed + std::fabs(d[0])) / f.area[0];
+            r1[fi] = (speed + std::fabs(d[1])) / f.area[1];
+        });
+        pre_rate.assign(ncell, 0.0);
+        for (size_t fi = 0; fi < nf; ++fi) {
+            pre_rate[faces[fi].left] += r0[fi];
+            if (!faces[fi].boundary) pre_rate[faces[fi].right] += r1[fi];
+        }
+        pre_rate_max = *std::max_element(pre_rate.begin(), pre_rate.end());
+        pre_limit = pre_rate_max > 0 ? o.cfl / pre_rate_max : o.dt_max;
+    }
+
+    // preheat.cpp:160-200 (RHS): dH/dt of the current H and the outward
+    // boundary flux (boundary faces in edge order).
+    double preheat_rhs() {
+        parallel_for(ncell, [&](int k) { rh[k].update(H, nx, area[k]); });
+        std::fill(rhsH.begin(), rhsH.end(), 0.0);
+        const size_t nf = faces.size();
+        std::vector<double> fl(nf);
+        parallel_for((int)nf, [&](int fi) {
+            const Face& f = faces[fi];
+            std::vector<Pt> vel;
+            face_velocity(f, vel);
+            std::vector<double> left(nq), right(nq);
+            std::vector<AdvectBC> data(nq);
+            for (int q = 0; q < nq; ++q) {
+                const Pt p = B::map_edge(gp[q], f.a, f.b);
+                // StateReconstruction::Enthalpy with the limiter factor 1.
+                const double hl = rh[f.left].evaluate(p);
+                left[q] = H[f.left] + 1.0 * (hl - H[f.left]);
+                if (f.boundary) {
+                    // EvaluateAdvectionBoundary (initialization.cpp:469-489).
+                    const double speed = vel[q].x * f.normal.x + vel[q].y * f.normal.y;
+                    require(std::isfinite(speed), E_OUTOFRANGE, "normal speed must be finite");
+                    if (o.H_policy == 2 || speed == 0) data[q].type = 2;
+                    else if (speed < 0) {
+                        require(o.H_policy == 0, E_OUTOFRANGE, "Backflow encountered on an outflow-only boundary.");
+                        data[q].type = 0;
+                        data[q].value = o.inflow_H;
+                    } else data[q].type = 1;
+                } else {
+                    const double hr = rh[f.right].evaluate(p);
+                    right[q] = H[f.right] + 1.0 * (hr - H[f.right]);
+                }
+            }
+            const double advection = f.boundary ? B::advect_boundary(f.a, f.b, gp, gw, vel, left, data)
+                                                : B::advect(f.a, f.b, gp, gw, vel, left, right, o.lf_global != 0, o.lf_global_speed);
+            std::vector<double> samples(f.diffusion.samples.size(), 0.0);
+            for (size_t q = 0; q < samples.size(); ++q) {
+                const int side = f.diffusion.sides[q];
+                if (side != 2) samples[q] = H[side == 0 ? f.left : f.right];
+            }
+            double diffusion;
+            std::vector<double> deriv;
+            B::diffuse(f.diffusion, samples, kappa, f.boundary ? &wall_bc[wall_of(f)] : nullptr, diffusion, deriv);
+            fl[fi] = advection + diffusion;
+        });
+        double boundary = 0;
+        for (size_t fi = 0; fi < nf; ++fi) {
+            const Face& f = faces[fi];
+            rhsH[f.left] += -fl[fi] / f.area[0];
+            if (!f.boundary) rhsH[f.right] += fl[fi] / f.area[1];
+            else boundary += fl[fi];
+        }
+        return boundary;
+    }
+
+    // preheat.cpp:235-253: Build, the step limit and the first history row.
+    void preheat_begin(orc_preheat_step& first) {
+        require(time <= t_end, E_OUTOFRANGE, "State time exceeds time.end");
+        require(o.cfl <= 1, E_OUTOFRANGE, "Explicit preheat requires time.step.cfl <= 1");
+        preheat_build();
+        pre_integral = integral(H);
+        pre_steps = 0;
+        pre_ready = true;
+        first = orc_preheat_step{};
+        first.time = time; first.step = accepted; first.integral = pre_integral;
+        first.minimum = *std::min_element(H.begin(), H.end());
+        first.maximum = *std::max_element(H.begin(), H.end());
+    }
+
+    // preheat.cpp:254-282: one forward-Euler step (false at time.end).
+    bool preheat_step(long long max_steps, orc_preheat_step& row) {
+        if (!(time < t_end)) return false;
+        require(pre_steps < max_steps, E_NOT_CONVERGED, "maximum_steps reached before time.end");
+        const double remaining = t_end - time;
+        double dt = fixed ? o.dt_initial : std::min(o.dt_max, pre_limit);
+        if (!fixed && pre_steps == 0) dt = std::min(dt, o.dt_initial);
+        dt = std::min(dt, remaining);
+        const double roundoff = 8 * std::numeric_limits<double>::epsilon() * std::max({std::fabs(t_end), std::fabs(time), dt});
+        if (remaining - dt <= roundoff) dt = remaining;
+        require(dt <= pre_limit * (1 + 1e-12), E_OUTOFRANGE, "Requested step exceeds advection/diffusion limit");
+        require(dt >= o.dt_min || dt == remaining, E_OUTOFRANGE, "Stable step is below time.step.minimum");
+        require(time + dt > time && std::isfinite(dt), E_FP, "Time step does not advance finite time");
+        row = orc_preheat_step{};
+        row.dt = dt; row.courant = dt * pre_rate_max;
+        row.boundaryFlux = preheat_rhs();
+        std::vector<double> cand(ncell);
+        bool finite = true;
+        for (int k = 0; k < ncell; ++k) { cand[k] = H[k] + dt * rhsH[k]; finite = finite && std::isfinite(cand[k]); }
+        require(finite, E_FP, "Nonfinite preheat candidate rejected");
+        row.integral = integral(cand);
+        row.balanceError = row.integral - pre_integral + dt * row.boundaryFlux;
+        const double tol = 1e-10 * (1 + std::fabs(row.integral) + std::fabs(pre_integral) + std::fabs(dt * row.boundaryFlux));
+        require(std::fabs(row.balanceError) <= tol, E_PLIB, "Preheat heat balance failed; candidate rejected");
+        row.minimum = *std::min_element(cand.begin(), cand.end());
+        row.maximum = *std::max_element(cand.begin(), cand.end());
+        H = cand;
+        time = dt == remaining ? t_end : time + dt;
+        ++accepted; ++pre_steps;
+        row.time = time; row.step = accepted;
+        pre_integral = row.integral;
+        return true;
+    }
+
+    // preheat.cpp:202-233 (Diagnostics): T, phi per cell from the 5x5
+    // quadrature of the phase of the unlimited reconstruction of H and C.
+    void preheat_diagnostics() {
+        update();
+        parallel_for(ncell, [&](int k) {
+            const int i = k % nx, j = k / nx;
+            const Quad q = corners(i, j);
+            double t = 0, ph = 0;
+            for (int b = 0; b < nq; ++b)
+                for (int a = 0; a < nq; ++a) {
+                    const Pt ref{gp[a], gp[b]};
+                    const Pt p = B::map_cell(ref, q);
+                    double h, c;
+                    evaluate(k, p, h, c);
+                    orc_phase s; int code = 0;
+                    if (!B::phase(mat, der, h, c, pressure_at(p), s, code)) throw Error{E_PHASE + code, "Phase evaluation failed"};
+                    const double weight = gw[a] * gw[b] * B::cell_jacobian(ref, q) / area[k];
+                    t += weight * s.TDp; ph += weight * s.phil;
+                }
+            T[k] = t; phi[k] = ph;
+        });
+    }
 };
 
 
@@ -633,7 +822,7 @@ struct Api {
         auto& d = static_cast<Handle<B>*>(h)->d;
         std::copy(H, H + d.ncell, d.H.begin());
         std::copy(C, C + d.ncell, d.C.begin());
-        d.time = time; d.accepted = 0; d.have_current = false;
+        d.time = time; d.accepted = 0; d.have_current = false; d.pre_ready = false;
         return 0;
     }
     static int get_state(const void* h, double* H, double* C, double* T, double* phi) {
@@ -706,6 +895,52 @@ struct Api {
         d.fixed = control == 1;
         d.t_end = t_end;
         return 0;
+    }
+
+    static int preheat_begin(void* h, double* rate, double* limit, orc_preheat_step* first) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        try {
+            orc_preheat_step r;
+            d.preheat_begin(r);
+            if (rate) std::copy(d.pre_rate.begin(), d.pre_rate.end(), rate);
+            if (limit) *limit = d.pre_limit;
+            if (first) *first = r;
+            return 0;
+        } catch (const Error& e) { d.pre_ready = false; return e.code; }
+    }
+    static int preheat_rhs(void* h, double* rhs, double* boundary) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        try {
+            const double b = d.preheat_rhs();
+            if (rhs) std::copy(d.rhsH.begin(), d.rhsH.end(), rhs);
+            if (boundary) *boundary = b;
+            return 0;
+        } catch (const Error& e) { return e.code; }
+    }
+    // Up to nsteps steps (fewer at time.end); on failure the last accepted
+    // state stays (preheat.h:24-25).
+    static int preheat_advance(void* h, long long max_steps, long long nsteps, orc_preheat_step* rows, long long* taken) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        long long n = 0;
+        int code = 0;
+        if (!d.pre_ready) code = E_WRONGSTATE;
+        else {
+            try {
+                orc_preheat_step r;
+                while (n < nsteps && d.preheat_step(max_steps, r)) { if (rows) rows[n] = r; ++n; }
+            } catch (const Error& e) { code = e.code; }
+        }
+        if (taken) *taken = n;
+        return code;
+    }
+    static int preheat_diagnostics(void* h, double* T, double* phi) {
+        auto& d = static_cast<Handle<B>*>(h)->d;
+        try {
+            d.preheat_diagnostics();
+            if (T) std::copy(d.T.begin(), d.T.end(), T);
+            if (phi) std::copy(d.phi.begin(), d.phi.end(), phi);
+            return 0;
+        } catch (const Error& e) { return e.code; }
     }
 
     static int step(void* h, int nsteps, orc_step_report* report) {

@@ -109,6 +109,16 @@ struct Restated {
                         double& flux, std::vector<double>& deriv) {
         integrate_diffusion(s, samples, kappa, bc, flux, deriv);
     }
+    static double advect(Pt a, Pt b, const std::vector<double>& p, const std::vector<double>& w,
+                         const std::vector<Pt>& vel, const std::vector<double>& left, const std::vector<double>& right,
+                         bool global, double speed) {
+        return integrate_advective_flux(a, b, p, w, vel, left, right, global, speed);
+    }
+    static double advect_boundary(Pt a, Pt b, const std::vector<double>& p, const std::vector<double>& w,
+                                  const std::vector<Pt>& vel, const std::vector<double>& interior,
+                                  const std::vector<AdvectBC>& data) {
+        return integrate_advective_boundary_flux(a, b, p, w, vel, interior, data);
+    }
     static bool derive(const orc_material& m, orc_derived& d) { return orc_internal::derive(m, d); }
 };
 
@@ -150,6 +160,20 @@ extern "C" int orc_transport_set_diffusion(orc_transport* t, double kappa, const
 }
 extern "C" int orc_transport_set_time_control(orc_transport* t, int control, double t_end) {
     return RestatedApi::set_time_control(t, control, t_end);
+}
+
+extern "C" int orc_preheat_begin(orc_transport* t, double* rate, double* limit, orc_preheat_step* first) {
+    return RestatedApi::preheat_begin(t, rate, limit, first);
+}
+extern "C" int orc_preheat_rhs(orc_transport* t, double* rhs, double* boundary_flux) {
+    return RestatedApi::preheat_rhs(t, rhs, boundary_flux);
+}
+extern "C" int orc_preheat_advance(orc_transport* t, long long max_steps, long long nsteps, orc_preheat_step* rows,
+                                   long long* taken) {
+    return RestatedApi::preheat_advance(t, max_steps, nsteps, rows, taken);
+}
+extern "C" int orc_preheat_diagnostics(orc_transport* t, double* T, double* phi) {
+    return RestatedApi::preheat_diagnostics(t, T, phi);
 }
 
 // Synthetic-input noise: SplitMix64 keyed like src/core/mesh.cpp:40-44

@@ -4,7 +4,7 @@ Run in a container where the reference sources are mounted (they are not on
 GPU machines):
 
     make -C oracle ref            # compiles the reference's sources into oracle/_ref
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [phase] [transport] [preheat]
 
 Writes, next to this script:
   phase_golden.npz      inputs and EutecticModel::evaluate outputs of the
@@ -18,6 +18,9 @@ Writes, next to this script:
                         seeded synthetic workloads: one RHS and short runs on
                         20x20 and on small meshes with every boundary class,
                         plus 200-step SSPRK2 and SSPRK3 runs of 20x20.
+  preheat_golden.npz    the reference-backed legacy dry preheat on the seeded
+                        cases of tests/preheat_cases.py.
+Arguments (phase, transport, preheat) select fixtures; none = all.
 """
 from __future__ import annotations
 
@@ -142,8 +145,34 @@ def transport_golden():
     print("transport_golden.npz:", len(data), "arrays")
 
 
+ROW_FIELDS = ["step", "time", "dt", "courant", "integral", "minimum", "maximum", "boundaryFlux", "balanceError"]
+
+
+def preheat_golden():
+    """The reference-backed preheat (src/couple/preheat.cpp driver over the
+    reference's reconstruction, advective and diffusive flux functions) on the
+    seeded cases of tests/preheat_cases.py: Build, one RHS, the whole run and
+    the diagnostics."""
+    import preheat_cases as pc
+    data = {}
+    for name, case in pc.CASES.items():
+        r = pc.oracle_run(case, po.reference())
+        assert r["begin"] == 0 and r["rhs_code"] == 0 and r["run"] == 0 and r["diag"] == 0, name
+        for k in ["rate", "rhs", "H", "T", "phi"]:
+            data[f"{name}_{k}"] = r[k]
+        data[f"{name}_scalars"] = np.array([r["limit"], r["bflux"]])
+        data[f"{name}_rows"] = np.array([[row[f] for f in ROW_FIELDS] for row in [r["first"]] + r["rows"]])
+    np.savez_compressed(os.path.join(HERE, "preheat_golden.npz"), **data)
+    print("preheat_golden.npz:", len(data), "arrays")
+
+
 if __name__ == "__main__":
     if not po.reference_available():
         sys.exit("reference build missing: run `make -C oracle ref` where the reference is mounted")
-    phase_golden()
-    transport_golden()
+    which = sys.argv[1:] or ["phase", "transport", "preheat"]
+    if "phase" in which:
+        phase_golden()
+    if "transport" in which:
+        transport_golden()
+    if "preheat" in which:
+        preheat_golden()

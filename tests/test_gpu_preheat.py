@@ -1,0 +1,189 @@
+"""GPU parity of the legacy dry preheat (src/couple/preheat.cpp) against the
+reference-backed golden runs and the oracle.
+
+Bars (FP64 kernels against the reference's 80-bit long double internals):
+per-cell relative error 1e-12 for the rate, the final H and the diagnostic
+T and phi (|x - ref| / max(|ref|, 1e-3 max|ref|)); the RHS, a signed sum of
+face fluxes, against its infinity norm (1e-12); step sizes, integrals and
+extrema of every history row 1e-12 relative (the boundary flux 1e-12 of
+max(1, |ref|)); failure statuses equal.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from mantlepar_b200 import synthetic as sy
+import preheat_cases as pc
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = np.load(os.path.join(os.path.dirname(__file__), "golden", "preheat_golden.npz"))
+ROW_FIELDS = ["step", "time", "dt", "courant", "integral", "minimum", "maximum", "boundaryFlux", "balanceError"]
+RTOL = 1e-12
+
+
+def rel(a, b):
+    b = np.asarray(b)
+    return np.max(np.abs(np.asarray(a) - b) / np.maximum(np.abs(b), 1e-3 * max(np.max(np.abs(b)), 1e-300)))
+
+
+def rel_inf(a, b):
+    b = np.asarray(b)
+    return np.max(np.abs(np.asarray(a) - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+def check_rows(rows, ref):
+    """rows: list of dicts (first row included); ref: golden row matrix."""
+    assert len(rows) == len(ref)
+    for row, r in zip(rows, ref):
+        want = dict(zip(ROW_FIELDS, r))
+        assert row["step"] == want["step"]
+        for k in ["time", "dt", "courant", "integral", "minimum", "maximum"]:
+            assert abs(row[k] - want[k]) <= RTOL * max(abs(want[k]), 1e-300), (k, row[k], want[k])
+        assert abs(row["boundaryFlux"] - want["boundaryFlux"]) <= RTOL * max(1.0, abs(want["boundaryFlux"]))
+
+
+@pytest.mark.parametrize("name", list(pc.CASES))
+def test_preheat_matches_reference(cuda_lib, name):
+    case = pc.CASES[name]
+    p = pc.gpu_instance(case)
+    rate, limit, first = p.begin()
+    assert rel(rate, GOLDEN[f"{name}_rate"]) <= RTOL
+    lim_ref, bflux_ref = GOLDEN[f"{name}_scalars"]
+    assert abs(limit - lim_ref) <= RTOL * lim_ref
+    rhs, bflux = p.rhs()
+    assert rel_inf(rhs, GOLDEN[f"{name}_rhs"]) <= RTOL
+    assert abs(bflux - bflux_ref) <= RTOL * max(1.0, abs(bflux_ref))
+    code, rows = p.advance(10000)
+    assert code == 0
+    check_rows([first] + rows, GOLDEN[f"{name}_rows"])
+    H, time, accepted = p.get_state()
+    assert time == case.end and accepted == len(rows)
+    assert rel(H, GOLDEN[f"{name}_H"]) <= RTOL
+    T, phi = p.diagnostics()
+    assert rel(T, GOLDEN[f"{name}_T"]) <= RTOL
+    assert rel(phi, GOLDEN[f"{name}_phi"]) <= RTOL if np.max(GOLDEN[f"{name}_phi"]) > 0 else np.all(phi == 0)
+
+
+def test_preheat_run_report(cuda_lib):
+    """mp_preheat_run: AdvanceLegacyPreheat's report and history in one call."""
+    case = pc.CASES["through_diffusion"]
+    p = pc.gpu_instance(case)
+    code, rep, rows, T, phi = p.run()
+    assert code == 0
+    ref = GOLDEN["through_diffusion_rows"]
+    check_rows(rows, ref)
+    assert rep["initialTime"] == 0.0 and rep["finalTime"] == case.end
+    assert abs(rep["finalIntegral"] - ref[-1][4]) <= RTOL * abs(ref[-1][4])
+    bint = sum(r["dt"] * r["boundaryFlux"] for r in rows[1:])
+    assert abs(rep["boundaryIntegral"] - bint) <= 1e-14
+    assert rel(T, GOLDEN["through_diffusion_T"]) <= RTOL
+
+
+def test_preheat_long_run_crosses_batches(cuda_lib):
+    """More steps than one device batch (512): the device-side step chain
+    continues across host round trips; every row matches the oracle."""
+    case = pc.PreheatCase(sy.Workload(nx=16, ny=12, seed=4), through=0.05, kappa=1e-3,
+                          thermal_type=(1, 1, 0, 0), thermal_value=(1.0, 0.2, 0.0, 0.0), dt_max=2e-4, end=0.15)
+    ref = pc.oracle_run(case)
+    assert ref["run"] == 0 and len(ref["rows"]) > 700
+    p = pc.gpu_instance(case)
+    _, _, first = p.begin()
+    code, rows = p.advance(100000)
+    assert code == 0
+    check_rows([first] + rows, np.array([[r[f] for f in ROW_FIELDS] for r in [ref["first"]] + ref["rows"]]))
+    H, _, _ = p.get_state()
+    assert rel(H, ref["H"]) <= 1e-11
+
+
+def test_preheat_advance_in_pieces(cuda_lib):
+    """advance(n) in pieces reproduces one advance to time.end."""
+    case = pc.CASES["closed"]
+    a = pc.gpu_instance(case)
+    a.begin()
+    _, ra = a.advance(1000)
+    b = pc.gpu_instance(case)
+    b.begin()
+    rb = []
+    while True:
+        code, got = b.advance(2)
+        assert code == 0
+        rb += got
+        if len(got) < 2:
+            break
+    assert ra == rb
+    assert np.array_equal(a.get_state()[0], b.get_state()[0])
+
+
+def _failure(**kw):
+    case = pc.PreheatCase(sy.Workload(nx=6, ny=6, seed=2), **kw)
+    ref = pc.oracle_run(case)
+    p = pc.gpu_instance(case)
+    from mantlepar_b200._capi import MPError
+    out = {}
+    try:
+        p.begin()
+        out["begin"] = 0
+    except MPError as e:
+        out["begin"] = e.code
+        return ref, out, p
+    code, rows = p.advance(100000, raise_on_error=False)
+    out["run"], out["rows"] = code, rows
+    return ref, out, p
+
+
+def test_preheat_failures_match_reference(cuda_lib):
+    # Backflow through an outflow-only wall.
+    ref, out, _ = _failure(through=0.3, H_policy=1)
+    assert out["run"] == ref["run"] == 63 and out["rows"] == []
+    # A fixed step above the rate limit.
+    ref, out, _ = _failure(control=1, dt_initial=1.0, end=2.0)
+    assert out["run"] == ref["run"] == 63
+    # maximumSteps: the allowed steps are kept, then NOT_CONVERGED.
+    ref, out, p = _failure(max_steps=3, end=1.0, dt_max=1e-3)
+    assert out["run"] == ref["run"] == 91 and len(out["rows"]) == 3
+    H, time, accepted = p.get_state()
+    assert accepted == 3 and abs(time - ref["rows"][-1]["time"]) <= 1e-15
+    assert rel(H, ref["H"]) <= RTOL
+    # State time after time.end; a global LF speed below a flow speed.
+    assert _failure(end=-1.0)[1]["begin"] == 63
+    assert _failure(through=0.3, lf_global=1, lf_global_speed=0.01)[1]["begin"] == 63
+
+
+def test_preheat_rejected_candidate_keeps_state(cuda_lib):
+    """A non-finite candidate is rejected on the device (preheat.cpp:268-269):
+    no row, the state and clock stay at the last accepted step. The state is
+    finite but so large that H + dt*rhs overflows."""
+    case = pc.PreheatCase(sy.Workload(nx=8, ny=8, seed=2), through=0.2, end=0.05)
+    p = pc.gpu_instance(case)
+    H, C = case.state()
+    H = H * 1e306
+    p.set_state(H, C)
+    p.begin()
+    code, rows = p.advance(100, raise_on_error=False)
+    t = pc.oracle_instance(case)
+    t.set_state(H, C)
+    t.preheat_begin()
+    ref_code, ref_rows = t.preheat_advance(100)
+    assert code == ref_code and code in (63, 72) and len(rows) == len(ref_rows)
+    H1, time, accepted = p.get_state()
+    assert np.array_equal(H1, H) and time == 0.0 and accepted == 0
+
+
+def test_preheat_large_mesh_properties(cuda_lib):
+    """1280x2560, 20 steps, closed box: every row's heat balance holds, the
+    boundary flux is zero and the heat integral is conserved to roundoff."""
+    w = sy.Workload(nx=1280, ny=2560)
+    case = pc.PreheatCase(w, kappa=1e-5, end=1.0, dt_max=1e-4)
+    p = pc.gpu_instance(case)
+    _, limit, first = p.begin()
+    code, rows = p.advance(20)
+    assert code == 0 and len(rows) == 20
+    prev = first["integral"]
+    for r in rows:
+        assert r["boundaryFlux"] == 0.0
+        assert abs(r["integral"] - prev) <= 1e-12 * abs(prev)
+        prev = r["integral"]
+    H, time, accepted = p.get_state()
+    assert accepted == 20 and np.all(np.isfinite(H))
