@@ -224,6 +224,52 @@ def timed_steps(obj, steps, stream):
     return e0.elapsed_time(e1), out
 
 
+# Legacy dry preheat (src/couple/preheat.cpp) per cell-step: unlimited H
+# reconstruction (read H, write 9 coefficients), edge fluxes (read both
+# sides' coefficients and averages, 2 edges x 5 normal velocities, write 2
+# fluxes), update (read H and 4 fluxes, write H): 8 + 72 + 72 + 8 + 80 + 16 +
+# 8 + 16 + 8 bytes.
+PREHEAT_BYTES_PER_CELL_STEP = 288
+
+
+def preheat_form(steps, stream, nx=None, ny=None):
+    """The legacy dry preheat on the plain mesh (1280x2560): forward Euler with
+    kappa = 1e-4 and wall temperatures, the synthetic Stokes flow plus an
+    upward through-flow of 0.05 (inflow at the bottom wall); `steps` accepted
+    steps, device-timed on the instance's stream."""
+    import torch
+    from mantlepar_b200 import synthetic as sy
+    from mantlepar_b200.preheat import Preheat, PreheatConfig
+    w = sy.Workload(nx=nx or WORKLOAD["nx"], ny=ny or WORKLOAD["ny"])
+    vs, _ = sy.face_velocity(w)
+    vs = vs.copy()
+    vs[:w.nx * (w.ny + 1)] -= 0.05
+    H, Cc = sy.initial_state(w)
+    p = Preheat(w, PreheatConfig(end=1e9, max_steps=1 << 40, dt_initial=1e-4, dt_max=1e-4, cfl=0.5,
+                                 diffusivity=1e-4, thermal_type=(1, 1, 0, 0), thermal_value=(0.9, 0.2, 0.0, 0.0)),
+                stream=stream.cuda_stream)
+    p.set_velocity(vs)
+    p.set_state(H, Cc)
+    _, limit, _ = p.begin()
+    p.advance(3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    code, rows = p.advance(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    p.close()
+    ms_step = ms / steps
+    return {"value": w.cells * steps / (ms * 1e-3), "unit": "cell-updates/s", "steps": steps,
+            "ms_per_step": ms_step, "status": code, "accepted": len(rows),
+            "max_balance_error": max(abs(r["balanceError"]) for r in rows),
+            "achieved_gbs": PREHEAT_BYTES_PER_CELL_STEP * w.cells / (ms_step * 1e-3) / 1e9,
+            "bytes_per_cell_step": PREHEAT_BYTES_PER_CELL_STEP,
+            "config": f"{w.nx}x{w.ny}, kappa=1e-4, wall temperatures bottom 0.9 / top 0.2, through-flow 0.05, "
+                      f"dt 1e-4 (rate limit {limit:.3g}), host round trip every 512 steps"}
+
+
 def run_forms(args, stream):
     """The mixed-precision large instance and the batched uneven meshes."""
     from mantlepar_b200 import synthetic as sy
@@ -290,6 +336,7 @@ def run_forms(args, stream):
         "features": "kappa=1e-4 with wall temperatures, lithostatic pressure, adiabatic source (alpha0=3e-5)",
         "retries": sum(r["retries"] for r in reps)}
     tp.close()
+    forms["preheat_1280x2560"] = preheat_form(max(args.form_steps, 50), stream)
     # Served: a seeded Poisson stream (200 req/s) of uneven solves, mixed
     # precision, submitted in real time; memory admission against a 64 GiB budget.
     if args.serve_requests > 0:
@@ -514,11 +561,18 @@ def main():
     ap.add_argument("--form-steps", type=int, default=5, help="timed steps of each extra form")
     ap.add_argument("--nx", type=int, default=WORKLOAD["nx"], help="cells in x (profiling of smaller cases)")
     ap.add_argument("--ny", type=int, default=WORKLOAD["ny"], help="cells in y")
+    ap.add_argument("--preheat-only", action="store_true",
+                    help="time only the legacy dry preheat form (profiling)")
     ap.add_argument("--decompose", action="store_true",
                     help="one mesh in row slabs across the ranks (strong scaling) instead of one mesh per rank")
     args = ap.parse_args()
     WORKLOAD.update(nx=args.nx, ny=args.ny)
     world, rank, local = dist_setup()
+    if args.preheat_only:
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps({"form": "preheat", **preheat_form(args.steps, torch.cuda.Stream(), args.nx, args.ny)}))
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
     elif args.decompose:

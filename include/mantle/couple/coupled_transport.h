@@ -1,6 +1,7 @@
 // C++ host layer of the coupled H/C transport over the mantlepar_b200 C ABI,
 // shaped like mantle::couple::AdvancePhaseCoupled and its stage RHS
-// (src/couple/evolve.h:17, evolve.cpp:279-384,428-519 of the reference).
+// (src/couple/evolve.h:17, evolve.cpp:279-384,428-519 of the reference), and
+// of the legacy dry preheat AdvanceLegacyPreheat (src/couple/preheat.h:26).
 //
 // The reference's Configuration / InitialState carry PETSc, MPI, MFEM and
 // YAML types; here they are plain structs holding the subset the transport
@@ -156,6 +157,36 @@ int RHS(const Configuration& configuration, const InitialState& state, const Edg
 // H, C, T, phi, time and acceptedSteps.
 int AdvancePhaseCoupled(const Configuration& configuration, InitialState& state, const FlowSupplier& flow,
                         std::vector<StepRecord>* history = nullptr);
+
+// Legacy dry preheat (src/couple/preheat.h:6-31): one row per accepted step
+// (and the initial state first), and the run's report.
+struct PreheatStep {
+    long step = 0;
+    double time = 0, dt = 0, courant = 0;
+    double integral = 0, minimum = 0, maximum = 0;
+    double boundaryFlux = 0, balanceError = 0;
+};
+struct PreheatReport {
+    double initialTime = 0, finalTime = 0, stepLimit = 0;
+    double initialIntegral = 0, finalIntegral = 0, boundaryIntegral = 0;
+    std::vector<PreheatStep> history;
+};
+
+// AdvanceLegacyPreheat (preheat.cpp:235-287): H_t + div(us H - kappa grad H)
+// = 0 with C fixed and `flow.solid` the frozen Stokes velocity (normal
+// components at the edge Gauss points; the Darcy part is unused, the flow
+// is dry). Forward Euler from state.time to configuration.time.end with the
+// time controls, thermalDiffusivity, the per-wall thermal conditions, the
+// enthalpy advection rule and the stabilizer of `configuration`; the phase
+// model and pressure give the final T and phi (Diagnostics). Returns 0 or an
+// mp_status; on failure H, time and acceptedSteps hold the last accepted
+// step and the phase fields are not refreshed.
+int AdvanceLegacyPreheat(const Configuration& configuration, InitialState& state, const EdgeVelocities& flow,
+                         PreheatReport& report);
+
+// preheat_history.csv (WritePreheatHistory, preheat.cpp:289-312) at `path`.
+int WritePreheatHistory(const std::string& path, const Configuration& configuration, const Mesh& mesh,
+                        const PreheatReport& report);
 
 // Number of edges of a mesh (AlongI edges first, then AlongJ).
 inline long EdgeCount(const Mesh& m) { return (long)m.nx * (m.ny + 1) + (long)(m.nx + 1) * m.ny; }

@@ -1,10 +1,12 @@
 // Coupled H/C transport host layer over the C ABI (include/mantle/couple/
 // coupled_transport.h): the time loop of the reference's Run
-// (src/couple/evolve.cpp:428-511) drives mp_transport_* on the GPU.
+// (src/couple/evolve.cpp:428-511) drives mp_transport_* on the GPU, and
+// AdvanceLegacyPreheat (src/couple/preheat.cpp:235-312) drives mp_preheat_*.
 #include "mantle/couple/coupled_transport.h"
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <limits>
 #include <stdexcept>
 #include <string>
@@ -265,6 +267,112 @@ int AdvancePhaseCoupled(const Configuration& c, InitialState& state, const FlowS
     st = read_back();
     if (st == MP_OK) state = cur;
     return finish(st);
+}
+
+int AdvanceLegacyPreheat(const Configuration& c, InitialState& state, const EdgeVelocities& flow,
+                         PreheatReport& report) {
+    const int control = control_of(c.time);
+    if (control < 0) return MP_ERR_ARG_OUTOFRANGE;
+    const Mesh mesh = state.mesh;
+    const size_t ncell = (size_t)mesh.nx * mesh.ny;
+    if (state.enthalpy.size() != ncell || state.composition.size() != ncell) return MP_ERR_ARG_SIZ;
+    if (flow.solid.size() != (size_t)EdgeCount(mesh) * 5) return MP_ERR_ARG_SIZ;
+    const auto& p = c.phase.parameters();
+    mp_preheat_opts o{};
+    o.material = mp_material{p.Tm0, p.Te0, p.nu, p.L, p.cp, p.Xe, p.rho, p.rhor, p.mus, p.mul, p.k0, p.g, p.alpha0};
+    o.pressure_model = c.pressureModel == PressureModel::Lithostatic ? MP_PRESSURE_LITHOSTATIC : MP_PRESSURE_CONSTANT;
+    o.pressure = c.pressureModel == PressureModel::Lithostatic ? c.surfaceY : c.pressure;
+    o.end = c.time.end;
+    o.max_steps = c.time.maximumSteps;
+    o.control = control;
+    o.dt_initial = c.time.initialStep;
+    o.dt_min = c.time.minimumStep;
+    o.dt_max = c.time.maximumStep;
+    o.cfl = c.time.cfl;
+    o.diffusivity = c.thermalDiffusivity;
+    for (int w = 0; w < 4; ++w) {
+        const auto& tc = c.boundary.temperature[w];
+        o.thermal_type[w] = tc.policy == ThermalPolicy::Temperature ? MP_THERMAL_TEMPERATURE
+                          : (tc.policy == ThermalPolicy::OutwardFlux ? MP_THERMAL_FLUX : MP_THERMAL_ZERO_FLUX);
+        o.thermal_value[w] = tc.value;
+    }
+    o.H_policy = policy(c.boundary.enthalpy.policy);
+    o.inflow_H = c.boundary.enthalpy.inflow;
+    o.lf_global = c.stabilizer.mode == LaxFriedrichsMode::Global ? 1 : 0;
+    o.lf_global_speed = c.stabilizer.globalSpeed;
+    const mp_mesh_desc d{mesh.nx, mesh.ny, mesh.x0, mesh.x1, mesh.y0, mesh.y1};
+    mp_preheat* h = nullptr;
+    mp_status st = mp_preheat_create(&d, &o, nullptr, &h);
+    if (st != MP_OK) return st;
+    auto finish = [&](mp_status s) { mp_preheat_destroy(h); return (int)s; };
+    st = mp_preheat_set_velocity(h, flow.solid.data());
+    if (st == MP_OK)
+        st = mp_preheat_set_state(h, state.enthalpy.data(), state.composition.data(), state.time, state.acceptedSteps);
+    if (st != MP_OK) return finish(st);
+    PreheatReport rep;
+    mp_preheat_step first{};
+    double limit = 0;
+    st = mp_preheat_begin(h, nullptr, &limit, &first);
+    if (st != MP_OK) return finish(st);
+    auto row = [](const mp_preheat_step& r) {
+        PreheatStep out;
+        out.step = (long)r.step; out.time = r.time; out.dt = r.dt; out.courant = r.courant;
+        out.integral = r.integral; out.minimum = r.minimum; out.maximum = r.maximum;
+        out.boundaryFlux = r.boundaryFlux; out.balanceError = r.balanceError;
+        return out;
+    };
+    rep.initialTime = rep.finalTime = state.time;
+    rep.stepLimit = limit;
+    rep.initialIntegral = rep.finalIntegral = first.integral;
+    rep.history.push_back(row(first));
+    std::vector<mp_preheat_step> chunk(1024);
+    for (;;) {
+        long long got = 0;
+        st = mp_preheat_advance(h, (long long)chunk.size(), chunk.data(), &got);
+        for (long long k = 0; k < got; ++k) {
+            rep.history.push_back(row(chunk[k]));
+            rep.finalIntegral = chunk[k].integral;
+            rep.boundaryIntegral += chunk[k].dt * chunk[k].boundaryFlux;
+        }
+        if (st != MP_OK || got < (long long)chunk.size()) break;
+    }
+    // The last accepted H, time and step count, on success and on failure.
+    std::vector<double> H(ncell);
+    double t = 0;
+    long long accepted = 0;
+    const mp_status rs = mp_preheat_get_state(h, H.data(), &t, &accepted);
+    if (rs != MP_OK) return finish(rs);
+    state.enthalpy.swap(H);
+    state.time = t;
+    state.acceptedSteps = (long)accepted;
+    rep.finalTime = t;
+    report = std::move(rep);
+    if (st != MP_OK) return finish(st);
+    std::vector<double> T(ncell), phi(ncell);
+    st = mp_preheat_diagnostics(h, T.data(), phi.data());
+    if (st != MP_OK) return finish(st);
+    state.temperature.swap(T);
+    state.porosity.swap(phi);
+    return finish(MP_OK);
+}
+
+int WritePreheatHistory(const std::string& path, const Configuration& c, const Mesh& mesh,
+                        const PreheatReport& report) {
+    const std::string tmp = path + ".tmp";
+    std::FILE* f = std::fopen(tmp.c_str(), "w");
+    if (!f) return MP_ERR_ARG_WRONG;
+    const auto& d = c.phase.derived();
+    const double area = (mesh.x1 - mesh.x0) * (mesh.y1 - mesh.y0);
+    const double year = 365.0 * 24 * 3600;
+    std::fprintf(f, "step,time,time_years,dt,dt_s,courant,H_integral,h_mean_J_kg,h_min_J_kg,h_max_J_kg,"
+                    "outward_H_flux,balance_error\n");
+    for (const auto& r : report.history)
+        std::fprintf(f, "%ld,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g\n", r.step, r.time,
+                     r.time * d.t0 / year, r.dt, r.dt * d.t0, r.courant, r.integral, r.integral / area * d.h0,
+                     r.minimum * d.h0, r.maximum * d.h0, r.boundaryFlux, r.balanceError);
+    const bool ok = std::fclose(f) == 0;
+    if (!ok || std::rename(tmp.c_str(), path.c_str()) != 0) return MP_ERR_ARG_WRONG;
+    return MP_OK;
 }
 
 }  // namespace mantle::couple

@@ -98,3 +98,55 @@ def test_maximum_steps_stops_with_not_converged(driver, tmp_path):
     w = sy.Workload(nx=20, ny=20)
     got = run(driver, tmp_path, w, 1.0, 0, 1e30, 2, max_steps=3)
     assert got["status"] == 91 and got["accepted"] == 3 and len(got["hist"]) == 3
+
+
+@pytest.fixture(scope="module")
+def preheat_driver(cuda_lib, tmp_path_factory):
+    from mantlepar_b200 import build
+    build.build_host()
+    exe = str(tmp_path_factory.mktemp("cpp") / "run_preheat")
+    cxx = os.environ.get("CXX") or shutil.which("g++")
+    pkg = os.path.join(ROOT, "mantlepar_b200")
+    subprocess.run([cxx, "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "run_preheat.cpp"), "-L", pkg,
+                    "-l:libmantle_b200_host.so", "-l:libmantlepar_b200.so", f"-Wl,-rpath,{pkg}", "-o", exe],
+                   check=True)
+    return exe
+
+
+@pytest.mark.parametrize("name", ["through_diffusion", "global_fixed"])
+def test_advance_legacy_preheat_matches_reference(preheat_driver, tmp_path, name):
+    """AdvanceLegacyPreheat and WritePreheatHistory (src/couple/preheat.cpp:
+    235-312) through the C++ layer: rows, final H, T and phi within 1e-12 of
+    the reference-backed golden run; the CSV holds the reference's columns."""
+    import preheat_cases as pc
+    from mantlepar_b200.preheat import HISTORY_COLUMNS
+    case = pc.CASES[name]
+    w = case.w
+    H, C = case.state()
+    head = np.array([w.nx, w.ny, w.x0, w.x1, w.y0, w.y1, case.end, case.control, case.dt_initial, case.dt_min,
+                     case.dt_max, case.cfl, case.max_steps, case.kappa, *case.thermal_type, *case.thermal_value,
+                     case.H_policy, case.inflow_H, case.lf_global, case.lf_global_speed, case.pressure_model,
+                     case.surface_y, 0.0, 0.0], float)
+    assert head.size == 30
+    inp, out, csv = str(tmp_path / "in.bin"), str(tmp_path / "out.bin"), str(tmp_path / "preheat_history.csv")
+    np.concatenate([head, H, C, np.ravel(case.velocity())]).tofile(inp)
+    subprocess.run([preheat_driver, inp, out, csv], check=True, capture_output=True, text=True, timeout=300)
+    d = np.fromfile(out)
+    n = w.cells
+    st, time, acc, nrows = d[:4]
+    assert int(st) == 0 and time == case.end
+    Hf, T, phi = d[4:4 + n], d[4 + n:4 + 2 * n], d[4 + 2 * n:4 + 3 * n]
+    rows = d[4 + 3 * n:4 + 3 * n + 9 * int(nrows)].reshape(-1, 9)
+    rep = d[4 + 3 * n + 9 * int(nrows):]
+    G = np.load(os.path.join(ROOT, "tests", "golden", "preheat_golden.npz"))
+    ref = G[f"{name}_rows"]
+    assert rows.shape == ref.shape and int(acc) == int(ref[-1][0])
+    assert np.array_equal(rows[:, 0], ref[:, 0])
+    assert np.max(np.abs(rows[:, 1:7] - ref[:, 1:7]) / np.maximum(np.abs(ref[:, 1:7]), 1e-300)) <= 1e-12
+    assert rel(Hf, G[f"{name}_H"]) <= 1e-12 and rel(T, G[f"{name}_T"]) <= 1e-12
+    assert rep[1] == case.end and abs(rep[4] - ref[-1][4]) <= 1e-12 * abs(ref[-1][4])
+    lines = open(csv).read().splitlines()
+    assert lines[0] == HISTORY_COLUMNS and len(lines) == 1 + ref.shape[0]
+    last = [float(x) for x in lines[-1].split(",")]
+    assert int(last[0]) == int(ref[-1][0]) and last[1] == rows[-1][1] and last[6] == rows[-1][4]
