@@ -180,6 +180,25 @@ mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_transport_opts*
                               mp_stream_t stream, mp_transport** out);
 void mp_transport_destroy(mp_transport* t);
 
+/* General quad meshes: the reference's perturbed-quadrilateral and stretched
+ * families (src/core/mesh.cpp:27-55, input mesh.family
+ * "perturbed_quadrilateral"), or any logically rectangular mesh of convex
+ * quads. xy holds the (nx+1)*(ny+1) vertices, x fastest, as (x, y) pairs;
+ * mesh gives nx, ny and the domain. Every cell gets its own reconstruction
+ * tables (built on the host at create, TensorStencilPoly::Initialize and
+ * SetTargetSmoothness per stencil, src/mlweno/tensorstencilpoly.cpp:146-231,
+ * 383-398) and every evaluation point its own geometry. FP64 only; cells
+ * failing the reference's quad check (src/core/quad_validation.h) ->
+ * MP_ERR_ARG_WRONG. All other mp_transport_* calls apply unchanged. */
+enum { MP_MESH_RECTANGULAR = 0, MP_MESH_PERTURBED = 1, MP_MESH_SINE_STRETCHED = 2 };
+mp_status mp_transport_create_quads(const mp_mesh_desc* mesh, const double* xy, const mp_transport_opts* opts,
+                                    mp_stream_t stream, mp_transport** out);
+/* Vertices of a reference mesh family (VertexAt, src/core/mesh.cpp:27-55):
+ * perturbation in [0, 0.25) of the spacing for MP_MESH_PERTURBED, keyed by
+ * seed (SplitMix64, as the reference). xy: (nx+1)*(ny+1) (x, y) pairs. */
+mp_status mp_mesh_vertices(const mp_mesh_desc* mesh, int family, double perturbation, unsigned long long seed,
+                           double* xy);
+
 /* Flow supplier output (stays on PETSc in a coupled run): normal solid and
  * Darcy velocity at every edge Gauss point, arrays of edges*5 doubles.
  * Replaces the samples of SampleInitialFlow (src/couple/flow_sampling.cpp:62-121). */

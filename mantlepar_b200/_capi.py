@@ -172,6 +172,8 @@ def lib() -> C.CDLL:
         "mp_transport_set_hooks": (i, [vp, vp, vp, vp]),
         "mp_transport_get_time": (i, [vp, dp, C.POINTER(C.c_int)]),
         "mp_batch_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
+        "mp_transport_create_quads": (i, [C.POINTER(MeshDesc), vp, C.POINTER(TransportOpts), vp, C.POINTER(vp)]),
+        "mp_mesh_vertices": (i, [C.POINTER(MeshDesc), i, d, C.c_ulonglong, vp]),
         "mp_preheat_create": (i, [C.POINTER(MeshDesc), C.POINTER(PreheatOpts), vp, C.POINTER(vp)]),
         "mp_preheat_destroy": (None, [vp]),
         "mp_preheat_set_velocity": (i, [vp, vp]),

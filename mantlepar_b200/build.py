@@ -27,7 +27,7 @@ LIB = os.path.join(HERE, "libmantlepar_b200.so")
 HOST_LIB = os.path.join(HERE, "libmantle_b200_host.so")
 HOST_SOURCES = [os.path.join(HERE, "host", "eutectic_model.cpp"), os.path.join(HERE, "host", "coupled_transport.cpp")]
 
-SOURCES = ["phase_api.cu", "transport.cu", "tables.cpp", "mp_noalloc.cu", "batch.cu", "serve.cpp", "preheat.cu"]
+SOURCES = ["phase_api.cu", "transport.cu", "tables.cpp", "mp_noalloc.cu", "batch.cu", "serve.cpp", "preheat.cu", "quad_tables.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
          "-I", os.path.join(ROOT, "include")]

@@ -1,0 +1,569 @@
+// Transport stage kernels of a general (logically rectangular) quad mesh:
+// perturbed-quadrilateral and stretched meshes, where every cell has its own
+// stencil geometry (src/core/mesh.cpp:27-55; src/mlweno/reconstruction.cpp:
+// 109-210). Same stage as the uniform kernels (src/couple/evolve.cpp:279-384),
+// with
+//   * per-cell candidate matrices and smoothness forms read from HBM
+//     (quad_tables.hpp) instead of one table set in the kernel parameters;
+//   * every evaluation point mapped from the cell's corners (bilinear map,
+//     edge interpolation, normal-line samples with per-edge spacing) into the
+//     cell's frame, and the limited polynomial evaluated as a full Q2 form;
+//   * physical edge lengths, normals and cell areas of each cell and edge.
+// The per-point physics (phase, porosity, velocities, fluxes, rate) is the
+// uniform kernels' own device code.
+#ifndef MP_QUAD_KERNELS_CUH
+#define MP_QUAD_KERNELS_CUH
+
+#include "common.hpp"
+#include "phase_math.cuh"
+#include "stage_device.cuh"
+#include "stage_kernels.cuh"
+
+namespace mp {
+namespace {
+
+// Device pointers of a QuadTables (SoA per cell; spacing per edge and point)
+// and the mesh-wide Gauss rule and derivative weights.
+struct QuadDev {
+    const double* xy;
+    const double* G0;
+    const double* S9;
+    const double* T4;
+    const double* S4;
+    const double* geo;
+    const double* sp;
+    double gq[5], gw[5];
+    double dif_c_int[4], dif_c_bnd[5];
+};
+
+// Adiabatic-source inputs and per-cell outputs (null when alpha0 = 0).
+struct SourcePtrs {
+    const double* cvs_y = nullptr;
+    const double* cud_y = nullptr;
+    double* srcH = nullptr;
+    double* srcR = nullptr;
+    double* srcS = nullptr;
+};
+
+
+struct P2 {
+    double x, y;
+};
+
+__device__ __forceinline__ P2 vtx(const QuadDev& q, int nx, int I, int J) {
+    const size_t k = (size_t)J * (nx + 1) + I;
+    return P2{__ldg(q.xy + 2 * k), __ldg(q.xy + 2 * k + 1)};
+}
+// integral.cpp:91-121: edge interpolation, bilinear map, Jacobian on [-1,1]^2.
+__device__ __forceinline__ P2 lerp_edge(double r, P2 a, P2 b) {
+    const double s = 0.5 * (1.0 - r), t = 0.5 * (1.0 + r);
+    return P2{s * a.x + t * b.x, s * a.y + t * b.y};
+}
+__device__ __forceinline__ P2 bilinear(double rx, double ry, const P2* c) {
+    return lerp_edge(ry, lerp_edge(rx, c[0], c[1]), lerp_edge(rx, c[3], c[2]));
+}
+__device__ __forceinline__ double jacobian(double rx, double ry, const P2* c) {
+    const double s = 0.5 * (1.0 + rx), t = 0.5 * (1.0 + ry);
+    const double xi_x = 0.5 * ((1.0 - t) * (c[1].x - c[0].x) + t * (c[2].x - c[3].x));
+    const double xi_y = 0.5 * ((1.0 - t) * (c[1].y - c[0].y) + t * (c[2].y - c[3].y));
+    const double et_x = 0.5 * ((1.0 - s) * (c[3].x - c[0].x) + s * (c[2].x - c[1].x));
+    const double et_y = 0.5 * ((1.0 - s) * (c[3].y - c[0].y) + s * (c[2].y - c[1].y));
+    return xi_x * et_y - xi_y * et_x;
+}
+// integral.cpp:62-89: length and unit normal (dy, -dx)/length of a -> b.
+__device__ __forceinline__ void edge_geometry(P2 a, P2 b, double& len, P2& n) {
+    const double dx = b.x - a.x, dy = b.y - a.y;
+    const double scale = fmax(fabs(dx), fabs(dy));
+    const double ux = dx / scale, uy = dy / scale;
+    const double norm = sqrt(ux * ux + uy * uy);
+    len = scale * norm;
+    n = P2{uy / norm, -ux / norm};
+}
+// Full Q2 form, monomial m = j*3 + i of xi^i eta^j.
+__device__ __forceinline__ double q2v(const double* D, double x, double y) {
+    const double r0 = D[0] + x * (D[1] + x * D[2]);
+    const double r1 = D[3] + x * (D[4] + x * D[5]);
+    const double r2 = D[6] + x * (D[7] + x * D[8]);
+    return r0 + y * (r1 + y * r2);
+}
+
+// The cell's frame: centre, 1/h, and corners.
+struct CellFrame {
+    double cx, cy, inv_h, area;
+    P2 c[4];
+};
+__device__ __forceinline__ CellFrame cell_frame(const QuadDev& q, int nx, size_t N, long long cell) {
+    const int i = (int)(cell % nx), j = (int)(cell / nx);
+    CellFrame f;
+    f.cx = __ldg(q.geo + cell);
+    f.cy = __ldg(q.geo + N + cell);
+    f.inv_h = 1.0 / __ldg(q.geo + 2 * N + cell);
+    f.area = __ldg(q.geo + 3 * N + cell);
+    f.c[0] = vtx(q, nx, i, j); f.c[1] = vtx(q, nx, i + 1, j);
+    f.c[2] = vtx(q, nx, i + 1, j + 1); f.c[3] = vtx(q, nx, i, j + 1);
+    return f;
+}
+
+// Edge e of cell (i, j) in counter-clockwise order (0 bottom, 1 right, 2 top,
+// 3 left): its mesh edge id, whether it is a wall, and whether the cell's
+// point order runs against the canonical one.
+__device__ __forceinline__ void cell_edge(int nx, int ny, int i, int j, int e, long long& id, bool& wall, bool& rev) {
+    const long long nI = (long long)nx * (ny + 1);
+    if (e == 0) { id = (long long)j * nx + i; wall = j == 0; rev = false; }
+    else if (e == 1) { id = nI + (long long)j * (nx + 1) + i + 1; wall = i == nx - 1; rev = false; }
+    else if (e == 2) { id = (long long)(j + 1) * nx + i; wall = j == ny - 1; rev = true; }
+    else { id = nI + (long long)j * (nx + 1) + i; wall = i == 0; rev = true; }
+}
+
+// Visit every normal-line diffusion sample on this cell's side of its four
+// edges (diffusiveflux.cpp:255-334, 4 samples; interior edges 2 on each side
+// at offsets -1.5, -0.5 spacings from the edge, wall edges 4 at -4..-1).
+template <class F>
+__device__ __forceinline__ void visit_samples(const QuadDev& q, int nx, int ny, int i, int j, const CellFrame& f, F&& visit) {
+    for (int e = 0; e < 4; ++e) {
+        long long id;
+        bool wall, rev;
+        cell_edge(nx, ny, i, j, e, id, wall, rev);
+        const P2 a = f.c[e], b = f.c[(e + 1) & 3];
+        double len;
+        P2 n;
+        edge_geometry(a, b, len, n);
+        for (int k = 0; k < kNQ; ++k) {
+            const P2 p = lerp_edge(q.gq[k], a, b);
+            const double sp = __ldg(q.sp + id * kNQ + (rev ? kNQ - 1 - k : k));
+            const int ns = wall ? 4 : 2;
+            for (int s = 0; s < ns; ++s) {
+                const double d = (wall ? (double)(s - 4) : (double)s - 1.5) * sp;
+                visit(P2{p.x + d * n.x, p.y + d * n.y});
+            }
+        }
+    }
+}
+
+// Folded smoothness row offsets: entry (r, c >= r) of an n x n form.
+__device__ __forceinline__ int fold_at(int n, int r, int c) { return r * n - (r * (r - 1)) / 2 + (c - r); }
+
+// One field's deviation polynomial D from the 3x3 neighbourhood with the
+// cell's own tables (same candidate set, weights and clipping as
+// reconstruct() of the uniform path).
+__device__ __forceinline__ int reconstruct_quad(const QuadDev& q, size_t N, long long cell, int ci, int cj,
+                                                double eA, const double (&u)[3][3], double (&D)[9]) {
+    double d[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) d[a][b] = u[a][b] - u[1][1];
+    const int offi[4] = {0, 0, -1, -1}, offj[4] = {-1, 0, -1, 0};
+    bool on[5];
+    on[0] = (ci == 1 && cj == 1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        on[k + 1] = !((offi[k] == 0 && ci == 2) || (offi[k] == -1 && ci == 0) || (offj[k] == 0 && cj == 2) ||
+                      (offj[k] == -1 && cj == 0));
+    double sig[5];
+    int st = 0;
+    if (on[0]) {
+        double diff[8];
+#pragma unroll
+        for (int c = 1; c < 9; ++c) diff[c - 1] = d[c / 3][c % 3] - d[0][0];
+        auto SF = [&](int k) { return __ldg(q.S9 + (size_t)k * N + cell); };
+        auto S = [&](int r, int c) { const double v = SF(fold_at(8, r, c)); return r == c ? v : 0.5 * v; };
+        sig[0] = smoothness<double, 8>(SF, S, diff);
+        if (sig[0] < 0.0) st = MP_ERR_FP;
+    } else {
+        sig[0] = 0;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!on[k + 1]) { sig[k + 1] = 0; continue; }
+        const int oi = offi[k], oj = offj[k];
+        const double a0 = d[1 + oj][1 + oi];
+        double diff[3];
+#pragma unroll
+        for (int c = 1; c < 4; ++c) diff[c - 1] = d[1 + oj + c / 2][1 + oi + c % 2] - a0;
+        auto SF = [&](int m) { return __ldg(q.S4 + (size_t)(k * 6 + m) * N + cell); };
+        auto S = [&](int r, int c) { const double v = SF(fold_at(3, r, c)); return r == c ? v : 0.5 * v; };
+        sig[k + 1] = smoothness<double, 3>(SF, S, diff);
+        if (sig[k + 1] < 0.0) st = MP_ERR_FP;
+    }
+    double w[5];
+    weights<double>(sig, on, eA, w);
+    if (!isfinite(w[0] + w[1] + w[2] + w[3] + w[4])) st = MP_ERR_FP;
+#pragma unroll
+    for (int m = 0; m < 9; ++m) D[m] = 0;
+    if (on[0]) {
+        double diff[8];
+#pragma unroll
+        for (int c = 1; c < 9; ++c) diff[c - 1] = d[c / 3][c % 3] - d[0][0];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) {
+            double v = m == 0 ? d[0][0] : 0.0;
+#pragma unroll
+            for (int c = 1; c < 9; ++c) v += diff[c - 1] * __ldg(q.G0 + (size_t)((c - 1) * 9 + m) * N + cell);
+            D[m] = w[0] * v;
+        }
+    }
+    const int slot[4] = {0, 1, 3, 4};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!on[k + 1]) continue;
+        const int oi = offi[k], oj = offj[k];
+        const double a0 = d[1 + oj][1 + oi];
+        double diff[3];
+#pragma unroll
+        for (int c = 1; c < 4; ++c) diff[c - 1] = d[1 + oj + c / 2][1 + oi + c % 2] - a0;
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) {
+            double v = mm == 0 ? a0 : 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v += diff[c] * __ldg(q.T4 + (size_t)(k * 12 + c * 4 + mm) * N + cell);
+            D[slot[mm]] += w[k + 1] * v;
+        }
+    }
+    return st;
+}
+
+// ------------------------------------------------------------------ kernels
+
+// Reconstruction, limiter over the cell's own limiter points
+// (state_reconstruction.cpp:136-192), limited coefficients.
+__global__ void __launch_bounds__(128) quad_recon_kernel(int nx, int ny, const double* __restrict__ H,
+                                                         const double* __restrict__ C, double* __restrict__ rec,
+                                                         unsigned char* __restrict__ flags, unsigned long long* status,
+                                                         double* theta, Physics ph, QuadDev q) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= nx || j >= ny) return;
+    const long long cell = (long long)j * nx + i;
+    const size_t N = (size_t)nx * ny;
+    const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
+    const CellFrame f = cell_frame(q, nx, N, cell);
+    const double eA = 1e-2 * f.area;
+    double DH[9], DC[9];
+    double mH = 0, mC = 0, loH = 0, hiH = 0, loC = 0, hiC = 0;
+    int st = 0, st_lim = 0;
+#pragma unroll
+    for (int fi = 0; fi < 2; ++fi) {
+        const double* F = fi ? C : H;
+        double u[3][3];
+#pragma unroll
+        for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+            for (int di = 0; di < 3; ++di) {
+                const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
+                u[dj][di] = __ldg(F + (size_t)jj * nx + ii);
+            }
+        double lo = u[1][1], hi = u[1][1];
+#pragma unroll
+        for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+            for (int di = 0; di < 3; ++di) { lo = fmin(lo, u[dj][di]); hi = fmax(hi, u[dj][di]); }
+        const int s1 = reconstruct_quad(q, N, cell, ci, cj, eA, u, fi ? DC : DH);
+        st = st ? st : s1;
+        if (fi == 0) { mH = u[1][1]; loH = fmax(0.0, lo); hiH = hi; }
+        else { mC = u[1][1]; loC = fmax(0.0, lo); hiC = fmin(ph.k.Xe, hi); }
+    }
+    if (!(isfinite(mH) && mH >= 0.0 && isfinite(mC) && mC >= 0.0 && mC <= ph.k.Xe)) st_lim = E_OUTOFRANGE;
+    double hmx = -INFINITY, hmn = INFINITY, cmx = -INFINITY, cmn = INFINITY;
+    bool bad = false;
+    auto visit = [&](P2 p) {
+        const double x = (p.x - f.cx) * f.inv_h, y = (p.y - f.cy) * f.inv_h;
+        const double vh = q2v(DH, x, y), vc = q2v(DC, x, y);
+        bad = bad || !isfinite(vh) || !isfinite(vc);
+        hmx = fmax(hmx, vh); hmn = fmin(hmn, vh);
+        cmx = fmax(cmx, vc); cmn = fmin(cmn, vc);
+    };
+    // Limiter points (state_reconstruction.cpp:152-168): centre, 5x5 Gauss
+    // points, 5 points per edge, the normal-line samples on this side.
+    visit(bilinear(0.0, 0.0, f.c));
+    for (int a = 0; a < kNQ; ++a)
+        for (int b = 0; b < kNQ; ++b) visit(bilinear(q.gq[a], q.gq[b], f.c));
+    for (int e = 0; e < 4; ++e)
+        for (int k = 0; k < kNQ; ++k) visit(lerp_edge(q.gq[k], f.c[e], f.c[(e + 1) & 3]));
+    visit_samples(q, nx, ny, i, j, f, visit);
+    if (bad) st_lim = st_lim ? st_lim : E_FP;
+    const double thH = theta_of(mH, loH, hiH, hmx, hmn);
+    const double thC = theta_of(mC, loC, hiC, cmx, cmn);
+    if (theta) { theta[cell] = thH; theta[N + cell] = thC; }
+    // Diffusion-sample admissibility as the uniform path: provably safe when
+    // the largest neighbour average is below the liquidus at the lowest
+    // eutectic temperature over the cell's height range.
+    double ylo = f.c[0].y, yhi = f.c[0].y;
+    for (int k = 1; k < 4; ++k) { ylo = fmin(ylo, f.c[k].y); yhi = fmax(yhi, f.c[k].y); }
+    const double tep = ph.litho ? fmin(tep_at(ph, ylo), tep_at(ph, yhi)) : ph.Tep;
+    const double Hliq = tep + (1.0 - hiC / ph.k.Xe) + ph.k.LD;
+    const bool safe = tep >= 0.0 && hiH + 1e-12 * (1.0 + fabs(hiH)) < Hliq;
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+        rec[(size_t)m * N + cell] = DH[m] * thH;
+        rec[(size_t)(m + 9) * N + cell] = DC[m] * thC;
+    }
+    flags[cell] = safe ? 0 : FLAG_CHECK;
+    if (st) record_error(status, PART_UPDATE, cell, st);
+    if (st_lim) record_error(status, PART_LIMIT, cell, st_lim);
+}
+
+// 5x5 cell quadrature of T and phi on the bilinear map, wet flag, adiabatic
+// source, and the exact check of the diffusion samples when flagged.
+__global__ void __launch_bounds__(128) quad_cellphase_kernel(int nx, int ny, const double* __restrict__ H,
+                                                             const double* __restrict__ C, const double* __restrict__ rec,
+                                                             unsigned char* __restrict__ flags, double* __restrict__ T,
+                                                             double* __restrict__ phi, unsigned long long* status,
+                                                             Physics ph, QuadDev q, SourcePtrs src) {
+    const long long N = (long long)nx * ny;
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= N) return;
+    const int i = (int)(cell % nx), j = (int)(cell / nx);
+    const CellFrame f = cell_frame(q, nx, (size_t)N, cell);
+    const double mH = __ldg(H + cell), mC = __ldg(C + cell);
+    double DH[9], DC[9];
+    load_rec(rec, (size_t)N, cell, DH, DC);
+    int st_por = 0, st_cell = 0, st_face = 0;
+    double Tsum = 0.0, Psum = 0.0, Ssum = 0.0, Rsum = 0.0, Wsum = 0.0;
+    bool wet = false;
+    for (int b = 0; b < kNQ; ++b)
+        for (int a = 0; a < kNQ; ++a) {
+            const P2 p = bilinear(q.gq[a], q.gq[b], f.c);
+            const double wj = q.gw[a] * q.gw[b] * jacobian(q.gq[a], q.gq[b], f.c);
+            const double x = (p.x - f.cx) * f.inv_h, y = (p.y - f.cy) * f.inv_h;
+            const double tep = ph.litho ? tep_at(ph, p.y) : ph.Tep;
+            PhaseLean pl;
+            const int s = phase_stage_lean(ph.sk, mH + q2v(DH, x, y), mC + q2v(DC, x, y), tep, pl);
+            if (s) { st_por = st_por ? st_por : s; continue; }
+            if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_cell = st_cell ? st_cell : E_OUTOFRANGE;
+            const double w = wj / f.area;
+            Tsum += w * pl.T;
+            Psum += w * pl.phil;
+            wet = wet || pl.phil > 0.0;
+            if (ph.source) {
+                const long long at = cell * (kNQ * kNQ) + b * kNQ + a;
+                const double factor = pl.phil == 0.0 ? 0.0 : (ph.theta == 0.0 ? pl.phil : pow(pl.phil, 1.0 + ph.theta));
+                const double vy = __ldg(src.cvs_y + at) + factor * __ldg(src.cud_y + at);
+                const double s_ = -ph.cooling * pl.T * vy;
+                Ssum += w * s_;
+                Rsum += w * ph.cooling * fabs(vy);
+                Wsum += wj * s_;
+            }
+        }
+    const unsigned char fl = flags[cell];
+    if (fl & FLAG_CHECK) {
+        visit_samples(q, nx, ny, i, j, f, [&](P2 p) {
+            const double x = (p.x - f.cx) * f.inv_h, y = (p.y - f.cy) * f.inv_h;
+            const double tep = ph.litho ? tep_at(ph, p.y) : ph.Tep;
+            PhaseLean pl;
+            const int s = phase_stage_lean(ph.sk, mH + q2v(DH, x, y), mC + q2v(DC, x, y), tep, pl);
+            if (s) { st_face = st_face ? st_face : s; return; }
+            if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_face = st_face ? st_face : E_OUTOFRANGE;
+        });
+    }
+    if (st_por) record_error(status, PART_POROSITY, cell, st_por);
+    if (st_face) record_error(status, PART_FACES, cell, st_face);
+    if (st_cell) record_error(status, PART_CELLS, cell, st_cell);
+    flags[cell] = (unsigned char)((fl & FLAG_CHECK) | (wet ? FLAG_WET : 0));
+    T[cell] = Tsum;
+    phi[cell] = Psum;
+    if (ph.source) { src.srcH[cell] = Ssum; src.srcR[cell] = Rsum; src.srcS[cell] = Wsum; }
+}
+
+// Left/right cells and oriented vertices of edge e (evolve.cpp:230-251).
+struct QuadEdge {
+    bool horizontal, boundary, reverse;
+    long long L, R;
+    int wall;
+    P2 a, b;
+};
+__device__ __forceinline__ QuadEdge quad_edge(const QuadDev& q, int nx, int ny, long long e) {
+    const long long nI = (long long)nx * (ny + 1);
+    QuadEdge g;
+    g.R = -1;
+    g.wall = -1;
+    P2 v0, v1;
+    if (e < nI) {
+        const int i = (int)(e % nx), j = (int)(e / nx);
+        g.horizontal = true;
+        g.boundary = j == 0 || j == ny;
+        g.reverse = j == ny;
+        g.L = g.reverse ? (long long)(j - 1) * nx + i : (long long)j * nx + i;
+        if (!g.boundary) g.R = (long long)(j - 1) * nx + i;
+        else g.wall = j == 0 ? 0 : 1;
+        v0 = vtx(q, nx, i, j); v1 = vtx(q, nx, i + 1, j);
+    } else {
+        const long long k = e - nI;
+        const int i = (int)(k % (nx + 1)), j = (int)(k / (nx + 1));
+        g.horizontal = false;
+        g.boundary = i == 0 || i == nx;
+        g.reverse = i == 0;
+        g.L = g.reverse ? (long long)j * nx : (long long)j * nx + (i - 1);
+        if (!g.boundary) g.R = (long long)j * nx + i;
+        else g.wall = i == 0 ? 2 : 3;
+        v0 = vtx(q, nx, i, j); v1 = vtx(q, nx, i, j + 1);
+    }
+    g.a = g.reverse ? v1 : v0;
+    g.b = g.reverse ? v0 : v1;
+    return g;
+}
+
+struct Side {
+    double cx, cy, inv_h, mH, mC;
+    double DH[9], DC[9];
+};
+__device__ __forceinline__ void load_side(const QuadDev& q, size_t N, const double* H, const double* C,
+                                          const double* rec, long long cell, Side& s) {
+    s.cx = __ldg(q.geo + cell);
+    s.cy = __ldg(q.geo + N + cell);
+    s.inv_h = 1.0 / __ldg(q.geo + 2 * N + cell);
+    s.mH = __ldg(H + cell);
+    s.mC = __ldg(C + cell);
+    load_rec(rec, N, cell, s.DH, s.DC);
+}
+__device__ __forceinline__ void side_values(const Side& s, P2 p, double& h, double& c) {
+    const double x = (p.x - s.cx) * s.inv_h, y = (p.y - s.cy) * s.inv_h;
+    h = s.mH + q2v(s.DH, x, y);
+    c = s.mC + q2v(s.DC, x, y);
+}
+
+// Face fluxes, edge porosity and rate of one edge at its 5 Gauss points.
+__global__ void __launch_bounds__(128) quad_face_kernel(int nx, int ny, const double* __restrict__ H,
+                                                        const double* __restrict__ C, const double* __restrict__ rec,
+                                                        const unsigned char* __restrict__ flags,
+                                                        const double* __restrict__ vsn, const double* __restrict__ udn,
+                                                        double* __restrict__ face, unsigned long long* status,
+                                                        Physics ph, QuadDev q) {
+    const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nE) return;
+    const size_t N = (size_t)nx * ny;
+    const QuadEdge g = quad_edge(q, nx, ny, e);
+    double len;
+    P2 nrm;
+    edge_geometry(g.a, g.b, len, nrm);
+    Side sl, sr;
+    load_side(q, N, H, C, rec, g.L, sl);
+    if (!g.boundary) load_side(q, N, H, C, rec, g.R, sr);
+    const bool wetL = (flags[g.L] & FLAG_WET) != 0, wetR = g.boundary ? true : (flags[g.R] & FLAG_WET) != 0;
+    const double sgn = g.reverse ? -1.0 : 1.0;
+    double fluxH = 0.0, fluxC = 0.0, fluxMix = 0.0, rate = 0.0;
+    int st = 0;
+    for (int k = 0; k < kNQ; ++k) {
+        const int cq = g.reverse ? kNQ - 1 - k : k;
+        const P2 p = lerp_edge(q.gq[k], g.a, g.b);
+        const double vs = sgn * __ldg(vsn + e * kNQ + cq);
+        const double ud = sgn * __ldg(udn + e * kNQ + cq);
+        const double tep = ph.litho ? tep_at(ph, p.y) : ph.Tep;
+        double hL, cL, hR, cR;
+        PhaseLean A, B;
+        side_values(sl, p, hL, cL);
+        int s = phase_stage(ph.sk, hL, cL, tep, A);
+        if (!s && !(A.T >= 0.0 && A.phil < 1.0)) s = E_OUTOFRANGE;
+        if (g.boundary) { B = A; hR = hL; cR = cL; }
+        else {
+            side_values(sr, p, hR, cR);
+            int s2 = phase_stage(ph.sk, hR, cR, tep, B);
+            if (!s2 && !(B.T >= 0.0 && B.phil < 1.0)) s2 = E_OUTOFRANGE;
+            s = s ? s : s2;
+        }
+        if (s) { st = st ? st : s; continue; }
+        const PointFlux pf = face_point(ph, A, B, cL, cR, wetL, wetR, g.boundary, vs, ud, tep, ph.k.LD, st);
+        const double w = 0.5 * len * q.gw[k];
+        fluxH += w * pf.fh;
+        fluxC += w * pf.fc;
+        fluxMix += w * pf.vn;
+        rate += w * pf.speed;
+    }
+    if (st) record_error(status, PART_FACES, g.L, st);
+    face[e] = fluxH;
+    face[nE + e] = fluxC;
+    face[2 * nE + e] = rate;
+    face[3 * nE + e] = fluxMix;
+}
+
+// Diffusive H flux and rate of one edge (diffusiveflux.cpp:105-200 through
+// evolve.cpp:330-347): temperatures of the limited states at the normal-line
+// samples, spacing per edge point.
+__global__ void __launch_bounds__(128) quad_diffusion_kernel(int nx, int ny, const double* __restrict__ H,
+                                                             const double* __restrict__ C,
+                                                             const double* __restrict__ rec, double* __restrict__ face,
+                                                             unsigned long long* status, Physics ph, QuadDev q) {
+    const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nE) return;
+    const size_t N = (size_t)nx * ny;
+    const QuadEdge g = quad_edge(q, nx, ny, e);
+    const int type = g.boundary ? ph.wall_type[g.wall] : 1;
+    if (g.boundary && type == 0) return;
+    double len;
+    P2 nrm;
+    edge_geometry(g.a, g.b, len, nrm);
+    Side sl, sr;
+    if (type == 1) {
+        load_side(q, N, H, C, rec, g.L, sl);
+        if (!g.boundary) load_side(q, N, H, C, rec, g.R, sr);
+    }
+    double integral = 0.0, rate = face[2 * nE + e];
+    const double kappa = ph.kappa;
+    int st = 0;
+    for (int k = 0; k < kNQ; ++k) {
+        const double w = len * q.gw[k] / 2;
+        if (g.boundary && type == 2) { integral += w * ph.wall_value[g.wall]; continue; }
+        const int cq = g.reverse ? kNQ - 1 - k : k;
+        const P2 p = lerp_edge(q.gq[k], g.a, g.b);
+        const double sp = __ldg(q.sp + e * kNQ + cq);
+        const int count = g.boundary ? 5 : 4;
+        double v[5];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const bool left = g.boundary || s < 2;
+            const double d = (g.boundary ? (double)(s - 4) : (double)s - 1.5) * sp;
+            const P2 x = P2{p.x + d * nrm.x, p.y + d * nrm.y};
+            double h, c;
+            side_values(left ? sl : sr, x, h, c);
+            const double tep = ph.litho ? tep_at(ph, x.y) : ph.Tep;
+            PhaseLean pl;
+            int s1 = phase_stage_lean(ph.sk, h, c, tep, pl);
+            if (!s1 && !(pl.T >= 0.0 && pl.phil < 1.0)) s1 = E_OUTOFRANGE;
+            if (s1) st = st ? st : s1;
+            v[s] = s1 ? 0.0 : pl.T;
+        }
+        v[4] = g.boundary ? ph.wall_value[g.wall] : 0.0;
+        const double* c = g.boundary ? q.dif_c_bnd : q.dif_c_int;
+        const double last = v[count - 1];
+        double grad = 0.0, clast = 0.0;
+        for (int s = 0; s + 1 < count; ++s) { grad += c[s] * (v[s] - last); clast -= c[s]; }
+        grad /= sp;
+        if (!isfinite(grad)) st = st ? st : E_FP;
+        integral -= w * kappa * grad;
+        const double scale = -w * kappa / sp;
+        for (int s = 0; s < count; ++s) {
+            if (g.boundary && s + 1 == count) continue;
+            rate += fabs(scale * (s + 1 == count ? clast : c[s]));
+        }
+    }
+    if (st) record_error(status, PART_FACES, g.L, st);
+    face[e] += integral;
+    face[2 * nE + e] = rate;
+}
+
+// Reconstruction + limiter, cell phase, faces (+ diffusion) of state (H, C)
+// on a general quad mesh; the accumulation is the shared sum kernel.
+void launch_quad_stage(const QuadDev& q, int nx, int ny, const Physics& ph, const double* H, const double* C,
+                       double* rec, unsigned char* flags, double* T, double* phi, const double* vsn, const double* udn,
+                       double* face, unsigned long long* status, double* theta, const SourcePtrs& src,
+                       cudaStream_t s) {
+    const long long N = (long long)nx * ny;
+    const long long NE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
+    dim3 blk(32, 4), grd((nx + 31) / 32, (ny + 3) / 4);
+    quad_recon_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, flags, status, theta, ph, q);
+    quad_cellphase_kernel<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, flags, T, phi, status, ph, q,
+                                                                      src);
+    quad_face_kernel<<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, flags, vsn, udn, face, status,
+                                                                  ph, q);
+    count_launch(3);
+    if (ph.diffusion) {
+        quad_diffusion_kernel<<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, face, status, ph, q);
+        count_launch();
+    }
+}
+
+}  // namespace
+}  // namespace mp
+
+#endif

@@ -467,6 +467,73 @@ __device__ __forceinline__ int side_phase(const Physics& ph, const SideLine& s, 
     return st;
 }
 
+// One edge Gauss point of the face fluxes from both sides' phase states:
+// edge porosity, transport velocities, Lax-Friedrichs fluxes or the boundary
+// policy (evolve.cpp:36-52,292-329; initial_flow.cpp:94-117), and the point's
+// CFL rate term before its quadrature weight; st keeps the first failure.
+// Used by the general-quad face kernel. face_edge below carries the same
+// statements inline: called from there, this function changes the uniform
+// face kernel's register allocation (12 more bytes of spills, 2% slower).
+struct PointFlux {
+    double fh, fc, vn, speed;   // speed: (aC + aH + 2 |vs|) * sens
+};
+__device__ __forceinline__ PointFlux face_point(const Physics& ph, const PhaseLean& A, const PhaseLean& B, double cL,
+                                                double cR, bool wetL, bool wetR, bool boundary, double vs, double ud,
+                                                double tep, double LD, int& st) {
+    // Edge porosity: harmonic mean of both sides, zero next to a dry cell
+    // (initial_flow.cpp:94-117). PhaseTransportVelocities (evolve.cpp:36-52)
+    // on normal components: bulk = ephi cl + (1 - ephi) cs, and the
+    // composition velocity adds cl/bulk times the Darcy flux. With
+    // S = phil_A + phil_B and Q = S bulk, ephi = 2 phil_A phil_B / S and
+    // cl/bulk = cl S / Q come from one division 1/(S Q) where it is in range.
+    const double cl = 0.5 * (A.cl + B.cl), cs = 0.5 * (A.cs + B.cs);
+    const double S = A.phil + B.phil;
+    double ephi = 0.0, clb = 0.0;   // clb = cl/bulk where bulk > 0, else 0
+    if (wetL && wetR && S > 0.0) {
+        const double P2 = 2.0 * A.phil * B.phil;
+        const double Q = P2 * (cl - cs) + cs * S;
+        const double SQ = S * Q;
+        if (SQ > 1e-290 && SQ < 1e290) {
+            const double x = 1.0 / SQ;
+            ephi = P2 * (Q * x);
+            clb = cl * (S * (S * x));
+        } else {
+            ephi = P2 / S;
+            const double bulk = ephi * cl + (1.0 - ephi) * cs;
+            clb = bulk > 0.0 ? cl / bulk : 0.0;
+        }
+    }
+    const double factor = ephi == 0.0 ? 0.0 : (ph.theta == 0.0 ? ephi : pow(ephi, 1.0 + ph.theta));
+    const double flux = factor * ud;
+    const double vn = vs + flux;
+    const double ve = vs + clb * flux;
+    const double aH = ph.lf_global ? ph.lf_speed : fabs(vn);
+    const double aC = ph.lf_global ? ph.lf_speed : fabs(ve);
+    if (ph.lf_global && !(aH + 1e-14 >= fabs(vn) && aC + 1e-14 >= fabs(ve))) st = st ? st : E_OUTOFRANGE;
+    double fh = 0.5 * (vn * (A.T + B.T) - aH * (B.T - A.T)) - LD * (1.0 - ephi) * vs;
+    double fc = 0.5 * (ve * (cL + cR) - aC * (cR - cL));
+    if (boundary) {
+        // EvaluateAdvectionBoundary (initialization.cpp:469-489) per field.
+        const int kh = (ph.Hpol == MP_BC_ZERO_FLUX || vn == 0.0) ? 2 : (vn < 0.0 ? 0 : 1);
+        const int kc = (ph.Cpol == MP_BC_ZERO_FLUX || ve == 0.0) ? 2 : (ve < 0.0 ? 0 : 1);
+        if ((kh == 0 && ph.Hpol != MP_BC_INFLOW_OUTFLOW) || (kc == 0 && ph.Cpol != MP_BC_INFLOW_OUTFLOW))
+            st = st ? st : E_OUTOFRANGE;
+        const double inC = kc == 0 ? ph.inflowC : cL;
+        double Tb = A.T;
+        if (kh == 0) {
+            PhaseLean pin;
+            const int s3 = phase_stage(ph.sk, ph.inflowH, inC, tep, pin);
+            if (s3) st = st ? st : s3;
+            Tb = pin.T;
+        }
+        fh = kh == 2 ? 0.0 : vn * Tb - LD * (1.0 - ephi) * vs;
+        fc = kc == 2 ? 0.0 : ve * (kc == 0 ? ph.inflowC : cL);
+    }
+    const double sens = 1.0 + fmax(fabs(A.dTdC), fabs(B.dTdC));
+    if (!isfinite(sens)) st = st ? st : E_FP;
+    return PointFlux{fh, fc, vn, (aC + aH + 2.0 * fabs(vs)) * sens};
+}
+
 // kExt: the lithostatic pressure is compiled in.
 template <class R, bool kExt = false>
 __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& ph, long long e) {
@@ -731,6 +798,8 @@ struct SumArgs {
     const double* srcH = nullptr;
     const double* srcR = nullptr;
     const double* srcS = nullptr;
+    // General quad meshes: the area of every cell (else `area` for all).
+    const double* cell_area = nullptr;
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -776,14 +845,14 @@ __device__ void block_reduce_write(Partial v, Partial* out) {
 
 // Per-cell accumulation + RK combination; folds the cell's contribution to
 // the stage reductions into v.
-// kSrc: the adiabatic source terms are added.
-template <bool kSrc = false>
+// kSrc: the adiabatic source terms are added. kArea: per-cell areas.
+template <bool kSrc = false, bool kArea = false>
 __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partial& v) {
     const int nx = a.nx, ny = a.ny;
     const long long nI = (long long)nx * (ny + 1);
     const long long nE = nI + (long long)(nx + 1) * ny;
     const int i = (int)(cell % (unsigned)nx), j = (int)(cell / (unsigned)nx);
-    const double A = a.area, invA = a.inv_area;
+    const double A = kArea ? __ldg(a.cell_area + cell) : a.area, invA = kArea ? 1.0 / A : a.inv_area;
     // Faces of this cell in the reference's id order: bottom, top, left, right,
     // each with the sign of its side (evolve.cpp:350-354).
     const long long eb = (long long)j * nx + i, et = (long long)(j + 1) * nx + i;
@@ -839,23 +908,24 @@ __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partia
 
 // The kSumPer cells of this thread in the sum block starting at first.
 // `first` counts from the start of the accumulated range [cbeg, cend).
-template <bool kSrc = false>
+template <bool kSrc = false, bool kArea = false>
 __device__ __forceinline__ Partial sum_cells(const SumArgs& a, long long first) {
     const long long end = a.cend >= 0 ? a.cend : (long long)a.nx * a.ny;
     Partial v = partial_identity();
 #pragma unroll
     for (int k = 0; k < kSumPer; ++k) {
         const long long c = a.cbeg + first + k * kRedBlock + threadIdx.x;
-        if (c < end) sum_cell<kSrc>(a, (unsigned)c, v);
+        if (c < end) sum_cell<kSrc, kArea>(a, (unsigned)c, v);
     }
     return v;
 }
 
 // U1 = U^n + dt*L^n over the kSumPer cells of this thread, with the
-// admissibility/integral partials of U1.
+// admissibility/integral partials of U1 (cell_area: per-cell areas, or null
+// for `area` everywhere).
 __device__ __forceinline__ Partial axpy_cells(long long n, const double* H0, const double* C0, const double* LH,
                                               const double* LC, double dt, double area, double* H1, double* C1,
-                                              long long first) {
+                                              long long first, const double* cell_area = nullptr) {
     Partial v = partial_identity();
 #pragma unroll
     for (int q = 0; q < kSumPer; ++q) {
@@ -864,7 +934,8 @@ __device__ __forceinline__ Partial axpy_cells(long long n, const double* H0, con
         const double h = __dadd_rn(H0[k], __dmul_rn(dt, LH[k]));
         const double c = __dadd_rn(C0[k], __dmul_rn(dt, LC[k]));
         H1[k] = h; C1[k] = c;
-        v.HI += h * area; v.CI += c * area;
+        const double A = cell_area ? __ldg(cell_area + k) : area;
+        v.HI += h * A; v.CI += c * A;
         v.Hmin = fmin(v.Hmin, h); v.Cmin = fmin(v.Cmin, c); v.Cmax = fmax(v.Cmax, c);
         v.nonfinite = fmax(v.nonfinite, (isfinite(h) && isfinite(c)) ? 0.0 : 1.0);
     }

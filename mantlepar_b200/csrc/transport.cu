@@ -17,6 +17,8 @@
 #include "stage_device.cuh"
 #include "stage_kernels.cuh"
 #include "tables.hpp"
+#include "quad_kernels.cuh"
+#include "quad_tables.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -99,17 +101,17 @@ __global__ void __launch_bounds__(128) diffusion_kernel(FaceArgs<R> a, Physics p
     if (k < nh + nv) diffusion_edge(b, ph, k < nh ? h0 + k : v0 + (k - nh));
 }
 
-template <bool kSrc>
+template <bool kSrc, bool kArea = false>
 __global__ void __launch_bounds__(kRedBlock) sum_kernel(SumArgs a) {
-    const Partial v = sum_cells<kSrc>(a, (long long)blockIdx.x * kSumCells);
+    const Partial v = sum_cells<kSrc, kArea>(a, (long long)blockIdx.x * kSumCells);
     block_reduce_write(v, a.partial + blockIdx.x);
 }
 
 // U1 = U^n + dt*L^n with the admissibility/integral partials of U1.
 __global__ void __launch_bounds__(kRedBlock) axpy_kernel(int n, const double* H0, const double* C0, const double* LH,
                                                          const double* LC, double dt, double area, double* H1,
-                                                         double* C1, Partial* partial) {
-    const Partial v = axpy_cells(n, H0, C0, LH, LC, dt, area, H1, C1, (long long)blockIdx.x * kSumCells);
+                                                         double* C1, Partial* partial, const double* cell_area) {
+    const Partial v = axpy_cells(n, H0, C0, LH, LC, dt, area, H1, C1, (long long)blockIdx.x * kSumCells, cell_area);
     block_reduce_write(v, partial + blockIdx.x);
 }
 
@@ -178,6 +180,12 @@ struct mp_transport {
     // per-cell source sums of a stage.
     double *cvs_y = nullptr, *cud_y = nullptr, *srcH = nullptr, *srcR = nullptr, *srcS = nullptr;
     mp::Totals curTot{};                   // totals of L(U^n)
+    // General quad mesh (mp_transport_create_quads): per-cell tables in HBM;
+    // cell_area points into them (null on a uniform mesh).
+    bool quad = false;
+    mp::QuadDev qdev{};
+    double* qbuf = nullptr;                // one allocation holding every table
+    const double* cell_area = nullptr;
     // Optional per-kernel timing (CUDA events on this handle's stream).
     bool profile = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -228,6 +236,7 @@ void free_all(mp_transport* t) {
                     t->rec, t->flags, t->vsn, t->udn, t->face, t->rate, t->partial, t->d_tot, t->d_status,
                     t->cvs_y, t->cud_y, t->srcH, t->srcR, t->srcS};
     for (void* b : bufs) if (b) cudaFree(b);
+    if (t->qbuf) cudaFree(t->qbuf);
     if (t->h_tot) cudaFreeHost(t->h_tot);
     if (t->h_status) cudaFreeHost(t->h_status);
 }
@@ -308,7 +317,13 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
         }
         sb = SourceBufs{t->cvs_y, t->cud_y, t->srcH, t->srcR, t->srcS};
     }
-    if (t->mixed) {
+    if (t->quad) {
+        timed(t, 0, [&] {
+            launch_quad_stage(t->qdev, t->nx, t->ny, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
+                              t->vsn, t->udn, t->face, t->d_status, theta,
+                              SourcePtrs{sb.cvs_y, sb.cud_y, sb.srcH, sb.srcR, sb.srcS}, s);
+        });
+    } else if (t->mixed) {
         launch_stage_kernels<float>(t->nx, t->ny, t->range, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
                                     t->vsn, t->udn, t->face, t->d_status, theta, s, prof, sb);
     } else {
@@ -318,12 +333,18 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
     {
         SumArgs a{t->nx, t->ny, t->host_tab.area, 1.0 / t->host_tab.area, t->face, H, C, t->H, t->C, outH, outC, t->rate, mode, a0, a1, dt,
                   t->partial, nullptr, t->range.gj0, t->range.gny, (long long)t->range.own0 * t->nx,
-                  (long long)t->range.own1 * t->nx, sb.srcH, sb.srcR, sb.srcS};
-        if (sb.srcH) timed(t, 3, [&] { sum_kernel<true><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
-        else timed(t, 3, [&] { sum_kernel<false><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
+                  (long long)t->range.own1 * t->nx, sb.srcH, sb.srcR, sb.srcS, t->cell_area};
+        if (t->quad) {
+            if (sb.srcH) timed(t, 3, [&] { sum_kernel<true, true><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
+            else timed(t, 3, [&] { sum_kernel<false, true><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
+        } else {
+            if (sb.srcH) timed(t, 3, [&] { sum_kernel<true><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
+            else timed(t, 3, [&] { sum_kernel<false><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
+        }
     }
     timed(t, 4, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, t->sum_blocks, t->d_tot); });
-    count_launch(5);
+    count_launch(t->quad ? 2 : 5);
+    if (!t->quad && t->ph.diffusion) count_launch();
     MP_CUDA(cudaGetLastError());
     return MP_OK;
 }
@@ -405,7 +426,8 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
         timed(t, 4, [&] {
             axpy_kernel<<<nblk_axpy, kRedBlock, 0, s>>>((int)on, t->H + o0, t->C + o0, t->LH + o0, t->LC + o0, dt,
                                                          t->host_tab.area,
-                                                         t->S1H + o0, t->S1C + o0, t->partial);
+                                                         t->S1H + o0, t->S1C + o0, t->partial,
+                                                         t->cell_area ? t->cell_area + o0 : nullptr);
         });
         timed(t, 4, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, nblk_axpy, t->d_tot); });
         count_launch(2);
@@ -492,7 +514,7 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
 namespace {
 // A whole mesh (slab = false) or the row slab [row_begin, row_end) of `mesh`.
 mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int row_end, const mp_transport_opts* opts,
-                      mp_stream_t stream, mp_transport** out) {
+                      mp_stream_t stream, mp_transport** out, const double* xy = nullptr) {
     using namespace mp;
     if (!mesh || !opts || !out) { set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (mesh->nx < 2 || mesh->ny < 2) { set_error("Transport requires at least 2x2 cells"); return MP_ERR_ARG_SIZ; }
@@ -505,6 +527,18 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
     mp_derived der;
     MP_TRY(derive_checked(opts->material, der));
     if (!(opts->inflow_C >= 0 && opts->inflow_C <= opts->material.Xe)) { set_error("Composition must lie in [0, phase.parameters.Xe]"); return MP_ERR_ARG_OUTOFRANGE; }
+    QuadTables qt;
+    if (xy) {
+        if (opts->precision != MP_PRECISION_FP64) { set_error("general quad meshes run in FP64"); return MP_ERR_ARG_WRONG; }
+        long long bad = -1;
+        if (validate_quads(mesh->nx, mesh->ny, xy, &bad)) {
+            set_error("Mesh has non-real/non-finite coordinates or an inverted, degenerate, or nearly singular "
+                      "quadrilateral (cell %lld)", bad);
+            return MP_ERR_ARG_WRONG;
+        }
+        const int qs = build_quad_tables(mesh->nx, mesh->ny, xy, 0, qt);
+        if (qs) { set_error("per-cell stencil table construction failed"); return (mp_status)qs; }
+    }
     if (slab && !(row_begin >= 0 && row_begin < row_end && row_end <= mesh->ny)) {
         set_error("slab rows [%d, %d) outside [0, %d)", row_begin, row_end, mesh->ny);
         return MP_ERR_ARG_OUTOFRANGE;
@@ -565,6 +599,26 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
     if (e == cudaSuccess) e = cudaMallocHost((void**)&t->h_status, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemsetAsync(t->vsn, 0, NE * kNQ * sizeof(double), t->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(t->udn, 0, NE * kNQ * sizeof(double), t->stream);
+    if (xy && e == cudaSuccess) {
+        // Per-cell tables of a general quad mesh, one allocation.
+        const size_t V = qt.xy.size(), NEq = qt.spacing.size();
+        const size_t total = V + (size_t)(kQG0 + kQS9 + kQT4 + kQS4 + kQGeo) * N + NEq;
+        e = cudaMalloc((void**)&t->qbuf, total * sizeof(double));
+        double* at = t->qbuf;
+        auto put = [&](const std::vector<double>& v) -> const double* {
+            if (e == cudaSuccess) e = cudaMemcpyAsync(at, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, t->stream);
+            const double* p = at;
+            at += v.size();
+            return p;
+        };
+        QuadDev& q = t->qdev;
+        q.xy = put(qt.xy); q.G0 = put(qt.G0); q.S9 = put(qt.S9); q.T4 = put(qt.T4); q.S4 = put(qt.S4);
+        q.geo = put(qt.geo); q.sp = put(qt.spacing);
+        for (int k = 0; k < 5; ++k) { q.gq[k] = qt.gq[k]; q.gw[k] = qt.gw[k]; q.dif_c_bnd[k] = qt.dif_c_bnd[k]; }
+        for (int k = 0; k < 4; ++k) q.dif_c_int[k] = qt.dif_c_int[k];
+        t->cell_area = q.geo + 3 * N;
+        t->quad = true;
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
     if (e != cudaSuccess) { free_all(t); delete t; return cuda_status(e, "mp_transport_create"); }
     *out = t;
@@ -575,6 +629,21 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
 extern "C" mp_status mp_transport_create(const mp_mesh_desc* mesh, const mp_transport_opts* opts, mp_stream_t stream,
                                          mp_transport** out) {
     return create_impl(mesh, false, 0, 0, opts, stream, out);
+}
+
+extern "C" mp_status mp_transport_create_quads(const mp_mesh_desc* mesh, const double* xy, const mp_transport_opts* opts,
+                                               mp_stream_t stream, mp_transport** out) {
+    if (!xy) { mp::set_error("null vertex array"); return MP_ERR_ARG_WRONG; }
+    return create_impl(mesh, false, 0, 0, opts, stream, out, xy);
+}
+
+extern "C" mp_status mp_mesh_vertices(const mp_mesh_desc* mesh, int family, double perturbation, unsigned long long seed,
+                                      double* xy) {
+    if (!mesh || !xy) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    const int st = mp::mesh_vertices(mesh->nx, mesh->ny, mesh->x0, mesh->x1, mesh->y0, mesh->y1, family, perturbation,
+                                     seed, xy);
+    if (st) mp::set_error("mesh: unknown family, non-finite or empty domain, or perturbation outside [0, 0.25)");
+    return (mp_status)st;
 }
 
 extern "C" mp_status mp_transport_create_slab(const mp_mesh_desc* global_mesh, int row_begin, int row_end,

@@ -173,6 +173,94 @@ def cell_velocity(w: Workload) -> tuple[np.ndarray, np.ndarray]:
     return vs_y, np.full_like(vs_y, w.darcy)
 
 
+# ---------------------------------------------------------------- quad meshes
+
+MESH_RECTANGULAR, MESH_PERTURBED, MESH_SINE_STRETCHED = 0, 1, 2
+
+
+def quad_vertices(w: Workload, family: int = MESH_PERTURBED, perturbation: float = 0.2, seed: int = 11) -> np.ndarray:
+    """Vertices of the reference's mesh families (src/core/mesh.cpp:27-55,
+    VertexAt): (nx+1)*(ny+1) (x, y) pairs, x fastest. Perturbed: interior
+    vertices moved by perturbation * spacing * (2U - 1), U the SplitMix64
+    noise keyed seed + 2*index (+1 for y); sine-stretched:
+    x = x0 + L sin(pi/2 * i/nx)."""
+    M, N = w.nx + 1, w.ny + 1
+    L, Hh = w.x1 - w.x0, w.y1 - w.y0
+    hx, hy = L / float(M - 1), Hh / float(N - 1)
+    i = np.arange(M, dtype=np.float64)[None, :].repeat(N, 0)
+    j = np.arange(N, dtype=np.float64)[:, None].repeat(M, 1)
+    x = w.x0 + i * hx
+    y = w.y0 + j * hy
+    if family == MESH_SINE_STRETCHED:
+        x = w.x0 + L * np.sin(0.5 * math.pi * (i / (M - 1)))
+        y = w.y0 + Hh * np.sin(0.5 * math.pi * (j / (N - 1)))
+    elif family == MESH_PERTURBED:
+        idx = (np.arange(N, dtype=np.uint64)[:, None] * np.uint64(M) + np.arange(M, dtype=np.uint64)[None, :])
+        nxn = 2.0 * unit_noise(seed, 0, idx) - 1.0
+        nyn = 2.0 * unit_noise(seed, 1, idx) - 1.0
+        inner = np.zeros((N, M), bool)
+        inner[1:-1, 1:-1] = True
+        x = np.where(inner, x + perturbation * hx * nxn, x)
+        y = np.where(inner, y + perturbation * hy * nyn, y)
+    x[:, 0], x[:, -1] = w.x0, w.x0 + L
+    y[0, :], y[-1, :] = w.y0, w.y0 + Hh
+    return np.ascontiguousarray(np.stack([x, y], -1).reshape(-1))
+
+
+def _flow(x, y, A):
+    """Solid velocity of psi = A sin(2 pi x) sin(pi y): (dpsi/dy, -dpsi/dx)."""
+    vx = math.pi * A * np.sin(2 * math.pi * x) * np.cos(math.pi * y)
+    vy = -2 * math.pi * A * np.cos(2 * math.pi * x) * np.sin(math.pi * y)
+    return vx, vy
+
+
+def face_velocity_quads(w: Workload, xy: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """face_velocity on a general quad mesh: normal components of the same
+    streamfunction flow and u_d = (0, darcy) at the 5 Gauss points of every
+    edge against its canonical right normal (dy, -dx)/len; solid normal
+    velocity exactly zero on wall edges."""
+    V = xy.reshape(w.ny + 1, w.nx + 1, 2)
+    t = 0.5 * (1.0 + GAUSS5_POINTS)
+    out_vs, out_ud = [], []
+    for a, b, wall in (
+        (V[:, :-1], V[:, 1:], np.r_[True, np.zeros(w.ny - 1, bool), True][:, None].repeat(w.nx, 1)),      # AlongI
+        (V[:-1, :], V[1:, :], np.zeros((w.ny, w.nx + 1), bool) | np.r_[True, np.zeros(w.nx - 1, bool), True][None, :]),
+    ):
+        d = b - a
+        length = np.hypot(d[..., 0], d[..., 1])
+        n = np.stack([d[..., 1], -d[..., 0]], -1) / length[..., None]
+        p = a[..., None, :] + t[None, None, :, None] * d[..., None, :]          # (rows, cols, 5, 2)
+        vx, vy = _flow(p[..., 0], p[..., 1], w.psi_amplitude)
+        vs = vx * n[..., None, 0] + vy * n[..., None, 1]
+        vs[wall] = 0.0
+        ud = np.broadcast_to(w.darcy * n[..., None, 1], vs.shape)
+        out_vs.append(vs.reshape(-1, 5))
+        out_ud.append(np.ascontiguousarray(ud).reshape(-1, 5))
+    return np.ascontiguousarray(np.concatenate(out_vs)), np.ascontiguousarray(np.concatenate(out_ud))
+
+
+def cell_velocity_quads(w: Workload, xy: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """cell_velocity on a general quad mesh: the vertical components at the
+    bilinear images of the 5x5 Gauss points, [cell*25 + b*5 + a]."""
+    V = xy.reshape(w.ny + 1, w.nx + 1, 2)
+    c0, c1, c2, c3 = V[:-1, :-1], V[:-1, 1:], V[1:, 1:], V[1:, :-1]
+    g = GAUSS5_POINTS
+    s = 0.5 * (1 - g)[None, :, None]
+    r = 0.5 * (1 + g)[None, :, None]
+    out = np.zeros((w.ny, w.nx, 5, 5))
+    for b in range(5):
+        sb, tb = 0.5 * (1 - g[b]), 0.5 * (1 + g[b])
+        for a in range(5):
+            sa, ta = 0.5 * (1 - g[a]), 0.5 * (1 + g[a])
+            lo = sa * c0 + ta * c1
+            hi = sa * c3 + ta * c2
+            p = sb * lo + tb * hi
+            out[:, :, b, a] = _flow(p[..., 0], p[..., 1], w.psi_amplitude)[1]
+    del s, r
+    vs_y = np.ascontiguousarray(out.reshape(-1))
+    return vs_y, np.full_like(vs_y, w.darcy)
+
+
 # The BASELINE workloads, named by what they are.
 def plain_small() -> Workload:
     """20x20 plain FP64 instance, 200 steps (the run.sh --grid 20 size)."""

@@ -65,7 +65,9 @@ class TransportConfig:
 class Transport:
     """One transport instance resident on the GPU."""
 
-    def __init__(self, w: Workload, config: TransportConfig | None = None, stream=None):
+    def __init__(self, w: Workload, config: TransportConfig | None = None, stream=None, vertices=None):
+        """vertices: (nx+1)*(ny+1) (x, y) pairs of a general quad mesh
+        (mp_transport_create_quads); None for the uniform mesh of w."""
         self._lib = _capi.lib()
         self.w = w
         self.config = config or TransportConfig(cfl=w.cfl, integrator=w.integrator)
@@ -73,7 +75,12 @@ class Transport:
         opts = self.config.to_c()
         h = C.c_void_p()
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
-        _capi.check(self._lib.mp_transport_create(C.byref(mesh), C.byref(opts), s, C.byref(h)))
+        if vertices is None:
+            _capi.check(self._lib.mp_transport_create(C.byref(mesh), C.byref(opts), s, C.byref(h)))
+        else:
+            xy = np.ascontiguousarray(vertices, dtype=np.float64)
+            _capi.check(self._lib.mp_transport_create_quads(C.byref(mesh), xy.ctypes.data, C.byref(opts), s,
+                                                             C.byref(h)))
         self._h = h
 
     def close(self):
@@ -155,3 +162,12 @@ class Transport:
         if raise_on_error:
             _capi.check(code)
         return code, out
+
+
+def mesh_vertices(w: Workload, family: int, perturbation: float = 0.0, seed: int = 1) -> np.ndarray:
+    """Vertices of a reference mesh family from the library (mp_mesh_vertices)."""
+    xy = np.zeros(2 * (w.nx + 1) * (w.ny + 1))
+    mesh = _capi.MeshDesc(w.nx, w.ny, w.x0, w.x1, w.y0, w.y1)
+    _capi.check(_capi.lib().mp_mesh_vertices(C.byref(mesh), int(family), float(perturbation), int(seed),
+                                             xy.ctypes.data))
+    return xy

@@ -83,6 +83,12 @@ typedef struct orc_transport_opts {
     double lf_global_speed;
     int uniform_tables;         /* 1: one stencil table set for all cells (uniform mesh) */
     int threads;                /* OpenMP threads (0 = default) */
+    /* Mesh family (src/core/mesh.cpp:27-55): 0 rectangular, 1 perturbed
+     * quadrilateral (interior vertices moved by perturbation * spacing *
+     * SplitMix64 noise keyed by seed), 2 sine-stretched. */
+    int mesh_family;
+    double perturbation;
+    unsigned long long seed;
 } orc_transport_opts;
 
 typedef struct orc_step_report {
@@ -122,6 +128,8 @@ int orc_transport_set_pressure_model(orc_transport* t, int model, double value);
  * [cell*25 + b*5 + a], for the adiabatic source (evolve.cpp:359-369). */
 int orc_transport_set_cell_velocity(orc_transport* t, const double* vs_y, const double* ud_y);
 int orc_transport_limiter(orc_transport* t, double* thetaH, double* thetaC);
+/* The mesh vertices, (nx+1)*(ny+1) (x, y) pairs, x fastest. */
+int orc_transport_vertices(const orc_transport* t, double* xy);
 
 /* Legacy dry preheat (src/couple/preheat.cpp:65-287) on a transport handle:
  * the Stokes velocity is vs_n of set_face_velocity (ud_n unused), H is

@@ -57,7 +57,8 @@ class TransportOpts(C.Structure):
                 ("theta", C.c_double), ("inflow_H", C.c_double), ("inflow_C", C.c_double),
                 ("H_policy", C.c_int), ("C_policy", C.c_int), ("integrator", C.c_int),
                 ("lf_global", C.c_int), ("lf_global_speed", C.c_double),
-                ("uniform_tables", C.c_int), ("threads", C.c_int)]
+                ("uniform_tables", C.c_int), ("threads", C.c_int), ("mesh_family", C.c_int),
+                ("perturbation", C.c_double), ("seed", C.c_ulonglong)]
 
 
 class StepReport(C.Structure):
@@ -107,6 +108,8 @@ class _Lib:
         t("rhs").argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 5 + [C.POINTER(StepReport)]
         t("limiter").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         t("step").argtypes = [C.c_void_p, C.c_int, C.POINTER(StepReport)]
+        t("vertices").restype = C.c_int
+        t("vertices").argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         p = lambda n: getattr(L, f"{prefix}_preheat_{n}")
         for n in ["begin", "rhs", "advance", "diagnostics"]:
             p(n).restype = C.c_int
@@ -190,13 +193,15 @@ class PhaseOracle:
 
 def transport_opts(w, *, uniform_tables=False, threads=0, integrator=None, pressure=0.0,
                    dt_initial=1e30, dt_max=1e30, dt_min=1e-14, cfl=None, inflow_H=1.0, H_policy=0,
-                   lf_global=0, lf_global_speed=0.0) -> TransportOpts:
+                   lf_global=0, lf_global_speed=0.0, mesh_family=0, perturbation=0.0,
+                   mesh_seed=1) -> TransportOpts:
     return TransportOpts(nx=w.nx, ny=w.ny, x0=w.x0, x1=w.x1, y0=w.y0, y1=w.y1, pressure=pressure,
                          cfl=w.cfl if cfl is None else cfl, dt_initial=dt_initial, dt_max=dt_max,
                          dt_min=dt_min, theta=0.0, inflow_H=inflow_H, inflow_C=0.3, H_policy=int(H_policy),
                          C_policy=0, integrator=int(integrator if integrator is not None else w.integrator),
                          lf_global=int(lf_global), lf_global_speed=float(lf_global_speed),
-                         uniform_tables=int(uniform_tables), threads=int(threads))
+                         uniform_tables=int(uniform_tables), threads=int(threads),
+                         mesh_family=int(mesh_family), perturbation=float(perturbation), seed=int(mesh_seed))
 
 
 class TransportOracle:
@@ -268,6 +273,11 @@ class TransportOracle:
         b = np.ascontiguousarray(ud_y, dtype=np.float64)
         self._cellv = (a, b)
         return self.lib.f("transport_set_cell_velocity")(self.h, _dptr(a), _dptr(b))
+
+    def vertices(self) -> np.ndarray:
+        xy = np.zeros(2 * (self.w.nx + 1) * (self.w.ny + 1))
+        self.lib.f("transport_vertices")(self.h, _dptr(xy))
+        return xy
 
     def set_time_control(self, control: int, t_end: float = float("inf")):
         return self.lib.f("transport_set_time_control")(self.h, int(control), float(t_end))

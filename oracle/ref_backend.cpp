@@ -275,6 +275,7 @@ int ref_transport_set_diffusion(void* t, double kappa, const int* types, const d
     return RefApi::set_diffusion(t, kappa, types, values);
 }
 
+int ref_transport_vertices(const void* t, double* xy) { return RefApi::vertices(t, xy); }
 int ref_preheat_begin(void* t, double* rate, double* limit, orc_preheat_step* first) {
     return RefApi::preheat_begin(t, rate, limit, first);
 }

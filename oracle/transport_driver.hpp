@@ -130,15 +130,30 @@ struct Driver {
         return Quad{{vert[(size_t)j * M + i], vert[(size_t)j * M + i + 1], vert[(size_t)(j + 1) * M + i + 1], vert[(size_t)(j + 1) * M + i]}};
     }
 
-    // mesh.cpp:27-55 (uniform family), integral-based areas as MeshInfo::CacheAreas.
+    // mesh.cpp:27-55 (VertexAt: rectangular, perturbed, sine-stretched),
+    // integral-based areas as MeshInfo::CacheAreas.
     void build_mesh() {
         const int M = nx + 1, N = ny + 1;
         const double L = o.x1 - o.x0, Hh = o.y1 - o.y0;
         const double hx = L / (double)(M - 1), hy = Hh / (double)(N - 1);
+        require(o.mesh_family >= 0 && o.mesh_family <= 2, E_OUTOFRANGE, "Unknown mesh family");
+        require(o.mesh_family != 1 || (std::isfinite(o.perturbation) && o.perturbation >= 0 && o.perturbation < 0.25),
+                E_OUTOFRANGE, "Perturbation must satisfy 0 <= perturbation < 0.25");
+        const double pi = 3.14159265358979323846;
+        auto signed_noise = [](uint64_t key) { return 2.0 * unit_noise(key) - 1.0; };
         vert.resize((size_t)M * N);
         for (int j = 0; j < N; ++j)
             for (int i = 0; i < M; ++i) {
                 Pt p{o.x0 + (double)i * hx, o.y0 + (double)j * hy};
+                if (o.mesh_family == 2) {
+                    const double s = (double)i / (M - 1), t = (double)j / (N - 1);
+                    p.x = o.x0 + L * std::sin(0.5 * pi * s);
+                    p.y = o.y0 + Hh * std::sin(0.5 * pi * t);
+                } else if (o.mesh_family == 1 && i > 0 && i < M - 1 && j > 0 && j < N - 1) {
+                    const uint64_t index = (uint64_t)j * (uint64_t)M + (uint64_t)i;
+                    p.x += o.perturbation * hx * signed_noise(o.seed + 2 * index);
+                    p.y += o.perturbation * hy * signed_noise(o.seed + 2 * index + 1);
+                }
                 if (i == 0) p.x = o.x0;
                 if (i == M - 1) p.x = o.x0 + L;
                 if (j == 0) p.y = o.y0;
@@ -889,6 +904,11 @@ struct Api {
         return 0;
     }
 
+    static int vertices(const void* h, double* xy) {
+        const auto& d = static_cast<const Handle<B>*>(h)->d;
+        for (size_t k = 0; k < d.vert.size(); ++k) { xy[2 * k] = d.vert[k].x; xy[2 * k + 1] = d.vert[k].y; }
+        return 0;
+    }
     static int set_time_control(void* h, int control, double t_end) {
         auto& d = static_cast<Handle<B>*>(h)->d;
         if (control != 0 && control != 1) return E_OUTOFRANGE;

@@ -162,6 +162,7 @@ extern "C" int orc_transport_set_time_control(orc_transport* t, int control, dou
     return RestatedApi::set_time_control(t, control, t_end);
 }
 
+extern "C" int orc_transport_vertices(const orc_transport* t, double* xy) { return RestatedApi::vertices(t, xy); }
 extern "C" int orc_preheat_begin(orc_transport* t, double* rate, double* limit, orc_preheat_step* first) {
     return RestatedApi::preheat_begin(t, rate, limit, first);
 }

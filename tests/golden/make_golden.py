@@ -4,7 +4,7 @@ Run in a container where the reference sources are mounted (they are not on
 GPU machines):
 
     make -C oracle ref            # compiles the reference's sources into oracle/_ref
-    python tests/golden/make_golden.py [phase] [transport] [preheat]
+    python tests/golden/make_golden.py [phase] [transport] [preheat] [quads]
 
 Writes, next to this script:
   phase_golden.npz      inputs and EutecticModel::evaluate outputs of the
@@ -20,7 +20,9 @@ Writes, next to this script:
                         plus 200-step SSPRK2 and SSPRK3 runs of 20x20.
   preheat_golden.npz    the reference-backed legacy dry preheat on the seeded
                         cases of tests/preheat_cases.py.
-Arguments (phase, transport, preheat) select fixtures; none = all.
+  quads_golden.npz      the reference-backed transport on perturbed-quadrilateral
+                        and sine-stretched meshes: RHS, limiter, 10 SSPRK3 steps.
+Arguments (phase, transport, preheat, quads) select fixtures; none = all.
 """
 from __future__ import annotations
 
@@ -166,13 +168,42 @@ def preheat_golden():
     print("preheat_golden.npz:", len(data), "arrays")
 
 
+def quads_golden():
+    """The reference-backed transport on perturbed-quadrilateral and
+    sine-stretched meshes (src/core/mesh.cpp:27-55): one RHS with the limiter
+    factors, and 10 SSPRK3 steps."""
+    import quad_cases as qc
+    data = {}
+    for name in qc.QUAD_CASES:
+        t, xy, _, _ = qc.quad_oracle(name, po.reference())
+        code, r = t.rhs()
+        assert code == 0, (name, code)
+        code, thH, thC = t.limiter()
+        assert code == 0
+        for k in ["rhsH", "rhsC", "T", "phi", "rate"]:
+            data[f"{name}_rhs_{k}"] = r[k]
+        data[f"{name}_rhs_totals"] = np.array([r["boundaryH"], r["boundaryC"], r["maxRate"], r["divergence"]])
+        data[f"{name}_thetaH"], data[f"{name}_thetaC"] = thH, thC
+        data[f"{name}_xy"] = xy
+        t, _, _, _ = qc.quad_oracle(name, po.reference())
+        code, reps = t.step(10)
+        assert code == 0, (name, code)
+        data[f"{name}_rk3_10"] = np.stack(t.get_state())
+        data[f"{name}_rk3_10_dt"] = np.array([x["dt"] for x in reps])
+        data[f"{name}_rk3_10_retries"] = np.array([x["retries"] for x in reps])
+    np.savez_compressed(os.path.join(HERE, "quads_golden.npz"), **data)
+    print("quads_golden.npz:", len(data), "arrays")
+
+
 if __name__ == "__main__":
     if not po.reference_available():
         sys.exit("reference build missing: run `make -C oracle ref` where the reference is mounted")
-    which = sys.argv[1:] or ["phase", "transport", "preheat"]
+    which = sys.argv[1:] or ["phase", "transport", "preheat", "quads"]
     if "phase" in which:
         phase_golden()
     if "transport" in which:
         transport_golden()
     if "preheat" in which:
         preheat_golden()
+    if "quads" in which:
+        quads_golden()
