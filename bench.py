@@ -270,6 +270,33 @@ def preheat_form(steps, stream, nx=None, ny=None):
                       f"dt 1e-4 (rate limit {limit:.3g}), host round trip every 512 steps"}
 
 
+def quads_form(steps, stream, nx=None, ny=None):
+    """The plain FP64 workload on the reference's perturbed-quadrilateral mesh
+    (perturbation 0.2, seed 11): per-cell tables in HBM, every evaluation
+    point mapped from the cell corners; SSPRK3, device-timed steps."""
+    import torch
+    from mantlepar_b200 import synthetic as sy
+    from mantlepar_b200.transport import Transport, TransportConfig
+    w = sy.Workload(nx=nx or WORKLOAD["nx"], ny=ny or WORKLOAD["ny"])
+    xy = sy.quad_vertices(w, sy.MESH_PERTURBED, 0.2, 11)
+    t0 = time.perf_counter()
+    t = Transport(w, TransportConfig(cfl=w.cfl, integrator=3), stream=stream.cuda_stream, vertices=xy)
+    setup_s = time.perf_counter() - t0
+    t.set_face_velocity(*sy.face_velocity_quads(w, xy))
+    t.set_state(*sy.initial_state(w))
+    t.step(1)
+    t.profile(True)
+    ms, (_, reps) = timed_steps(t, steps, stream)
+    kms, kn = t.kernel_times()
+    t.close()
+    stages = 3 * steps + sum(r["retries"] for r in reps) * 3
+    return {"value": w.cells * steps / (ms * 1e-3), "unit": "cell-updates/s", "steps": steps, "ms_per_step": ms / steps,
+            "retries": sum(r["retries"] for r in reps), "table_setup_s": setup_s,
+            "stage_kernels_ms": {"recon+cellphase+face": kms[0] / max(kn[0], 1), "sum": kms[3] / max(kn[3], 1)},
+            "stages": stages,
+            "config": f"{w.nx}x{w.ny} perturbed quadrilateral (0.2, seed 11), SSPRK3, CFL 0.4, material S"}
+
+
 def run_forms(args, stream):
     """The mixed-precision large instance and the batched uneven meshes."""
     from mantlepar_b200 import synthetic as sy
@@ -337,6 +364,7 @@ def run_forms(args, stream):
         "retries": sum(r["retries"] for r in reps)}
     tp.close()
     forms["preheat_1280x2560"] = preheat_form(max(args.form_steps, 50), stream)
+    forms["perturbed_quads_1280x2560"] = quads_form(args.form_steps, stream)
     # Served: a seeded Poisson stream (200 req/s) of uneven solves, mixed
     # precision, submitted in real time; memory admission against a 64 GiB budget.
     if args.serve_requests > 0:
@@ -563,6 +591,8 @@ def main():
     ap.add_argument("--ny", type=int, default=WORKLOAD["ny"], help="cells in y")
     ap.add_argument("--preheat-only", action="store_true",
                     help="time only the legacy dry preheat form (profiling)")
+    ap.add_argument("--quads-only", action="store_true",
+                    help="time only the perturbed-quadrilateral form (profiling)")
     ap.add_argument("--decompose", action="store_true",
                     help="one mesh in row slabs across the ranks (strong scaling) instead of one mesh per rank")
     args = ap.parse_args()
@@ -572,6 +602,11 @@ def main():
         import torch
         torch.cuda.set_device(local)
         print(json.dumps({"form": "preheat", **preheat_form(args.steps, torch.cuda.Stream(), args.nx, args.ny)}))
+        return
+    if args.quads_only:
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps({"form": "perturbed_quads", **quads_form(args.steps, torch.cuda.Stream(), args.nx, args.ny)}))
         return
     if args.impl == "reference":
         run_reference(args, world, rank)

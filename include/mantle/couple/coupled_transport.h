@@ -86,9 +86,14 @@ struct Configuration {
     bool mixedPrecision = false;         // FP32 smoothness/weights/limiter scan
 };
 
+// The cell grid and domain; `vertices` ((nx+1)*(ny+1) (x, y) pairs, x
+// fastest) makes it a general quad mesh such as the reference's
+// "perturbed_quadrilateral" family (mp_mesh_vertices builds them); empty =
+// the uniform rectangular mesh of the domain.
 struct Mesh {
     int nx = 0, ny = 0;
     double x0 = 0, x1 = 1, y0 = 0, y1 = 1;
+    std::vector<double> vertices;
 };
 
 struct InitialState {

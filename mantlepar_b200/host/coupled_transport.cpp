@@ -66,7 +66,10 @@ mp_transport* create(const Configuration& c, const Mesh& m, bool continuing) {
     const mp_mesh_desc d{m.nx, m.ny, m.x0, m.x1, m.y0, m.y1};
     const mp_transport_opts o = options(c, continuing);
     mp_transport* h = nullptr;
-    mp_status st = mp_transport_create(&d, &o, nullptr, &h);
+    if (!m.vertices.empty() && m.vertices.size() != 2 * (size_t)(m.nx + 1) * (m.ny + 1))
+        throw std::invalid_argument("Mesh::vertices must hold (nx+1)*(ny+1) (x, y) pairs");
+    mp_status st = m.vertices.empty() ? mp_transport_create(&d, &o, nullptr, &h)
+                                      : mp_transport_create_quads(&d, m.vertices.data(), &o, nullptr, &h);
     if (st != MP_OK) throw_status(st);
     st = mp_transport_set_time_control(h, control, c.time.end);
     if (st == MP_OK) {
@@ -274,6 +277,7 @@ int AdvanceLegacyPreheat(const Configuration& c, InitialState& state, const Edge
     const int control = control_of(c.time);
     if (control < 0) return MP_ERR_ARG_OUTOFRANGE;
     const Mesh mesh = state.mesh;
+    if (!mesh.vertices.empty()) return MP_ERR_ARG_WRONG;   // the preheat kernels take rectangular meshes
     const size_t ncell = (size_t)mesh.nx * mesh.ny;
     if (state.enthalpy.size() != ncell || state.composition.size() != ncell) return MP_ERR_ARG_SIZ;
     if (flow.solid.size() != (size_t)EdgeCount(mesh) * 5) return MP_ERR_ARG_SIZ;

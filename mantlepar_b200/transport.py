@@ -164,6 +164,20 @@ class Transport:
         return code, out
 
 
+    def profile(self, enable: bool = True):
+        """Per-kernel CUDA-event timing on (resets the accumulators) or off."""
+        _capi.check(self._lib.mp_transport_profile(self._h, int(enable)))
+
+    def kernel_times(self):
+        """(ms[6], launches[6]) accumulated since profile(True): reconstruction
+        (on a general quad mesh: the whole reconstruction, cell phase and face
+        work), cell phase, faces, accumulation, axpy and reductions."""
+        ms = (C.c_double * 6)()
+        n = (C.c_ulonglong * 6)()
+        _capi.check(self._lib.mp_transport_kernel_times(self._h, ms, n))
+        return list(ms), list(n)
+
+
 def mesh_vertices(w: Workload, family: int, perturbation: float = 0.0, seed: int = 1) -> np.ndarray:
     """Vertices of a reference mesh family from the library (mp_mesh_vertices)."""
     xy = np.zeros(2 * (w.nx + 1) * (w.ny + 1))
