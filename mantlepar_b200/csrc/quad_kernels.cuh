@@ -225,22 +225,21 @@ __device__ __forceinline__ int reconstruct_quad(const QuadDev& q, size_t N, long
 
 // ------------------------------------------------------------------ kernels
 
-// Reconstruction, limiter over the cell's own limiter points
-// (state_reconstruction.cpp:136-192), limited coefficients.
-__global__ void __launch_bounds__(128) quad_recon_kernel(int nx, int ny, const double* __restrict__ H,
-                                                         const double* __restrict__ C, double* __restrict__ rec,
-                                                         unsigned char* __restrict__ flags, unsigned long long* status,
-                                                         double* theta, Physics ph, QuadDev q) {
+// Reconstruction (Reconstruction::Update, src/mlweno/reconstruction.cpp:
+// 275-355) of H and C with the cell's own tables: the unlimited deviation
+// polynomials into rec. The limiter runs in the next kernel, so that neither
+// kernel holds both the table-driven weights and the point scan in
+// registers (the table reads need many warps in flight).
+__global__ void __launch_bounds__(128, 4) quad_weno_kernel(int nx, int ny, const double* __restrict__ H,
+                                                           const double* __restrict__ C, double* __restrict__ rec,
+                                                           unsigned long long* status, QuadDev q) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= nx || j >= ny) return;
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
-    const CellFrame f = cell_frame(q, nx, N, cell);
-    const double eA = 1e-2 * f.area;
-    double DH[9], DC[9];
-    double mH = 0, mC = 0, loH = 0, hiH = 0, loC = 0, hiC = 0;
-    int st = 0, st_lim = 0;
+    const double eA = 1e-2 * __ldg(q.geo + 3 * N + cell);
+    int st = 0;
 #pragma unroll
     for (int fi = 0; fi < 2; ++fi) {
         const double* F = fi ? C : H;
@@ -252,16 +251,48 @@ __global__ void __launch_bounds__(128) quad_recon_kernel(int nx, int ny, const d
                 const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
                 u[dj][di] = __ldg(F + (size_t)jj * nx + ii);
             }
-        double lo = u[1][1], hi = u[1][1];
-#pragma unroll
-        for (int dj = 0; dj < 3; ++dj)
-#pragma unroll
-            for (int di = 0; di < 3; ++di) { lo = fmin(lo, u[dj][di]); hi = fmax(hi, u[dj][di]); }
-        const int s1 = reconstruct_quad(q, N, cell, ci, cj, eA, u, fi ? DC : DH);
+        double D[9];
+        const int s1 = reconstruct_quad(q, N, cell, ci, cj, eA, u, D);
         st = st ? st : s1;
-        if (fi == 0) { mH = u[1][1]; loH = fmax(0.0, lo); hiH = hi; }
-        else { mC = u[1][1]; loC = fmax(0.0, lo); hiC = fmin(ph.k.Xe, hi); }
+#pragma unroll
+        for (int m = 0; m < 9; ++m) rec[(size_t)(m + 9 * fi) * N + cell] = D[m];
     }
+    if (st) record_error(status, PART_UPDATE, cell, st);
+}
+
+// Limiter over the cell's own limiter points (state_reconstruction.cpp:
+// 136-192): theta of H and C from the unlimited polynomials in rec, which
+// are scaled in place.
+__global__ void __launch_bounds__(128, 4) quad_limit_kernel(int nx, int ny, const double* __restrict__ H,
+                                                         const double* __restrict__ C, double* __restrict__ rec,
+                                                         unsigned char* __restrict__ flags, unsigned long long* status,
+                                                         double* theta, Physics ph, QuadDev q) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= nx || j >= ny) return;
+    const long long cell = (long long)j * nx + i;
+    const size_t N = (size_t)nx * ny;
+    const CellFrame f = cell_frame(q, nx, N, cell);
+    double DH[9], DC[9];
+    load_rec(rec, N, cell, DH, DC);
+    // 3x3 neighbour bounds of the averages (state_reconstruction.cpp:189-196).
+    double lo[2], hi[2], m[2];
+#pragma unroll
+    for (int fi = 0; fi < 2; ++fi) {
+        const double* F = fi ? C : H;
+        m[fi] = __ldg(F + cell);
+        lo[fi] = m[fi]; hi[fi] = m[fi];
+#pragma unroll
+        for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+            for (int di = -1; di <= 1; ++di) {
+                const int ii = min(max(i + di, 0), nx - 1), jj = min(max(j + dj, 0), ny - 1);
+                const double v = __ldg(F + (size_t)jj * nx + ii);
+                lo[fi] = fmin(lo[fi], v); hi[fi] = fmax(hi[fi], v);
+            }
+    }
+    const double mH = m[0], mC = m[1];
+    const double loH = fmax(0.0, lo[0]), hiH = hi[0], loC = fmax(0.0, lo[1]), hiC = fmin(ph.k.Xe, hi[1]);
+    int st_lim = 0;
     if (!(isfinite(mH) && mH >= 0.0 && isfinite(mC) && mC >= 0.0 && mC <= ph.k.Xe)) st_lim = E_OUTOFRANGE;
     double hmx = -INFINITY, hmn = INFINITY, cmx = -INFINITY, cmn = INFINITY;
     bool bad = false;
@@ -293,18 +324,17 @@ __global__ void __launch_bounds__(128) quad_recon_kernel(int nx, int ny, const d
     const double Hliq = tep + (1.0 - hiC / ph.k.Xe) + ph.k.LD;
     const bool safe = tep >= 0.0 && hiH + 1e-12 * (1.0 + fabs(hiH)) < Hliq;
 #pragma unroll
-    for (int m = 0; m < 9; ++m) {
-        rec[(size_t)m * N + cell] = DH[m] * thH;
-        rec[(size_t)(m + 9) * N + cell] = DC[m] * thC;
+    for (int k = 0; k < 9; ++k) {
+        rec[(size_t)k * N + cell] = DH[k] * thH;
+        rec[(size_t)(k + 9) * N + cell] = DC[k] * thC;
     }
     flags[cell] = safe ? 0 : FLAG_CHECK;
-    if (st) record_error(status, PART_UPDATE, cell, st);
     if (st_lim) record_error(status, PART_LIMIT, cell, st_lim);
 }
 
 // 5x5 cell quadrature of T and phi on the bilinear map, wet flag, adiabatic
 // source, and the exact check of the diffusion samples when flagged.
-__global__ void __launch_bounds__(128) quad_cellphase_kernel(int nx, int ny, const double* __restrict__ H,
+__global__ void __launch_bounds__(128, 4) quad_cellphase_kernel(int nx, int ny, const double* __restrict__ H,
                                                              const double* __restrict__ C, const double* __restrict__ rec,
                                                              unsigned char* __restrict__ flags, double* __restrict__ T,
                                                              double* __restrict__ phi, unsigned long long* status,
@@ -422,7 +452,7 @@ __device__ __forceinline__ void side_values(const Side& s, P2 p, double& h, doub
 }
 
 // Face fluxes, edge porosity and rate of one edge at its 5 Gauss points.
-__global__ void __launch_bounds__(128) quad_face_kernel(int nx, int ny, const double* __restrict__ H,
+__global__ void __launch_bounds__(128, 3) quad_face_kernel(int nx, int ny, const double* __restrict__ H,
                                                         const double* __restrict__ C, const double* __restrict__ rec,
                                                         const unsigned char* __restrict__ flags,
                                                         const double* __restrict__ vsn, const double* __restrict__ udn,
@@ -551,12 +581,13 @@ void launch_quad_stage(const QuadDev& q, int nx, int ny, const Physics& ph, cons
     const long long N = (long long)nx * ny;
     const long long NE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
     dim3 blk(32, 4), grd((nx + 31) / 32, (ny + 3) / 4);
-    quad_recon_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, flags, status, theta, ph, q);
+    quad_weno_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, status, q);
+    quad_limit_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, flags, status, theta, ph, q);
     quad_cellphase_kernel<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, flags, T, phi, status, ph, q,
                                                                       src);
     quad_face_kernel<<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, flags, vsn, udn, face, status,
                                                                   ph, q);
-    count_launch(3);
+    count_launch(4);
     if (ph.diffusion) {
         quad_diffusion_kernel<<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, face, status, ph, q);
         count_launch();
