@@ -168,6 +168,46 @@ def cpu_run(nsteps_min: int, seconds: float, threads: int):
     return w.cells * steps / el, threads, kind, f"{w.nx}x{w.ny} sub-instance of the same construction, {steps} SSPRK3 steps", steps, el
 
 
+def cpu_form_baseline(form: str, seconds: float = 6.0, threads: int = 0) -> dict:
+    """The reference build (oracle/_ref; else the restated oracle) on a bounded
+    160x320 sample of a form's workload, all host threads: cell-updates/s."""
+    import sys as _sys
+    from oracle import pyoracle as po
+    from mantlepar_b200 import synthetic as sy
+    threads = threads or os.cpu_count() or 1
+    kind = "reference" if po.reference_available() else "port"
+    lib = po.reference() if kind == "reference" else po.restated()
+    w = sy.Workload(**CPU_SAMPLE)
+    if form == "preheat":
+        _sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import preheat_cases as pc
+        case = pc.PreheatCase(w, through=0.05, kappa=1e-4, thermal_type=(1, 1, 0, 0),
+                              thermal_value=(0.9, 0.2, 0.0, 0.0), end=1e9, dt_initial=1e-4, dt_max=1e-4)
+        t = pc.oracle_instance(case, lib)
+        assert t.preheat_begin()[0] == 0
+        steps, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < seconds:
+            code, rows = t.preheat_advance(5)
+            assert code == 0
+            steps += len(rows)
+        sample = f"{w.nx}x{w.ny} sub-instance, {steps} forward-Euler steps"
+    else:
+        t = po.TransportOracle(sy.material_s(), w, lib=lib, integrator=3, threads=threads, mesh_family=1,
+                               perturbation=0.2, mesh_seed=11)
+        xy = t.vertices()
+        t.set_face_velocity(*sy.face_velocity_quads(w, xy))
+        t.set_state(*sy.initial_state(w))
+        assert t.step(1)[0] == 0
+        steps, t0 = 0, time.perf_counter()
+        while steps < 1 or time.perf_counter() - t0 < seconds:
+            assert t.step(1)[0] == 0
+            steps += 1
+        sample = f"{w.nx}x{w.ny} perturbed sub-instance, {steps} SSPRK3 steps"
+    el = time.perf_counter() - t0
+    t.close()
+    return {"value": w.cells * steps / el, "unit": "cell-updates/s", "cores": threads, "kind": kind, "sample": sample}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -267,9 +307,15 @@ def preheat_form(steps, stream, nx=None, ny=None):
             "ms_per_step": ms_step, "status": code, "accepted": len(rows),
             "max_balance_error": max(abs(r["balanceError"]) for r in rows),
             "achieved_gbs": PREHEAT_BYTES_PER_CELL_STEP * w.cells / (ms_step * 1e-3) / 1e9,
+            "hbm_frac_of_measured": PREHEAT_BYTES_PER_CELL_STEP * w.cells / (ms_step * 1e-3) / 1e9 / peaks()[0],
             "bytes_per_cell_step": PREHEAT_BYTES_PER_CELL_STEP,
             "config": f"{w.nx}x{w.ny}, kappa=1e-4, wall temperatures bottom 0.9 / top 0.2, through-flow 0.05, "
                       f"dt 1e-4 (rate limit {limit:.3g}), host round trip every 512 steps"}
+
+
+# Per-cell tables a stage of the general-quad path streams (G0 72, S9 36,
+# T4 48, S4 24, geometry 4 doubles).
+QUAD_TABLE_BYTES_PER_CELL = 184 * 8
 
 
 def quads_form(steps, stream, nx=None, ny=None):
@@ -292,8 +338,10 @@ def quads_form(steps, stream, nx=None, ny=None):
     kms, kn = t.kernel_times()
     t.close()
     stages = 3 * steps + sum(r["retries"] for r in reps) * 3
+    table_gbs = QUAD_TABLE_BYTES_PER_CELL * w.cells * kn[0] / max(kms[0], 1e-9) / 1e6
     return {"value": w.cells * steps / (ms * 1e-3), "unit": "cell-updates/s", "steps": steps, "ms_per_step": ms / steps,
             "retries": sum(r["retries"] for r in reps), "table_setup_s": setup_s,
+            "table_stream_gbs": table_gbs, "table_stream_frac_of_measured_hbm": table_gbs / peaks()[0],
             "stage_kernels_ms": {"recon+cellphase+face": kms[0] / max(kn[0], 1), "sum": kms[3] / max(kn[3], 1)},
             "stages": stages,
             "config": f"{w.nx}x{w.ny} perturbed quadrilateral (0.2, seed 11), SSPRK3, CFL 0.4, material S"}
@@ -367,6 +415,9 @@ def run_forms(args, stream):
     tp.close()
     forms["preheat_1280x2560"] = preheat_form(max(args.form_steps, 50), stream)
     forms["perturbed_quads_1280x2560"] = quads_form(args.form_steps, stream)
+    if not args.no_cpu_baseline:
+        forms["preheat_1280x2560"]["cpu_baseline"] = cpu_form_baseline("preheat")
+        forms["perturbed_quads_1280x2560"]["cpu_baseline"] = cpu_form_baseline("quads")
     # Served: a seeded Poisson stream (200 req/s) of uneven solves, mixed
     # precision, submitted in real time; memory admission against a 64 GiB budget.
     if args.serve_requests > 0:

@@ -55,6 +55,8 @@ CASES = {
                                 lf_global_speed=1.5, control=1, dt_initial=4e-3, end=0.03,
                                 thermal_type=(2, 1, 1, 0), thermal_value=(-0.02, 0.3, 0.7, 0.0),
                                 pressure_model=1),
+    "tiny_2x2": PreheatCase(sy.Workload(nx=2, ny=2, seed=4), through=0.2, kappa=3e-3, end=0.02,
+                            thermal_type=(1, 2, 1, 0), thermal_value=(1.0, -0.01, 0.5, 0.0)),
 }
 
 

@@ -13,11 +13,13 @@ def quad_case(name):
         "p3x5": (sy.Workload(nx=3, ny=5, seed=7), 1, 0.24, {}),
         "p9x11_diff": (sy.Workload(nx=9, ny=11, seed=3), 1, 0.15, {"diffusion": True}),
         "s8x7": (sy.Workload(nx=8, ny=7, seed=2, psi_amplitude=0.05), 2, 0.0, {}),
+        "p2x2": (sy.Workload(nx=2, ny=2, seed=9), 1, 0.2, {}),
+        "p5x4_diff": (sy.Workload(nx=5, ny=4, seed=13, noise_H=0.1), 1, 0.24, {"diffusion": True}),
     }
     return cases[name]
 
 
-QUAD_CASES = ["p12x10", "p3x5", "p9x11_diff", "s8x7"]
+QUAD_CASES = ["p12x10", "p3x5", "p9x11_diff", "s8x7", "p2x2", "p5x4_diff"]
 
 
 def quad_oracle(name, lib=None, integrator=3):
