@@ -142,13 +142,13 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_run(nsteps_min: int, seconds: float, threads: int):
+def cpu_run(nsteps_min: int, seconds: float, threads: int, sample: dict | None = None):
     """Reference CPU implementation on the bounded sample: returns (value, cores, kind, sample, steps, time)."""
     from oracle import pyoracle as po
     from mantlepar_b200 import synthetic as sy
     kind = "reference" if po.reference_available() else "port"
     lib = po.reference() if kind == "reference" else po.restated()
-    w = sy.Workload(**CPU_SAMPLE)
+    w = sy.Workload(**(sample or CPU_SAMPLE))
     t = po.TransportOracle(sy.material_s(), w, lib=lib, integrator=3, threads=threads)
     vs, ud = sy.face_velocity(w)
     H, C = sy.initial_state(w)
@@ -621,6 +621,9 @@ def run_gpu(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, kind, sample, _, _ = cpu_run(2, CPU_SECONDS, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": kind, "sample": sample}
+        # The same sample on one core, recorded beside the all-core figure.
+        v1, _, _, sample1, _, _ = cpu_run(1, CPU_SECONDS / 3, 1, dict(nx=40, ny=80))
+        line["cpu_baseline"]["one_core"] = {"value": v1, "cores": 1, "sample": sample1}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
