@@ -189,7 +189,8 @@ void mp_transport_destroy(mp_transport* t);
  * SetTargetSmoothness per stencil, src/mlweno/tensorstencilpoly.cpp:146-231,
  * 383-398) and every evaluation point its own geometry. FP64 only; cells
  * failing the reference's quad check (src/core/quad_validation.h) ->
- * MP_ERR_ARG_WRONG. All other mp_transport_* calls apply unchanged. */
+ * MP_ERR_ARG_WRONG. All other mp_transport_* calls apply unchanged; row
+ * slabs: mp_transport_create_quads_slab. */
 enum { MP_MESH_RECTANGULAR = 0, MP_MESH_PERTURBED = 1, MP_MESH_SINE_STRETCHED = 2 };
 mp_status mp_transport_create_quads(const mp_mesh_desc* mesh, const double* xy, const mp_transport_opts* opts,
                                     mp_stream_t stream, mp_transport** out);
@@ -290,6 +291,11 @@ mp_status mp_transport_create_slab(const mp_mesh_desc* global_mesh, int row_begi
                                    const mp_transport_opts* opts, mp_stream_t stream, mp_transport** out);
 /* local_rows: rows held (owned + halos); row0: global row of local row 0;
  * own_begin/own_end: local rows owned. */
+/* A row slab of a general quad mesh: xy holds the vertices of the WHOLE
+ * mesh (as mp_transport_create_quads); every local cell's tables are built
+ * from its stencil in the whole mesh, so slabs reproduce the single run. */
+mp_status mp_transport_create_quads_slab(const mp_mesh_desc* global_mesh, const double* xy, int row_begin, int row_end,
+                                         const mp_transport_opts* opts, mp_stream_t stream, mp_transport** out);
 mp_status mp_transport_slab_layout(const mp_transport* t, int* local_rows, int* row0, int* own_begin, int* own_end);
 mp_status mp_transport_set_hooks(mp_transport* t, mp_halo_fn halo, mp_combine_fn combine, void* user);
 

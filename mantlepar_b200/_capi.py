@@ -174,6 +174,8 @@ def lib() -> C.CDLL:
         "mp_batch_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
         "mp_transport_create_quads": (i, [C.POINTER(MeshDesc), vp, C.POINTER(TransportOpts), vp, C.POINTER(vp)]),
         "mp_mesh_vertices": (i, [C.POINTER(MeshDesc), i, d, C.c_ulonglong, vp]),
+        "mp_transport_create_quads_slab": (i, [C.POINTER(MeshDesc), vp, i, i, C.POINTER(TransportOpts), vp,
+                                               C.POINTER(vp)]),
         "mp_preheat_create": (i, [C.POINTER(MeshDesc), C.POINTER(PreheatOpts), vp, C.POINTER(vp)]),
         "mp_preheat_destroy": (None, [vp]),
         "mp_preheat_set_velocity": (i, [vp, vp]),

@@ -105,13 +105,16 @@ __device__ __forceinline__ CellFrame cell_frame(const QuadDev& q, int nx, size_t
 }
 
 // Edge e of cell (i, j) in counter-clockwise order (0 bottom, 1 right, 2 top,
-// 3 left): its mesh edge id, whether it is a wall, and whether the cell's
-// point order runs against the canonical one.
-__device__ __forceinline__ void cell_edge(int nx, int ny, int i, int j, int e, long long& id, bool& wall, bool& rev) {
+// 3 left): its local edge id, whether it is a wall, and whether the cell's
+// point order runs against the canonical one. Local rows j of a mesh whose
+// local row 0 is global row gj0 of gny global rows.
+__device__ __forceinline__ void cell_edge(int nx, int ny, int i, int j, int gj0, int gny, int e, long long& id,
+                                          bool& wall, bool& rev) {
     const long long nI = (long long)nx * (ny + 1);
-    if (e == 0) { id = (long long)j * nx + i; wall = j == 0; rev = false; }
+    const int gj = gj0 + j;
+    if (e == 0) { id = (long long)j * nx + i; wall = gj == 0; rev = false; }
     else if (e == 1) { id = nI + (long long)j * (nx + 1) + i + 1; wall = i == nx - 1; rev = false; }
-    else if (e == 2) { id = (long long)(j + 1) * nx + i; wall = j == ny - 1; rev = true; }
+    else if (e == 2) { id = (long long)(j + 1) * nx + i; wall = gj == gny - 1; rev = true; }
     else { id = nI + (long long)j * (nx + 1) + i; wall = i == 0; rev = true; }
 }
 
@@ -119,11 +122,12 @@ __device__ __forceinline__ void cell_edge(int nx, int ny, int i, int j, int e, l
 // edges (diffusiveflux.cpp:255-334, 4 samples; interior edges 2 on each side
 // at offsets -1.5, -0.5 spacings from the edge, wall edges 4 at -4..-1).
 template <class F>
-__device__ __forceinline__ void visit_samples(const QuadDev& q, int nx, int ny, int i, int j, const CellFrame& f, F&& visit) {
+__device__ __forceinline__ void visit_samples(const QuadDev& q, int nx, int ny, int gj0, int gny, int i, int j,
+                                              const CellFrame& f, F&& visit) {
     for (int e = 0; e < 4; ++e) {
         long long id;
         bool wall, rev;
-        cell_edge(nx, ny, i, j, e, id, wall, rev);
+        cell_edge(nx, ny, i, j, gj0, gny, e, id, wall, rev);
         const P2 a = f.c[e], b = f.c[(e + 1) & 3];
         double len;
         P2 n;
@@ -232,12 +236,14 @@ __device__ __forceinline__ int reconstruct_quad(const QuadDev& q, size_t N, long
 // registers (the table reads need many warps in flight).
 __global__ void __launch_bounds__(128, 4) quad_weno_kernel(int nx, int ny, const double* __restrict__ H,
                                                            const double* __restrict__ C, double* __restrict__ rec,
-                                                           unsigned long long* status, QuadDev q) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= nx || j >= ny) return;
+                                                           unsigned long long* status, QuadDev q, int gj0, int gny,
+                                                           int jlo, int jhi) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = jlo + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    if (i >= nx || j >= jhi) return;
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
-    const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
+    const int gj = gj0 + j;
+    const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = gj == 0 ? 0 : (gj == gny - 1 ? 2 : 1);
     const double eA = 1e-2 * __ldg(q.geo + 3 * N + cell);
     int st = 0;
 #pragma unroll
@@ -257,7 +263,7 @@ __global__ void __launch_bounds__(128, 4) quad_weno_kernel(int nx, int ny, const
 #pragma unroll
         for (int m = 0; m < 9; ++m) rec[(size_t)(m + 9 * fi) * N + cell] = D[m];
     }
-    if (st) record_error(status, PART_UPDATE, cell, st);
+    if (st) record_error(status, PART_UPDATE, cell + (long long)gj0 * nx, st);
 }
 
 // Limiter over the cell's own limiter points (state_reconstruction.cpp:
@@ -266,9 +272,10 @@ __global__ void __launch_bounds__(128, 4) quad_weno_kernel(int nx, int ny, const
 __global__ void __launch_bounds__(128, 4) quad_limit_kernel(int nx, int ny, const double* __restrict__ H,
                                                          const double* __restrict__ C, double* __restrict__ rec,
                                                          unsigned char* __restrict__ flags, unsigned long long* status,
-                                                         double* theta, Physics ph, QuadDev q) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= nx || j >= ny) return;
+                                                         double* theta, Physics ph, QuadDev q, int gj0, int gny,
+                                                         int jlo, int jhi) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = jlo + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    if (i >= nx || j >= jhi) return;
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
     const CellFrame f = cell_frame(q, nx, N, cell);
@@ -310,7 +317,7 @@ __global__ void __launch_bounds__(128, 4) quad_limit_kernel(int nx, int ny, cons
         for (int b = 0; b < kNQ; ++b) visit(bilinear(q.gq[a], q.gq[b], f.c));
     for (int e = 0; e < 4; ++e)
         for (int k = 0; k < kNQ; ++k) visit(lerp_edge(q.gq[k], f.c[e], f.c[(e + 1) & 3]));
-    visit_samples(q, nx, ny, i, j, f, visit);
+    visit_samples(q, nx, ny, gj0, gny, i, j, f, visit);
     if (bad) st_lim = st_lim ? st_lim : E_FP;
     const double thH = theta_of(mH, loH, hiH, hmx, hmn);
     const double thC = theta_of(mC, loC, hiC, cmx, cmn);
@@ -329,7 +336,7 @@ __global__ void __launch_bounds__(128, 4) quad_limit_kernel(int nx, int ny, cons
         rec[(size_t)(k + 9) * N + cell] = DC[k] * thC;
     }
     flags[cell] = safe ? 0 : FLAG_CHECK;
-    if (st_lim) record_error(status, PART_LIMIT, cell, st_lim);
+    if (st_lim) record_error(status, PART_LIMIT, cell + (long long)gj0 * nx, st_lim);
 }
 
 // 5x5 cell quadrature of T and phi on the bilinear map, wet flag, adiabatic
@@ -338,10 +345,11 @@ __global__ void __launch_bounds__(128, 4) quad_cellphase_kernel(int nx, int ny, 
                                                              const double* __restrict__ C, const double* __restrict__ rec,
                                                              unsigned char* __restrict__ flags, double* __restrict__ T,
                                                              double* __restrict__ phi, unsigned long long* status,
-                                                             Physics ph, QuadDev q, SourcePtrs src) {
+                                                             Physics ph, QuadDev q, SourcePtrs src, int gj0, int gny,
+                                                             long long c0, long long c1) {
     const long long N = (long long)nx * ny;
-    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= N) return;
+    const long long cell = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= c1) return;
     const int i = (int)(cell % nx), j = (int)(cell / nx);
     const CellFrame f = cell_frame(q, nx, (size_t)N, cell);
     const double mH = __ldg(H + cell), mC = __ldg(C + cell);
@@ -376,7 +384,7 @@ __global__ void __launch_bounds__(128, 4) quad_cellphase_kernel(int nx, int ny, 
         }
     const unsigned char fl = flags[cell];
     if (fl & FLAG_CHECK) {
-        visit_samples(q, nx, ny, i, j, f, [&](P2 p) {
+        visit_samples(q, nx, ny, gj0, gny, i, j, f, [&](P2 p) {
             const double x = (p.x - f.cx) * f.inv_h, y = (p.y - f.cy) * f.inv_h;
             const double tep = ph.litho ? tep_at(ph, p.y) : ph.Tep;
             PhaseLean pl;
@@ -385,9 +393,10 @@ __global__ void __launch_bounds__(128, 4) quad_cellphase_kernel(int nx, int ny, 
             if (!(pl.T >= 0.0 && pl.phil < 1.0)) st_face = st_face ? st_face : E_OUTOFRANGE;
         });
     }
-    if (st_por) record_error(status, PART_POROSITY, cell, st_por);
-    if (st_face) record_error(status, PART_FACES, cell, st_face);
-    if (st_cell) record_error(status, PART_CELLS, cell, st_cell);
+    const long long key = cell + (long long)gj0 * nx;
+    if (st_por) record_error(status, PART_POROSITY, key, st_por);
+    if (st_face) record_error(status, PART_FACES, key, st_face);
+    if (st_cell) record_error(status, PART_CELLS, key, st_cell);
     flags[cell] = (unsigned char)((fl & FLAG_CHECK) | (wet ? FLAG_WET : 0));
     T[cell] = Tsum;
     phi[cell] = Psum;
@@ -401,7 +410,7 @@ struct QuadEdge {
     int wall;
     P2 a, b;
 };
-__device__ __forceinline__ QuadEdge quad_edge(const QuadDev& q, int nx, int ny, long long e) {
+__device__ __forceinline__ QuadEdge quad_edge(const QuadDev& q, int nx, int ny, int gj0, int gny, long long e) {
     const long long nI = (long long)nx * (ny + 1);
     QuadEdge g;
     g.R = -1;
@@ -409,12 +418,13 @@ __device__ __forceinline__ QuadEdge quad_edge(const QuadDev& q, int nx, int ny, 
     P2 v0, v1;
     if (e < nI) {
         const int i = (int)(e % nx), j = (int)(e / nx);
+        const int gj = gj0 + j;
         g.horizontal = true;
-        g.boundary = j == 0 || j == ny;
-        g.reverse = j == ny;
+        g.boundary = gj == 0 || gj == gny;
+        g.reverse = gj == gny;
         g.L = g.reverse ? (long long)(j - 1) * nx + i : (long long)j * nx + i;
         if (!g.boundary) g.R = (long long)(j - 1) * nx + i;
-        else g.wall = j == 0 ? 0 : 1;
+        else g.wall = gj == 0 ? 0 : 1;
         v0 = vtx(q, nx, i, j); v1 = vtx(q, nx, i + 1, j);
     } else {
         const long long k = e - nI;
@@ -457,12 +467,14 @@ __global__ void __launch_bounds__(128, 3) quad_face_kernel(int nx, int ny, const
                                                         const unsigned char* __restrict__ flags,
                                                         const double* __restrict__ vsn, const double* __restrict__ udn,
                                                         double* __restrict__ face, unsigned long long* status,
-                                                        Physics ph, QuadDev q) {
+                                                        Physics ph, QuadDev q, int gj0, int gny, long long h0,
+                                                        long long nh, long long v0, long long nv) {
     const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nE) return;
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nh + nv) return;
+    const long long e = k < nh ? h0 + k : v0 + (k - nh);
     const size_t N = (size_t)nx * ny;
-    const QuadEdge g = quad_edge(q, nx, ny, e);
+    const QuadEdge g = quad_edge(q, nx, ny, gj0, gny, e);
     double len;
     P2 nrm;
     edge_geometry(g.a, g.b, len, nrm);
@@ -499,7 +511,7 @@ __global__ void __launch_bounds__(128, 3) quad_face_kernel(int nx, int ny, const
         fluxMix += w * pf.vn;
         rate += w * pf.speed;
     }
-    if (st) record_error(status, PART_FACES, g.L, st);
+    if (st) record_error(status, PART_FACES, g.L + (long long)gj0 * nx, st);
     face[e] = fluxH;
     face[nE + e] = fluxC;
     face[2 * nE + e] = rate;
@@ -512,12 +524,15 @@ __global__ void __launch_bounds__(128, 3) quad_face_kernel(int nx, int ny, const
 __global__ void __launch_bounds__(128) quad_diffusion_kernel(int nx, int ny, const double* __restrict__ H,
                                                              const double* __restrict__ C,
                                                              const double* __restrict__ rec, double* __restrict__ face,
-                                                             unsigned long long* status, Physics ph, QuadDev q) {
+                                                             unsigned long long* status, Physics ph, QuadDev q,
+                                                             int gj0, int gny, long long h0, long long nh, long long v0,
+                                                             long long nv) {
     const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nE) return;
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nh + nv) return;
+    const long long e = k < nh ? h0 + k : v0 + (k - nh);
     const size_t N = (size_t)nx * ny;
-    const QuadEdge g = quad_edge(q, nx, ny, e);
+    const QuadEdge g = quad_edge(q, nx, ny, gj0, gny, e);
     const int type = g.boundary ? ph.wall_type[g.wall] : 1;
     if (g.boundary && type == 0) return;
     double len;
@@ -567,29 +582,33 @@ __global__ void __launch_bounds__(128) quad_diffusion_kernel(int nx, int ny, con
             rate += fabs(scale * (s + 1 == count ? clast : c[s]));
         }
     }
-    if (st) record_error(status, PART_FACES, g.L, st);
+    if (st) record_error(status, PART_FACES, g.L + (long long)gj0 * nx, st);
     face[e] += integral;
     face[2 * nE + e] = rate;
 }
 
-// Reconstruction + limiter, cell phase, faces (+ diffusion) of state (H, C)
-// on a general quad mesh; the accumulation is the shared sum kernel.
-void launch_quad_stage(const QuadDev& q, int nx, int ny, const Physics& ph, const double* H, const double* C,
+// Reconstruction, limiter, cell phase, faces (+ diffusion) of state (H, C)
+// on a general quad mesh; the accumulation is the shared sum kernel. Local
+// rows [rec0, rec1) are reconstructed, the edges [h0, h0+nh) and [v0, v0+nv)
+// (those of the advanced rows) get fluxes; local row 0 is global row gj0 of
+// gny (a whole mesh: gj0 = 0, gny = ny).
+void launch_quad_stage(const QuadDev& q, int nx, int ny, int gj0, int gny, int rec0, int rec1, long long h0,
+                       long long nh, long long v0, long long nv, const Physics& ph, const double* H, const double* C,
                        double* rec, unsigned char* flags, double* T, double* phi, const double* vsn, const double* udn,
                        double* face, unsigned long long* status, double* theta, const SourcePtrs& src,
                        cudaStream_t s) {
-    const long long N = (long long)nx * ny;
-    const long long NE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
-    dim3 blk(32, 4), grd((nx + 31) / 32, (ny + 3) / 4);
-    quad_weno_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, status, q);
-    quad_limit_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, flags, status, theta, ph, q);
-    quad_cellphase_kernel<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, flags, T, phi, status, ph, q,
-                                                                      src);
-    quad_face_kernel<<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, flags, vsn, udn, face, status,
-                                                                  ph, q);
+    dim3 blk(32, 4), grd((nx + 31) / 32, (rec1 - rec0 + 3) / 4);
+    quad_weno_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, status, q, gj0, gny, rec0, rec1);
+    quad_limit_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, flags, status, theta, ph, q, gj0, gny, rec0, rec1);
+    const long long c0 = (long long)rec0 * nx, c1 = (long long)rec1 * nx;
+    quad_cellphase_kernel<<<(unsigned)((c1 - c0 + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, flags, T, phi, status,
+                                                                            ph, q, src, gj0, gny, c0, c1);
+    const unsigned ge = (unsigned)((nh + nv + 127) / 128);
+    quad_face_kernel<<<ge, 128, 0, s>>>(nx, ny, H, C, rec, flags, vsn, udn, face, status, ph, q, gj0, gny, h0, nh, v0,
+                                        nv);
     count_launch(4);
     if (ph.diffusion) {
-        quad_diffusion_kernel<<<(unsigned)((NE + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, face, status, ph, q);
+        quad_diffusion_kernel<<<ge, 128, 0, s>>>(nx, ny, H, C, rec, face, status, ph, q, gj0, gny, h0, nh, v0, nv);
         count_launch();
     }
 }

@@ -166,13 +166,16 @@ int validate_quads(int nx, int ny, const double* xy, long long* bad) {
     return MP_OK;
 }
 
-int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables& t) {
+int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables& t, int row0, int rows) {
     if (nx < 2 || ny < 2) return MP_ERR_ARG_SIZ;
-    const size_t N = (size_t)nx * ny;
-    const size_t NI = (size_t)nx * (ny + 1), NE = NI + (size_t)(nx + 1) * ny;
-    t.nx = nx; t.ny = ny;
-    t.xy.assign(xy, xy + 2 * (size_t)(nx + 1) * (ny + 1));
-    const VertexMesh m{nx, ny, t.xy.data()};
+    if (rows < 0) { row0 = 0; rows = ny; }
+    if (row0 < 0 || rows < 1 || row0 + rows > ny) return MP_ERR_ARG_OUTOFRANGE;
+    // Tables of the local rows [row0, row0 + rows) of the global mesh, in local numbering.
+    const size_t N = (size_t)nx * rows;
+    const size_t NI = (size_t)nx * (rows + 1), NE = NI + (size_t)(nx + 1) * rows;
+    t.nx = nx; t.ny = rows;
+    t.xy.assign(xy + 2 * (size_t)row0 * (nx + 1), xy + 2 * (size_t)(row0 + rows + 1) * (nx + 1));
+    const VertexMesh m{nx, ny, xy};
     std::vector<double> p1, w1, gp, gw;
     gauss_legendre(1, p1, w1);
     gauss_legendre(5, gp, gw);
@@ -186,9 +189,10 @@ int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables&
     t.geo.assign(kQGeo * N, 0.0);
     t.spacing.assign(5 * NE, 0.0);
     const int offi[4] = {0, 0, -1, -1}, offj[4] = {-1, 0, -1, 0};
-    int st = parallel_rows(ny, threads, [&](int j) -> int {
+    int st = parallel_rows(rows, threads, [&](int jl) -> int {
+        const int j = row0 + jl;
         for (int i = 0; i < nx; ++i) {
-            const size_t cell = (size_t)j * nx + i;
+            const size_t cell = (size_t)jl * nx + i;
             const Quad target = m.cell(i, j);
             const double area = cell_integral(target, p1, w1, [](V2) { return 1.0; });
             if (!(area > 0) || !std::isfinite(area)) return MP_ERR_ARG_WRONG;
@@ -234,9 +238,10 @@ int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables&
     // Edge spacing in the reference's face orientation (evolve.cpp:230-251):
     // the left cell has the oriented edge counter-clockwise; a wall edge
     // whose canonical left cell is missing is reversed.
-    st = parallel_rows(ny + 1, threads, [&](int j) -> int {
+    st = parallel_rows(rows + 1, threads, [&](int jl) -> int {
+        const int j = row0 + jl;
         for (int i = 0; i < nx; ++i) {           // AlongI edge (i, j)
-            const size_t e = (size_t)j * nx + i;
+            const size_t e = (size_t)jl * nx + i;
             const V2 v0 = m.vert(i, j), v1 = m.vert(i + 1, j);
             double sp[5];
             if (j == ny) {
@@ -248,9 +253,9 @@ int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables&
                 for (int q = 0; q < 5; ++q) t.spacing[e * 5 + q] = sp[q];
             }
         }
-        if (j == ny) return 0;
+        if (jl == rows) return 0;
         for (int i = 0; i <= nx; ++i) {          // AlongJ edge (i, j)
-            const size_t e = NI + (size_t)j * (nx + 1) + i;
+            const size_t e = NI + (size_t)jl * (nx + 1) + i;
             const V2 v0 = m.vert(i, j), v1 = m.vert(i, j + 1);
             double sp[5];
             if (i == 0) {

@@ -51,8 +51,10 @@ int mesh_vertices(int nx, int ny, double x0, double x1, double y0, double y1, in
 // MP_ERR_ARG_WRONG with the first bad cell in *bad.
 int validate_quads(int nx, int ny, const double* xy, long long* bad);
 
-// Build the tables on `threads` host threads (0 = all). Returns 0 or an mp_status.
-int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables& t);
+// Build the tables on `threads` host threads (0 = all): of the whole nx x ny
+// mesh, or (rows >= 0) of its rows [row0, row0 + rows) in local numbering,
+// each cell's stencil taken from the whole mesh. Returns 0 or an mp_status.
+int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables& t, int row0 = 0, int rows = -1);
 
 }  // namespace mp
 

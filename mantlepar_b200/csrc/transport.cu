@@ -318,10 +318,15 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
         sb = SourceBufs{t->cvs_y, t->cud_y, t->srcH, t->srcR, t->srcS};
     }
     if (t->quad) {
+        const StageRange& rg = t->range;
+        const int gny = rg.gny > 0 ? rg.gny : t->ny;
+        const long long nI = (long long)t->nx * (t->ny + 1);
+        const long long h0 = (long long)rg.own0 * t->nx, nh = (long long)(rg.own1 - rg.own0 + 1) * t->nx;
+        const long long v0 = nI + (long long)rg.own0 * (t->nx + 1), nv = (long long)(rg.own1 - rg.own0) * (t->nx + 1);
         timed(t, 0, [&] {
-            launch_quad_stage(t->qdev, t->nx, t->ny, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
-                              t->vsn, t->udn, t->face, t->d_status, theta,
-                              SourcePtrs{sb.cvs_y, sb.cud_y, sb.srcH, sb.srcR, sb.srcS}, s);
+            launch_quad_stage(t->qdev, t->nx, t->ny, rg.gj0, gny, rg.rec0, rg.rec1, h0, nh, v0, nv, t->ph, H, C,
+                              static_cast<double*>(t->rec), t->flags, t->T, t->phi, t->vsn, t->udn, t->face,
+                              t->d_status, theta, SourcePtrs{sb.cvs_y, sb.cud_y, sb.srcH, sb.srcR, sb.srcS}, s);
         });
     } else if (t->mixed) {
         launch_stage_kernels<float>(t->nx, t->ny, t->range, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
@@ -536,8 +541,6 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
                       "quadrilateral (cell %lld)", bad);
             return MP_ERR_ARG_WRONG;
         }
-        const int qs = build_quad_tables(mesh->nx, mesh->ny, xy, 0, qt);
-        if (qs) { set_error("per-cell stencil table construction failed"); return (mp_status)qs; }
     }
     if (slab && !(row_begin >= 0 && row_begin < row_end && row_end <= mesh->ny)) {
         set_error("slab rows [%d, %d) outside [0, %d)", row_begin, row_end, mesh->ny);
@@ -560,6 +563,11 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
         t->range.rec1 = ht > 0 ? t->range.own1 + 1 : t->range.own1;
     } else {
         t->range = whole(mesh->ny);
+    }
+    if (xy) {
+        // Tables of the local rows, each cell's stencil from the whole mesh.
+        const int qs = build_quad_tables(mesh->nx, mesh->ny, xy, 0, qt, t->range.gj0, t->ny);
+        if (qs) { delete t; set_error("per-cell stencil table construction failed"); return (mp_status)qs; }
     }
     t->N = (size_t)t->nx * t->ny;
     t->NE = (size_t)t->nx * (t->ny + 1) + (size_t)(t->nx + 1) * t->ny;
@@ -635,6 +643,13 @@ extern "C" mp_status mp_transport_create_quads(const mp_mesh_desc* mesh, const d
                                                mp_stream_t stream, mp_transport** out) {
     if (!xy) { mp::set_error("null vertex array"); return MP_ERR_ARG_WRONG; }
     return create_impl(mesh, false, 0, 0, opts, stream, out, xy);
+}
+
+extern "C" mp_status mp_transport_create_quads_slab(const mp_mesh_desc* global_mesh, const double* xy, int row_begin,
+                                                    int row_end, const mp_transport_opts* opts, mp_stream_t stream,
+                                                    mp_transport** out) {
+    if (!xy) { mp::set_error("null vertex array"); return MP_ERR_ARG_WRONG; }
+    return create_impl(global_mesh, true, row_begin, row_end, opts, stream, out, xy);
 }
 
 extern "C" mp_status mp_mesh_vertices(const mp_mesh_desc* mesh, int family, double perturbation, unsigned long long seed,

@@ -82,7 +82,10 @@ def device_view(ptr: int, n: int, device: int) -> torch.Tensor:
 class Slab:
     """One row slab of a global mesh on the current GPU."""
 
-    def __init__(self, w: Workload, rows: tuple[int, int], config: TransportConfig | None = None, stream=None):
+    def __init__(self, w: Workload, rows: tuple[int, int], config: TransportConfig | None = None, stream=None,
+                 vertices=None):
+        """vertices: the whole mesh's (nx+1)*(ny+1) (x, y) pairs for a general
+        quad mesh (mp_transport_create_quads_slab); None for the uniform mesh."""
         self._lib = _capi.lib()
         self.w = w
         self.rows = rows
@@ -91,8 +94,14 @@ class Slab:
         opts = self.config.to_c()
         h = C.c_void_p()
         self.stream = stream if stream is not None else torch.cuda.current_stream()
-        _capi.check(self._lib.mp_transport_create_slab(C.byref(mesh), int(rows[0]), int(rows[1]), C.byref(opts),
-                                                        self.stream.cuda_stream, C.byref(h)))
+        if vertices is None:
+            _capi.check(self._lib.mp_transport_create_slab(C.byref(mesh), int(rows[0]), int(rows[1]), C.byref(opts),
+                                                            self.stream.cuda_stream, C.byref(h)))
+        else:
+            xy = np.ascontiguousarray(vertices, dtype=np.float64)
+            _capi.check(self._lib.mp_transport_create_quads_slab(C.byref(mesh), xy.ctypes.data, int(rows[0]),
+                                                                  int(rows[1]), C.byref(opts), self.stream.cuda_stream,
+                                                                  C.byref(h)))
         self._h = h
         lr, r0, o0, o1 = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         _capi.check(self._lib.mp_transport_slab_layout(h, C.byref(lr), C.byref(r0), C.byref(o0), C.byref(o1)))
