@@ -341,7 +341,7 @@ def quads_form(steps, stream, nx=None, ny=None):
     table_gbs = QUAD_TABLE_BYTES_PER_CELL * w.cells * kn[0] / max(kms[0], 1e-9) / 1e6
     return {"value": w.cells * steps / (ms * 1e-3), "unit": "cell-updates/s", "steps": steps, "ms_per_step": ms / steps,
             "retries": sum(r["retries"] for r in reps), "table_setup_s": setup_s,
-            "table_stream_gbs": table_gbs, "table_stream_frac_of_measured_hbm": table_gbs / peaks()[0],
+            "tables_gbs_over_stage": table_gbs, "tables_frac_of_measured_hbm_over_stage": table_gbs / peaks()[0],
             "stage_kernels_ms": {"recon+cellphase+face": kms[0] / max(kn[0], 1), "sum": kms[3] / max(kn[3], 1)},
             "stages": stages,
             "config": f"{w.nx}x{w.ny} perturbed quadrilateral (0.2, seed 11), SSPRK3, CFL 0.4, material S"}

@@ -27,7 +27,7 @@ LIB = os.path.join(HERE, "libmantlepar_b200.so")
 HOST_LIB = os.path.join(HERE, "libmantle_b200_host.so")
 HOST_SOURCES = [os.path.join(HERE, "host", "eutectic_model.cpp"), os.path.join(HERE, "host", "coupled_transport.cpp")]
 
-SOURCES = ["phase_api.cu", "transport.cu", "tables.cpp", "mp_noalloc.cu", "batch.cu", "serve.cpp", "preheat.cu", "quad_tables.cpp"]
+SOURCES = ["phase_api.cu", "transport.cu", "tables.cpp", "mp_noalloc.cu", "batch.cu", "serve.cpp", "preheat.cu", "quad_tables.cpp", "quad_table_kernels.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
          "-I", os.path.join(ROOT, "include")]
@@ -40,9 +40,14 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found: the mantlepar_b200 CUDA library cannot be built")
 
 
+# Per-source flags: the GPU table builder rounds every operation as the host
+# builder does (no FMA contraction).
+SOURCE_FLAGS = {"quad_table_kernels.cu": ["--fmad=false"]}
+
+
 def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
-    cmd = [nvcc()] + ARCH + FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+    cmd = [nvcc()] + ARCH + FLAGS + SOURCE_FLAGS.get(src, []) + ["-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

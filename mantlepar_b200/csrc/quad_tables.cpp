@@ -166,7 +166,8 @@ int validate_quads(int nx, int ny, const double* xy, long long* bad) {
     return MP_OK;
 }
 
-int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables& t, int row0, int rows) {
+int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables& t, int row0, int rows,
+                      bool cell_tables) {
     if (nx < 2 || ny < 2) return MP_ERR_ARG_SIZ;
     if (rows < 0) { row0 = 0; rows = ny; }
     if (row0 < 0 || rows < 1 || row0 + rows > ny) return MP_ERR_ARG_OUTOFRANGE;
@@ -180,16 +181,19 @@ int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables&
     gauss_legendre(1, p1, w1);
     gauss_legendre(5, gp, gw);
     for (int q = 0; q < 5; ++q) { t.gq[q] = gp[q]; t.gw[q] = gw[q]; }
+    for (int q = 0; q < 3; ++q) { t.gq3[q] = gauss_rule_cached(3).first[q]; t.gw3[q] = gauss_rule_cached(3).second[q]; }
+    t.gq1 = p1[0]; t.gw1 = w1[0];
     derivative_weights(4, true, t.dif_c_int);
     derivative_weights(5, false, t.dif_c_bnd);
-    t.G0.assign(kQG0 * N, 0.0);
-    t.S9.assign(kQS9 * N, 0.0);
-    t.T4.assign(kQT4 * N, 0.0);
-    t.S4.assign(kQS4 * N, 0.0);
-    t.geo.assign(kQGeo * N, 0.0);
     t.spacing.assign(5 * NE, 0.0);
+    const size_t NC = cell_tables ? N : 0;
+    t.G0.assign(kQG0 * NC, 0.0);
+    t.S9.assign(kQS9 * NC, 0.0);
+    t.T4.assign(kQT4 * NC, 0.0);
+    t.S4.assign(kQS4 * NC, 0.0);
+    t.geo.assign(kQGeo * NC, 0.0);
     const int offi[4] = {0, 0, -1, -1}, offj[4] = {-1, 0, -1, 0};
-    int st = parallel_rows(rows, threads, [&](int jl) -> int {
+    int st = !cell_tables ? 0 : parallel_rows(rows, threads, [&](int jl) -> int {
         const int j = row0 + jl;
         for (int i = 0; i < nx; ++i) {
             const size_t cell = (size_t)jl * nx + i;

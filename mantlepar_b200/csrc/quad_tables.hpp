@@ -18,6 +18,8 @@
 #ifndef MP_QUAD_TABLES_HPP
 #define MP_QUAD_TABLES_HPP
 
+#include <cuda_runtime.h>
+
 #include <vector>
 
 namespace mp {
@@ -36,6 +38,7 @@ struct QuadTables {
     // canonical point order (diffusiveflux.cpp:255-334, 4 samples, extent 0.9).
     std::vector<double> spacing;
     double gq[5], gw[5];           // Gauss rule on [-1, 1]
+    double gq3[3], gw3[3], gq1, gw1;   // the moment / smoothness and area rules
     double dif_c_int[4], dif_c_bnd[5];
 };
 
@@ -53,8 +56,21 @@ int validate_quads(int nx, int ny, const double* xy, long long* bad);
 
 // Build the tables on `threads` host threads (0 = all): of the whole nx x ny
 // mesh, or (rows >= 0) of its rows [row0, row0 + rows) in local numbering,
-// each cell's stencil taken from the whole mesh. Returns 0 or an mp_status.
-int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables& t, int row0 = 0, int rows = -1);
+// each cell's stencil taken from the whole mesh. cell_tables = false leaves
+// the per-cell arrays (G0, S9, T4, S4, geo) empty: the vertices, the edge
+// spacing, the rules and weights only. Returns 0 or an mp_status.
+int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables& t, int row0 = 0, int rows = -1,
+                      bool cell_tables = true);
+
+// The per-cell arrays of the same tables (identical values: the host
+// builder's arithmetic without FMA contraction) on the GPU, written into the
+// device arrays of ncell = nx * rows cells (layout as QuadTables); d_xy holds
+// the whole mesh's vertices; d_failed is one device int of scratch.
+// Synchronous on `stream`. Returns 0, MP_ERR_ARG_WRONG (a singular stencil
+// or a cell without positive area) or MP_ERR_CUDA.
+int build_quad_cell_tables_gpu(int nx, int ny, const double* d_xy, int row0, int rows, const double* gq3,
+                               const double* gw3, double gq1, double gw1, double* G0, double* S9, double* T4,
+                               double* S4, double* geo, int* d_failed, cudaStream_t stream);
 
 }  // namespace mp
 

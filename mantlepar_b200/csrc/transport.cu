@@ -565,8 +565,9 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
         t->range = whole(mesh->ny);
     }
     if (xy) {
-        // Tables of the local rows, each cell's stencil from the whole mesh.
-        const int qs = build_quad_tables(mesh->nx, mesh->ny, xy, 0, qt, t->range.gj0, t->ny);
+        // Vertices and edge spacing of the local rows on the host; the
+        // per-cell tables are built on the GPU below.
+        const int qs = build_quad_tables(mesh->nx, mesh->ny, xy, 0, qt, t->range.gj0, t->ny, false);
         if (qs) { delete t; set_error("per-cell stencil table construction failed"); return (mp_status)qs; }
     }
     t->N = (size_t)t->nx * t->ny;
@@ -608,24 +609,51 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
     if (e == cudaSuccess) e = cudaMemsetAsync(t->vsn, 0, NE * kNQ * sizeof(double), t->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(t->udn, 0, NE * kNQ * sizeof(double), t->stream);
     if (xy && e == cudaSuccess) {
-        // Per-cell tables of a general quad mesh, one allocation.
+        // Per-cell tables of a general quad mesh, one allocation: vertices of
+        // the local rows and edge spacing from the host, the cell tables
+        // built on the GPU from the whole mesh's vertices.
         const size_t V = qt.xy.size(), NEq = qt.spacing.size();
         const size_t total = V + (size_t)(kQG0 + kQS9 + kQT4 + kQS4 + kQGeo) * N + NEq;
         e = cudaMalloc((void**)&t->qbuf, total * sizeof(double));
         double* at = t->qbuf;
-        auto put = [&](const std::vector<double>& v) -> const double* {
-            if (e == cudaSuccess) e = cudaMemcpyAsync(at, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, t->stream);
-            const double* p = at;
-            at += v.size();
+        auto put = [&](const std::vector<double>* v, size_t n) -> double* {
+            if (v && e == cudaSuccess) e = cudaMemcpyAsync(at, v->data(), n * sizeof(double), cudaMemcpyHostToDevice, t->stream);
+            double* p = at;
+            at += n;
             return p;
         };
         QuadDev& q = t->qdev;
-        q.xy = put(qt.xy); q.G0 = put(qt.G0); q.S9 = put(qt.S9); q.T4 = put(qt.T4); q.S4 = put(qt.S4);
-        q.geo = put(qt.geo); q.sp = put(qt.spacing);
+        double *G0, *S9, *T4, *S4, *geo;
+        q.xy = put(&qt.xy, V);
+        q.G0 = G0 = put(nullptr, (size_t)kQG0 * N);
+        q.S9 = S9 = put(nullptr, (size_t)kQS9 * N);
+        q.T4 = T4 = put(nullptr, (size_t)kQT4 * N);
+        q.S4 = S4 = put(nullptr, (size_t)kQS4 * N);
+        q.geo = geo = put(nullptr, (size_t)kQGeo * N);
+        q.sp = put(&qt.spacing, NEq);
         for (int k = 0; k < 5; ++k) { q.gq[k] = qt.gq[k]; q.gw[k] = qt.gw[k]; q.dif_c_bnd[k] = qt.dif_c_bnd[k]; }
         for (int k = 0; k < 4; ++k) q.dif_c_int[k] = qt.dif_c_int[k];
         t->cell_area = q.geo + 3 * N;
         t->quad = true;
+        double* d_all = nullptr;
+        int* d_failed = nullptr;
+        const size_t VA = 2 * (size_t)(mesh->nx + 1) * (mesh->ny + 1);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&d_all, VA * sizeof(double) + sizeof(int));
+        if (e == cudaSuccess) {
+            d_failed = reinterpret_cast<int*>(d_all + VA);
+            e = cudaMemcpyAsync(d_all, xy, VA * sizeof(double), cudaMemcpyHostToDevice, t->stream);
+        }
+        int gs = MP_OK;
+        if (e == cudaSuccess)
+            gs = build_quad_cell_tables_gpu(mesh->nx, mesh->ny, d_all, t->range.gj0, t->ny, qt.gq3, qt.gw3, qt.gq1,
+                                            qt.gw1, G0, S9, T4, S4, geo, d_failed, t->stream);
+        if (d_all) cudaFree(d_all);
+        if (e == cudaSuccess && gs != MP_OK) {
+            free_all(t); delete t;
+            if (gs == MP_ERR_CUDA) return cuda_status(cudaGetLastError(), "per-cell stencil tables");
+            set_error("per-cell stencil table construction failed (singular stencil or degenerate cell)");
+            return (mp_status)gs;
+        }
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
     if (e != cudaSuccess) { free_all(t); delete t; return cuda_status(e, "mp_transport_create"); }
