@@ -1,6 +1,11 @@
-// Host construction of the per-cell tables of a general quad mesh (see
-// quad_tables.hpp). The geometry and stencil arithmetic is the uniform
-// builder's (geometry.hpp), applied to every cell's own stencil.
+// Host construction of the tables of a general quad mesh (see
+// quad_tables.hpp): the vertices of the local rows and the normal-line
+// sample spacing of every edge (long double ray exits), and -- with
+// cell_tables -- the per-cell tables, whose arithmetic (the uniform
+// builder's, geometry.hpp, applied to every cell's own stencil) the GPU
+// builder in quad_table_kernels.cu reproduces bit for bit; the library
+// builds the per-cell tables on the GPU, and this host form is the one the
+// GPU tables are checked against.
 #include "quad_tables.hpp"
 #include "geometry.hpp"
 

@@ -169,3 +169,22 @@ def test_quad_large_mesh_steps(cuda_lib):
     assert all(abs(r["balanceH"]) < 1e-10 * abs(r["H_integral"]) for r in reps)
     H, C, T, phi = t.get_state()
     assert np.all(np.isfinite(H)) and H.min() >= 0 and C.min() >= 0 and C.max() <= 0.5
+
+
+def test_gpu_tables_equal_host_builder(cuda_lib, tmp_path):
+    """The GPU table builder (no FMA contraction) reproduces the host
+    builder's per-cell candidate matrices, smoothness forms and geometry bit
+    for bit, whole mesh, slab and boundary classes."""
+    import subprocess
+    from mantlepar_b200 import build as B
+    exe = str(tmp_path / "quad_tables_check")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    obj = str(tmp_path / "qtk.o")
+    subprocess.run([B.nvcc()] + B.ARCH + ["-O3", "-std=c++17", "--fmad=false", "-c",
+                    os.path.join(B.CSRC, "quad_table_kernels.cu"), "-o", obj], check=True)
+    subprocess.run([B.nvcc()] + B.ARCH + ["-O3", "-std=c++17", "-I", B.CSRC,
+                    os.path.join(root, "tests", "cpp", "quad_tables_check.cu"), os.path.join(B.CSRC, "quad_tables.cpp"),
+                    obj, "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:]
+    assert "TOTAL DIFFERENT 0" in r.stdout
