@@ -187,3 +187,42 @@ def test_preheat_large_mesh_properties(cuda_lib):
         prev = r["integral"]
     H, time, accepted = p.get_state()
     assert accepted == 20 and np.all(np.isfinite(H))
+
+
+def test_preheat_then_evolve_through_the_handoff_files(cuda_lib, tmp_path):
+    """The reference's workflow (mantle_couple_preheat, then
+    mantle_couple_evolve -preheat DIR): the preheated H and the fixed C go
+    through cellH1.dat / cellC1.dat / transport_state.json bit for bit, and
+    the coupled transport continues from them at the preheat's end time,
+    step for step with the oracle started from the same files."""
+    from oracle import pyoracle as po
+    from mantlepar_b200 import handoff
+    from mantlepar_b200.phase import EutecticModel
+    from mantlepar_b200.transport import Transport, TransportConfig
+    case = pc.CASES["through_diffusion"]
+    w = case.w
+    p = pc.gpu_instance(case)
+    code, _, _, _, _ = p.run()
+    assert code == 0
+    H, time, accepted = p.get_state()
+    _, C = case.state()
+    derived = EutecticModel(sy.material_s()).derived()
+    mesh = handoff.MeshInfo.of(w)
+    handoff.write_state(str(tmp_path), mesh, H, C, time, accepted, derived)
+    H2, C2, t2 = handoff.read_state(str(tmp_path), mesh, derived, sy.material_s().Xe)
+    assert np.array_equal(H2, H) and np.array_equal(C2, C) and t2 == time == case.end
+    t = Transport(w, TransportConfig(cfl=w.cfl, integrator=2))
+    o = po.TransportOracle(sy.material_s(), w, integrator=2)
+    for x in (t, o):
+        x.set_face_velocity(*sy.face_velocity(w))
+        x.set_state(H2, C2, t2)
+    _, got = t.step(3)
+    code, ref = o.step(3)
+    assert code == 0
+    assert all(r["status"] == 0 for r in got)
+    assert got[0]["time"] > t2 and got[-1]["time"] > got[0]["time"]
+    for a, b in zip(got, ref):
+        assert abs(a["time"] - b["time"]) <= 1e-12 * abs(b["time"])
+    a, b = np.stack(t.get_state()), np.stack(o.get_state())
+    for k in range(4):
+        assert rel(a[k], b[k]) <= 1e-11, k
