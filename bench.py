@@ -178,11 +178,12 @@ def cpu_form_baseline(form: str, seconds: float = 6.0, threads: int = 0) -> dict
     kind = "reference" if po.reference_available() else "port"
     lib = po.reference() if kind == "reference" else po.restated()
     w = sy.Workload(**CPU_SAMPLE)
-    if form == "preheat":
+    if form in ("preheat", "preheat_perturbed"):
         _sys.path.insert(0, os.path.join(ROOT, "tests"))
         import preheat_cases as pc
+        quad = dict(family=sy.MESH_PERTURBED, perturbation=0.2, mesh_seed=11) if form == "preheat_perturbed" else {}
         case = pc.PreheatCase(w, through=0.05, kappa=1e-4, thermal_type=(1, 1, 0, 0),
-                              thermal_value=(0.9, 0.2, 0.0, 0.0), end=1e9, dt_initial=1e-4, dt_max=1e-4)
+                              thermal_value=(0.9, 0.2, 0.0, 0.0), end=1e9, dt_initial=1e-4, dt_max=1e-4, **quad)
         t = pc.oracle_instance(case, lib)
         assert t.preheat_begin()[0] == 0
         steps, t0 = 0, time.perf_counter()
@@ -190,7 +191,7 @@ def cpu_form_baseline(form: str, seconds: float = 6.0, threads: int = 0) -> dict
             code, rows = t.preheat_advance(5)
             assert code == 0
             steps += len(rows)
-        sample = f"{w.nx}x{w.ny} sub-instance, {steps} forward-Euler steps"
+        sample = f"{w.nx}x{w.ny}{' perturbed' if quad else ''} sub-instance, {steps} forward-Euler steps"
     else:
         t = po.TransportOracle(sy.material_s(), w, lib=lib, integrator=3, threads=threads, mesh_family=1,
                                perturbation=0.2, mesh_seed=11)
@@ -274,22 +275,30 @@ def timed_steps(obj, steps, stream):
 PREHEAT_BYTES_PER_CELL_STEP = 288
 
 
-def preheat_form(steps, stream, nx=None, ny=None):
-    """The legacy dry preheat on the plain mesh (1280x2560): forward Euler with
-    kappa = 1e-4 and wall temperatures, the synthetic Stokes flow plus an
-    upward through-flow of 0.05 (inflow at the bottom wall); `steps` accepted
-    steps, device-timed on the instance's stream."""
+def preheat_form(steps, stream, nx=None, ny=None, perturbed=False):
+    """The legacy dry preheat on the plain mesh (1280x2560), or on the
+    perturbed-quadrilateral mesh (perturbation 0.2, seed 11) with per-cell
+    tables: forward Euler with kappa = 1e-4 and wall temperatures, the
+    synthetic Stokes flow plus an upward through-flow of 0.05 (inflow at the
+    bottom wall); `steps` accepted steps, device-timed on the instance's
+    stream."""
     import torch
     from mantlepar_b200 import synthetic as sy
     from mantlepar_b200.preheat import Preheat, PreheatConfig
     w = sy.Workload(nx=nx or WORKLOAD["nx"], ny=ny or WORKLOAD["ny"])
-    vs, _ = sy.face_velocity(w)
-    vs = vs.copy()
-    vs[:w.nx * (w.ny + 1)] -= 0.05
+    xy = None
+    if perturbed:
+        xy = sy.quad_vertices(w, sy.MESH_PERTURBED, 0.2, 11)
+        vs, ud = sy.face_velocity_quads(w, xy)
+        vs = vs + 0.05 * (ud / w.darcy)
+    else:
+        vs, _ = sy.face_velocity(w)
+        vs = vs.copy()
+        vs[:w.nx * (w.ny + 1)] -= 0.05
     H, Cc = sy.initial_state(w)
     p = Preheat(w, PreheatConfig(end=1e9, max_steps=1 << 40, dt_initial=1e-4, dt_max=1e-4, cfl=0.5,
                                  diffusivity=1e-4, thermal_type=(1, 1, 0, 0), thermal_value=(0.9, 0.2, 0.0, 0.0)),
-                stream=stream.cuda_stream)
+                stream=stream.cuda_stream, vertices=xy)
     p.set_velocity(vs)
     p.set_state(H, Cc)
     _, limit, _ = p.begin()
@@ -303,19 +312,25 @@ def preheat_form(steps, stream, nx=None, ny=None):
     ms = e0.elapsed_time(e1)
     p.close()
     ms_step = ms / steps
+    nbytes = PREHEAT_BYTES_PER_CELL_STEP + (PREHEAT_QUAD_EXTRA_BYTES if perturbed else 0)
     return {"value": w.cells * steps / (ms * 1e-3), "unit": "cell-updates/s", "steps": steps,
             "ms_per_step": ms_step, "status": code, "accepted": len(rows),
             "max_balance_error": max(abs(r["balanceError"]) for r in rows),
-            "achieved_gbs": PREHEAT_BYTES_PER_CELL_STEP * w.cells / (ms_step * 1e-3) / 1e9,
-            "hbm_frac_of_measured": PREHEAT_BYTES_PER_CELL_STEP * w.cells / (ms_step * 1e-3) / 1e9 / peaks()[0],
-            "bytes_per_cell_step": PREHEAT_BYTES_PER_CELL_STEP,
-            "config": f"{w.nx}x{w.ny}, kappa=1e-4, wall temperatures bottom 0.9 / top 0.2, through-flow 0.05, "
-                      f"dt 1e-4 (rate limit {limit:.3g}), host round trip every 512 steps"}
+            "achieved_gbs": nbytes * w.cells / (ms_step * 1e-3) / 1e9,
+            "hbm_frac_of_measured": nbytes * w.cells / (ms_step * 1e-3) / 1e9 / peaks()[0],
+            "bytes_per_cell_step": nbytes,
+            "config": f"{w.nx}x{w.ny}{' perturbed (0.2, seed 11)' if perturbed else ''}, kappa=1e-4, wall "
+                      f"temperatures bottom 0.9 / top 0.2, through-flow 0.05, dt = min(1e-4, rate limit {limit:.3g}), "
+                      f"host round trip every 512 steps"}
 
 
 # Per-cell tables a stage of the general-quad path streams (G0 72, S9 36,
 # T4 48, S4 24, geometry 4 doubles).
 QUAD_TABLE_BYTES_PER_CELL = 184 * 8
+# What a preheat step on a general quad mesh reads beyond the uniform one:
+# the per-cell tables, the normal-line spacing of the 2 owned edges x 5
+# points, and one vertex (x, y) per cell.
+PREHEAT_QUAD_EXTRA_BYTES = QUAD_TABLE_BYTES_PER_CELL + 2 * 5 * 8 + 16
 
 
 def quads_form(steps, stream, nx=None, ny=None):
@@ -414,9 +429,11 @@ def run_forms(args, stream):
         "retries": sum(r["retries"] for r in reps)}
     tp.close()
     forms["preheat_1280x2560"] = preheat_form(max(args.form_steps, 50), stream)
+    forms["preheat_perturbed_1280x2560"] = preheat_form(max(args.form_steps, 50), stream, perturbed=True)
     forms["perturbed_quads_1280x2560"] = quads_form(args.form_steps, stream)
     if not args.no_cpu_baseline:
         forms["preheat_1280x2560"]["cpu_baseline"] = cpu_form_baseline("preheat")
+        forms["preheat_perturbed_1280x2560"]["cpu_baseline"] = cpu_form_baseline("preheat_perturbed")
         forms["perturbed_quads_1280x2560"]["cpu_baseline"] = cpu_form_baseline("quads")
     # Served: a seeded Poisson stream (200 req/s) of uneven solves, mixed
     # precision, submitted in real time; memory admission against a 64 GiB budget.
@@ -702,6 +719,8 @@ def main():
                     help="time only the legacy dry preheat form (profiling)")
     ap.add_argument("--quads-only", action="store_true",
                     help="time only the perturbed-quadrilateral form (profiling)")
+    ap.add_argument("--perturbed", action="store_true",
+                    help="with --preheat-only: the preheat on the perturbed-quadrilateral mesh")
     ap.add_argument("--decompose", action="store_true",
                     help="one mesh in row slabs across the ranks (strong scaling) instead of one mesh per rank")
     args = ap.parse_args()
@@ -710,7 +729,8 @@ def main():
     if args.preheat_only:
         import torch
         torch.cuda.set_device(local)
-        print(json.dumps({"form": "preheat", **preheat_form(args.steps, torch.cuda.Stream(), args.nx, args.ny)}))
+        print(json.dumps({"form": "preheat_perturbed" if args.perturbed else "preheat",
+                          **preheat_form(args.steps, torch.cuda.Stream(), args.nx, args.ny, args.perturbed)}))
         return
     if args.quads_only:
         import torch

@@ -183,9 +183,10 @@ struct PreheatReport {
 // is dry). Forward Euler from state.time to configuration.time.end with the
 // time controls, thermalDiffusivity, the per-wall thermal conditions, the
 // enthalpy advection rule and the stabilizer of `configuration`; the phase
-// model and pressure give the final T and phi (Diagnostics). Returns 0 or an
-// mp_status; on failure H, time and acceptedSteps hold the last accepted
-// step and the phase fields are not refreshed.
+// model and pressure give the final T and phi (Diagnostics). state.mesh may
+// be a general quad mesh (Mesh::vertices). Returns 0 or an mp_status; on
+// failure H, time and acceptedSteps hold the last accepted step and the
+// phase fields are not refreshed.
 int AdvanceLegacyPreheat(const Configuration& configuration, InitialState& state, const EdgeVelocities& flow,
                          PreheatReport& report);
 

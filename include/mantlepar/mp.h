@@ -185,7 +185,7 @@ void mp_transport_destroy(mp_transport* t);
  * "perturbed_quadrilateral"), or any logically rectangular mesh of convex
  * quads. xy holds the (nx+1)*(ny+1) vertices, x fastest, as (x, y) pairs;
  * mesh gives nx, ny and the domain. Every cell gets its own reconstruction
- * tables (built on the host at create, TensorStencilPoly::Initialize and
+ * tables (built at create, TensorStencilPoly::Initialize and
  * SetTargetSmoothness per stencil, src/mlweno/tensorstencilpoly.cpp:146-231,
  * 383-398) and every evaluation point its own geometry. FP64 only; cells
  * failing the reference's quad check (src/core/quad_validation.h) ->
@@ -349,6 +349,14 @@ typedef struct mp_preheat mp_preheat;
 
 mp_status mp_preheat_create(const mp_mesh_desc* mesh, const mp_preheat_opts* opts, mp_stream_t stream,
                             mp_preheat** out);
+/* The preheat on a general quad mesh (the reference's Build and RHS read
+ * each face's and cell's own corners, preheat.cpp:86-117,166-196, so its
+ * preheat runs on every mesh family): xy as mp_transport_create_quads,
+ * per-cell reconstruction tables, physical edge lengths, normal-line
+ * spacing per edge point and per-cell areas. Same calls and results
+ * otherwise; invalid quads -> MP_ERR_ARG_WRONG. */
+mp_status mp_preheat_create_quads(const mp_mesh_desc* mesh, const double* xy, const mp_preheat_opts* opts,
+                                  mp_stream_t stream, mp_preheat** out);
 void mp_preheat_destroy(mp_preheat* p);
 /* Stokes velocity at the edge Gauss points: normal components [edge*5 + q]
  * in the canonical order of this header (the x component on AlongJ edges,

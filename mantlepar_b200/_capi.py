@@ -177,6 +177,7 @@ def lib() -> C.CDLL:
         "mp_transport_create_quads_slab": (i, [C.POINTER(MeshDesc), vp, i, i, C.POINTER(TransportOpts), vp,
                                                C.POINTER(vp)]),
         "mp_preheat_create": (i, [C.POINTER(MeshDesc), C.POINTER(PreheatOpts), vp, C.POINTER(vp)]),
+        "mp_preheat_create_quads": (i, [C.POINTER(MeshDesc), vp, C.POINTER(PreheatOpts), vp, C.POINTER(vp)]),
         "mp_preheat_destroy": (None, [vp]),
         "mp_preheat_set_velocity": (i, [vp, vp]),
         "mp_preheat_set_state": (i, [vp, vp, vp, d, C.c_longlong]),

@@ -16,10 +16,18 @@
 // The step sizes do not depend on the state (the rate is fixed at Build), so
 // the host plans a batch of steps and issues them without waiting; a failed
 // step sets the status word and every kernel queued after it returns at once.
+//
+// On a general quad mesh (mp_preheat_create_quads; the reference's preheat
+// runs on any mesh family, preheat.cpp:86-117) the reconstruction, face,
+// rate and diagnostics kernels have quad forms that read the per-cell
+// tables, map every point from the cell's corners and use physical edge
+// lengths, normal-line spacing per edge point and per-cell areas.
 #include "common.hpp"
 #include "phase_math.cuh"
 #include "stage_device.cuh"
 #include "stage_kernels.cuh"
+#include "quad_device.cuh"
+#include "quad_tables.hpp"
 #include "tables.hpp"
 
 #include <algorithm>
@@ -287,7 +295,10 @@ __global__ void __launch_bounds__(128) pre_face_kernel(int nx, int ny, const dou
 // Per-cell sum of the face fluxes (faces bottom, top, left, right in id order,
 // each with its side's sign, preheat.cpp:195-197), the forward-Euler
 // candidate and the step's checks (preheat.cpp:267-273).
+// kQuad: per-cell areas (general quad mesh) instead of the uniform one.
+template <bool kQuad>
 __global__ void __launch_bounds__(kPreBlock) pre_update_kernel(int nx, int ny, double area, double inv_area,
+                                                                const double* __restrict__ cell_area,
                                                                 const double* __restrict__ H, const double* __restrict__ flux,
                                                                 double* __restrict__ Hout, double* __restrict__ rhs,
                                                                 int mode, double dt, int row, PreRow* rows,
@@ -303,12 +314,17 @@ __global__ void __launch_bounds__(kPreBlock) pre_update_kernel(int nx, int ny, d
         if (cell >= N) continue;
         const double h = __ldg(H + cell);
         double cand = h;
+        double a = area;
+        if constexpr (kQuad) a = __ldg(cell_area + cell);
         if (mode != PRE_MEASURE) {
             const int i = (int)(cell % nx), j = (int)(cell / nx);
             const long long eb = (long long)j * nx + i, et = eb + nx;
             const long long el = nI + (long long)j * (nx + 1) + i, er = el + 1;
             const double fb = __ldg(flux + eb), ft = __ldg(flux + et), fl = __ldg(flux + el), fr = __ldg(flux + er);
-            const double r = (((-fb) + (j == ny - 1 ? -ft : ft)) + (i == 0 ? -fl : fl) - fr) * inv_area;
+            const double sum = ((-fb) + (j == ny - 1 ? -ft : ft)) + (i == 0 ? -fl : fl) - fr;
+            double r;
+            if constexpr (kQuad) r = sum / a;
+            else r = sum * inv_area;
             double b = 0.0;
             if (j == 0) b += fb;
             if (j == ny - 1) b += ft;
@@ -321,7 +337,7 @@ __global__ void __launch_bounds__(kPreBlock) pre_update_kernel(int nx, int ny, d
                 Hout[cell] = cand;
             }
         }
-        v.integral += cand * area;
+        v.integral += cand * a;
         v.minimum = fmin(v.minimum, cand);
         v.maximum = fmax(v.maximum, cand);
         v.nonfinite = fmax(v.nonfinite, isfinite(cand) ? 0.0 : 1.0);
@@ -474,6 +490,236 @@ __global__ void __launch_bounds__(128) pre_diag_kernel(int nx, int ny, const dou
     phi[cell] = Ps;
 }
 
+// ------------------------------------------------- general quad mesh forms
+
+// H-only reconstruction with the cell's own tables, without the limiter.
+__global__ void __launch_bounds__(128, 4) pre_quad_recon_kernel(int nx, int ny, const double* __restrict__ H,
+                                                                double* __restrict__ rec, unsigned long long* status,
+                                                                QuadDev q) {
+    if (halted(status)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= nx || j >= ny) return;
+    const long long cell = (long long)j * nx + i;
+    const size_t N = (size_t)nx * ny;
+    const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
+    const double eA = 1e-2 * __ldg(q.geo + 3 * N + cell);
+    double u[3][3];
+#pragma unroll
+    for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+        for (int di = 0; di < 3; ++di) {
+            const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
+            u[dj][di] = __ldg(H + (size_t)jj * nx + ii);
+        }
+    double D[9];
+    const int st = reconstruct_quad(q, N, cell, ci, cj, eA, u, D);
+#pragma unroll
+    for (int m = 0; m < 9; ++m) rec[(size_t)m * N + cell] = D[m];
+    if (st) record_error(status, PART_UPDATE, cell, st);
+}
+
+// One side of an edge: the cell's frame and its H polynomial.
+struct PreSide {
+    double cx, cy, inv_h, m;
+    double D[9];
+};
+__device__ __forceinline__ void pre_side(const QuadDev& q, size_t N, const double* H, const double* rec, long long cell,
+                                         PreSide& s) {
+    s.cx = __ldg(q.geo + cell);
+    s.cy = __ldg(q.geo + N + cell);
+    s.inv_h = 1.0 / __ldg(q.geo + 2 * N + cell);
+    s.m = __ldg(H + cell);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s.D[k] = __ldg(rec + (size_t)k * N + cell);
+}
+__device__ __forceinline__ double pre_trace(const PreSide& s, P2 p) {
+    return s.m + q2v(s.D, (p.x - s.cx) * s.inv_h, (p.y - s.cy) * s.inv_h);
+}
+
+// Edge flux of preheat.cpp:166-196 on a general quad mesh: the traces at the
+// edge's Gauss points in each side's frame, the linear-law Lax-Friedrichs
+// flux or the boundary policy with weights L w_q / 2, and the diffusion of
+// the cell averages with the normal-line spacing of each edge point.
+__global__ void __launch_bounds__(128) pre_quad_face_kernel(int nx, int ny, const double* __restrict__ H,
+                                                            const double* __restrict__ rec,
+                                                            const double* __restrict__ vn, double* __restrict__ flux,
+                                                            unsigned long long* status,
+                                                            const __grid_constant__ PreheatPhys pp, QuadDev q) {
+    if (halted(status)) return;
+    const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nE) return;
+    const size_t N = (size_t)nx * ny;
+    const QuadEdge g = quad_edge(q, nx, ny, 0, ny, e);
+    double len;
+    P2 nrm;
+    edge_geometry(g.a, g.b, len, nrm);
+    PreSide sl, sr;
+    pre_side(q, N, H, rec, g.L, sl);
+    if (!g.boundary) pre_side(q, N, H, rec, g.R, sr);
+    const double mL = sl.m, mR = g.boundary ? mL : sr.m;
+    const double sgn = g.reverse ? -1.0 : 1.0;
+    int st = 0;
+    double sum = 0.0;
+#pragma unroll
+    for (int k = 0; k < kNQ; ++k) {
+        const int cq = g.reverse ? kNQ - 1 - k : k;
+        const P2 p = lerp_edge(q.gq[k], g.a, g.b);
+        const double v = sgn * __ldg(vn + e * kNQ + cq);
+        const double uL = pre_trace(sl, p);
+        if (!isfinite(v) || !isfinite(uL)) st = st ? st : E_OUTOFRANGE;
+        double f;
+        if (g.boundary) {
+            if (pp.Hpol == MP_BC_ZERO_FLUX || v == 0.0) f = 0.0;
+            else if (v < 0.0) {
+                if (pp.Hpol != MP_BC_INFLOW_OUTFLOW) st = st ? st : E_OUTOFRANGE;
+                f = v * pp.inflowH;
+            } else f = v * uL;
+        } else {
+            const double uR = pre_trace(sr, p);
+            if (!isfinite(uR)) st = st ? st : E_OUTOFRANGE;
+            const double a = pp.lf_global ? pp.lf_speed : fabs(v);
+            if (!speed_bounds(a, fabs(v))) st = st ? st : E_OUTOFRANGE;
+            f = 0.5 * (v * uL + v * uR - a * (uR - uL));
+        }
+        if (!isfinite(f)) st = st ? st : E_FP;
+        sum += 0.5 * len * q.gw[k] * f;
+    }
+    if (pp.diffusion) {
+        // Interior samples [L, L, R, R], wall samples [L, L, L, L, wall
+        // value]; gradient sum_k c_k (v_k - v_last) / spacing at each point.
+        const int type = g.boundary ? pp.wall_type[g.wall] : MP_THERMAL_TEMPERATURE;
+        const double wv = g.boundary ? pp.wall_value[g.wall] : 0.0;
+        if (type == MP_THERMAL_FLUX) {
+#pragma unroll
+            for (int k = 0; k < kNQ; ++k) sum += len * q.gw[k] / 2 * wv;
+        } else if (type == MP_THERMAL_TEMPERATURE) {
+            double integral = 0.0;
+#pragma unroll
+            for (int k = 0; k < kNQ; ++k) {
+                const int cq = g.reverse ? kNQ - 1 - k : k;
+                const double sp = __ldg(q.sp + e * kNQ + cq);
+                double grad = 0.0;
+                if (g.boundary) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) grad += q.dif_c_bnd[c] * (mL - wv);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) grad += q.dif_c_int[c] * ((c < 2 ? mL : mR) - mR);
+                }
+                grad /= sp;
+                if (!isfinite(grad)) st = st ? st : E_FP;
+                integral -= len * q.gw[k] / 2 * pp.kappa * grad;
+            }
+            sum += integral;
+        }
+    }
+    flux[e] = sum;
+    if (st) record_error(status, PART_FACES, e, st);
+}
+
+// Build (preheat.cpp:130-156) on a general quad mesh: per edge the LF speed
+// sum_q L w_q alpha / 2 and the diffusion derivatives at zero samples per
+// side; (speed + |derivative|) / area of the left [e] and right [NE + e] cell.
+__global__ void __launch_bounds__(128) pre_quad_rate_edge_kernel(int nx, int ny, const double* __restrict__ vn,
+                                                                 double* __restrict__ rr, unsigned long long* status,
+                                                                 const __grid_constant__ PreheatPhys pp, QuadDev q) {
+    const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nE) return;
+    const size_t N = (size_t)nx * ny;
+    const QuadEdge g = quad_edge(q, nx, ny, 0, ny, e);
+    double len;
+    P2 nrm;
+    edge_geometry(g.a, g.b, len, nrm);
+    int st = 0;
+    double speed = 0.0;
+#pragma unroll
+    for (int k = 0; k < kNQ; ++k) {
+        const int cq = g.reverse ? kNQ - 1 - k : k;
+        const double v = __ldg(vn + e * kNQ + cq);
+        const double ns = fabs(v);
+        if (!isfinite(v)) st = E_OUTOFRANGE;
+        const double a = pp.lf_global ? pp.lf_speed : ns;
+        if (!(a + 1e-14 >= ns)) st = E_OUTOFRANGE;
+        speed = __dadd_rn(speed, __dmul_rn(__dmul_rn(__dmul_rn(0.5, len), q.gw[k]), a));
+    }
+    double d0 = 0.0, d1 = 0.0;
+    const int type = g.boundary ? pp.wall_type[g.wall] : MP_THERMAL_TEMPERATURE;
+    if (type == MP_THERMAL_TEMPERATURE) {
+        double clast = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) clast -= q.dif_c_int[c];
+#pragma unroll
+        for (int k = 0; k < kNQ; ++k) {
+            const int cq = g.reverse ? kNQ - 1 - k : k;
+            const double sp = __ldg(q.sp + e * kNQ + cq);
+            const double scale = -(len * q.gw[k] / 2) * pp.kappa / sp;
+            if (g.boundary) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) d0 += scale * q.dif_c_bnd[c];
+            } else {
+                d0 += scale * q.dif_c_int[0];
+                d0 += scale * q.dif_c_int[1];
+                d1 += scale * q.dif_c_int[2];
+                d1 += scale * clast;
+            }
+        }
+    }
+    const double aL = __ldg(q.geo + 3 * N + g.L), aR = g.boundary ? aL : __ldg(q.geo + 3 * N + g.R);
+    rr[e] = (speed + fabs(d0)) / aL;
+    rr[nE + e] = (speed + fabs(d1)) / aR;
+    if (st) record_error(status, PART_FACES, e, st);
+}
+
+// Diagnostics (preheat.cpp:202-233) on a general quad mesh: the unlimited
+// reconstructions of H and C and the 5x5 quadrature of T and phi on the
+// bilinear map, weights w_a w_b J / area.
+__global__ void __launch_bounds__(128) pre_quad_diag_kernel(int nx, int ny, const double* __restrict__ H,
+                                                            const double* __restrict__ C, double* __restrict__ T,
+                                                            double* __restrict__ phi, unsigned long long* status,
+                                                            Physics ph, QuadDev q) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= nx || j >= ny) return;
+    const long long cell = (long long)j * nx + i;
+    const size_t N = (size_t)nx * ny;
+    const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
+    const CellFrame f = cell_frame(q, nx, N, cell);
+    const double eA = 1e-2 * f.area;
+    double D[2][9];
+    double m[2];
+    int st = 0;
+    for (int fi = 0; fi < 2; ++fi) {
+        const double* F = fi ? C : H;
+        double u[3][3];
+        for (int dj = 0; dj < 3; ++dj)
+            for (int di = 0; di < 3; ++di) {
+                const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
+                u[dj][di] = __ldg(F + (size_t)jj * nx + ii);
+            }
+        m[fi] = u[1][1];
+        const int s = reconstruct_quad(q, N, cell, ci, cj, eA, u, D[fi]);
+        st = st ? st : s;
+    }
+    if (st) { record_error(status, PART_UPDATE, cell, st); return; }
+    double Ts = 0.0, Ps = 0.0;
+    for (int b = 0; b < kNQ; ++b)
+        for (int a = 0; a < kNQ; ++a) {
+            const P2 p = bilinear(q.gq[a], q.gq[b], f.c);
+            const double x = (p.x - f.cx) * f.inv_h, y = (p.y - f.cy) * f.inv_h;
+            const double tep = ph.litho ? tep_at(ph, p.y) : ph.Tep;
+            PhaseLean pl;
+            const int s = phase_stage_lean(ph.sk, m[0] + q2v(D[0], x, y), m[1] + q2v(D[1], x, y), tep, pl);
+            if (s) { st = st ? st : s; continue; }
+            const double w = q.gw[a] * q.gw[b] * jacobian(q.gq[a], q.gq[b], f.c) / f.area;
+            Ts += w * pl.T;
+            Ps += w * pl.phil;
+        }
+    if (st) record_error(status, PART_CELLS, cell, st);
+    T[cell] = Ts;
+    phi[cell] = Ps;
+}
+
 }  // namespace
 }  // namespace mp
 
@@ -508,6 +754,10 @@ struct mp_preheat {
     bool ready = false;             // begin() done for the current state
     double rate_max = 0.0, limit = 0.0;
     unsigned int acc_seen = 0;      // ctl->accepted after the last batch
+    // General quad mesh (mp_preheat_create_quads): per-cell tables in HBM.
+    bool quad = false;
+    mp::QuadDev qdev{};
+    double* qbuf = nullptr;         // one allocation holding every table
 };
 
 namespace mp {
@@ -517,7 +767,7 @@ constexpr int kBatch = 512;         // steps issued per host round trip
 
 void pre_free(mp_preheat* p) {
     void* bufs[] = {p->Hb[0], p->Hb[1], p->C, p->rec, p->vn, p->flux, p->rr, p->rate, p->rhs, p->T, p->phi,
-                    p->partial, p->ctl, p->rows, p->d_status};
+                    p->partial, p->ctl, p->rows, p->d_status, p->qbuf};
     for (void* b : bufs) if (b) cudaFree(b);
     if (p->h_ctl) cudaFreeHost(p->h_ctl);
     if (p->h_rows) cudaFreeHost(p->h_rows);
@@ -555,6 +805,14 @@ mp_status read_status(mp_preheat* p) {
 // The three kernels of one RHS evaluation / step on state Hb[src].
 void launch_rhs_kernels(mp_preheat* p, const double* H) {
     const int nx = p->nx, ny = p->ny;
+    if (p->quad) {
+        dim3 blk(32, 4), grd((nx + 31) / 32, (ny + 3) / 4);
+        pre_quad_recon_kernel<<<grd, blk, 0, p->stream>>>(nx, ny, H, p->rec, p->d_status, p->qdev);
+        pre_quad_face_kernel<<<(unsigned)((p->NE + 127) / 128), 128, 0, p->stream>>>(nx, ny, H, p->rec, p->vn, p->flux,
+                                                                                     p->d_status, p->pp, p->qdev);
+        count_launch(2);
+        return;
+    }
     {
         dim3 blk(32, 4), grd((nx + 31) / 32, (ny + 3) / 4);
         pre_recon_kernel<<<grd, blk, 0, p->stream>>>(nx, ny, H, p->rec, p->d_status, p->ptab);
@@ -565,9 +823,15 @@ void launch_rhs_kernels(mp_preheat* p, const double* H) {
 }
 
 void launch_update(mp_preheat* p, const double* H, double* Hout, int mode, double dt, int row) {
-    pre_update_kernel<<<p->blocks, kPreBlock, 0, p->stream>>>(p->nx, p->ny, p->host_tab.area, 1.0 / p->host_tab.area,
-                                                             H, p->flux, Hout, p->rhs, mode, dt, row, p->rows,
-                                                             p->partial, p->ctl, p->d_status);
+    if (p->quad)
+        pre_update_kernel<true><<<p->blocks, kPreBlock, 0, p->stream>>>(p->nx, p->ny, 0.0, 0.0, p->qdev.geo + 3 * p->N,
+                                                                       H, p->flux, Hout, p->rhs, mode, dt, row,
+                                                                       p->rows, p->partial, p->ctl, p->d_status);
+    else
+        pre_update_kernel<false><<<p->blocks, kPreBlock, 0, p->stream>>>(p->nx, p->ny, p->host_tab.area,
+                                                                        1.0 / p->host_tab.area, nullptr, H, p->flux,
+                                                                        Hout, p->rhs, mode, dt, row, p->rows,
+                                                                        p->partial, p->ctl, p->d_status);
     count_launch();
 }
 
@@ -598,8 +862,9 @@ mp_status plan_step(const mp_preheat* p, double time, long long steps, double& d
 
 // -------------------------------------------------------------------- C ABI
 
-extern "C" mp_status mp_preheat_create(const mp_mesh_desc* mesh, const mp_preheat_opts* opts, mp_stream_t stream,
-                                       mp_preheat** out) {
+namespace {
+mp_status preheat_create_impl(const mp_mesh_desc* mesh, const double* xy, const mp_preheat_opts* opts,
+                              mp_stream_t stream, mp_preheat** out) {
     using namespace mp;
     if (!mesh || !opts || !out) { set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (mesh->nx < 2 || mesh->ny < 2) { set_error("Preheat requires at least 2x2 cells"); return MP_ERR_ARG_SIZ; }
@@ -623,6 +888,19 @@ extern "C" mp_status mp_preheat_create(const mp_mesh_desc* mesh, const mp_prehea
         }
     mp_derived der;
     MP_TRY(derive_checked(opts->material, der));
+    QuadTables qt;
+    if (xy) {
+        long long bad = -1;
+        if (validate_quads(mesh->nx, mesh->ny, xy, &bad)) {
+            set_error("Mesh has non-real/non-finite coordinates or an inverted, degenerate, or nearly singular "
+                      "quadrilateral (cell %lld)", bad);
+            return MP_ERR_ARG_WRONG;
+        }
+        // Vertices and edge spacing on the host; the per-cell tables are
+        // built on the GPU below.
+        const int qs = build_quad_tables(mesh->nx, mesh->ny, xy, 0, qt, 0, mesh->ny, false);
+        if (qs) { set_error("per-cell stencil table construction failed"); return (mp_status)qs; }
+    }
     mp_preheat* p = new mp_preheat;
     p->mesh = *mesh; p->opts = *opts; p->der = der;
     p->stream = (cudaStream_t)stream;
@@ -659,9 +937,11 @@ extern "C" mp_status mp_preheat_create(const mp_mesh_desc* mesh, const mp_prehea
     }
     pp.Hpol = opts->H_policy; pp.inflowH = opts->inflow_H;
     pp.lf_global = opts->lf_global; pp.lf_speed = opts->lf_global_speed;
-    const int tb = build_stage_tables(mesh->nx, mesh->ny, mesh->x0, mesh->x1, mesh->y0, mesh->y1, p->host_tab);
-    if (tb) { delete p; set_error("stencil table construction failed"); return (mp_status)tb; }
-    make_param_tables(p->host_tab, p->ptab);
+    if (!xy) {
+        const int tb = build_stage_tables(mesh->nx, mesh->ny, mesh->x0, mesh->x1, mesh->y0, mesh->y1, p->host_tab);
+        if (tb) { delete p; set_error("stencil table construction failed"); return (mp_status)tb; }
+        make_param_tables(p->host_tab, p->ptab);
+    }
     p->blocks = (int)((p->N + kPreCells - 1) / kPreCells);
     const size_t N = p->N, NE = p->NE;
     cudaError_t e = cudaSuccess;
@@ -681,10 +961,31 @@ extern "C" mp_status mp_preheat_create(const mp_mesh_desc* mesh, const mp_prehea
     if (e == cudaSuccess) e = cudaMemsetAsync(p->vn, 0, NE * kNQ * sizeof(double), p->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(p->ctl, 0, sizeof(PreCtl), p->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(p->d_status, 0xff, sizeof(unsigned long long), p->stream);
+    if (xy && e == cudaSuccess) {
+        const int gs = upload_quad_tables(p->nx, p->ny, xy, qt, 0, p->ny, p->stream, &p->qbuf, p->qdev, &e);
+        p->quad = true;
+        if (gs == MP_ERR_ARG_WRONG) {
+            pre_free(p); delete p;
+            set_error("per-cell stencil table construction failed (singular stencil or degenerate cell)");
+            return (mp_status)gs;
+        }
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
     if (e != cudaSuccess) { pre_free(p); delete p; return cuda_status(e, "mp_preheat_create"); }
     *out = p;
     return MP_OK;
+}
+}  // namespace
+
+extern "C" mp_status mp_preheat_create(const mp_mesh_desc* mesh, const mp_preheat_opts* opts, mp_stream_t stream,
+                                       mp_preheat** out) {
+    return preheat_create_impl(mesh, nullptr, opts, stream, out);
+}
+
+extern "C" mp_status mp_preheat_create_quads(const mp_mesh_desc* mesh, const double* xy, const mp_preheat_opts* opts,
+                                             mp_stream_t stream, mp_preheat** out) {
+    if (!xy) { mp::set_error("null vertex array"); return MP_ERR_ARG_WRONG; }
+    return preheat_create_impl(mesh, xy, opts, stream, out);
 }
 
 extern "C" void mp_preheat_destroy(mp_preheat* p) {
@@ -734,9 +1035,13 @@ extern "C" mp_status mp_preheat_begin(mp_preheat* p, double* rate, double* limit
     p->ready = false;
     if (!(p->time <= p->opts.end)) { set_error("State time exceeds time.end"); return MP_ERR_ARG_OUTOFRANGE; }
     MP_TRY(reset_status(p));
-    pre_rate_edge_kernel<<<(unsigned)((p->NE + 127) / 128), 128, 0, p->stream>>>(p->nx, p->ny, p->host_tab.area,
-                                                                                 p->vn, p->rr, p->d_status, p->pp,
-                                                                                 p->ptab);
+    if (p->quad)
+        pre_quad_rate_edge_kernel<<<(unsigned)((p->NE + 127) / 128), 128, 0, p->stream>>>(p->nx, p->ny, p->vn, p->rr,
+                                                                                          p->d_status, p->pp, p->qdev);
+    else
+        pre_rate_edge_kernel<<<(unsigned)((p->NE + 127) / 128), 128, 0, p->stream>>>(p->nx, p->ny, p->host_tab.area,
+                                                                                     p->vn, p->rr, p->d_status, p->pp,
+                                                                                     p->ptab);
     pre_rate_cell_kernel<<<p->blocks, kPreBlock, 0, p->stream>>>(p->nx, p->ny, p->rr, p->rate, p->partial, p->ctl);
     count_launch(2);
     MP_CUDA(cudaGetLastError());
@@ -847,8 +1152,12 @@ extern "C" mp_status mp_preheat_diagnostics(mp_preheat* p, double* T, double* ph
     if (!p) { set_error("null argument"); return MP_ERR_ARG_WRONG; }
     MP_TRY(reset_status(p));
     dim3 blk(32, 4), grd((p->nx + 31) / 32, (p->ny + 3) / 4);
-    pre_diag_kernel<<<grd, blk, 0, p->stream>>>(p->nx, p->ny, p->Hb[p->cur], p->C, p->T, p->phi, p->d_status, p->ph,
-                                                p->ptab);
+    if (p->quad)
+        pre_quad_diag_kernel<<<grd, blk, 0, p->stream>>>(p->nx, p->ny, p->Hb[p->cur], p->C, p->T, p->phi, p->d_status,
+                                                         p->ph, p->qdev);
+    else
+        pre_diag_kernel<<<grd, blk, 0, p->stream>>>(p->nx, p->ny, p->Hb[p->cur], p->C, p->T, p->phi, p->d_status,
+                                                    p->ph, p->ptab);
     count_launch();
     MP_CUDA(cudaGetLastError());
     MP_TRY(read_status(p));

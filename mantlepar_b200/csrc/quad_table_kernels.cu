@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <vector>
 
 #include "../../include/mantlepar/mp.h"
 
@@ -261,6 +262,56 @@ int build_quad_cell_tables_gpu(int nx, int ny, const double* d_xy, int row0, int
     if (cudaMemcpyAsync(&failed, d_failed, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess) return MP_ERR_CUDA;
     if (cudaStreamSynchronize(stream) != cudaSuccess) return MP_ERR_CUDA;
     return failed ? MP_ERR_ARG_WRONG : MP_OK;
+}
+
+int upload_quad_tables(int nx, int ny, const double* xy, const QuadTables& qt, int row0, int rows,
+                       cudaStream_t stream, double** buf, QuadDev& q, cudaError_t* cuda_err) {
+    cudaError_t e = cudaSuccess;
+    *buf = nullptr;
+    const size_t N = (size_t)nx * rows;
+    const size_t V = qt.xy.size(), NEq = qt.spacing.size();
+    const size_t total = V + (size_t)(kQG0 + kQS9 + kQT4 + kQS4 + kQGeo) * N + NEq;
+    e = cudaMalloc((void**)buf, total * sizeof(double));
+    double* at = *buf;
+    auto put = [&](const std::vector<double>* v, size_t n) -> double* {
+        if (v && e == cudaSuccess) e = cudaMemcpyAsync(at, v->data(), n * sizeof(double), cudaMemcpyHostToDevice, stream);
+        double* p = at;
+        at += n;
+        return p;
+    };
+    double *G0, *S9, *T4, *S4, *geo;
+    q.xy = put(&qt.xy, V);
+    q.G0 = G0 = put(nullptr, (size_t)kQG0 * N);
+    q.S9 = S9 = put(nullptr, (size_t)kQS9 * N);
+    q.T4 = T4 = put(nullptr, (size_t)kQT4 * N);
+    q.S4 = S4 = put(nullptr, (size_t)kQS4 * N);
+    q.geo = geo = put(nullptr, (size_t)kQGeo * N);
+    q.sp = put(&qt.spacing, NEq);
+    for (int k = 0; k < 5; ++k) { q.gq[k] = qt.gq[k]; q.gw[k] = qt.gw[k]; q.dif_c_bnd[k] = qt.dif_c_bnd[k]; }
+    for (int k = 0; k < 4; ++k) q.dif_c_int[k] = qt.dif_c_int[k];
+    // The whole mesh's vertices and the failure flag, for the builder only.
+    double* d_all = nullptr;
+    int* d_failed = nullptr;
+    const size_t VA = 2 * (size_t)(nx + 1) * (ny + 1);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d_all, VA * sizeof(double) + sizeof(int));
+    if (e == cudaSuccess) {
+        d_failed = reinterpret_cast<int*>(d_all + VA);
+        e = cudaMemcpyAsync(d_all, xy, VA * sizeof(double), cudaMemcpyHostToDevice, stream);
+    }
+    int gs = MP_OK;
+    if (e == cudaSuccess)
+        gs = build_quad_cell_tables_gpu(nx, ny, d_all, row0, rows, qt.gq3, qt.gw3, qt.gq1, qt.gw1, G0, S9, T4, S4, geo,
+                                        d_failed, stream);
+    if (gs == MP_ERR_CUDA) {
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaErrorUnknown;
+    }
+    if (d_all) cudaFree(d_all);
+    if (e != cudaSuccess) {
+        if (cuda_err) *cuda_err = e;
+        return MP_ERR_CUDA;
+    }
+    return gs;
 }
 
 }  // namespace mp

@@ -42,6 +42,20 @@ struct QuadTables {
     double dif_c_int[4], dif_c_bnd[5];
 };
 
+// Device pointers of a QuadTables (SoA per cell; spacing per edge and point)
+// and the mesh-wide Gauss rule and derivative weights.
+struct QuadDev {
+    const double* xy;
+    const double* G0;
+    const double* S9;
+    const double* T4;
+    const double* S4;
+    const double* geo;
+    const double* sp;
+    double gq[5], gw[5];
+    double dif_c_int[4], dif_c_bnd[5];
+};
+
 // Vertices of the reference's mesh families (src/core/mesh.cpp:27-55):
 // 0 rectangular, 1 perturbed quadrilateral (interior vertices displaced by
 // perturbation * spacing * SplitMix64 noise keyed by seed), 2 sine-stretched.
@@ -71,6 +85,17 @@ int build_quad_tables(int nx, int ny, const double* xy, int threads, QuadTables&
 int build_quad_cell_tables_gpu(int nx, int ny, const double* d_xy, int row0, int rows, const double* gq3,
                                const double* gw3, double gq1, double gw1, double* G0, double* S9, double* T4,
                                double* S4, double* geo, int* d_failed, cudaStream_t stream);
+
+// One device allocation *buf (cudaMalloc; the caller frees it, after a
+// failure too) holding the tables of local rows [row0, row0 + rows) of a
+// general quad mesh: the vertices and edge spacing of qt (built with
+// cell_tables = false) copied from the host, and the per-cell arrays built
+// on the GPU from the whole mesh's vertices xy (host memory). Fills q with
+// the device pointers, the rules and the derivative weights. Synchronous on
+// `stream`. Returns 0, MP_ERR_ARG_WRONG (a singular stencil or a cell
+// without positive area) or MP_ERR_CUDA with the CUDA error in *cuda_err.
+int upload_quad_tables(int nx, int ny, const double* xy, const QuadTables& qt, int row0, int rows,
+                       cudaStream_t stream, double** buf, QuadDev& q, cudaError_t* cuda_err);
 
 }  // namespace mp
 

@@ -612,45 +612,12 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
         // Per-cell tables of a general quad mesh, one allocation: vertices of
         // the local rows and edge spacing from the host, the cell tables
         // built on the GPU from the whole mesh's vertices.
-        const size_t V = qt.xy.size(), NEq = qt.spacing.size();
-        const size_t total = V + (size_t)(kQG0 + kQS9 + kQT4 + kQS4 + kQGeo) * N + NEq;
-        e = cudaMalloc((void**)&t->qbuf, total * sizeof(double));
-        double* at = t->qbuf;
-        auto put = [&](const std::vector<double>* v, size_t n) -> double* {
-            if (v && e == cudaSuccess) e = cudaMemcpyAsync(at, v->data(), n * sizeof(double), cudaMemcpyHostToDevice, t->stream);
-            double* p = at;
-            at += n;
-            return p;
-        };
-        QuadDev& q = t->qdev;
-        double *G0, *S9, *T4, *S4, *geo;
-        q.xy = put(&qt.xy, V);
-        q.G0 = G0 = put(nullptr, (size_t)kQG0 * N);
-        q.S9 = S9 = put(nullptr, (size_t)kQS9 * N);
-        q.T4 = T4 = put(nullptr, (size_t)kQT4 * N);
-        q.S4 = S4 = put(nullptr, (size_t)kQS4 * N);
-        q.geo = geo = put(nullptr, (size_t)kQGeo * N);
-        q.sp = put(&qt.spacing, NEq);
-        for (int k = 0; k < 5; ++k) { q.gq[k] = qt.gq[k]; q.gw[k] = qt.gw[k]; q.dif_c_bnd[k] = qt.dif_c_bnd[k]; }
-        for (int k = 0; k < 4; ++k) q.dif_c_int[k] = qt.dif_c_int[k];
-        t->cell_area = q.geo + 3 * N;
+        const int gs = upload_quad_tables(mesh->nx, mesh->ny, xy, qt, t->range.gj0, t->ny, t->stream, &t->qbuf, t->qdev,
+                                          &e);
+        t->cell_area = t->qdev.geo + 3 * N;
         t->quad = true;
-        double* d_all = nullptr;
-        int* d_failed = nullptr;
-        const size_t VA = 2 * (size_t)(mesh->nx + 1) * (mesh->ny + 1);
-        if (e == cudaSuccess) e = cudaMalloc((void**)&d_all, VA * sizeof(double) + sizeof(int));
-        if (e == cudaSuccess) {
-            d_failed = reinterpret_cast<int*>(d_all + VA);
-            e = cudaMemcpyAsync(d_all, xy, VA * sizeof(double), cudaMemcpyHostToDevice, t->stream);
-        }
-        int gs = MP_OK;
-        if (e == cudaSuccess)
-            gs = build_quad_cell_tables_gpu(mesh->nx, mesh->ny, d_all, t->range.gj0, t->ny, qt.gq3, qt.gw3, qt.gq1,
-                                            qt.gw1, G0, S9, T4, S4, geo, d_failed, t->stream);
-        if (d_all) cudaFree(d_all);
-        if (e == cudaSuccess && gs != MP_OK) {
+        if (gs == MP_ERR_ARG_WRONG) {
             free_all(t); delete t;
-            if (gs == MP_ERR_CUDA) return cuda_status(cudaGetLastError(), "per-cell stencil tables");
             set_error("per-cell stencil table construction failed (singular stencil or degenerate cell)");
             return (mp_status)gs;
         }

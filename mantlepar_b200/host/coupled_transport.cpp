@@ -277,7 +277,8 @@ int AdvanceLegacyPreheat(const Configuration& c, InitialState& state, const Edge
     const int control = control_of(c.time);
     if (control < 0) return MP_ERR_ARG_OUTOFRANGE;
     const Mesh mesh = state.mesh;
-    if (!mesh.vertices.empty()) return MP_ERR_ARG_WRONG;   // the preheat kernels take rectangular meshes
+    if (!mesh.vertices.empty() && mesh.vertices.size() != 2 * (size_t)(mesh.nx + 1) * (mesh.ny + 1))
+        return MP_ERR_ARG_SIZ;
     const size_t ncell = (size_t)mesh.nx * mesh.ny;
     if (state.enthalpy.size() != ncell || state.composition.size() != ncell) return MP_ERR_ARG_SIZ;
     if (flow.solid.size() != (size_t)EdgeCount(mesh) * 5) return MP_ERR_ARG_SIZ;
@@ -306,7 +307,8 @@ int AdvanceLegacyPreheat(const Configuration& c, InitialState& state, const Edge
     o.lf_global_speed = c.stabilizer.globalSpeed;
     const mp_mesh_desc d{mesh.nx, mesh.ny, mesh.x0, mesh.x1, mesh.y0, mesh.y1};
     mp_preheat* h = nullptr;
-    mp_status st = mp_preheat_create(&d, &o, nullptr, &h);
+    mp_status st = mesh.vertices.empty() ? mp_preheat_create(&d, &o, nullptr, &h)
+                                         : mp_preheat_create_quads(&d, mesh.vertices.data(), &o, nullptr, &h);
     if (st != MP_OK) return st;
     auto finish = [&](mp_status s) { mp_preheat_destroy(h); return (int)s; };
     st = mp_preheat_set_velocity(h, flow.solid.data());

@@ -82,7 +82,9 @@ class Preheat:
 
     CFL, FIXED = 0, 1
 
-    def __init__(self, w: Workload, config: PreheatConfig | None = None, stream=None):
+    def __init__(self, w: Workload, config: PreheatConfig | None = None, stream=None, vertices=None):
+        """vertices: (nx+1)*(ny+1) (x, y) pairs of a general quad mesh
+        (mp_preheat_create_quads); None for the uniform mesh of w."""
         self._lib = _capi.lib()
         self.w = w
         self.config = config or PreheatConfig()
@@ -90,7 +92,12 @@ class Preheat:
         opts = self.config.to_c()
         h = C.c_void_p()
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
-        _capi.check(self._lib.mp_preheat_create(C.byref(mesh), C.byref(opts), s, C.byref(h)))
+        if vertices is None:
+            _capi.check(self._lib.mp_preheat_create(C.byref(mesh), C.byref(opts), s, C.byref(h)))
+        else:
+            xy = np.ascontiguousarray(vertices, dtype=np.float64)
+            _capi.check(self._lib.mp_preheat_create_quads(C.byref(mesh), xy.ctypes.data, C.byref(opts), s,
+                                                           C.byref(h)))
         self._h = h
 
     def close(self):

@@ -6,7 +6,8 @@
 //                   thermal type[4] value[4] H_policy(0 inflow/outflow,
 //                   1 outflow, 2 zero flux) inflow_H lf_global lf_speed
 //                   pressure_model(0 constant, 1 lithostatic) surface_y,
-//                   then H[N] C[N] vs[5E]
+//                   has_vertices(0, 1) 0, then H[N] C[N] vs[5E] and, with
+//                   has_vertices, the (nx+1)*(ny+1) (x, y) vertex pairs
 // output (doubles): status, time, acceptedSteps, rows, H[N] T[N] phi[N],
 //                   rows x (step time dt courant integral minimum maximum
 //                   boundaryFlux balanceError), the six report scalars;
@@ -59,6 +60,11 @@ int main(int argc, char** argv) {
     v.solid.resize(E);
     if (std::fread(s.enthalpy.data(), 8, N, f) != N || std::fread(s.composition.data(), 8, N, f) != N ||
         std::fread(v.solid.data(), 8, E, f) != E) return 2;
+    if (h[28] == 1) {
+        const size_t V = 2 * (size_t)(m.nx + 1) * (m.ny + 1);
+        s.mesh.vertices.resize(V);
+        if (std::fread(s.mesh.vertices.data(), 8, V, f) != V) return 2;
+    }
     std::fclose(f);
 
     PreheatReport rep;

@@ -33,12 +33,27 @@ class PreheatCase:
     cfl: float = 0.5
     pressure_model: int = 0                   # 0 constant (0 Pa), 1 lithostatic
     surface_y: float = 1.1
+    family: int = 0                           # MESH_RECTANGULAR / PERTURBED / SINE
+    perturbation: float = 0.0
+    mesh_seed: int = 11
+
+    def vertices(self):
+        """Vertices of a general quad mesh (None on the uniform mesh)."""
+        if self.family == sy.MESH_RECTANGULAR:
+            return None
+        return sy.quad_vertices(self.w, self.family, self.perturbation, self.mesh_seed)
 
     def velocity(self) -> np.ndarray:
         """Normal Stokes velocity at the edge Gauss points, [edge, q]."""
+        nI = self.w.nx * (self.w.ny + 1)
+        if self.family != sy.MESH_RECTANGULAR:
+            # The through-flow (0, through) against each edge's own normal.
+            vs, ud = sy.face_velocity_quads(self.w, self.vertices())
+            vs = vs + self.through * (ud / self.w.darcy)
+            vs[:self.w.nx] += self.bottom_outflow
+            return np.ascontiguousarray(vs)
         vs, _ = sy.face_velocity(self.w)
         vs = vs.copy()
-        nI = self.w.nx * (self.w.ny + 1)
         vs[:nI] += -self.through                # upward: v . (0, -1)
         vs[:self.w.nx] += self.bottom_outflow   # bottom wall: (0, -1) is outward
         return np.ascontiguousarray(vs)
@@ -57,6 +72,21 @@ CASES = {
                                 pressure_model=1),
     "tiny_2x2": PreheatCase(sy.Workload(nx=2, ny=2, seed=4), through=0.2, kappa=3e-3, end=0.02,
                             thermal_type=(1, 2, 1, 0), thermal_value=(1.0, -0.01, 0.5, 0.0)),
+    # General quad meshes (the reference's preheat reads every face's and
+    # cell's own corners, preheat.cpp:86-117).
+    "quad_through": PreheatCase(sy.Workload(nx=9, ny=7, seed=3), through=0.3, kappa=2e-3,
+                                thermal_type=(1, 1, 0, 2), thermal_value=(1.2, 0.1, 0.0, 0.05),
+                                family=sy.MESH_PERTURBED, perturbation=0.2),
+    "quad_sine_fixed": PreheatCase(sy.Workload(nx=8, ny=6, seed=11), through=0.1, kappa=1e-3, lf_global=1,
+                                   lf_global_speed=1.5, control=1, dt_initial=1e-3, end=0.006,
+                                   thermal_type=(2, 1, 1, 0), thermal_value=(-0.02, 0.3, 0.7, 0.0),
+                                   pressure_model=1, family=sy.MESH_SINE_STRETCHED),
+    "quad_outflow": PreheatCase(sy.Workload(nx=6, ny=9, seed=21, noise_H=0.08), bottom_outflow=0.2, kappa=5e-4,
+                                H_policy=1, thermal_type=(1, 0, 2, 2), thermal_value=(0.4, 0.0, 0.01, -0.01),
+                                end=0.02, family=sy.MESH_PERTURBED, perturbation=0.24),
+    "quad_2x2": PreheatCase(sy.Workload(nx=2, ny=2, seed=8), through=0.2, kappa=3e-3, end=0.02,
+                            thermal_type=(1, 2, 1, 0), thermal_value=(1.0, -0.01, 0.5, 0.0),
+                            family=sy.MESH_PERTURBED, perturbation=0.2),
 }
 
 
@@ -65,7 +95,10 @@ def oracle_instance(case: PreheatCase, lib=None):
     from oracle import pyoracle as po
     t = po.TransportOracle(sy.material_s(), case.w, lib=lib, H_policy=case.H_policy, inflow_H=case.inflow_H,
                            lf_global=case.lf_global, lf_global_speed=case.lf_global_speed, cfl=case.cfl,
-                           dt_initial=case.dt_initial, dt_max=case.dt_max, dt_min=case.dt_min)
+                           dt_initial=case.dt_initial, dt_max=case.dt_max, dt_min=case.dt_min,
+                           mesh_family=case.family, perturbation=case.perturbation, mesh_seed=case.mesh_seed)
+    if case.family != sy.MESH_RECTANGULAR:
+        assert np.array_equal(t.vertices(), case.vertices())
     vs = case.velocity()
     t.set_face_velocity(vs, np.zeros_like(vs))
     H, C = case.state()
@@ -108,7 +141,7 @@ def gpu_config(case: PreheatCase):
 
 def gpu_instance(case: PreheatCase):
     from mantlepar_b200.preheat import Preheat
-    p = Preheat(case.w, gpu_config(case))
+    p = Preheat(case.w, gpu_config(case), vertices=case.vertices())
     p.set_velocity(case.velocity())
     H, C = case.state()
     p.set_state(H, C)

@@ -114,11 +114,12 @@ def preheat_driver(cuda_lib, tmp_path_factory):
     return exe
 
 
-@pytest.mark.parametrize("name", ["through_diffusion", "global_fixed"])
+@pytest.mark.parametrize("name", ["through_diffusion", "global_fixed", "quad_through"])
 def test_advance_legacy_preheat_matches_reference(preheat_driver, tmp_path, name):
     """AdvanceLegacyPreheat and WritePreheatHistory (src/couple/preheat.cpp:
-    235-312) through the C++ layer: rows, final H, T and phi within 1e-12 of
-    the reference-backed golden run; the CSV holds the reference's columns."""
+    235-312) through the C++ layer, on uniform and perturbed meshes: rows,
+    final H, T and phi within 1e-12 of the reference-backed golden run; the
+    CSV holds the reference's columns."""
     import preheat_cases as pc
     from mantlepar_b200.preheat import HISTORY_COLUMNS
     case = pc.CASES[name]
@@ -127,10 +128,11 @@ def test_advance_legacy_preheat_matches_reference(preheat_driver, tmp_path, name
     head = np.array([w.nx, w.ny, w.x0, w.x1, w.y0, w.y1, case.end, case.control, case.dt_initial, case.dt_min,
                      case.dt_max, case.cfl, case.max_steps, case.kappa, *case.thermal_type, *case.thermal_value,
                      case.H_policy, case.inflow_H, case.lf_global, case.lf_global_speed, case.pressure_model,
-                     case.surface_y, 0.0, 0.0], float)
+                     case.surface_y, 0.0 if case.family == 0 else 1.0, 0.0], float)
     assert head.size == 30
     inp, out, csv = str(tmp_path / "in.bin"), str(tmp_path / "out.bin"), str(tmp_path / "preheat_history.csv")
-    np.concatenate([head, H, C, np.ravel(case.velocity())]).tofile(inp)
+    xy = case.vertices()
+    np.concatenate([head, H, C, np.ravel(case.velocity())] + ([] if xy is None else [xy])).tofile(inp)
     subprocess.run([preheat_driver, inp, out, csv], check=True, capture_output=True, text=True, timeout=300)
     d = np.fromfile(out)
     n = w.cells

@@ -226,3 +226,57 @@ def test_preheat_then_evolve_through_the_handoff_files(cuda_lib, tmp_path):
     a, b = np.stack(t.get_state()), np.stack(o.get_state())
     for k in range(4):
         assert rel(a[k], b[k]) <= 1e-11, k
+
+
+def test_preheat_quads_on_a_rectangular_mesh_match_the_uniform_form(cuda_lib):
+    """mp_preheat_create_quads given the vertices of the uniform mesh runs the
+    per-cell-table kernels; every row, the final H and the diagnostics agree
+    with the uniform kernels to roundoff."""
+    from mantlepar_b200.preheat import Preheat
+    case = pc.CASES["through_diffusion"]
+    a = pc.gpu_instance(case)
+    b = Preheat(case.w, pc.gpu_config(case), vertices=sy.quad_vertices(case.w, sy.MESH_RECTANGULAR))
+    b.set_velocity(case.velocity())
+    b.set_state(*case.state())
+    ra, la, fa = a.begin()
+    rb, lb, fb = b.begin()
+    assert rel(rb, ra) <= RTOL and abs(lb - la) <= RTOL * la
+    ca, rows_a = a.advance(1000)
+    cb, rows_b = b.advance(1000)
+    assert ca == cb == 0 and len(rows_a) == len(rows_b)
+    for x, y in zip(rows_a, rows_b):
+        assert x["step"] == y["step"] and x["time"] == y["time"]
+        assert abs(x["integral"] - y["integral"]) <= RTOL * abs(y["integral"])
+    assert rel(b.get_state()[0], a.get_state()[0]) <= RTOL
+    for x, y in zip(b.diagnostics(), a.diagnostics()):
+        assert rel(x, y) <= RTOL if np.max(y) > 0 else np.all(x == 0)
+
+
+def test_preheat_rejects_invalid_quads(cuda_lib):
+    from mantlepar_b200._capi import MPError
+    from mantlepar_b200.preheat import Preheat
+    w = sy.Workload(nx=4, ny=4)
+    xy = sy.quad_vertices(w, sy.MESH_RECTANGULAR).reshape(5, 5, 2).copy()
+    xy[2, 2] = xy[3, 3] + [0.01, 0.01]          # fold one interior vertex past its neighbour
+    with pytest.raises(MPError) as e:
+        Preheat(w, pc.gpu_config(pc.PreheatCase(w)), vertices=xy.reshape(-1))
+    assert e.value.code == 62
+
+
+def test_preheat_quad_large_mesh_properties(cuda_lib):
+    """1280x2560 perturbed-quadrilateral mesh, closed box, 10 steps: the heat
+    balance of every row holds, the boundary flux is zero and the heat
+    integral is conserved to roundoff."""
+    w = sy.Workload(nx=1280, ny=2560)
+    case = pc.PreheatCase(w, kappa=1e-5, end=1.0, dt_max=1e-4, family=sy.MESH_PERTURBED, perturbation=0.2)
+    p = pc.gpu_instance(case)
+    _, limit, first = p.begin()
+    code, rows = p.advance(10)
+    assert code == 0 and len(rows) == 10
+    prev = first["integral"]
+    for r in rows:
+        assert r["boundaryFlux"] == 0.0
+        assert abs(r["integral"] - prev) <= 1e-12 * abs(prev)
+        prev = r["integral"]
+    H, _, accepted = p.get_state()
+    assert accepted == 10 and np.all(np.isfinite(H))
