@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(128) pre_face_kernel(int nx, int ny, const dou
         double f;
         if (g.boundary) {
             // EvaluateAdvectionBoundary (initialization.cpp:469-489) and the
-            // physical boundary flux (advectiveflux.cpp:227-267).
+            // physical boundary flux (advectiveflux.cpp:229-271).
             if (pp.Hpol == MP_BC_ZERO_FLUX || v == 0.0) f = 0.0;
             else if (v < 0.0) {
                 if (pp.Hpol != MP_BC_INFLOW_OUTFLOW) st = st ? st : E_OUTOFRANGE;
