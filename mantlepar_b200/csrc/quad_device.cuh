@@ -194,6 +194,153 @@ __device__ __forceinline__ int reconstruct_quad(const QuadDev& q, size_t N, long
     return st;
 }
 
+// Both fields' deviation polynomials (H and C share the cell's stencils,
+// so they share its tables) with one read of every table entry: per field
+// the operations and their order are those of reconstruct_quad, so DH and DC
+// equal two reconstruct_quad calls bit for bit. Returns the first failure
+// in field order (H, then C).
+__device__ __forceinline__ int reconstruct_quad2(const QuadDev& q, size_t N, long long cell, int ci, int cj,
+                                                 double eA, const double (&uH)[3][3], const double (&uC)[3][3],
+                                                 double (&DH)[9], double (&DC)[9]) {
+    double dH[3][3], dC[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            dH[a][b] = uH[a][b] - uH[1][1];
+            dC[a][b] = uC[a][b] - uC[1][1];
+        }
+    const int offi[4] = {0, 0, -1, -1}, offj[4] = {-1, 0, -1, 0};
+    bool on[5];
+    on[0] = (ci == 1 && cj == 1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        on[k + 1] = !((offi[k] == 0 && ci == 2) || (offi[k] == -1 && ci == 0) || (offj[k] == 0 && cj == 2) ||
+                      (offj[k] == -1 && cj == 0));
+    double sgH[5], sgC[5];
+    int stH = 0, stC = 0;
+    auto fast_ok = [](double v) { return v >= 0.0 && v < INFINITY; };
+    if (on[0]) {
+        double fH[8], fC[8];
+#pragma unroll
+        for (int c = 1; c < 9; ++c) {
+            fH[c - 1] = dH[c / 3][c % 3] - dH[0][0];
+            fC[c - 1] = dC[c / 3][c % 3] - dC[0][0];
+        }
+        auto SF = [&](int k) { return __ldg(q.S9 + (size_t)k * N + cell); };
+        auto S = [&](int r, int c) { const double v = SF(fold_at(8, r, c)); return r == c ? v : 0.5 * v; };
+        // The FMA chains of smoothness<double, 8> for both fields.
+        double sumH = 0, sumC = 0;
+        int k = 0;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const double s0 = SF(k++);
+            double tH = s0 * fH[r], tC = s0 * fC[r];
+#pragma unroll
+            for (int c = r + 1; c < 8; ++c) {
+                const double sv = SF(k++);
+                tH = fma(sv, fH[c], tH);
+                tC = fma(sv, fC[c], tC);
+            }
+            sumH = fma(fH[r], tH, sumH);
+            sumC = fma(fC[r], tC, sumC);
+        }
+        sgH[0] = fast_ok(sumH) ? sumH : smoothness<double, 8>(SF, S, fH);
+        sgC[0] = fast_ok(sumC) ? sumC : smoothness<double, 8>(SF, S, fC);
+        if (sgH[0] < 0.0) stH = MP_ERR_FP;
+        if (sgC[0] < 0.0) stC = MP_ERR_FP;
+    } else {
+        sgH[0] = 0;
+        sgC[0] = 0;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!on[k + 1]) { sgH[k + 1] = 0; sgC[k + 1] = 0; continue; }
+        const int oi = offi[k], oj = offj[k];
+        const double aH = dH[1 + oj][1 + oi], aC = dC[1 + oj][1 + oi];
+        double fH[3], fC[3];
+#pragma unroll
+        for (int c = 1; c < 4; ++c) {
+            fH[c - 1] = dH[1 + oj + c / 2][1 + oi + c % 2] - aH;
+            fC[c - 1] = dC[1 + oj + c / 2][1 + oi + c % 2] - aC;
+        }
+        auto SF = [&](int m) { return __ldg(q.S4 + (size_t)(k * 6 + m) * N + cell); };
+        auto S = [&](int r, int c) { const double v = SF(fold_at(3, r, c)); return r == c ? v : 0.5 * v; };
+        double sumH = 0, sumC = 0;
+        int m = 0;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            const double s0 = SF(m++);
+            double tH = s0 * fH[r], tC = s0 * fC[r];
+#pragma unroll
+            for (int c = r + 1; c < 3; ++c) {
+                const double sv = SF(m++);
+                tH = fma(sv, fH[c], tH);
+                tC = fma(sv, fC[c], tC);
+            }
+            sumH = fma(fH[r], tH, sumH);
+            sumC = fma(fC[r], tC, sumC);
+        }
+        sgH[k + 1] = fast_ok(sumH) ? sumH : smoothness<double, 3>(SF, S, fH);
+        sgC[k + 1] = fast_ok(sumC) ? sumC : smoothness<double, 3>(SF, S, fC);
+        if (sgH[k + 1] < 0.0) stH = MP_ERR_FP;
+        if (sgC[k + 1] < 0.0) stC = MP_ERR_FP;
+    }
+    double wH[5], wC[5];
+    weights<double>(sgH, on, eA, wH);
+    weights<double>(sgC, on, eA, wC);
+    if (!isfinite(wH[0] + wH[1] + wH[2] + wH[3] + wH[4])) stH = MP_ERR_FP;
+    if (!isfinite(wC[0] + wC[1] + wC[2] + wC[3] + wC[4])) stC = MP_ERR_FP;
+#pragma unroll
+    for (int m = 0; m < 9; ++m) { DH[m] = 0; DC[m] = 0; }
+    if (on[0]) {
+        double fH[8], fC[8];
+#pragma unroll
+        for (int c = 1; c < 9; ++c) {
+            fH[c - 1] = dH[c / 3][c % 3] - dH[0][0];
+            fC[c - 1] = dC[c / 3][c % 3] - dC[0][0];
+        }
+#pragma unroll
+        for (int m = 0; m < 9; ++m) {
+            double vH = m == 0 ? dH[0][0] : 0.0, vC = m == 0 ? dC[0][0] : 0.0;
+#pragma unroll
+            for (int c = 1; c < 9; ++c) {
+                const double g = __ldg(q.G0 + (size_t)((c - 1) * 9 + m) * N + cell);
+                vH += fH[c - 1] * g;
+                vC += fC[c - 1] * g;
+            }
+            DH[m] = wH[0] * vH;
+            DC[m] = wC[0] * vC;
+        }
+    }
+    const int slot[4] = {0, 1, 3, 4};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!on[k + 1]) continue;
+        const int oi = offi[k], oj = offj[k];
+        const double aH = dH[1 + oj][1 + oi], aC = dC[1 + oj][1 + oi];
+        double fH[3], fC[3];
+#pragma unroll
+        for (int c = 1; c < 4; ++c) {
+            fH[c - 1] = dH[1 + oj + c / 2][1 + oi + c % 2] - aH;
+            fC[c - 1] = dC[1 + oj + c / 2][1 + oi + c % 2] - aC;
+        }
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) {
+            double vH = mm == 0 ? aH : 0.0, vC = mm == 0 ? aC : 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const double t = __ldg(q.T4 + (size_t)(k * 12 + c * 4 + mm) * N + cell);
+                vH += fH[c] * t;
+                vC += fC[c] * t;
+            }
+            DH[slot[mm]] += wH[k + 1] * vH;
+            DC[slot[mm]] += wC[k + 1] * vC;
+        }
+    }
+    return stH ? stH : stC;
+}
+
 // Left/right cells and oriented vertices of edge e (evolve.cpp:230-251).
 struct QuadEdge {
     bool horizontal, boundary, reverse;

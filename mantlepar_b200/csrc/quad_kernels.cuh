@@ -35,11 +35,11 @@ struct SourcePtrs {
 // ------------------------------------------------------------------ kernels
 
 // Reconstruction (Reconstruction::Update, src/mlweno/reconstruction.cpp:
-// 275-355) of H and C with the cell's own tables: the unlimited deviation
-// polynomials into rec. The limiter runs in the next kernel, so that neither
+// 275-355) of H and C with the cell's own tables, each table entry read once
+// for both fields: the unlimited deviation polynomials into rec. The limiter runs in the next kernel, so that neither
 // kernel holds both the table-driven weights and the point scan in
 // registers (the table reads need many warps in flight).
-__global__ void __launch_bounds__(128, 4) quad_weno_kernel(int nx, int ny, const double* __restrict__ H,
+__global__ void __launch_bounds__(128, 3) quad_weno_kernel(int nx, int ny, const double* __restrict__ H,
                                                            const double* __restrict__ C, double* __restrict__ rec,
                                                            unsigned long long* status, QuadDev q, int gj0, int gny,
                                                            int jlo, int jhi) {
@@ -50,23 +50,21 @@ __global__ void __launch_bounds__(128, 4) quad_weno_kernel(int nx, int ny, const
     const int gj = gj0 + j;
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = gj == 0 ? 0 : (gj == gny - 1 ? 2 : 1);
     const double eA = 1e-2 * __ldg(q.geo + 3 * N + cell);
-    int st = 0;
+    double uH[3][3], uC[3][3];
 #pragma unroll
-    for (int fi = 0; fi < 2; ++fi) {
-        const double* F = fi ? C : H;
-        double u[3][3];
+    for (int dj = 0; dj < 3; ++dj)
 #pragma unroll
-        for (int dj = 0; dj < 3; ++dj)
+        for (int di = 0; di < 3; ++di) {
+            const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
+            uH[dj][di] = __ldg(H + (size_t)jj * nx + ii);
+            uC[dj][di] = __ldg(C + (size_t)jj * nx + ii);
+        }
+    double DH[9], DC[9];
+    const int st = reconstruct_quad2(q, N, cell, ci, cj, eA, uH, uC, DH, DC);
 #pragma unroll
-            for (int di = 0; di < 3; ++di) {
-                const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
-                u[dj][di] = __ldg(F + (size_t)jj * nx + ii);
-            }
-        double D[9];
-        const int s1 = reconstruct_quad(q, N, cell, ci, cj, eA, u, D);
-        st = st ? st : s1;
-#pragma unroll
-        for (int m = 0; m < 9; ++m) rec[(size_t)(m + 9 * fi) * N + cell] = D[m];
+    for (int m = 0; m < 9; ++m) {
+        rec[(size_t)m * N + cell] = DH[m];
+        rec[(size_t)(m + 9) * N + cell] = DC[m];
     }
     if (st) record_error(status, PART_UPDATE, cell + (long long)gj0 * nx, st);
 }
