@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(128) pre_recon_kernel(int nx, int ny, const do
 }
 
 // Edge flux of preheat.cpp:166-196: advection + diffusion of H.
-__global__ void __launch_bounds__(128) pre_face_kernel(int nx, int ny, const double* __restrict__ H,
+__global__ void __launch_bounds__(128, 8) pre_face_kernel(int nx, int ny, const double* __restrict__ H,
                                                        const double* __restrict__ rec, const double* __restrict__ vn,
                                                        double* __restrict__ flux, unsigned long long* status,
                                                        const __grid_constant__ PreheatPhys pp,

@@ -226,7 +226,7 @@ __device__ __forceinline__ void side_values(const Side& s, P2 p, double& h, doub
 }
 
 // Face fluxes, edge porosity and rate of one edge at its 5 Gauss points.
-__global__ void __launch_bounds__(128, 3) quad_face_kernel(int nx, int ny, const double* __restrict__ H,
+__global__ void __launch_bounds__(128, 4) quad_face_kernel(int nx, int ny, const double* __restrict__ H,
                                                         const double* __restrict__ C, const double* __restrict__ rec,
                                                         const unsigned char* __restrict__ flags,
                                                         const double* __restrict__ vsn, const double* __restrict__ udn,
