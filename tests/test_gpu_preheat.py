@@ -117,6 +117,9 @@ def test_preheat_advance_in_pieces(cuda_lib):
 
 
 def _failure(**kw):
+    kw.setdefault("family", sy.MESH_RECTANGULAR)
+    if kw["family"] != sy.MESH_RECTANGULAR:
+        kw.setdefault("perturbation", 0.2)
     case = pc.PreheatCase(sy.Workload(nx=6, ny=6, seed=2), **kw)
     ref = pc.oracle_run(case)
     p = pc.gpu_instance(case)
@@ -133,22 +136,23 @@ def _failure(**kw):
     return ref, out, p
 
 
-def test_preheat_failures_match_reference(cuda_lib):
+@pytest.mark.parametrize("family", [sy.MESH_RECTANGULAR, sy.MESH_PERTURBED], ids=["uniform", "perturbed"])
+def test_preheat_failures_match_reference(cuda_lib, family):
     # Backflow through an outflow-only wall.
-    ref, out, _ = _failure(through=0.3, H_policy=1)
+    ref, out, _ = _failure(through=0.3, H_policy=1, family=family)
     assert out["run"] == ref["run"] == 63 and out["rows"] == []
     # A fixed step above the rate limit.
-    ref, out, _ = _failure(control=1, dt_initial=1.0, end=2.0)
+    ref, out, _ = _failure(control=1, dt_initial=1.0, end=2.0, family=family)
     assert out["run"] == ref["run"] == 63
     # maximumSteps: the allowed steps are kept, then NOT_CONVERGED.
-    ref, out, p = _failure(max_steps=3, end=1.0, dt_max=1e-3)
+    ref, out, p = _failure(max_steps=3, end=1.0, dt_max=1e-3, family=family)
     assert out["run"] == ref["run"] == 91 and len(out["rows"]) == 3
     H, time, accepted = p.get_state()
     assert accepted == 3 and abs(time - ref["rows"][-1]["time"]) <= 1e-15
     assert rel(H, ref["H"]) <= RTOL
     # State time after time.end; a global LF speed below a flow speed.
-    assert _failure(end=-1.0)[1]["begin"] == 63
-    assert _failure(through=0.3, lf_global=1, lf_global_speed=0.01)[1]["begin"] == 63
+    assert _failure(end=-1.0, family=family)[1]["begin"] == 63
+    assert _failure(through=0.3, lf_global=1, lf_global_speed=0.01, family=family)[1]["begin"] == 63
 
 
 def test_preheat_rejected_candidate_keeps_state(cuda_lib):

@@ -338,3 +338,34 @@ def test_product_features_on_slabs_equal_single(cuda_lib):
         assert code == 0 and [x["dt"] for x in r] == [x["dt"] for x in reps]
     got = np.concatenate([np.stack(s.get_state()) for s in slabs], axis=1)
     assert np.array_equal(got, ref)
+
+
+def test_ssprk2_order_on_the_cooling_box(cuda_lib):
+    """The reference's SSPRK2 order test (src/couple/test/test_evolution.py:
+    119-145) on the GPU: the 2x2 box cools uniformly (cells equal to 1e-12),
+    the error against the exact exponential mode falls by 3.8-4.2 when the
+    fixed step halves, and the final H matches the oracle to 1e-12."""
+    from test_oracle_transport import COOLING_BOX, COOLING_DECAY, cooling_box_oracle
+    from mantlepar_b200.transport import Transport, TransportConfig
+    w = COOLING_BOX
+    exact = 2 + .1 * np.exp(-COOLING_DECAY * .1)
+    errors = []
+    for dt in (.01, .005):
+        t = Transport(w, TransportConfig(material=sy.Material(), cfl=0.4, integrator=2, dt_initial=dt, dt_max=dt,
+                                         dt_min=1e-12, H_policy=2, C_policy=2, diffusivity=0.01))
+        t.set_thermal_bc((1, 1, 1, 1), (2.0, 2.0, 2.0, 2.0))
+        t.set_pressure_model(t.LITHOSTATIC, 0.0)
+        t.set_cell_velocity(np.zeros(w.cells * 25), np.zeros(w.cells * 25))
+        z = np.zeros(w.edges * 5)
+        t.set_face_velocity(z, z)
+        t.set_state(np.full(w.cells, 2.1), np.full(w.cells, .05))
+        t.set_time_control(1, 0.1)
+        _, reps = t.step(100)
+        assert t.get_time() == (0.1, round(.1 / dt))
+        H = t.get_state()[0]
+        assert np.max(np.abs(H - H[0])) <= 1e-12
+        o = cooling_box_oracle(dt)
+        assert o.step(100)[0] == 0
+        assert rel(H, o.get_state()[0]) <= 1e-12
+        errors.append(abs(H[0] - exact))
+    assert 3.8 < errors[0] / errors[1] < 4.2, errors

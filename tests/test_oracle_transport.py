@@ -218,3 +218,45 @@ def test_source_requires_cell_velocities():
     t.set_state(H, C)
     code, _ = t.rhs()
     assert code == 73
+
+
+# The reference's SSPRK2 order test (src/couple/test/test_evolution.py:119-145):
+# a uniform, dry, motionless 2x2 box of the product input's mesh and material
+# (cells 0.25 wide on [0, 0.5] x [-0.5, 0], lithostatic pressure with the
+# surface at y = 0) at H = 2.1, C = 0.05 cools through walls held at T = 2
+# with kappa = 0.01; its semidiscrete thermal mode decays exactly as
+# exp(-decay t), decay = 2 kappa (25/12) / (0.9 * 0.25 / 4) / 0.25, so SSPRK2
+# with fixed steps 0.01 and 0.005 to t = 0.1 has an error ratio near 4.
+COOLING_BOX = sy.Workload(nx=2, ny=2, x0=0.0, x1=0.5, y0=-0.5, y1=0.0)
+COOLING_DECAY = 2 * .01 * (25 / 12) / (.9 * .25 / 4) / .25
+
+
+def cooling_box_oracle(dt, lib=None):
+    w = COOLING_BOX
+    o = po.TransportOracle(sy.Material(), w, lib=lib, integrator=2, cfl=0.4, dt_initial=dt, dt_max=dt,
+                           dt_min=1e-12, H_policy=2, C_policy=2)
+    assert o.set_diffusion(0.01, (1, 1, 1, 1), (2.0, 2.0, 2.0, 2.0)) == 0
+    assert o.set_pressure_model(1, 0.0) == 0
+    assert o.set_cell_velocity(np.zeros(w.cells * 25), np.zeros(w.cells * 25)) == 0
+    z = np.zeros(w.edges * 5)
+    o.set_face_velocity(z, z)
+    o.set_state(np.full(w.cells, 2.1), np.full(w.cells, .05))
+    assert o.set_time_control(1, 0.1) == 0
+    return o
+
+
+def test_ssprk2_order_on_the_cooling_box():
+    exact = 2 + .1 * np.exp(-COOLING_DECAY * .1)
+    errors = []
+    for dt in (.01, .005):
+        o = cooling_box_oracle(dt)
+        code, reps = o.step(100)
+        assert code == 0 and sum(1 for r in reps if r["dt"] > 0) == round(.1 / dt)
+        H = o.get_state()[0]
+        assert np.max(np.abs(H - H[0])) <= 1e-12
+        errors.append(abs(H[0] - exact))
+        if po.reference_available():
+            r = cooling_box_oracle(dt, po.reference())
+            assert r.step(100)[0] == 0
+            assert np.array_equal(r.get_state()[0], H)
+    assert 3.8 < errors[0] / errors[1] < 4.2, errors
