@@ -352,7 +352,8 @@ def test_ssprk2_order_on_the_cooling_box(cuda_lib):
     errors = []
     for dt in (.01, .005):
         t = Transport(w, TransportConfig(material=sy.Material(), cfl=0.4, integrator=2, dt_initial=dt, dt_max=dt,
-                                         dt_min=1e-12, H_policy=2, C_policy=2, diffusivity=0.01))
+                                         dt_min=1e-12, H_policy=2, C_policy=2, inflow_C=0.05,
+                                         diffusivity=0.01))
         t.set_thermal_bc((1, 1, 1, 1), (2.0, 2.0, 2.0, 2.0))
         t.set_pressure_model(t.LITHOSTATIC, 0.0)
         t.set_cell_velocity(np.zeros(w.cells * 25), np.zeros(w.cells * 25))

@@ -234,7 +234,7 @@ COOLING_DECAY = 2 * .01 * (25 / 12) / (.9 * .25 / 4) / .25
 def cooling_box_oracle(dt, lib=None):
     w = COOLING_BOX
     o = po.TransportOracle(sy.Material(), w, lib=lib, integrator=2, cfl=0.4, dt_initial=dt, dt_max=dt,
-                           dt_min=1e-12, H_policy=2, C_policy=2)
+                           dt_min=1e-12, H_policy=2, C_policy=2, inflow_C=0.05)
     assert o.set_diffusion(0.01, (1, 1, 1, 1), (2.0, 2.0, 2.0, 2.0)) == 0
     assert o.set_pressure_model(1, 0.0) == 0
     assert o.set_cell_velocity(np.zeros(w.cells * 25), np.zeros(w.cells * 25)) == 0
