@@ -239,6 +239,20 @@ def face_velocity_quads(w: Workload, xy: np.ndarray) -> tuple[np.ndarray, np.nda
     return np.ascontiguousarray(np.concatenate(out_vs)), np.ascontiguousarray(np.concatenate(out_ud))
 
 
+def uniform_face_velocity(w: Workload, xy: np.ndarray, U: float, V: float) -> np.ndarray:
+    """Normal components of the uniform velocity (U, V) at the 5 Gauss points
+    of every edge against its canonical right normal (dy, -dx)/len, [edge*5 + q];
+    xy: the mesh vertices (quad_vertices, any family)."""
+    P = xy.reshape(w.ny + 1, w.nx + 1, 2)
+    out = []
+    for a, b in ((P[:, :-1], P[:, 1:]), (P[:-1, :], P[1:, :])):   # AlongI, then AlongJ
+        d = b - a
+        length = np.hypot(d[..., 0], d[..., 1])
+        vn = (U * d[..., 1] - V * d[..., 0]) / length
+        out.append(np.repeat(vn.reshape(-1, 1), 5, axis=1))
+    return np.ascontiguousarray(np.concatenate(out).reshape(-1))
+
+
 def cell_velocity_quads(w: Workload, xy: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     """cell_velocity on a general quad mesh: the vertical components at the
     bilinear images of the 5x5 Gauss points, [cell*25 + b*5 + a]."""

@@ -370,3 +370,34 @@ def test_ssprk2_order_on_the_cooling_box(cuda_lib):
         assert rel(H, o.get_state()[0]) <= 1e-12
         errors.append(abs(H[0] - exact))
     assert 3.8 < errors[0] / errors[1] < 4.2, errors
+
+
+@pytest.mark.parametrize("nx,ny", [(12, 10), (1280, 2560)], ids=["12x10", "1280x2560"])
+@pytest.mark.parametrize("family", [sy.MESH_RECTANGULAR, sy.MESH_PERTURBED], ids=["uniform", "perturbed"])
+def test_constant_state_is_preserved(cuda_lib, family, nx, ny):
+    """Constant preservation (src/mlweno/test/test_advection_diffusion.cpp:
+    125-148, 2e-10 there), a size-independent property: a uniform state in a
+    uniform flow with matching inflow values has a zero RHS to roundoff (at
+    12x10 equal to the oracle's), and two SSPRK3 steps keep it uniform."""
+    from mantlepar_b200.transport import Transport, TransportConfig
+    w = sy.Workload(nx=nx, ny=ny)
+    xy = sy.quad_vertices(w, family, 0.2, 11)
+    t = Transport(w, TransportConfig(cfl=w.cfl, integrator=3, inflow_H=0.6, inflow_C=0.31),
+                  vertices=None if family == sy.MESH_RECTANGULAR else xy)
+    t.set_face_velocity(sy.uniform_face_velocity(w, xy, 0.3, 0.2), sy.uniform_face_velocity(w, xy, 0.0, 0.01))
+    t.set_state(np.full(w.cells, 0.6), np.full(w.cells, 0.31))
+    r = t.rhs()
+    assert r["phi"].min() > 0
+    for k in ("rhsH", "rhsC"):
+        assert np.max(np.abs(r[k])) <= 1e-13 * r["maxRate"], k
+    if nx == 12:
+        from test_oracle_transport import constant_state_oracle
+        o, _ = constant_state_oracle(w, family)
+        code, ref = o.rhs()
+        assert code == 0
+        for k in ("T", "phi", "rate"):
+            assert rel(r[k], ref[k]) <= RTOL_STAGE, k
+    _, reps = t.step(2)
+    assert all(x["status"] == 0 for x in reps)
+    H, C, _, _ = t.get_state()
+    assert np.max(np.abs(H - 0.6)) <= 1e-13 and np.max(np.abs(C - 0.31)) <= 1e-13

@@ -260,3 +260,28 @@ def test_ssprk2_order_on_the_cooling_box():
             assert r.step(100)[0] == 0
             assert np.array_equal(r.get_state()[0], H)
     assert 3.8 < errors[0] / errors[1] < 4.2, errors
+
+
+def constant_state_oracle(w, family, lib=None):
+    """A uniform state (H 0.6, C 0.31: solid and liquid) in the uniform flow
+    v_s = (0.3, 0.2), u_d = (0, 0.01), inflow values equal to the state."""
+    o = po.TransportOracle(sy.material_s(), w, lib=lib, integrator=3, inflow_H=0.6, inflow_C=0.31,
+                           mesh_family=family, perturbation=0.2, mesh_seed=11)
+    xy = o.vertices()
+    o.set_face_velocity(sy.uniform_face_velocity(w, xy, 0.3, 0.2), sy.uniform_face_velocity(w, xy, 0.0, 0.01))
+    o.set_state(np.full(w.cells, 0.6), np.full(w.cells, 0.31))
+    return o, xy
+
+
+@pytest.mark.parametrize("family", [sy.MESH_RECTANGULAR, sy.MESH_PERTURBED, sy.MESH_SINE_STRETCHED])
+def test_constant_state_is_preserved(family):
+    """Constant preservation (src/mlweno/test/test_advection_diffusion.cpp:
+    125-148, 2e-10 there): a uniform state in a uniform flow has a zero RHS
+    to roundoff, in the restated and the reference build."""
+    w = sy.Workload(nx=12, ny=10)
+    for lib in [None] + ([po.reference()] if po.reference_available() else []):
+        o, _ = constant_state_oracle(w, family, lib)
+        code, r = o.rhs()
+        assert code == 0 and r["phi"].min() > 0
+        for k in ("rhsH", "rhsC"):
+            assert np.max(np.abs(r[k])) <= 1e-13 * r["maxRate"], k
