@@ -272,6 +272,7 @@ int upload_quad_tables(int nx, int ny, const double* xy, const QuadTables& qt, i
     const size_t V = qt.xy.size(), NEq = qt.spacing.size();
     const size_t total = V + (size_t)(kQG0 + kQS9 + kQT4 + kQS4 + kQGeo) * N + NEq;
     e = cudaMalloc((void**)buf, total * sizeof(double));
+    if (e != cudaSuccess) *buf = nullptr;
     double* at = *buf;
     auto put = [&](const std::vector<double>* v, size_t n) -> double* {
         if (v && e == cudaSuccess) e = cudaMemcpyAsync(at, v->data(), n * sizeof(double), cudaMemcpyHostToDevice, stream);
@@ -293,7 +294,10 @@ int upload_quad_tables(int nx, int ny, const double* xy, const QuadTables& qt, i
     double* d_all = nullptr;
     int* d_failed = nullptr;
     const size_t VA = 2 * (size_t)(nx + 1) * (ny + 1);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&d_all, VA * sizeof(double) + sizeof(int));
+    if (e == cudaSuccess) {
+        e = cudaMalloc((void**)&d_all, VA * sizeof(double) + sizeof(int));
+        if (e != cudaSuccess) d_all = nullptr;
+    }
     if (e == cudaSuccess) {
         d_failed = reinterpret_cast<int*>(d_all + VA);
         e = cudaMemcpyAsync(d_all, xy, VA * sizeof(double), cudaMemcpyHostToDevice, stream);
