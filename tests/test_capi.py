@@ -46,3 +46,28 @@ def test_host_layer_exports_the_phase_model_interface(cuda_lib):
         assert "mantle::phase::" + member in out, member
     deps = subprocess.run(["ldd", build.HOST_LIB], capture_output=True, text=True).stdout
     assert "libmantlepar_b200.so" in deps
+
+
+def test_invalid_quad_meshes_are_rejected_before_device_work(cuda_lib):
+    """mp_transport_create_quads and mp_preheat_create_quads check the vertex
+    array on the host (the reference's quad validation) before any device
+    call: a null array or a folded cell gives MP_ERR_ARG_WRONG and no handle,
+    with no GPU present."""
+    import ctypes as C
+    import numpy as np
+    from mantlepar_b200 import synthetic as sy
+    from mantlepar_b200.preheat import PreheatConfig
+    from mantlepar_b200.transport import TransportConfig
+    w = sy.Workload(nx=4, ny=4)
+    mesh = _capi.MeshDesc(w.nx, w.ny, w.x0, w.x1, w.y0, w.y1)
+    xy = sy.quad_vertices(w, sy.MESH_RECTANGULAR).reshape(5, 5, 2).copy()
+    xy[2, 2] = xy[3, 3] + [0.01, 0.01]            # fold one interior vertex past its neighbour
+    bad = np.ascontiguousarray(xy.reshape(-1))
+    t_opts, p_opts = TransportConfig().to_c(), PreheatConfig().to_c()
+    for xy_ptr in (None, bad.ctypes.data):
+        h = C.c_void_p()
+        assert cuda_lib.mp_transport_create_quads(C.byref(mesh), xy_ptr, C.byref(t_opts), None, C.byref(h)) == 62
+        assert not h.value
+        assert cuda_lib.mp_preheat_create_quads(C.byref(mesh), xy_ptr, C.byref(p_opts), None, C.byref(h)) == 62
+        assert not h.value
+    assert b"quadrilateral" in cuda_lib.mp_last_error_string()
