@@ -193,17 +193,19 @@ def test_preheat_large_mesh_properties(cuda_lib):
     assert accepted == 20 and np.all(np.isfinite(H))
 
 
-def test_preheat_then_evolve_through_the_handoff_files(cuda_lib, tmp_path):
+@pytest.mark.parametrize("name", ["through_diffusion", "quad_through"], ids=["uniform", "perturbed"])
+def test_preheat_then_evolve_through_the_handoff_files(cuda_lib, tmp_path, name):
     """The reference's workflow (mantle_couple_preheat, then
-    mantle_couple_evolve -preheat DIR): the preheated H and the fixed C go
-    through cellH1.dat / cellC1.dat / transport_state.json bit for bit, and
-    the coupled transport continues from them at the preheat's end time,
-    step for step with the oracle started from the same files."""
+    mantle_couple_evolve -preheat DIR; on a perturbed-quadrilateral mesh as
+    its warped-mesh restart): the preheated H and the fixed C go through
+    cellH1.dat / cellC1.dat / transport_state.json bit for bit, and the
+    coupled transport continues from them at the preheat's end time, step for
+    step with the oracle started from the same files."""
     from oracle import pyoracle as po
     from mantlepar_b200 import handoff
     from mantlepar_b200.phase import EutecticModel
     from mantlepar_b200.transport import Transport, TransportConfig
-    case = pc.CASES["through_diffusion"]
+    case = pc.CASES[name]
     w = case.w
     p = pc.gpu_instance(case)
     code, _, _, _, _ = p.run()
@@ -211,14 +213,21 @@ def test_preheat_then_evolve_through_the_handoff_files(cuda_lib, tmp_path):
     H, time, accepted = p.get_state()
     _, C = case.state()
     derived = EutecticModel(sy.material_s()).derived()
-    mesh = handoff.MeshInfo.of(w)
+    if case.family == sy.MESH_RECTANGULAR:
+        mesh = handoff.MeshInfo.of(w)
+    else:
+        mesh = handoff.MeshInfo(w.nx, w.ny, (w.x0, w.x1, w.y0, w.y1), "perturbed_quadrilateral", case.perturbation,
+                                case.mesh_seed)
     handoff.write_state(str(tmp_path), mesh, H, C, time, accepted, derived)
     H2, C2, t2 = handoff.read_state(str(tmp_path), mesh, derived, sy.material_s().Xe)
     assert np.array_equal(H2, H) and np.array_equal(C2, C) and t2 == time == case.end
-    t = Transport(w, TransportConfig(cfl=w.cfl, integrator=2))
-    o = po.TransportOracle(sy.material_s(), w, integrator=2)
+    xy = case.vertices()
+    t = Transport(w, TransportConfig(cfl=w.cfl, integrator=2), vertices=xy)
+    o = po.TransportOracle(sy.material_s(), w, integrator=2, mesh_family=case.family, perturbation=case.perturbation,
+                           mesh_seed=case.mesh_seed)
+    vs, ud = sy.face_velocity(w) if xy is None else sy.face_velocity_quads(w, xy)
     for x in (t, o):
-        x.set_face_velocity(*sy.face_velocity(w))
+        x.set_face_velocity(vs, ud)
         x.set_state(H2, C2, t2)
     _, got = t.step(3)
     code, ref = o.step(3)
