@@ -253,6 +253,25 @@ def uniform_face_velocity(w: Workload, xy: np.ndarray, U: float, V: float) -> np
     return np.ascontiguousarray(np.concatenate(out).reshape(-1))
 
 
+def cell_centroids(w: Workload, xy: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Area centroids of the cells of a quad mesh, [j*nx + i] (the shoelace
+    formula in coordinates relative to each cell's first corner, so that the
+    products do not cancel on small cells)."""
+    P = xy.reshape(w.ny + 1, w.nx + 1, 2)
+    o = P[:-1, :-1]
+    v = [P[:-1, :-1] - o, P[:-1, 1:] - o, P[1:, 1:] - o, P[1:, :-1] - o]   # counter-clockwise
+    A2 = 0.0
+    sx = 0.0
+    sy_ = 0.0
+    for k in range(4):
+        a, b = v[k], v[(k + 1) % 4]
+        cr = a[..., 0] * b[..., 1] - b[..., 0] * a[..., 1]
+        A2 = A2 + cr
+        sx = sx + (a[..., 0] + b[..., 0]) * cr
+        sy_ = sy_ + (a[..., 1] + b[..., 1]) * cr
+    return (o[..., 0] + sx / (3 * A2)).reshape(-1), (o[..., 1] + sy_ / (3 * A2)).reshape(-1)
+
+
 def cell_velocity_quads(w: Workload, xy: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     """cell_velocity on a general quad mesh: the vertical components at the
     bilinear images of the 5x5 Gauss points, [cell*25 + b*5 + a]."""

@@ -293,3 +293,30 @@ def test_preheat_quad_large_mesh_properties(cuda_lib):
         prev = r["integral"]
     H, _, accepted = p.get_state()
     assert accepted == 10 and np.all(np.isfinite(H))
+
+
+@pytest.mark.parametrize("nx,ny,families", [(12, 10, (0, 1, 2)), (1280, 2560, (0, 1))], ids=["12x10", "1280x2560"])
+def test_linear_field_gives_the_exact_rhs(cuda_lib, nx, ny, families):
+    """Linear exactness, a size-independent property: the preheat RHS of a
+    linear H in a uniform flow is -v . grad H in every cell off the inflow
+    walls (1e-13 at 12x10, where it also equals the oracle's RHS; 1e-10 at
+    1280x2560, where roundoff grows like 1/h), on uniform, perturbed and
+    stretched meshes: the GPU-built per-cell tables reproduce linear data."""
+    from test_oracle_preheat import LINEAR_RHS, linear_field_case
+    from mantlepar_b200.preheat import Preheat
+    w = sy.Workload(nx=nx, ny=ny)
+    for family in families:
+        case, xy, vs, H = linear_field_case(w, family)
+        p = Preheat(w, pc.gpu_config(case), vertices=None if family == sy.MESH_RECTANGULAR else xy)
+        p.set_velocity(vs)
+        p.set_state(H, np.full(w.cells, 0.3))
+        rhs, _ = p.rhs()
+        r = rhs.reshape(w.ny, w.nx)
+        assert np.max(np.abs(r[1:, 1:] - LINEAR_RHS)) <= (1e-13 if nx == 12 else 1e-10), family
+        if nx == 12:
+            t = pc.oracle_instance(case)
+            t.set_face_velocity(vs, np.zeros_like(vs))
+            t.set_state(H, np.full(w.cells, 0.3))
+            code, ref, _ = t.preheat_rhs()
+            assert code == 0 and rel_inf(rhs, ref) <= RTOL, family
+        p.close()

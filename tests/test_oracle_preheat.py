@@ -85,3 +85,40 @@ def test_preheat_failures():
     # A global LF speed below a flow normal speed.
     r = _codes(through=0.3, lf_global=1, lf_global_speed=0.01)
     assert r["begin"] == 63
+
+
+# Linear exactness: every candidate polynomial reproduces linear data, so the
+# unlimited reconstruction of a linear H is exact, the traces of both sides
+# agree and the linear-law flux of the uniform flow v integrates exactly:
+# the preheat RHS is -v . grad H in every cell not on an inflow wall (the
+# bottom and left walls for v = (0.3, 0.2)), on any quad mesh.
+LINEAR_H = (0.7, 0.5, -0.3)           # c + a x + b y
+LINEAR_V = (0.3, 0.2)
+LINEAR_RHS = -(LINEAR_V[0] * LINEAR_H[1] + LINEAR_V[1] * LINEAR_H[2])
+
+
+def linear_field_case(w, family):
+    case = pc.PreheatCase(w, family=family, perturbation=0.2)
+    xy = pc.sy.quad_vertices(w, family, 0.2, case.mesh_seed)
+    x, y = pc.sy.cell_centroids(w, xy)
+    H = LINEAR_H[0] + LINEAR_H[1] * x + LINEAR_H[2] * y
+    return case, xy, pc.sy.uniform_face_velocity(w, xy, *LINEAR_V), H
+
+
+@pytest.mark.parametrize("family", [0, 1, 2], ids=["uniform", "perturbed", "sine"])
+def test_linear_field_gives_the_exact_rhs(family):
+    w = pc.sy.Workload(nx=12, ny=10)
+    case, xy, vs, H = linear_field_case(w, family)
+    out = []
+    for lib in [None] + ([po.reference()] if po.reference_available() else []):
+        t = pc.oracle_instance(case, lib)
+        t.set_face_velocity(vs, np.zeros_like(vs))
+        t.set_state(H, np.full(w.cells, 0.3))
+        code, rhs, _ = t.preheat_rhs()
+        assert code == 0
+        out.append(rhs)
+    r = out[0].reshape(w.ny, w.nx)
+    assert np.max(np.abs(r[1:, 1:] - LINEAR_RHS)) <= 1e-13
+    assert np.max(np.abs(r[0])) > 1e-3          # the inflow wall's cells see the inflow value
+    if len(out) == 2:
+        assert np.array_equal(bits(out[0]), bits(out[1]))
