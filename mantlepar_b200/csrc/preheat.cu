@@ -503,18 +503,18 @@ __global__ void __launch_bounds__(128, 4) pre_quad_recon_kernel(int nx, int ny, 
     const size_t N = (size_t)nx * ny;
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
     const double eA = 1e-2 * __ldg(q.geo + 3 * N + cell);
-    double u[3][3];
+    double u[1][3][3];
 #pragma unroll
     for (int dj = 0; dj < 3; ++dj)
 #pragma unroll
         for (int di = 0; di < 3; ++di) {
             const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
-            u[dj][di] = __ldg(H + (size_t)jj * nx + ii);
+            u[0][dj][di] = __ldg(H + (size_t)jj * nx + ii);
         }
-    double D[9];
-    const int st = reconstruct_quad(q, N, cell, ci, cj, eA, u, D);
+    double D[1][9];
+    const int st = reconstruct_quad<1>(q, N, cell, ci, cj, eA, u, D);
 #pragma unroll
-    for (int m = 0; m < 9; ++m) rec[(size_t)m * N + cell] = D[m];
+    for (int m = 0; m < 9; ++m) rec[(size_t)m * N + cell] = D[0][m];
     if (st) record_error(status, PART_UPDATE, cell, st);
 }
 
@@ -686,21 +686,16 @@ __global__ void __launch_bounds__(128) pre_quad_diag_kernel(int nx, int ny, cons
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
     const CellFrame f = cell_frame(q, nx, N, cell);
     const double eA = 1e-2 * f.area;
+    double u[2][3][3];
+    for (int dj = 0; dj < 3; ++dj)
+        for (int di = 0; di < 3; ++di) {
+            const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
+            u[0][dj][di] = __ldg(H + (size_t)jj * nx + ii);
+            u[1][dj][di] = __ldg(C + (size_t)jj * nx + ii);
+        }
+    const double m[2] = {u[0][1][1], u[1][1][1]};
     double D[2][9];
-    double m[2];
-    int st = 0;
-    for (int fi = 0; fi < 2; ++fi) {
-        const double* F = fi ? C : H;
-        double u[3][3];
-        for (int dj = 0; dj < 3; ++dj)
-            for (int di = 0; di < 3; ++di) {
-                const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
-                u[dj][di] = __ldg(F + (size_t)jj * nx + ii);
-            }
-        m[fi] = u[1][1];
-        const int s = reconstruct_quad(q, N, cell, ci, cj, eA, u, D[fi]);
-        st = st ? st : s;
-    }
+    int st = reconstruct_quad<2>(q, N, cell, ci, cj, eA, u, D);
     if (st) { record_error(status, PART_UPDATE, cell, st); return; }
     double Ts = 0.0, Ps = 0.0;
     for (int b = 0; b < kNQ; ++b)

@@ -114,102 +114,37 @@ __device__ __forceinline__ void visit_samples(const QuadDev& q, int nx, int ny, 
 // Folded smoothness row offsets: entry (r, c >= r) of an n x n form.
 __device__ __forceinline__ int fold_at(int n, int r, int c) { return r * n - (r * (r - 1)) / 2 + (c - r); }
 
-// One field's deviation polynomial D from the 3x3 neighbourhood with the
-// cell's own tables (same candidate set, weights and clipping as
-// reconstruct() of the uniform path).
-__device__ __forceinline__ int reconstruct_quad(const QuadDev& q, size_t N, long long cell, int ci, int cj,
-                                                double eA, const double (&u)[3][3], double (&D)[9]) {
-    double d[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int b = 0; b < 3; ++b) d[a][b] = u[a][b] - u[1][1];
-    const int offi[4] = {0, 0, -1, -1}, offj[4] = {-1, 0, -1, 0};
-    bool on[5];
-    on[0] = (ci == 1 && cj == 1);
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-        on[k + 1] = !((offi[k] == 0 && ci == 2) || (offi[k] == -1 && ci == 0) || (offj[k] == 0 && cj == 2) ||
-                      (offj[k] == -1 && cj == 0));
-    double sig[5];
-    int st = 0;
-    if (on[0]) {
-        double diff[8];
-#pragma unroll
-        for (int c = 1; c < 9; ++c) diff[c - 1] = d[c / 3][c % 3] - d[0][0];
-        auto SF = [&](int k) { return __ldg(q.S9 + (size_t)k * N + cell); };
-        auto S = [&](int r, int c) { const double v = SF(fold_at(8, r, c)); return r == c ? v : 0.5 * v; };
-        sig[0] = smoothness<double, 8>(SF, S, diff);
-        if (sig[0] < 0.0) st = MP_ERR_FP;
-    } else {
-        sig[0] = 0;
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        if (!on[k + 1]) { sig[k + 1] = 0; continue; }
-        const int oi = offi[k], oj = offj[k];
-        const double a0 = d[1 + oj][1 + oi];
-        double diff[3];
-#pragma unroll
-        for (int c = 1; c < 4; ++c) diff[c - 1] = d[1 + oj + c / 2][1 + oi + c % 2] - a0;
-        auto SF = [&](int m) { return __ldg(q.S4 + (size_t)(k * 6 + m) * N + cell); };
-        auto S = [&](int r, int c) { const double v = SF(fold_at(3, r, c)); return r == c ? v : 0.5 * v; };
-        sig[k + 1] = smoothness<double, 3>(SF, S, diff);
-        if (sig[k + 1] < 0.0) st = MP_ERR_FP;
-    }
-    double w[5];
-    weights<double>(sig, on, eA, w);
-    if (!isfinite(w[0] + w[1] + w[2] + w[3] + w[4])) st = MP_ERR_FP;
-#pragma unroll
-    for (int m = 0; m < 9; ++m) D[m] = 0;
-    if (on[0]) {
-        double diff[8];
-#pragma unroll
-        for (int c = 1; c < 9; ++c) diff[c - 1] = d[c / 3][c % 3] - d[0][0];
-#pragma unroll
-        for (int m = 0; m < 9; ++m) {
-            double v = m == 0 ? d[0][0] : 0.0;
-#pragma unroll
-            for (int c = 1; c < 9; ++c) v += diff[c - 1] * __ldg(q.G0 + (size_t)((c - 1) * 9 + m) * N + cell);
-            D[m] = w[0] * v;
-        }
-    }
-    const int slot[4] = {0, 1, 3, 4};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        if (!on[k + 1]) continue;
-        const int oi = offi[k], oj = offj[k];
-        const double a0 = d[1 + oj][1 + oi];
-        double diff[3];
-#pragma unroll
-        for (int c = 1; c < 4; ++c) diff[c - 1] = d[1 + oj + c / 2][1 + oi + c % 2] - a0;
-#pragma unroll
-        for (int mm = 0; mm < 4; ++mm) {
-            double v = mm == 0 ? a0 : 0.0;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) v += diff[c] * __ldg(q.T4 + (size_t)(k * 12 + c * 4 + mm) * N + cell);
-            D[slot[mm]] += w[k + 1] * v;
-        }
-    }
-    return st;
+// smoothness<>'s decision for a chain that failed its range test (roundoff
+// at sigma ~ 0, or bad data), out of line: form n x n, folded entries at
+// base[k * stride].
+template <int NN>
+__device__ __noinline__ double smoothness_out_of_line(const double* base, size_t stride, const double* diff) {
+    auto SF = [&](int k) { return __ldg(base + (size_t)k * stride); };
+    auto S = [&](int r, int c) { const double v = SF(fold_at(NN, r, c)); return r == c ? v : 0.5 * v; };
+    return smoothness<double, NN>(SF, S, diff);
 }
 
-// Both fields' deviation polynomials (H and C share the cell's stencils,
-// so they share its tables) with one read of every table entry: per field
-// the operations and their order are those of reconstruct_quad, so DH and DC
-// equal two reconstruct_quad calls bit for bit. Returns the first failure
-// in field order (H, then C).
-__device__ __forceinline__ int reconstruct_quad2(const QuadDev& q, size_t N, long long cell, int ci, int cj,
-                                                 double eA, const double (&uH)[3][3], const double (&uC)[3][3],
-                                                 double (&DH)[9], double (&DC)[9]) {
-    double dH[3][3], dC[3][3];
+// The deviation polynomials D[f] of F fields from their 3x3 neighbourhoods
+// u[f] with the cell's own tables (same candidate set, weights and clipping
+// as reconstruct() of the uniform path). The fields share the cell's
+// stencils and so its tables: every table entry is read once and applied to
+// each field, and per field the operations run in the same order whatever F
+// is, so a field's result does not depend on the fields reconstructed with
+// it. For F > 1 smoothness<>'s FMA chains are formed here for all fields at
+// once, and a chain that fails its range test is decided by smoothness<> out
+// of line (it forms the same chain again, then the term-by-term sum), so
+// that the rare path does not cost the multi-field form registers; F = 1
+// calls smoothness<> inline. Returns the first failure in field order.
+template <int F>
+__device__ __forceinline__ int reconstruct_quad(const QuadDev& q, size_t N, long long cell, int ci, int cj,
+                                                double eA, const double (&u)[F][3][3], double (&D)[F][9]) {
+    double d[F][3][3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
+    for (int f = 0; f < F; ++f)
 #pragma unroll
-        for (int b = 0; b < 3; ++b) {
-            dH[a][b] = uH[a][b] - uH[1][1];
-            dC[a][b] = uC[a][b] - uC[1][1];
-        }
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) d[f][a][b] = u[f][a][b] - u[f][1][1];
     const int offi[4] = {0, 0, -1, -1}, offj[4] = {-1, 0, -1, 0};
     bool on[5];
     on[0] = (ci == 1 && cj == 1);
@@ -217,100 +152,129 @@ __device__ __forceinline__ int reconstruct_quad2(const QuadDev& q, size_t N, lon
     for (int k = 0; k < 4; ++k)
         on[k + 1] = !((offi[k] == 0 && ci == 2) || (offi[k] == -1 && ci == 0) || (offj[k] == 0 && cj == 2) ||
                       (offj[k] == -1 && cj == 0));
-    double sgH[5], sgC[5];
-    int stH = 0, stC = 0;
+    double sg[F][5];
+    int st[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) st[f] = 0;
     auto fast_ok = [](double v) { return v >= 0.0 && v < INFINITY; };
     if (on[0]) {
-        double fH[8], fC[8];
+        double fd[F][8];
 #pragma unroll
-        for (int c = 1; c < 9; ++c) {
-            fH[c - 1] = dH[c / 3][c % 3] - dH[0][0];
-            fC[c - 1] = dC[c / 3][c % 3] - dC[0][0];
-        }
+        for (int f = 0; f < F; ++f)
+#pragma unroll
+            for (int c = 1; c < 9; ++c) fd[f][c - 1] = d[f][c / 3][c % 3] - d[f][0][0];
         auto SF = [&](int k) { return __ldg(q.S9 + (size_t)k * N + cell); };
         auto S = [&](int r, int c) { const double v = SF(fold_at(8, r, c)); return r == c ? v : 0.5 * v; };
-        // The FMA chains of smoothness<double, 8> for both fields.
-        double sumH = 0, sumC = 0;
-        int k = 0;
+        if constexpr (F == 1) {
+            sg[0][0] = smoothness<double, 8>(SF, S, fd[0]);
+        } else {
+            double sum[F];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const double s0 = SF(k++);
-            double tH = s0 * fH[r], tC = s0 * fC[r];
+            for (int f = 0; f < F; ++f) sum[f] = 0;
+            int k = 0;
 #pragma unroll
-            for (int c = r + 1; c < 8; ++c) {
-                const double sv = SF(k++);
-                tH = fma(sv, fH[c], tH);
-                tC = fma(sv, fC[c], tC);
+            for (int r = 0; r < 8; ++r) {
+                const double s0 = SF(k++);
+                double t[F];
+#pragma unroll
+                for (int f = 0; f < F; ++f) t[f] = s0 * fd[f][r];
+#pragma unroll
+                for (int c = r + 1; c < 8; ++c) {
+                    const double sv = SF(k++);
+#pragma unroll
+                    for (int f = 0; f < F; ++f) t[f] = fma(sv, fd[f][c], t[f]);
+                }
+#pragma unroll
+                for (int f = 0; f < F; ++f) sum[f] = fma(fd[f][r], t[f], sum[f]);
             }
-            sumH = fma(fH[r], tH, sumH);
-            sumC = fma(fC[r], tC, sumC);
+#pragma unroll
+            for (int f = 0; f < F; ++f)
+                sg[f][0] = fast_ok(sum[f]) ? sum[f] : smoothness_out_of_line<8>(q.S9 + cell, N, fd[f]);
         }
-        sgH[0] = fast_ok(sumH) ? sumH : smoothness<double, 8>(SF, S, fH);
-        sgC[0] = fast_ok(sumC) ? sumC : smoothness<double, 8>(SF, S, fC);
-        if (sgH[0] < 0.0) stH = MP_ERR_FP;
-        if (sgC[0] < 0.0) stC = MP_ERR_FP;
+#pragma unroll
+        for (int f = 0; f < F; ++f)
+            if (sg[f][0] < 0.0) st[f] = MP_ERR_FP;
     } else {
-        sgH[0] = 0;
-        sgC[0] = 0;
+#pragma unroll
+        for (int f = 0; f < F; ++f) sg[f][0] = 0;
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        if (!on[k + 1]) { sgH[k + 1] = 0; sgC[k + 1] = 0; continue; }
-        const int oi = offi[k], oj = offj[k];
-        const double aH = dH[1 + oj][1 + oi], aC = dC[1 + oj][1 + oi];
-        double fH[3], fC[3];
+        if (!on[k + 1]) {
 #pragma unroll
-        for (int c = 1; c < 4; ++c) {
-            fH[c - 1] = dH[1 + oj + c / 2][1 + oi + c % 2] - aH;
-            fC[c - 1] = dC[1 + oj + c / 2][1 + oi + c % 2] - aC;
+            for (int f = 0; f < F; ++f) sg[f][k + 1] = 0;
+            continue;
+        }
+        const int oi = offi[k], oj = offj[k];
+        double fd[F][3];
+#pragma unroll
+        for (int f = 0; f < F; ++f) {
+            const double a0 = d[f][1 + oj][1 + oi];
+#pragma unroll
+            for (int c = 1; c < 4; ++c) fd[f][c - 1] = d[f][1 + oj + c / 2][1 + oi + c % 2] - a0;
         }
         auto SF = [&](int m) { return __ldg(q.S4 + (size_t)(k * 6 + m) * N + cell); };
         auto S = [&](int r, int c) { const double v = SF(fold_at(3, r, c)); return r == c ? v : 0.5 * v; };
-        double sumH = 0, sumC = 0;
-        int m = 0;
+        if constexpr (F == 1) {
+            sg[0][k + 1] = smoothness<double, 3>(SF, S, fd[0]);
+        } else {
+            double sum[F];
 #pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            const double s0 = SF(m++);
-            double tH = s0 * fH[r], tC = s0 * fC[r];
+            for (int f = 0; f < F; ++f) sum[f] = 0;
+            int m = 0;
 #pragma unroll
-            for (int c = r + 1; c < 3; ++c) {
-                const double sv = SF(m++);
-                tH = fma(sv, fH[c], tH);
-                tC = fma(sv, fC[c], tC);
+            for (int r = 0; r < 3; ++r) {
+                const double s0 = SF(m++);
+                double t[F];
+#pragma unroll
+                for (int f = 0; f < F; ++f) t[f] = s0 * fd[f][r];
+#pragma unroll
+                for (int c = r + 1; c < 3; ++c) {
+                    const double sv = SF(m++);
+#pragma unroll
+                    for (int f = 0; f < F; ++f) t[f] = fma(sv, fd[f][c], t[f]);
+                }
+#pragma unroll
+                for (int f = 0; f < F; ++f) sum[f] = fma(fd[f][r], t[f], sum[f]);
             }
-            sumH = fma(fH[r], tH, sumH);
-            sumC = fma(fC[r], tC, sumC);
+#pragma unroll
+            for (int f = 0; f < F; ++f)
+                sg[f][k + 1] = fast_ok(sum[f]) ? sum[f]
+                                               : smoothness_out_of_line<3>(q.S4 + (size_t)k * 6 * N + cell, N, fd[f]);
         }
-        sgH[k + 1] = fast_ok(sumH) ? sumH : smoothness<double, 3>(SF, S, fH);
-        sgC[k + 1] = fast_ok(sumC) ? sumC : smoothness<double, 3>(SF, S, fC);
-        if (sgH[k + 1] < 0.0) stH = MP_ERR_FP;
-        if (sgC[k + 1] < 0.0) stC = MP_ERR_FP;
+#pragma unroll
+        for (int f = 0; f < F; ++f)
+            if (sg[f][k + 1] < 0.0) st[f] = MP_ERR_FP;
     }
-    double wH[5], wC[5];
-    weights<double>(sgH, on, eA, wH);
-    weights<double>(sgC, on, eA, wC);
-    if (!isfinite(wH[0] + wH[1] + wH[2] + wH[3] + wH[4])) stH = MP_ERR_FP;
-    if (!isfinite(wC[0] + wC[1] + wC[2] + wC[3] + wC[4])) stC = MP_ERR_FP;
+    double w[F][5];
 #pragma unroll
-    for (int m = 0; m < 9; ++m) { DH[m] = 0; DC[m] = 0; }
+    for (int f = 0; f < F; ++f) weights<double>(sg[f], on, eA, w[f]);
+#pragma unroll
+    for (int f = 0; f < F; ++f)
+        if (!isfinite(w[f][0] + w[f][1] + w[f][2] + w[f][3] + w[f][4])) st[f] = MP_ERR_FP;
+#pragma unroll
+    for (int f = 0; f < F; ++f)
+#pragma unroll
+        for (int mm = 0; mm < 9; ++mm) D[f][mm] = 0;
     if (on[0]) {
-        double fH[8], fC[8];
+        double fd[F][8];
 #pragma unroll
-        for (int c = 1; c < 9; ++c) {
-            fH[c - 1] = dH[c / 3][c % 3] - dH[0][0];
-            fC[c - 1] = dC[c / 3][c % 3] - dC[0][0];
-        }
+        for (int f = 0; f < F; ++f)
 #pragma unroll
-        for (int m = 0; m < 9; ++m) {
-            double vH = m == 0 ? dH[0][0] : 0.0, vC = m == 0 ? dC[0][0] : 0.0;
+            for (int c = 1; c < 9; ++c) fd[f][c - 1] = d[f][c / 3][c % 3] - d[f][0][0];
+#pragma unroll
+        for (int mm = 0; mm < 9; ++mm) {
+            double v[F];
+#pragma unroll
+            for (int f = 0; f < F; ++f) v[f] = mm == 0 ? d[f][0][0] : 0.0;
 #pragma unroll
             for (int c = 1; c < 9; ++c) {
-                const double g = __ldg(q.G0 + (size_t)((c - 1) * 9 + m) * N + cell);
-                vH += fH[c - 1] * g;
-                vC += fC[c - 1] * g;
+                const double g = __ldg(q.G0 + (size_t)((c - 1) * 9 + mm) * N + cell);
+#pragma unroll
+                for (int f = 0; f < F; ++f) v[f] += fd[f][c - 1] * g;
             }
-            DH[m] = wH[0] * vH;
-            DC[m] = wC[0] * vC;
+#pragma unroll
+            for (int f = 0; f < F; ++f) D[f][mm] = w[f][0] * v[f];
         }
     }
     const int slot[4] = {0, 1, 3, 4};
@@ -318,27 +282,32 @@ __device__ __forceinline__ int reconstruct_quad2(const QuadDev& q, size_t N, lon
     for (int k = 0; k < 4; ++k) {
         if (!on[k + 1]) continue;
         const int oi = offi[k], oj = offj[k];
-        const double aH = dH[1 + oj][1 + oi], aC = dC[1 + oj][1 + oi];
-        double fH[3], fC[3];
+        double a0[F], fd[F][3];
 #pragma unroll
-        for (int c = 1; c < 4; ++c) {
-            fH[c - 1] = dH[1 + oj + c / 2][1 + oi + c % 2] - aH;
-            fC[c - 1] = dC[1 + oj + c / 2][1 + oi + c % 2] - aC;
+        for (int f = 0; f < F; ++f) {
+            a0[f] = d[f][1 + oj][1 + oi];
+#pragma unroll
+            for (int c = 1; c < 4; ++c) fd[f][c - 1] = d[f][1 + oj + c / 2][1 + oi + c % 2] - a0[f];
         }
 #pragma unroll
         for (int mm = 0; mm < 4; ++mm) {
-            double vH = mm == 0 ? aH : 0.0, vC = mm == 0 ? aC : 0.0;
+            double v[F];
+#pragma unroll
+            for (int f = 0; f < F; ++f) v[f] = mm == 0 ? a0[f] : 0.0;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const double t = __ldg(q.T4 + (size_t)(k * 12 + c * 4 + mm) * N + cell);
-                vH += fH[c] * t;
-                vC += fC[c] * t;
+                const double tv = __ldg(q.T4 + (size_t)(k * 12 + c * 4 + mm) * N + cell);
+#pragma unroll
+                for (int f = 0; f < F; ++f) v[f] += fd[f][c] * tv;
             }
-            DH[slot[mm]] += wH[k + 1] * vH;
-            DC[slot[mm]] += wC[k + 1] * vC;
+#pragma unroll
+            for (int f = 0; f < F; ++f) D[f][slot[mm]] += w[f][k + 1] * v[f];
         }
     }
-    return stH ? stH : stC;
+#pragma unroll
+    for (int f = 0; f < F; ++f)
+        if (st[f]) return st[f];
+    return 0;
 }
 
 // Left/right cells and oriented vertices of edge e (evolve.cpp:230-251).

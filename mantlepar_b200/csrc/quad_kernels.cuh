@@ -50,21 +50,21 @@ __global__ void __launch_bounds__(128, 3) quad_weno_kernel(int nx, int ny, const
     const int gj = gj0 + j;
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = gj == 0 ? 0 : (gj == gny - 1 ? 2 : 1);
     const double eA = 1e-2 * __ldg(q.geo + 3 * N + cell);
-    double uH[3][3], uC[3][3];
+    double u[2][3][3];
 #pragma unroll
     for (int dj = 0; dj < 3; ++dj)
 #pragma unroll
         for (int di = 0; di < 3; ++di) {
             const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
-            uH[dj][di] = __ldg(H + (size_t)jj * nx + ii);
-            uC[dj][di] = __ldg(C + (size_t)jj * nx + ii);
+            u[0][dj][di] = __ldg(H + (size_t)jj * nx + ii);
+            u[1][dj][di] = __ldg(C + (size_t)jj * nx + ii);
         }
-    double DH[9], DC[9];
-    const int st = reconstruct_quad2(q, N, cell, ci, cj, eA, uH, uC, DH, DC);
+    double D[2][9];
+    const int st = reconstruct_quad<2>(q, N, cell, ci, cj, eA, u, D);
 #pragma unroll
     for (int m = 0; m < 9; ++m) {
-        rec[(size_t)m * N + cell] = DH[m];
-        rec[(size_t)(m + 9) * N + cell] = DC[m];
+        rec[(size_t)m * N + cell] = D[0][m];
+        rec[(size_t)(m + 9) * N + cell] = D[1][m];
     }
     if (st) record_error(status, PART_UPDATE, cell + (long long)gj0 * nx, st);
 }
