@@ -87,8 +87,8 @@ extern "C" mp_status mp_transport_rhs_noalloc(const mp_mesh_desc* mesh, const mp
         set_error("mp_transport_rhs_noalloc: %zu cells exceed its fixed scratch limit of %zu cells", N, kMaxCells);
         return MP_ERR_ARG_SIZ;
     }
-    if (opts->diffusivity != 0.0) { set_error("thermal diffusion (kappa > 0) is not supported by this build"); return MP_ERR_ARG_WRONG; }
-    if (opts->material.alpha0 != 0.0) { set_error("adiabatic source (alpha0 != 0) is not supported by this build"); return MP_ERR_ARG_WRONG; }
+    if (opts->diffusivity != 0.0) { set_error("thermal diffusion (kappa > 0) is not supported by mp_transport_rhs_noalloc"); return MP_ERR_ARG_WRONG; }
+    if (opts->material.alpha0 != 0.0) { set_error("adiabatic source (alpha0 != 0) is not supported by mp_transport_rhs_noalloc"); return MP_ERR_ARG_WRONG; }
     if (opts->precision != MP_PRECISION_FP64) { set_error("mp_transport_rhs_noalloc evaluates the FP64 stage"); return MP_ERR_ARG_WRONG; }
     if (raw_partial_bytes(N) > kPartBytes || raw_totals_bytes() > 256) { set_error("scratch layout too small"); return MP_ERR_ARG_SIZ; }
     StageTables tab;
