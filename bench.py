@@ -43,13 +43,16 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(nx=1280, ny=2560)
 ALG_BYTES_PER_CELL_STAGE = 144          # read U^(k), U^n; write U^(k+1); 2 faces x 5 q x 8 B v_s.n; write T, phi
 # Executed FP64 operations per cell per stage (DFMA counted as 2, DADD/DMUL
-# as 1) of the stage kernels, from the ncu capture summarised in
-# profiles/transport_stage_full_640x1280.md: reconstruction 2073, cell phase
-# 1188, faces 1703, accumulation ~48 (per-cell figures are size-independent).
+# as 1) of the stage kernels, from an ncu capture of a 640x1280 stage:
+# reconstruction 2073, cell phase 1188, faces 1703, accumulation ~48
+# (per-cell figures are size-independent).
 FP64_FLOPS_PER_CELL_STAGE = 5012
 # DRAM bytes per cell per stage of the four stage kernels from the same capture
 # (640x1280 keeps every stage array above L2 size; traffic scales with cells).
 DRAM_BYTES_PER_CELL_STAGE = 924
+# B200 FP64 (vector and tensor) datasheet figure per GPU of an HGX B200
+# (296 TFLOP/s for 8 GPUs); the driver measures no FP64 peak.
+FP64_DATASHEET_TFLOPS = 37.0
 CPU_SAMPLE = dict(nx=160, ny=320)
 CPU_SECONDS = 12.0
 
@@ -234,7 +237,9 @@ def run_reference(args, world, rank):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_block(),
+            "config": dict(config_block(),
+                           cpu_sample=f"{w.nx}x{w.ny} sub-instance of the same construction per step; the per-cell "
+                                      "rate is extrapolated to the named workload (same config in name only)"),
             "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": kind,
                              "sample": f"{w.nx}x{w.ny} sub-instance per step (bounded sample of the 1280x2560 workload), SSPRK3"},
             "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -378,22 +383,53 @@ def run_forms(args, stream):
         t = Transport(w, TransportConfig(cfl=w.cfl, integrator=3, precision=prec), stream=stream.cuda_stream)
         t.set_face_velocity(vs, ud)
         t.set_state(H, Cc)
-        t.step(1)
-        ms, _ = timed_steps(t, args.form_steps, stream)
+        ms, _ = timed_steps(t, args.mixed_steps, stream)
         res[prec] = (ms, t.get_state())
         t.close()
     errs = {name: rel_errors(a, b) for name, a, b in zip(["H", "C", "T", "phi"], res[1][1], res[0][1])}
     forms["mixed_4096x4096"] = {
-        "value": w.cells * args.form_steps / (res[1][0] * 1e-3), "unit": "cell-updates/s",
-        "fp64_value": w.cells * args.form_steps / (res[0][0] * 1e-3),
-        "steps": args.form_steps, "errors_vs_fp64_path": errs,
-        "precision": "FP32 smoothness/weights/limiter scan; FP64 coefficients, phase, fluxes"}
+        "value": w.cells * args.mixed_steps / (res[1][0] * 1e-3), "unit": "cell-updates/s",
+        "fp64_value": w.cells * args.mixed_steps / (res[0][0] * 1e-3),
+        "steps": args.mixed_steps, "errors_vs_fp64_path": errs,
+        "bitwise_equal_to_fp64_path": all(bool(np.array_equal(a, b)) for a, b in zip(res[1][1], res[0][1])),
+        "precision": "FP32 screen of the limiter scan with an exact FP64 certificate; every value FP64 "
+                     "(smoothness, weights, coefficients, limited values, phase, fluxes, accumulation)"}
     del res
-    # Batched: 256 uneven meshes (seed 3), mixed and FP64, autotuned tiles.
+    # Config 0: the 20x20 instance, 200 SSPRK3 steps, through the
+    # single-instance path: device-resident steps (CUDA graph, one host wait
+    # per 64 steps) and the host-driven loop (one host wait per stage).
+    w0 = sy.plain_small()
+    H0, C0 = sy.initial_state(w0)
+    vs0, ud0 = sy.face_velocity(w0)
+    small = {}
+    for dev in (True, False):
+        t = Transport(w0, TransportConfig(cfl=w0.cfl, integrator=3), stream=stream.cuda_stream)
+        t.set_device_steps(dev)
+        t.set_face_velocity(vs0, ud0)
+        t.set_state(H0, C0)
+        t.step(3)
+        t.set_state(H0, C0)
+        syncs0 = t.host_syncs()
+        ms, (_, reps) = timed_steps(t, w0.steps, stream)
+        small[dev] = (ms, t.host_syncs() - syncs0, sum(r["retries"] for r in reps), t.get_state())
+        t.close()
+    forms["plain_fp64_20x20"] = {
+        "value": w0.cells * w0.steps / (small[True][0] * 1e-3), "unit": "cell-updates/s", "steps": w0.steps,
+        "ms_per_step": small[True][0] / w0.steps, "host_syncs_per_step": small[True][1] / w0.steps,
+        "retries": small[True][2],
+        "host_loop": {"value": w0.cells * w0.steps / (small[False][0] * 1e-3), "ms_per_step": small[False][0] / w0.steps,
+                      "host_syncs_per_step": small[False][1] / w0.steps},
+        "device_equals_host_loop": all(bool(np.array_equal(a, b)) for a, b in zip(small[True][3], small[False][3])),
+        "config": "20x20 on [0,0.5]x[0,1], SSPRK3, CFL 0.4, material S, single instance (state reset before timing)"}
+    # Batched: 256 uneven meshes (seed 3), 100 steps, mixed and FP64,
+    # autotuned tiles, device-resident steps; FP64 also with the host loop.
     ws = sy.batched_instances(256, seed=3)
     cells = sum(x.cells for x in ws)
-    for prec, name in ((1, "batched_mixed_256"), (0, "batched_fp64_256")):
+    nsteps = args.batch_steps
+    for prec, name, dev in ((1, "batched_mixed_256", True), (0, "batched_fp64_256", True),
+                            (0, "batched_fp64_256_host_loop", False)):
         b = Batch(ws, TransportConfig(cfl=0.4, integrator=3, precision=prec), stream=stream.cuda_stream)
+        b.set_device_steps(dev)
         for i, x in enumerate(ws):
             vs_i, ud_i = sy.face_velocity(x)
             H_i, C_i = sy.initial_state(x)
@@ -401,12 +437,29 @@ def run_forms(args, stream):
             b.set_state(i, H_i, C_i)
         tile, _ = b.autotune(reps=1)
         b.step(1)
-        ms, reps = timed_steps(b, args.form_steps, stream)
+        syncs0 = b.host_syncs()
+        ms, reps = timed_steps(b, nsteps, stream)
         ok = all(r[i]["status"] == 0 for r in reps for i in range(len(ws)))
-        forms[name] = {"value": cells * args.form_steps / (ms * 1e-3), "unit": "cell-updates/s",
-                       "instances": len(ws), "cells": cells, "steps": args.form_steps,
-                       "autotuned_tile": list(tile), "all_instances_healthy": ok}
+        forms[name] = {"value": cells * nsteps / (ms * 1e-3), "unit": "cell-updates/s",
+                       "instances": len(ws), "cells": cells, "steps": nsteps, "ms_per_step": ms / nsteps,
+                       "host_syncs_per_step": (b.host_syncs() - syncs0) / nsteps,
+                       "device_steps": dev, "autotuned_tile": list(tile), "all_instances_healthy": ok}
         b.close()
+    # The same 256 meshes one at a time through the plain single-instance
+    # FP64 path (device-resident steps): what running them without the
+    # batched engine costs.
+    ms_solo = 0.0
+    for x in ws:
+        t = Transport(x, TransportConfig(cfl=0.4, integrator=3), stream=stream.cuda_stream)
+        t.set_face_velocity(*sy.face_velocity(x))
+        t.set_state(*sy.initial_state(x))
+        t.step(1)
+        ms, _ = timed_steps(t, nsteps, stream)
+        ms_solo += ms
+        t.close()
+    forms["plain_fp64_256_one_at_a_time"] = {
+        "value": cells * nsteps / (ms_solo * 1e-3), "unit": "cell-updates/s", "instances": len(ws), "steps": nsteps,
+        "note": "each of the 256 meshes advanced alone through mp_transport_step (device-resident steps), times summed"}
     # Product-input features on the plain workload: thermal diffusion, a
     # lithostatic pressure and the adiabatic source (FP64).
     import dataclasses
@@ -598,10 +651,12 @@ def run_gpu(args, world, rank, local):
     kernel_ms = {n: kms[k] / max(kn[k], 1) for k, n in enumerate(names)}
     line = None
     if rank == 0:
-        roof64 = {"bound": "fp64", "peak": fp64.value, "unit": "TFLOP/s", "peak_kind": "measured (FMA probe)"}
+        roof64 = {"bound": "fp64", "peak": fp64.value, "unit": "TFLOP/s", "peak_kind": "measured (FMA probe)",
+                  "peak_datasheet": FP64_DATASHEET_TFLOPS}
         if FP64_FLOPS_PER_CELL_STAGE:
             a64 = FP64_FLOPS_PER_CELL_STAGE * cells / (stage_ms * 1e-3) / 1e12
-            roof64.update(achieved=a64, frac=a64 / fp64.value, flops_per_cell_stage=FP64_FLOPS_PER_CELL_STAGE)
+            roof64.update(achieved=a64, frac=a64 / fp64.value, frac_of_datasheet=a64 / FP64_DATASHEET_TFLOPS,
+                          flops_per_cell_stage=FP64_FLOPS_PER_CELL_STAGE)
         else:
             roof64.update(achieved=None, frac=None)
         line = {
@@ -634,6 +689,8 @@ def run_gpu(args, world, rank, local):
         forms = run_forms(args, torch.cuda.current_stream(dev))
         forms["plain_fp64_1280x2560"] = {"value": value, "unit": "cell-updates/s"}
         forms["batched_mixed_over_plain_fp64"] = forms["batched_mixed_256"]["value"] / value
+        forms["batched_mixed_over_plain_fp64_same_meshes"] = (forms["batched_mixed_256"]["value"] /
+                                                              forms["plain_fp64_256_one_at_a_time"]["value"])
         line["forms"] = forms
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, kind, sample, _, _ = cpu_run(2, CPU_SECONDS, os.cpu_count() or 1)
@@ -713,6 +770,8 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed / batched forms")
     ap.add_argument("--serve-requests", type=int, default=10)
     ap.add_argument("--form-steps", type=int, default=5, help="timed steps of each extra form")
+    ap.add_argument("--mixed-steps", type=int, default=50, help="steps of the mixed-precision 4096x4096 form")
+    ap.add_argument("--batch-steps", type=int, default=100, help="steps of the 256-mesh batched forms")
     ap.add_argument("--nx", type=int, default=WORKLOAD["nx"], help="cells in x (profiling of smaller cases)")
     ap.add_argument("--ny", type=int, default=WORKLOAD["ny"], help="cells in y")
     ap.add_argument("--preheat-only", action="store_true",

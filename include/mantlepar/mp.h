@@ -222,6 +222,17 @@ mp_status mp_transport_rhs(mp_transport* t, double* rhsH, double* rhsC, double* 
  * is rolled back to the last accepted step (evolve.cpp:493-499). */
 mp_status mp_transport_step(mp_transport* t, int nsteps, mp_step_report* reports);
 
+/* Device-resident stepping (no counterpart in the reference, whose step loop
+ * is host code). With enable != 0 (the default) mp_transport_step on a
+ * uniform mesh without slab hooks runs as one CUDA graph per 64 steps: the
+ * step and retry loops are conditional graph nodes and every decision of the
+ * loop above is taken on the device, one host wait per graph launch; results,
+ * reports and errors equal the host-driven loop (enable = 0) bit for bit.
+ * Row slabs, general quad meshes and profiling runs use the host-driven loop. */
+mp_status mp_transport_set_device_steps(mp_transport* t, int enable);
+/* Host waits for device results made by the stepping and RHS calls so far. */
+mp_status mp_transport_run_stats(const mp_transport* t, unsigned long long* host_syncs);
+
 /* Time controls of the coupled loop (src/couple/evolve.cpp:449-457,483;
  * TimeInput in src/input/input.h:154-158). MP_TIME_CFL (default): dt =
  * min(remaining, first step ? dt_initial : dt_max, cfl / stage rate), halved
@@ -433,6 +444,17 @@ int mp_batch_finished(const mp_batch* b, int instance);
  * cells-per-thread on this batch and keeps the fastest; tile = {bx, by, cpt}. */
 mp_status mp_batch_autotune(mp_batch* b, int reps, int tile[3], double* best_ms);
 mp_status mp_batch_profile(mp_batch* b, int enable);
+/* Device-resident stepping (no counterpart in the reference, whose step loop
+ * is host code): with enable != 0 (the default) mp_batch_step runs its steps
+ * as one CUDA graph per 64 steps -- the step and retry loops are conditional
+ * graph nodes and every dt, courant, admissibility, retry and balance
+ * decision of the reference's loop (src/couple/evolve.cpp:449-507) is taken
+ * on the device -- with one host wait per graph launch; results equal the
+ * host-driven loop (enable = 0) bit for bit. Profiling (mp_batch_profile)
+ * uses the host-driven loop. */
+mp_status mp_batch_set_device_steps(mp_batch* b, int enable);
+/* Host waits for device results made by the stepping calls so far. */
+mp_status mp_batch_run_stats(const mp_batch* b, unsigned long long* host_syncs);
 mp_status mp_batch_kernel_times(mp_batch* b, double ms[6], unsigned long long launches[6]);
 
 /* --------------------------------------------------------------- serving */
@@ -472,11 +494,14 @@ mp_status mp_serve_set_policy(mp_server* s, int order, double resident_cells_tar
  * (its CPU code allocates freely). All scratch lives in one fixed file-scope
  * device array (about 7.3 MB per GPU that loads the library, held until the
  * process exits); meshes above 32768 cells (nx*ny) are rejected with
- * MP_ERR_ARG_SIZ. The first call on each device looks up that array's device
- * address, so make it before any stream capture. Calls share the array and
- * overwrite it; calls that overlap on the GPU race. All array arguments are
- * device pointers (H, C, rhsH, rhsC, T, phi: nx*ny; vs_n, ud_n: edges*5);
- * rate and totals may be NULL. Synchronous on `stream`. */
+ * MP_ERR_ARG_SIZ. Options are checked as mp_transport_create checks them;
+ * kappa > 0, alpha0 != 0 and MP_PRECISION_MIXED are rejected with
+ * MP_ERR_ARG_WRONG. Every call looks up the array's device address in the
+ * current context. Calls share the array and overwrite it; calls that
+ * overlap on the GPU race. All array arguments are device pointers (H, C,
+ * rhsH, rhsC, T, phi: nx*ny; vs_n, ud_n: edges*5); rate and totals may be
+ * NULL. The call is synchronous: it waits for `stream` and reads the stage
+ * totals and status back to the host before it returns. */
 mp_status mp_transport_rhs_noalloc(const mp_mesh_desc* mesh, const mp_transport_opts* opts,
                                    const double* H, const double* C, const double* vs_n, const double* ud_n,
                                    double* rhsH, double* rhsC, double* T, double* phi, double* rate,

@@ -134,6 +134,10 @@ def lib() -> C.CDLL:
         "mp_transport_rhs": (i, [vp, vp, vp, vp, vp, vp, C.POINTER(StageTotals)]),
         "mp_transport_step": (i, [vp, i, C.POINTER(StepReport)]),
         "mp_transport_limiter": (i, [vp, vp, vp]),
+        "mp_transport_set_device_steps": (i, [vp, i]),
+        "mp_transport_run_stats": (i, [vp, C.POINTER(C.c_ulonglong)]),
+        "mp_batch_set_device_steps": (i, [vp, i]),
+        "mp_batch_run_stats": (i, [vp, C.POINTER(C.c_ulonglong)]),
         "mp_transport_profile": (i, [vp, i]),
         "mp_transport_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
         "mp_probe_fp64_peak": (i, [vp, C.POINTER(C.c_double)]),

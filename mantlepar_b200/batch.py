@@ -100,6 +100,17 @@ class Batch:
         return [[{k: getattr(reps[s * slots + i], k) for k in REPORT_FIELDS} for i in range(slots)]
                 for s in range(nsteps)]
 
+    def set_device_steps(self, enable: bool = True):
+        """step() as CUDA graphs with every instance's step decisions on the
+        device (default) or as the host-driven loop."""
+        _capi.check(self._lib.mp_batch_set_device_steps(self._h, int(enable)))
+
+    def host_syncs(self) -> int:
+        """Host waits for device results made by step() so far."""
+        n = C.c_ulonglong(0)
+        _capi.check(self._lib.mp_batch_run_stats(self._h, C.byref(n)))
+        return n.value
+
     def autotune(self, reps: int = 2):
         tile = (C.c_int * 3)()
         best = C.c_double(0)

@@ -17,6 +17,7 @@
 #include "phase_math.cuh"
 #include "stage_device.cuh"
 #include "stage_kernels.cuh"
+#include "step_ctl.cuh"
 #include "tables.hpp"
 
 #include <algorithm>
@@ -28,6 +29,7 @@ namespace mp {
 
 PhaseConst phase_const(const mp_material& p, const mp_derived& d);
 mp_status derive_checked(const mp_material& p, mp_derived& d);
+mp_status validate_opts(const mp_transport_opts& o, mp_derived* der_out);
 
 namespace {
 
@@ -52,6 +54,13 @@ struct AxpyArgs {
     const double* dtp;
     double area;
     Partial* partial;
+};
+
+// Commit of an accepted step: the stage state that holds U^{n+1} becomes U^n.
+struct CommitArgs {
+    int n;
+    const double *srcH, *srcC;
+    double *dstH, *dstC;
 };
 
 // Work items: block -> instance and the first element of its tile (faces:
@@ -113,6 +122,20 @@ __global__ void __launch_bounds__(kRedBlock) batch_axpy_kernel(const AxpyArgs* a
     const AxpyArgs& a = args[w.inst];
     const Partial v = axpy_cells(a.n, a.H0, a.C0, a.LH, a.LC, *a.dtp, a.area, a.H1, a.C1, w.a);
     block_reduce_write(v, a.partial + w.part);
+}
+
+// Copy of U^{n+1} into U^n for the instances that accepted their step (the
+// accumulation work list: kSumCells cells per block).
+__global__ void __launch_bounds__(kRedBlock) batch_commit_kernel(const CommitArgs* args, const Work* work,
+                                                                 const int* active) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    const CommitArgs& a = args[w.inst];
+#pragma unroll
+    for (int q = 0; q < kSumPer; ++q) {
+        const long long k = (long long)w.a + q * kRedBlock + threadIdx.x;
+        if (k < a.n) { a.dstH[k] = a.srcH[k]; a.dstC[k] = a.srcC[k]; }
+    }
 }
 
 // One block per instance: fixed-order reduction of its block partials (the
@@ -190,6 +213,21 @@ struct mp_batch {
     int* h_active = nullptr;
     mp::Tuning tune;
     size_t bytes_in_use = 0;
+    // Device-resident stepping: one CUDA graph runs up to kGraphChunk steps
+    // of every instance (step and attempt loops as conditional WHILE nodes,
+    // decisions by the step controller); rebuilt when captured arguments
+    // change (gen).
+    bool use_graph = true;
+    unsigned long long gen = 1, graph_gen = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_slots = 0;
+    mp::InstCtl *d_ctl = nullptr, *h_ctl = nullptr;
+    mp::CtlHeader *d_hdr = nullptr, *h_hdr = nullptr;
+    mp_step_report *d_rep = nullptr, *h_rep = nullptr;
+    mp::CommitArgs* d_commit = nullptr;
+    int stage_kernels = 0;             // kernels of one stage kind (graph launch count)
+    unsigned long long host_syncs = 0; // host waits of the stepping calls
     // profiling
     bool profile = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -297,6 +335,7 @@ mp_status rebuild_args(mp_batch* b, int slots) {
     std::vector<InstArgs<R>> args[NKIND];
     for (int k = 0; k < NKIND; ++k) args[k].resize(slots);
     std::vector<AxpyArgs> ax(slots);
+    std::vector<CommitArgs> cm(slots);
     std::vector<int> part_off(slots, 0), part_cnt(slots, 0);
     std::vector<Work> wr, wp, wf, ws;
     int parts = 0;
@@ -329,6 +368,8 @@ mp_status rebuild_args(mp_batch* b, int slots) {
         }
         ax[i] = AxpyArgs{(int)in.N, in.H, in.C, in.LH, in.LC, in.S1H, in.S1C, b->d_dt + i, in.host_tab.area,
                          b->d_partial + parts};
+        const bool rk3 = b->opts.integrator == MP_SSPRK3;
+        cm[i] = CommitArgs{(int)in.N, rk3 ? in.S1H : in.S2H, rk3 ? in.S1C : in.S2C, in.H, in.C};
         for (int ty = 0; ty < in.ny; ty += tu.by)
             for (int tx = 0; tx < in.nx; tx += tu.bx * tu.cpt) wr.push_back(Work{i, tx, ty, 0});
         for (size_t c = 0; c < in.N; c += 128) wp.push_back(Work{i, (int)c, 0, 0});
@@ -346,6 +387,8 @@ mp_status rebuild_args(mp_batch* b, int slots) {
     size_t dummy = 0;
     MP_TRY(ensure(&b->d_axpy, slots, dummy, s));
     MP_CUDA(cudaMemcpyAsync(b->d_axpy, ax.data(), slots * sizeof(AxpyArgs), cudaMemcpyHostToDevice, s));
+    MP_TRY(ensure(&b->d_commit, slots, dummy, s));
+    MP_CUDA(cudaMemcpyAsync(b->d_commit, cm.data(), slots * sizeof(CommitArgs), cudaMemcpyHostToDevice, s));
     MP_TRY(ensure(&b->d_wrecon, wr.size(), dummy, s));
     MP_TRY(ensure(&b->d_wphase, wp.size(), dummy, s));
     MP_TRY(ensure(&b->d_wface, wf.size(), dummy, s));
@@ -397,6 +440,7 @@ mp_status rebuild(mp_batch* b) {
     if (b->mixed) MP_TRY(rebuild_args<float>(b, slots));
     else MP_TRY(rebuild_args<double>(b, slots));
     b->dirty = false;
+    b->gen += 1;      // the captured graph refers to the old argument arrays
     return MP_OK;
 }
 
@@ -424,6 +468,7 @@ void launch_kind(mp_batch* b, int kind) {
 
 // Stage of one kind on the active instances; totals and status to the host.
 mp_status run_stage(mp_batch* b, int kind, const std::vector<int>& act) {
+    NvtxRange range("mp_batch stage");
     MP_TRY(set_active(b, act));
     const int slots = (int)b->inst.size();
     MP_CUDA(cudaMemsetAsync(b->d_status, 0xff, slots * sizeof(unsigned long long), b->stream));
@@ -433,6 +478,7 @@ mp_status run_stage(mp_batch* b, int kind, const std::vector<int>& act) {
     MP_CUDA(cudaMemcpyAsync(b->h_tot, b->d_tot, slots * sizeof(Totals), cudaMemcpyDeviceToHost, b->stream));
     MP_CUDA(cudaMemcpyAsync(b->h_status, b->d_status, slots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->stream));
     MP_CUDA(cudaStreamSynchronize(b->stream));
+    b->host_syncs += 1;
     harvest(b);
     return MP_OK;
 }
@@ -448,6 +494,7 @@ mp_status run_axpy(mp_batch* b, const std::vector<int>& act) {
     MP_CUDA(cudaGetLastError());
     MP_CUDA(cudaMemcpyAsync(b->h_tot, b->d_tot, slots * sizeof(Totals), cudaMemcpyDeviceToHost, s));
     MP_CUDA(cudaStreamSynchronize(s));
+    b->host_syncs += 1;
     harvest(b);
     return MP_OK;
 }
@@ -483,6 +530,7 @@ mp_status eval_missing(mp_batch* b) {
 
 // One accepted step of every healthy instance (the reference's loop per instance).
 mp_status step_all(mp_batch* b, std::vector<mp_step_report>& reps) {
+    NvtxRange range("mp_batch step (host loop)");
     MP_TRY(rebuild(b));
     MP_TRY(eval_missing(b));
     const int slots = (int)b->inst.size();
@@ -629,6 +677,197 @@ mp_status autotune(mp_batch* b, int reps, double* best_ms) {
     return MP_OK;
 }
 
+// ------------------------------------------------------- device-resident steps
+
+constexpr int kGraphChunk = 64;        // steps per graph launch (report rows)
+
+StepOpts step_opts(const mp_batch* b) {
+    const mp_transport_opts& o = b->opts;
+    StepOpts so{};
+    so.cfl = o.cfl; so.dt_initial = o.dt_initial; so.dt_max = o.dt_max; so.dt_min = o.dt_min; so.Xe = o.material.Xe;
+    so.rk3 = o.integrator == MP_SSPRK3;
+    so.fixed = 0;
+    so.snap_end = 1; so.end_reports = 0; so.restore_time = 0;
+    return so;
+}
+
+// Current leaf nodes of a capture (the dependencies of the next node).
+mp_status capture_leaves(cudaStream_t s, std::vector<cudaGraphNode_t>& out) {
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    MP_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &nd));
+    out.assign(deps, deps + nd);
+    return MP_OK;
+}
+
+// A conditional WHILE node in `g` after `deps`; its body graph in *body.
+mp_status add_while(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, cudaGraphConditionalHandle h,
+                    cudaGraphNode_t* node, cudaGraph_t* body) {
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    MP_CUDA(cudaGraphAddNode(node, g, deps.empty() ? nullptr : deps.data(), deps.size(), &p));
+    *body = p.conditional.phGraph_out[0];
+    return MP_OK;
+}
+
+// The graph of up to kGraphChunk steps of every instance:
+//   WHILE run:  begin -> WHILE attempt: {attempt, axpy, reduce, gate,
+//               stage B, control [, stage C, control]} -> commit, copy,
+//               stage P (L(U^{n+1})), control (run condition).
+template <class R>
+mp_status capture_graph(mp_batch* b, cudaGraph_t* out) {
+    cudaStream_t s = b->stream;
+    const int slots = (int)b->inst.size();
+    const StepOpts so = step_opts(b);
+    const bool rk3 = so.rk3 != 0;
+    cudaGraph_t g = nullptr;
+    MP_CUDA(cudaGraphCreate(&g, 0));
+    *out = g;
+    cudaGraphConditionalHandle run, attempt;
+    MP_CUDA(cudaGraphConditionalHandleCreate(&run, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNode_t run_node, attempt_node;
+    cudaGraph_t step_body, attempt_body;
+    MP_TRY(add_while(g, {}, run, &run_node, &step_body));
+    MP_CUDA(cudaGraphConditionalHandleCreate(&attempt, step_body, 0, 0));
+    const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+    cudaGraph_t tmp;
+    // Step begin.
+    MP_CUDA(cudaStreamBeginCaptureToGraph(s, step_body, nullptr, nullptr, 0, mode));
+    ctl_begin_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_hdr, b->d_rep, attempt);
+    std::vector<cudaGraphNode_t> leaves;
+    MP_TRY(capture_leaves(s, leaves));
+    MP_CUDA(cudaStreamEndCapture(s, &tmp));
+    MP_TRY(add_while(step_body, leaves, attempt, &attempt_node, &attempt_body));
+    // One attempt.
+    MP_CUDA(cudaStreamBeginCaptureToGraph(s, attempt_body, nullptr, nullptr, 0, mode));
+    ctl_attempt_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_hdr, b->d_active, b->d_dt);
+    if (b->n_wsum) batch_axpy_kernel<<<b->n_wsum, kRedBlock, 0, s>>>(b->d_axpy, b->d_wsum, b->d_active);
+    batch_reduce_kernel<<<slots, 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot);
+    ctl_after_axpy_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_tot, b->d_status, b->d_active);
+    launch_kind<R>(b, KIND_B);
+    ctl_after_stage_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_tot, b->d_status, b->d_active, 2,
+                                                      rk3 ? 0 : 1, b->d_hdr, attempt);
+    if (rk3) {
+        launch_kind<R>(b, KIND_C);
+        ctl_after_stage_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_tot, b->d_status, b->d_active, 3, 1,
+                                                          b->d_hdr, attempt);
+    }
+    MP_CUDA(cudaStreamEndCapture(s, &tmp));
+    // Commit and L(U^{n+1}).
+    MP_CUDA(cudaStreamBeginCaptureToGraph(s, step_body, &attempt_node, nullptr, 1, mode));
+    ctl_commit_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_hdr, b->d_rep, b->d_status, b->d_active);
+    if (b->n_wsum) batch_commit_kernel<<<b->n_wsum, kRedBlock, 0, s>>>(b->d_commit, b->d_wsum, b->d_active);
+    launch_kind<R>(b, KIND_P);
+    ctl_after_rhs_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_tot, b->d_status, b->d_rep, b->d_hdr, 0,
+                                                    run);
+    MP_CUDA(cudaStreamEndCapture(s, &tmp));
+    MP_CUDA(cudaGetLastError());
+    return MP_OK;
+}
+
+void release_graph(mp_batch* b) {
+    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->graph_exec = nullptr;
+    b->graph = nullptr;
+    b->graph_gen = 0;
+}
+
+mp_status ensure_graph(mp_batch* b) {
+    const int slots = (int)b->inst.size();
+    cudaStream_t s = b->stream;
+    if (slots > b->graph_slots) {
+        for (void* p : {(void*)b->d_ctl, (void*)b->d_hdr, (void*)b->d_rep}) if (p) cudaFreeAsync(p, s);
+        for (void* p : {(void*)b->h_ctl, (void*)b->h_hdr, (void*)b->h_rep}) if (p) cudaFreeHost(p);
+        const int cap = std::max(slots, 8);
+        MP_CUDA(cudaMallocAsync((void**)&b->d_ctl, cap * sizeof(InstCtl), s));
+        MP_CUDA(cudaMallocAsync((void**)&b->d_hdr, sizeof(CtlHeader), s));
+        MP_CUDA(cudaMallocAsync((void**)&b->d_rep, (size_t)kGraphChunk * cap * sizeof(mp_step_report), s));
+        MP_CUDA(cudaMallocHost((void**)&b->h_ctl, cap * sizeof(InstCtl)));
+        MP_CUDA(cudaMallocHost((void**)&b->h_hdr, sizeof(CtlHeader)));
+        MP_CUDA(cudaMallocHost((void**)&b->h_rep, (size_t)kGraphChunk * cap * sizeof(mp_step_report)));
+        b->graph_slots = cap;
+        b->gen += 1;
+    }
+    if (b->graph_exec && b->graph_gen == b->gen) return MP_OK;
+    release_graph(b);
+    b->stage_kernels = (b->n_wrecon ? 1 : 0) + (b->n_wphase ? 1 : 0) + (b->n_wface ? 1 : 0) +
+                       (b->n_wface && b->ph.diffusion ? 1 : 0) + (b->n_wsum ? 1 : 0) + 1;
+    // Capture on a private stream (the caller's may be the legacy default
+    // stream, which cannot be captured); the graph runs on the caller's.
+    cudaStream_t cap = nullptr;
+    MP_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaStream_t user = b->stream;
+    b->stream = cap;
+    g_capturing = true;
+    const mp_status st = b->mixed ? capture_graph<float>(b, &b->graph) : capture_graph<double>(b, &b->graph);
+    g_capturing = false;
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(cap, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        cudaGraph_t tmp;
+        cudaStreamEndCapture(cap, &tmp);
+    }
+    b->stream = user;
+    cudaStreamDestroy(cap);
+    if (st != MP_OK) { release_graph(b); return st; }
+    MP_CUDA(cudaGraphInstantiate(&b->graph_exec, b->graph, 0));
+    b->graph_gen = b->gen;
+    return MP_OK;
+}
+
+// nsteps steps of every instance on the device: one graph launch and one host
+// wait per kGraphChunk steps. Same decisions and results as step_all.
+mp_status graph_steps(mp_batch* b, int nsteps, mp_step_report* reports) {
+    NvtxRange range("mp_batch steps (device-resident graph)");
+    MP_TRY(rebuild(b));
+    MP_TRY(eval_missing(b));
+    MP_TRY(ensure_graph(b));
+    const int slots = (int)b->inst.size();
+    cudaStream_t s = b->stream;
+    for (int done = 0; done < nsteps; done += kGraphChunk) {
+        const int chunk = std::min(kGraphChunk, nsteps - done);
+        for (int i = 0; i < slots; ++i) {
+            const MPInstance& in = b->inst[i];
+            InstCtl& c = b->h_ctl[i];
+            c = InstCtl{};
+            c.used = in.used ? 1 : 0;
+            c.time = in.time; c.t_end = in.t_end;
+            c.accepted = in.accepted; c.status = in.status; c.have_L = in.have_L ? 1 : 0;
+            c.cur = in.cur;
+        }
+        *b->h_hdr = CtlHeader{0, chunk, 0, 0, 0};
+        MP_CUDA(cudaMemcpyAsync(b->d_ctl, b->h_ctl, slots * sizeof(InstCtl), cudaMemcpyHostToDevice, s));
+        MP_CUDA(cudaMemcpyAsync(b->d_hdr, b->h_hdr, sizeof(CtlHeader), cudaMemcpyHostToDevice, s));
+        MP_CUDA(cudaGraphLaunch(b->graph_exec, s));
+        MP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, slots * sizeof(InstCtl), cudaMemcpyDeviceToHost, s));
+        MP_CUDA(cudaMemcpyAsync(b->h_hdr, b->d_hdr, sizeof(CtlHeader), cudaMemcpyDeviceToHost, s));
+        MP_CUDA(cudaMemcpyAsync(b->h_rep, b->d_rep, (size_t)chunk * slots * sizeof(mp_step_report),
+                                cudaMemcpyDeviceToHost, s));
+        MP_CUDA(cudaStreamSynchronize(s));
+        b->host_syncs += 1;
+        const CtlHeader h = *b->h_hdr;
+        // Kernels the graph ran: per step 5 control/copy kernels and one
+        // stage; per attempt 4 control/axpy kernels and one or two stages.
+        const int per_attempt = 4 + (b->stage_kernels + 1) * (b->opts.integrator == MP_SSPRK3 ? 2 : 1);
+        count_launch((unsigned long long)h.step * (3 + b->stage_kernels + 1) +
+                     (unsigned long long)h.total_attempts * per_attempt);
+        for (int i = 0; i < slots; ++i) {
+            MPInstance& in = b->inst[i];
+            if (!in.used) continue;
+            const InstCtl& c = b->h_ctl[i];
+            in.time = c.time; in.accepted = c.accepted; in.status = c.status; in.have_L = c.have_L != 0;
+            in.cur = c.cur;
+        }
+        if (reports)
+            std::memcpy(reports + (size_t)done * slots, b->h_rep, (size_t)chunk * slots * sizeof(mp_step_report));
+    }
+    return MP_OK;
+}
+
 }  // namespace
 }  // namespace mp
 
@@ -638,13 +877,9 @@ extern "C" mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, cons
                                      mp_stream_t stream, mp_batch** out) {
     using namespace mp;
     if (!opts || !out || count < 0 || (count > 0 && !meshes)) { set_error("null argument"); return MP_ERR_ARG_WRONG; }
-    if (!(opts->cfl > 0 && opts->cfl <= 1)) { set_error("Coupled CFL must be in (0,1]"); return MP_ERR_ARG_OUTOFRANGE; }
-    if (opts->integrator != MP_SSPRK2 && opts->integrator != MP_SSPRK3) { set_error("integrator must be 2 or 3"); return MP_ERR_ARG_OUTOFRANGE; }
-    if (!(std::isfinite(opts->diffusivity) && opts->diffusivity >= 0.0)) { set_error("Diffusivity must be finite and nonnegative"); return MP_ERR_ARG_OUTOFRANGE; }
-    if (opts->material.alpha0 != 0.0) { set_error("the batched engine does not take cell-point velocities: adiabatic source (alpha0 != 0) needs the single-instance path"); return MP_ERR_ARG_WRONG; }
-    if (opts->precision != MP_PRECISION_FP64 && opts->precision != MP_PRECISION_MIXED) { set_error("unknown precision"); return MP_ERR_ARG_OUTOFRANGE; }
     mp_derived der;
-    MP_TRY(derive_checked(opts->material, der));
+    MP_TRY(validate_opts(*opts, &der));
+    if (opts->material.alpha0 != 0.0) { set_error("the batched engine does not take cell-point velocities: adiabatic source (alpha0 != 0) needs the single-instance path"); return MP_ERR_ARG_WRONG; }
     mp_batch* b = new mp_batch;
     b->opts = *opts; b->der = der;
     b->stream = (cudaStream_t)stream;
@@ -674,6 +909,9 @@ extern "C" mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, cons
 extern "C" void mp_batch_destroy(mp_batch* b) {
     if (!b) return;
     cudaStreamSynchronize(b->stream);
+    mp::release_graph(b);
+    for (void* p : {(void*)b->d_ctl, (void*)b->d_hdr, (void*)b->d_rep, (void*)b->d_commit}) if (p) cudaFreeAsync(p, b->stream);
+    for (void* p : {(void*)b->h_ctl, (void*)b->h_hdr, (void*)b->h_rep}) if (p) cudaFreeHost(p);
     for (MPInstance& in : b->inst) if (in.used && in.arena) cudaFreeAsync(in.arena, b->stream);
     for (int k = 0; k < mp::NKIND; ++k) if (b->d_args[k]) cudaFreeAsync(b->d_args[k], b->stream);
     for (void* p : {(void*)b->d_axpy, (void*)b->d_wrecon, (void*)b->d_wphase, (void*)b->d_wface, (void*)b->d_wsum,
@@ -750,7 +988,9 @@ extern "C" mp_status mp_batch_get_state(mp_batch* b, int i, double* H, double* C
     if (C) MP_CUDA(cudaMemcpyAsync(C, in->C, by, cudaMemcpyDefault, b->stream));
     if (T) MP_CUDA(cudaMemcpyAsync(T, in->T, by, cudaMemcpyDefault, b->stream));
     if (phi) MP_CUDA(cudaMemcpyAsync(phi, in->phi, by, cudaMemcpyDefault, b->stream));
-    MP_CUDA(cudaStreamSynchronize(b->stream));
+    // time, accepted and status are host records, current once a step call
+    // has returned: no wait unless an array was requested.
+    if (H || C || T || phi) MP_CUDA(cudaStreamSynchronize(b->stream));
     if (time) *time = in->time;
     if (accepted) *accepted = in->accepted;
     if (status) *status = in->status;
@@ -759,6 +999,10 @@ extern "C" mp_status mp_batch_get_state(mp_batch* b, int i, double* H, double* C
 
 extern "C" mp_status mp_batch_step(mp_batch* b, int nsteps, mp_step_report* reports) {
     if (!b) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (nsteps < 0) { mp::set_error("nsteps must be nonnegative"); return MP_ERR_ARG_OUTOFRANGE; }
+    bool any = false;
+    for (const MPInstance& in : b->inst) any = any || in.used;
+    if (b->use_graph && !b->profile && any && nsteps > 0) return mp::graph_steps(b, nsteps, reports);
     std::vector<mp_step_report> reps;
     const int slots = (int)b->inst.size();
     for (int k = 0; k < nsteps; ++k) {
@@ -824,5 +1068,18 @@ extern "C" mp_status mp_batch_set_thermal_bc(mp_batch* b, const int* type, const
     }
     b->ph.diffusion = b->ph.kappa > 0.0 || flux;
     for (auto& in : b->inst) in.have_L = false;
+    b->gen += 1;      // the stage kernels take the physics by value
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_set_device_steps(mp_batch* b, int enable) {
+    if (!b) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    b->use_graph = enable != 0;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_run_stats(const mp_batch* b, unsigned long long* host_syncs) {
+    if (!b || !host_syncs) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    *host_syncs = b->host_syncs;
     return MP_OK;
 }

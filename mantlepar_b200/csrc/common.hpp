@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -16,7 +18,23 @@ namespace mp {
 void set_error(const char* fmt, ...);
 extern std::atomic<unsigned long long> g_launches;
 
-inline void count_launch(unsigned long long n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+// Set while this thread captures a CUDA graph: captured launches are counted
+// when the graph runs, not when it is built.
+inline thread_local bool g_capturing = false;
+
+inline void count_launch(unsigned long long n = 1) {
+    if (!g_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+
+// A named NVTX range over a scope of host work (stage launches, step loops,
+// graph runs), for a profiler's timeline; without an attached tool the push
+// and pop do nothing.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Map a CUDA error to MP_ERR_CUDA (or MP_ERR_NOMEM) and record its text.
 inline mp_status cuda_status(cudaError_t e, const char* what) {

@@ -14,16 +14,17 @@
 //  - at most kMaxCells cells (nx*ny <= 32768); larger meshes are rejected
 //    with MP_ERR_ARG_SIZ; the array holds about 7.3 MB on every GPU that
 //    loads this library, until the process exits;
-//  - the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current, so make the first
-//    call on each device before any stream capture;
+//  - every call looks up the array's device address on the current device
+//    (cudaGetSymbolAddress, a host-side lookup with no device work), so a
+//    context that was torn down and created again is served at its new
+//    address;
+//  - the call is synchronous: it reads the stage totals and the status word
+//    back to the host and waits for the stream;
 //  - all calls share the array, and each call overwrites what the previous
 //    one left there; calls whose work overlaps on the GPU race on it, so
 //    issue them in one stream or serialise them.
 #include "common.hpp"
 #include "tables.hpp"
-
-#include <mutex>
 
 namespace mp {
 
@@ -33,6 +34,7 @@ mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double
                         void* totals, unsigned long long* status, mp_stage_totals* out, cudaStream_t s);
 size_t raw_partial_bytes(size_t ncell);
 size_t raw_totals_bytes();
+mp_status validate_opts(const mp_transport_opts& o, mp_derived* der_out);
 
 namespace {
 
@@ -51,20 +53,12 @@ constexpr size_t kScratchBytes = kStatOff + 256;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-std::mutex g_lock;
-void* g_addr[256] = {};   // device address of g_scratch per device ordinal
-
+// The device address of g_scratch in the current context. In host code the
+// array's name is only a host-side stand-in; kernels need this address.
 mp_status scratch_address(unsigned char** out) {
-    int dev = 0;
-    MP_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 256) { set_error("device ordinal out of range"); return MP_ERR_ARG_OUTOFRANGE; }
-    std::lock_guard<std::mutex> guard(g_lock);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        MP_CUDA(cudaGetSymbolAddress(&p, g_scratch));
-        g_addr[dev] = p;
-    }
-    *out = static_cast<unsigned char*>(g_addr[dev]);
+    void* p = nullptr;
+    MP_CUDA(cudaGetSymbolAddress(&p, g_scratch));
+    *out = static_cast<unsigned char*>(p);
     return MP_OK;
 }
 
@@ -87,6 +81,8 @@ extern "C" mp_status mp_transport_rhs_noalloc(const mp_mesh_desc* mesh, const mp
         set_error("mp_transport_rhs_noalloc: %zu cells exceed its fixed scratch limit of %zu cells", N, kMaxCells);
         return MP_ERR_ARG_SIZ;
     }
+    // The same option checks as mp_transport_create, then this entry point's own limits.
+    MP_TRY(validate_opts(*opts, nullptr));
     if (opts->diffusivity != 0.0) { set_error("thermal diffusion (kappa > 0) is not supported by mp_transport_rhs_noalloc"); return MP_ERR_ARG_WRONG; }
     if (opts->material.alpha0 != 0.0) { set_error("adiabatic source (alpha0 != 0) is not supported by mp_transport_rhs_noalloc"); return MP_ERR_ARG_WRONG; }
     if (opts->precision != MP_PRECISION_FP64) { set_error("mp_transport_rhs_noalloc evaluates the FP64 stage"); return MP_ERR_ARG_WRONG; }

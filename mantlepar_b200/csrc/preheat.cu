@@ -188,7 +188,6 @@ __global__ void __launch_bounds__(128) pre_recon_kernel(int nx, int ny, const do
     if (halted(status)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= nx || j >= ny) return;
-    const Tab<double> tab = param_tab<double>(p);
     const StageHot& t = p.d;
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
@@ -202,7 +201,7 @@ __global__ void __launch_bounds__(128) pre_recon_kernel(int nx, int ny, const do
         }
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
     double D[9];
-    const int st = reconstruct<double>(tab, t, ci, cj, u, D);
+    const int st = reconstruct(t, ci, cj, u, D);
 #pragma unroll
     for (int m = 0; m < 9; ++m) rec[(size_t)m * N + cell] = D[m];
     if (st) record_error(status, PART_UPDATE, cell, st);
@@ -448,7 +447,6 @@ __global__ void __launch_bounds__(128) pre_diag_kernel(int nx, int ny, const dou
                                                        const __grid_constant__ ParamTables p) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= nx || j >= ny) return;
-    const Tab<double> tab = param_tab<double>(p);
     const StageHot& t = p.d;
     const long long cell = (long long)j * nx + i;
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = j == 0 ? 0 : (j == ny - 1 ? 2 : 1);
@@ -464,7 +462,7 @@ __global__ void __launch_bounds__(128) pre_diag_kernel(int nx, int ny, const dou
                 u[dj][di] = __ldg(F + (size_t)jj * nx + ii);
             }
         m[f] = u[1][1];
-        const int s = reconstruct<double>(tab, t, ci, cj, u, D[f]);
+        const int s = reconstruct(t, ci, cj, u, D[f]);
         st = st ? st : s;
     }
     if (st) { record_error(status, PART_UPDATE, cell, st); return; }
@@ -1085,6 +1083,7 @@ extern "C" mp_status mp_preheat_rhs(mp_preheat* p, double* rhs, double* boundary
 }
 
 extern "C" mp_status mp_preheat_advance(mp_preheat* p, long long nsteps, mp_preheat_step* rows, long long* taken) {
+    mp::NvtxRange range("mp_preheat advance");
     using namespace mp;
     if (taken) *taken = 0;
     if (!p) { set_error("null argument"); return MP_ERR_ARG_WRONG; }

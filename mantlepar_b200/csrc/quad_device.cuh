@@ -248,7 +248,7 @@ __device__ __forceinline__ int reconstruct_quad(const QuadDev& q, size_t N, long
     }
     double w[F][5];
 #pragma unroll
-    for (int f = 0; f < F; ++f) weights<double>(sg[f], on, eA, w[f]);
+    for (int f = 0; f < F; ++f) weights(sg[f], on, eA, w[f]);
 #pragma unroll
     for (int f = 0; f < F; ++f)
         if (!isfinite(w[f][0] + w[f][1] + w[f][2] + w[f][3] + w[f][4])) st[f] = MP_ERR_FP;

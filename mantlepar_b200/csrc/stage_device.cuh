@@ -7,9 +7,12 @@
 //   R(x) = u_t + sum_k w_k P_k(x)  ==  u_t + D(xi, eta),
 // the 2x2 candidates being re-expanded about the target centre. The limiter
 // (state_reconstruction.cpp:136-192) then scales D by theta, so each limited
-// evaluation at a point is one 9-term polynomial. R is the arithmetic type of
-// the reconstruction (double for the FP64 path, float for the mixed path);
-// centred differences are formed in FP64 before the conversion.
+// evaluation at a point is one 9-term polynomial. Smoothness indicators,
+// weights and coefficients are FP64 in every form: the weights are
+// (sigma + epsA)^-7 ratios, so an FP32 sigma moves them by several FP32 ulps,
+// and the limited values handed to the phase inversion would carry that
+// error (about 3e-9 absolute on a deviation of 0.05, more than the porosity
+// of a cell near the solidus tolerates at 1e-6 relative).
 #ifndef MP_STAGE_DEVICE_CUH
 #define MP_STAGE_DEVICE_CUH
 
@@ -30,6 +33,7 @@ struct StageTablesF {
     float SF4[4][6];
     float X, Y, epsA, logEpsA2;
     float gx[kNQ], gy[kNQ];
+    float mono[9];
     float line_c[kMaxLines];
 };
 
@@ -49,6 +53,7 @@ inline void tables_to_float(const StageHot& t, StageTablesF& f) {
     for (int k = 0; k < 4; ++k) for (int a = 0; a < 6; ++a) f.SF4[k][a] = (float)t.SF4[k][a];
     f.X = (float)t.X; f.Y = (float)t.Y; f.epsA = (float)t.epsA; f.logEpsA2 = (float)(2.0 * std::log(t.epsA));
     for (int q = 0; q < kNQ; ++q) { f.gx[q] = (float)t.gx[q]; f.gy[q] = (float)t.gy[q]; }
+    for (int m = 0; m < 9; ++m) f.mono[m] = (float)t.mono[m];
     for (int l = 0; l < kMaxLines; ++l) f.line_c[l] = (float)t.line_c[l];
 }
 
@@ -74,6 +79,7 @@ template <> struct Tab<double> {
     __device__ double epsA() const { return t->epsA; }
     __device__ double gx(int q) const { return t->gx[q]; }
     __device__ double gy(int q) const { return t->gy[q]; }
+    __device__ double mono(int m) const { return t->mono[m]; }
     __device__ double line_c(int l) const { return t->line_c[l]; }
 };
 template <> struct Tab<float> {
@@ -90,6 +96,7 @@ template <> struct Tab<float> {
     __device__ float epsA() const { return f->epsA; }
     __device__ float gx(int q) const { return f->gx[q]; }
     __device__ float gy(int q) const { return f->gy[q]; }
+    __device__ float mono(int m) const { return f->mono[m]; }
     __device__ float line_c(int l) const { return f->line_c[l]; }
 };
 
@@ -154,85 +161,54 @@ __device__ __forceinline__ R smoothness(GF&& SF, G&& S, const R* diff) {
 // the 3x3 order-2 candidate, 5 for the 2x2 order-1 candidates
 // (reconstruction.cpp:43-54,212-265). Written as ratios r = epsA/(sigma+epsA)
 // in (0,1] with the common factor (epsA)^-7 divided out, so nothing
-// overflows. In FP32 the powers would underflow, so each ratio is split into
-// mantissa and binary exponent and the exponents are summed as integers; the
-// weights are returned normalised in FP64 (sum exactly 1 to FP64 rounding).
-template <class R>
-__device__ __forceinline__ void weights(const R* sig, const bool* on, R eA, double* w) {
-    if constexpr (sizeof(R) == 8) {
-        // The five reciprocals 1/(sigma_k + epsA) from one division: prefix
-        // and suffix products of s_k = sigma_k + epsA (s_k >= epsA > 0).
-        double sk[5], pre[5], suf[5];
+// overflows; normalised to sum 1.
+__device__ __forceinline__ void weights(const double* sig, const bool* on, double eA, double* w) {
+    // The five reciprocals 1/(sigma_k + epsA) from one division: prefix
+    // and suffix products of s_k = sigma_k + epsA (s_k >= epsA > 0).
+    double sk[5], pre[5], suf[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) sk[k] = sig[k] + eA;
-        pre[0] = 1.0;
+    for (int k = 0; k < 5; ++k) sk[k] = sig[k] + eA;
+    pre[0] = 1.0;
 #pragma unroll
-        for (int k = 1; k < 5; ++k) pre[k] = pre[k - 1] * sk[k - 1];
-        suf[4] = 1.0;
+    for (int k = 1; k < 5; ++k) pre[k] = pre[k - 1] * sk[k - 1];
+    suf[4] = 1.0;
 #pragma unroll
-        for (int k = 3; k >= 0; --k) suf[k] = suf[k + 1] * sk[k + 1];
-        const double P = pre[4] * sk[4];
-        double inv_s[5];
-        if (P > 1e-290 && P < 1e290) {
-            const double invP = 1.0 / P;
+    for (int k = 3; k >= 0; --k) suf[k] = suf[k + 1] * sk[k + 1];
+    const double P = pre[4] * sk[4];
+    double inv_s[5];
+    if (P > 1e-290 && P < 1e290) {
+        const double invP = 1.0 / P;
 #pragma unroll
-            for (int k = 0; k < 5; ++k) inv_s[k] = (pre[k] * suf[k]) * invP;
-        } else {
-#pragma unroll
-            for (int k = 0; k < 5; ++k) inv_s[k] = 1.0 / sk[k];
-        }
-        double alpha[5];
-        const double scale = on[0] ? eA * eA : 1.0;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            const double r = eA * inv_s[k];
-            const double r2 = r * r;
-            alpha[k] = !on[k] ? 0.0 : (k == 0 ? r2 * r2 * r2 * r : scale * (r2 * r2 * r));
-        }
-        double sum = 0;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) sum += alpha[k];
-        const double inv = 1.0 / sum;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) w[k] = alpha[k] * inv;
+        for (int k = 0; k < 5; ++k) inv_s[k] = (pre[k] * suf[k]) * invP;
     } else {
-        int ea;
-        const float fa = frexpf(eA, &ea);
-        const float fa2 = fa * fa;
-        float mant[5];
-        int ex[5], emax = -1 << 30;
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            int e;
-            const float f = frexpf(eA / (sig[k] + eA), &e);
-            const float f2 = f * f;
-            if (k == 0) { mant[k] = f2 * f2 * f2 * f; ex[k] = 7 * e; }
-            else { mant[k] = f2 * f2 * f * (on[0] ? fa2 : 1.0f); ex[k] = 5 * e + (on[0] ? 2 * ea : 0); }
-            if (on[k]) emax = max(emax, ex[k]);
-        }
-        double alpha[5], sum = 0;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            alpha[k] = on[k] ? (double)ldexpf(mant[k], max(ex[k] - emax, -200)) : 0.0;
-            sum += alpha[k];
-        }
-        const double inv = 1.0 / sum;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) w[k] = alpha[k] * inv;
+        for (int k = 0; k < 5; ++k) inv_s[k] = 1.0 / sk[k];
     }
+    double alpha[5];
+    const double scale = on[0] ? eA * eA : 1.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const double r = eA * inv_s[k];
+        const double r2 = r * r;
+        alpha[k] = !on[k] ? 0.0 : (k == 0 ? r2 * r2 * r2 * r : scale * (r2 * r2 * r));
+    }
+    double sum = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) sum += alpha[k];
+    const double inv = 1.0 / sum;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) w[k] = alpha[k] * inv;
 }
 
 // Build D (9 coefficients, FP64) for one field from the 3x3 neighbourhood
-// u[dj][di] (index 1,1 = target). The smoothness indicators and the weights
-// are computed in R (FP32 on the mixed path); the coefficients and D stay
-// FP64 because every limited value handed to the phase inversion is built
-// from them. Candidate mask by boundary class (ci, cj): stencils that leave
-// the domain are dropped (reconstruction.cpp:150-153). Returns a nonzero
-// PETSC_ERR_FP-class status when a smoothness form is negative beyond
-// roundoff or the weights cannot be normalised.
-template <class R>
-__device__ __forceinline__ int reconstruct(const Tab<R>& t, const StageHot& td, int ci, int cj,
-                                           const double (&u)[3][3], double (&D)[9]) {
+// u[dj][di] (index 1,1 = target). Candidate mask by boundary class (ci, cj):
+// stencils that leave the domain are dropped (reconstruction.cpp:150-153).
+// Returns a nonzero PETSC_ERR_FP-class status when a smoothness form is
+// negative beyond roundoff or the weights cannot be normalised.
+__device__ __forceinline__ int reconstruct(const StageHot& td, int ci, int cj, const double (&u)[3][3],
+                                           double (&D)[9]) {
+    using R = double;
+    const Tab<double> t{&td};
     double d[3][3];
 #pragma unroll
     for (int a = 0; a < 3; ++a)
@@ -240,7 +216,6 @@ __device__ __forceinline__ int reconstruct(const Tab<R>& t, const StageHot& td, 
         for (int b = 0; b < 3; ++b) d[a][b] = u[a][b] - u[1][1];
     // Candidate order: 3x3 at (-1,-1); 2x2 at (0,-1), (0,0), (-1,-1), (-1,0).
     const int offi[4] = {0, 0, -1, -1}, offj[4] = {-1, 0, -1, 0};
-    static_assert(sizeof(R) == 4 || sizeof(R) == 8, "R is float or double");
     bool on[5];
     on[0] = (ci == 1 && cj == 1);
 #pragma unroll
@@ -273,7 +248,7 @@ __device__ __forceinline__ int reconstruct(const Tab<R>& t, const StageHot& td, 
         if (sig[k + 1] < R(0)) st = MP_ERR_FP;
     }
     double w[5];
-    weights<R>(sig, on, t.epsA(), w);
+    weights(sig, on, t.epsA(), w);
     if (!isfinite(w[0] + w[1] + w[2] + w[3] + w[4])) st = MP_ERR_FP;
     // Pass 2: weighted coefficients accumulated into D (FP64).
 #pragma unroll

@@ -121,6 +121,7 @@ struct ReconArgs {
     unsigned long long* status;
     double* theta;         // optional (2 * ncell): limiter factors for H, C
     int gj0 = 0, gny = 0;  // slab: global row of local row 0, global rows
+    const int* gate = nullptr;   // device flag: the launch does nothing while it is 0
 };
 
 // Max/min of the deviation polynomial over the class's limiter points by
@@ -168,8 +169,17 @@ __device__ __forceinline__ void line_candidates(const StageHot& t, const Tab<R>&
 // and the larger of a pair is e_k + |a1| s_k: three candidates per line for
 // the maximum and three for the minimum. With every |D_m| below scan_guard
 // no value can overflow, so no per-point finiteness test is needed;
-// otherwise the exact scan runs. For R = float the lines holding the
-// extremes are evaluated again in FP64, so theta is formed from FP64 values.
+// otherwise the exact scan runs.
+//
+// R = float screens the lines in FP32 and returns the FP64 scan's values
+// exactly. An FP32 candidate and the FP64 candidate of the same point differ
+// by less than err = 1.5e-6 (|D_0| + beta) (beta = sum_m>0 |D_m| mono[m]
+// bounds the polynomial's variation over the points; the FP32 evaluation
+// makes about ten roundings of 2^-24 of that magnitude, its coordinates
+// included, the FP64 one far less). When the leading line of an extreme is
+// ahead of the runner-up by more than 2 err, the FP64 extreme lies on it,
+// and that line alone is evaluated again in FP64 (same operations as the
+// FP64 scan, so the same value); otherwise the FP64 scan runs.
 template <class R>
 __device__ __forceinline__ void scan_lines(const StageHot& t, const Tab<R>& tb, int l0, int l1, const double* Dd,
                                            double& mx, double& mn, bool& bad) {
@@ -177,46 +187,51 @@ __device__ __forceinline__ void scan_lines(const StageHot& t, const Tab<R>& tb, 
 #pragma unroll
     for (int m = 0; m < 9; ++m) small = small && fabs(Dd[m]) < t.scan_guard;
     if (!small) { scan_lines_exact(t, l0, l1, Dd, mx, mn, bad); return; }
-    R D[9];
+    const Tab<double> td{&t};
+    const double gx1 = t.gx[3], gx2 = t.gx[4], gy1 = t.gy[3], gy2 = t.gy[4];
+    const double hx1 = gx1 * gx1, hx2 = gx2 * gx2, hy1 = gy1 * gy1, hy2 = gy2 * gy2;
+    if constexpr (sizeof(R) == 4) {
+        float D[9];
 #pragma unroll
-    for (int m = 0; m < 9; ++m) D[m] = (R)Dd[m];
-    const R sx1 = tb.gx(3), sx2 = tb.gx(4), sy1 = tb.gy(3), sy2 = tb.gy(4);
-    const R qx1 = sx1 * sx1, qx2 = sx2 * sx2, qy1 = sy1 * sy1, qy2 = sy2 * sy2;
-    if constexpr (sizeof(R) == 8) {
-        double rmx = D[0], rmn = D[0];   // cell centre
-        for (int l = l0; l < l1; ++l) {
-            double p0, p1, p2, m1, m2;
-            line_candidates<double>(t, tb, l, D, sx1, sx2, sy1, sy2, qx1, qx2, qy1, qy2, p0, p1, p2, m1, m2);
-            rmx = p0 > rmx ? p0 : rmx; rmx = p1 > rmx ? p1 : rmx; rmx = p2 > rmx ? p2 : rmx;
-            rmn = p0 < rmn ? p0 : rmn; rmn = m1 < rmn ? m1 : rmn; rmn = m2 < rmn ? m2 : rmn;
-        }
-        mx = rmx; mn = rmn;
-    } else {
-        // FP32: keep the line holding each extreme; its candidates are then
-        // evaluated again in FP64.
-        float rmx = D[0], rmn = D[0];
-        int lmx = -1, lmn = -1;          // -1 = centre
+        for (int m = 0; m < 9; ++m) D[m] = (float)Dd[m];
+        float beta = 0.0f;
+#pragma unroll
+        for (int m = 1; m < 9; ++m) beta = fmaf(fabsf(D[m]), tb.mono(m), beta);
+        const float err2 = 3.0e-6f * (fabsf(D[0]) + beta);
+        const float sx1 = tb.gx(3), sx2 = tb.gx(4), sy1 = tb.gy(3), sy2 = tb.gy(4);
+        const float qx1 = sx1 * sx1, qx2 = sx2 * sx2, qy1 = sy1 * sy1, qy2 = sy2 * sy2;
+        float rmx = D[0], rmn = D[0];                 // the centre leads at first (line -1)
+        float smx = -INFINITY, smn = INFINITY;        // runners-up
+        int lmx = -1, lmn = -1;
         for (int l = l0; l < l1; ++l) {
             float p0, p1, p2, m1, m2;
             line_candidates<float>(t, tb, l, D, sx1, sx2, sy1, sy2, qx1, qx2, qy1, qy2, p0, p1, p2, m1, m2);
             const float lx = fmaxf(p0, fmaxf(p1, p2)), ln = fminf(p0, fminf(m1, m2));
-            if (lx > rmx) { rmx = lx; lmx = l; }
-            if (ln < rmn) { rmn = ln; lmn = l; }
+            if (lx > rmx) { smx = rmx; rmx = lx; lmx = l; } else { smx = fmaxf(smx, lx); }
+            if (ln < rmn) { smn = rmn; rmn = ln; lmn = l; } else { smn = fminf(smn, ln); }
         }
-        const Tab<double> td{&t};
-        const double gx1 = t.gx[3], gx2 = t.gx[4], gy1 = t.gy[3], gy2 = t.gy[4];
-        const double hx1 = gx1 * gx1, hx2 = gx2 * gx2, hy1 = gy1 * gy1, hy2 = gy2 * gy2;
-        mx = Dd[0]; mn = Dd[0];
-        double p0, p1, p2, m1, m2;
-        if (lmx >= 0) {
-            line_candidates<double>(t, td, lmx, Dd, gx1, gx2, gy1, gy2, hx1, hx2, hy1, hy2, p0, p1, p2, m1, m2);
-            mx = fmax(p0, fmax(p1, p2));
-        }
-        if (lmn >= 0) {
-            line_candidates<double>(t, td, lmn, Dd, gx1, gx2, gy1, gy2, hx1, hx2, hy1, hy2, p0, p1, p2, m1, m2);
-            mn = fmin(p0, fmin(m1, m2));
+        if (rmx - smx > err2 && smn - rmn > err2) {
+            double p0, p1, p2, m1, m2;
+            mx = Dd[0]; mn = Dd[0];
+            if (lmx >= 0) {
+                line_candidates<double>(t, td, lmx, Dd, gx1, gx2, gy1, gy2, hx1, hx2, hy1, hy2, p0, p1, p2, m1, m2);
+                mx = p0 > mx ? p0 : mx; mx = p1 > mx ? p1 : mx; mx = p2 > mx ? p2 : mx;
+            }
+            if (lmn >= 0) {
+                line_candidates<double>(t, td, lmn, Dd, gx1, gx2, gy1, gy2, hx1, hx2, hy1, hy2, p0, p1, p2, m1, m2);
+                mn = p0 < mn ? p0 : mn; mn = m1 < mn ? m1 : mn; mn = m2 < mn ? m2 : mn;
+            }
+            return;
         }
     }
+    double rmx = Dd[0], rmn = Dd[0];   // cell centre
+    for (int l = l0; l < l1; ++l) {
+        double p0, p1, p2, m1, m2;
+        line_candidates<double>(t, td, l, Dd, gx1, gx2, gy1, gy2, hx1, hx2, hy1, hy2, p0, p1, p2, m1, m2);
+        rmx = p0 > rmx ? p0 : rmx; rmx = p1 > rmx ? p1 : rmx; rmx = p2 > rmx ? p2 : rmx;
+        rmn = p0 < rmn ? p0 : rmn; rmn = m1 < rmn ? m1 : rmn; rmn = m2 < rmn ? m2 : rmn;
+    }
+    mx = rmx; mn = rmn;
 }
 
 // theta of one field: min over points of (bound - mean)/(v - mean) for v
@@ -268,11 +283,11 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
             for (int di = 0; di < 3; ++di) { lo = fmin(lo, u[dj][di]); hi = fmax(hi, u[dj][di]); }
         if (f == 0) {
             mH = u[1][1]; loH = fmax(0.0, lo); hiH = hi;
-            const int s1 = reconstruct<R>(a.tab, t, ci, cj, u, DH);
+            const int s1 = reconstruct(t, ci, cj, u, DH);
             st = st ? st : s1;
         } else {
             mC = u[1][1]; loC = fmax(0.0, lo); hiC = fmin(ph.k.Xe, hi);
-            const int s1 = reconstruct<R>(a.tab, t, ci, cj, u, DC);
+            const int s1 = reconstruct(t, ci, cj, u, DC);
             st = st ? st : s1;
         }
     }
@@ -330,6 +345,7 @@ struct CellPhaseArgs {
     double* srcH = nullptr;
     double* srcR = nullptr;
     double* srcS = nullptr;
+    const int* gate = nullptr;   // device flag: the launch does nothing while it is 0
 };
 
 __device__ __forceinline__ void load_rec(const double* rec, size_t N, long long cell, double* DH, double* DC) {
@@ -438,6 +454,7 @@ struct FaceArgs {
     double* face;          // 4 * nedge SoA: fluxH, fluxC, rate, fluxMixture
     unsigned long long* status;
     int gj0 = 0, gny = 0;  // slab: global row of local row 0, global rows
+    const int* gate = nullptr;   // device flag: the launch does nothing while it is 0
 };
 
 // Limited H and C of one side along the edge line: v(s) = m + c0 + s*(c1 + s*c2).
@@ -800,7 +817,10 @@ struct SumArgs {
     const double* srcS = nullptr;
     // General quad meshes: the area of every cell (else `area` for all).
     const double* cell_area = nullptr;
+    const int* gate = nullptr;   // device flag: the launch does nothing while it is 0
 };
+
+__device__ __forceinline__ bool gated_off(const int* gate) { return gate && *gate == 0; }
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

@@ -1,21 +1,27 @@
 // Coupled H/C transport on B200: FP64 stage kernels, the SSPRK2/SSPRK3 time
 // loop and the mp_transport_* entry points.
 //
-// One stage L(U) (RHS, src/couple/evolve.cpp:279-384) is three kernels:
-//   cell_kernel  per cell: candidate smoothness + weights, limiter theta,
-//                limited deviation polynomials, 5x5 cell quadrature of the
-//                phase (T, phi, wet flag), diffusion-sample admissibility;
-//   face_kernel  per edge: limited evaluations on both sides at the 5 Gauss
-//                points, phase, edge porosity, transport velocities, local
-//                Lax-Friedrichs fluxes, boundary policy, CFL rate;
-//   sum_kernel   per cell: conservative accumulation in the reference's face
-//                order, the Runge-Kutta combination and block reductions.
-// The time loop (evolve.cpp:428-511) runs on the host with one small
-// device->host read per stage for dt, the CFL retry and the balance check.
+// One stage L(U) (RHS, src/couple/evolve.cpp:279-384) is four kernels and a
+// fixed-order reduction:
+//   recon_kernel      per cell: candidate smoothness + weights, limiter theta,
+//                     limited deviation polynomials;
+//   cellphase_kernel  per cell: 5x5 cell quadrature of the phase (T, phi, wet
+//                     flag), diffusion-sample admissibility;
+//   face_kernel       per edge: limited evaluations on both sides at the 5
+//                     Gauss points, phase, edge porosity, transport
+//                     velocities, local Lax-Friedrichs fluxes, boundary
+//                     policy, CFL rate;
+//   sum_kernel        per cell: conservative accumulation in the reference's
+//                     face order, the Runge-Kutta combination, block partials.
+// The time loop (evolve.cpp:428-511) runs on the device (graph_steps: a CUDA
+// graph of the stage kernels and the step controller, one host wait per 64
+// steps) or, for row slabs, general quad meshes and profiling runs, on the
+// host (do_step: one small device->host read per stage).
 #include "common.hpp"
 #include "phase_math.cuh"
 #include "stage_device.cuh"
 #include "stage_kernels.cuh"
+#include "step_ctl.cuh"
 #include "tables.hpp"
 #include "quad_kernels.cuh"
 #include "quad_tables.hpp"
@@ -61,6 +67,7 @@ struct SourceBufs {
 template <class R>
 __global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
                                                     int jlo, int jhi) {
+    if (gated_off(a.gate)) return;
     ReconArgs<R> b = a;
     b.tab = param_tab<R>(p);
     const int j = jlo + (int)(blockIdx.y * blockDim.y + threadIdx.y);
@@ -69,6 +76,7 @@ __global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph, 
 template <class R, bool kExt>
 __global__ void __launch_bounds__(128, 8) cellphase_kernel(CellPhaseArgs<R> a, Physics ph,
                                                         const __grid_constant__ ParamTables p, long long c0, long long c1) {
+    if (gated_off(a.gate)) return;
     CellPhaseArgs<R> b = a;
     b.tab = param_tab<R>(p);
     const long long cell = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -81,6 +89,7 @@ __global__ void __launch_bounds__(128, 8) cellphase_kernel(CellPhaseArgs<R> a, P
 template <class R, bool kExt, bool kRange>
 __global__ void __launch_bounds__(128, 5) face_kernel(FaceArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
                                                       long long h0, long long nh, long long v0, long long nv) {
+    if (gated_off(a.gate)) return;
     FaceArgs<R> b = a;
     b.tab = param_tab<R>(p);
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -95,6 +104,7 @@ __global__ void __launch_bounds__(128, 5) face_kernel(FaceArgs<R> a, Physics ph,
 template <class R>
 __global__ void __launch_bounds__(128) diffusion_kernel(FaceArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
                                                         long long h0, long long nh, long long v0, long long nv) {
+    if (gated_off(a.gate)) return;
     FaceArgs<R> b = a;
     b.tab = param_tab<R>(p);
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -103,20 +113,37 @@ __global__ void __launch_bounds__(128) diffusion_kernel(FaceArgs<R> a, Physics p
 
 template <bool kSrc, bool kArea = false>
 __global__ void __launch_bounds__(kRedBlock) sum_kernel(SumArgs a) {
+    if (gated_off(a.gate)) return;
     const Partial v = sum_cells<kSrc, kArea>(a, (long long)blockIdx.x * kSumCells);
     block_reduce_write(v, a.partial + blockIdx.x);
 }
 
-// U1 = U^n + dt*L^n with the admissibility/integral partials of U1.
+// U1 = U^n + dt*L^n with the admissibility/integral partials of U1 (dtp:
+// dt read from device memory; gate: see ReconArgs).
 __global__ void __launch_bounds__(kRedBlock) axpy_kernel(int n, const double* H0, const double* C0, const double* LH,
                                                          const double* LC, double dt, double area, double* H1,
-                                                         double* C1, Partial* partial, const double* cell_area) {
-    const Partial v = axpy_cells(n, H0, C0, LH, LC, dt, area, H1, C1, (long long)blockIdx.x * kSumCells, cell_area);
+                                                         double* C1, Partial* partial, const double* cell_area,
+                                                         const double* dtp = nullptr, const int* gate = nullptr) {
+    if (gated_off(gate)) return;
+    const Partial v = axpy_cells(n, H0, C0, LH, LC, dtp ? *dtp : dt, area, H1, C1, (long long)blockIdx.x * kSumCells,
+                                 cell_area);
     block_reduce_write(v, partial + blockIdx.x);
 }
 
+// Commit of an accepted step on the device: U^{n+1} (a stage buffer) into U^n.
+__global__ void __launch_bounds__(kRedBlock) commit_kernel(long long n, const double* sH, const double* sC, double* H,
+                                                           double* C, const int* gate) {
+    if (gated_off(gate)) return;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        H[k] = sH[k];
+        C[k] = sC[k];
+    }
+}
+
 // Fixed-order reduction of the block partials into one Totals.
-__global__ void __launch_bounds__(1024) reduce_kernel(const Partial* partial, int nblocks, Totals* out) {
+__global__ void __launch_bounds__(1024) reduce_kernel(const Partial* partial, int nblocks, Totals* out,
+                                                      const int* gate = nullptr) {
+    if (gated_off(gate)) return;
     Partial v = partial_identity();
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x) fold_partial(v, partial[b]);
     __shared__ Partial result;
@@ -186,6 +213,20 @@ struct mp_transport {
     mp::QuadDev qdev{};
     double* qbuf = nullptr;                // one allocation holding every table
     const double* cell_area = nullptr;
+    // Device-resident stepping (uniform meshes without hooks; not while
+    // profiling): mp_transport_step runs up to kGraphSteps steps per CUDA
+    // graph launch, decisions by the step controller; the graph is captured
+    // again when a setter changes what it captured (gen).
+    bool use_graph = true;
+    unsigned long long gen = 1, graph_gen = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    mp::InstCtl *d_ctl = nullptr, *h_ctl = nullptr;
+    mp::CtlHeader *d_hdr = nullptr, *h_hdr = nullptr;
+    mp_step_report *d_rep = nullptr, *h_rep = nullptr;
+    int* d_gate = nullptr;
+    double* d_dt = nullptr;
+    unsigned long long host_syncs = 0;     // host waits for device results in stepping calls
     // Optional per-kernel timing (CUDA events on this handle's stream).
     bool profile = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -231,6 +272,10 @@ void harvest(mp_transport* t) {
 }
 
 void free_all(mp_transport* t) {
+    if (t->graph_exec) cudaGraphExecDestroy(t->graph_exec);
+    if (t->graph) cudaGraphDestroy(t->graph);
+    for (void* p : {(void*)t->d_ctl, (void*)t->d_hdr, (void*)t->d_rep, (void*)t->d_gate, (void*)t->d_dt}) if (p) cudaFree(p);
+    for (void* p : {(void*)t->h_ctl, (void*)t->h_hdr, (void*)t->h_rep}) if (p) cudaFreeHost(p);
     for (cudaEvent_t e : t->ev_pool) cudaEventDestroy(e);
     void* bufs[] = {t->H, t->C, t->S1H, t->S1C, t->S2H, t->S2C, t->LH, t->LC, t->T, t->phi,
                     t->rec, t->flags, t->vsn, t->udn, t->face, t->rate, t->partial, t->d_tot, t->d_status,
@@ -260,24 +305,24 @@ template <class R>
 void launch_stage_kernels(int nx, int ny, const StageRange& rg, const ParamTables& pt, const Physics& ph, const double* H, const double* C, double* rec,
                           unsigned char* flags, double* T, double* phi, const double* vsn, const double* udn,
                           double* face, unsigned long long* status, double* theta, cudaStream_t s,
-                          mp_transport* prof, const SourceBufs& src = SourceBufs{}) {
+                          mp_transport* prof, const SourceBufs& src = SourceBufs{}, const int* gate = nullptr) {
     const size_t NE = (size_t)nx * (ny + 1) + (size_t)(nx + 1) * ny;
     auto run = [&](int kind, auto&& f) { if (prof) timed(prof, kind, f); else f(); };
     {
-        ReconArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, status, theta, rg.gj0, rg.gny};
+        ReconArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, status, theta, rg.gj0, rg.gny, gate};
         dim3 blk(32, 4), grd((nx + 31) / 32, (rg.rec1 - rg.rec0 + 3) / 4);
         run(0, [&] { recon_kernel<R><<<grd, blk, 0, s>>>(a, ph, pt, rg.rec0, rg.rec1); });
     }
     {
         CellPhaseArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, T, phi, status, rg.gj0, rg.gny,
-                           src.cvs_y, src.cud_y, src.srcH, src.srcR, src.srcS};
+                           src.cvs_y, src.cud_y, src.srcH, src.srcR, src.srcS, gate};
         const long long c0 = (long long)rg.rec0 * nx, c1 = (long long)rg.rec1 * nx;
         const unsigned g = (unsigned)((c1 - c0 + 127) / 128);
         if (ph.litho || ph.source) run(1, [&] { cellphase_kernel<R, true><<<g, 128, 0, s>>>(a, ph, pt, c0, c1); });
         else run(1, [&] { cellphase_kernel<R, false><<<g, 128, 0, s>>>(a, ph, pt, c0, c1); });
     }
     {
-        FaceArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, vsn, udn, face, status, rg.gj0, rg.gny};
+        FaceArgs<R> a{nx, ny, Tab<R>{}, H, C, rec, flags, vsn, udn, face, status, rg.gj0, rg.gny, gate};
         const long long nI = (long long)nx * (ny + 1);
         const long long h0 = (long long)rg.own0 * nx, nh = (long long)(rg.own1 - rg.own0 + 1) * nx;
         const long long v0 = nI + (long long)rg.own0 * (nx + 1), nv = (long long)(rg.own1 - rg.own0) * (nx + 1);
@@ -298,8 +343,12 @@ void launch_stage_kernels(int nx, int ny, const StageRange& rg, const ParamTable
 
 // Launch one stage evaluation of state (H, C). mode SUM_STORE_L writes L to
 // (outH, outC); SUM_RK writes a0*U^n + a1*(U + dt*L). Totals land in *d_tot.
+// gate / dtp (device-resident steps): a device flag that switches the whole
+// launch off, and dt read from device memory.
 mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mode, double a0, double a1, double dt,
-                       double* outH, double* outC, double* theta = nullptr) {
+                       double* outH, double* outC, double* theta = nullptr, const int* gate = nullptr,
+                       const double* dtp = nullptr) {
+    NvtxRange range("mp_transport stage");
     cudaStream_t s = t->stream;
     if (t->halo) {
         // A slab: its neighbours' owned rows into this stage input's halo rows.
@@ -330,15 +379,15 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
         });
     } else if (t->mixed) {
         launch_stage_kernels<float>(t->nx, t->ny, t->range, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
-                                    t->vsn, t->udn, t->face, t->d_status, theta, s, prof, sb);
+                                    t->vsn, t->udn, t->face, t->d_status, theta, s, prof, sb, gate);
     } else {
         launch_stage_kernels<double>(t->nx, t->ny, t->range, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T,
-                                     t->phi, t->vsn, t->udn, t->face, t->d_status, theta, s, prof, sb);
+                                     t->phi, t->vsn, t->udn, t->face, t->d_status, theta, s, prof, sb, gate);
     }
     {
         SumArgs a{t->nx, t->ny, t->host_tab.area, 1.0 / t->host_tab.area, t->face, H, C, t->H, t->C, outH, outC, t->rate, mode, a0, a1, dt,
-                  t->partial, nullptr, t->range.gj0, t->range.gny, (long long)t->range.own0 * t->nx,
-                  (long long)t->range.own1 * t->nx, sb.srcH, sb.srcR, sb.srcS, t->cell_area};
+                  t->partial, dtp, t->range.gj0, t->range.gny, (long long)t->range.own0 * t->nx,
+                  (long long)t->range.own1 * t->nx, sb.srcH, sb.srcR, sb.srcS, t->cell_area, gate};
         if (t->quad) {
             if (sb.srcH) timed(t, 3, [&] { sum_kernel<true, true><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
             else timed(t, 3, [&] { sum_kernel<false, true><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
@@ -347,7 +396,7 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
             else timed(t, 3, [&] { sum_kernel<false><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
         }
     }
-    timed(t, 4, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, t->sum_blocks, t->d_tot); });
+    timed(t, 4, [&] { reduce_kernel<<<1, 1024, 0, s>>>(t->partial, t->sum_blocks, t->d_tot, gate); });
     count_launch(t->quad ? 2 : 5);
     if (!t->quad && t->ph.diffusion) count_launch();
     MP_CUDA(cudaGetLastError());
@@ -359,6 +408,7 @@ mp_status read_totals(mp_transport* t, Totals& out, bool& failed, const char* wh
     MP_CUDA(cudaMemcpyAsync(t->h_tot, t->d_tot, sizeof(Totals), cudaMemcpyDeviceToHost, s));
     MP_CUDA(cudaMemcpyAsync(t->h_status, t->d_status, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     MP_CUDA(cudaStreamSynchronize(s));
+    t->host_syncs += 1;
     harvest(t);
     if (t->combine) {
         // A slab: totals and the first failure across all slabs.
@@ -400,6 +450,7 @@ bool admissible(const Totals& tot, double Xe) {
 
 // One accepted step (evolve.cpp:449-507), SSPRK2 or Shu-Osher SSPRK3.
 mp_status do_step(mp_transport* t, mp_step_report& rep) {
+    NvtxRange range("mp_transport step (host loop)");
     cudaStream_t s = t->stream;
     if (!t->have_L) MP_TRY(eval_current(t));
     const mp_transport_opts& o = t->opts;
@@ -511,10 +562,231 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
     return MP_OK;
 }
 
+// ------------------------------------------------------- device-resident steps
+
+constexpr int kGraphSteps = 64;        // steps per graph launch (report rows)
+
+bool graph_usable(const mp_transport* t) {
+    return t->use_graph && !t->profile && !t->halo && !t->combine && !t->quad && !(t->ph.source && !t->cvs_y);
+}
+
+StepOpts single_step_opts(const mp_transport* t) {
+    const mp_transport_opts& o = t->opts;
+    StepOpts so{};
+    so.cfl = o.cfl; so.dt_initial = o.dt_initial; so.dt_max = o.dt_max; so.dt_min = o.dt_min; so.Xe = o.material.Xe;
+    so.rk3 = o.integrator == MP_SSPRK3;
+    so.fixed = t->fixed ? 1 : 0;
+    so.snap_end = 0; so.end_reports = 1; so.restore_time = 1;
+    return so;
+}
+
+mp_status capture_leaves(cudaStream_t s, std::vector<cudaGraphNode_t>& out) {
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    MP_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &nd));
+    out.assign(deps, deps + nd);
+    return MP_OK;
+}
+
+mp_status add_while(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, cudaGraphConditionalHandle h,
+                    cudaGraphNode_t* node, cudaGraph_t* body) {
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    MP_CUDA(cudaGraphAddNode(node, g, deps.empty() ? nullptr : deps.data(), deps.size(), &p));
+    *body = p.conditional.phGraph_out[0];
+    return MP_OK;
+}
+
+// The graph of up to kGraphSteps steps, the same kernels as do_step:
+//   WHILE run:  begin -> WHILE attempt: {attempt, axpy, reduce, gate, stage 2,
+//               control [, stage 3, control]} -> commit, copy, L(U^{n+1}),
+//               control (run condition).
+mp_status capture_steps(mp_transport* t, cudaGraph_t g) {
+    cudaStream_t s = t->stream;
+    const StepOpts so = single_step_opts(t);
+    const bool rk3 = so.rk3 != 0;
+    cudaGraphConditionalHandle run, attempt;
+    MP_CUDA(cudaGraphConditionalHandleCreate(&run, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNode_t run_node, attempt_node;
+    cudaGraph_t step_body, attempt_body, tmp;
+    MP_TRY(add_while(g, {}, run, &run_node, &step_body));
+    MP_CUDA(cudaGraphConditionalHandleCreate(&attempt, step_body, 0, 0));
+    const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+    MP_CUDA(cudaStreamBeginCaptureToGraph(s, step_body, nullptr, nullptr, 0, mode));
+    ctl_begin_kernel<<<1, kCtlThreads, 0, s>>>(t->d_ctl, 1, so, t->d_hdr, t->d_rep, attempt);
+    std::vector<cudaGraphNode_t> leaves;
+    MP_TRY(capture_leaves(s, leaves));
+    MP_CUDA(cudaStreamEndCapture(s, &tmp));
+    MP_TRY(add_while(step_body, leaves, attempt, &attempt_node, &attempt_body));
+    const size_t o0 = own_begin(t), on = own_count(t);
+    const int nblk_axpy = (int)((on + kSumCells - 1) / kSumCells);
+    MP_CUDA(cudaStreamBeginCaptureToGraph(s, attempt_body, nullptr, nullptr, 0, mode));
+    ctl_attempt_kernel<<<1, kCtlThreads, 0, s>>>(t->d_ctl, 1, so, t->d_hdr, t->d_gate, t->d_dt);
+    axpy_kernel<<<nblk_axpy, kRedBlock, 0, s>>>((int)on, t->H + o0, t->C + o0, t->LH + o0, t->LC + o0, 0.0,
+                                                 t->host_tab.area, t->S1H + o0, t->S1C + o0, t->partial, nullptr,
+                                                 t->d_dt, t->d_gate);
+    reduce_kernel<<<1, 1024, 0, s>>>(t->partial, nblk_axpy, t->d_tot, t->d_gate);
+    ctl_after_axpy_kernel<<<1, kCtlThreads, 0, s>>>(t->d_ctl, 1, so, t->d_tot, t->d_status, t->d_gate);
+    MP_TRY(launch_stage(t, t->S1H, t->S1C, SUM_RK, rk3 ? 0.75 : 0.5, rk3 ? 0.25 : 0.5, 0.0, t->S2H, t->S2C, nullptr,
+                        t->d_gate, t->d_dt));
+    ctl_after_stage_kernel<<<1, kCtlThreads, 0, s>>>(t->d_ctl, 1, so, t->d_tot, t->d_status, t->d_gate, 2, rk3 ? 0 : 1,
+                                                      t->d_hdr, attempt);
+    if (rk3) {
+        MP_TRY(launch_stage(t, t->S2H, t->S2C, SUM_RK, 1.0 / 3.0, 2.0 / 3.0, 0.0, t->S1H, t->S1C, nullptr, t->d_gate,
+                            t->d_dt));
+        ctl_after_stage_kernel<<<1, kCtlThreads, 0, s>>>(t->d_ctl, 1, so, t->d_tot, t->d_status, t->d_gate, 3, 1,
+                                                          t->d_hdr, attempt);
+    }
+    MP_CUDA(cudaStreamEndCapture(s, &tmp));
+    MP_CUDA(cudaStreamBeginCaptureToGraph(s, step_body, &attempt_node, nullptr, 1, mode));
+    ctl_commit_kernel<<<1, kCtlThreads, 0, s>>>(t->d_ctl, 1, so, t->d_hdr, t->d_rep, t->d_status, t->d_gate);
+    const unsigned cgrid = (unsigned)std::min<size_t>((t->N + kRedBlock - 1) / kRedBlock, 148 * 8);
+    commit_kernel<<<cgrid, kRedBlock, 0, s>>>((long long)t->N, rk3 ? t->S1H : t->S2H, rk3 ? t->S1C : t->S2C, t->H,
+                                              t->C, t->d_gate);
+    MP_TRY(launch_stage(t, t->H, t->C, SUM_STORE_L, 0, 0, 0, t->LH, t->LC, nullptr, t->d_gate, nullptr));
+    ctl_after_rhs_kernel<<<1, kCtlThreads, 0, s>>>(t->d_ctl, 1, so, t->d_tot, t->d_status, t->d_rep, t->d_hdr, 1, run);
+    MP_CUDA(cudaStreamEndCapture(s, &tmp));
+    MP_CUDA(cudaGetLastError());
+    return MP_OK;
+}
+
+void release_graph(mp_transport* t) {
+    if (t->graph_exec) cudaGraphExecDestroy(t->graph_exec);
+    if (t->graph) cudaGraphDestroy(t->graph);
+    t->graph_exec = nullptr;
+    t->graph = nullptr;
+    t->graph_gen = 0;
+}
+
+mp_status ensure_graph(mp_transport* t) {
+    if (!t->d_ctl) {
+        MP_CUDA(cudaMalloc((void**)&t->d_ctl, sizeof(InstCtl)));
+        MP_CUDA(cudaMalloc((void**)&t->d_hdr, sizeof(CtlHeader)));
+        MP_CUDA(cudaMalloc((void**)&t->d_rep, kGraphSteps * sizeof(mp_step_report)));
+        MP_CUDA(cudaMalloc((void**)&t->d_gate, sizeof(int)));
+        MP_CUDA(cudaMalloc((void**)&t->d_dt, sizeof(double)));
+        MP_CUDA(cudaMallocHost((void**)&t->h_ctl, sizeof(InstCtl)));
+        MP_CUDA(cudaMallocHost((void**)&t->h_hdr, sizeof(CtlHeader)));
+        MP_CUDA(cudaMallocHost((void**)&t->h_rep, kGraphSteps * sizeof(mp_step_report)));
+    }
+    if (t->graph_exec && t->graph_gen == t->gen) return MP_OK;
+    release_graph(t);
+    MP_CUDA(cudaGraphCreate(&t->graph, 0));
+    // Capture on a private stream (the caller's may be the legacy default
+    // stream, which cannot be captured); the graph runs on the caller's.
+    cudaStream_t cap = nullptr;
+    MP_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaStream_t user = t->stream;
+    t->stream = cap;
+    g_capturing = true;
+    const mp_status st = capture_steps(t, t->graph);
+    g_capturing = false;
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(cap, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        cudaGraph_t tmp;
+        cudaStreamEndCapture(cap, &tmp);
+    }
+    t->stream = user;
+    cudaStreamDestroy(cap);
+    if (st != MP_OK) {
+        release_graph(t);
+        return st;
+    }
+    MP_CUDA(cudaGraphInstantiate(&t->graph_exec, t->graph, 0));
+    t->graph_gen = t->gen;
+    return MP_OK;
+}
+
+// The host loop's message for the failure the controller recorded.
+mp_status graph_failure(mp_transport* t, const InstCtl& c) {
+    switch (c.fail) {
+    case FAIL_STAGE:
+        *t->h_status = c.word;
+        return check_status(t, "RHS");
+    case FAIL_RATE: set_error("RHS: nonfinite coupled stage rate"); return MP_ERR_FP;
+    case FAIL_RETRIES: set_error("Coupled step cannot satisfy admissibility/CFL above minimum step"); return MP_ERR_NOT_CONVERGED;
+    case FAIL_FIXED_LIMIT: set_error("Fixed time step exceeds the phase-coupled CFL bound; use control: cfl"); return MP_ERR_ARG_OUTOFRANGE;
+    case FAIL_FIXED_STAGE: set_error("Fixed coupled step failed stage admissibility/CFL"); return MP_ERR_ARG_OUTOFRANGE;
+    case FAIL_BALANCE:
+        set_error("Coupled finite-volume conservation balance failed (H %.3e, C %.3e)", c.bal_H, c.bal_C);
+        return MP_ERR_PLIB;
+    default: set_error("step failed"); return (mp_status)c.status;
+    }
+}
+
+// nsteps accepted steps on the device: one graph launch and one host wait
+// per kGraphSteps steps. Same decisions, results and reports as the host
+// loop of mp_transport_step.
+mp_status graph_steps(mp_transport* t, int nsteps, mp_step_report* reports) {
+    NvtxRange range("mp_transport steps (device-resident graph)");
+    if (!t->have_L) MP_TRY(eval_current(t));
+    MP_TRY(ensure_graph(t));
+    cudaStream_t s = t->stream;
+    const int sk = 5 + (t->ph.diffusion ? 1 : 0);           // kernels of one stage evaluation
+    const bool rk3 = t->opts.integrator == MP_SSPRK3;
+    for (int done = 0; done < nsteps; done += kGraphSteps) {
+        const int chunk = std::min(kGraphSteps, nsteps - done);
+        InstCtl& c = *t->h_ctl;
+        c = InstCtl{};
+        c.used = 1; c.time = t->time; c.t_end = t->t_end; c.accepted = t->accepted; c.have_L = 1; c.cur = t->curTot;
+        *t->h_hdr = CtlHeader{0, chunk, 0, 0, 0};
+        MP_CUDA(cudaMemcpyAsync(t->d_ctl, t->h_ctl, sizeof(InstCtl), cudaMemcpyHostToDevice, s));
+        MP_CUDA(cudaMemcpyAsync(t->d_hdr, t->h_hdr, sizeof(CtlHeader), cudaMemcpyHostToDevice, s));
+        MP_CUDA(cudaGraphLaunch(t->graph_exec, s));
+        MP_CUDA(cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(InstCtl), cudaMemcpyDeviceToHost, s));
+        MP_CUDA(cudaMemcpyAsync(t->h_hdr, t->d_hdr, sizeof(CtlHeader), cudaMemcpyDeviceToHost, s));
+        MP_CUDA(cudaMemcpyAsync(t->h_rep, t->d_rep, (size_t)chunk * sizeof(mp_step_report), cudaMemcpyDeviceToHost, s));
+        MP_CUDA(cudaStreamSynchronize(s));
+        t->host_syncs += 1;
+        const CtlHeader h = *t->h_hdr;
+        count_launch((unsigned long long)h.step * (4 + sk) + (unsigned long long)h.total_attempts * (4 + (sk + 1) * (rk3 ? 2 : 1)));
+        t->time = c.time;
+        t->accepted = c.accepted;
+        t->curTot = c.cur;
+        t->have_L = c.have_L != 0 && c.status == 0;
+        if (c.status) {
+            int k = 0;
+            while (k < h.step - 1 && t->h_rep[k].status == 0) ++k;
+            if (reports) {
+                std::memcpy(reports + done, t->h_rep, (size_t)k * sizeof(mp_step_report));
+                reports[done + k] = mp_step_report{};
+                reports[done + k].status = c.status;
+            }
+            t->have_L = false;
+            return graph_failure(t, c);
+        }
+        if (reports) std::memcpy(reports + done, t->h_rep, (size_t)chunk * sizeof(mp_step_report));
+    }
+    return MP_OK;
+}
+
 }  // namespace
 }  // namespace mp
 
 // -------------------------------------------------------------------- C ABI
+
+namespace mp {
+// The option checks every transport entry point makes before any device work
+// (time controls, integrator, diffusivity, precision, boundary policies, the
+// material's derived scales and the inflow composition), so one options
+// struct is accepted or rejected alike by all of them.
+mp_status validate_opts(const mp_transport_opts& o, mp_derived* der_out) {
+    if (!(o.cfl > 0 && o.cfl <= 1)) { set_error("Coupled CFL must be in (0,1]"); return MP_ERR_ARG_OUTOFRANGE; }
+    if (o.integrator != MP_SSPRK2 && o.integrator != MP_SSPRK3) { set_error("integrator must be 2 or 3"); return MP_ERR_ARG_OUTOFRANGE; }
+    if (!(std::isfinite(o.diffusivity) && o.diffusivity >= 0.0)) { set_error("Diffusivity must be finite and nonnegative"); return MP_ERR_ARG_OUTOFRANGE; }
+    if (o.precision != MP_PRECISION_FP64 && o.precision != MP_PRECISION_MIXED) { set_error("unknown precision"); return MP_ERR_ARG_OUTOFRANGE; }
+    if (o.H_policy < 0 || o.H_policy > 2 || o.C_policy < 0 || o.C_policy > 2) { set_error("unknown boundary policy"); return MP_ERR_ARG_OUTOFRANGE; }
+    mp_derived der;
+    MP_TRY(derive_checked(o.material, der));
+    if (!(o.inflow_C >= 0 && o.inflow_C <= o.material.Xe)) { set_error("Composition must lie in [0, phase.parameters.Xe]"); return MP_ERR_ARG_OUTOFRANGE; }
+    if (der_out) *der_out = der;
+    return MP_OK;
+}
+}  // namespace mp
 
 namespace {
 // A whole mesh (slab = false) or the row slab [row_begin, row_end) of `mesh`.
@@ -524,14 +796,8 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
     if (!mesh || !opts || !out) { set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (mesh->nx < 2 || mesh->ny < 2) { set_error("Transport requires at least 2x2 cells"); return MP_ERR_ARG_SIZ; }
     if (mesh_too_large(mesh->nx, mesh->ny)) { set_error("mesh has 2^31 edges or more"); return MP_ERR_ARG_SIZ; }
-    if (!(opts->cfl > 0 && opts->cfl <= 1)) { set_error("Coupled CFL must be in (0,1]"); return MP_ERR_ARG_OUTOFRANGE; }
-    if (opts->integrator != MP_SSPRK2 && opts->integrator != MP_SSPRK3) { set_error("integrator must be 2 or 3"); return MP_ERR_ARG_OUTOFRANGE; }
-    if (!(std::isfinite(opts->diffusivity) && opts->diffusivity >= 0.0)) { set_error("Diffusivity must be finite and nonnegative"); return MP_ERR_ARG_OUTOFRANGE; }
-    if (opts->precision != MP_PRECISION_FP64 && opts->precision != MP_PRECISION_MIXED) { set_error("unknown precision"); return MP_ERR_ARG_OUTOFRANGE; }
-    if (opts->H_policy < 0 || opts->H_policy > 2 || opts->C_policy < 0 || opts->C_policy > 2) { set_error("unknown boundary policy"); return MP_ERR_ARG_OUTOFRANGE; }
     mp_derived der;
-    MP_TRY(derive_checked(opts->material, der));
-    if (!(opts->inflow_C >= 0 && opts->inflow_C <= opts->material.Xe)) { set_error("Composition must lie in [0, phase.parameters.Xe]"); return MP_ERR_ARG_OUTOFRANGE; }
+    MP_TRY(validate_opts(*opts, &der));
     QuadTables qt;
     if (xy) {
         if (opts->precision != MP_PRECISION_FP64) { set_error("general quad meshes run in FP64"); return MP_ERR_ARG_WRONG; }
@@ -677,6 +943,7 @@ extern "C" mp_status mp_transport_set_hooks(mp_transport* t, mp_halo_fn halo, mp
     t->combine = combine;
     t->hook_user = user;
     t->have_L = false;
+    t->gen += 1;
     return MP_OK;
 }
 
@@ -742,6 +1009,7 @@ extern "C" mp_status mp_transport_rhs(mp_transport* t, double* rhsH, double* rhs
 extern "C" mp_status mp_transport_step(mp_transport* t, int nsteps, mp_step_report* reports) {
     if (!t) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (nsteps < 0) { mp::set_error("nsteps must be nonnegative"); return MP_ERR_ARG_OUTOFRANGE; }
+    if (nsteps > 0 && mp::graph_usable(t)) return mp::graph_steps(t, nsteps, reports);
     for (int k = 0; k < nsteps; ++k) {
         // At the end time (within 32 ulp of it, evolve.cpp:450-451) stepping stops;
         // the remaining reports keep dt = 0 and the end time.
@@ -777,6 +1045,7 @@ extern "C" mp_status mp_transport_set_time_control(mp_transport* t, int control,
     }
     t->fixed = control == MP_TIME_FIXED;
     t->t_end = t_end;
+    t->gen += 1;
     return MP_OK;
 }
 
@@ -794,6 +1063,7 @@ extern "C" mp_status mp_transport_set_thermal_bc(mp_transport* t, const int* typ
     }
     t->ph.diffusion = t->ph.kappa > 0.0 || flux;
     t->have_L = false;
+    t->gen += 1;
     return MP_OK;
 }
 
@@ -822,6 +1092,7 @@ extern "C" mp_status mp_transport_set_pressure_model(mp_transport* t, int model,
         return MP_ERR_ARG_OUTOFRANGE;
     }
     t->have_L = false;
+    t->gen += 1;
     return MP_OK;
 }
 
@@ -841,6 +1112,7 @@ extern "C" mp_status mp_transport_set_cell_velocity(mp_transport* t, const doubl
     MP_CUDA(cudaMemsetAsync(t->srcS, 0, t->N * sizeof(double), t->stream));
     MP_CUDA(cudaStreamSynchronize(t->stream));
     t->have_L = false;
+    t->gen += 1;
     return MP_OK;
 }
 
@@ -991,3 +1263,15 @@ mp_status stage_rhs_raw(int nx, int ny, const mp_transport_opts& o, const double
 }
 
 }  // namespace mp
+
+extern "C" mp_status mp_transport_set_device_steps(mp_transport* t, int enable) {
+    if (!t) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    t->use_graph = enable != 0;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_transport_run_stats(const mp_transport* t, unsigned long long* host_syncs) {
+    if (!t || !host_syncs) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    *host_syncs = t->host_syncs;
+    return MP_OK;
+}

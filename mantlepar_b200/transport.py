@@ -164,6 +164,17 @@ class Transport:
         return code, out
 
 
+    def set_device_steps(self, enable: bool = True):
+        """step() as CUDA graphs with the step decisions on the device (default)
+        or as the host-driven loop (one device->host read per stage)."""
+        _capi.check(self._lib.mp_transport_set_device_steps(self._h, int(enable)))
+
+    def host_syncs(self) -> int:
+        """Host waits for device results made by step() and rhs() so far."""
+        n = C.c_ulonglong(0)
+        _capi.check(self._lib.mp_transport_run_stats(self._h, C.byref(n)))
+        return n.value
+
     def profile(self, enable: bool = True):
         """Per-kernel CUDA-event timing on (resets the accumulators) or off."""
         _capi.check(self._lib.mp_transport_profile(self._h, int(enable)))

@@ -54,6 +54,9 @@ inline QuadVertices Q(const orc::Quad& q) { return QuadVertices{{P(q[0]), P(q[1]
 inline void check(PetscErrorCode e) { if (e) throw orc::Error{(int)e, "reference routine failed"}; }
 
 struct RefBackend {
+    // Reconstruction::Initialize reads the shared MeshInfo and writes only the
+    // cell's own object: cells are set up across threads.
+    static constexpr bool kParallelInit = true;
     MeshInfo mesh;
     const EutecticModel* model = nullptr;
     std::unique_ptr<EutecticModel> own;

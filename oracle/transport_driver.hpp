@@ -223,12 +223,19 @@ struct Driver {
         build_faces();
         backend.setup(*this);
         rh.resize(ncell); rc.resize(ncell);
-        for (int j = 0; j < ny; ++j)
-            for (int i = 0; i < nx; ++i) {
-                const int k = cell_id(i, j);
-                rh[k].init(backend, *this, i, j, std::sqrt(area[k]));
-                rc[k] = rh[k];
-            }
+        // Per-cell reconstruction setup. A backend whose setup touches only
+        // the cell's own data (B::kParallelInit) runs it across threads; the
+        // restated backend shares a table pool and runs it in cell order.
+        auto init_cell = [&](int k) {
+            const int i = k % nx, j = k / nx;
+            rh[k].init(backend, *this, i, j, std::sqrt(area[k]));
+            rc[k] = rh[k];
+        };
+        if constexpr (B::kParallelInit) {
+            parallel_for(ncell, init_cell);
+        } else {
+            for (int k = 0; k < ncell; ++k) init_cell(k);
+        }
         H.assign(ncell, 0); C.assign(ncell, 0); T.assign(ncell, 0); phi.assign(ncell, 0);
         oldH.assign(ncell, 0); oldC.assign(ncell, 0);
         lim_h.assign(ncell, 1); lim_c.assign(ncell, 1);
@@ -852,6 +859,9 @@ struct Api {
         auto& d = static_cast<Handle<B>*>(h)->d;
         try {
             const auto r = d.rhs();
+            // The RHS of the accepted state is what the next step starts from
+            // (Driver::step computes exactly this on entry): keep it.
+            d.oldH = d.H; d.oldC = d.C; d.current = r; d.have_current = true;
             if (rhsH) std::copy(d.rhsH.begin(), d.rhsH.end(), rhsH);
             if (rhsC) std::copy(d.rhsC.begin(), d.rhsC.end(), rhsC);
             if (T) std::copy(d.T.begin(), d.T.end(), T);

@@ -23,6 +23,7 @@ bool derive(const orc_material& m, orc_derived& d);
 namespace orc {
 
 struct Restated {
+    static constexpr bool kParallelInit = false;   // cells share the table pool
     std::vector<CandidateSet> sets;   // per cell
     std::vector<std::unique_ptr<StencilTables>> pool;
     std::map<std::tuple<int, int, int>, const StencilTables*> shared;

@@ -71,3 +71,57 @@ def test_invalid_quad_meshes_are_rejected_before_device_work(cuda_lib):
         assert cuda_lib.mp_preheat_create_quads(C.byref(mesh), xy_ptr, C.byref(p_opts), None, C.byref(h)) == 62
         assert not h.value
     assert b"quadrilateral" in cuda_lib.mp_last_error_string()
+
+
+def _noalloc_call(lib, mesh, opts):
+    """mp_transport_rhs_noalloc with placeholder (never dereferenced) device
+    pointers: every case below is rejected on the host before device work."""
+    import ctypes as C
+    fake = C.c_void_p(16)
+    return lib.mp_transport_rhs_noalloc(C.byref(mesh), C.byref(opts), fake, fake, fake, fake, fake, fake, fake, fake,
+                                        None, None, None)
+
+
+def test_noalloc_checks_options_as_the_allocating_entry_points(cuda_lib):
+    """One options struct is rejected alike by mp_transport_create,
+    mp_batch_create and mp_transport_rhs_noalloc: bad boundary policies and
+    an inflow composition outside [0, Xe] give MP_ERR_ARG_OUTOFRANGE from
+    each, before any device call (no GPU is present here)."""
+    import ctypes as C
+    import dataclasses
+    from mantlepar_b200 import synthetic as sy
+    from mantlepar_b200.transport import TransportConfig
+    w = sy.Workload(nx=8, ny=8)
+    mesh = _capi.MeshDesc(w.nx, w.ny, w.x0, w.x1, w.y0, w.y1)
+    base = TransportConfig(cfl=0.4, integrator=3)
+    bad = [dataclasses.replace(base, H_policy=3), dataclasses.replace(base, C_policy=-1),
+           dataclasses.replace(base, inflow_C=0.6), dataclasses.replace(base, inflow_C=-0.1),
+           dataclasses.replace(base, cfl=1.5), dataclasses.replace(base, integrator=4),
+           dataclasses.replace(base, precision=7)]
+    for cfg in bad:
+        opts = cfg.to_c()
+        h = C.c_void_p()
+        c_create = cuda_lib.mp_transport_create(C.byref(mesh), C.byref(opts), None, C.byref(h))
+        c_batch = cuda_lib.mp_batch_create(C.byref(mesh), 1, C.byref(opts), None, C.byref(h))
+        c_noalloc = _noalloc_call(cuda_lib, mesh, opts)
+        assert c_create == c_batch == c_noalloc == 63, (cfg, c_create, c_batch, c_noalloc)
+        assert not h.value
+
+
+def test_noalloc_rejects_unsupported_options_on_the_host(cuda_lib):
+    """Thermal diffusion, the adiabatic source and the mixed-precision form
+    are not evaluated by mp_transport_rhs_noalloc: MP_ERR_ARG_WRONG, with a
+    message naming the entry point; a mesh above 32768 cells: MP_ERR_ARG_SIZ."""
+    import dataclasses
+    from mantlepar_b200 import synthetic as sy
+    from mantlepar_b200.transport import TransportConfig
+    w = sy.Workload(nx=8, ny=8)
+    mesh = _capi.MeshDesc(w.nx, w.ny, w.x0, w.x1, w.y0, w.y1)
+    base = TransportConfig(cfl=0.4, integrator=3)
+    for cfg in (dataclasses.replace(base, diffusivity=1e-4),
+                dataclasses.replace(base, material=dataclasses.replace(sy.material_s(), alpha0=3e-5)),
+                dataclasses.replace(base, precision=1)):
+        assert _noalloc_call(cuda_lib, mesh, cfg.to_c()) == 62
+        assert b"mp_transport_rhs_noalloc" in cuda_lib.mp_last_error_string()
+    big = _capi.MeshDesc(2, 16385, w.x0, w.x1, w.y0, w.y1)
+    assert _noalloc_call(cuda_lib, big, base.to_c()) == 60

@@ -1,13 +1,15 @@
-"""Mixed precision: smoothness indicators, weights and the limiter scan in
-FP32; basis coefficients, limited values, phase inversion and flux
-accumulation in FP64.
+"""Mixed precision (MP_PRECISION_MIXED): the limiter scan is screened in
+FP32; every value (smoothness indicators, weights, coefficients, limited
+values, phase inversion, fluxes, accumulation) stays FP64.
 
-Two error measures against the FP64 reference, reported per field (max, L2):
-per-cell |x - ref| / max(|ref|, 1e-3 * max|ref|) and normwise
-max|x - ref| / max|ref|. The bar is 1e-6: normwise for every field, per cell
-for H, C and T. Porosity near the solidus (phi ~ 1e-3 max) turns the ~1e-6
-relative FP32 weight error into ~1e-5 per-cell relative (absolute phi error
-~2e-8); that per-cell figure is asserted at 1e-4 and reported."""
+The FP32 screen keeps, for each extreme, the leading line and the runner-up;
+when the lead exceeds twice a rigorous bound on the FP32-FP64 difference, the
+leading line alone is evaluated again in FP64, else the FP64 scan runs. The
+limiter factors, and so every result, therefore equal the FP64 path's bit for
+bit; the tests assert that, and the stated bar of the form, 1e-6 per cell
+|x - ref| / max(|ref|, 1e-3 max|ref|) on H, C, T and phi against the
+reference's golden runs (the measured error is that of the FP64 path,
+below 1e-12)."""
 import os
 
 import numpy as np
@@ -23,14 +25,7 @@ TOL = 1e-6
 def errors(got, ref):
     scale = np.maximum(np.abs(ref), 1e-3 * np.max(np.abs(ref)))
     e = np.abs(got - ref) / scale
-    return float(np.max(e)), float(np.sqrt(np.mean(e ** 2))), float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
-
-
-def check(name, got, ref, label):
-    mx, l2, nw = errors(got, ref)
-    print(f"{label} {name}: per-cell max {mx:.3e} L2 {l2:.3e} normwise {nw:.3e}")
-    assert nw <= TOL, (name, nw)
-    assert mx <= (1e-4 if name == "phi" else TOL), (name, mx)
+    return float(np.max(e)), float(np.sqrt(np.mean(e ** 2)))
 
 
 def make(w, integrator, precision):
@@ -50,15 +45,23 @@ def test_mixed_200_steps_against_reference(cuda_lib, integ):
     got = np.stack(t.get_state())
     ref = GOLDEN[f"w20_rk{integ}_200"]
     for k, name in enumerate(["H", "C", "T", "phi"]):
-        check(name, got[k], ref[k], f"mixed SSPRK{integ} 200 steps")
+        mx, l2 = errors(got[k], ref[k])
+        print(f"mixed SSPRK{integ} 200 steps {name}: per-cell max {mx:.3e} L2 {l2:.3e}")
+        assert mx <= TOL, (name, mx)
+    f = make(sy.plain_small(), integ, 0)
+    _, reps64 = f.step(200)
+    assert np.array_equal(got, np.stack(f.get_state()))
+    assert [r["dt"] for r in reps] == [r["dt"] for r in reps64]
 
 
-def test_mixed_against_fp64_path_at_size(cuda_lib):
-    """A 512x1024 instance with the raised noise of the mixed workload: the
-    FP64 GPU path (1e-12 to the reference) stands in for the oracle."""
+def test_mixed_equals_fp64_path_at_size(cuda_lib):
+    """A 512x1024 instance with the raised noise of the mixed workload (many
+    limited cells, populated phase boundaries): 10 SSPRK3 steps, bitwise."""
     w = sy.Workload(nx=512, ny=1024, noise_H=0.1, seed=2)
     a, b = make(w, 3, 1), make(w, 3, 0)
+    ta, tb = a.limiter(), b.limiter()
+    assert np.array_equal(ta[0], tb[0]) and np.array_equal(ta[1], tb[1])
     a.step(10)
     b.step(10)
     for name, x, y in zip(["H", "C", "T", "phi"], a.get_state(), b.get_state()):
-        check(name, x, y, "mixed vs fp64 512x1024")
+        assert np.array_equal(x, y), name

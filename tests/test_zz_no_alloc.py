@@ -29,7 +29,9 @@ def _rel_inf(a, b):
     return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
 
 
-def _noalloc(w, cfg, H, Cc, vs, ud):
+def _noalloc(w, cfg, H, Cc, vs, ud, with_optional=True):
+    """One call of the entry point on device copies of the inputs; with
+    with_optional=False the optional rate and totals outputs are NULL."""
     import torch
     from mantlepar_b200 import _capi
     lib = _capi.lib()
@@ -41,20 +43,30 @@ def _noalloc(w, cfg, H, Cc, vs, ud):
     opts = cfg.to_c()
     tot = _capi.StageTotals()
     stream = torch.cuda.current_stream(dev).cuda_stream
+    ptrs = [o.data_ptr() for o in outs]
+    if not with_optional:
+        ptrs[4] = None
     code = lib.mp_transport_rhs_noalloc(C.byref(mesh), C.byref(opts), Hd.data_ptr(), Cd.data_ptr(), vd.data_ptr(),
-                                        ud_.data_ptr(), *[o.data_ptr() for o in outs], C.byref(tot), stream)
+                                        ud_.data_ptr(), *ptrs, C.byref(tot) if with_optional else None, stream)
     _capi.check(code)
     rhsH, rhsC, T, phi, rate = (o.cpu().numpy() for o in outs)
-    return dict(rhsH=rhsH, rhsC=rhsC, T=T, phi=phi, rate=rate, maxRate=tot.maxRate,
-                boundaryH=tot.boundaryH, boundaryC=tot.boundaryC)
+    out = dict(rhsH=rhsH, rhsC=rhsC, T=T, phi=phi)
+    if with_optional:
+        out.update(rate=rate, maxRate=tot.maxRate, boundaryH=tot.boundaryH, boundaryC=tot.boundaryC)
+    return out
 
 
-@pytest.mark.parametrize("shape", [(20, 20), (64, 128), (3, 5)])
+# (2, 16384) and (16384, 2) hold the most edges the fixed face region is
+# sized for (2.5 * 32768 + 2); (128, 256) is exactly 32768 cells. The two
+# skinny meshes take a domain of square cells.
+@pytest.mark.parametrize("shape", [(20, 20), (64, 128), (3, 5), (2, 16384), (16384, 2), (128, 256)])
 def test_noalloc_stage_matches_allocating_entry_point(shape):
     from mantlepar_b200 import build
     build.build()
     from mantlepar_b200.transport import Transport, TransportConfig
-    w = sy.Workload(nx=shape[0], ny=shape[1], seed=11)
+    nx, ny = shape
+    skinny = max(nx, ny) >= 16 * min(nx, ny)
+    w = sy.Workload(nx=nx, ny=ny, seed=11, x1=(nx / ny if skinny else 0.5))
     cfg = TransportConfig(cfl=w.cfl, integrator=3)
     H, Cc = sy.initial_state(w)
     vs, ud = sy.face_velocity(w)
@@ -85,3 +97,18 @@ def test_noalloc_rejects_meshes_above_its_limit():
     with pytest.raises(MPError) as err:
         _noalloc(w, TransportConfig(), H, Cc, vs, ud)
     assert err.value.code == 60
+
+
+def test_noalloc_optional_outputs_may_be_null():
+    """rate and totals may be NULL: the other outputs are unchanged."""
+    from mantlepar_b200 import build
+    build.build()
+    from mantlepar_b200.transport import TransportConfig
+    w = sy.Workload(nx=24, ny=40, seed=5)
+    cfg = TransportConfig(cfl=w.cfl, integrator=3)
+    H, Cc = sy.initial_state(w)
+    vs, ud = sy.face_velocity(w)
+    full = _noalloc(w, cfg, H, Cc, vs, ud)
+    bare = _noalloc(w, cfg, H, Cc, vs, ud, with_optional=False)
+    for k in ("rhsH", "rhsC", "T", "phi"):
+        assert np.array_equal(full[k], bare[k]), k
