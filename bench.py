@@ -17,7 +17,7 @@ e2e        the same metric through the C ABI with host buffers: per step the
            step's inputs and the last step's results run on two copy streams
            during the current step (the sequential figure is reported beside);
 roofline   one stage evaluation (the four stage kernels) counted as one launch
-           against the measured HBM copy bandwidth (algorithmic 144 B/cell/stage),
+           against the measured HBM copy bandwidth (algorithmic 224 B/cell/stage),
            plus roofline_fp64 against a measured FP64 FMA peak (the binding roof);
 cpu_baseline  the reference's own phase/mlweno/core sources (oracle/_ref) or the
            restated oracle, all host threads, on a bounded 160x320 sample.
@@ -41,7 +41,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(nx=1280, ny=2560)
-ALG_BYTES_PER_CELL_STAGE = 144          # read U^(k), U^n; write U^(k+1); 2 faces x 5 q x 8 B v_s.n; write T, phi
+# Algorithmic bytes per cell per stage: read U^(k) and U^n (32), write
+# U^(k+1) (16), write T, phi (16), and the flow supplier's normal solid and
+# Darcy velocities at the 5 Gauss points of the cell's 2 owned edges (2 x 80;
+# both are per-point inputs, sampled from the flow solution in the reference).
+ALG_BYTES_PER_CELL_STAGE = 224
 # Executed FP64 operations per cell per stage (DFMA counted as 2, DADD/DMUL
 # as 1) of the stage kernels, from an ncu capture of a 640x1280 stage:
 # reconstruction 2073, cell phase 1188, faces 1703, accumulation ~48
@@ -136,6 +140,18 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def host_available_bytes():
+    """MemAvailable of the host (bytes), or None where it cannot be read."""
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return None
 
 
 def dist_setup():
@@ -488,23 +504,54 @@ def run_forms(args, stream):
         forms["preheat_1280x2560"]["cpu_baseline"] = cpu_form_baseline("preheat")
         forms["preheat_perturbed_1280x2560"]["cpu_baseline"] = cpu_form_baseline("preheat_perturbed")
         forms["perturbed_quads_1280x2560"]["cpu_baseline"] = cpu_form_baseline("quads")
-    # Served: a seeded Poisson stream (200 req/s) of uneven solves, mixed
-    # precision, submitted in real time; memory admission against a 64 GiB budget.
+    # Served (mixed precision, memory admission, continuous batching), two
+    # runs of 200 requests of the seeded stream:
+    #  (a) the specified load, 200 req/s with nx up to 1280: about 500 times
+    #      one GPU's capacity, so the run is bounded in wall time and the
+    #      requests still queued or running at the bound are reported as
+    #      censored (their latency is at least the time they waited);
+    #  (b) a load one GPU sustains: the same generator with nx up to 320,
+    #      offered at 70% of the capacity measured in (a).
     if args.serve_requests > 0:
-        from mantlepar_b200.serve import Server, poisson_requests, run_stream
+        from mantlepar_b200.serve import Server, poisson_requests, request_work, run_stream
+
+        def served(reqs, wall):
+            srv = Server(TransportConfig(cfl=0.4, integrator=3, precision=1), memory_budget=64 << 30)
+            srv.set_policy(Server.SMALLEST_WORK, 4.0e6)
+            out = run_stream(srv, reqs, wall_limit=wall)
+            srv.close()
+            out.pop("results")
+            return out
+
         reqs = poisson_requests(args.serve_requests, rate=200.0, seed=4)
-        srv = Server(TransportConfig(cfl=0.4, integrator=3, precision=1), memory_budget=64 << 30)
-        srv.set_policy(Server.SMALLEST_WORK, 4.0e6)
-        out = run_stream(srv, reqs)
-        srv.close()
-        queue = np.array([r["queue_s"] for r in out["results"]]) * 1e3
-        forms["served_poisson_200rps"] = {
-            "value": out["value"], "unit": "cell-updates/s", "p50_ms": out["p50_ms"], "p99_ms": out["p99_ms"],
-            "mean_ms": out["mean_ms"], "queue_p50_ms": float(np.percentile(queue, 50)),
-            "requests": out["requests"], "arrival_span_s": reqs[-1].arrival, "wall_s": out["wall_s"],
-            "gpu_busy_value": out["gpu_busy_value"], "all_ok": out["all_ok"],
-            "admission": "smallest estimated work first, 4e6 resident cells, 64 GiB budget",
-            "note": "latency = completion - submission; the first requests of the stream; 200 req/s offers about 500x one GPU's capacity, so queueing dominates"}
+        # Queued requests keep their inputs (H, C and the face velocities) in
+        # host memory: keep that below a third of what the host has free.
+        avail = host_available_bytes()
+        kept, total = [], 0
+        for r in reqs:
+            need = 8 * (2 * r.workload.cells + 10 * r.workload.edges)
+            if avail and total + need > avail / 3:
+                break
+            kept.append(r)
+            total += need
+        reqs = kept
+        a = served(reqs, args.serve_wall)
+        forms["served_poisson_200rps"] = dict(
+            a, requests_drawn=args.serve_requests, offered_rate_rps=200.0, arrival_span_s=reqs[-1].arrival,
+            offered_cell_updates=float(sum(request_work(r) for r in reqs)),
+            admission="smallest estimated work first, 4e6 resident cells, 64 GiB budget",
+            note=f"nx in 20..1280; bounded at {args.serve_wall:.0f} s of wall time: completed requests give the "
+                 "latency percentiles, censored ones are still queued or running")
+        small = poisson_requests(args.serve_requests, rate=1.0, seed=5, max_nx=320)
+        mean_work = float(np.mean([request_work(r) for r in small]))
+        capacity = a["gpu_busy_value"] / mean_work
+        rate = 0.7 * capacity
+        small = poisson_requests(args.serve_requests, rate=rate, seed=5, max_nx=320)
+        b_ = served(small, args.serve_wall)
+        forms["served_sustained"] = dict(
+            b_, offered_rate_rps=rate, arrival_span_s=small[-1].arrival, capacity_rps_estimate=capacity,
+            note="nx in 20..320 (ny = nx * U{1,2}, t_final U[0.01, 0.1]), offered at 70% of the capacity "
+                 "estimated from run (a)'s GPU throughput and the stream's mean work")
     return forms
 
 
@@ -768,7 +815,8 @@ def main():
     ap.add_argument("--impl", default="mantlepar_b200", choices=["mantlepar_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed / batched forms")
-    ap.add_argument("--serve-requests", type=int, default=10)
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-wall", type=float, default=90.0, help="wall-time bound of each served run (s)")
     ap.add_argument("--form-steps", type=int, default=5, help="timed steps of each extra form")
     ap.add_argument("--mixed-steps", type=int, default=50, help="steps of the mixed-precision 4096x4096 form")
     ap.add_argument("--batch-steps", type=int, default=100, help="steps of the 256-mesh batched forms")

@@ -439,6 +439,13 @@ mp_status mp_batch_step(mp_batch* b, int nsteps, mp_step_report* reports);
 mp_status mp_batch_set_end_time(mp_batch* b, int instance, double t_end);
 /* mp_transport_set_thermal_bc for every instance of the batch. */
 mp_status mp_batch_set_thermal_bc(mp_batch* b, const int* type, const double* value);
+/* Adiabatic source (alpha0 != 0, src/couple/evolve.cpp:359-369) of one
+ * instance: the vertical solid and Darcy velocities at its 25 cell quadrature
+ * points [cell*25 + b*5 + a], as mp_transport_set_cell_velocity. With alpha0
+ * != 0 every instance needs them before it steps (MP_ERR_ARG_WRONGSTATE
+ * otherwise); they take 424 bytes per cell beyond mp_batch_instance_bytes,
+ * counted in mp_batch_bytes_in_use. */
+mp_status mp_batch_set_cell_velocity(mp_batch* b, int instance, const double* vs_y, const double* ud_y);
 int mp_batch_finished(const mp_batch* b, int instance);
 /* Project autotuner: times the candidate reconstruction tile shapes and
  * cells-per-thread on this batch and keeps the fastest; tile = {bx, by, cpt}. */

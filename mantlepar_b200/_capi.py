@@ -11,7 +11,9 @@ import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-LIB_PATH = os.path.join(HERE, "libmantlepar_b200.so")
+# MP_CHECKED=1 loads the bounds-checked build (python -m mantlepar_b200.build --checked).
+LIB_PATH = os.path.join(HERE, "libmantlepar_b200_checked.so" if os.environ.get("MP_CHECKED") == "1"
+                        else "libmantlepar_b200.so")
 HEADER = os.path.join(ROOT, "include", "mantlepar", "mp.h")
 
 STATUS = {
@@ -137,6 +139,7 @@ def lib() -> C.CDLL:
         "mp_transport_set_device_steps": (i, [vp, i]),
         "mp_transport_run_stats": (i, [vp, C.POINTER(C.c_ulonglong)]),
         "mp_batch_set_device_steps": (i, [vp, i]),
+        "mp_batch_set_cell_velocity": (i, [vp, i, vp, vp]),
         "mp_batch_run_stats": (i, [vp, C.POINTER(C.c_ulonglong)]),
         "mp_transport_profile": (i, [vp, i]),
         "mp_transport_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),

@@ -100,6 +100,12 @@ class Batch:
         return [[{k: getattr(reps[s * slots + i], k) for k in REPORT_FIELDS} for i in range(slots)]
                 for s in range(nsteps)]
 
+    def set_cell_velocity(self, i: int, vs_y, ud_y):
+        """Vertical solid / Darcy velocity at instance i's cell quadrature
+        points [cell*25 + b*5 + a] (adiabatic source, alpha0 != 0)."""
+        a, b = _host(vs_y), _host(ud_y)
+        _capi.check(self._lib.mp_batch_set_cell_velocity(self._h, int(i), _ptr(a), _ptr(b)))
+
     def set_device_steps(self, enable: bool = True):
         """step() as CUDA graphs with every instance's step decisions on the
         device (default) or as the host-driven loop."""

@@ -23,6 +23,10 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmantlepar_b200.so")
+# Bounds-checked variant (-DMP_CHECKED): every stage element checks the cell
+# and edge indices it derives and records a status instead of an access
+# outside its arrays. Loaded instead of LIB when MP_CHECKED=1.
+CHECKED_LIB = os.path.join(HERE, "libmantlepar_b200_checked.so")
 # C++ host layer (mantle::phase::EutecticModel over the C ABI), linked to LIB.
 HOST_LIB = os.path.join(HERE, "libmantle_b200_host.so")
 HOST_SOURCES = [os.path.join(HERE, "host", "eutectic_model.cpp"), os.path.join(HERE, "host", "coupled_transport.cpp")]
@@ -45,9 +49,11 @@ def nvcc() -> str:
 SOURCE_FLAGS = {"quad_table_kernels.cu": ["--fmad=false"]}
 
 
-def _compile(src: str, verbose: bool) -> str:
-    obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
-    cmd = [nvcc()] + ARCH + FLAGS + SOURCE_FLAGS.get(src, []) + ["-c", os.path.join(CSRC, src), "-o", obj]
+def _compile(src: str, verbose: bool, checked: bool = False) -> str:
+    out_dir = os.path.join(BUILD, "checked") if checked else BUILD
+    obj = os.path.join(out_dir, os.path.splitext(src)[0] + ".o")
+    extra = ["-DMP_CHECKED"] if checked else []
+    cmd = [nvcc()] + ARCH + FLAGS + extra + SOURCE_FLAGS.get(src, []) + ["-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -56,6 +62,21 @@ def _compile(src: str, verbose: bool) -> str:
     if verbose:
         sys.stderr.write(r.stderr)
     return obj
+
+
+def build_checked(force: bool = False) -> str:
+    """Compile the bounds-checked variant of the library (CHECKED_LIB)."""
+    os.makedirs(os.path.join(BUILD, "checked"), exist_ok=True)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "mantlepar", "mp.h")]
+    if not force and os.path.exists(CHECKED_LIB) and os.path.getmtime(CHECKED_LIB) >= max(os.path.getmtime(d) for d in deps):
+        return CHECKED_LIB
+    with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        objs = list(ex.map(lambda s: _compile(s, False, True), SOURCES))
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", CHECKED_LIB] + objs + ["-Xcompiler", "-pthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    return CHECKED_LIB
 
 
 def build(verbose: bool = False, force: bool = False) -> str:
@@ -90,3 +111,5 @@ def build_host() -> str:
 
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))
+    if "--checked" in sys.argv:
+        print(build_checked(force="-f" in sys.argv))

@@ -81,12 +81,13 @@ __global__ void __launch_bounds__(128) batch_recon_kernel(const InstArgs<R>* arg
     for (int c = 0; c < cpt; ++c) recon_cell(a, ph, w.a + c * blockDim.x + threadIdx.x, j);
 }
 
-template <class R>
+// kExt: the adiabatic source (alpha0 != 0) is compiled in.
+template <class R, bool kExt>
 __global__ void __launch_bounds__(128, 8) batch_phase_kernel(const InstArgs<R>* args, const Work* work, const int* active,
                                                           Physics ph) {
     const Work w = work[blockIdx.x];
     if (!active[w.inst]) return;
-    cellphase_cell(args[w.inst].phase, ph, (long long)w.a + threadIdx.x);
+    cellphase_cell<R, kExt>(args[w.inst].phase, ph, (long long)w.a + threadIdx.x);
 }
 
 template <class R>
@@ -107,12 +108,13 @@ __global__ void __launch_bounds__(128) batch_diffusion_kernel(const InstArgs<R>*
     if (e < w.b) diffusion_edge(args[w.inst].face, ph, e);
 }
 
-template <class R>
+// kSrc: the adiabatic source terms are added.
+template <class R, bool kSrc>
 __global__ void __launch_bounds__(kRedBlock) batch_sum_kernel(const InstArgs<R>* args, const Work* work, const int* active) {
     const Work w = work[blockIdx.x];
     if (!active[w.inst]) return;
     const SumArgs& a = args[w.inst].sum;
-    const Partial v = sum_cells(a, w.a);
+    const Partial v = sum_cells<kSrc>(a, w.a);
     block_reduce_write(v, a.partial + w.part);
 }
 
@@ -172,6 +174,12 @@ struct MPInstance {
     mp::StageTables* tab;
     mp::StageTablesF* tabF;
     mp::StageTables host_tab;
+    // Adiabatic source (alpha0 != 0): vertical solid and Darcy velocities at
+    // the 25 cell quadrature points and the per-cell source sums, one
+    // allocation made by mp_batch_set_cell_velocity.
+    void* src_arena = nullptr;
+    size_t src_bytes = 0;
+    double *cvs_y = nullptr, *cud_y = nullptr, *srcH = nullptr, *srcR = nullptr, *srcS = nullptr;
     double time = 0.0;
     double t_end = INFINITY;          // time.end of this instance
     int accepted = 0;
@@ -314,7 +322,8 @@ mp_status alloc_instance(mp_batch* b, MPInstance& in, const mp_mesh_desc& m) {
 
 void free_instance(mp_batch* b, MPInstance& in) {
     if (in.arena) cudaFreeAsync(in.arena, b->stream);
-    b->bytes_in_use -= in.bytes;
+    if (in.src_arena) cudaFreeAsync(in.src_arena, b->stream);
+    b->bytes_in_use -= in.bytes + in.src_bytes;
     in = MPInstance{};
     b->dirty = true;
 }
@@ -357,14 +366,15 @@ mp_status rebuild_args(mp_batch* b, int slots) {
             double* outC = k == KIND_P ? in.LC : (k == KIND_B ? in.S2C : in.S1C);
             InstArgs<R>& a = args[k][i];
             a.recon = ReconArgs<R>{in.nx, in.ny, tb, inH, inC, in.rec, in.flags, b->d_status + i, nullptr};
-            a.phase = CellPhaseArgs<R>{in.nx, in.ny, tb, inH, inC, in.rec, in.flags, in.T, in.phi, b->d_status + i};
+            a.phase = CellPhaseArgs<R>{in.nx, in.ny, tb, inH, inC, in.rec, in.flags, in.T, in.phi, b->d_status + i,
+                                       0, 0, in.cvs_y, in.cud_y, in.srcH, in.srcR, in.srcS};
             a.face = FaceArgs<R>{in.nx, in.ny, tb, inH, inC, in.rec, in.flags, in.vsn, in.udn, in.face, b->d_status + i};
             const bool rk3 = b->opts.integrator == MP_SSPRK3;
             const double a0 = k == KIND_B ? (rk3 ? 0.75 : 0.5) : (1.0 / 3.0);
             const double a1 = k == KIND_B ? (rk3 ? 0.25 : 0.5) : (2.0 / 3.0);
             a.sum = SumArgs{in.nx, in.ny, in.host_tab.area, 1.0 / in.host_tab.area, in.face, inH, inC, in.H, in.C, outH, outC, in.rate,
                             k == KIND_P ? (int)SUM_STORE_L : (int)SUM_RK, a0, a1, 0.0, b->d_partial + parts,
-                            b->d_dt + i};
+                            b->d_dt + i, 0, 0, 0, -1, in.srcH, in.srcR, in.srcS, nullptr, nullptr, b->d_status + i};
         }
         ax[i] = AxpyArgs{(int)in.N, in.H, in.C, in.LH, in.LC, in.S1H, in.S1C, b->d_dt + i, in.host_tab.area,
                          b->d_partial + parts};
@@ -457,11 +467,17 @@ void launch_kind(mp_batch* b, int kind) {
     const InstArgs<R>* args = static_cast<const InstArgs<R>*>(b->d_args[kind]);
     const Tuning tu = b->tune;
     if (b->n_wrecon) timed(b, 0, [&] { batch_recon_kernel<R><<<b->n_wrecon, dim3(tu.bx, tu.by), 0, s>>>(args, b->d_wrecon, b->d_active, b->ph, tu.cpt); });
-    if (b->n_wphase) timed(b, 1, [&] { batch_phase_kernel<R><<<b->n_wphase, 128, 0, s>>>(args, b->d_wphase, b->d_active, b->ph); });
+    if (b->n_wphase) {
+        if (b->ph.source) timed(b, 1, [&] { batch_phase_kernel<R, true><<<b->n_wphase, 128, 0, s>>>(args, b->d_wphase, b->d_active, b->ph); });
+        else timed(b, 1, [&] { batch_phase_kernel<R, false><<<b->n_wphase, 128, 0, s>>>(args, b->d_wphase, b->d_active, b->ph); });
+    }
     if (b->n_wface) timed(b, 2, [&] { batch_face_kernel<R><<<b->n_wface, 128, 0, s>>>(args, b->d_wface, b->d_active, b->ph); });
     if (b->n_wface && b->ph.diffusion)
         timed(b, 2, [&] { batch_diffusion_kernel<R><<<b->n_wface, 128, 0, s>>>(args, b->d_wface, b->d_active, b->ph); });
-    if (b->n_wsum) timed(b, 3, [&] { batch_sum_kernel<R><<<b->n_wsum, kRedBlock, 0, s>>>(args, b->d_wsum, b->d_active); });
+    if (b->n_wsum) {
+        if (b->ph.source) timed(b, 3, [&] { batch_sum_kernel<R, true><<<b->n_wsum, kRedBlock, 0, s>>>(args, b->d_wsum, b->d_active); });
+        else timed(b, 3, [&] { batch_sum_kernel<R, false><<<b->n_wsum, kRedBlock, 0, s>>>(args, b->d_wsum, b->d_active); });
+    }
     timed(b, 4, [&] { batch_reduce_kernel<<<(int)b->inst.size(), 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot); });
     count_launch(5);
 }
@@ -505,6 +521,19 @@ bool admissible_tot(const Totals& t, double Xe) {
     return t.nonfinite == 0.0 && t.Hmin >= 0.0 && t.Cmin >= 0.0 && t.Cmax <= Xe;
 }
 
+// With the adiabatic source on, every instance needs its cell-point
+// velocities (the single-instance path's rule).
+mp_status check_sources(const mp_batch* b) {
+    if (!b->ph.source) return MP_OK;
+    for (size_t i = 0; i < b->inst.size(); ++i)
+        if (b->inst[i].used && !b->inst[i].cvs_y) {
+            set_error("instance %zu: the adiabatic source (alpha0 != 0) needs the flow velocities at the cell "
+                      "quadrature points (mp_batch_set_cell_velocity)", i);
+            return MP_ERR_ARG_WRONGSTATE;
+        }
+    return MP_OK;
+}
+
 // L(U^n) for instances that lack it.
 mp_status eval_missing(mp_batch* b) {
     const int slots = (int)b->inst.size();
@@ -531,6 +560,7 @@ mp_status eval_missing(mp_batch* b) {
 // One accepted step of every healthy instance (the reference's loop per instance).
 mp_status step_all(mp_batch* b, std::vector<mp_step_report>& reps) {
     NvtxRange range("mp_batch step (host loop)");
+    MP_TRY(check_sources(b));
     MP_TRY(rebuild(b));
     MP_TRY(eval_missing(b));
     const int slots = (int)b->inst.size();
@@ -598,17 +628,21 @@ mp_status step_all(mp_batch* b, std::vector<mp_step_report>& reps) {
         if (!done[i]) continue;
         MPInstance& in = b->inst[i];
         const Totals fin = rk3 ? third[i] : second[i];
-        double repH, repC, bH, bC;
+        const Totals& f = first[i];
+        const Totals& sd = second[i];
+        double repH, repC, repS, bH, bC;
         if (rk3) {
-            repH = (first[i].bH + second[i].bH) / 6 + third[i].bH * (2.0 / 3.0);
-            repC = (first[i].bC + second[i].bC) / 6 + third[i].bC * (2.0 / 3.0);
-            bH = fin.HI - first[i].HI + dt[i] * repH;
-            bC = fin.CI - first[i].CI + dt[i] * repC;
+            repH = (f.bH + sd.bH) / 6 + third[i].bH * (2.0 / 3.0);
+            repC = (f.bC + sd.bC) / 6 + third[i].bC * (2.0 / 3.0);
+            repS = (f.sH + sd.sH) / 6 + third[i].sH * (2.0 / 3.0);
+            bH = fin.HI - f.HI + dt[i] * (repH - repS);
+            bC = fin.CI - f.CI + dt[i] * repC;
         } else {
-            repH = .5 * (first[i].bH + second[i].bH);
-            repC = .5 * (first[i].bC + second[i].bC);
-            bH = fin.HI - first[i].HI + .5 * dt[i] * (first[i].bH + second[i].bH);
-            bC = fin.CI - first[i].CI + .5 * dt[i] * (first[i].bC + second[i].bC);
+            repH = .5 * (f.bH + sd.bH);
+            repC = .5 * (f.bC + sd.bC);
+            repS = .5 * (f.sH + sd.sH);
+            bH = fin.HI - f.HI + .5 * dt[i] * (f.bH + sd.bH - f.sH - sd.sH);
+            bC = fin.CI - f.CI + .5 * dt[i] * (f.bC + sd.bC);
         }
         if (!(std::fabs(bH) < 1e-10 * std::max(1.0, std::fabs(first[i].HI)) && std::fabs(bC) < 1e-10)) {
             in.status = MP_ERR_PLIB;
@@ -625,7 +659,7 @@ mp_status step_all(mp_batch* b, std::vector<mp_step_report>& reps) {
         in.have_L = false;
         mp_step_report& r = reps[i];
         r.retries = retries[i]; r.dt = dt[i]; r.time = in.time; r.courant = courant[i];
-        r.boundaryH = repH; r.boundaryC = repC; r.balanceH = bH; r.balanceC = bC;
+        r.boundaryH = repH; r.boundaryC = repC; r.sourceH = repS; r.balanceH = bH; r.balanceC = bC;
         r.H_integral = fin.HI; r.C_integral = fin.CI;
     }
     MP_TRY(eval_missing(b));
@@ -823,6 +857,7 @@ mp_status ensure_graph(mp_batch* b) {
 // wait per kGraphChunk steps. Same decisions and results as step_all.
 mp_status graph_steps(mp_batch* b, int nsteps, mp_step_report* reports) {
     NvtxRange range("mp_batch steps (device-resident graph)");
+    MP_TRY(check_sources(b));
     MP_TRY(rebuild(b));
     MP_TRY(eval_missing(b));
     MP_TRY(ensure_graph(b));
@@ -879,7 +914,6 @@ extern "C" mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, cons
     if (!opts || !out || count < 0 || (count > 0 && !meshes)) { set_error("null argument"); return MP_ERR_ARG_WRONG; }
     mp_derived der;
     MP_TRY(validate_opts(*opts, &der));
-    if (opts->material.alpha0 != 0.0) { set_error("the batched engine does not take cell-point velocities: adiabatic source (alpha0 != 0) needs the single-instance path"); return MP_ERR_ARG_WRONG; }
     mp_batch* b = new mp_batch;
     b->opts = *opts; b->der = der;
     b->stream = (cudaStream_t)stream;
@@ -894,7 +928,8 @@ extern "C" mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, cons
     for (int w = 0; w < 4; ++w) { b->ph.wall_type[w] = 0; b->ph.wall_value[w] = 0.0; }
     b->ph.diffusion = opts->diffusivity > 0.0;
     b->ph.litho = 0; b->ph.tep_a = b->ph.tep_b = b->ph.surface = 0.0;
-    b->ph.source = 0; b->ph.cooling = 0.0;
+    b->ph.source = opts->material.alpha0 != 0.0;
+    b->ph.cooling = opts->material.alpha0 * der.l0 * opts->material.g / opts->material.cp;
     b->inst.resize(count);
     for (int i = 0; i < count; ++i) {
         if (meshes[i].nx < 2 || meshes[i].ny < 2) { set_error("instance %d: at least 2x2 cells", i); mp_batch_destroy(b); return MP_ERR_ARG_SIZ; }
@@ -1081,5 +1116,32 @@ extern "C" mp_status mp_batch_set_device_steps(mp_batch* b, int enable) {
 extern "C" mp_status mp_batch_run_stats(const mp_batch* b, unsigned long long* host_syncs) {
     if (!b || !host_syncs) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
     *host_syncs = b->host_syncs;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_set_cell_velocity(mp_batch* b, int i, const double* vs_y, const double* ud_y) {
+    MPInstance* in;
+    MP_TRY(batch_slot(b, i, &in));
+    if (!vs_y || !ud_y) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    const size_t n = in->N * mp::kNQ * mp::kNQ;
+    cudaStream_t s = b->stream;
+    if (!in->src_arena) {
+        const size_t a = (n * sizeof(double) + 255) / 256 * 256, c = (in->N * sizeof(double) + 255) / 256 * 256;
+        in->src_bytes = 2 * a + 3 * c;
+        MP_CUDA(cudaMallocAsync(&in->src_arena, in->src_bytes, s));
+        unsigned char* p = static_cast<unsigned char*>(in->src_arena);
+        in->cvs_y = reinterpret_cast<double*>(p); p += a;
+        in->cud_y = reinterpret_cast<double*>(p); p += a;
+        in->srcH = reinterpret_cast<double*>(p); p += c;
+        in->srcR = reinterpret_cast<double*>(p); p += c;
+        in->srcS = reinterpret_cast<double*>(p);
+        b->bytes_in_use += in->src_bytes;
+        b->dirty = true;                // the argument records take the new pointers
+    }
+    MP_CUDA(cudaMemcpyAsync(in->cvs_y, vs_y, n * sizeof(double), cudaMemcpyDefault, s));
+    MP_CUDA(cudaMemcpyAsync(in->cud_y, ud_y, n * sizeof(double), cudaMemcpyDefault, s));
+    MP_CUDA(cudaMemsetAsync(in->srcH, 0, 3 * ((in->N * sizeof(double) + 255) / 256 * 256), s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    in->have_L = false;
     return MP_OK;
 }

@@ -208,6 +208,11 @@ void run(mp_server* s) {
 
 extern "C" mp_status mp_serve_create(const mp_transport_opts* opts, size_t memory_budget, mp_server** out) {
     if (!opts || !out) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (opts->material.alpha0 != 0.0) {
+        mp::set_error("served requests carry no cell-point velocities: the adiabatic source (alpha0 != 0) needs "
+                      "mp_batch_set_cell_velocity or the single-instance path");
+        return MP_ERR_ARG_WRONG;
+    }
     auto* s = new mp_server;
     s->opts = *opts;
     s->budget = memory_budget;

@@ -98,10 +98,30 @@ __device__ __forceinline__ int global_ny(const A& a) { return a.gny > 0 ? a.gny 
 // Status word: the smallest key wins. The key orders failures as the
 // reference's RHS meets them (evolve.cpp:279-384): reconstruction update,
 // limiter, porosity sampling, face loop, cell quadrature; then by cell/edge.
-enum : int { PART_UPDATE = 0, PART_LIMIT = 1, PART_POROSITY = 2, PART_FACES = 3, PART_CELLS = 4 };
+enum : int { PART_UPDATE = 0, PART_LIMIT = 1, PART_POROSITY = 2, PART_FACES = 3, PART_CELLS = 4, PART_CHECK = 7 };
 __device__ __forceinline__ void record_error(unsigned long long* status, int part, long long where, int code) {
     atomicMin(status, ((unsigned long long)part << 56) | ((unsigned long long)where << 8) | (unsigned long long)(code & 0xff));
 }
+
+// Bounds-checked build (MP_CHECKED, libmantlepar_b200_checked.so): every
+// cell and edge index a stage element derives is checked against its array
+// before use; one outside [0, n) records MP_ERR_ARG_OUTOFRANGE with part
+// PART_CHECK and the index in the status word, and the element returns
+// without touching memory. In the default build the check compiles away.
+#ifdef MP_CHECKED
+#define MP_CHECK_INDEX(status, idx, n)                                                        \
+    do {                                                                                      \
+        const long long mp_i_ = (long long)(idx);                                            \
+        if (!(mp_i_ >= 0 && mp_i_ < (long long)(n))) {                                       \
+            if (status) record_error((status), PART_CHECK, mp_i_ < 0 ? 0 : mp_i_, MP_ERR_ARG_OUTOFRANGE); \
+            return;                                                                           \
+        }                                                                                     \
+    } while (0)
+#else
+#define MP_CHECK_INDEX(status, idx, n) \
+    do {                               \
+    } while (0)
+#endif
 
 
 // ------------------------------------------------------- reconstruction kernel
@@ -253,6 +273,7 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
     const int nx = a.nx, ny = a.ny;
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
+    MP_CHECK_INDEX(a.status, cell, N);
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1);
     const int gj = a.gj0 + j, gny = global_ny(a);
     const int cj = gj == 0 ? 0 : (gj == gny - 1 ? 2 : 1);
@@ -272,6 +293,7 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
 #pragma unroll
             for (int di = 0; di < 3; ++di) {
                 const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
+                MP_CHECK_INDEX(a.status, (long long)jj * nx + ii, N);
                 u[dj][di] = __ldg(F + (size_t)jj * nx + ii);
             }
         // 3x3 neighbour bounds (state_reconstruction.cpp:189-196); the clamped
@@ -364,6 +386,7 @@ template <class R, bool kExt = false>
 __device__ __forceinline__ void cellphase_cell(const CellPhaseArgs<R>& a, const Physics& ph, long long cell) {
     const long long N = (long long)a.nx * a.ny;
     if (cell >= N) return;
+    MP_CHECK_INDEX(a.status, cell, N);
     const StageHot& t = *a.tab.t;
     const double mH = __ldg(a.H + cell), mC = __ldg(a.C + cell);
     double DH[9], DC[9];
@@ -592,6 +615,8 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
         rfix = -t.X;
         len = t.len_v;
     }
+    MP_CHECK_INDEX(a.status, L, N);
+    if (!boundary) MP_CHECK_INDEX(a.status, Rc, N);
     SideLine sl, sr;
     side_line(a, N, L, horizontal, lfix, sl);
     if (!boundary) side_line(a, N, Rc, horizontal, rfix, sr);
@@ -723,6 +748,8 @@ __device__ __forceinline__ void diffusion_edge(const FaceArgs<R>& a, const Physi
     }
     const int type = boundary ? ph.wall_type[wall] : 1;
     if (boundary && type == 0) return;             // zero flux: nothing added
+    MP_CHECK_INDEX(a.status, L, N);
+    if (!boundary) MP_CHECK_INDEX(a.status, Rc, N);
     const int o = horizontal ? 0 : 1;
     double DL[9], CL[9], DR[9], CR[9];
     double mHL = 0, mCL = 0, mHR = 0, mCR = 0;
@@ -818,6 +845,7 @@ struct SumArgs {
     // General quad meshes: the area of every cell (else `area` for all).
     const double* cell_area = nullptr;
     const int* gate = nullptr;   // device flag: the launch does nothing while it is 0
+    unsigned long long* status = nullptr;   // status word of the index checks (MP_CHECKED)
 };
 
 __device__ __forceinline__ bool gated_off(const int* gate) { return gate && *gate == 0; }
@@ -872,11 +900,14 @@ __device__ __forceinline__ void sum_cell(const SumArgs& a, unsigned cell, Partia
     const long long nI = (long long)nx * (ny + 1);
     const long long nE = nI + (long long)(nx + 1) * ny;
     const int i = (int)(cell % (unsigned)nx), j = (int)(cell / (unsigned)nx);
+    MP_CHECK_INDEX(a.status, cell, (long long)nx * ny);
     const double A = kArea ? __ldg(a.cell_area + cell) : a.area, invA = kArea ? 1.0 / A : a.inv_area;
     // Faces of this cell in the reference's id order: bottom, top, left, right,
     // each with the sign of its side (evolve.cpp:350-354).
     const long long eb = (long long)j * nx + i, et = (long long)(j + 1) * nx + i;
     const long long el = nI + (long long)j * (nx + 1) + i, er = el + 1;
+    MP_CHECK_INDEX(a.status, et, nI);
+    MP_CHECK_INDEX(a.status, er, nE);
     const int gj = a.gj0 + j, gny = global_ny(a);
     const double sb = -1.0, stp = (gj == gny - 1) ? -1.0 : 1.0, sl = (i == 0) ? -1.0 : 1.0, sr = -1.0;
     const long long ids[4] = {eb, et, el, er};

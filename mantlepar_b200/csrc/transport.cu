@@ -291,6 +291,10 @@ mp_status check_status(mp_transport* t, const char* where) {
     if (v == ~0ULL) return MP_OK;
     const long long cell = (long long)((v >> 8) & ((1ULL << 48) - 1));
     const int code = (int)(v & 0xff);
+    if ((int)(v >> 56) == PART_CHECK) {
+        set_error("%s: index check: index %lld outside its array (bounds-checked build)", where, cell);
+        return (mp_status)code;
+    }
     const char* what = code == MP_ERR_ARG_OUTOFRANGE ? "inadmissible state (T < 0, porosity >= 1, C outside [0,Xe] or backflow)"
                      : code == MP_ERR_FP ? "non-finite value in reconstruction, smoothness or CFL rate"
                      : code == MP_ERR_PHASE_INVALID ? "phase input outside [0, Xe] or non-finite"
@@ -387,7 +391,7 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
     {
         SumArgs a{t->nx, t->ny, t->host_tab.area, 1.0 / t->host_tab.area, t->face, H, C, t->H, t->C, outH, outC, t->rate, mode, a0, a1, dt,
                   t->partial, dtp, t->range.gj0, t->range.gny, (long long)t->range.own0 * t->nx,
-                  (long long)t->range.own1 * t->nx, sb.srcH, sb.srcR, sb.srcS, t->cell_area, gate};
+                  (long long)t->range.own1 * t->nx, sb.srcH, sb.srcR, sb.srcS, t->cell_area, gate, t->d_status};
         if (t->quad) {
             if (sb.srcH) timed(t, 3, [&] { sum_kernel<true, true><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });
             else timed(t, 3, [&] { sum_kernel<false, true><<<t->sum_blocks, kRedBlock, 0, s>>>(a); });

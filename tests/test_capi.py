@@ -125,3 +125,13 @@ def test_noalloc_rejects_unsupported_options_on_the_host(cuda_lib):
         assert b"mp_transport_rhs_noalloc" in cuda_lib.mp_last_error_string()
     big = _capi.MeshDesc(2, 16385, w.x0, w.x1, w.y0, w.y1)
     assert _noalloc_call(cuda_lib, big, base.to_c()) == 60
+
+
+def test_checked_variant_exports_the_same_symbols(cuda_lib):
+    """The bounds-checked build (MP_CHECKED) exports every declared symbol too."""
+    from mantlepar_b200 import build
+    path = build.build_checked()
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = [n for n in _capi.header_functions() if n not in exported]
+    assert not missing, missing

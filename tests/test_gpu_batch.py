@@ -91,3 +91,53 @@ def test_add_remove_and_autotune_keep_results(cuda_lib):
     got = b.get_state(k)
     assert np.array_equal(got["H"], H3) and np.array_equal(got["C"], C3)
     assert b.bytes_in_use() == sum(b.instance_bytes(w) for w in (WORKLOADS[1], WORKLOADS[3]))
+
+
+@pytest.mark.parametrize("device_steps", [True, False])
+def test_batch_adiabatic_source_equals_solo(cuda_lib, device_steps):
+    """alpha0 != 0 with thermal diffusion: every instance takes its own
+    cell-point velocities (src/couple/evolve.cpp:359-369); each equals its
+    single-instance run bit for bit, source integral in the reports."""
+    import dataclasses
+    from mantlepar_b200.batch import Batch
+    from mantlepar_b200.transport import Transport, TransportConfig
+    mat = dataclasses.replace(sy.material_s(), alpha0=3e-5)
+    cfg = TransportConfig(material=mat, cfl=0.4, integrator=3, diffusivity=1e-4)
+    ws = WORKLOADS[:4]
+    b = Batch(ws, cfg)
+    b.set_device_steps(device_steps)
+    b.set_thermal_bc((1, 1, 0, 0), (0.9, 0.2, 0.0, 0.0))
+    for i, w in enumerate(ws):
+        vs, ud = sy.face_velocity(w)
+        H, C = sy.initial_state(w)
+        b.set_face_velocity(i, vs, ud)
+        b.set_state(i, H, C)
+        b.set_cell_velocity(i, *sy.cell_velocity(w))
+    reps = b.step(6)
+    for i, w in enumerate(ws):
+        t = Transport(w, cfg)
+        t.set_thermal_bc((1, 1, 0, 0), (0.9, 0.2, 0.0, 0.0))
+        t.set_cell_velocity(*sy.cell_velocity(w))
+        t.set_face_velocity(*sy.face_velocity(w))
+        t.set_state(*sy.initial_state(w))
+        _, sreps = t.step(6)
+        got = b.get_state(i)
+        assert got["status"] == 0 and got["accepted"] == 6
+        for a, x in zip((got["H"], got["C"], got["T"], got["phi"]), t.get_state()):
+            assert np.array_equal(a, x)
+        assert [r[i]["sourceH"] for r in reps] == [r["sourceH"] for r in sreps]
+        assert [r[i]["balanceH"] for r in reps] == [r["balanceH"] for r in sreps]
+        assert any(r["sourceH"] != 0.0 for r in sreps)
+        t.close()
+    b.close()
+
+
+def test_batch_source_needs_cell_velocities(cuda_lib):
+    import dataclasses
+    from mantlepar_b200._capi import MPError
+    from mantlepar_b200.transport import TransportConfig
+    mat = dataclasses.replace(sy.material_s(), alpha0=3e-5)
+    b = batch_of(WORKLOADS[:2], TransportConfig(material=mat, cfl=0.4, integrator=3))
+    with pytest.raises(MPError) as err:
+        b.step(1)
+    assert err.value.code == 73
