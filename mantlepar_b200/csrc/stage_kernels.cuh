@@ -280,14 +280,17 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
     const long long key = cell + (long long)a.gj0 * nx;
     int st_lim = 0;
 
-    double u[3][3];
-    double DH[9], DC[9];
-    double mH, mC, loH, hiH, loC, hiC;
+    // One field at a time -- gather, reconstruct, limiter scan, theta, write
+    // its 9 record entries -- so only one deviation polynomial is live.
+    const int cls = cj * 3 + ci;
+    const int l0 = t.line_off[cls], l1 = t.line_off[cls + 1];
+    double mH = 0.0, mC = 0.0, hiH = 0.0, hiC = 0.0;
     int st = 0;
-    // Enthalpy, then composition: one 3x3 gather at a time keeps registers low.
-#pragma unroll
+    bool bad = false;
+#pragma unroll 1
     for (int f = 0; f < 2; ++f) {
         const double* F = f ? a.C : a.H;
+        double u[3][3];
 #pragma unroll
         for (int dj = 0; dj < 3; ++dj)
 #pragma unroll
@@ -303,30 +306,24 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
         for (int dj = 0; dj < 3; ++dj)
 #pragma unroll
             for (int di = 0; di < 3; ++di) { lo = fmin(lo, u[dj][di]); hi = fmax(hi, u[dj][di]); }
-        if (f == 0) {
-            mH = u[1][1]; loH = fmax(0.0, lo); hiH = hi;
-            const int s1 = reconstruct(t, ci, cj, u, DH);
-            st = st ? st : s1;
-        } else {
-            mC = u[1][1]; loC = fmax(0.0, lo); hiC = fmin(ph.k.Xe, hi);
-            const int s1 = reconstruct(t, ci, cj, u, DC);
-            st = st ? st : s1;
-        }
+        const double m = u[1][1];
+        lo = fmax(0.0, lo);
+        if (f) hi = fmin(ph.k.Xe, hi);
+        double D[9];
+        const int s1 = reconstruct(t, ci, cj, u, D);
+        st = st ? st : s1;
+        // Limiter over the class's points, evaluated line by line.
+        double dmx, dmn;
+        scan_lines<R>(t, a.tab, l0, l1, D, dmx, dmn, bad);
+        const double th = theta_of(m, lo, hi, dmx, dmn);
+        if (a.theta) a.theta[(size_t)f * N + cell] = th;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) a.rec[(size_t)(k + 9 * f) * N + cell] = D[k] * th;
+        if (f) { mC = m; hiC = hi; } else { mH = m; hiH = hi; }
     }
     // state_reconstruction.cpp:187-188: admissible means.
     if (!(isfinite(mH) && mH >= 0.0 && isfinite(mC) && mC >= 0.0 && mC <= ph.k.Xe)) st_lim = E_OUTOFRANGE;
-
-    // Limiter over the class's points, evaluated line by line.
-    const int cls = cj * 3 + ci;
-    const int l0 = t.line_off[cls], l1 = t.line_off[cls + 1];
-    double hmx, hmn, cmx, cmn;
-    bool bad = false;
-    scan_lines<R>(t, a.tab, l0, l1, DH, hmx, hmn, bad);
-    scan_lines<R>(t, a.tab, l0, l1, DC, cmx, cmn, bad);
     if (bad) st_lim = st_lim ? st_lim : E_FP;
-    const double thH = theta_of(mH, loH, hiH, hmx, hmn);
-    const double thC = theta_of(mC, loC, hiC, cmx, cmn);
-    if (a.theta) { a.theta[cell] = thH; a.theta[N + cell] = thC; }
     // Diffusion samples (zero diffusivity: kept for their admissibility
     // check). Limited values at limiter points stay in [lo, hi], so the
     // samples are admissible when hi_H is below the liquidus at hi_C and
@@ -335,11 +332,6 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
     const double tep = ph.litho ? fmin(tep_at(ph, t.y0 + gj * t.dy), tep_at(ph, t.y0 + (gj + 1) * t.dy)) : ph.Tep;
     const double Hliq = tep + (1.0 - hiC / ph.k.Xe) + ph.k.LD;
     const bool safe = tep >= 0.0 && hiH + 1e-12 * (1.0 + fabs(hiH)) < Hliq;
-#pragma unroll
-    for (int m = 0; m < 9; ++m) {
-        a.rec[(size_t)m * N + cell] = DH[m] * thH;
-        a.rec[(size_t)(m + 9) * N + cell] = DC[m] * thC;
-    }
     a.flags[cell] = safe ? 0 : FLAG_CHECK;
     if (st) record_error(a.status, PART_UPDATE, key, st);
     if (st_lim) record_error(a.status, PART_LIMIT, key, st_lim);

@@ -64,8 +64,14 @@ struct SourceBufs {
 // blocks per SM (register caps) as measured fastest on B200: cell phase 8,
 // faces 5; the reconstruction keeps its natural register count.
 // Rows [jlo, jhi) are reconstructed (all rows, or a slab's owned rows +- 1).
+// Minimum resident 128-thread blocks per SM of the reconstruction kernels
+// (a register cap): the one-field-at-a-time reconstruction fits 80 registers
+// without spills.
+#ifndef MP_RECON_BLOCKS
+#define MP_RECON_BLOCKS 6
+#endif
 template <class R>
-__global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
+__global__ void __launch_bounds__(128, MP_RECON_BLOCKS) recon_kernel(ReconArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
                                                     int jlo, int jhi) {
     if (gated_off(a.gate)) return;
     ReconArgs<R> b = a;
