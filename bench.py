@@ -408,8 +408,8 @@ def run_forms(args, stream):
         "fp64_value": w.cells * args.mixed_steps / (res[0][0] * 1e-3),
         "steps": args.mixed_steps, "errors_vs_fp64_path": errs,
         "bitwise_equal_to_fp64_path": all(bool(np.array_equal(a, b)) for a, b in zip(res[1][1], res[0][1])),
-        "precision": "FP32 screen of the limiter scan with an exact FP64 certificate; every value FP64 "
-                     "(smoothness, weights, coefficients, limited values, phase, fluxes, accumulation)"}
+        "precision": "FP64 stage (the form's 1e-6 per-cell bar admits no FP32 value on this path; an exact "
+                     "FP32 screen of the limiter scan measured slower than the FP64 scan)"}
     del res
     # Config 0: the 20x20 instance, 200 SSPRK3 steps, through the
     # single-instance path: device-resident steps (CUDA graph, one host wait
@@ -513,7 +513,7 @@ def run_forms(args, stream):
     #  (b) a load one GPU sustains: the same generator with nx up to 320,
     #      offered at 70% of the capacity measured in (a).
     if args.serve_requests > 0:
-        from mantlepar_b200.serve import Server, poisson_requests, request_work, run_stream
+        from mantlepar_b200.serve import Server, input_bytes, poisson_requests, request_work, run_stream
 
         def served(reqs, wall):
             srv = Server(TransportConfig(cfl=0.4, integrator=3, precision=1), memory_budget=64 << 30)
@@ -524,12 +524,13 @@ def run_forms(args, stream):
             return out
 
         reqs = poisson_requests(args.serve_requests, rate=200.0, seed=4)
-        # Queued requests keep their inputs (H, C and the face velocities) in
-        # host memory: keep that below a third of what the host has free.
+        # Inputs are prepared before the clock (face velocities once per
+        # mesh shape) and queued requests keep a copy in the server: keep
+        # twice the inputs' bytes below a third of the host's free memory.
         avail = host_available_bytes()
         kept, total = [], 0
         for r in reqs:
-            need = 8 * (2 * r.workload.cells + 10 * r.workload.edges)
+            need = 2 * input_bytes(r)
             if avail and total + need > avail / 3:
                 break
             kept.append(r)
@@ -584,10 +585,11 @@ def run_gpu(args, world, rank, local):
             pg.barrier()
         torch.cuda.synchronize()
 
-    # ---- resident throughput with per-kernel event timing
-    _capi.check(lib.mp_transport_profile(t._h, 1))
+    # ---- resident throughput: the default device-resident steps (CUDA graph,
+    # step decisions on the device)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches0 = _capi.kernel_launches()
+    syncs0 = t.host_syncs()
     barrier()
     with ClockSampler(local) as clk:
         barrier()
@@ -598,7 +600,19 @@ def run_gpu(args, world, rank, local):
         torch.cuda.synchronize()
         clk.mark_end()
     launches = _capi.kernel_launches() - launches0
+    host_syncs = t.host_syncs() - syncs0
     ms = e0.elapsed_time(e1)
+    # ---- per-kernel CUDA-event timing for the roofline: a second run of
+    # the same length through the host-driven loop (events around every
+    # kernel on the transport's stream)
+    _capi.check(lib.mp_transport_profile(t._h, 1))
+    e0p, e1p = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0p.record(stream)
+    t.step(args.steps)
+    e1p.record(stream)
+    torch.cuda.synchronize()
+    ms_profiled = e0p.elapsed_time(e1p)
     kms = (C.c_double * 6)()
     kn = (C.c_ulonglong * 6)()
     _capi.check(lib.mp_transport_kernel_times(t._h, kms, kn))
@@ -725,6 +739,8 @@ def run_gpu(args, world, rank, local):
                     "sequential": {"value": e2e_seq_value, "ms_per_step": ms_seq / args.steps},
                     "pipelined_equals_sequential": pipe_same},
             "gpu_launches": int(launches),
+            "host_syncs_per_step": host_syncs / args.steps,
+            "host_loop_ms_per_step": ms_profiled / args.steps,
             "clocks": clk.summary(),
             "retries": retries,
         }

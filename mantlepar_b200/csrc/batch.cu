@@ -72,7 +72,7 @@ struct Tuning { int bx = 32, by = 4, cpt = 1; };
 // ------------------------------------------------------------ batched kernels
 
 #ifndef MP_RECON_BLOCKS
-#define MP_RECON_BLOCKS 6   // register cap of the reconstruction kernel (see transport.cu)
+#define MP_RECON_BLOCKS 4   // register cap of the reconstruction kernel (see transport.cu)
 #endif
 template <class R>
 __global__ void __launch_bounds__(128, MP_RECON_BLOCKS) batch_recon_kernel(const InstArgs<R>* args, const Work* work, const int* active,
@@ -175,7 +175,6 @@ struct MPInstance {
     double *H, *C, *S1H, *S1C, *S2H, *S2C, *LH, *LC, *T, *phi, *rec, *rate, *vsn, *udn, *face;
     unsigned char* flags;
     mp::StageTables* tab;
-    mp::StageTablesF* tabF;
     mp::StageTables host_tab;
     // Adiabatic source (alpha0 != 0): vertical solid and Darcy velocities at
     // the 25 cell quadrature points and the per-cell source sums, one
@@ -203,7 +202,6 @@ struct mp_batch {
     mp_derived der;
     mp::Physics ph;
     cudaStream_t stream = nullptr;
-    bool mixed = false;
     std::vector<MPInstance> inst;
     // device tables rebuilt when the set changes
     bool dirty = true;
@@ -261,7 +259,7 @@ size_t instance_bytes(int nx, int ny) {
     b += align256(N);                            // flags
     b += 2 * align256(NE * kNQ * sizeof(double));// vsn udn
     b += align256(4 * NE * sizeof(double));      // face
-    b += align256(sizeof(StageTables)) + align256(sizeof(StageTablesF));
+    b += align256(sizeof(StageTables));
     return b;
 }
 
@@ -308,14 +306,10 @@ mp_status alloc_instance(mp_batch* b, MPInstance& in, const mp_mesh_desc& m) {
     in.udn = static_cast<double*>(take(NE * kNQ * sizeof(double)));
     in.face = static_cast<double*>(take(4 * NE * sizeof(double)));
     in.tab = static_cast<StageTables*>(take(sizeof(StageTables)));
-    in.tabF = static_cast<StageTablesF*>(take(sizeof(StageTablesF)));
-    StageTablesF tf;
-    tables_to_float(in.host_tab, tf);
     MP_CUDA(cudaMemcpyAsync(in.tab, &in.host_tab, sizeof(StageTables), cudaMemcpyHostToDevice, b->stream));
-    MP_CUDA(cudaMemcpyAsync(in.tabF, &tf, sizeof(StageTablesF), cudaMemcpyHostToDevice, b->stream));
     MP_CUDA(cudaMemsetAsync(in.vsn, 0, NE * kNQ * sizeof(double), b->stream));
     MP_CUDA(cudaMemsetAsync(in.udn, 0, NE * kNQ * sizeof(double), b->stream));
-    MP_CUDA(cudaStreamSynchronize(b->stream));   // tf lives on this stack frame
+    MP_CUDA(cudaStreamSynchronize(b->stream));   // the copy source is the instance record, which a later add may move
     in.used = true;
     in.time = 0.0; in.accepted = 0; in.have_L = false; in.status = 0;
     b->bytes_in_use += in.bytes;
@@ -357,7 +351,6 @@ mp_status rebuild_args(mp_batch* b, int slots) {
         if (!in.used) continue;
         Tab<R> tb;
         tb.t = in.tab;
-        if constexpr (sizeof(R) == 4) tb.f = in.tabF;
         const int nsum = (int)((in.N + kSumCells - 1) / kSumCells);
         part_off[i] = parts; part_cnt[i] = nsum;
         Partial* pp = nullptr;  // fixed below once the partial array exists
@@ -450,8 +443,7 @@ mp_status rebuild(mp_batch* b) {
         MP_CUDA(cudaMallocAsync((void**)&b->d_partial, std::max(parts, 1) * sizeof(Partial), s));
         b->partial_cap = parts;
     }
-    if (b->mixed) MP_TRY(rebuild_args<float>(b, slots));
-    else MP_TRY(rebuild_args<double>(b, slots));
+    MP_TRY(rebuild_args<double>(b, slots));
     b->dirty = false;
     b->gen += 1;      // the captured graph refers to the old argument arrays
     return MP_OK;
@@ -491,8 +483,7 @@ mp_status run_stage(mp_batch* b, int kind, const std::vector<int>& act) {
     MP_TRY(set_active(b, act));
     const int slots = (int)b->inst.size();
     MP_CUDA(cudaMemsetAsync(b->d_status, 0xff, slots * sizeof(unsigned long long), b->stream));
-    if (b->mixed) launch_kind<float>(b, kind);
-    else launch_kind<double>(b, kind);
+    launch_kind<double>(b, kind);
     MP_CUDA(cudaGetLastError());
     MP_CUDA(cudaMemcpyAsync(b->h_tot, b->d_tot, slots * sizeof(Totals), cudaMemcpyDeviceToHost, b->stream));
     MP_CUDA(cudaMemcpyAsync(b->h_status, b->d_status, slots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->stream));
@@ -695,9 +686,9 @@ mp_status autotune(mp_batch* b, int reps, double* best_ms) {
         b->dirty = true;
         MP_TRY(rebuild(b));
         MP_TRY(set_active(b, act));
-        if (b->mixed) launch_kind<float>(b, KIND_P); else launch_kind<double>(b, KIND_P);   // warm-up
+        launch_kind<double>(b, KIND_P);   // warm-up
         cudaEventRecord(e0, b->stream);
-        for (int r = 0; r < reps; ++r) { if (b->mixed) launch_kind<float>(b, KIND_P); else launch_kind<double>(b, KIND_P); }
+        for (int r = 0; r < reps; ++r) launch_kind<double>(b, KIND_P);
         cudaEventRecord(e1, b->stream);
         MP_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -841,7 +832,7 @@ mp_status ensure_graph(mp_batch* b) {
     cudaStream_t user = b->stream;
     b->stream = cap;
     g_capturing = true;
-    const mp_status st = b->mixed ? capture_graph<float>(b, &b->graph) : capture_graph<double>(b, &b->graph);
+    const mp_status st = capture_graph<double>(b, &b->graph);
     g_capturing = false;
     cudaStreamCaptureStatus cs;
     if (cudaStreamIsCapturing(cap, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
@@ -920,7 +911,6 @@ extern "C" mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, cons
     mp_batch* b = new mp_batch;
     b->opts = *opts; b->der = der;
     b->stream = (cudaStream_t)stream;
-    b->mixed = opts->precision == MP_PRECISION_MIXED;
     b->ph.k = phase_const(opts->material, der);
     b->ph.sk = stage_const(b->ph.k);
     if (eutectic_temperature(b->ph.k, opts->pressure, b->ph.Tep)) { delete b; set_error("pressure must be finite"); return MP_ERR_ARG_OUTOFRANGE; }

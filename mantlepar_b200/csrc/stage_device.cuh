@@ -23,44 +23,12 @@
 
 namespace mp {
 
-// Table entries in the arithmetic type R (FP32 copies for the mixed path).
-struct StageTablesF {
-    float C9[9][9];
-    float S9[8][8];
-    float C4[4][4];
-    float S4[4][3][3];
-    float SF9[36];
-    float SF4[4][6];
-    float X, Y, epsA, logEpsA2;
-    float gx[kNQ], gy[kNQ];
-    float mono[9];
-    float line_c[kMaxLines];
-};
-
-// The tables a single-instance launch passes by value (__grid_constant__):
-// FP64 set and its FP32 copy.
+// The tables a single-instance launch passes by value (__grid_constant__).
 struct ParamTables {
     StageHot d;
-    StageTablesF f;
 };
 
-inline void tables_to_float(const StageHot& t, StageTablesF& f) {
-    for (int a = 0; a < 9; ++a) for (int b = 0; b < 9; ++b) f.C9[a][b] = (float)t.C9[a][b];
-    for (int a = 0; a < 8; ++a) for (int b = 0; b < 8; ++b) f.S9[a][b] = (float)t.S9[a][b];
-    for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) f.C4[a][b] = (float)t.C4[a][b];
-    for (int k = 0; k < 4; ++k) for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) f.S4[k][a][b] = (float)t.S4[k][a][b];
-    for (int k = 0; k < 36; ++k) f.SF9[k] = (float)t.SF9[k];
-    for (int k = 0; k < 4; ++k) for (int a = 0; a < 6; ++a) f.SF4[k][a] = (float)t.SF4[k][a];
-    f.X = (float)t.X; f.Y = (float)t.Y; f.epsA = (float)t.epsA; f.logEpsA2 = (float)(2.0 * std::log(t.epsA));
-    for (int q = 0; q < kNQ; ++q) { f.gx[q] = (float)t.gx[q]; f.gy[q] = (float)t.gy[q]; }
-    for (int m = 0; m < 9; ++m) f.mono[m] = (float)t.mono[m];
-    for (int l = 0; l < kMaxLines; ++l) f.line_c[l] = (float)t.line_c[l];
-}
-
-inline void make_param_tables(const StageTables& t, ParamTables& p) {
-    p.d = static_cast<const StageHot&>(t);
-    tables_to_float(t, p.f);
-}
+inline void make_param_tables(const StageTables& t, ParamTables& p) { p.d = static_cast<const StageHot&>(t); }
 
 template <class R> struct Tab;
 // Tab pointing at the parameter-space copy (inside a kernel taking a
@@ -79,33 +47,13 @@ template <> struct Tab<double> {
     __device__ double epsA() const { return t->epsA; }
     __device__ double gx(int q) const { return t->gx[q]; }
     __device__ double gy(int q) const { return t->gy[q]; }
-    __device__ double mono(int m) const { return t->mono[m]; }
     __device__ double line_c(int l) const { return t->line_c[l]; }
-};
-template <> struct Tab<float> {
-    const StageHot* t;
-    const StageTablesF* f;
-    __device__ float C9(int c, int m) const { return f->C9[c][m]; }
-    __device__ float S9(int r, int c) const { return f->S9[r][c]; }
-    __device__ float C4(int c, int m) const { return f->C4[c][m]; }
-    __device__ float S4(int k, int r, int c) const { return f->S4[k][r][c]; }
-    __device__ float SF9(int k) const { return f->SF9[k]; }
-    __device__ float SF4(int p, int k) const { return f->SF4[p][k]; }
-    __device__ float X() const { return f->X; }
-    __device__ float Y() const { return f->Y; }
-    __device__ float epsA() const { return f->epsA; }
-    __device__ float gx(int q) const { return f->gx[q]; }
-    __device__ float gy(int q) const { return f->gy[q]; }
-    __device__ float mono(int m) const { return f->mono[m]; }
-    __device__ float line_c(int l) const { return f->line_c[l]; }
 };
 
 template <> __device__ __forceinline__ Tab<double> param_tab<double>(const ParamTables& p) { return Tab<double>{&p.d}; }
-template <> __device__ __forceinline__ Tab<float> param_tab<float>(const ParamTables& p) { return Tab<float>{&p.d, &p.f}; }
 
 template <class R> __device__ __forceinline__ R eps_of();
 template <> __device__ __forceinline__ double eps_of<double>() { return 2.220446049250313e-16; }
-template <> __device__ __forceinline__ float eps_of<float>() { return 1.1920929e-07f; }
 
 // Row / column coefficients of a Q2 polynomial (coefficient m = j*3 + i of
 // xi^i eta^j): along the row eta = y, p(xi) = a0 + xi*(a1 + xi*a2).

@@ -190,64 +190,19 @@ __device__ __forceinline__ void line_candidates(const StageHot& t, const Tab<R>&
 // the maximum and three for the minimum. With every |D_m| below scan_guard
 // no value can overflow, so no per-point finiteness test is needed;
 // otherwise the exact scan runs.
-//
-// R = float screens the lines in FP32 and returns the FP64 scan's values
-// exactly. An FP32 candidate and the FP64 candidate of the same point differ
-// by less than err = 1.5e-6 (|D_0| + beta) (beta = sum_m>0 |D_m| mono[m]
-// bounds the polynomial's variation over the points; the FP32 evaluation
-// makes about ten roundings of 2^-24 of that magnitude, its coordinates
-// included, the FP64 one far less). When the leading line of an extreme is
-// ahead of the runner-up by more than 2 err, the FP64 extreme lies on it,
-// and that line alone is evaluated again in FP64 (same operations as the
-// FP64 scan, so the same value); otherwise the FP64 scan runs.
 template <class R>
-__device__ __forceinline__ void scan_lines(const StageHot& t, const Tab<R>& tb, int l0, int l1, const double* Dd,
+__device__ __forceinline__ void scan_lines(const StageHot& t, const Tab<R>& tb, int l0, int l1, const double* D,
                                            double& mx, double& mn, bool& bad) {
     bool small = true;
 #pragma unroll
-    for (int m = 0; m < 9; ++m) small = small && fabs(Dd[m]) < t.scan_guard;
-    if (!small) { scan_lines_exact(t, l0, l1, Dd, mx, mn, bad); return; }
-    const Tab<double> td{&t};
-    const double gx1 = t.gx[3], gx2 = t.gx[4], gy1 = t.gy[3], gy2 = t.gy[4];
-    const double hx1 = gx1 * gx1, hx2 = gx2 * gx2, hy1 = gy1 * gy1, hy2 = gy2 * gy2;
-    if constexpr (sizeof(R) == 4) {
-        float D[9];
-#pragma unroll
-        for (int m = 0; m < 9; ++m) D[m] = (float)Dd[m];
-        float beta = 0.0f;
-#pragma unroll
-        for (int m = 1; m < 9; ++m) beta = fmaf(fabsf(D[m]), tb.mono(m), beta);
-        const float err2 = 3.0e-6f * (fabsf(D[0]) + beta);
-        const float sx1 = tb.gx(3), sx2 = tb.gx(4), sy1 = tb.gy(3), sy2 = tb.gy(4);
-        const float qx1 = sx1 * sx1, qx2 = sx2 * sx2, qy1 = sy1 * sy1, qy2 = sy2 * sy2;
-        float rmx = D[0], rmn = D[0];                 // the centre leads at first (line -1)
-        float smx = -INFINITY, smn = INFINITY;        // runners-up
-        int lmx = -1, lmn = -1;
-        for (int l = l0; l < l1; ++l) {
-            float p0, p1, p2, m1, m2;
-            line_candidates<float>(t, tb, l, D, sx1, sx2, sy1, sy2, qx1, qx2, qy1, qy2, p0, p1, p2, m1, m2);
-            const float lx = fmaxf(p0, fmaxf(p1, p2)), ln = fminf(p0, fminf(m1, m2));
-            if (lx > rmx) { smx = rmx; rmx = lx; lmx = l; } else { smx = fmaxf(smx, lx); }
-            if (ln < rmn) { smn = rmn; rmn = ln; lmn = l; } else { smn = fminf(smn, ln); }
-        }
-        if (rmx - smx > err2 && smn - rmn > err2) {
-            double p0, p1, p2, m1, m2;
-            mx = Dd[0]; mn = Dd[0];
-            if (lmx >= 0) {
-                line_candidates<double>(t, td, lmx, Dd, gx1, gx2, gy1, gy2, hx1, hx2, hy1, hy2, p0, p1, p2, m1, m2);
-                mx = p0 > mx ? p0 : mx; mx = p1 > mx ? p1 : mx; mx = p2 > mx ? p2 : mx;
-            }
-            if (lmn >= 0) {
-                line_candidates<double>(t, td, lmn, Dd, gx1, gx2, gy1, gy2, hx1, hx2, hy1, hy2, p0, p1, p2, m1, m2);
-                mn = p0 < mn ? p0 : mn; mn = m1 < mn ? m1 : mn; mn = m2 < mn ? m2 : mn;
-            }
-            return;
-        }
-    }
-    double rmx = Dd[0], rmn = Dd[0];   // cell centre
+    for (int m = 0; m < 9; ++m) small = small && fabs(D[m]) < t.scan_guard;
+    if (!small) { scan_lines_exact(t, l0, l1, D, mx, mn, bad); return; }
+    const double sx1 = tb.gx(3), sx2 = tb.gx(4), sy1 = tb.gy(3), sy2 = tb.gy(4);
+    const double qx1 = sx1 * sx1, qx2 = sx2 * sx2, qy1 = sy1 * sy1, qy2 = sy2 * sy2;
+    double rmx = D[0], rmn = D[0];   // cell centre
     for (int l = l0; l < l1; ++l) {
         double p0, p1, p2, m1, m2;
-        line_candidates<double>(t, td, l, Dd, gx1, gx2, gy1, gy2, hx1, hx2, hy1, hy2, p0, p1, p2, m1, m2);
+        line_candidates<double>(t, tb, l, D, sx1, sx2, sy1, sy2, qx1, qx2, qy1, qy2, p0, p1, p2, m1, m2);
         rmx = p0 > rmx ? p0 : rmx; rmx = p1 > rmx ? p1 : rmx; rmx = p2 > rmx ? p2 : rmx;
         rmn = p0 < rmn ? p0 : rmn; rmn = m1 < rmn ? m1 : rmn; rmn = m2 < rmn ? m2 : rmn;
     }

@@ -175,16 +175,6 @@ int build_stage_tables(int nx, int ny, double x0, double x1, double y0, double y
     }
     t.pt_off[9] = at;
     t.line_off[9] = nl;
-    // Monomial bounds over the scanned points: rows take xi = X*g_q and eta =
-    // line_c, columns xi = line_c and eta = Y*g_q.
-    double xb = 0.0, yb = 0.0;
-    for (int q = 0; q < kNQ; ++q) { xb = std::max(xb, std::fabs(t.gx[q])); yb = std::max(yb, std::fabs(t.gy[q])); }
-    for (int l = 0; l < nl; ++l) {
-        if (t.line_dir[l] == 0) yb = std::max(yb, std::fabs(t.line_c[l]));
-        else xb = std::max(xb, std::fabs(t.line_c[l]));
-    }
-    for (int j = 0; j < 3; ++j)
-        for (int i = 0; i < 3; ++i) t.mono[j * 3 + i] = std::pow(xb, i) * std::pow(yb, j);
     return MP_OK;
 }
 

@@ -71,11 +71,6 @@ struct StageHot {
     // value is finite (in FP32 too): 1e36 / (16 max(1, X^2) max(1, Y^2)),
     // the points lying within |xi| <= X, |eta| <= Y.
     double scan_guard;
-    // Bound of |xi^i eta^j| (index m = j*3 + i) over every point the limiter
-    // scan evaluates, in any class: XB^i YB^j with XB, YB the largest |xi|,
-    // |eta| of the line points. With beta = sum_m>0 |D_m| mono[m], every
-    // limiter value of a deviation polynomial D lies within D_0 +- beta.
-    double mono[9];
     // Limiter points grouped into 5-point lines: apart from the cell centre,
     // every limiter point lies on a row eta = line_c with xi = X*g_q, or on a
     // column xi = line_c with eta = Y*g_q (q = 0..4). Class c owns lines

@@ -65,10 +65,12 @@ struct SourceBufs {
 // faces 5; the reconstruction keeps its natural register count.
 // Rows [jlo, jhi) are reconstructed (all rows, or a slab's owned rows +- 1).
 // Minimum resident 128-thread blocks per SM of the reconstruction kernels
-// (a register cap): the one-field-at-a-time reconstruction fits 80 registers
-// without spills.
+// (a register cap). Measured at 1280x2560 (CUDA events per stage): 4 blocks
+// (the kernel's natural 108 registers) 0.576 ms; 5, 6, 7, 8 blocks (96, 80,
+// 72, 64 registers) 0.615, 0.627, 0.631, 0.631 ms -- more resident warps do
+// not pay for the tighter allocation.
 #ifndef MP_RECON_BLOCKS
-#define MP_RECON_BLOCKS 6
+#define MP_RECON_BLOCKS 4
 #endif
 template <class R>
 __global__ void __launch_bounds__(128, MP_RECON_BLOCKS) recon_kernel(ReconArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
@@ -184,7 +186,6 @@ struct mp_transport {
     double *T = nullptr, *phi = nullptr;
     void* rec = nullptr;                    // 18 * N doubles (limited deviation polynomials)
     unsigned char* flags = nullptr;         // wet | exact-check flags per cell
-    bool mixed = false;
     double *vsn = nullptr, *udn = nullptr;
     double* face = nullptr;
     double* rate = nullptr;
@@ -387,9 +388,6 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
                               static_cast<double*>(t->rec), t->flags, t->T, t->phi, t->vsn, t->udn, t->face,
                               t->d_status, theta, SourcePtrs{sb.cvs_y, sb.cud_y, sb.srcH, sb.srcR, sb.srcS}, s);
         });
-    } else if (t->mixed) {
-        launch_stage_kernels<float>(t->nx, t->ny, t->range, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T, t->phi,
-                                    t->vsn, t->udn, t->face, t->d_status, theta, s, prof, sb, gate);
     } else {
         launch_stage_kernels<double>(t->nx, t->ny, t->range, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T,
                                      t->phi, t->vsn, t->udn, t->face, t->d_status, theta, s, prof, sb, gate);
@@ -850,7 +848,6 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
     t->NE = (size_t)t->nx * (t->ny + 1) + (size_t)(t->nx + 1) * t->ny;
     t->ph.k = phase_const(opts->material, der);
     t->ph.sk = stage_const(t->ph.k);
-    t->mixed = opts->precision == MP_PRECISION_MIXED;
     double Tep;
     if (eutectic_temperature(t->ph.k, opts->pressure, Tep)) { delete t; set_error("pressure must be finite"); return MP_ERR_ARG_OUTOFRANGE; }
     t->ph.Tep = Tep; t->ph.theta = opts->theta;

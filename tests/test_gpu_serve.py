@@ -66,3 +66,22 @@ def test_oversized_request_is_refused(cuda_lib):
     with pytest.raises(MPError):
         srv.set_policy(0, -1)
     srv.close()
+
+
+def test_bounded_stream_reports_completed_and_censored(cuda_lib):
+    """run_stream with a wall bound: a short stream of small solves finishes
+    within it; with a bound shorter than the work, the unfinished requests
+    are reported as censored and the server still shuts down cleanly."""
+    from mantlepar_b200.serve import Server, poisson_requests, run_stream
+    from mantlepar_b200.transport import TransportConfig
+    reqs = poisson_requests(6, rate=50.0, seed=7, max_nx=60)
+    srv = Server(TransportConfig(cfl=0.4, integrator=3, precision=1), memory_budget=1 << 30)
+    out = run_stream(srv, reqs, wall_limit=120.0)
+    srv.close()
+    assert out["completed"] == 6 and out["censored"] == 0 and out["all_ok"]
+    assert out["p50_ms"] <= out["p99_ms"] and out["service_p50_ms"] > 0
+    big = poisson_requests(4, rate=50.0, seed=8, max_nx=1280)
+    srv = Server(TransportConfig(cfl=0.4, integrator=3, precision=1), memory_budget=8 << 30)
+    out = run_stream(srv, big, wall_limit=1.0)
+    srv.close()
+    assert out["completed"] + out["censored"] == 4 and out["censored"] >= 1
