@@ -466,8 +466,11 @@ mp_status mp_batch_profile(mp_batch* b, int enable);
  * host-driven loop (enable = 0) bit for bit. Profiling (mp_batch_profile)
  * uses the host-driven loop. */
 mp_status mp_batch_set_device_steps(mp_batch* b, int enable);
-/* Host waits for device results made by the stepping calls so far. */
-mp_status mp_batch_run_stats(const mp_batch* b, unsigned long long* host_syncs);
+/* Host waits for device results made by the stepping calls so far, and the
+ * number of times the step graph was captured (again only when an array's
+ * capacity grows, the tile is retuned or the physics changes -- not when
+ * instances come and go). Either pointer may be NULL. */
+mp_status mp_batch_run_stats(const mp_batch* b, unsigned long long* host_syncs, unsigned long long* graph_captures);
 mp_status mp_batch_kernel_times(mp_batch* b, double ms[6], unsigned long long launches[6]);
 
 /* --------------------------------------------------------------- serving */

@@ -140,7 +140,7 @@ def lib() -> C.CDLL:
         "mp_transport_run_stats": (i, [vp, C.POINTER(C.c_ulonglong)]),
         "mp_batch_set_device_steps": (i, [vp, i]),
         "mp_batch_set_cell_velocity": (i, [vp, i, vp, vp]),
-        "mp_batch_run_stats": (i, [vp, C.POINTER(C.c_ulonglong)]),
+        "mp_batch_run_stats": (i, [vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
         "mp_transport_profile": (i, [vp, i]),
         "mp_transport_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
         "mp_probe_fp64_peak": (i, [vp, C.POINTER(C.c_double)]),

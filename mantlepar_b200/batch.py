@@ -114,7 +114,13 @@ class Batch:
     def host_syncs(self) -> int:
         """Host waits for device results made by step() so far."""
         n = C.c_ulonglong(0)
-        _capi.check(self._lib.mp_batch_run_stats(self._h, C.byref(n)))
+        _capi.check(self._lib.mp_batch_run_stats(self._h, C.byref(n), None))
+        return n.value
+
+    def graph_captures(self) -> int:
+        """Times the step graph was captured so far."""
+        n = C.c_ulonglong(0)
+        _capi.check(self._lib.mp_batch_run_stats(self._h, None, C.byref(n)))
         return n.value
 
     def autotune(self, reps: int = 2):

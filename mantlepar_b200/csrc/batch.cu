@@ -209,7 +209,12 @@ struct mp_batch {
     void* d_args[mp::NKIND] = {nullptr, nullptr, nullptr};
     mp::AxpyArgs* d_axpy = nullptr;
     mp::Work *d_wrecon = nullptr, *d_wphase = nullptr, *d_wface = nullptr, *d_wsum = nullptr;
+    // Work lists: filled entries n_w*, allocated (and launched) cap_w*; the
+    // entries past n_w* name the sentinel slot `slots`, never active, so a
+    // change of the instance set rewrites contents only and the captured
+    // graph stays valid until a capacity grows.
     int n_wrecon = 0, n_wphase = 0, n_wface = 0, n_wsum = 0;
+    int cap_wrecon = 0, cap_wphase = 0, cap_wface = 0, cap_wsum = 0;
     int *d_active = nullptr, *d_part_off = nullptr, *d_part_cnt = nullptr;
     mp::Partial* d_partial = nullptr;
     int partial_cap = 0;
@@ -237,6 +242,7 @@ struct mp_batch {
     mp::CommitArgs* d_commit = nullptr;
     int stage_kernels = 0;             // kernels of one stage kind (graph launch count)
     unsigned long long host_syncs = 0; // host waits of the stepping calls
+    unsigned long long captures = 0;   // graph captures
     // profiling
     bool profile = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -325,13 +331,17 @@ void free_instance(mp_batch* b, MPInstance& in) {
     b->dirty = true;
 }
 
+// Grow-only device array: at least `need` entries, with headroom; *grown is
+// set when the array moved (the captured graph must then be captured again).
 template <class T>
-mp_status ensure(T** p, size_t count, size_t& cap_bytes_tracker, cudaStream_t s) {
-    (void)cap_bytes_tracker;
+mp_status grow(T** p, int& cap, int need, cudaStream_t s, bool* grown) {
+    if (*p && need <= cap) return MP_OK;
     if (*p) cudaFreeAsync(*p, s);
     *p = nullptr;
-    if (count == 0) count = 1;
-    MP_CUDA(cudaMallocAsync((void**)p, count * sizeof(T), s));
+    const int n = std::max(need + need / 2, 64);
+    MP_CUDA(cudaMallocAsync((void**)p, (size_t)n * sizeof(T), s));
+    cap = n;
+    *grown = true;
     return MP_OK;
 }
 
@@ -385,27 +395,33 @@ mp_status rebuild_args(mp_batch* b, int slots) {
     }
     (void)parts;
     cudaStream_t s = b->stream;
-    for (int k = 0; k < NKIND; ++k) {
-        if (b->d_args[k]) cudaFreeAsync(b->d_args[k], s);
-        MP_CUDA(cudaMallocAsync(&b->d_args[k], std::max<size_t>(1, slots) * sizeof(InstArgs<R>), s));
-        MP_CUDA(cudaMemcpyAsync(b->d_args[k], args[k].data(), slots * sizeof(InstArgs<R>), cudaMemcpyHostToDevice, s));
-    }
-    size_t dummy = 0;
-    MP_TRY(ensure(&b->d_axpy, slots, dummy, s));
-    MP_CUDA(cudaMemcpyAsync(b->d_axpy, ax.data(), slots * sizeof(AxpyArgs), cudaMemcpyHostToDevice, s));
-    MP_TRY(ensure(&b->d_commit, slots, dummy, s));
-    MP_CUDA(cudaMemcpyAsync(b->d_commit, cm.data(), slots * sizeof(CommitArgs), cudaMemcpyHostToDevice, s));
-    MP_TRY(ensure(&b->d_wrecon, wr.size(), dummy, s));
-    MP_TRY(ensure(&b->d_wphase, wp.size(), dummy, s));
-    MP_TRY(ensure(&b->d_wface, wf.size(), dummy, s));
-    MP_TRY(ensure(&b->d_wsum, ws.size(), dummy, s));
-    if (!wr.empty()) MP_CUDA(cudaMemcpyAsync(b->d_wrecon, wr.data(), wr.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
-    if (!wp.empty()) MP_CUDA(cudaMemcpyAsync(b->d_wphase, wp.data(), wp.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
-    if (!wf.empty()) MP_CUDA(cudaMemcpyAsync(b->d_wface, wf.data(), wf.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
-    if (!ws.empty()) MP_CUDA(cudaMemcpyAsync(b->d_wsum, ws.data(), ws.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+    // Per-slot records live in arrays of b->slots entries (allocated in rebuild).
+    const int cap = b->slots;
+    for (int k = 0; k < NKIND; ++k) args[k].resize(cap);
+    ax.resize(cap);
+    cm.resize(cap);
+    part_off.resize(cap, 0);
+    part_cnt.resize(cap, 0);
+    for (int k = 0; k < NKIND; ++k)
+        MP_CUDA(cudaMemcpyAsync(b->d_args[k], args[k].data(), cap * sizeof(InstArgs<R>), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaMemcpyAsync(b->d_axpy, ax.data(), cap * sizeof(AxpyArgs), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaMemcpyAsync(b->d_commit, cm.data(), cap * sizeof(CommitArgs), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaMemcpyAsync(b->d_part_off, part_off.data(), cap * sizeof(int), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaMemcpyAsync(b->d_part_cnt, part_cnt.data(), cap * sizeof(int), cudaMemcpyHostToDevice, s));
+    // Work lists, padded to their capacity with the sentinel slot.
+    bool grown = false;
     b->n_wrecon = (int)wr.size(); b->n_wphase = (int)wp.size(); b->n_wface = (int)wf.size(); b->n_wsum = (int)ws.size();
-    MP_CUDA(cudaMemcpyAsync(b->d_part_off, part_off.data(), slots * sizeof(int), cudaMemcpyHostToDevice, s));
-    MP_CUDA(cudaMemcpyAsync(b->d_part_cnt, part_cnt.data(), slots * sizeof(int), cudaMemcpyHostToDevice, s));
+    MP_TRY(grow(&b->d_wrecon, b->cap_wrecon, b->n_wrecon, s, &grown));
+    MP_TRY(grow(&b->d_wphase, b->cap_wphase, b->n_wphase, s, &grown));
+    MP_TRY(grow(&b->d_wface, b->cap_wface, b->n_wface, s, &grown));
+    MP_TRY(grow(&b->d_wsum, b->cap_wsum, b->n_wsum, s, &grown));
+    const Work pad{cap, 0, 0, 0};
+    wr.resize(b->cap_wrecon, pad); wp.resize(b->cap_wphase, pad); wf.resize(b->cap_wface, pad); ws.resize(b->cap_wsum, pad);
+    MP_CUDA(cudaMemcpyAsync(b->d_wrecon, wr.data(), wr.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaMemcpyAsync(b->d_wphase, wp.data(), wp.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaMemcpyAsync(b->d_wface, wf.data(), wf.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaMemcpyAsync(b->d_wsum, ws.data(), ws.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+    if (grown) b->gen += 1;
     MP_CUDA(cudaStreamSynchronize(s));   // host vectors go out of scope
     return MP_OK;
 }
@@ -414,38 +430,48 @@ mp_status rebuild(mp_batch* b) {
     if (!b->dirty) return MP_OK;
     cudaStream_t s = b->stream;
     const int slots = (int)b->inst.size();
-    // per-slot arrays
-    if (slots > b->slots) {
+    // Per-slot arrays, with headroom; d_active has one more entry, the
+    // sentinel slot named by padded work items, which stays 0.
+    if (slots > b->slots || b->slots == 0) {
         for (void* p : {(void*)b->d_active, (void*)b->d_part_off, (void*)b->d_part_cnt, (void*)b->d_tot,
-                        (void*)b->d_status, (void*)b->d_dt})
+                        (void*)b->d_status, (void*)b->d_dt, (void*)b->d_axpy, (void*)b->d_commit, b->d_args[0],
+                        b->d_args[1], b->d_args[2]})
             if (p) cudaFreeAsync(p, s);
         if (b->h_tot) cudaFreeHost(b->h_tot);
         if (b->h_status) cudaFreeHost(b->h_status);
         if (b->h_dt) cudaFreeHost(b->h_dt);
         if (b->h_active) cudaFreeHost(b->h_active);
-        const int cap = std::max(slots, 8);
-        MP_CUDA(cudaMallocAsync((void**)&b->d_active, cap * sizeof(int), s));
+        const int cap = std::max(slots + slots / 2, 8);
+        MP_CUDA(cudaMallocAsync((void**)&b->d_active, (cap + 1) * sizeof(int), s));
+        MP_CUDA(cudaMemsetAsync(b->d_active, 0, (cap + 1) * sizeof(int), s));
         MP_CUDA(cudaMallocAsync((void**)&b->d_part_off, cap * sizeof(int), s));
         MP_CUDA(cudaMallocAsync((void**)&b->d_part_cnt, cap * sizeof(int), s));
         MP_CUDA(cudaMallocAsync((void**)&b->d_tot, cap * sizeof(Totals), s));
         MP_CUDA(cudaMallocAsync((void**)&b->d_status, cap * sizeof(unsigned long long), s));
+        MP_CUDA(cudaMemsetAsync(b->d_status, 0xff, cap * sizeof(unsigned long long), s));
         MP_CUDA(cudaMallocAsync((void**)&b->d_dt, cap * sizeof(double), s));
+        MP_CUDA(cudaMallocAsync((void**)&b->d_axpy, cap * sizeof(AxpyArgs), s));
+        MP_CUDA(cudaMallocAsync((void**)&b->d_commit, cap * sizeof(CommitArgs), s));
+        for (int k = 0; k < NKIND; ++k) MP_CUDA(cudaMallocAsync(&b->d_args[k], cap * sizeof(InstArgs<double>), s));
         MP_CUDA(cudaMallocHost((void**)&b->h_tot, cap * sizeof(Totals)));
         MP_CUDA(cudaMallocHost((void**)&b->h_status, cap * sizeof(unsigned long long)));
         MP_CUDA(cudaMallocHost((void**)&b->h_dt, cap * sizeof(double)));
         MP_CUDA(cudaMallocHost((void**)&b->h_active, cap * sizeof(int)));
+        for (int i = 0; i < cap; ++i) b->h_active[i] = 0;
         b->slots = cap;
+        b->gen += 1;
     }
     int parts = 0;
     for (const MPInstance& in : b->inst) if (in.used) parts += (int)((in.N + kSumCells - 1) / kSumCells);
     if (parts > b->partial_cap) {
         if (b->d_partial) cudaFreeAsync(b->d_partial, s);
-        MP_CUDA(cudaMallocAsync((void**)&b->d_partial, std::max(parts, 1) * sizeof(Partial), s));
-        b->partial_cap = parts;
+        const int n = std::max(parts + parts / 2, 64);
+        MP_CUDA(cudaMallocAsync((void**)&b->d_partial, n * sizeof(Partial), s));
+        b->partial_cap = n;
+        b->gen += 1;
     }
     MP_TRY(rebuild_args<double>(b, slots));
     b->dirty = false;
-    b->gen += 1;      // the captured graph refers to the old argument arrays
     return MP_OK;
 }
 
@@ -461,19 +487,16 @@ void launch_kind(mp_batch* b, int kind) {
     cudaStream_t s = b->stream;
     const InstArgs<R>* args = static_cast<const InstArgs<R>*>(b->d_args[kind]);
     const Tuning tu = b->tune;
-    if (b->n_wrecon) timed(b, 0, [&] { batch_recon_kernel<R><<<b->n_wrecon, dim3(tu.bx, tu.by), 0, s>>>(args, b->d_wrecon, b->d_active, b->ph, tu.cpt); });
-    if (b->n_wphase) {
-        if (b->ph.source) timed(b, 1, [&] { batch_phase_kernel<R, true><<<b->n_wphase, 128, 0, s>>>(args, b->d_wphase, b->d_active, b->ph); });
-        else timed(b, 1, [&] { batch_phase_kernel<R, false><<<b->n_wphase, 128, 0, s>>>(args, b->d_wphase, b->d_active, b->ph); });
-    }
-    if (b->n_wface) timed(b, 2, [&] { batch_face_kernel<R><<<b->n_wface, 128, 0, s>>>(args, b->d_wface, b->d_active, b->ph); });
-    if (b->n_wface && b->ph.diffusion)
-        timed(b, 2, [&] { batch_diffusion_kernel<R><<<b->n_wface, 128, 0, s>>>(args, b->d_wface, b->d_active, b->ph); });
-    if (b->n_wsum) {
-        if (b->ph.source) timed(b, 3, [&] { batch_sum_kernel<R, true><<<b->n_wsum, kRedBlock, 0, s>>>(args, b->d_wsum, b->d_active); });
-        else timed(b, 3, [&] { batch_sum_kernel<R, false><<<b->n_wsum, kRedBlock, 0, s>>>(args, b->d_wsum, b->d_active); });
-    }
-    timed(b, 4, [&] { batch_reduce_kernel<<<(int)b->inst.size(), 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot); });
+    // Grids cover the work lists' capacities (padded items exit at once).
+    timed(b, 0, [&] { batch_recon_kernel<R><<<b->cap_wrecon, dim3(tu.bx, tu.by), 0, s>>>(args, b->d_wrecon, b->d_active, b->ph, tu.cpt); });
+    if (b->ph.source) timed(b, 1, [&] { batch_phase_kernel<R, true><<<b->cap_wphase, 128, 0, s>>>(args, b->d_wphase, b->d_active, b->ph); });
+    else timed(b, 1, [&] { batch_phase_kernel<R, false><<<b->cap_wphase, 128, 0, s>>>(args, b->d_wphase, b->d_active, b->ph); });
+    timed(b, 2, [&] { batch_face_kernel<R><<<b->cap_wface, 128, 0, s>>>(args, b->d_wface, b->d_active, b->ph); });
+    if (b->ph.diffusion)
+        timed(b, 2, [&] { batch_diffusion_kernel<R><<<b->cap_wface, 128, 0, s>>>(args, b->d_wface, b->d_active, b->ph); });
+    if (b->ph.source) timed(b, 3, [&] { batch_sum_kernel<R, true><<<b->cap_wsum, kRedBlock, 0, s>>>(args, b->d_wsum, b->d_active); });
+    else timed(b, 3, [&] { batch_sum_kernel<R, false><<<b->cap_wsum, kRedBlock, 0, s>>>(args, b->d_wsum, b->d_active); });
+    timed(b, 4, [&] { batch_reduce_kernel<<<b->slots, 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot); });
     count_launch(5);
 }
 
@@ -498,8 +521,8 @@ mp_status run_axpy(mp_batch* b, const std::vector<int>& act) {
     const int slots = (int)b->inst.size();
     cudaStream_t s = b->stream;
     MP_CUDA(cudaMemcpyAsync(b->d_dt, b->h_dt, slots * sizeof(double), cudaMemcpyHostToDevice, s));
-    if (b->n_wsum) timed(b, 4, [&] { batch_axpy_kernel<<<b->n_wsum, kRedBlock, 0, s>>>(b->d_axpy, b->d_wsum, b->d_active); });
-    timed(b, 4, [&] { batch_reduce_kernel<<<slots, 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot); });
+    timed(b, 4, [&] { batch_axpy_kernel<<<b->cap_wsum, kRedBlock, 0, s>>>(b->d_axpy, b->d_wsum, b->d_active); });
+    timed(b, 4, [&] { batch_reduce_kernel<<<b->slots, 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot); });
     count_launch(2);
     MP_CUDA(cudaGetLastError());
     MP_CUDA(cudaMemcpyAsync(b->h_tot, b->d_tot, slots * sizeof(Totals), cudaMemcpyDeviceToHost, s));
@@ -699,6 +722,7 @@ mp_status autotune(mp_batch* b, int reps, double* best_ms) {
     b->tune = pick;
     b->dirty = true;
     MP_TRY(rebuild(b));
+    b->gen += 1;      // the captured graph has the block shape of the old tile
     // the timing runs overwrote L and T/phi of every instance: recompute L(U^n)
     for (MPInstance& in : b->inst) in.have_L = false;
     if (best_ms) *best_ms = best / reps;
@@ -749,7 +773,7 @@ mp_status add_while(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, cud
 template <class R>
 mp_status capture_graph(mp_batch* b, cudaGraph_t* out) {
     cudaStream_t s = b->stream;
-    const int slots = (int)b->inst.size();
+    const int slots = b->slots;          // control records of every slot of the capacity
     const StepOpts so = step_opts(b);
     const bool rk3 = so.rk3 != 0;
     cudaGraph_t g = nullptr;
@@ -773,8 +797,8 @@ mp_status capture_graph(mp_batch* b, cudaGraph_t* out) {
     // One attempt.
     MP_CUDA(cudaStreamBeginCaptureToGraph(s, attempt_body, nullptr, nullptr, 0, mode));
     ctl_attempt_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_hdr, b->d_active, b->d_dt);
-    if (b->n_wsum) batch_axpy_kernel<<<b->n_wsum, kRedBlock, 0, s>>>(b->d_axpy, b->d_wsum, b->d_active);
-    batch_reduce_kernel<<<slots, 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot);
+    batch_axpy_kernel<<<b->cap_wsum, kRedBlock, 0, s>>>(b->d_axpy, b->d_wsum, b->d_active);
+    batch_reduce_kernel<<<b->slots, 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot);
     ctl_after_axpy_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_tot, b->d_status, b->d_active);
     launch_kind<R>(b, KIND_B);
     ctl_after_stage_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_tot, b->d_status, b->d_active, 2,
@@ -788,7 +812,7 @@ mp_status capture_graph(mp_batch* b, cudaGraph_t* out) {
     // Commit and L(U^{n+1}).
     MP_CUDA(cudaStreamBeginCaptureToGraph(s, step_body, &attempt_node, nullptr, 1, mode));
     ctl_commit_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_hdr, b->d_rep, b->d_status, b->d_active);
-    if (b->n_wsum) batch_commit_kernel<<<b->n_wsum, kRedBlock, 0, s>>>(b->d_commit, b->d_wsum, b->d_active);
+    batch_commit_kernel<<<b->cap_wsum, kRedBlock, 0, s>>>(b->d_commit, b->d_wsum, b->d_active);
     launch_kind<R>(b, KIND_P);
     ctl_after_rhs_kernel<<<1, kCtlThreads, 0, s>>>(b->d_ctl, slots, so, b->d_tot, b->d_status, b->d_rep, b->d_hdr, 0,
                                                     run);
@@ -806,12 +830,11 @@ void release_graph(mp_batch* b) {
 }
 
 mp_status ensure_graph(mp_batch* b) {
-    const int slots = (int)b->inst.size();
     cudaStream_t s = b->stream;
-    if (slots > b->graph_slots) {
+    if (b->slots != b->graph_slots) {
         for (void* p : {(void*)b->d_ctl, (void*)b->d_hdr, (void*)b->d_rep}) if (p) cudaFreeAsync(p, s);
         for (void* p : {(void*)b->h_ctl, (void*)b->h_hdr, (void*)b->h_rep}) if (p) cudaFreeHost(p);
-        const int cap = std::max(slots, 8);
+        const int cap = b->slots;
         MP_CUDA(cudaMallocAsync((void**)&b->d_ctl, cap * sizeof(InstCtl), s));
         MP_CUDA(cudaMallocAsync((void**)&b->d_hdr, sizeof(CtlHeader), s));
         MP_CUDA(cudaMallocAsync((void**)&b->d_rep, (size_t)kGraphChunk * cap * sizeof(mp_step_report), s));
@@ -823,8 +846,7 @@ mp_status ensure_graph(mp_batch* b) {
     }
     if (b->graph_exec && b->graph_gen == b->gen) return MP_OK;
     release_graph(b);
-    b->stage_kernels = (b->n_wrecon ? 1 : 0) + (b->n_wphase ? 1 : 0) + (b->n_wface ? 1 : 0) +
-                       (b->n_wface && b->ph.diffusion ? 1 : 0) + (b->n_wsum ? 1 : 0) + 1;
+    b->stage_kernels = 5 + (b->ph.diffusion ? 1 : 0);
     // Capture on a private stream (the caller's may be the legacy default
     // stream, which cannot be captured); the graph runs on the caller's.
     cudaStream_t cap = nullptr;
@@ -844,6 +866,7 @@ mp_status ensure_graph(mp_batch* b) {
     if (st != MP_OK) { release_graph(b); return st; }
     MP_CUDA(cudaGraphInstantiate(&b->graph_exec, b->graph, 0));
     b->graph_gen = b->gen;
+    b->captures += 1;
     return MP_OK;
 }
 
@@ -856,25 +879,27 @@ mp_status graph_steps(mp_batch* b, int nsteps, mp_step_report* reports) {
     MP_TRY(eval_missing(b));
     MP_TRY(ensure_graph(b));
     const int slots = (int)b->inst.size();
+    const int cap = b->slots;            // control records and report rows cover the capacity
     cudaStream_t s = b->stream;
     for (int done = 0; done < nsteps; done += kGraphChunk) {
         const int chunk = std::min(kGraphChunk, nsteps - done);
-        for (int i = 0; i < slots; ++i) {
-            const MPInstance& in = b->inst[i];
+        for (int i = 0; i < cap; ++i) {
             InstCtl& c = b->h_ctl[i];
             c = InstCtl{};
+            if (i >= slots) continue;
+            const MPInstance& in = b->inst[i];
             c.used = in.used ? 1 : 0;
             c.time = in.time; c.t_end = in.t_end;
             c.accepted = in.accepted; c.status = in.status; c.have_L = in.have_L ? 1 : 0;
             c.cur = in.cur;
         }
         *b->h_hdr = CtlHeader{0, chunk, 0, 0, 0};
-        MP_CUDA(cudaMemcpyAsync(b->d_ctl, b->h_ctl, slots * sizeof(InstCtl), cudaMemcpyHostToDevice, s));
+        MP_CUDA(cudaMemcpyAsync(b->d_ctl, b->h_ctl, cap * sizeof(InstCtl), cudaMemcpyHostToDevice, s));
         MP_CUDA(cudaMemcpyAsync(b->d_hdr, b->h_hdr, sizeof(CtlHeader), cudaMemcpyHostToDevice, s));
         MP_CUDA(cudaGraphLaunch(b->graph_exec, s));
-        MP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, slots * sizeof(InstCtl), cudaMemcpyDeviceToHost, s));
+        MP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, cap * sizeof(InstCtl), cudaMemcpyDeviceToHost, s));
         MP_CUDA(cudaMemcpyAsync(b->h_hdr, b->d_hdr, sizeof(CtlHeader), cudaMemcpyDeviceToHost, s));
-        MP_CUDA(cudaMemcpyAsync(b->h_rep, b->d_rep, (size_t)chunk * slots * sizeof(mp_step_report),
+        MP_CUDA(cudaMemcpyAsync(b->h_rep, b->d_rep, (size_t)chunk * cap * sizeof(mp_step_report),
                                 cudaMemcpyDeviceToHost, s));
         MP_CUDA(cudaStreamSynchronize(s));
         b->host_syncs += 1;
@@ -892,7 +917,9 @@ mp_status graph_steps(mp_batch* b, int nsteps, mp_step_report* reports) {
             in.cur = c.cur;
         }
         if (reports)
-            std::memcpy(reports + (size_t)done * slots, b->h_rep, (size_t)chunk * slots * sizeof(mp_step_report));
+            for (int k = 0; k < chunk; ++k)
+                std::memcpy(reports + (size_t)(done + k) * slots, b->h_rep + (size_t)k * cap,
+                            (size_t)slots * sizeof(mp_step_report));
     }
     return MP_OK;
 }
@@ -1106,9 +1133,11 @@ extern "C" mp_status mp_batch_set_device_steps(mp_batch* b, int enable) {
     return MP_OK;
 }
 
-extern "C" mp_status mp_batch_run_stats(const mp_batch* b, unsigned long long* host_syncs) {
-    if (!b || !host_syncs) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
-    *host_syncs = b->host_syncs;
+extern "C" mp_status mp_batch_run_stats(const mp_batch* b, unsigned long long* host_syncs,
+                                        unsigned long long* graph_captures) {
+    if (!b) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (host_syncs) *host_syncs = b->host_syncs;
+    if (graph_captures) *graph_captures = b->captures;
     return MP_OK;
 }
 

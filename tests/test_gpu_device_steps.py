@@ -182,3 +182,35 @@ def test_batch_graph_equals_host_loop(cuda_lib, integ, precision):
     assert g[1][4]["status"] == 63 and g[1][2]["time"] == 4e-3
     assert sum(r[0]["retries"] for r in g[0]) > 0
     assert g[2] <= 2 + 2 and h[2] >= 3 * 70
+
+
+def test_batch_graph_survives_instance_changes(cuda_lib):
+    """Instances leaving and joining rewrite the batch's device records in
+    place: the step graph is captured once, and the results equal the
+    host-driven loop's for the same sequence of changes."""
+    from mantlepar_b200.batch import Batch
+    from mantlepar_b200.transport import TransportConfig
+    cfg = TransportConfig(cfl=0.4, integrator=3)
+    out = []
+    for dev in (True, False):
+        b = Batch(WORKLOADS[:3], cfg)
+        b.set_device_steps(dev)
+        for i, w in enumerate(WORKLOADS[:3]):
+            b.set_face_velocity(i, *sy.face_velocity(w))
+            b.set_state(i, *sy.initial_state(w))
+        r1 = b.step(5)
+        b.remove(1)
+        k = b.add(WORKLOADS[3])
+        b.set_face_velocity(k, *sy.face_velocity(WORKLOADS[3]))
+        b.set_state(k, *sy.initial_state(WORKLOADS[3]))
+        r2 = b.step(5)
+        b.remove(0)
+        r3 = b.step(3)
+        states = [b.get_state(i) for i in (1, 2)]
+        out.append((r1, r2, r3, states, b.graph_captures()))
+        b.close()
+    assert out[0][:3] == out[1][:3]
+    for a, c in zip(out[0][3], out[1][3]):
+        for key in ("H", "C", "T", "phi"):
+            assert np.array_equal(a[key], c[key])
+    assert out[0][4] == 1 and out[1][4] == 0
