@@ -433,13 +433,53 @@ struct SideLine {
     double h0, h1, h2, c0, c1, c2;
 };
 
-template <class R>
+// Where an edge's cells' records, means and flags come from: global memory
+// (RecGlobal), or a shared-memory tile of the face-tile kernel (RecTile).
+struct RecGlobal {
+    template <class R>
+    __device__ __forceinline__ void load(const FaceArgs<R>& a, size_t N, long long cell, double* DH, double* DC,
+                                         double& mH, double& mC) const {
+        load_rec(a.rec, N, cell, DH, DC);
+        mH = __ldg(a.H + cell);
+        mC = __ldg(a.C + cell);
+    }
+    template <class R>
+    __device__ __forceinline__ unsigned char flags(const FaceArgs<R>& a, long long cell) const { return a.flags[cell]; }
+};
+
+// A shared-memory tile of TW x TH cells whose corner is global cell (i0, j0):
+// records [m][r][c], means [field][r][c] and flags [r][c].
+template <int TW, int TH>
+struct RecTile {
+    const double* rec;
+    const double* mean;
+    const unsigned char* fl;
+    int i0, j0, nx;
+    __device__ __forceinline__ int slot(long long cell) const {
+        const int ci = (int)(cell % nx), cj = (int)(cell / nx);
+        return (cj - j0) * TW + (ci - i0);
+    }
+    template <class R>
+    __device__ __forceinline__ void load(const FaceArgs<R>&, size_t, long long cell, double* DH, double* DC,
+                                         double& mH, double& mC) const {
+        const int k = slot(cell);
+#pragma unroll
+        for (int m = 0; m < 9; ++m) {
+            DH[m] = rec[m * TW * TH + k];
+            DC[m] = rec[(m + 9) * TW * TH + k];
+        }
+        mH = mean[k];
+        mC = mean[TW * TH + k];
+    }
+    template <class R>
+    __device__ __forceinline__ unsigned char flags(const FaceArgs<R>&, long long cell) const { return fl[slot(cell)]; }
+};
+
+template <class R, class Src>
 __device__ __forceinline__ void side_line(const FaceArgs<R>& a, size_t N, long long cell, bool row, double fixed,
-                                          SideLine& s) {
+                                          SideLine& s, const Src& src) {
     double DH[9], DC[9];
-    load_rec(a.rec, N, cell, DH, DC);
-    s.mH = __ldg(a.H + cell);
-    s.mC = __ldg(a.C + cell);
+    src.load(a, N, cell, DH, DC, s.mH, s.mC);
     if (row) { q2_row(DH, fixed, s.h0, s.h1, s.h2); q2_row(DC, fixed, s.c0, s.c1, s.c2); }
     else { q2_col(DH, fixed, s.h0, s.h1, s.h2); q2_col(DC, fixed, s.c0, s.c1, s.c2); }
 }
@@ -521,9 +561,11 @@ __device__ __forceinline__ PointFlux face_point(const Physics& ph, const PhaseLe
     return PointFlux{fh, fc, vn, (aC + aH + 2.0 * fabs(vs)) * sens};
 }
 
-// kExt: the lithostatic pressure is compiled in.
-template <class R, bool kExt = false>
-__device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& ph, long long e) {
+// kExt: the lithostatic pressure is compiled in. Src: where the records of
+// the edge's cells are read (RecGlobal or a shared-memory RecTile).
+template <class R, bool kExt = false, class Src = RecGlobal>
+__device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& ph, long long e,
+                                          const Src& src = Src{}) {
     const int nx = a.nx, ny = a.ny;
     const long long nI = (long long)nx * (ny + 1);
     const long long nE = nI + (long long)(nx + 1) * ny;
@@ -565,9 +607,9 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
     MP_CHECK_INDEX(a.status, L, N);
     if (!boundary) MP_CHECK_INDEX(a.status, Rc, N);
     SideLine sl, sr;
-    side_line(a, N, L, horizontal, lfix, sl);
-    if (!boundary) side_line(a, N, Rc, horizontal, rfix, sr);
-    const bool wetL = (a.flags[L] & FLAG_WET) != 0, wetR = boundary ? true : (a.flags[Rc] & FLAG_WET) != 0;
+    side_line(a, N, L, horizontal, lfix, sl, src);
+    if (!boundary) side_line(a, N, Rc, horizontal, rfix, sr, src);
+    const bool wetL = (src.flags(a, L) & FLAG_WET) != 0, wetR = boundary ? true : (src.flags(a, Rc) & FLAG_WET) != 0;
     const double sgn = reverse ? -1.0 : 1.0;
     const double LD = ph.k.LD;
     double fluxH = 0.0, fluxC = 0.0, fluxMix = 0.0, rate = 0.0;
