@@ -5,8 +5,9 @@ per-cell relative error of a state field is |x - ref| / max(|ref|, 1e-3 *
 max|ref|) and the FP64 bar is 1e-12 per cell for one stage and for short
 runs. Stage right-hand sides are sums of face fluxes of both signs, so their
 error is measured against their infinity norm (same 1e-12 bar). Over 200
-steps the FP64 (GPU) and 80-bit (reference) roundings drift apart slowly;
-that bound (1e-10) is stated in the test.
+steps the FP64 (GPU) and 80-bit (reference) roundings drift apart slowly
+(measured: phi 4.3e-13 per cell after 200 SSPRK2 steps, 2.4e-13 after 200
+SSPRK3 steps); the runs are deterministic, and the same 1e-12 bar holds.
 """
 import os
 
@@ -22,7 +23,7 @@ CASES = {"w20": sy.Workload(nx=20, ny=20), "w2x2": sy.Workload(nx=2, ny=2),
          "w3x5": sy.Workload(nx=3, ny=5, seed=7), "w7x4": sy.Workload(nx=7, ny=4, seed=9, noise_H=0.1)}
 RTOL_STAGE = 1e-12
 RTOL_RUN10 = 1e-12
-RTOL_RUN200 = 1e-10
+RTOL_RUN200 = 1e-12
 
 
 def rel(a, b):
