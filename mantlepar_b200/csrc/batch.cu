@@ -71,11 +71,8 @@ struct Tuning { int bx = 32, by = 4, cpt = 1; };
 
 // ------------------------------------------------------------ batched kernels
 
-#ifndef MP_RECON_BLOCKS
-#define MP_RECON_BLOCKS 4   // register cap of the reconstruction kernel (see transport.cu)
-#endif
 template <class R>
-__global__ void __launch_bounds__(128, MP_RECON_BLOCKS) batch_recon_kernel(const InstArgs<R>* args, const Work* work, const int* active,
+__global__ void __launch_bounds__(128) batch_recon_kernel(const InstArgs<R>* args, const Work* work, const int* active,
                                                           Physics ph, int cpt) {
     const Work w = work[blockIdx.x];
     if (!active[w.inst]) return;

@@ -235,17 +235,14 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
     const long long key = cell + (long long)a.gj0 * nx;
     int st_lim = 0;
 
-    // One field at a time -- gather, reconstruct, limiter scan, theta, write
-    // its 9 record entries -- so only one deviation polynomial is live.
-    const int cls = cj * 3 + ci;
-    const int l0 = t.line_off[cls], l1 = t.line_off[cls + 1];
-    double mH = 0.0, mC = 0.0, hiH = 0.0, hiC = 0.0;
+    double u[3][3];
+    double DH[9], DC[9];
+    double mH, mC, loH, hiH, loC, hiC;
     int st = 0;
-    bool bad = false;
-#pragma unroll 1
+    // Enthalpy, then composition: one 3x3 gather at a time keeps registers low.
+#pragma unroll
     for (int f = 0; f < 2; ++f) {
         const double* F = f ? a.C : a.H;
-        double u[3][3];
 #pragma unroll
         for (int dj = 0; dj < 3; ++dj)
 #pragma unroll
@@ -261,24 +258,30 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
         for (int dj = 0; dj < 3; ++dj)
 #pragma unroll
             for (int di = 0; di < 3; ++di) { lo = fmin(lo, u[dj][di]); hi = fmax(hi, u[dj][di]); }
-        const double m = u[1][1];
-        lo = fmax(0.0, lo);
-        if (f) hi = fmin(ph.k.Xe, hi);
-        double D[9];
-        const int s1 = reconstruct(t, ci, cj, u, D);
-        st = st ? st : s1;
-        // Limiter over the class's points, evaluated line by line.
-        double dmx, dmn;
-        scan_lines<R>(t, a.tab, l0, l1, D, dmx, dmn, bad);
-        const double th = theta_of(m, lo, hi, dmx, dmn);
-        if (a.theta) a.theta[(size_t)f * N + cell] = th;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) a.rec[(size_t)(k + 9 * f) * N + cell] = D[k] * th;
-        if (f) { mC = m; hiC = hi; } else { mH = m; hiH = hi; }
+        if (f == 0) {
+            mH = u[1][1]; loH = fmax(0.0, lo); hiH = hi;
+            const int s1 = reconstruct(t, ci, cj, u, DH);
+            st = st ? st : s1;
+        } else {
+            mC = u[1][1]; loC = fmax(0.0, lo); hiC = fmin(ph.k.Xe, hi);
+            const int s1 = reconstruct(t, ci, cj, u, DC);
+            st = st ? st : s1;
+        }
     }
     // state_reconstruction.cpp:187-188: admissible means.
     if (!(isfinite(mH) && mH >= 0.0 && isfinite(mC) && mC >= 0.0 && mC <= ph.k.Xe)) st_lim = E_OUTOFRANGE;
+
+    // Limiter over the class's points, evaluated line by line.
+    const int cls = cj * 3 + ci;
+    const int l0 = t.line_off[cls], l1 = t.line_off[cls + 1];
+    double hmx, hmn, cmx, cmn;
+    bool bad = false;
+    scan_lines<R>(t, a.tab, l0, l1, DH, hmx, hmn, bad);
+    scan_lines<R>(t, a.tab, l0, l1, DC, cmx, cmn, bad);
     if (bad) st_lim = st_lim ? st_lim : E_FP;
+    const double thH = theta_of(mH, loH, hiH, hmx, hmn);
+    const double thC = theta_of(mC, loC, hiC, cmx, cmn);
+    if (a.theta) { a.theta[cell] = thH; a.theta[N + cell] = thC; }
     // Diffusion samples (zero diffusivity: kept for their admissibility
     // check). Limited values at limiter points stay in [lo, hi], so the
     // samples are admissible when hi_H is below the liquidus at hi_C and
@@ -287,6 +290,11 @@ __device__ __forceinline__ void recon_cell(const ReconArgs<R>& a, const Physics&
     const double tep = ph.litho ? fmin(tep_at(ph, t.y0 + gj * t.dy), tep_at(ph, t.y0 + (gj + 1) * t.dy)) : ph.Tep;
     const double Hliq = tep + (1.0 - hiC / ph.k.Xe) + ph.k.LD;
     const bool safe = tep >= 0.0 && hiH + 1e-12 * (1.0 + fabs(hiH)) < Hliq;
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+        a.rec[(size_t)m * N + cell] = DH[m] * thH;
+        a.rec[(size_t)(m + 9) * N + cell] = DC[m] * thC;
+    }
     a.flags[cell] = safe ? 0 : FLAG_CHECK;
     if (st) record_error(a.status, PART_UPDATE, key, st);
     if (st_lim) record_error(a.status, PART_LIMIT, key, st_lim);
@@ -433,53 +441,13 @@ struct SideLine {
     double h0, h1, h2, c0, c1, c2;
 };
 
-// Where an edge's cells' records, means and flags come from: global memory
-// (RecGlobal), or a shared-memory tile of the face-tile kernel (RecTile).
-struct RecGlobal {
-    template <class R>
-    __device__ __forceinline__ void load(const FaceArgs<R>& a, size_t N, long long cell, double* DH, double* DC,
-                                         double& mH, double& mC) const {
-        load_rec(a.rec, N, cell, DH, DC);
-        mH = __ldg(a.H + cell);
-        mC = __ldg(a.C + cell);
-    }
-    template <class R>
-    __device__ __forceinline__ unsigned char flags(const FaceArgs<R>& a, long long cell) const { return a.flags[cell]; }
-};
-
-// A shared-memory tile of TW x TH cells whose corner is global cell (i0, j0):
-// records [m][r][c], means [field][r][c] and flags [r][c].
-template <int TW, int TH>
-struct RecTile {
-    const double* rec;
-    const double* mean;
-    const unsigned char* fl;
-    int i0, j0, nx;
-    __device__ __forceinline__ int slot(long long cell) const {
-        const int ci = (int)(cell % nx), cj = (int)(cell / nx);
-        return (cj - j0) * TW + (ci - i0);
-    }
-    template <class R>
-    __device__ __forceinline__ void load(const FaceArgs<R>&, size_t, long long cell, double* DH, double* DC,
-                                         double& mH, double& mC) const {
-        const int k = slot(cell);
-#pragma unroll
-        for (int m = 0; m < 9; ++m) {
-            DH[m] = rec[m * TW * TH + k];
-            DC[m] = rec[(m + 9) * TW * TH + k];
-        }
-        mH = mean[k];
-        mC = mean[TW * TH + k];
-    }
-    template <class R>
-    __device__ __forceinline__ unsigned char flags(const FaceArgs<R>&, long long cell) const { return fl[slot(cell)]; }
-};
-
-template <class R, class Src>
+template <class R>
 __device__ __forceinline__ void side_line(const FaceArgs<R>& a, size_t N, long long cell, bool row, double fixed,
-                                          SideLine& s, const Src& src) {
+                                          SideLine& s) {
     double DH[9], DC[9];
-    src.load(a, N, cell, DH, DC, s.mH, s.mC);
+    load_rec(a.rec, N, cell, DH, DC);
+    s.mH = __ldg(a.H + cell);
+    s.mC = __ldg(a.C + cell);
     if (row) { q2_row(DH, fixed, s.h0, s.h1, s.h2); q2_row(DC, fixed, s.c0, s.c1, s.c2); }
     else { q2_col(DH, fixed, s.h0, s.h1, s.h2); q2_col(DC, fixed, s.c0, s.c1, s.c2); }
 }
@@ -561,11 +529,9 @@ __device__ __forceinline__ PointFlux face_point(const Physics& ph, const PhaseLe
     return PointFlux{fh, fc, vn, (aC + aH + 2.0 * fabs(vs)) * sens};
 }
 
-// kExt: the lithostatic pressure is compiled in. Src: where the records of
-// the edge's cells are read (RecGlobal or a shared-memory RecTile).
-template <class R, bool kExt = false, class Src = RecGlobal>
-__device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& ph, long long e,
-                                          const Src& src = Src{}) {
+// kExt: the lithostatic pressure is compiled in.
+template <class R, bool kExt = false>
+__device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& ph, long long e) {
     const int nx = a.nx, ny = a.ny;
     const long long nI = (long long)nx * (ny + 1);
     const long long nE = nI + (long long)(nx + 1) * ny;
@@ -607,9 +573,9 @@ __device__ __forceinline__ void face_edge(const FaceArgs<R>& a, const Physics& p
     MP_CHECK_INDEX(a.status, L, N);
     if (!boundary) MP_CHECK_INDEX(a.status, Rc, N);
     SideLine sl, sr;
-    side_line(a, N, L, horizontal, lfix, sl, src);
-    if (!boundary) side_line(a, N, Rc, horizontal, rfix, sr, src);
-    const bool wetL = (src.flags(a, L) & FLAG_WET) != 0, wetR = boundary ? true : (src.flags(a, Rc) & FLAG_WET) != 0;
+    side_line(a, N, L, horizontal, lfix, sl);
+    if (!boundary) side_line(a, N, Rc, horizontal, rfix, sr);
+    const bool wetL = (a.flags[L] & FLAG_WET) != 0, wetR = boundary ? true : (a.flags[Rc] & FLAG_WET) != 0;
     const double sgn = reverse ? -1.0 : 1.0;
     const double LD = ph.k.LD;
     double fluxH = 0.0, fluxC = 0.0, fluxMix = 0.0, rate = 0.0;

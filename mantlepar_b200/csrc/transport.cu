@@ -64,16 +64,8 @@ struct SourceBufs {
 // blocks per SM (register caps) as measured fastest on B200: cell phase 8,
 // faces 5; the reconstruction keeps its natural register count.
 // Rows [jlo, jhi) are reconstructed (all rows, or a slab's owned rows +- 1).
-// Minimum resident 128-thread blocks per SM of the reconstruction kernels
-// (a register cap). Measured at 1280x2560 (CUDA events per stage): 4 blocks
-// (the kernel's natural 108 registers) 0.576 ms; 5, 6, 7, 8 blocks (96, 80,
-// 72, 64 registers) 0.615, 0.627, 0.631, 0.631 ms -- more resident warps do
-// not pay for the tighter allocation.
-#ifndef MP_RECON_BLOCKS
-#define MP_RECON_BLOCKS 4
-#endif
 template <class R>
-__global__ void __launch_bounds__(128, MP_RECON_BLOCKS) recon_kernel(ReconArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
+__global__ void __launch_bounds__(128) recon_kernel(ReconArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
                                                     int jlo, int jhi) {
     if (gated_off(a.gate)) return;
     ReconArgs<R> b = a;
@@ -108,53 +100,6 @@ __global__ void __launch_bounds__(128, 5) face_kernel(FaceArgs<R> a, Physics ph,
         face_edge<R, kExt>(b, ph, k);
     }
 }
-// Faces of a whole uniform mesh by 32x4-cell tiles: the block stages the
-// records, means and flags of its cells and of a one-cell halo (the column to
-// the left, the row below) in shared memory, then every thread evaluates the
-// edges its cell owns -- bottom and left, and the top or right wall edge of
-// the last row or column -- with face_edge reading the tile. Each record is
-// read from global memory about once (1.3 times with the halo) instead of
-// once per edge side; the per-edge arithmetic is face_edge's.
-constexpr int kFaceTX = 32, kFaceTY = 4, kFaceTW = kFaceTX + 1, kFaceTH = kFaceTY + 1;
-template <class R, bool kExt>
-__global__ void __launch_bounds__(kFaceTX * kFaceTY, 5) face_tile_kernel(FaceArgs<R> a, Physics ph,
-                                                                         const __grid_constant__ ParamTables p) {
-    if (gated_off(a.gate)) return;
-    FaceArgs<R> b = a;
-    b.tab = param_tab<R>(p);
-    __shared__ double s_rec[kRec * kFaceTH * kFaceTW];
-    __shared__ double s_mean[2 * kFaceTH * kFaceTW];
-    __shared__ unsigned char s_fl[kFaceTH * kFaceTW];
-    const int nx = a.nx, ny = a.ny;
-    const size_t N = (size_t)nx * ny;
-    const int i0 = (int)blockIdx.x * kFaceTX - 1, j0 = (int)blockIdx.y * kFaceTY - 1;
-    const int tid = threadIdx.y * kFaceTX + threadIdx.x;
-    for (int k = tid; k < kFaceTH * kFaceTW; k += kFaceTX * kFaceTY) {
-        const int gi = i0 + k % kFaceTW, gj = j0 + k / kFaceTW;
-        if (gi < 0 || gi >= nx || gj < 0 || gj >= ny) continue;
-        const size_t cell = (size_t)gj * nx + gi;
-#pragma unroll
-        for (int m = 0; m < kRec; ++m) s_rec[m * kFaceTH * kFaceTW + k] = __ldg(a.rec + m * N + cell);
-        s_mean[k] = __ldg(a.H + cell);
-        s_mean[kFaceTH * kFaceTW + k] = __ldg(a.C + cell);
-        s_fl[k] = a.flags[cell];
-    }
-    __syncthreads();
-    const int i = (int)blockIdx.x * kFaceTX + threadIdx.x, j = (int)blockIdx.y * kFaceTY + threadIdx.y;
-    if (i >= nx || j >= ny) return;
-    const RecTile<kFaceTW, kFaceTH> src{s_rec, s_mean, s_fl, i0, j0, nx};
-    const long long nI = (long long)nx * (ny + 1);
-    const int owned = 2 + (j == ny - 1 ? 1 : 0) + (i == nx - 1 ? 1 : 0);
-    for (int k = 0; k < owned; ++k) {
-        long long e;
-        if (k == 0) e = (long long)j * nx + i;                                          // bottom
-        else if (k == 1) e = nI + (long long)j * (nx + 1) + i;                          // left
-        else if (k == 2 && j == ny - 1) e = (long long)ny * nx + i;                     // top wall
-        else e = nI + (long long)j * (nx + 1) + nx;                                     // right wall
-        face_edge<R, kExt>(b, ph, e, src);
-    }
-}
-
 // The diffusive part of the same edges (only launched when diffusion is on).
 template <class R>
 __global__ void __launch_bounds__(128) diffusion_kernel(FaceArgs<R> a, Physics ph, const __grid_constant__ ParamTables p,
@@ -391,9 +336,8 @@ void launch_stage_kernels(int nx, int ny, const StageRange& rg, const ParamTable
             if (ph.litho) run(2, [&] { face_kernel<R, true, true><<<g, 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
             else run(2, [&] { face_kernel<R, false, true><<<g, 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
         } else {
-            const dim3 tb(kFaceTX, kFaceTY), tg((nx + kFaceTX - 1) / kFaceTX, (ny + kFaceTY - 1) / kFaceTY);
-            if (ph.litho) run(2, [&] { face_tile_kernel<R, true><<<tg, tb, 0, s>>>(a, ph, pt); });
-            else run(2, [&] { face_tile_kernel<R, false><<<tg, tb, 0, s>>>(a, ph, pt); });
+            if (ph.litho) run(2, [&] { face_kernel<R, true, false><<<g, 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
+            else run(2, [&] { face_kernel<R, false, false><<<g, 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
         }
         if (ph.diffusion)
             run(2, [&] { diffusion_kernel<R><<<(unsigned)((nh + nv + 127) / 128), 128, 0, s>>>(a, ph, pt, h0, nh, v0, nv); });
