@@ -18,6 +18,13 @@
 namespace {
 
 typedef long double ld;
+// Per-cell evaluation type: long double as in the reference; ORC_FP64_CELL
+// evaluates the per-cell steps in double (the derived scales stay long double).
+#ifdef ORC_FP64_CELL
+typedef double lc;
+#else
+typedef long double lc;
+#endif
 
 struct Fail { int code; };
 
@@ -73,8 +80,8 @@ orc_derived derive_or_throw(const orc_material& p) {
 double shifted_temperature(const orc_material& p, const orc_derived& d, double TD, double P) {
     finite_or_throw(TD);
     finite_or_throw(P);
-    const ld shift = (ld)P / p.nu / d.dT;
-    return to_double_checked((ld)TD + shift);
+    const lc shift = (lc)P / p.nu / d.dT;
+    return to_double_checked((lc)TD + shift);
 }
 
 // eutectic_rescaled.cpp:163-185
@@ -83,11 +90,11 @@ orc_bounds bounds_or_throw(const orc_material& p, const orc_derived& d, double C
     if (C < 0.0 || C > p.Xe) throw Fail{ORC_INVALID};
     orc_bounds b{};
     b.Tep = shifted_temperature(p, d, d.TDe0, P);
-    b.Tmp = to_double_checked((ld)b.Tep + 1.0L);
-    const ld r = (ld)C / p.Xe;
-    b.H_eutectic_end = to_double_checked((ld)b.Tep + d.LD * r);
-    b.H_liquidus = to_double_checked((ld)b.Tep + (1.0L - r) + d.LD);
-    if (C == 0.0) b.H_liquidus = to_double_checked((ld)b.Tmp + d.LD);
+    b.Tmp = to_double_checked((lc)b.Tep + 1.0L);
+    const lc r = (lc)C / p.Xe;
+    b.H_eutectic_end = to_double_checked((lc)b.Tep + d.LD * r);
+    b.H_liquidus = to_double_checked((lc)b.Tep + (1.0L - r) + d.LD);
+    if (C == 0.0) b.H_liquidus = to_double_checked((lc)b.Tmp + d.LD);
     if (b.Tmp <= b.Tep || b.H_liquidus <= b.Tep || (C == 0.0 && b.H_liquidus <= b.Tmp))
         throw Fail{ORC_OVERFLOW};
     return b;
@@ -107,23 +114,23 @@ int region_of(double H, double C, const orc_bounds& b) {
 }
 
 // eutectic_rescaled.cpp:108-114
-double clip_fraction(ld v) {
-    const ld tol = 64.0L * std::numeric_limits<double>::epsilon();
+double clip_fraction(lc v) {
+    const lc tol = 64.0L * std::numeric_limits<double>::epsilon();
     if (!std::isfinite(v) || v < -tol || v > 1.0L + tol) throw Fail{ORC_RUNTIME};
-    return (double)std::min(std::max(v, 0.0L), 1.0L);
+    return (double)std::min(std::max(v, (lc)0), (lc)1);
 }
 
 // eutectic_rescaled.cpp:116-121
-double minus_magnitude(ld m) {
-    if (m > (ld)std::numeric_limits<double>::max()) return -std::numeric_limits<double>::infinity();
+double minus_magnitude(lc m) {
+    if (m > (lc)std::numeric_limits<double>::max()) return -std::numeric_limits<double>::infinity();
     return -(double)m;
 }
 
 orc_phase evaluate_or_throw(const orc_material& p, const orc_derived& d, double H, double C, double P) {
     finite_or_throw(H);
     const orc_bounds b = bounds_or_throw(p, d, C, P);
-    const ld LD = d.LD;
-    const ld Xe = p.Xe;
+    const lc LD = d.LD;
+    const lc Xe = p.Xe;
     orc_phase s{};
     s.region = region_of(H, C, b);
     s.Tep = b.Tep;
@@ -132,7 +139,7 @@ orc_phase evaluate_or_throw(const orc_material& p, const orc_derived& d, double 
         s.phi1 = 1.0; s.TDp = H; s.dTD_dHD = 1.0;
         break;
     case 6:
-        s.phil = clip_fraction(((ld)H - b.Tmp) / LD);
+        s.phil = clip_fraction(((lc)H - b.Tmp) / LD);
         s.phi1 = 1.0 - s.phil;
         s.TDp = b.Tmp;
         break;
@@ -140,9 +147,9 @@ orc_phase evaluate_or_throw(const orc_material& p, const orc_derived& d, double 
         s.phi1 = 1.0 - C; s.phi2 = C; s.TDp = H; s.dTD_dHD = 1.0;
         break;
     case 3: {
-        const ld cap = (ld)C / Xe;
-        const ld melt = (H == b.H_eutectic_end) ? cap : std::min(cap, ((ld)H - b.Tep) / LD);
-        const ld second = std::max(0.0L, (ld)C - melt * Xe);
+        const lc cap = (lc)C / Xe;
+        const lc melt = (H == b.H_eutectic_end) ? cap : std::min(cap, ((lc)H - b.Tep) / LD);
+        const lc second = std::max((lc)0, (lc)C - melt * Xe);
         s.phil = clip_fraction(melt);
         s.phi2 = clip_fraction(second);
         s.phi1 = clip_fraction(1.0L - melt - second);
@@ -152,14 +159,14 @@ orc_phase evaluate_or_throw(const orc_material& p, const orc_derived& d, double 
     }
     case 4: {
         // LD*phi^2 - (H - Tmp)*phi - C/Xe = 0, cancellation-free root choice.
-        const ld a = (ld)H - b.Tmp;
-        const ld r = (ld)C / Xe;
-        const ld disc = std::hypot(a, 2.0L * std::sqrt(LD) * std::sqrt(r));
-        const ld melt = a >= 0.0L ? (a + disc) / (2.0L * LD) : 2.0L * r / (disc - a);
+        const lc a = (lc)H - b.Tmp;
+        const lc r = (lc)C / Xe;
+        const lc disc = std::hypot(a, 2.0L * std::sqrt(LD) * std::sqrt(r));
+        const lc melt = a >= 0.0L ? (a + disc) / (2.0L * LD) : 2.0L * r / (disc - a);
         s.phil = clip_fraction(melt);
         s.phi1 = clip_fraction(1.0L - melt);
-        s.cl = clip_fraction((ld)C / melt);
-        s.TDp = to_double_checked(a >= 0.0L ? (ld)b.Tmp - r / melt : (ld)H - LD * melt);
+        s.cl = clip_fraction((lc)C / melt);
+        s.TDp = to_double_checked(a >= 0.0L ? (lc)b.Tmp - r / melt : (lc)H - LD * melt);
         s.dTD_dHD = clip_fraction(a >= 0.0L ? 2.0L * (LD / disc) * (r / (disc + a))
                                             : 0.5L * (1.0L - a / disc));
         s.dTD_dCD = minus_magnitude((LD / disc) / Xe);
@@ -167,12 +174,12 @@ orc_phase evaluate_or_throw(const orc_material& p, const orc_derived& d, double 
     }
     case 5:
         s.phil = 1.0; s.cl = C;
-        s.TDp = to_double_checked((ld)H - LD);
+        s.TDp = to_double_checked((lc)H - LD);
         s.dTD_dHD = 1.0;
         break;
     }
     if (C == 0.0 && H > b.Tep && s.region != 5) {
-        const ld gap = std::fabs((ld)H - b.Tmp);
+        const lc gap = std::fabs((lc)H - b.Tmp);
         s.dTD_dCD = gap == 0.0L ? -std::numeric_limits<double>::infinity()
                                 : minus_magnitude((LD / gap) / Xe);
     }

@@ -14,6 +14,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
+FP64_PATH = os.path.join(HERE, "liboracle_fp64.so")
 REF_PATH = os.path.join(HERE, "_ref", "libmpref.so")
 
 PHASE_FIELDS = ["phi1", "phi2", "phil", "cl", "cs", "region", "TDp", "Tep",
@@ -132,6 +133,17 @@ def restated() -> "_Lib":
             raise RuntimeError(f"oracle library missing: {LIB_PATH} (run make -C oracle)")
         _LIBS["orc"] = _Lib(LIB_PATH, "orc")
     return _LIBS["orc"]
+
+
+def restated_fp64() -> "_Lib":
+    """The restatement with its per-cell and per-face steps in double instead
+    of the reference's long double: the distance between its results and
+    restated()'s is the results' own sensitivity to intermediate precision."""
+    if "orc64" not in _LIBS:
+        if not os.path.exists(FP64_PATH):
+            raise RuntimeError(f"oracle library missing: {FP64_PATH} (run make -C oracle)")
+        _LIBS["orc64"] = _Lib(FP64_PATH, "orc")
+    return _LIBS["orc64"]
 
 
 def reference_available() -> bool:

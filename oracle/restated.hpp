@@ -29,6 +29,15 @@
 namespace orc {
 
 typedef long double ld;
+// Per-cell and per-face evaluation type. The reference evaluates these steps
+// in long double (80-bit on x86-64); building with ORC_FP64_CELL evaluates
+// the same steps in double, which measures how far the results move with the
+// precision of the intermediates alone (tables and geometry stay long double).
+#ifdef ORC_FP64_CELL
+typedef double lc;
+#else
+typedef long double lc;
+#endif
 
 struct Pt { double x = 0, y = 0; };
 typedef std::array<Pt, 4> Quad;
@@ -267,19 +276,19 @@ struct StencilPoly {
 
     // tensorstencilpoly.cpp:400-459 (value only)
     static double apply_smoothness(const std::vector<double>& m, const double* avg, int n) {
-        ld diff[16];
-        for (int i = 0; i < n; ++i) diff[i] = (ld)avg[i] - avg[0];
-        ld sum = 0, mag = 0;
+        lc diff[16];
+        for (int i = 0; i < n; ++i) diff[i] = (lc)avg[i] - avg[0];
+        lc sum = 0, mag = 0;
         for (int r = 0; r < n; ++r)
             for (int c = 0; c < n; ++c) {
-                const ld term = diff[r] * m[(size_t)r * n + c] * diff[c];
+                const lc term = diff[r] * m[(size_t)r * n + c] * diff[c];
                 sum += term;
                 mag += std::fabs(term);
             }
         require(std::isfinite(sum) && std::isfinite(mag), E_FP, "Smoothness evaluation overflowed");
-        const ld tol = 64 * (ld)std::numeric_limits<double>::epsilon() * mag;
+        const lc tol = 64 * (lc)std::numeric_limits<double>::epsilon() * mag;
         require(sum >= -tol, E_FP, "Smoothness quadratic form is negative beyond roundoff");
-        return (double)std::max(0.0L, sum);
+        return (double)std::max((lc)0, sum);
     }
 
     // tensorstencilpoly.cpp:293-316 + :247-270 (value, dx=dy=0)
@@ -319,10 +328,10 @@ struct CandidateSet {
 inline int eta_of(int r) { return r == 1 ? 1 : (r == 2 ? 3 : 4); }
 
 // log(sigma + eps*A) without forming eps*A (reconstruction.cpp:46-54).
-inline ld log_denominator(double sigma, ld logReg) {
+inline lc log_denominator(double sigma, lc logReg) {
     if (sigma == 0) return logReg;
-    const ld ls = std::log((ld)sigma);
-    const ld hi = std::max(ls, logReg), lo = std::min(ls, logReg);
+    const lc ls = std::log((lc)sigma);
+    const lc hi = std::max(ls, logReg), lo = std::min(ls, logReg);
     return hi + std::log1p(std::exp(lo - hi));
 }
 
@@ -348,18 +357,18 @@ struct Recon {
         }
         const double eps = 1e-2;
         const int s = 1;
-        ld logA[6];
-        const ld logReg = std::log((ld)eps) + std::log((ld)area);
+        lc logA[6];
+        const lc logReg = std::log((lc)eps) + std::log((lc)area);
         for (size_t k = 0; k < nc; ++k) {
             const int r = set->cand[k].order + 1;
-            const ld ex = (ld)s * r + eta_of(r);
-            logA[k] = std::log((ld)set->cand[k].linear) - ex * log_denominator(sig[k], logReg);
+            const lc ex = (lc)s * r + eta_of(r);
+            logA[k] = std::log((lc)set->cand[k].linear) - ex * log_denominator(sig[k], logReg);
             require(std::isfinite(logA[k]), E_FP, "Polynomial log weight is not finite");
         }
-        logA[nc] = -std::numeric_limits<ld>::infinity();  // constant candidate disabled
-        ld mx = logA[0];
+        logA[nc] = -std::numeric_limits<lc>::infinity();  // constant candidate disabled
+        lc mx = logA[0];
         for (size_t k = 1; k <= nc; ++k) mx = std::max(mx, logA[k]);
-        ld sum = 0;
+        lc sum = 0;
         for (size_t k = 0; k <= nc; ++k) { logA[k] = std::exp(logA[k] - mx); sum += logA[k]; }
         require(std::isfinite(sum) && sum > 0, E_FP, "Invalid ML-WENO weight normalization");
         for (size_t k = 0; k < nc; ++k) w[k] = (double)(logA[k] / sum);
@@ -367,10 +376,10 @@ struct Recon {
 
     // reconstruction.cpp:477-502
     double evaluate(Pt p) const {
-        ld result = target;
+        lc result = target;
         for (size_t k = 0; k < set->cand.size(); ++k) {
             if (w[k] == 0) continue;
-            result += (ld)w[k] * set->cand[k].poly.evaluate(centered[k], p);
+            result += (lc)w[k] * set->cand[k].poly.evaluate(centered[k], p);
         }
         require(std::isfinite(result), E_FP, "Reconstructed value is not representable");
         return (double)result;
@@ -463,14 +472,14 @@ struct ThermalBC { int type = 0; double value = 0; };
 inline void integrate_diffusion(const Sampling& s, const std::vector<double>& samples, double kappa,
                                 const ThermalBC* bc, double& flux, std::vector<double>& deriv) {
     const size_t nq = s.points.size(), count = s.coefficients.size();
-    auto real = [](ld v) {
-        require(std::isfinite(v) && std::fabs(v) <= (ld)std::numeric_limits<double>::max(), E_FP,
+    auto real = [](lc v) {
+        require(std::isfinite(v) && std::fabs(v) <= (lc)std::numeric_limits<double>::max(), E_FP,
                 "Diffusion geometry, flux or derivative is not representable");
         return (double)v;
     };
-    ld last_coef = 0;
+    lc last_coef = 0;
     for (size_t k = 0; k + 1 < count; ++k) last_coef -= s.coefficients[k];
-    ld integral = 0;
+    lc integral = 0;
     deriv.assign(samples.size(), 0.0);
     std::vector<double> v(count);
     for (size_t q = 0; q < nq; ++q) {
@@ -479,7 +488,7 @@ inline void integrate_diffusion(const Sampling& s, const std::vector<double>& sa
         if (bc) {
             if (type == 0) continue;
             require(std::isfinite(bc->value), E_OUTOFRANGE, "Boundary data must be finite");
-            if (type == 2) { integral += (ld)weight * bc->value; continue; }
+            if (type == 2) { integral += (lc)weight * bc->value; continue; }
         }
         require(std::isfinite(kappa) && kappa >= 0, E_OUTOFRANGE, "Diffusivity must be finite and nonnegative");
         for (size_t k = 0; k < count; ++k) {
@@ -488,14 +497,14 @@ inline void integrate_diffusion(const Sampling& s, const std::vector<double>& sa
             require(std::isfinite(u), E_OUTOFRANGE, "Diffusion sample state must be finite");
             v[k] = u;
         }
-        ld gradient = 0;
-        for (size_t k = 0; k + 1 < count; ++k) gradient += (ld)s.coefficients[k] * ((ld)v[k] - v.back());
+        lc gradient = 0;
+        for (size_t k = 0; k + 1 < count; ++k) gradient += (lc)s.coefficients[k] * ((lc)v[k] - v.back());
         gradient /= s.spacing[q];
         require(std::isfinite(gradient), E_FP, "Sampled normal derivative overflowed");
-        integral -= (ld)weight * kappa * gradient;
-        const ld scale = -(ld)weight * kappa / s.spacing[q];
+        integral -= (lc)weight * kappa * gradient;
+        const lc scale = -(lc)weight * kappa / s.spacing[q];
         for (size_t k = 0; k < count; ++k) {
-            const ld coef = k + 1 == count ? last_coef : (ld)s.coefficients[k];
+            const lc coef = k + 1 == count ? last_coef : (lc)s.coefficients[k];
             const double partial = real(scale * coef * 1.0);
             if (!(bc && k + 1 == count)) deriv[q * count + k] = partial;
         }
@@ -543,12 +552,12 @@ inline void build_sampling(Pt a, Pt b, const Quad& left, const Quad* right,
 struct AdvectBC { int type = 1; double value = 0; };
 
 // advectiveflux.cpp:8-18 (RealValue) and :41-48 (NormalVelocity).
-inline double real_value(ld v) {
-    require(std::isfinite(v) && std::fabs(v) <= (ld)std::numeric_limits<double>::max(), E_FP,
+inline double real_value(lc v) {
+    require(std::isfinite(v) && std::fabs(v) <= (lc)std::numeric_limits<double>::max(), E_FP,
             "Advective flux or derivative is not representable");
     return (double)v;
 }
-inline double normal_velocity(Pt v, Pt n) { return real_value((ld)v.x * n.x + (ld)v.y * n.y); }
+inline double normal_velocity(Pt v, Pt n) { return real_value((lc)v.x * n.x + (lc)v.y * n.y); }
 
 // advectiveflux.cpp:20-39 (CheckPoint) for the point fields the flux reads.
 inline void check_point(Pt p, Pt v, Pt n) {
@@ -564,7 +573,7 @@ inline void check_point(Pt p, Pt v, Pt n) {
 inline void linear_flux(double u, Pt v, Pt n, double& value, double& derivative) {
     require(std::isfinite(u), E_OUTOFRANGE, "Advective trace must be finite");
     derivative = normal_velocity(v, n);
-    value = real_value((ld)derivative * u);
+    value = real_value((lc)derivative * u);
 }
 
 // advectiveflux.cpp:82-87 (relative roundoff allowance of a speed bound).
@@ -583,7 +592,7 @@ inline double integrate_advective_flux(Pt a, Pt b, const std::vector<double>& rp
     edge_geometry(a, b, length, normal);
     for (const Pt& v : vel) require(std::isfinite(v.x) && std::isfinite(v.y), E_OUTOFRANGE, "Edge velocity must be finite");
     if (global) require(std::isfinite(global_speed) && global_speed >= 0, E_OUTOFRANGE, "Global LF speed must be finite and nonnegative");
-    ld sum = 0;
+    lc sum = 0;
     for (size_t q = 0; q < rp.size(); ++q) {
         const Pt p = map_edge(rp[q], a, b);
         check_point(p, vel[q], normal);
@@ -593,9 +602,9 @@ inline double integrate_advective_flux(Pt a, Pt b, const std::vector<double>& rp
         const double speed = std::max(std::fabs(dl), std::fabs(dr));
         const double alpha = global ? global_speed : speed;
         require(speed_bounds(alpha, speed), E_OUTOFRANGE, "Supplied global LF speed is smaller than the current local bound");
-        const ld jump = (ld)right[q] - left[q];
-        const double flux = real_value(((ld)fl + fr - (ld)alpha * jump) / 2);
-        const ld weight = (ld)rw[q] * length / 2;
+        const lc jump = (lc)right[q] - left[q];
+        const double flux = real_value(((lc)fl + fr - (lc)alpha * jump) / 2);
+        const lc weight = (lc)rw[q] * length / 2;
         sum += weight * flux;
     }
     return real_value(sum);
@@ -610,7 +619,7 @@ inline double integrate_advective_boundary_flux(Pt a, Pt b, const std::vector<do
     double length; Pt normal;
     edge_geometry(a, b, length, normal);
     for (const Pt& v : vel) require(std::isfinite(v.x) && std::isfinite(v.y), E_OUTOFRANGE, "Edge velocity must be finite");
-    ld sum = 0;
+    lc sum = 0;
     for (size_t q = 0; q < rp.size(); ++q) {
         require(data[q].type >= 0 && data[q].type <= 2, E_WRONG, "Unknown advection boundary policy");
         require(std::isfinite(interior[q]), E_OUTOFRANGE, "Interior boundary trace must be finite");
@@ -620,7 +629,7 @@ inline double integrate_advective_boundary_flux(Pt a, Pt b, const std::vector<do
         const bool outflow = data[q].type == 1;
         double f, d;
         linear_flux(outflow ? interior[q] : data[q].value, vel[q], normal, f, d);
-        const ld weight = (ld)rw[q] * length / 2;
+        const lc weight = (lc)rw[q] * length / 2;
         sum += weight * f;
     }
     return real_value(sum);

@@ -101,8 +101,8 @@ struct Restated {
     // EutecticModel::staticPressure(zD) (eutectic_rescaled.cpp:151-161).
     static double static_pressure(const orc_material& m, const orc_derived& d, double zD) {
         require(std::isfinite(zD), E_PHASE + 1, "zD must be finite");
-        const long double v = (long double)m.rho * m.g * zD * d.l0;
-        require(std::isfinite(v) && std::fabs(v) <= (long double)std::numeric_limits<double>::max(), E_PHASE + 2,
+        const lc v = (lc)m.rho * m.g * zD * d.l0;
+        require(std::isfinite(v) && std::fabs(v) <= (lc)std::numeric_limits<double>::max(), E_PHASE + 2,
                 "static pressure is not representable");
         return (double)v;
     }

