@@ -200,6 +200,11 @@ void mp_transport_destroy(mp_transport* t);
 enum { MP_MESH_RECTANGULAR = 0, MP_MESH_PERTURBED = 1, MP_MESH_SINE_STRETCHED = 2 };
 mp_status mp_transport_create_quads(const mp_mesh_desc* mesh, const double* xy, const mp_transport_opts* opts,
                                     mp_stream_t stream, mp_transport** out);
+/* Device bytes a whole-mesh transport of this mesh allocates (quads != 0:
+ * a general quad mesh, its per-cell tables and the builder's transient copy
+ * of the vertices included); 0 for an invalid mesh. No counterpart in the
+ * reference (host memory there). */
+size_t mp_transport_instance_bytes(const mp_mesh_desc* mesh, int quads);
 /* Vertices of a reference mesh family (VertexAt, src/core/mesh.cpp:27-55):
  * perturbation in [0, 0.25) of the spacing for MP_MESH_PERTURBED, keyed by
  * seed (SplitMix64, as the reference). xy: (nx+1)*(ny+1) (x, y) pairs. */
@@ -491,6 +496,16 @@ mp_status mp_serve_create(const mp_transport_opts* opts, size_t memory_budget, m
 void mp_serve_destroy(mp_server* s);
 mp_status mp_serve_submit(mp_server* s, const mp_mesh_desc* mesh, const double* H, const double* C,
                           const double* vs_n, const double* ud_n, double t_final, long long* id);
+/* A request on a general quad mesh (the vertices xy as
+ * mp_transport_create_quads; the perturbed-quadrilateral and stretched
+ * families of src/core/mesh.cpp:27-55). It is admitted under the same budget
+ * and resident-cell target, and advanced one step per loop iteration beside
+ * the batched uniform-mesh requests by a transport of its own (per-cell
+ * tables built on admission). A mesh failing the quad check finishes with
+ * MP_ERR_ARG_WRONG in its status; the server continues. */
+mp_status mp_serve_submit_quads(mp_server* s, const mp_mesh_desc* mesh, const double* xy, const double* H,
+                                const double* C, const double* vs_n, const double* ud_n, double t_final,
+                                long long* id);
 /* Block until request id finishes (timeout_s < 0: no limit; on expiry
  * MP_ERR_TIMEOUT and the request stays queued/running). */
 mp_status mp_serve_wait(mp_server* s, long long id, double timeout_s, double* H, double* C, double* T,

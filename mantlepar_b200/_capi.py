@@ -164,6 +164,7 @@ def lib() -> C.CDLL:
         "mp_serve_create": (i, [C.POINTER(TransportOpts), sz, C.POINTER(vp)]),
         "mp_serve_destroy": (None, [vp]),
         "mp_serve_submit": (i, [vp, C.POINTER(MeshDesc), vp, vp, vp, vp, d, C.POINTER(C.c_longlong)]),
+        "mp_serve_submit_quads": (i, [vp, C.POINTER(MeshDesc), vp, vp, vp, vp, vp, d, C.POINTER(C.c_longlong)]),
         "mp_serve_wait": (i, [vp, C.c_longlong, d, vp, vp, vp, vp, C.POINTER(RequestInfo)]),
         "mp_serve_stats": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                C.POINTER(C.c_int), C.POINTER(C.c_int)]),
@@ -180,6 +181,7 @@ def lib() -> C.CDLL:
         "mp_transport_get_time": (i, [vp, dp, C.POINTER(C.c_int)]),
         "mp_batch_kernel_times": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
         "mp_transport_create_quads": (i, [C.POINTER(MeshDesc), vp, C.POINTER(TransportOpts), vp, C.POINTER(vp)]),
+        "mp_transport_instance_bytes": (sz, [C.POINTER(MeshDesc), i]),
         "mp_mesh_vertices": (i, [C.POINTER(MeshDesc), i, d, C.c_ulonglong, vp]),
         "mp_transport_create_quads_slab": (i, [C.POINTER(MeshDesc), vp, i, i, C.POINTER(TransportOpts), vp,
                                                C.POINTER(vp)]),

@@ -14,7 +14,10 @@
 // stage kernel for all of them), so work that arrives while others are on the
 // GPU joins at the next step. A request leaves when it reaches its final time
 // or fails; its result is copied out and its memory freed for the queue.
-// State stays resident on the device between steps.
+// State stays resident on the device between steps. A request on a general
+// quad mesh gets a transport of its own (per-cell tables, quad_kernels.cuh),
+// admitted under the same budget and target and stepped once per loop
+// iteration after the batch's step, on the same stream.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -63,6 +66,9 @@ struct Request {
     double work = 0;                       // admission-order estimate
     Clock::time_point submitted, admitted, finished;
     int slot = -1;
+    bool quad = false;                     // general quad mesh: own transport
+    std::vector<double> xy;                // its vertices until admission
+    mp_transport* t = nullptr;
     int status = 0;
     int accepted = 0;
     double time = 0;
@@ -87,6 +93,7 @@ struct mp_server {
     int order = MP_SERVE_SMALLEST_WORK;
     double resident_target = 4.0e6;        // cells; 0 = no limit
     double resident_cells = 0;
+    size_t quad_bytes = 0;                 // device bytes of the quad-mesh transports
     bool stop = false;
     mp_status fatal = MP_OK;
     std::string fatal_msg;
@@ -116,26 +123,37 @@ void admit(mp_server* s) {
                 for (auto it = s->queue.begin(); it != s->queue.end(); ++it)
                     if ((*it)->work < (*pick)->work) pick = it;
             r = *pick;
-            if (mp_batch_bytes_in_use(s->batch) + r->bytes > s->budget) return;
+            if (mp_batch_bytes_in_use(s->batch) + s->quad_bytes + r->bytes > s->budget) return;
             s->queue.erase(pick);
         }
         int slot = -1;
-        mp_status st = mp_batch_add(s->batch, &r->mesh, &slot);
-        if (st == MP_OK) st = mp_batch_set_face_velocity(s->batch, slot, r->vs.data(), r->ud.data());
-        if (st == MP_OK) st = mp_batch_set_state(s->batch, slot, r->H.data(), r->C.data(), 0.0);
-        if (st == MP_OK) st = mp_batch_set_end_time(s->batch, slot, r->t_final);
+        mp_status st;
+        if (r->quad) {
+            st = mp_transport_create_quads(&r->mesh, r->xy.data(), &s->opts, (mp_stream_t)s->stream, &r->t);
+            if (st == MP_OK) st = mp_transport_set_face_velocity(r->t, r->vs.data(), r->ud.data());
+            if (st == MP_OK) st = mp_transport_set_state(r->t, r->H.data(), r->C.data(), 0.0);
+            if (st == MP_OK) st = mp_transport_set_time_control(r->t, MP_TIME_CFL, r->t_final);
+        } else {
+            st = mp_batch_add(s->batch, &r->mesh, &slot);
+            if (st == MP_OK) st = mp_batch_set_face_velocity(s->batch, slot, r->vs.data(), r->ud.data());
+            if (st == MP_OK) st = mp_batch_set_state(s->batch, slot, r->H.data(), r->C.data(), 0.0);
+            if (st == MP_OK) st = mp_batch_set_end_time(s->batch, slot, r->t_final);
+        }
         r->admitted = Clock::now();
         if (st != MP_OK) {
             if (slot >= 0) mp_batch_remove(s->batch, slot);
+            if (r->t) { mp_transport_destroy(r->t); r->t = nullptr; }
             std::lock_guard<std::mutex> g(s->m);
             r->status = st; r->done = true; r->finished = Clock::now();
             s->cv_done.notify_all();
             continue;
         }
         r->slot = slot;
+        if (r->quad) s->quad_bytes += r->bytes;
         s->resident_cells += (double)r->cells;
         r->H.clear(); r->H.shrink_to_fit(); r->C.clear(); r->C.shrink_to_fit();
         r->vs.clear(); r->vs.shrink_to_fit(); r->ud.clear(); r->ud.shrink_to_fit();
+        r->xy.clear(); r->xy.shrink_to_fit();
         std::lock_guard<std::mutex> g(s->m);
         s->active.push_back(r);
     }
@@ -145,6 +163,27 @@ void admit(mp_server* s) {
 void retire(mp_server* s) {
     std::vector<std::shared_ptr<Request>> keep;
     for (auto& r : s->active) {
+        if (r->quad) {
+            double time = 0;
+            int acc = 0;
+            const mp_status tg = mp_transport_get_time(r->t, &time, &acc);
+            if (tg != MP_OK && !r->status) r->status = tg;
+            if (!r->status && time < r->t_final) { keep.push_back(r); continue; }
+            r->oH.resize(r->cells); r->oC.resize(r->cells); r->oT.resize(r->cells); r->oP.resize(r->cells);
+            const mp_status gs = mp_transport_get_state(r->t, r->oH.data(), r->oC.data(), r->oT.data(), r->oP.data());
+            if (gs != MP_OK && !r->status) r->status = gs;
+            r->time = time;
+            r->accepted = acc;
+            mp_transport_destroy(r->t);
+            r->t = nullptr;
+            std::lock_guard<std::mutex> g(s->m);
+            s->quad_bytes -= r->bytes;
+            s->resident_cells -= (double)r->cells;
+            r->finished = Clock::now();
+            r->done = true;
+            s->cv_done.notify_all();
+            continue;
+        }
         double time = 0;
         int acc = 0, status = 0;
         mp_batch_get_state(s->batch, r->slot, nullptr, nullptr, nullptr, nullptr, &time, &acc, &status);
@@ -175,10 +214,25 @@ void run(mp_server* s) {
         if (s->active.empty()) continue;
         // Cell-updates of this step: one per cell of every request that accepts it.
         std::vector<int> before(s->active.size());
-        for (size_t k = 0; k < s->active.size(); ++k)
-            mp_batch_get_state(s->batch, s->active[k]->slot, nullptr, nullptr, nullptr, nullptr, nullptr, &before[k], nullptr);
+        bool batched = false;
+        for (size_t k = 0; k < s->active.size(); ++k) {
+            const auto& r = s->active[k];
+            if (r->quad) mp_transport_get_time(r->t, nullptr, &before[k]);
+            else {
+                batched = true;
+                mp_batch_get_state(s->batch, r->slot, nullptr, nullptr, nullptr, nullptr, nullptr, &before[k], nullptr);
+            }
+        }
         const auto a = Clock::now();
-        const mp_status st = mp_batch_step(s->batch, 1, nullptr);
+        const mp_status st = batched ? mp_batch_step(s->batch, 1, nullptr) : MP_OK;
+        // Quad-mesh requests: one step each; a failure ends that request only
+        // (its state is rolled back to the last accepted step).
+        if (st == MP_OK)
+            for (auto& r : s->active)
+                if (r->quad && !r->status) {
+                    const mp_status qs = mp_transport_step(r->t, 1, nullptr);
+                    if (qs != MP_OK) r->status = qs;
+                }
         const auto b = Clock::now();
         if (st != MP_OK) {
             std::lock_guard<std::mutex> g(s->m);
@@ -190,9 +244,11 @@ void run(mp_server* s) {
         }
         double upd = 0;
         for (size_t k = 0; k < s->active.size(); ++k) {
-            int acc = 0;
-            mp_batch_get_state(s->batch, s->active[k]->slot, nullptr, nullptr, nullptr, nullptr, nullptr, &acc, nullptr);
-            upd += (double)(acc - before[k]) * (double)s->active[k]->cells;
+            const auto& r = s->active[k];
+            int acc = before[k];
+            if (r->quad) mp_transport_get_time(r->t, nullptr, &acc);
+            else mp_batch_get_state(s->batch, r->slot, nullptr, nullptr, nullptr, nullptr, nullptr, &acc, nullptr);
+            upd += (double)(acc - before[k]) * (double)r->cells;
         }
         {
             std::lock_guard<std::mutex> g(s->m);
@@ -234,13 +290,17 @@ extern "C" void mp_serve_destroy(mp_server* s) {
     }
     s->cv_work.notify_all();
     if (s->loop.joinable()) s->loop.join();
+    for (auto& r : s->active)
+        if (r->t) { mp_transport_destroy(r->t); r->t = nullptr; }
     mp_batch_destroy(s->batch);
     cudaStreamDestroy(s->stream);
     delete s;
 }
 
-extern "C" mp_status mp_serve_submit(mp_server* s, const mp_mesh_desc* mesh, const double* H, const double* C,
-                                     const double* vs_n, const double* ud_n, double t_final, long long* id) {
+namespace {
+
+mp_status submit_impl(mp_server* s, const mp_mesh_desc* mesh, const double* xy, const double* H, const double* C,
+                      const double* vs_n, const double* ud_n, double t_final, long long* id) {
     if (!s || !mesh || !H || !C || !vs_n || !ud_n || !id) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
     if (mesh->nx < 2 || mesh->ny < 2) { mp::set_error("Transport requires at least 2x2 cells"); return MP_ERR_ARG_SIZ; }
     if (mp::mesh_too_large(mesh->nx, mesh->ny)) { mp::set_error("mesh has 2^31 edges or more"); return MP_ERR_ARG_SIZ; }
@@ -249,11 +309,13 @@ extern "C" mp_status mp_serve_submit(mp_server* s, const mp_mesh_desc* mesh, con
     r->mesh = *mesh;
     r->cells = (size_t)mesh->nx * mesh->ny;
     const size_t edges = (size_t)mesh->nx * (mesh->ny + 1) + (size_t)(mesh->nx + 1) * mesh->ny;
-    r->bytes = mp_batch_instance_bytes(mesh);
+    r->quad = xy != nullptr;
+    r->bytes = r->quad ? mp_transport_instance_bytes(mesh, 1) : mp_batch_instance_bytes(mesh);
     if (r->bytes > s->budget) {
         mp::set_error("request needs %zu device bytes, above the server budget of %zu", r->bytes, s->budget);
         return MP_ERR_NOMEM;
     }
+    if (r->quad) r->xy.assign(xy, xy + 2 * (size_t)(mesh->nx + 1) * (mesh->ny + 1));
     r->H.assign(H, H + r->cells);
     r->C.assign(C, C + r->cells);
     r->vs.assign(vs_n, vs_n + edges * 5);
@@ -272,6 +334,20 @@ extern "C" mp_status mp_serve_submit(mp_server* s, const mp_mesh_desc* mesh, con
     }
     s->cv_work.notify_all();
     return MP_OK;
+}
+
+}  // namespace
+
+extern "C" mp_status mp_serve_submit(mp_server* s, const mp_mesh_desc* mesh, const double* H, const double* C,
+                                     const double* vs_n, const double* ud_n, double t_final, long long* id) {
+    return submit_impl(s, mesh, nullptr, H, C, vs_n, ud_n, t_final, id);
+}
+
+extern "C" mp_status mp_serve_submit_quads(mp_server* s, const mp_mesh_desc* mesh, const double* xy, const double* H,
+                                           const double* C, const double* vs_n, const double* ud_n, double t_final,
+                                           long long* id) {
+    if (!xy) { mp::set_error("null vertex array"); return MP_ERR_ARG_WRONG; }
+    return submit_impl(s, mesh, xy, H, C, vs_n, ud_n, t_final, id);
 }
 
 extern "C" mp_status mp_serve_wait(mp_server* s, long long id, double timeout_s, double* H, double* C, double* T,

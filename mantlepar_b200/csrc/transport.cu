@@ -905,6 +905,25 @@ extern "C" mp_status mp_transport_create_quads(const mp_mesh_desc* mesh, const d
     return create_impl(mesh, false, 0, 0, opts, stream, out, xy);
 }
 
+extern "C" size_t mp_transport_instance_bytes(const mp_mesh_desc* mesh, int quads) {
+    using namespace mp;
+    if (!mesh || mesh->nx < 2 || mesh->ny < 2 || mesh_too_large(mesh->nx, mesh->ny)) return 0;
+    const size_t nx = (size_t)mesh->nx, ny = (size_t)mesh->ny, N = nx * ny;
+    const size_t NE = nx * (ny + 1) + (nx + 1) * ny;
+    size_t b = 11 * N * sizeof(double)                          // state, stage buffers, L, T, phi, rate
+             + (size_t)kRec * N * sizeof(double) + N             // records, flags
+             + 2 * NE * kNQ * sizeof(double) + 4 * NE * sizeof(double)   // velocities, face values
+             + ((N + kSumCells - 1) / kSumCells) * sizeof(Partial) + sizeof(Totals) + 64;
+    if (quads) {
+        const size_t V = 2 * (nx + 1) * (ny + 1);
+        // Per-cell tables and geometry, vertices, edge spacing; the builder's
+        // copy of the vertices is held while the tables are built.
+        b += ((size_t)(kQG0 + kQS9 + kQT4 + kQS4 + kQGeo) * N + V + NE * kNQ) * sizeof(double) +
+             V * sizeof(double) + sizeof(int);
+    }
+    return b;
+}
+
 extern "C" mp_status mp_transport_create_quads_slab(const mp_mesh_desc* global_mesh, const double* xy, int row_begin,
                                                     int row_end, const mp_transport_opts* opts, mp_stream_t stream,
                                                     mp_transport** out) {

@@ -17,7 +17,7 @@ import time
 import numpy as np
 
 from . import _capi
-from .synthetic import Workload, face_velocity, initial_state
+from .synthetic import Workload, face_velocity, face_velocity_quads, initial_state
 from .transport import TransportConfig
 
 
@@ -62,16 +62,26 @@ class Server:
         except Exception:
             pass
 
-    def submit(self, w: Workload, t_final: float, H=None, Cc=None, vs=None, ud=None) -> int:
+    def submit(self, w: Workload, t_final: float, H=None, Cc=None, vs=None, ud=None, vertices=None) -> int:
+        """Queue one solve. vertices ((nx+1)*(ny+1) (x, y) pairs) makes it a
+        general-quad-mesh request (mp_serve_submit_quads); its face velocities
+        then belong to that mesh's edges."""
         if H is None:
             H, Cc = initial_state(w)
         if vs is None:
-            vs, ud = face_velocity(w)
+            vs, ud = face_velocity(w) if vertices is None else face_velocity_quads(w, vertices)
         m = _capi.MeshDesc(w.nx, w.ny, w.x0, w.x1, w.y0, w.y1)
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (H, Cc, vs, ud)]
         rid = C.c_longlong(0)
-        _capi.check(self._lib.mp_serve_submit(self._h, C.byref(m), *[a.ctypes.data for a in arrs],
-                                              float(t_final), C.byref(rid)))
+        if vertices is None:
+            _capi.check(self._lib.mp_serve_submit(self._h, C.byref(m), *[a.ctypes.data for a in arrs],
+                                                  float(t_final), C.byref(rid)))
+        else:
+            xy = np.ascontiguousarray(vertices, dtype=np.float64)
+            if xy.size != 2 * (w.nx + 1) * (w.ny + 1):
+                raise ValueError("vertices must hold (nx+1)*(ny+1) (x, y) pairs")
+            _capi.check(self._lib.mp_serve_submit_quads(self._h, C.byref(m), xy.ctypes.data,
+                                                        *[a.ctypes.data for a in arrs], float(t_final), C.byref(rid)))
         self._cells[rid.value] = w.cells
         return rid.value
 

@@ -135,3 +135,18 @@ def test_checked_variant_exports_the_same_symbols(cuda_lib):
     exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
     missing = [n for n in _capi.header_functions() if n not in exported]
     assert not missing, missing
+
+
+def test_transport_instance_bytes_is_host_arithmetic(cuda_lib):
+    """mp_transport_instance_bytes (the serving budget of a quad-mesh request)
+    needs no device: 0 for an invalid mesh, the per-cell tables of a quad mesh
+    on top of the uniform transport's arrays, and growth with the cell count."""
+    import ctypes as C
+    lib = _capi.lib()
+    def nbytes(nx, ny, quads):
+        return lib.mp_transport_instance_bytes(C.byref(_capi.MeshDesc(nx, ny, 0.0, 0.5, 0.0, 1.0)), quads)
+    assert nbytes(1, 8, 0) == 0 and nbytes(8, 1, 1) == 0
+    u, q = nbytes(64, 128, 0), nbytes(64, 128, 1)
+    assert 0 < u < q
+    assert (q - u) / (64 * 128) > 184 * 8      # per-cell tables: 184 doubles a cell
+    assert nbytes(128, 256, 1) > 3.9 * q

@@ -1,5 +1,7 @@
 """Serving: continuous batching with memory admission; every served result is
 bitwise the result of the same solve run alone."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -85,3 +87,64 @@ def test_bounded_stream_reports_completed_and_censored(cuda_lib):
     out = run_stream(srv, big, wall_limit=1.0)
     srv.close()
     assert out["completed"] + out["censored"] == 4 and out["censored"] >= 1
+
+
+def alone_quads(w, xy, tf, cfg):
+    """The same quad-mesh solve run alone, one step per call as the server
+    steps it."""
+    from mantlepar_b200.transport import Transport
+    t = Transport(w, cfg, vertices=xy)
+    t.set_face_velocity(*sy.face_velocity_quads(w, xy))
+    t.set_state(*sy.initial_state(w))
+    t.set_time_control(0, tf)
+    for _ in range(10000):
+        if t.get_time()[0] >= tf:
+            break
+        t.step(1)
+    H, C, T, phi = t.get_state()
+    time, acc = t.get_time()
+    t.close()
+    return dict(H=H, C=C, T=T, phi=phi, time=time, accepted=acc)
+
+
+def test_served_quad_mesh_requests_equal_solo_runs(cuda_lib):
+    """Perturbed-quadrilateral and sine-stretched requests (the reference's
+    mesh families) served beside uniform ones under a budget that queues
+    them: each quad result is bitwise the solo quad transport's, each uniform
+    result the solo batch's, and a folded quad mesh ends only its own request
+    with MP_ERR_ARG_WRONG."""
+    from mantlepar_b200.serve import Server
+    from mantlepar_b200.transport import TransportConfig
+    from mantlepar_b200 import _capi
+    cfg = TransportConfig(cfl=0.4, integrator=3)
+    quads = [(sy.Workload(nx=20, ny=20, seed=31), sy.MESH_PERTURBED, 0.01),
+             (sy.Workload(nx=24, ny=16, seed=32), sy.MESH_SINE_STRETCHED, 0.005),
+             (sy.Workload(nx=16, ny=32, seed=33), sy.MESH_PERTURBED, 0.008)]
+    uniform = [(sy.Workload(nx=20, ny=20, seed=34), 0.02), (sy.Workload(nx=40, ny=40, seed=35), 0.005)]
+    big = max(_capi.lib().mp_transport_instance_bytes(C.byref(_capi.MeshDesc(w.nx, w.ny, w.x0, w.x1, w.y0, w.y1)), 1)
+              for w, _, _ in quads)
+    srv = Server(cfg, memory_budget=2 * big)
+    ids = []
+    for k, (w, fam, tf) in enumerate(quads):
+        xy = sy.quad_vertices(w, fam, 0.2 if fam == sy.MESH_PERTURBED else 0.0, seed=11 + k)
+        ids.append(("q", w, xy, tf, srv.submit(w, tf, vertices=xy)))
+        uw, utf = uniform[k % len(uniform)]
+        if k < len(uniform):
+            ids.append(("u", uw, None, utf, srv.submit(uw, utf)))
+    wb = sy.Workload(nx=4, ny=4)
+    bad = sy.quad_vertices(wb, sy.MESH_RECTANGULAR).reshape(5, 5, 2).copy()
+    bad[2, 2] = bad[3, 3] + [0.01, 0.01]
+    bad_id = srv.submit(wb, 0.01, vertices=bad.reshape(-1), vs=np.zeros(40 * 5), ud=np.zeros(40 * 5))
+    got = {rid: srv.wait(rid, timeout=300.0) for *_, rid in ids}
+    bad_res = srv.wait(bad_id, timeout=60.0)
+    st = srv.stats()
+    srv.close()
+    assert bad_res["status"] == 62
+    assert st["cell_updates"] > 0
+    for kind, w, xy, tf, rid in ids:
+        g = got[rid]
+        assert g["status"] == 0 and g["time"] == tf, (kind, g["status"], g["time"])
+        ref = alone_quads(w, xy, tf, cfg) if kind == "q" else alone(w, tf, cfg)
+        assert g["accepted"] == ref["accepted"]
+        for k in ("H", "C", "T", "phi"):
+            assert np.array_equal(g[k], ref[k]), (kind, k)
