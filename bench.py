@@ -609,7 +609,7 @@ def run_gpu(args, world, rank, local):
     e0p, e1p = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     e0p.record(stream)
-    t.step(args.steps)
+    _, reps_p = t.step(args.steps)
     e1p.record(stream)
     torch.cuda.synchronize()
     ms_profiled = e0p.elapsed_time(e1p)
@@ -740,7 +740,11 @@ def run_gpu(args, world, rank, local):
                     "pipelined_equals_sequential": pipe_same},
             "gpu_launches": int(launches),
             "host_syncs_per_step": host_syncs / args.steps,
+            # The host-driven loop's run continues from the timed run's end
+            # state, so its steps take other retries: compare per stage.
             "host_loop_ms_per_step": ms_profiled / args.steps,
+            "host_loop_retries": sum(r["retries"] for r in reps_p),
+            "host_loop_ms_per_stage": ms_profiled / max(1, int(kn[0])),
             "clocks": clk.summary(),
             "retries": retries,
         }
