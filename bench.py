@@ -515,9 +515,9 @@ def run_forms(args, stream):
     if args.serve_requests > 0:
         from mantlepar_b200.serve import Server, input_bytes, poisson_requests, request_work, run_stream
 
-        def served(reqs, wall):
+        def served(reqs, wall, target):
             srv = Server(TransportConfig(cfl=0.4, integrator=3, precision=1), memory_budget=64 << 30)
-            srv.set_policy(Server.SMALLEST_WORK, 4.0e6)
+            srv.set_policy(Server.SMALLEST_WORK, target)
             out = run_stream(srv, reqs, wall_limit=wall)
             srv.close()
             out.pop("results")
@@ -536,7 +536,8 @@ def run_forms(args, stream):
             kept.append(r)
             total += need
         reqs = kept
-        a = served(reqs, args.serve_wall)
+        # A backlog: the throughput setting of the resident-cell target.
+        a = served(reqs, args.serve_wall, 4.0e6)
         forms["served_poisson_200rps"] = dict(
             a, requests_drawn=args.serve_requests, offered_rate_rps=200.0, arrival_span_s=reqs[-1].arrival,
             offered_cell_updates=float(sum(request_work(r) for r in reqs)),
@@ -548,9 +549,11 @@ def run_forms(args, stream):
         capacity = a["gpu_busy_value"] / mean_work
         rate = 0.7 * capacity
         small = poisson_requests(args.serve_requests, rate=rate, seed=5, max_nx=320)
-        b_ = served(small, args.serve_wall)
+        # A sustainable load: the server's default (latency) target.
+        b_ = served(small, args.serve_wall, 1.0e6)
         forms["served_sustained"] = dict(
             b_, offered_rate_rps=rate, arrival_span_s=small[-1].arrival, capacity_rps_estimate=capacity,
+            admission="smallest estimated work first, 1e6 resident cells (the default), 64 GiB budget",
             note="nx in 20..320 (ny = nx * U{1,2}, t_final U[0.01, 0.1]), offered at 70% of the capacity "
                  "estimated from run (a)'s GPU throughput and the stream's mean work")
     return forms

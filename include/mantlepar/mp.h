@@ -514,7 +514,11 @@ mp_status mp_serve_stats(mp_server* s, double* cell_updates, double* busy_s, lon
                          int* resident, int* queued);
 /* Admission order and resident-cell target (0 = admit while memory fits).
  * Default: smallest estimated work (cells * t_final * cells per unit length)
- * first, 4e6 cells. */
+ * first, 1e6 cells. A resident request advances one step per loop iteration
+ * and an iteration steps every resident request, so the target trades
+ * latency for throughput: on a B200, for meshes up to 320x640, 1e6 halves
+ * the median latency of 4e6 at a sustainable load for 2-8 % less throughput;
+ * a backlog is served faster with 4e6. */
 enum { MP_SERVE_FIFO = 0, MP_SERVE_SMALLEST_WORK = 1 };
 mp_status mp_serve_set_policy(mp_server* s, int order, double resident_cells_target);
 

@@ -91,7 +91,7 @@ struct mp_server {
     std::vector<std::shared_ptr<Request>> active;
     long long next_id = 1;
     int order = MP_SERVE_SMALLEST_WORK;
-    double resident_target = 4.0e6;        // cells; 0 = no limit
+    double resident_target = 1.0e6;        // cells; 0 = no limit
     double resident_cells = 0;
     size_t quad_bytes = 0;                 // device bytes of the quad-mesh transports
     bool stop = false;
