@@ -910,16 +910,21 @@ extern "C" size_t mp_transport_instance_bytes(const mp_mesh_desc* mesh, int quad
     if (!mesh || mesh->nx < 2 || mesh->ny < 2 || mesh_too_large(mesh->nx, mesh->ny)) return 0;
     const size_t nx = (size_t)mesh->nx, ny = (size_t)mesh->ny, N = nx * ny;
     const size_t NE = nx * (ny + 1) + (nx + 1) * ny;
-    size_t b = 11 * N * sizeof(double)                          // state, stage buffers, L, T, phi, rate
-             + (size_t)kRec * N * sizeof(double) + N             // records, flags
-             + 2 * NE * kNQ * sizeof(double) + 4 * NE * sizeof(double)   // velocities, face values
-             + ((N + kSumCells - 1) / kSumCells) * sizeof(Partial) + sizeof(Totals) + 64;
+    // Each array is its own cudaMalloc, which takes whole 2 MiB pages; the
+    // small control and reduction buffers share one more page.
+    const size_t page = (size_t)2 << 20;
+    auto pages = [&](size_t bytes) { return (bytes + page - 1) / page * page; };
+    size_t b = 11 * pages(N * sizeof(double))                   // state, stage buffers, L, T, phi, rate
+             + pages((size_t)kRec * N * sizeof(double)) + pages(N)   // records, flags
+             + 2 * pages(NE * kNQ * sizeof(double)) + pages(4 * NE * sizeof(double))   // velocities, face values
+             + pages(((N + kSumCells - 1) / kSumCells) * sizeof(Partial)) + page;
     if (quads) {
         const size_t V = 2 * (nx + 1) * (ny + 1);
-        // Per-cell tables and geometry, vertices, edge spacing; the builder's
-        // copy of the vertices is held while the tables are built.
-        b += ((size_t)(kQG0 + kQS9 + kQT4 + kQS4 + kQGeo) * N + V + NE * kNQ) * sizeof(double) +
-             V * sizeof(double) + sizeof(int);
+        // Per-cell tables and geometry, vertices and edge spacing in one
+        // allocation; the builder's copy of the vertices is held while the
+        // tables are built.
+        b += pages(((size_t)(kQG0 + kQS9 + kQT4 + kQS4 + kQGeo) * N + V + NE * kNQ) * sizeof(double)) +
+             pages(V * sizeof(double) + sizeof(int));
     }
     return b;
 }

@@ -146,7 +146,8 @@ def test_transport_instance_bytes_is_host_arithmetic(cuda_lib):
     def nbytes(nx, ny, quads):
         return lib.mp_transport_instance_bytes(C.byref(_capi.MeshDesc(nx, ny, 0.0, 0.5, 0.0, 1.0)), quads)
     assert nbytes(1, 8, 0) == 0 and nbytes(8, 1, 1) == 0
-    u, q = nbytes(64, 128, 0), nbytes(64, 128, 1)
+    u, q = nbytes(256, 512, 0), nbytes(256, 512, 1)
     assert 0 < u < q
-    assert (q - u) / (64 * 128) > 184 * 8      # per-cell tables: 184 doubles a cell
-    assert nbytes(128, 256, 1) > 3.9 * q
+    assert (q - u) / (256 * 512) > 184 * 8     # per-cell tables: 184 doubles a cell
+    assert nbytes(512, 1024, 1) > 3.5 * q      # whole 2 MiB pages per allocation
+    assert u % (2 << 20) == 0 and q % (2 << 20) == 0

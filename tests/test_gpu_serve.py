@@ -148,3 +148,29 @@ def test_served_quad_mesh_requests_equal_solo_runs(cuda_lib):
         assert g["accepted"] == ref["accepted"]
         for k in ("H", "C", "T", "phi"):
             assert np.array_equal(g[k], ref[k]), (kind, k)
+
+
+def test_transport_instance_bytes_covers_the_allocation(cuda_lib):
+    """The serving budget of a request (mp_transport_instance_bytes) covers
+    what creating its transport takes from the device, uniform and quad
+    mesh, and is not far above it (the quad estimate adds the builder's
+    transient copy of the vertices)."""
+    import torch
+    from mantlepar_b200 import _capi
+    from mantlepar_b200.transport import Transport, TransportConfig
+    lib = _capi.lib()
+    w = sy.Workload(nx=512, ny=1024)
+    mesh = _capi.MeshDesc(w.nx, w.ny, w.x0, w.x1, w.y0, w.y1)
+    for quads in (0, 1):
+        xy = sy.quad_vertices(w, sy.MESH_PERTURBED) if quads else None
+        est = lib.mp_transport_instance_bytes(C.byref(mesh), quads)
+        steady = est - ((2 * (w.nx + 1) * (w.ny + 1) * 8 + 4 + (2 << 20) - 1) // (2 << 20) * (2 << 20) if quads else 0)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        t = Transport(w, TransportConfig(cfl=0.4, integrator=3), vertices=xy)
+        torch.cuda.synchronize()
+        used = free0 - torch.cuda.mem_get_info()[0]
+        t.close()
+        print(f"quads={quads}: estimate {est / 2**20:.1f} MiB, taken {used / 2**20:.1f} MiB")
+        assert used <= est, (quads, used, est)
+        assert used >= 0.8 * steady, (quads, used, steady)
