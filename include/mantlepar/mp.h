@@ -202,8 +202,11 @@ mp_status mp_transport_create_quads(const mp_mesh_desc* mesh, const double* xy, 
                                     mp_stream_t stream, mp_transport** out);
 /* Device bytes a whole-mesh transport of this mesh allocates (quads != 0:
  * a general quad mesh, its per-cell tables and the builder's transient copy
- * of the vertices included); 0 for an invalid mesh. No counterpart in the
- * reference (host memory there). */
+ * of the vertices included), in whole 2 MiB allocation pages; 0 for an
+ * invalid mesh. Not included: the first quad-mesh transport of a process
+ * raises the CUDA runtime's per-thread stack reservation to the per-cell
+ * table builder's 2.7 KB (about 0.5 GB more on a B200), once, for the rest
+ * of the process. No counterpart in the reference (host memory there). */
 size_t mp_transport_instance_bytes(const mp_mesh_desc* mesh, int quads);
 /* Vertices of a reference mesh family (VertexAt, src/core/mesh.cpp:27-55):
  * perturbation in [0, 0.25) of the spacing for MP_MESH_PERTURBED, keyed by

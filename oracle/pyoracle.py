@@ -206,10 +206,10 @@ class PhaseOracle:
 def transport_opts(w, *, uniform_tables=False, threads=0, integrator=None, pressure=0.0,
                    dt_initial=1e30, dt_max=1e30, dt_min=1e-14, cfl=None, inflow_H=1.0, H_policy=0,
                    inflow_C=0.3, C_policy=0, lf_global=0, lf_global_speed=0.0, mesh_family=0, perturbation=0.0,
-                   mesh_seed=1) -> TransportOpts:
+                   mesh_seed=1, theta=0.0) -> TransportOpts:
     return TransportOpts(nx=w.nx, ny=w.ny, x0=w.x0, x1=w.x1, y0=w.y0, y1=w.y1, pressure=pressure,
                          cfl=w.cfl if cfl is None else cfl, dt_initial=dt_initial, dt_max=dt_max,
-                         dt_min=dt_min, theta=0.0, inflow_H=inflow_H, inflow_C=inflow_C, H_policy=int(H_policy),
+                         dt_min=dt_min, theta=float(theta), inflow_H=inflow_H, inflow_C=inflow_C, H_policy=int(H_policy),
                          C_policy=int(C_policy), integrator=int(integrator if integrator is not None else w.integrator),
                          lf_global=int(lf_global), lf_global_speed=float(lf_global_speed),
                          uniform_tables=int(uniform_tables), threads=int(threads),

@@ -154,13 +154,18 @@ def test_transport_instance_bytes_covers_the_allocation(cuda_lib):
     """The serving budget of a request (mp_transport_instance_bytes) covers
     what creating its transport takes from the device, uniform and quad
     mesh, and is not far above it (the quad estimate adds the builder's
-    transient copy of the vertices)."""
+    transient copy of the vertices). The first quad-mesh transport of a
+    process also raises the runtime's per-thread stack reservation for the
+    table builder (2.7 KB a thread), once for the process: a small quad
+    transport is made first, so that the measurement sees one request."""
     import torch
     from mantlepar_b200 import _capi
     from mantlepar_b200.transport import Transport, TransportConfig
     lib = _capi.lib()
     w = sy.Workload(nx=512, ny=1024)
     mesh = _capi.MeshDesc(w.nx, w.ny, w.x0, w.x1, w.y0, w.y1)
+    w0 = sy.Workload(nx=8, ny=8)
+    Transport(w0, TransportConfig(cfl=0.4, integrator=3), vertices=sy.quad_vertices(w0, sy.MESH_PERTURBED)).close()
     for quads in (0, 1):
         xy = sy.quad_vertices(w, sy.MESH_PERTURBED) if quads else None
         est = lib.mp_transport_instance_bytes(C.byref(mesh), quads)

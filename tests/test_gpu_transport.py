@@ -431,3 +431,61 @@ def test_constant_state_is_preserved(cuda_lib, family, nx, ny):
     assert all(x["status"] == 0 for x in reps)
     H, C, _, _ = t.get_state()
     assert np.max(np.abs(H - 0.6)) <= 1e-13 and np.max(np.abs(C - 0.31)) <= 1e-13
+
+
+@pytest.mark.parametrize("name", ["inflow_outflow", "darcy_exponent_2", "global_lf", "zero_flux_C",
+                                  "outflow_H_at_inflow"])
+def test_boundary_policies_match_oracle(cuda_lib, name):
+    """Flow through the walls (the advection boundary policy of every wall
+    point, initialization.cpp:469-489; the global Lax-Friedrichs speed; a
+    Darcy exponent of 2 in the transport velocities, evolve.cpp:36-52):
+    limiter factors, stage and 10 SSPRK3 steps against the reference build at
+    1e-12 with the same retries; the outflow-only enthalpy policy on an
+    inflow wall fails with the reference's error class (63) and leaves the
+    state untouched."""
+    import boundary_cases as bcs
+    from oracle import pyoracle as po
+    from mantlepar_b200._capi import MPError
+    from mantlepar_b200.transport import Transport, TransportConfig
+    kw, status = bcs.CASES[name]
+    lib = po.reference() if po.reference_available() else po.restated()
+    t = Transport(bcs.W, TransportConfig(cfl=bcs.W.cfl, integrator=3, **kw))
+    o = po.TransportOracle(sy.material_s(), bcs.W, lib=lib, integrator=3, **kw)
+    vs, ud = bcs.face_velocity()
+    H, C = sy.initial_state(bcs.W)
+    for x in (t, o):
+        x.set_face_velocity(vs, ud)
+        x.set_state(H, C)
+    if status:
+        assert o.rhs()[0] == status
+        with pytest.raises(MPError) as err:
+            t.rhs()
+        assert err.value.code == status
+        code, _ = t.step(1, raise_on_error=False)
+        assert code == status
+        assert np.array_equal(np.stack(t.get_state())[:2], np.stack([H, C]))
+        return
+    a, b = t.limiter()
+    code, ra, rb = o.limiter()
+    assert code == 0
+    assert np.max(np.abs(a - ra)) <= 1e-12 and np.max(np.abs(b - rb)) <= 1e-12
+    r = t.rhs()
+    code, ref = o.rhs()
+    assert code == 0
+    for k in ["T", "phi", "rate"]:
+        assert rel(r[k], ref[k]) <= RTOL_STAGE, k
+    for k in ["rhsH", "rhsC"]:
+        assert rel_inf(r[k], ref[k]) <= RTOL_STAGE, k
+    for k in ["boundaryH", "boundaryC"]:
+        assert abs(r[k] - ref[k]) <= 1e-12 * max(1.0, abs(ref[k])), k
+    assert abs(r["maxRate"] - ref["maxRate"]) <= RTOL_STAGE * ref["maxRate"]
+    _, got = t.step(10)
+    code, want = o.step(10)
+    assert code == 0
+    assert [x["retries"] for x in got] == [x["retries"] for x in want]
+    assert rel(np.array([x["dt"] for x in got]), np.array([x["dt"] for x in want])) <= RTOL_RUN10
+    ga, gb = np.stack(t.get_state()), np.stack(o.get_state())
+    for k in range(4):
+        assert rel(ga[k], gb[k]) <= RTOL_RUN10, k
+    t.close()
+    o.close()

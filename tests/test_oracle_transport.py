@@ -285,3 +285,35 @@ def test_constant_state_is_preserved(family):
         assert code == 0 and r["phi"].min() > 0
         for k in ("rhsH", "rhsC"):
             assert np.max(np.abs(r[k])) <= 1e-13 * r["maxRate"], k
+
+
+@pytest.mark.skipif(not po.reference_available(), reason="reference-backed oracle not built")
+@pytest.mark.parametrize("name", ["inflow_outflow", "darcy_exponent_2", "global_lf", "zero_flux_C",
+                                  "outflow_H_at_inflow"])
+def test_boundary_policies_restatement_equals_reference_bitwise(name):
+    """Flow through the walls (inflow/outflow/zero-flux policies, global LF
+    speed, Darcy exponent): the restatement equals the reference's own classes
+    bit for bit over a stage and 10 SSPRK3 steps, and both reject the
+    outflow-only policy on an inflow wall with the same error class."""
+    import boundary_cases as bcs
+    kw, status = bcs.CASES[name]
+    vs, ud = bcs.face_velocity()
+    H, C = sy.initial_state(bcs.W)
+    out = []
+    for lib in (po.restated(), po.reference()):
+        o = po.TransportOracle(sy.material_s(), bcs.W, lib=lib, integrator=3, **kw)
+        o.set_face_velocity(vs, ud)
+        o.set_state(H, C)
+        code, r = o.rhs()
+        code2, reps = o.step(10)
+        out.append((code, code2, r, np.stack(o.get_state()), [x["retries"] for x in reps]))
+        o.close()
+    (c1, s1, r1, st1, rt1), (c2, s2, r2, st2, rt2) = out
+    assert c1 == c2 == status and s1 == s2 == status
+    if status:
+        return
+    for k in ("rhsH", "rhsC", "T", "phi", "rate"):
+        assert np.array_equal(bits(r1[k]), bits(r2[k])), k
+    assert r1["boundaryH"] == r2["boundaryH"] and r1["boundaryC"] == r2["boundaryC"]
+    assert r1["boundaryH"] != 0.0                       # the walls carry flux
+    assert rt1 == rt2 and np.array_equal(bits(st1), bits(st2))
