@@ -238,11 +238,11 @@ mp_status mp_transport_step(mp_transport* t, int nsteps, mp_step_report* reports
 
 /* Device-resident stepping (no counterpart in the reference, whose step loop
  * is host code). With enable != 0 (the default) mp_transport_step on a
- * uniform mesh without slab hooks runs as one CUDA graph per 64 steps: the
+ * whole mesh (uniform or general quad) runs as one CUDA graph per 64 steps: the
  * step and retry loops are conditional graph nodes and every decision of the
  * loop above is taken on the device, one host wait per graph launch; results,
  * reports and errors equal the host-driven loop (enable = 0) bit for bit.
- * Row slabs, general quad meshes and profiling runs use the host-driven loop. */
+ * Row slabs and profiling runs use the host-driven loop. */
 mp_status mp_transport_set_device_steps(mp_transport* t, int enable);
 /* Host waits for device results made by the stepping and RHS calls so far. */
 mp_status mp_transport_run_stats(const mp_transport* t, unsigned long long* host_syncs);

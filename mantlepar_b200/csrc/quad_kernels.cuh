@@ -42,7 +42,8 @@ struct SourcePtrs {
 __global__ void __launch_bounds__(128, 3) quad_weno_kernel(int nx, int ny, const double* __restrict__ H,
                                                            const double* __restrict__ C, double* __restrict__ rec,
                                                            unsigned long long* status, QuadDev q, int gj0, int gny,
-                                                           int jlo, int jhi) {
+                                                           int jlo, int jhi, const int* gate) {
+    if (gated_off(gate)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = jlo + (int)(blockIdx.y * blockDim.y + threadIdx.y);
     if (i >= nx || j >= jhi) return;
     const long long cell = (long long)j * nx + i;
@@ -76,7 +77,8 @@ __global__ void __launch_bounds__(128, 4) quad_limit_kernel(int nx, int ny, cons
                                                          const double* __restrict__ C, double* __restrict__ rec,
                                                          unsigned char* __restrict__ flags, unsigned long long* status,
                                                          double* theta, Physics ph, QuadDev q, int gj0, int gny,
-                                                         int jlo, int jhi) {
+                                                         int jlo, int jhi, const int* gate) {
+    if (gated_off(gate)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = jlo + (int)(blockIdx.y * blockDim.y + threadIdx.y);
     if (i >= nx || j >= jhi) return;
     const long long cell = (long long)j * nx + i;
@@ -149,7 +151,8 @@ __global__ void __launch_bounds__(128, 4) quad_cellphase_kernel(int nx, int ny, 
                                                              unsigned char* __restrict__ flags, double* __restrict__ T,
                                                              double* __restrict__ phi, unsigned long long* status,
                                                              Physics ph, QuadDev q, SourcePtrs src, int gj0, int gny,
-                                                             long long c0, long long c1) {
+                                                             long long c0, long long c1, const int* gate) {
+    if (gated_off(gate)) return;
     const long long N = (long long)nx * ny;
     const long long cell = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= c1) return;
@@ -232,7 +235,8 @@ __global__ void __launch_bounds__(128, 4) quad_face_kernel(int nx, int ny, const
                                                         const double* __restrict__ vsn, const double* __restrict__ udn,
                                                         double* __restrict__ face, unsigned long long* status,
                                                         Physics ph, QuadDev q, int gj0, int gny, long long h0,
-                                                        long long nh, long long v0, long long nv) {
+                                                        long long nh, long long v0, long long nv, const int* gate) {
+    if (gated_off(gate)) return;
     const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nh + nv) return;
@@ -290,7 +294,8 @@ __global__ void __launch_bounds__(128) quad_diffusion_kernel(int nx, int ny, con
                                                              const double* __restrict__ rec, double* __restrict__ face,
                                                              unsigned long long* status, Physics ph, QuadDev q,
                                                              int gj0, int gny, long long h0, long long nh, long long v0,
-                                                             long long nv) {
+                                                             long long nv, const int* gate) {
+    if (gated_off(gate)) return;
     const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nh + nv) return;
@@ -355,24 +360,25 @@ __global__ void __launch_bounds__(128) quad_diffusion_kernel(int nx, int ny, con
 // on a general quad mesh; the accumulation is the shared sum kernel. Local
 // rows [rec0, rec1) are reconstructed, the edges [h0, h0+nh) and [v0, v0+nv)
 // (those of the advanced rows) get fluxes; local row 0 is global row gj0 of
-// gny (a whole mesh: gj0 = 0, gny = ny).
+// gny (a whole mesh: gj0 = 0, gny = ny). gate: device flag, every kernel
+// returns at once while it is 0 (the device-resident step graph).
 void launch_quad_stage(const QuadDev& q, int nx, int ny, int gj0, int gny, int rec0, int rec1, long long h0,
                        long long nh, long long v0, long long nv, const Physics& ph, const double* H, const double* C,
                        double* rec, unsigned char* flags, double* T, double* phi, const double* vsn, const double* udn,
                        double* face, unsigned long long* status, double* theta, const SourcePtrs& src,
-                       cudaStream_t s) {
+                       cudaStream_t s, const int* gate = nullptr) {
     dim3 blk(32, 4), grd((nx + 31) / 32, (rec1 - rec0 + 3) / 4);
-    quad_weno_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, status, q, gj0, gny, rec0, rec1);
-    quad_limit_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, flags, status, theta, ph, q, gj0, gny, rec0, rec1);
+    quad_weno_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, status, q, gj0, gny, rec0, rec1, gate);
+    quad_limit_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, flags, status, theta, ph, q, gj0, gny, rec0, rec1, gate);
     const long long c0 = (long long)rec0 * nx, c1 = (long long)rec1 * nx;
     quad_cellphase_kernel<<<(unsigned)((c1 - c0 + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, flags, T, phi, status,
-                                                                            ph, q, src, gj0, gny, c0, c1);
+                                                                            ph, q, src, gj0, gny, c0, c1, gate);
     const unsigned ge = (unsigned)((nh + nv + 127) / 128);
     quad_face_kernel<<<ge, 128, 0, s>>>(nx, ny, H, C, rec, flags, vsn, udn, face, status, ph, q, gj0, gny, h0, nh, v0,
-                                        nv);
+                                        nv, gate);
     count_launch(4);
     if (ph.diffusion) {
-        quad_diffusion_kernel<<<ge, 128, 0, s>>>(nx, ny, H, C, rec, face, status, ph, q, gj0, gny, h0, nh, v0, nv);
+        quad_diffusion_kernel<<<ge, 128, 0, s>>>(nx, ny, H, C, rec, face, status, ph, q, gj0, gny, h0, nh, v0, nv, gate);
         count_launch();
     }
 }

@@ -15,8 +15,8 @@
 //                     face order, the Runge-Kutta combination, block partials.
 // The time loop (evolve.cpp:428-511) runs on the device (graph_steps: a CUDA
 // graph of the stage kernels and the step controller, one host wait per 64
-// steps) or, for row slabs, general quad meshes and profiling runs, on the
-// host (do_step: one small device->host read per stage).
+// steps; uniform and general quad meshes) or, for row slabs and profiling
+// runs, on the host (do_step: one small device->host read per stage).
 #include "common.hpp"
 #include "phase_math.cuh"
 #include "stage_device.cuh"
@@ -378,7 +378,7 @@ mp_status launch_stage(mp_transport* t, const double* H, const double* C, int mo
         timed(t, 0, [&] {
             launch_quad_stage(t->qdev, t->nx, t->ny, rg.gj0, gny, rg.rec0, rg.rec1, h0, nh, v0, nv, t->ph, H, C,
                               static_cast<double*>(t->rec), t->flags, t->T, t->phi, t->vsn, t->udn, t->face,
-                              t->d_status, theta, SourcePtrs{sb.cvs_y, sb.cud_y, sb.srcH, sb.srcR, sb.srcS}, s);
+                              t->d_status, theta, SourcePtrs{sb.cvs_y, sb.cud_y, sb.srcH, sb.srcR, sb.srcS}, s, gate);
         });
     } else {
         launch_stage_kernels<double>(t->nx, t->ny, t->range, t->ptab, t->ph, H, C, static_cast<double*>(t->rec), t->flags, t->T,
@@ -567,7 +567,7 @@ mp_status do_step(mp_transport* t, mp_step_report& rep) {
 constexpr int kGraphSteps = 64;        // steps per graph launch (report rows)
 
 bool graph_usable(const mp_transport* t) {
-    return t->use_graph && !t->profile && !t->halo && !t->combine && !t->quad && !(t->ph.source && !t->cvs_y);
+    return t->use_graph && !t->profile && !t->halo && !t->combine && !(t->ph.source && !t->cvs_y);
 }
 
 StepOpts single_step_opts(const mp_transport* t) {
@@ -627,8 +627,8 @@ mp_status capture_steps(mp_transport* t, cudaGraph_t g) {
     MP_CUDA(cudaStreamBeginCaptureToGraph(s, attempt_body, nullptr, nullptr, 0, mode));
     ctl_attempt_kernel<<<1, kCtlThreads, 0, s>>>(t->d_ctl, 1, so, t->d_hdr, t->d_gate, t->d_dt);
     axpy_kernel<<<nblk_axpy, kRedBlock, 0, s>>>((int)on, t->H + o0, t->C + o0, t->LH + o0, t->LC + o0, 0.0,
-                                                 t->host_tab.area, t->S1H + o0, t->S1C + o0, t->partial, nullptr,
-                                                 t->d_dt, t->d_gate);
+                                                 t->host_tab.area, t->S1H + o0, t->S1C + o0, t->partial,
+                                                 t->cell_area ? t->cell_area + o0 : nullptr, t->d_dt, t->d_gate);
     reduce_kernel<<<1, 1024, 0, s>>>(t->partial, nblk_axpy, t->d_tot, t->d_gate);
     ctl_after_axpy_kernel<<<1, kCtlThreads, 0, s>>>(t->d_ctl, 1, so, t->d_tot, t->d_status, t->d_gate);
     MP_TRY(launch_stage(t, t->S1H, t->S1C, SUM_RK, rk3 ? 0.75 : 0.5, rk3 ? 0.25 : 0.5, 0.0, t->S2H, t->S2C, nullptr,
@@ -726,7 +726,9 @@ mp_status graph_steps(mp_transport* t, int nsteps, mp_step_report* reports) {
     if (!t->have_L) MP_TRY(eval_current(t));
     MP_TRY(ensure_graph(t));
     cudaStream_t s = t->stream;
-    const int sk = 5 + (t->ph.diffusion ? 1 : 0);           // kernels of one stage evaluation
+    // Kernels of one stage evaluation: reconstruction, cell phase, faces,
+    // sums, reduction (a quad mesh: WENO and limiter apart, one more).
+    const int sk = (t->quad ? 6 : 5) + (t->ph.diffusion ? 1 : 0);
     const bool rk3 = t->opts.integrator == MP_SSPRK3;
     for (int done = 0; done < nsteps; done += kGraphSteps) {
         const int chunk = std::min(kGraphSteps, nsteps - done);

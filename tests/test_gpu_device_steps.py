@@ -214,3 +214,31 @@ def test_batch_graph_survives_instance_changes(cuda_lib):
         for key in ("H", "C", "T", "phi"):
             assert np.array_equal(a[key], c[key])
     assert out[0][4] == 1 and out[1][4] == 0
+
+
+@pytest.mark.parametrize("family,integ,kappa", [(sy.MESH_PERTURBED, 3, 0.0), (sy.MESH_PERTURBED, 2, 0.0),
+                                                (sy.MESH_SINE_STRETCHED, 3, 0.0), (sy.MESH_PERTURBED, 3, 0.02)])
+def test_quad_mesh_graph_equals_host_loop(cuda_lib, family, integ, kappa):
+    """General quad meshes (per-cell tables) step in the same graph: states,
+    reports and retries equal the host-driven loop bit for bit, with one host
+    wait per 64 steps; with diffusion too."""
+    from mantlepar_b200.transport import Transport, TransportConfig
+    w = sy.Workload(nx=20, ny=24, seed=5)
+    xy = sy.quad_vertices(w, family, 0.2 if family == sy.MESH_PERTURBED else 0.0, seed=11)
+    cfg = TransportConfig(cfl=w.cfl, integrator=integ, diffusivity=kappa)
+    out = []
+    for dev in (True, False):
+        t = Transport(w, cfg, vertices=xy)
+        t.set_device_steps(dev)
+        t.set_face_velocity(*sy.face_velocity_quads(w, xy))
+        t.set_state(*sy.initial_state(w))
+        code, reps = t.step(150, raise_on_error=False)
+        out.append(dict(code=code, reps=reps, state=t.get_state(), time=t.get_time(), syncs=t.host_syncs(),
+                        msg=t._lib.mp_last_error_string() if code else b""))
+        t.close()
+    g, h = out
+    assert g["code"] == 0
+    if kappa == 0.0:
+        assert sum(r["retries"] for r in g["reps"]) > 0      # the run exercises CFL retries
+    assert_same(g, h)
+    assert g["syncs"] <= 1 + 3 and h["syncs"] >= (3 if integ == 3 else 2) * 150
