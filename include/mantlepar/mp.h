@@ -432,6 +432,15 @@ mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, const mp_transp
 void mp_batch_destroy(mp_batch* b);
 /* Add an instance in a free slot (or a new one); remove frees its memory. */
 mp_status mp_batch_add(mp_batch* b, const mp_mesh_desc* mesh, int* instance);
+/* Add an instance on a general quad mesh (the vertices xy as
+ * mp_transport_create_quads: the perturbed-quadrilateral and stretched
+ * families of src/core/mesh.cpp:27-55). Its per-cell tables are built on the
+ * GPU at add; its stage kernels are the quad mesh's, batched over the quad
+ * instances' own work lists, and the accumulation, step control and graph
+ * are shared with the uniform instances. Results equal the instance run
+ * alone through mp_transport_create_quads bit for bit. A mesh failing the
+ * quad check -> MP_ERR_ARG_WRONG and no instance. */
+mp_status mp_batch_add_quads(mp_batch* b, const mp_mesh_desc* mesh, const double* xy, int* instance);
 mp_status mp_batch_remove(mp_batch* b, int instance);
 /* Device bytes one instance of this mesh holds (memory admission). */
 size_t mp_batch_instance_bytes(const mp_mesh_desc* mesh);

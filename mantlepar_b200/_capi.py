@@ -151,6 +151,7 @@ def lib() -> C.CDLL:
         "mp_batch_add": (i, [vp, C.POINTER(MeshDesc), C.POINTER(C.c_int)]),
         "mp_batch_remove": (i, [vp, i]),
         "mp_batch_instance_bytes": (sz, [C.POINTER(MeshDesc)]),
+        "mp_batch_add_quads": (i, [vp, C.POINTER(MeshDesc), vp, C.POINTER(i)]),
         "mp_batch_bytes_in_use": (sz, [vp]),
         "mp_batch_slots": (i, [vp]),
         "mp_batch_set_face_velocity": (i, [vp, i, vp, vp]),

@@ -62,6 +62,18 @@ class Batch:
         self.cells[slot.value] = w.cells
         return slot.value
 
+    def add_quads(self, w: Workload, vertices) -> int:
+        """An instance on a general quad mesh: vertices holds the
+        (nx+1)*(ny+1) (x, y) pairs (mp_batch_add_quads)."""
+        m = mesh_of(w)
+        xy = np.ascontiguousarray(vertices, dtype=np.float64)
+        if xy.size != 2 * (w.nx + 1) * (w.ny + 1):
+            raise ValueError("vertices must hold (nx+1)*(ny+1) (x, y) pairs")
+        slot = C.c_int(-1)
+        _capi.check(self._lib.mp_batch_add_quads(self._h, C.byref(m), xy.ctypes.data, C.byref(slot)))
+        self.cells[slot.value] = w.cells
+        return slot.value
+
     def remove(self, i: int):
         _capi.check(self._lib.mp_batch_remove(self._h, int(i)))
         self.cells.pop(i, None)

@@ -19,6 +19,8 @@
 #include "stage_kernels.cuh"
 #include "step_ctl.cuh"
 #include "tables.hpp"
+#include "quad_kernels.cuh"
+#include "quad_tables.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -54,6 +56,7 @@ struct AxpyArgs {
     const double* dtp;
     double area;
     Partial* partial;
+    const double* cell_area;   // per-cell areas (general quad mesh), else null
 };
 
 // Commit of an accepted step: the stage state that holds U^{n+1} becomes U^n.
@@ -108,13 +111,59 @@ __global__ void __launch_bounds__(128) batch_diffusion_kernel(const InstArgs<R>*
     if (e < w.b) diffusion_edge(args[w.inst].face, ph, e);
 }
 
-// kSrc: the adiabatic source terms are added.
+// General quad meshes: the per-element bodies of the single-mesh quad
+// kernels (quad_kernels.cuh) over the quad instances' work lists.
+__global__ void __launch_bounds__(128, 3) batch_quad_weno_kernel(const QuadStageArgs* args, const Work* work,
+                                                                 const int* active) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    const QuadStageArgs& a = args[w.inst];
+    const int i = w.a + threadIdx.x, j = w.b + threadIdx.y;
+    if (i < a.nx && j < a.ny) quad_weno_cell(a, i, j);
+}
+
+__global__ void __launch_bounds__(128, 4) batch_quad_limit_kernel(const QuadStageArgs* args, const Work* work,
+                                                                  const int* active, Physics ph) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    const QuadStageArgs& a = args[w.inst];
+    const int i = w.a + threadIdx.x, j = w.b + threadIdx.y;
+    if (i < a.nx && j < a.ny) quad_limit_cell(a, ph, i, j);
+}
+
+__global__ void __launch_bounds__(128, 4) batch_quad_phase_kernel(const QuadStageArgs* args, const Work* work,
+                                                                  const int* active, Physics ph) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    const QuadStageArgs& a = args[w.inst];
+    const long long cell = (long long)w.a + threadIdx.x;
+    if (cell < (long long)a.nx * a.ny) quad_cellphase_cell(a, ph, cell);
+}
+
+__global__ void __launch_bounds__(128, 4) batch_quad_face_kernel(const QuadStageArgs* args, const Work* work,
+                                                                 const int* active, Physics ph) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    const long long e = (long long)w.a + threadIdx.x;
+    if (e < w.b) quad_face_edge(args[w.inst], ph, e);
+}
+
+__global__ void __launch_bounds__(128) batch_quad_diffusion_kernel(const QuadStageArgs* args, const Work* work,
+                                                                   const int* active, Physics ph) {
+    const Work w = work[blockIdx.x];
+    if (!active[w.inst]) return;
+    const long long e = (long long)w.a + threadIdx.x;
+    if (e < w.b) quad_diffusion_edge(args[w.inst], ph, e);
+}
+
+// kSrc: the adiabatic source terms are added. An instance with per-cell
+// areas (a general quad mesh) takes them.
 template <class R, bool kSrc>
 __global__ void __launch_bounds__(kRedBlock) batch_sum_kernel(const InstArgs<R>* args, const Work* work, const int* active) {
     const Work w = work[blockIdx.x];
     if (!active[w.inst]) return;
     const SumArgs& a = args[w.inst].sum;
-    const Partial v = sum_cells<kSrc>(a, w.a);
+    const Partial v = a.cell_area ? sum_cells<kSrc, true>(a, w.a) : sum_cells<kSrc>(a, w.a);
     block_reduce_write(v, a.partial + w.part);
 }
 
@@ -122,7 +171,7 @@ __global__ void __launch_bounds__(kRedBlock) batch_axpy_kernel(const AxpyArgs* a
     const Work w = work[blockIdx.x];
     if (!active[w.inst]) return;
     const AxpyArgs& a = args[w.inst];
-    const Partial v = axpy_cells(a.n, a.H0, a.C0, a.LH, a.LC, *a.dtp, a.area, a.H1, a.C1, w.a);
+    const Partial v = axpy_cells(a.n, a.H0, a.C0, a.LH, a.LC, *a.dtp, a.area, a.H1, a.C1, w.a, a.cell_area);
     block_reduce_write(v, a.partial + w.part);
 }
 
@@ -179,6 +228,13 @@ struct MPInstance {
     void* src_arena = nullptr;
     size_t src_bytes = 0;
     double *cvs_y = nullptr, *cud_y = nullptr, *srcH = nullptr, *srcR = nullptr, *srcS = nullptr;
+    // General quad mesh (mp_batch_add_quads): per-cell tables, vertices and
+    // edge spacing in one allocation, and the cell areas inside it.
+    bool quad = false;
+    double* qbuf = nullptr;
+    size_t qbytes = 0;
+    mp::QuadDev qdev{};
+    const double* cell_area = nullptr;
     double time = 0.0;
     double t_end = INFINITY;          // time.end of this instance
     int accepted = 0;
@@ -212,6 +268,13 @@ struct mp_batch {
     // graph stays valid until a capacity grows.
     int n_wrecon = 0, n_wphase = 0, n_wface = 0, n_wsum = 0;
     int cap_wrecon = 0, cap_wphase = 0, cap_wface = 0, cap_wsum = 0;
+    // General quad meshes: their own stage records and work lists (the
+    // accumulation, axpy and commit lists cover every instance).
+    bool has_quads = false;            // launch the quad kernels (set by the first quad instance)
+    void* d_qargs[mp::NKIND] = {nullptr, nullptr, nullptr};
+    mp::Work *d_wqrec = nullptr, *d_wqphase = nullptr, *d_wqface = nullptr;
+    int n_wqrec = 0, n_wqphase = 0, n_wqface = 0;
+    int cap_wqrec = 0, cap_wqphase = 0, cap_wqface = 0;
     int *d_active = nullptr, *d_part_off = nullptr, *d_part_cnt = nullptr;
     mp::Partial* d_partial = nullptr;
     int partial_cap = 0;
@@ -320,10 +383,69 @@ mp_status alloc_instance(mp_batch* b, MPInstance& in, const mp_mesh_desc& m) {
     return MP_OK;
 }
 
+// An instance on a general quad mesh: the arena of alloc_instance (its
+// uniform-table slot unused) and the per-cell tables built on the GPU, as
+// mp_transport_create_quads builds them.
+mp_status alloc_quad_instance(mp_batch* b, MPInstance& in, const mp_mesh_desc& m, const double* xy) {
+    long long bad = -1;
+    if (validate_quads(m.nx, m.ny, xy, &bad)) {
+        set_error("Mesh has non-real/non-finite coordinates or an inverted, degenerate, or nearly singular "
+                  "quadrilateral (cell %lld)", bad);
+        return MP_ERR_ARG_WRONG;
+    }
+    QuadTables qt;
+    const int qs = build_quad_tables(m.nx, m.ny, xy, 0, qt, 0, m.ny, false);
+    if (qs) { set_error("per-cell stencil table construction failed"); return (mp_status)qs; }
+    in.mesh = m; in.nx = m.nx; in.ny = m.ny;
+    in.N = (size_t)m.nx * m.ny;
+    in.NE = (size_t)m.nx * (m.ny + 1) + (size_t)(m.nx + 1) * m.ny;
+    in.bytes = instance_bytes(m.nx, m.ny);
+    MP_CUDA(cudaMallocAsync(&in.arena, in.bytes, b->stream));
+    unsigned char* p = static_cast<unsigned char*>(in.arena);
+    auto take = [&](size_t bytes) { void* r = p; p += align256(bytes); return r; };
+    const size_t N = in.N, NE = in.NE;
+    double** dbl[] = {&in.H, &in.C, &in.S1H, &in.S1C, &in.S2H, &in.S2C, &in.LH, &in.LC, &in.T, &in.phi, &in.rate};
+    for (double** q : dbl) *q = static_cast<double*>(take(N * sizeof(double)));
+    in.rec = static_cast<double*>(take(18 * N * sizeof(double)));
+    in.flags = static_cast<unsigned char*>(take(N));
+    in.vsn = static_cast<double*>(take(NE * kNQ * sizeof(double)));
+    in.udn = static_cast<double*>(take(NE * kNQ * sizeof(double)));
+    in.face = static_cast<double*>(take(4 * NE * sizeof(double)));
+    in.tab = nullptr;
+    MP_CUDA(cudaMemsetAsync(in.vsn, 0, NE * kNQ * sizeof(double), b->stream));
+    MP_CUDA(cudaMemsetAsync(in.udn, 0, NE * kNQ * sizeof(double), b->stream));
+    cudaError_t ce = cudaSuccess;
+    const int gs = upload_quad_tables(m.nx, m.ny, xy, qt, 0, m.ny, b->stream, &in.qbuf, in.qdev, &ce);
+    if (gs) {
+        cudaFreeAsync(in.arena, b->stream);
+        cudaStreamSynchronize(b->stream);
+        if (in.qbuf) cudaFree(in.qbuf);
+        in = MPInstance{};
+        if (gs == MP_ERR_ARG_WRONG) {
+            set_error("per-cell stencil table construction failed (singular stencil or degenerate cell)");
+            return MP_ERR_ARG_WRONG;
+        }
+        return cuda_status(ce, "mp_batch_add_quads");
+    }
+    in.qbytes = ((size_t)(kQG0 + kQS9 + kQT4 + kQS4 + kQGeo) * N + qt.xy.size() + qt.spacing.size()) * sizeof(double);
+    in.cell_area = in.qdev.geo + 3 * N;
+    in.quad = true;
+    in.used = true;
+    in.time = 0.0; in.accepted = 0; in.have_L = false; in.status = 0;
+    b->bytes_in_use += in.bytes + in.qbytes;
+    if (!b->has_quads) { b->has_quads = true; b->gen += 1; }
+    b->dirty = true;
+    return MP_OK;
+}
+
 void free_instance(mp_batch* b, MPInstance& in) {
     if (in.arena) cudaFreeAsync(in.arena, b->stream);
     if (in.src_arena) cudaFreeAsync(in.src_arena, b->stream);
-    b->bytes_in_use -= in.bytes + in.src_bytes;
+    if (in.qbuf) {
+        cudaStreamSynchronize(b->stream);
+        cudaFree(in.qbuf);
+    }
+    b->bytes_in_use -= in.bytes + in.src_bytes + in.qbytes;
     in = MPInstance{};
     b->dirty = true;
 }
@@ -347,6 +469,9 @@ template <class R>
 mp_status rebuild_args(mp_batch* b, int slots) {
     std::vector<InstArgs<R>> args[NKIND];
     for (int k = 0; k < NKIND; ++k) args[k].resize(slots);
+    std::vector<QuadStageArgs> qargs[NKIND];
+    for (int k = 0; k < NKIND; ++k) qargs[k].resize(slots);
+    std::vector<Work> wqr, wqp, wqf;
     std::vector<AxpyArgs> ax(slots);
     std::vector<CommitArgs> cm(slots);
     std::vector<int> part_off(slots, 0), part_cnt(slots, 0);
@@ -358,6 +483,7 @@ mp_status rebuild_args(mp_batch* b, int slots) {
         if (!in.used) continue;
         Tab<R> tb;
         tb.t = in.tab;
+        const double area = in.quad ? 1.0 : in.host_tab.area;   // a quad mesh: per-cell areas
         const int nsum = (int)((in.N + kSumCells - 1) / kSumCells);
         part_off[i] = parts; part_cnt[i] = nsum;
         Partial* pp = nullptr;  // fixed below once the partial array exists
@@ -375,18 +501,34 @@ mp_status rebuild_args(mp_batch* b, int slots) {
             const bool rk3 = b->opts.integrator == MP_SSPRK3;
             const double a0 = k == KIND_B ? (rk3 ? 0.75 : 0.5) : (1.0 / 3.0);
             const double a1 = k == KIND_B ? (rk3 ? 0.25 : 0.5) : (2.0 / 3.0);
-            a.sum = SumArgs{in.nx, in.ny, in.host_tab.area, 1.0 / in.host_tab.area, in.face, inH, inC, in.H, in.C, outH, outC, in.rate,
+            a.sum = SumArgs{in.nx, in.ny, area, 1.0 / area, in.face, inH, inC, in.H, in.C, outH, outC, in.rate,
                             k == KIND_P ? (int)SUM_STORE_L : (int)SUM_RK, a0, a1, 0.0, b->d_partial + parts,
-                            b->d_dt + i, 0, 0, 0, -1, in.srcH, in.srcR, in.srcS, nullptr, nullptr, b->d_status + i};
+                            b->d_dt + i, 0, 0, 0, -1, in.srcH, in.srcR, in.srcS, in.cell_area, nullptr, b->d_status + i};
+            if (in.quad) {
+                QuadStageArgs& q = qargs[k][i];
+                q.nx = in.nx; q.ny = in.ny; q.gj0 = 0; q.gny = in.ny;
+                q.H = inH; q.C = inC; q.rec = in.rec; q.flags = in.flags; q.T = in.T; q.phi = in.phi;
+                q.vsn = in.vsn; q.udn = in.udn; q.face = in.face; q.status = b->d_status + i; q.theta = nullptr;
+                q.q = in.qdev;
+                q.src = SourcePtrs{in.cvs_y, in.cud_y, in.srcH, in.srcR, in.srcS};
+            }
         }
-        ax[i] = AxpyArgs{(int)in.N, in.H, in.C, in.LH, in.LC, in.S1H, in.S1C, b->d_dt + i, in.host_tab.area,
-                         b->d_partial + parts};
+        ax[i] = AxpyArgs{(int)in.N, in.H, in.C, in.LH, in.LC, in.S1H, in.S1C, b->d_dt + i, area,
+                         b->d_partial + parts, in.cell_area};
         const bool rk3 = b->opts.integrator == MP_SSPRK3;
         cm[i] = CommitArgs{(int)in.N, rk3 ? in.S1H : in.S2H, rk3 ? in.S1C : in.S2C, in.H, in.C};
-        for (int ty = 0; ty < in.ny; ty += tu.by)
-            for (int tx = 0; tx < in.nx; tx += tu.bx * tu.cpt) wr.push_back(Work{i, tx, ty, 0});
-        for (size_t c = 0; c < in.N; c += 128) wp.push_back(Work{i, (int)c, 0, 0});
-        for (size_t e = 0; e < in.NE; e += 128) wf.push_back(Work{i, (int)e, (int)std::min(in.NE, e + 128), 0});
+        if (in.quad) {
+            // The quad kernels' tiles: 32x4 cells, 128 cells, 128 edges.
+            for (int ty = 0; ty < in.ny; ty += 4)
+                for (int tx = 0; tx < in.nx; tx += 32) wqr.push_back(Work{i, tx, ty, 0});
+            for (size_t c = 0; c < in.N; c += 128) wqp.push_back(Work{i, (int)c, 0, 0});
+            for (size_t e = 0; e < in.NE; e += 128) wqf.push_back(Work{i, (int)e, (int)std::min(in.NE, e + 128), 0});
+        } else {
+            for (int ty = 0; ty < in.ny; ty += tu.by)
+                for (int tx = 0; tx < in.nx; tx += tu.bx * tu.cpt) wr.push_back(Work{i, tx, ty, 0});
+            for (size_t c = 0; c < in.N; c += 128) wp.push_back(Work{i, (int)c, 0, 0});
+            for (size_t e = 0; e < in.NE; e += 128) wf.push_back(Work{i, (int)e, (int)std::min(in.NE, e + 128), 0});
+        }
         for (int s = 0; s < nsum; ++s) ws.push_back(Work{i, s * kSumCells, 0, s});
         parts += nsum;
     }
@@ -395,12 +537,15 @@ mp_status rebuild_args(mp_batch* b, int slots) {
     // Per-slot records live in arrays of b->slots entries (allocated in rebuild).
     const int cap = b->slots;
     for (int k = 0; k < NKIND; ++k) args[k].resize(cap);
+    for (int k = 0; k < NKIND; ++k) qargs[k].resize(cap);
     ax.resize(cap);
     cm.resize(cap);
     part_off.resize(cap, 0);
     part_cnt.resize(cap, 0);
     for (int k = 0; k < NKIND; ++k)
         MP_CUDA(cudaMemcpyAsync(b->d_args[k], args[k].data(), cap * sizeof(InstArgs<R>), cudaMemcpyHostToDevice, s));
+    for (int k = 0; k < NKIND; ++k)
+        MP_CUDA(cudaMemcpyAsync(b->d_qargs[k], qargs[k].data(), cap * sizeof(QuadStageArgs), cudaMemcpyHostToDevice, s));
     MP_CUDA(cudaMemcpyAsync(b->d_axpy, ax.data(), cap * sizeof(AxpyArgs), cudaMemcpyHostToDevice, s));
     MP_CUDA(cudaMemcpyAsync(b->d_commit, cm.data(), cap * sizeof(CommitArgs), cudaMemcpyHostToDevice, s));
     MP_CUDA(cudaMemcpyAsync(b->d_part_off, part_off.data(), cap * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -418,6 +563,16 @@ mp_status rebuild_args(mp_batch* b, int slots) {
     MP_CUDA(cudaMemcpyAsync(b->d_wphase, wp.data(), wp.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
     MP_CUDA(cudaMemcpyAsync(b->d_wface, wf.data(), wf.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
     MP_CUDA(cudaMemcpyAsync(b->d_wsum, ws.data(), ws.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+    if (b->has_quads) {
+        b->n_wqrec = (int)wqr.size(); b->n_wqphase = (int)wqp.size(); b->n_wqface = (int)wqf.size();
+        MP_TRY(grow(&b->d_wqrec, b->cap_wqrec, b->n_wqrec, s, &grown));
+        MP_TRY(grow(&b->d_wqphase, b->cap_wqphase, b->n_wqphase, s, &grown));
+        MP_TRY(grow(&b->d_wqface, b->cap_wqface, b->n_wqface, s, &grown));
+        wqr.resize(b->cap_wqrec, pad); wqp.resize(b->cap_wqphase, pad); wqf.resize(b->cap_wqface, pad);
+        MP_CUDA(cudaMemcpyAsync(b->d_wqrec, wqr.data(), wqr.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+        MP_CUDA(cudaMemcpyAsync(b->d_wqphase, wqp.data(), wqp.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+        MP_CUDA(cudaMemcpyAsync(b->d_wqface, wqf.data(), wqf.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+    }
     if (grown) b->gen += 1;
     MP_CUDA(cudaStreamSynchronize(s));   // host vectors go out of scope
     return MP_OK;
@@ -432,7 +587,7 @@ mp_status rebuild(mp_batch* b) {
     if (slots > b->slots || b->slots == 0) {
         for (void* p : {(void*)b->d_active, (void*)b->d_part_off, (void*)b->d_part_cnt, (void*)b->d_tot,
                         (void*)b->d_status, (void*)b->d_dt, (void*)b->d_axpy, (void*)b->d_commit, b->d_args[0],
-                        b->d_args[1], b->d_args[2]})
+                        b->d_args[1], b->d_args[2], b->d_qargs[0], b->d_qargs[1], b->d_qargs[2]})
             if (p) cudaFreeAsync(p, s);
         if (b->h_tot) cudaFreeHost(b->h_tot);
         if (b->h_status) cudaFreeHost(b->h_status);
@@ -450,6 +605,7 @@ mp_status rebuild(mp_batch* b) {
         MP_CUDA(cudaMallocAsync((void**)&b->d_axpy, cap * sizeof(AxpyArgs), s));
         MP_CUDA(cudaMallocAsync((void**)&b->d_commit, cap * sizeof(CommitArgs), s));
         for (int k = 0; k < NKIND; ++k) MP_CUDA(cudaMallocAsync(&b->d_args[k], cap * sizeof(InstArgs<double>), s));
+        for (int k = 0; k < NKIND; ++k) MP_CUDA(cudaMallocAsync(&b->d_qargs[k], cap * sizeof(QuadStageArgs), s));
         MP_CUDA(cudaMallocHost((void**)&b->h_tot, cap * sizeof(Totals)));
         MP_CUDA(cudaMallocHost((void**)&b->h_status, cap * sizeof(unsigned long long)));
         MP_CUDA(cudaMallocHost((void**)&b->h_dt, cap * sizeof(double)));
@@ -491,6 +647,18 @@ void launch_kind(mp_batch* b, int kind) {
     timed(b, 2, [&] { batch_face_kernel<R><<<b->cap_wface, 128, 0, s>>>(args, b->d_wface, b->d_active, b->ph); });
     if (b->ph.diffusion)
         timed(b, 2, [&] { batch_diffusion_kernel<R><<<b->cap_wface, 128, 0, s>>>(args, b->d_wface, b->d_active, b->ph); });
+    if (b->has_quads) {
+        // General quad meshes: reconstruction, limiter, cell phase (the wet
+        // flags the faces read), faces; the sums below cover every instance.
+        const QuadStageArgs* qa = static_cast<const QuadStageArgs*>(b->d_qargs[kind]);
+        timed(b, 0, [&] { batch_quad_weno_kernel<<<b->cap_wqrec, dim3(32, 4), 0, s>>>(qa, b->d_wqrec, b->d_active); });
+        timed(b, 0, [&] { batch_quad_limit_kernel<<<b->cap_wqrec, dim3(32, 4), 0, s>>>(qa, b->d_wqrec, b->d_active, b->ph); });
+        timed(b, 1, [&] { batch_quad_phase_kernel<<<b->cap_wqphase, 128, 0, s>>>(qa, b->d_wqphase, b->d_active, b->ph); });
+        timed(b, 2, [&] { batch_quad_face_kernel<<<b->cap_wqface, 128, 0, s>>>(qa, b->d_wqface, b->d_active, b->ph); });
+        if (b->ph.diffusion)
+            timed(b, 2, [&] { batch_quad_diffusion_kernel<<<b->cap_wqface, 128, 0, s>>>(qa, b->d_wqface, b->d_active, b->ph); });
+        count_launch(b->ph.diffusion ? 5 : 4);
+    }
     if (b->ph.source) timed(b, 3, [&] { batch_sum_kernel<R, true><<<b->cap_wsum, kRedBlock, 0, s>>>(args, b->d_wsum, b->d_active); });
     else timed(b, 3, [&] { batch_sum_kernel<R, false><<<b->cap_wsum, kRedBlock, 0, s>>>(args, b->d_wsum, b->d_active); });
     timed(b, 4, [&] { batch_reduce_kernel<<<b->slots, 1024, 0, s>>>(b->d_partial, b->d_part_off, b->d_part_cnt, b->d_active, b->d_tot); });
@@ -843,7 +1011,7 @@ mp_status ensure_graph(mp_batch* b) {
     }
     if (b->graph_exec && b->graph_gen == b->gen) return MP_OK;
     release_graph(b);
-    b->stage_kernels = 5 + (b->ph.diffusion ? 1 : 0);
+    b->stage_kernels = 5 + (b->ph.diffusion ? 1 : 0) + (b->has_quads ? (b->ph.diffusion ? 5 : 4) : 0);
     // Capture on a private stream (the caller's may be the legacy default
     // stream, which cannot be captured); the graph runs on the caller's.
     cudaStream_t cap = nullptr;
@@ -964,13 +1132,19 @@ extern "C" void mp_batch_destroy(mp_batch* b) {
     mp::release_graph(b);
     for (void* p : {(void*)b->d_ctl, (void*)b->d_hdr, (void*)b->d_rep, (void*)b->d_commit}) if (p) cudaFreeAsync(p, b->stream);
     for (void* p : {(void*)b->h_ctl, (void*)b->h_hdr, (void*)b->h_rep}) if (p) cudaFreeHost(p);
-    for (MPInstance& in : b->inst) if (in.used && in.arena) cudaFreeAsync(in.arena, b->stream);
+    for (MPInstance& in : b->inst) {
+        if (in.used && in.arena) cudaFreeAsync(in.arena, b->stream);
+        if (in.used && in.src_arena) cudaFreeAsync(in.src_arena, b->stream);
+    }
     for (int k = 0; k < mp::NKIND; ++k) if (b->d_args[k]) cudaFreeAsync(b->d_args[k], b->stream);
+    for (int k = 0; k < mp::NKIND; ++k) if (b->d_qargs[k]) cudaFreeAsync(b->d_qargs[k], b->stream);
+    for (void* p : {(void*)b->d_wqrec, (void*)b->d_wqphase, (void*)b->d_wqface}) if (p) cudaFreeAsync(p, b->stream);
     for (void* p : {(void*)b->d_axpy, (void*)b->d_wrecon, (void*)b->d_wphase, (void*)b->d_wface, (void*)b->d_wsum,
                     (void*)b->d_active, (void*)b->d_part_off, (void*)b->d_part_cnt, (void*)b->d_partial,
                     (void*)b->d_tot, (void*)b->d_status, (void*)b->d_dt})
         if (p) cudaFreeAsync(p, b->stream);
     cudaStreamSynchronize(b->stream);
+    for (MPInstance& in : b->inst) if (in.used && in.qbuf) cudaFree(in.qbuf);
     if (b->h_tot) cudaFreeHost(b->h_tot);
     if (b->h_status) cudaFreeHost(b->h_status);
     if (b->h_dt) cudaFreeHost(b->h_dt);
@@ -994,6 +1168,22 @@ extern "C" mp_status mp_batch_add(mp_batch* b, const mp_mesh_desc* mesh, int* in
     for (int i = 0; i < (int)b->inst.size(); ++i) if (!b->inst[i].used) { slot = i; break; }
     if (slot < 0) { slot = (int)b->inst.size(); b->inst.emplace_back(); }
     MP_TRY(mp::alloc_instance(b, b->inst[slot], *mesh));
+    *instance = slot;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_batch_add_quads(mp_batch* b, const mp_mesh_desc* mesh, const double* xy, int* instance) {
+    if (!b || !mesh || !xy || !instance) { mp::set_error("null argument"); return MP_ERR_ARG_WRONG; }
+    if (mesh->nx < 2 || mesh->ny < 2) { mp::set_error("Transport requires at least 2x2 cells"); return MP_ERR_ARG_SIZ; }
+    if (mp::mesh_too_large(mesh->nx, mesh->ny)) { mp::set_error("mesh has 2^31 edges or more"); return MP_ERR_ARG_SIZ; }
+    int slot = -1;
+    for (int i = 0; i < (int)b->inst.size(); ++i) if (!b->inst[i].used) { slot = i; break; }
+    if (slot < 0) { slot = (int)b->inst.size(); b->inst.emplace_back(); }
+    const mp_status st = mp::alloc_quad_instance(b, b->inst[slot], *mesh, xy);
+    if (st != MP_OK) {
+        if (slot == (int)b->inst.size() - 1 && !b->inst[slot].used) b->inst.pop_back();
+        return st;
+    }
     *instance = slot;
     return MP_OK;
 }

@@ -32,6 +32,25 @@ struct SourcePtrs {
     double* srcS = nullptr;
 };
 
+// Everything one stage of one quad mesh reads and writes (the single-mesh
+// launch passes it by value; the batched launch reads one per instance).
+struct QuadStageArgs {
+    int nx = 0, ny = 0, gj0 = 0, gny = 0;   // local rows; local row 0 is global row gj0 of gny
+    const double* H = nullptr;              // stage input
+    const double* C = nullptr;
+    double* rec = nullptr;                  // 18 * ncell deviation coefficients
+    unsigned char* flags = nullptr;
+    double* T = nullptr;
+    double* phi = nullptr;
+    const double* vsn = nullptr;            // [edge*5 + q], canonical
+    const double* udn = nullptr;
+    double* face = nullptr;                 // 4 * nedge: fluxH, fluxC, rate, fluxMixture
+    unsigned long long* status = nullptr;
+    double* theta = nullptr;                // optional limiter factors (2 * ncell)
+    QuadDev q{};
+    SourcePtrs src{};
+};
+
 // ------------------------------------------------------------------ kernels
 
 // Reconstruction (Reconstruction::Update, src/mlweno/reconstruction.cpp:
@@ -39,13 +58,13 @@ struct SourcePtrs {
 // for both fields: the unlimited deviation polynomials into rec. The limiter runs in the next kernel, so that neither
 // kernel holds both the table-driven weights and the point scan in
 // registers (the table reads need many warps in flight).
-__global__ void __launch_bounds__(128, 3) quad_weno_kernel(int nx, int ny, const double* __restrict__ H,
-                                                           const double* __restrict__ C, double* __restrict__ rec,
-                                                           unsigned long long* status, QuadDev q, int gj0, int gny,
-                                                           int jlo, int jhi, const int* gate) {
-    if (gated_off(gate)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = jlo + (int)(blockIdx.y * blockDim.y + threadIdx.y);
-    if (i >= nx || j >= jhi) return;
+__device__ __forceinline__ void quad_weno_cell(const QuadStageArgs& a, int i, int j) {
+    const int nx = a.nx, ny = a.ny, gj0 = a.gj0, gny = a.gny;
+    const double* __restrict__ H = a.H;
+    const double* __restrict__ C = a.C;
+    unsigned long long* status = a.status;
+    const QuadDev& q = a.q;
+    double* __restrict__ rec = a.rec;
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
     const int gj = gj0 + j;
@@ -69,18 +88,26 @@ __global__ void __launch_bounds__(128, 3) quad_weno_kernel(int nx, int ny, const
     }
     if (st) record_error(status, PART_UPDATE, cell + (long long)gj0 * nx, st);
 }
+__global__ void __launch_bounds__(128, 3) quad_weno_kernel(const __grid_constant__ QuadStageArgs a, int jlo, int jhi,
+                                                           const int* gate) {
+    if (gated_off(gate)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = jlo + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    if (i >= a.nx || j >= jhi) return;
+    quad_weno_cell(a, i, j);
+}
 
 // Limiter over the cell's own limiter points (state_reconstruction.cpp:
 // 136-192): theta of H and C from the unlimited polynomials in rec, which
 // are scaled in place.
-__global__ void __launch_bounds__(128, 4) quad_limit_kernel(int nx, int ny, const double* __restrict__ H,
-                                                         const double* __restrict__ C, double* __restrict__ rec,
-                                                         unsigned char* __restrict__ flags, unsigned long long* status,
-                                                         double* theta, Physics ph, QuadDev q, int gj0, int gny,
-                                                         int jlo, int jhi, const int* gate) {
-    if (gated_off(gate)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = jlo + (int)(blockIdx.y * blockDim.y + threadIdx.y);
-    if (i >= nx || j >= jhi) return;
+__device__ __forceinline__ void quad_limit_cell(const QuadStageArgs& a, const Physics& ph, int i, int j) {
+    const int nx = a.nx, ny = a.ny, gj0 = a.gj0, gny = a.gny;
+    const double* __restrict__ H = a.H;
+    const double* __restrict__ C = a.C;
+    unsigned long long* status = a.status;
+    const QuadDev& q = a.q;
+    double* __restrict__ rec = a.rec;
+    unsigned char* __restrict__ flags = a.flags;
+    double* theta = a.theta;
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
     const CellFrame f = cell_frame(q, nx, N, cell);
@@ -143,19 +170,29 @@ __global__ void __launch_bounds__(128, 4) quad_limit_kernel(int nx, int ny, cons
     flags[cell] = safe ? 0 : FLAG_CHECK;
     if (st_lim) record_error(status, PART_LIMIT, cell + (long long)gj0 * nx, st_lim);
 }
+__global__ void __launch_bounds__(128, 4) quad_limit_kernel(const __grid_constant__ QuadStageArgs a, Physics ph, int jlo,
+                                                         int jhi, const int* gate) {
+    if (gated_off(gate)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = jlo + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    if (i >= a.nx || j >= jhi) return;
+    quad_limit_cell(a, ph, i, j);
+}
+
 
 // 5x5 cell quadrature of T and phi on the bilinear map, wet flag, adiabatic
 // source, and the exact check of the diffusion samples when flagged.
-__global__ void __launch_bounds__(128, 4) quad_cellphase_kernel(int nx, int ny, const double* __restrict__ H,
-                                                             const double* __restrict__ C, const double* __restrict__ rec,
-                                                             unsigned char* __restrict__ flags, double* __restrict__ T,
-                                                             double* __restrict__ phi, unsigned long long* status,
-                                                             Physics ph, QuadDev q, SourcePtrs src, int gj0, int gny,
-                                                             long long c0, long long c1, const int* gate) {
-    if (gated_off(gate)) return;
+__device__ __forceinline__ void quad_cellphase_cell(const QuadStageArgs& a, const Physics& ph, long long cell) {
+    const int nx = a.nx, ny = a.ny, gj0 = a.gj0, gny = a.gny;
+    const double* __restrict__ H = a.H;
+    const double* __restrict__ C = a.C;
+    unsigned long long* status = a.status;
+    const QuadDev& q = a.q;
+    const double* __restrict__ rec = a.rec;
+    unsigned char* __restrict__ flags = a.flags;
+    double* __restrict__ T = a.T;
+    double* __restrict__ phi = a.phi;
+    const SourcePtrs& src = a.src;
     const long long N = (long long)nx * ny;
-    const long long cell = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= c1) return;
     const int i = (int)(cell % nx), j = (int)(cell / nx);
     const CellFrame f = cell_frame(q, nx, (size_t)N, cell);
     const double mH = __ldg(H + cell), mC = __ldg(C + cell);
@@ -208,6 +245,14 @@ __global__ void __launch_bounds__(128, 4) quad_cellphase_kernel(int nx, int ny, 
     phi[cell] = Psum;
     if (ph.source) { src.srcH[cell] = Ssum; src.srcR[cell] = Rsum; src.srcS[cell] = Wsum; }
 }
+__global__ void __launch_bounds__(128, 4) quad_cellphase_kernel(const __grid_constant__ QuadStageArgs a, Physics ph,
+                                                             long long c0, long long c1, const int* gate) {
+    if (gated_off(gate)) return;
+    const long long cell = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= c1) return;
+    quad_cellphase_cell(a, ph, cell);
+}
+
 
 struct Side {
     double cx, cy, inv_h, mH, mC;
@@ -229,18 +274,18 @@ __device__ __forceinline__ void side_values(const Side& s, P2 p, double& h, doub
 }
 
 // Face fluxes, edge porosity and rate of one edge at its 5 Gauss points.
-__global__ void __launch_bounds__(128, 4) quad_face_kernel(int nx, int ny, const double* __restrict__ H,
-                                                        const double* __restrict__ C, const double* __restrict__ rec,
-                                                        const unsigned char* __restrict__ flags,
-                                                        const double* __restrict__ vsn, const double* __restrict__ udn,
-                                                        double* __restrict__ face, unsigned long long* status,
-                                                        Physics ph, QuadDev q, int gj0, int gny, long long h0,
-                                                        long long nh, long long v0, long long nv, const int* gate) {
-    if (gated_off(gate)) return;
+__device__ __forceinline__ void quad_face_edge(const QuadStageArgs& a, const Physics& ph, long long e) {
+    const int nx = a.nx, ny = a.ny, gj0 = a.gj0, gny = a.gny;
+    const double* __restrict__ H = a.H;
+    const double* __restrict__ C = a.C;
+    unsigned long long* status = a.status;
+    const QuadDev& q = a.q;
+    const double* __restrict__ rec = a.rec;
+    const unsigned char* __restrict__ flags = a.flags;
+    const double* __restrict__ vsn = a.vsn;
+    const double* __restrict__ udn = a.udn;
+    double* __restrict__ face = a.face;
     const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
-    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nh + nv) return;
-    const long long e = k < nh ? h0 + k : v0 + (k - nh);
     const size_t N = (size_t)nx * ny;
     const QuadEdge g = quad_edge(q, nx, ny, gj0, gny, e);
     double len;
@@ -285,21 +330,28 @@ __global__ void __launch_bounds__(128, 4) quad_face_kernel(int nx, int ny, const
     face[2 * nE + e] = rate;
     face[3 * nE + e] = fluxMix;
 }
+__global__ void __launch_bounds__(128, 4) quad_face_kernel(const __grid_constant__ QuadStageArgs a, Physics ph,
+                                                        long long h0, long long nh, long long v0, long long nv,
+                                                        const int* gate) {
+    if (gated_off(gate)) return;
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nh + nv) return;
+    quad_face_edge(a, ph, k < nh ? h0 + k : v0 + (k - nh));
+}
+
 
 // Diffusive H flux and rate of one edge (diffusiveflux.cpp:105-200 through
 // evolve.cpp:330-347): temperatures of the limited states at the normal-line
 // samples, spacing per edge point.
-__global__ void __launch_bounds__(128) quad_diffusion_kernel(int nx, int ny, const double* __restrict__ H,
-                                                             const double* __restrict__ C,
-                                                             const double* __restrict__ rec, double* __restrict__ face,
-                                                             unsigned long long* status, Physics ph, QuadDev q,
-                                                             int gj0, int gny, long long h0, long long nh, long long v0,
-                                                             long long nv, const int* gate) {
-    if (gated_off(gate)) return;
+__device__ __forceinline__ void quad_diffusion_edge(const QuadStageArgs& a, const Physics& ph, long long e) {
+    const int nx = a.nx, ny = a.ny, gj0 = a.gj0, gny = a.gny;
+    const double* __restrict__ H = a.H;
+    const double* __restrict__ C = a.C;
+    unsigned long long* status = a.status;
+    const QuadDev& q = a.q;
+    const double* __restrict__ rec = a.rec;
+    double* __restrict__ face = a.face;
     const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
-    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nh + nv) return;
-    const long long e = k < nh ? h0 + k : v0 + (k - nh);
     const size_t N = (size_t)nx * ny;
     const QuadEdge g = quad_edge(q, nx, ny, gj0, gny, e);
     const int type = g.boundary ? ph.wall_type[g.wall] : 1;
@@ -355,6 +407,15 @@ __global__ void __launch_bounds__(128) quad_diffusion_kernel(int nx, int ny, con
     face[e] += integral;
     face[2 * nE + e] = rate;
 }
+__global__ void __launch_bounds__(128) quad_diffusion_kernel(const __grid_constant__ QuadStageArgs a, Physics ph,
+                                                             long long h0, long long nh, long long v0, long long nv,
+                                                             const int* gate) {
+    if (gated_off(gate)) return;
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nh + nv) return;
+    quad_diffusion_edge(a, ph, k < nh ? h0 + k : v0 + (k - nh));
+}
+
 
 // Reconstruction, limiter, cell phase, faces (+ diffusion) of state (H, C)
 // on a general quad mesh; the accumulation is the shared sum kernel. Local
@@ -367,18 +428,21 @@ void launch_quad_stage(const QuadDev& q, int nx, int ny, int gj0, int gny, int r
                        double* rec, unsigned char* flags, double* T, double* phi, const double* vsn, const double* udn,
                        double* face, unsigned long long* status, double* theta, const SourcePtrs& src,
                        cudaStream_t s, const int* gate = nullptr) {
+    QuadStageArgs a;
+    a.nx = nx; a.ny = ny; a.gj0 = gj0; a.gny = gny;
+    a.H = H; a.C = C; a.rec = rec; a.flags = flags; a.T = T; a.phi = phi;
+    a.vsn = vsn; a.udn = udn; a.face = face; a.status = status; a.theta = theta;
+    a.q = q; a.src = src;
     dim3 blk(32, 4), grd((nx + 31) / 32, (rec1 - rec0 + 3) / 4);
-    quad_weno_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, status, q, gj0, gny, rec0, rec1, gate);
-    quad_limit_kernel<<<grd, blk, 0, s>>>(nx, ny, H, C, rec, flags, status, theta, ph, q, gj0, gny, rec0, rec1, gate);
+    quad_weno_kernel<<<grd, blk, 0, s>>>(a, rec0, rec1, gate);
+    quad_limit_kernel<<<grd, blk, 0, s>>>(a, ph, rec0, rec1, gate);
     const long long c0 = (long long)rec0 * nx, c1 = (long long)rec1 * nx;
-    quad_cellphase_kernel<<<(unsigned)((c1 - c0 + 127) / 128), 128, 0, s>>>(nx, ny, H, C, rec, flags, T, phi, status,
-                                                                            ph, q, src, gj0, gny, c0, c1, gate);
+    quad_cellphase_kernel<<<(unsigned)((c1 - c0 + 127) / 128), 128, 0, s>>>(a, ph, c0, c1, gate);
     const unsigned ge = (unsigned)((nh + nv + 127) / 128);
-    quad_face_kernel<<<ge, 128, 0, s>>>(nx, ny, H, C, rec, flags, vsn, udn, face, status, ph, q, gj0, gny, h0, nh, v0,
-                                        nv, gate);
+    quad_face_kernel<<<ge, 128, 0, s>>>(a, ph, h0, nh, v0, nv, gate);
     count_launch(4);
     if (ph.diffusion) {
-        quad_diffusion_kernel<<<ge, 128, 0, s>>>(nx, ny, H, C, rec, face, status, ph, q, gj0, gny, h0, nh, v0, nv, gate);
+        quad_diffusion_kernel<<<ge, 128, 0, s>>>(a, ph, h0, nh, v0, nv, gate);
         count_launch();
     }
 }

@@ -141,3 +141,104 @@ def test_batch_source_needs_cell_velocities(cuda_lib):
     with pytest.raises(MPError) as err:
         b.step(1)
     assert err.value.code == 73
+
+
+QUADS = [(sy.Workload(nx=20, ny=24, seed=5), sy.MESH_PERTURBED, 0.2),
+         (sy.Workload(nx=16, ny=20, seed=6, psi_amplitude=0.15), sy.MESH_SINE_STRETCHED, 0.0),
+         (sy.Workload(nx=7, ny=9, seed=8), sy.MESH_PERTURBED, 0.1)]
+
+
+def solo_quads(w, xy, cfg, steps, kappa_bc=None):
+    from mantlepar_b200.transport import Transport
+    t = Transport(w, cfg, vertices=xy)
+    if kappa_bc:
+        t.set_thermal_bc(*kappa_bc)
+    t.set_face_velocity(*sy.face_velocity_quads(w, xy))
+    t.set_state(*sy.initial_state(w))
+    _, reps = t.step(steps)
+    out = t.get_state(), reps
+    t.close()
+    return out
+
+
+@pytest.mark.parametrize("integ,device_steps,kappa", [(3, True, 0.0), (2, True, 0.0), (3, False, 0.0),
+                                                      (3, True, 0.02)])
+def test_batch_with_quad_instances_equals_solo_bitwise(cuda_lib, integ, device_steps, kappa):
+    """General quad meshes (perturbed, sine-stretched) in one batch with
+    uniform meshes: every instance equals its own single-mesh run bit for bit
+    (states, dt, retries, balance), through the step graph and the host loop,
+    with diffusion too."""
+    from mantlepar_b200.batch import Batch
+    from mantlepar_b200.transport import TransportConfig
+    cfg = TransportConfig(cfl=0.4, integrator=integ, diffusivity=kappa)
+    bc = None          # zero-flux walls: the diffusion runs on the interior edges
+    uni = WORKLOADS[:2]
+    b = Batch(uni, cfg)
+    b.set_device_steps(device_steps)
+    if bc:
+        b.set_thermal_bc(*bc)
+    for i, w in enumerate(uni):
+        b.set_face_velocity(i, *sy.face_velocity(w))
+        b.set_state(i, *sy.initial_state(w))
+    slots = {}
+    for k, (w, fam, pert) in enumerate(QUADS):
+        xy = sy.quad_vertices(w, fam, pert, seed=21 + k)
+        i = b.add_quads(w, xy)
+        b.set_face_velocity(i, *sy.face_velocity_quads(w, xy))
+        b.set_state(i, *sy.initial_state(w))
+        slots[i] = (w, xy)
+    reps = b.step(40)
+    for i, (w, xy) in slots.items():
+        (H, C, T, phi), sreps = solo_quads(w, xy, cfg, 40, bc)
+        got = b.get_state(i)
+        assert got["status"] == 0 and got["accepted"] == 40
+        for a, x in ((got["H"], H), (got["C"], C), (got["T"], T), (got["phi"], phi)):
+            assert np.array_equal(a, x)
+        assert [r[i]["retries"] for r in reps] == [r["retries"] for r in sreps]
+        assert [r[i]["dt"] for r in reps] == [r["dt"] for r in sreps]
+        assert [r[i]["balanceH"] for r in reps] == [r["balanceH"] for r in sreps]
+    if not bc:
+        for i, w in enumerate(uni):
+            (H, C, T, phi), _ = solo(w, cfg, 40)
+            got = b.get_state(i)
+            assert np.array_equal(got["H"], H) and np.array_equal(got["phi"], phi)
+    b.close()
+
+
+def test_batch_quad_instances_come_and_go(cuda_lib):
+    """A folded quad mesh is refused (MP_ERR_ARG_WRONG, no instance); quad
+    instances removed and added again between steps leave the others' results
+    equal to their solo runs, and re-use the captured step graph."""
+    from mantlepar_b200._capi import MPError
+    from mantlepar_b200.batch import Batch
+    from mantlepar_b200.transport import TransportConfig
+    cfg = TransportConfig(cfl=0.4, integrator=3)
+    w0, fam0, p0 = QUADS[0]
+    xy0 = sy.quad_vertices(w0, fam0, p0, seed=21)
+    b = Batch([WORKLOADS[0]], cfg)
+    b.set_face_velocity(0, *sy.face_velocity(WORKLOADS[0]))
+    b.set_state(0, *sy.initial_state(WORKLOADS[0]))
+    wb = sy.Workload(nx=4, ny=4)
+    bad = sy.quad_vertices(wb, sy.MESH_RECTANGULAR).reshape(5, 5, 2).copy()
+    bad[2, 2] = bad[3, 3] + [0.01, 0.01]
+    with pytest.raises(MPError) as err:
+        b.add_quads(wb, bad.reshape(-1))
+    assert err.value.code == 62
+    q = b.add_quads(w0, xy0)
+    b.set_face_velocity(q, *sy.face_velocity_quads(w0, xy0))
+    b.set_state(q, *sy.initial_state(w0))
+    b.step(10)
+    captures = b.graph_captures()
+    b.remove(q)
+    q2 = b.add_quads(w0, xy0)
+    b.set_face_velocity(q2, *sy.face_velocity_quads(w0, xy0))
+    b.set_state(q2, *sy.initial_state(w0))
+    b.step(10)
+    assert b.graph_captures() == captures
+    (H, C, T, phi), _ = solo_quads(w0, xy0, cfg, 10)
+    got = b.get_state(q2)
+    assert got["status"] == 0 and np.array_equal(got["H"], H) and np.array_equal(got["phi"], phi)
+    (H, C, T, phi), _ = solo(WORKLOADS[0], cfg, 20)
+    got = b.get_state(0)
+    assert np.array_equal(got["H"], H) and np.array_equal(got["phi"], phi)
+    b.close()
