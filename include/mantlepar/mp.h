@@ -193,7 +193,8 @@ void mp_transport_destroy(mp_transport* t);
  * mesh gives nx, ny and the domain. Every cell gets its own reconstruction
  * tables (built at create, TensorStencilPoly::Initialize and
  * SetTargetSmoothness per stencil, src/mlweno/tensorstencilpoly.cpp:146-231,
- * 383-398) and every evaluation point its own geometry. FP64 only; cells
+ * 383-398) and every evaluation point its own geometry. FP64 (the mixed
+ * form evaluates the same FP64 stage); cells
  * failing the reference's quad check (src/core/quad_validation.h) ->
  * MP_ERR_ARG_WRONG. All other mp_transport_* calls apply unchanged; row
  * slabs: mp_transport_create_quads_slab. */
@@ -511,10 +512,10 @@ mp_status mp_serve_submit(mp_server* s, const mp_mesh_desc* mesh, const double* 
 /* A request on a general quad mesh (the vertices xy as
  * mp_transport_create_quads; the perturbed-quadrilateral and stretched
  * families of src/core/mesh.cpp:27-55). It is admitted under the same budget
- * and resident-cell target, and advanced one step per loop iteration beside
- * the batched uniform-mesh requests by a transport of its own (per-cell
- * tables built on admission). A mesh failing the quad check finishes with
- * MP_ERR_ARG_WRONG in its status; the server continues. */
+ * and resident-cell target and joins the same batch as a quad instance
+ * (mp_batch_add_quads: per-cell tables built on admission), advanced with
+ * the others one step per loop iteration. A mesh failing the quad check
+ * finishes with MP_ERR_ARG_WRONG in its status; the server continues. */
 mp_status mp_serve_submit_quads(mp_server* s, const mp_mesh_desc* mesh, const double* xy, const double* H,
                                 const double* C, const double* vs_n, const double* ud_n, double t_final,
                                 long long* id);

@@ -15,9 +15,8 @@
 // GPU joins at the next step. A request leaves when it reaches its final time
 // or fails; its result is copied out and its memory freed for the queue.
 // State stays resident on the device between steps. A request on a general
-// quad mesh gets a transport of its own (per-cell tables, quad_kernels.cuh),
-// admitted under the same budget and target and stepped once per loop
-// iteration after the batch's step, on the same stream.
+// quad mesh joins the same batch as a quad instance (per-cell tables built
+// on admission, its stage kernels batched over the quad instances).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,6 +34,7 @@
 #include "common.hpp"
 
 extern "C" {
+mp_status mp_batch_add_quads(mp_batch* b, const mp_mesh_desc* mesh, const double* xy, int* instance);
 mp_status mp_batch_create(const mp_mesh_desc* meshes, int count, const mp_transport_opts* opts, mp_stream_t stream,
                           mp_batch** out);
 void mp_batch_destroy(mp_batch* b);
@@ -66,9 +66,8 @@ struct Request {
     double work = 0;                       // admission-order estimate
     Clock::time_point submitted, admitted, finished;
     int slot = -1;
-    bool quad = false;                     // general quad mesh: own transport
+    bool quad = false;                     // general quad mesh
     std::vector<double> xy;                // its vertices until admission
-    mp_transport* t = nullptr;
     int status = 0;
     int accepted = 0;
     double time = 0;
@@ -93,7 +92,6 @@ struct mp_server {
     int order = MP_SERVE_SMALLEST_WORK;
     double resident_target = 1.0e6;        // cells; 0 = no limit
     double resident_cells = 0;
-    size_t quad_bytes = 0;                 // device bytes of the quad-mesh transports
     bool stop = false;
     mp_status fatal = MP_OK;
     std::string fatal_msg;
@@ -123,33 +121,24 @@ void admit(mp_server* s) {
                 for (auto it = s->queue.begin(); it != s->queue.end(); ++it)
                     if ((*it)->work < (*pick)->work) pick = it;
             r = *pick;
-            if (mp_batch_bytes_in_use(s->batch) + s->quad_bytes + r->bytes > s->budget) return;
+            if (mp_batch_bytes_in_use(s->batch) + r->bytes > s->budget) return;
             s->queue.erase(pick);
         }
         int slot = -1;
-        mp_status st;
-        if (r->quad) {
-            st = mp_transport_create_quads(&r->mesh, r->xy.data(), &s->opts, (mp_stream_t)s->stream, &r->t);
-            if (st == MP_OK) st = mp_transport_set_face_velocity(r->t, r->vs.data(), r->ud.data());
-            if (st == MP_OK) st = mp_transport_set_state(r->t, r->H.data(), r->C.data(), 0.0);
-            if (st == MP_OK) st = mp_transport_set_time_control(r->t, MP_TIME_CFL, r->t_final);
-        } else {
-            st = mp_batch_add(s->batch, &r->mesh, &slot);
-            if (st == MP_OK) st = mp_batch_set_face_velocity(s->batch, slot, r->vs.data(), r->ud.data());
-            if (st == MP_OK) st = mp_batch_set_state(s->batch, slot, r->H.data(), r->C.data(), 0.0);
-            if (st == MP_OK) st = mp_batch_set_end_time(s->batch, slot, r->t_final);
-        }
+        mp_status st = r->quad ? mp_batch_add_quads(s->batch, &r->mesh, r->xy.data(), &slot)
+                               : mp_batch_add(s->batch, &r->mesh, &slot);
+        if (st == MP_OK) st = mp_batch_set_face_velocity(s->batch, slot, r->vs.data(), r->ud.data());
+        if (st == MP_OK) st = mp_batch_set_state(s->batch, slot, r->H.data(), r->C.data(), 0.0);
+        if (st == MP_OK) st = mp_batch_set_end_time(s->batch, slot, r->t_final);
         r->admitted = Clock::now();
         if (st != MP_OK) {
             if (slot >= 0) mp_batch_remove(s->batch, slot);
-            if (r->t) { mp_transport_destroy(r->t); r->t = nullptr; }
             std::lock_guard<std::mutex> g(s->m);
             r->status = st; r->done = true; r->finished = Clock::now();
             s->cv_done.notify_all();
             continue;
         }
         r->slot = slot;
-        if (r->quad) s->quad_bytes += r->bytes;
         s->resident_cells += (double)r->cells;
         r->H.clear(); r->H.shrink_to_fit(); r->C.clear(); r->C.shrink_to_fit();
         r->vs.clear(); r->vs.shrink_to_fit(); r->ud.clear(); r->ud.shrink_to_fit();
@@ -163,27 +152,6 @@ void admit(mp_server* s) {
 void retire(mp_server* s) {
     std::vector<std::shared_ptr<Request>> keep;
     for (auto& r : s->active) {
-        if (r->quad) {
-            double time = 0;
-            int acc = 0;
-            const mp_status tg = mp_transport_get_time(r->t, &time, &acc);
-            if (tg != MP_OK && !r->status) r->status = tg;
-            if (!r->status && time < r->t_final) { keep.push_back(r); continue; }
-            r->oH.resize(r->cells); r->oC.resize(r->cells); r->oT.resize(r->cells); r->oP.resize(r->cells);
-            const mp_status gs = mp_transport_get_state(r->t, r->oH.data(), r->oC.data(), r->oT.data(), r->oP.data());
-            if (gs != MP_OK && !r->status) r->status = gs;
-            r->time = time;
-            r->accepted = acc;
-            mp_transport_destroy(r->t);
-            r->t = nullptr;
-            std::lock_guard<std::mutex> g(s->m);
-            s->quad_bytes -= r->bytes;
-            s->resident_cells -= (double)r->cells;
-            r->finished = Clock::now();
-            r->done = true;
-            s->cv_done.notify_all();
-            continue;
-        }
         double time = 0;
         int acc = 0, status = 0;
         mp_batch_get_state(s->batch, r->slot, nullptr, nullptr, nullptr, nullptr, &time, &acc, &status);
@@ -214,25 +182,10 @@ void run(mp_server* s) {
         if (s->active.empty()) continue;
         // Cell-updates of this step: one per cell of every request that accepts it.
         std::vector<int> before(s->active.size());
-        bool batched = false;
-        for (size_t k = 0; k < s->active.size(); ++k) {
-            const auto& r = s->active[k];
-            if (r->quad) mp_transport_get_time(r->t, nullptr, &before[k]);
-            else {
-                batched = true;
-                mp_batch_get_state(s->batch, r->slot, nullptr, nullptr, nullptr, nullptr, nullptr, &before[k], nullptr);
-            }
-        }
+        for (size_t k = 0; k < s->active.size(); ++k)
+            mp_batch_get_state(s->batch, s->active[k]->slot, nullptr, nullptr, nullptr, nullptr, nullptr, &before[k], nullptr);
         const auto a = Clock::now();
-        const mp_status st = batched ? mp_batch_step(s->batch, 1, nullptr) : MP_OK;
-        // Quad-mesh requests: one step each; a failure ends that request only
-        // (its state is rolled back to the last accepted step).
-        if (st == MP_OK)
-            for (auto& r : s->active)
-                if (r->quad && !r->status) {
-                    const mp_status qs = mp_transport_step(r->t, 1, nullptr);
-                    if (qs != MP_OK) r->status = qs;
-                }
+        const mp_status st = mp_batch_step(s->batch, 1, nullptr);
         const auto b = Clock::now();
         if (st != MP_OK) {
             std::lock_guard<std::mutex> g(s->m);
@@ -244,11 +197,9 @@ void run(mp_server* s) {
         }
         double upd = 0;
         for (size_t k = 0; k < s->active.size(); ++k) {
-            const auto& r = s->active[k];
-            int acc = before[k];
-            if (r->quad) mp_transport_get_time(r->t, nullptr, &acc);
-            else mp_batch_get_state(s->batch, r->slot, nullptr, nullptr, nullptr, nullptr, nullptr, &acc, nullptr);
-            upd += (double)(acc - before[k]) * (double)r->cells;
+            int acc = 0;
+            mp_batch_get_state(s->batch, s->active[k]->slot, nullptr, nullptr, nullptr, nullptr, nullptr, &acc, nullptr);
+            upd += (double)(acc - before[k]) * (double)s->active[k]->cells;
         }
         {
             std::lock_guard<std::mutex> g(s->m);
@@ -290,8 +241,6 @@ extern "C" void mp_serve_destroy(mp_server* s) {
     }
     s->cv_work.notify_all();
     if (s->loop.joinable()) s->loop.join();
-    for (auto& r : s->active)
-        if (r->t) { mp_transport_destroy(r->t); r->t = nullptr; }
     mp_batch_destroy(s->batch);
     cudaStreamDestroy(s->stream);
     delete s;

@@ -802,7 +802,6 @@ mp_status create_impl(const mp_mesh_desc* mesh, bool slab, int row_begin, int ro
     MP_TRY(validate_opts(*opts, &der));
     QuadTables qt;
     if (xy) {
-        if (opts->precision != MP_PRECISION_FP64) { set_error("general quad meshes run in FP64"); return MP_ERR_ARG_WRONG; }
         long long bad = -1;
         if (validate_quads(mesh->nx, mesh->ny, xy, &bad)) {
             set_error("Mesh has non-real/non-finite coordinates or an inverted, degenerate, or nearly singular "

@@ -151,9 +151,23 @@ def test_invalid_quad_meshes_are_rejected(cuda_lib):
     with pytest.raises(MPError) as e:
         Transport(w, TransportConfig(), vertices=xy.reshape(-1))
     assert e.value.code == 62
-    with pytest.raises(MPError) as e:
-        Transport(w, TransportConfig(precision=1), vertices=sy.quad_vertices(w, sy.MESH_PERTURBED))
-    assert e.value.code == 62
+
+
+def test_mixed_form_on_quads_equals_fp64(cuda_lib):
+    """The mixed form evaluates the FP64 stage on a general quad mesh too:
+    10 SSPRK3 steps equal the FP64 form bit for bit."""
+    from mantlepar_b200.transport import Transport, TransportConfig
+    w = sy.Workload(nx=12, ny=10, seed=3)
+    xy = sy.quad_vertices(w, sy.MESH_PERTURBED)
+    out = []
+    for precision in (0, 1):
+        t = Transport(w, TransportConfig(cfl=w.cfl, integrator=3, precision=precision), vertices=xy)
+        t.set_face_velocity(*sy.face_velocity_quads(w, xy))
+        t.set_state(*sy.initial_state(w))
+        _, reps = t.step(10)
+        out.append((np.stack(t.get_state()), [r["dt"] for r in reps]))
+        t.close()
+    assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
 
 
 def test_quad_large_mesh_steps(cuda_lib):
