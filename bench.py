@@ -476,6 +476,37 @@ def run_forms(args, stream):
     forms["plain_fp64_256_one_at_a_time"] = {
         "value": cells * nsteps / (ms_solo * 1e-3), "unit": "cell-updates/s", "instances": len(ws), "steps": nsteps,
         "note": "each of the 256 meshes advanced alone through mp_transport_step (device-resident steps), times summed"}
+    # Batched general quad meshes: 64 of the uneven meshes as
+    # perturbed-quadrilateral instances (perturbation 0.2), 20 SSPRK3 steps,
+    # device-resident; and the same meshes one at a time.
+    qws = sy.batched_instances(64, seed=3)
+    qxy = [sy.quad_vertices(x, sy.MESH_PERTURBED, 0.2, 11 + k) for k, x in enumerate(qws)]
+    qcells = sum(x.cells for x in qws)
+    qsteps = 20
+    b = Batch([], TransportConfig(cfl=0.4, integrator=3), stream=stream.cuda_stream)
+    for x, xy in zip(qws, qxy):
+        i = b.add_quads(x, xy)
+        b.set_face_velocity(i, *sy.face_velocity_quads(x, xy))
+        b.set_state(i, *sy.initial_state(x))
+    b.step(1)
+    ms, reps = timed_steps(b, qsteps, stream)
+    ok = all(r[i]["status"] == 0 for r in reps for i in range(len(qws)))
+    b.close()
+    ms_solo = 0.0
+    for x, xy in zip(qws, qxy):
+        t = Transport(x, TransportConfig(cfl=0.4, integrator=3), stream=stream.cuda_stream, vertices=xy)
+        t.set_face_velocity(*sy.face_velocity_quads(x, xy))
+        t.set_state(*sy.initial_state(x))
+        t.step(1)
+        m1, _ = timed_steps(t, qsteps, stream)
+        ms_solo += m1
+        t.close()
+    forms["batched_quads_64"] = {
+        "value": qcells * qsteps / (ms * 1e-3), "unit": "cell-updates/s", "instances": len(qws), "cells": qcells,
+        "steps": qsteps, "ms_per_step": ms / qsteps, "all_instances_healthy": ok,
+        "one_at_a_time": {"value": qcells * qsteps / (ms_solo * 1e-3), "ms_per_step": ms_solo / qsteps},
+        "config": "64 uneven meshes (nx 40..640, ny 40..960, seed 3) as perturbed-quadrilateral meshes (0.2), "
+                  "SSPRK3, CFL 0.4, device-resident steps"}
     # Product-input features on the plain workload: thermal diffusion, a
     # lithostatic pressure and the adiabatic source (FP64).
     import dataclasses
