@@ -242,3 +242,39 @@ def test_batch_quad_instances_come_and_go(cuda_lib):
     got = b.get_state(0)
     assert np.array_equal(got["H"], H) and np.array_equal(got["phi"], phi)
     b.close()
+
+
+def test_batch_quad_instances_with_adiabatic_source_equal_solo(cuda_lib):
+    """alpha0 != 0 on general quad meshes in a batch (cell-point velocities
+    at each quad cell's own quadrature points, evolve.cpp:359-369) with
+    thermal diffusion: each equals its single-mesh run bit for bit, the source
+    integral in the reports."""
+    import dataclasses
+    from mantlepar_b200.batch import Batch
+    from mantlepar_b200.transport import Transport, TransportConfig
+    mat = dataclasses.replace(sy.material_s(), alpha0=3e-5)
+    cfg = TransportConfig(material=mat, cfl=0.4, integrator=3, diffusivity=1e-4)
+    b = Batch([], cfg)
+    slots = {}
+    for k, (w, fam, pert) in enumerate(QUADS[:2]):
+        xy = sy.quad_vertices(w, fam, pert, seed=31 + k)
+        i = b.add_quads(w, xy)
+        b.set_face_velocity(i, *sy.face_velocity_quads(w, xy))
+        b.set_state(i, *sy.initial_state(w))
+        b.set_cell_velocity(i, *sy.cell_velocity_quads(w, xy))
+        slots[i] = (w, xy)
+    reps = b.step(6)
+    for i, (w, xy) in slots.items():
+        t = Transport(w, cfg, vertices=xy)
+        t.set_cell_velocity(*sy.cell_velocity_quads(w, xy))
+        t.set_face_velocity(*sy.face_velocity_quads(w, xy))
+        t.set_state(*sy.initial_state(w))
+        _, sreps = t.step(6)
+        got = b.get_state(i)
+        assert got["status"] == 0 and got["accepted"] == 6
+        for a, x in zip((got["H"], got["C"], got["T"], got["phi"]), t.get_state()):
+            assert np.array_equal(a, x)
+        assert [r[i]["sourceH"] for r in reps] == [r["sourceH"] for r in sreps]
+        assert any(r["sourceH"] != 0.0 for r in sreps)
+        t.close()
+    b.close()
