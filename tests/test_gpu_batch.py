@@ -145,7 +145,8 @@ def test_batch_source_needs_cell_velocities(cuda_lib):
 
 QUADS = [(sy.Workload(nx=20, ny=24, seed=5), sy.MESH_PERTURBED, 0.2),
          (sy.Workload(nx=16, ny=20, seed=6, psi_amplitude=0.15), sy.MESH_SINE_STRETCHED, 0.0),
-         (sy.Workload(nx=7, ny=9, seed=8), sy.MESH_PERTURBED, 0.1)]
+         (sy.Workload(nx=7, ny=9, seed=8), sy.MESH_PERTURBED, 0.1),
+         (sy.Workload(nx=2, ny=3, seed=12), sy.MESH_PERTURBED, 0.1)]
 
 
 def solo_quads(w, xy, cfg, steps, kappa_bc=None):
