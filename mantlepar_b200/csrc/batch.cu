@@ -4,8 +4,9 @@
 // Every stage is one launch per kernel over ALL active instances: a device
 // work map sends each thread block to (instance, tile) and the block's
 // instance record holds that instance's buffers and tables. The per-element
-// arithmetic is the single-instance path's (stage_kernels.cuh), and the
-// block grouping of the reductions is per instance, so each instance's
+// arithmetic is the single-instance path's (stage_kernels.cuh; for general
+// quad meshes quad_kernels.cuh, over the quad instances' own work lists), and
+// the block grouping of the reductions is per instance, so each instance's
 // result is bitwise the same alone and in a batch.
 //
 // The step logic is the reference's Run loop (src/couple/evolve.cpp:449-507)
