@@ -67,6 +67,7 @@ __device__ __forceinline__ void quad_weno_cell(const QuadStageArgs& a, int i, in
     double* __restrict__ rec = a.rec;
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
+    MP_CHECK_INDEX(status, cell, N);
     const int gj = gj0 + j;
     const int ci = i == 0 ? 0 : (i == nx - 1 ? 2 : 1), cj = gj == 0 ? 0 : (gj == gny - 1 ? 2 : 1);
     const double eA = 1e-2 * __ldg(q.geo + 3 * N + cell);
@@ -76,6 +77,7 @@ __device__ __forceinline__ void quad_weno_cell(const QuadStageArgs& a, int i, in
 #pragma unroll
         for (int di = 0; di < 3; ++di) {
             const int ii = min(max(i + di - 1, 0), nx - 1), jj = min(max(j + dj - 1, 0), ny - 1);
+            MP_CHECK_INDEX(status, (long long)jj * nx + ii, N);
             u[0][dj][di] = __ldg(H + (size_t)jj * nx + ii);
             u[1][dj][di] = __ldg(C + (size_t)jj * nx + ii);
         }
@@ -110,6 +112,7 @@ __device__ __forceinline__ void quad_limit_cell(const QuadStageArgs& a, const Ph
     double* theta = a.theta;
     const long long cell = (long long)j * nx + i;
     const size_t N = (size_t)nx * ny;
+    MP_CHECK_INDEX(status, cell, N);
     const CellFrame f = cell_frame(q, nx, N, cell);
     double DH[9], DC[9];
     load_rec(rec, N, cell, DH, DC);
@@ -125,6 +128,7 @@ __device__ __forceinline__ void quad_limit_cell(const QuadStageArgs& a, const Ph
 #pragma unroll
             for (int di = -1; di <= 1; ++di) {
                 const int ii = min(max(i + di, 0), nx - 1), jj = min(max(j + dj, 0), ny - 1);
+                MP_CHECK_INDEX(status, (long long)jj * nx + ii, N);
                 const double v = __ldg(F + (size_t)jj * nx + ii);
                 lo[fi] = fmin(lo[fi], v); hi[fi] = fmax(hi[fi], v);
             }
@@ -193,6 +197,7 @@ __device__ __forceinline__ void quad_cellphase_cell(const QuadStageArgs& a, cons
     double* __restrict__ phi = a.phi;
     const SourcePtrs& src = a.src;
     const long long N = (long long)nx * ny;
+    MP_CHECK_INDEX(status, cell, N);
     const int i = (int)(cell % nx), j = (int)(cell / nx);
     const CellFrame f = cell_frame(q, nx, (size_t)N, cell);
     const double mH = __ldg(H + cell), mC = __ldg(C + cell);
@@ -287,7 +292,10 @@ __device__ __forceinline__ void quad_face_edge(const QuadStageArgs& a, const Phy
     double* __restrict__ face = a.face;
     const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
     const size_t N = (size_t)nx * ny;
+    MP_CHECK_INDEX(status, e, nE);
     const QuadEdge g = quad_edge(q, nx, ny, gj0, gny, e);
+    MP_CHECK_INDEX(status, g.L, N);
+    if (!g.boundary) MP_CHECK_INDEX(status, g.R, N);
     double len;
     P2 nrm;
     edge_geometry(g.a, g.b, len, nrm);
@@ -353,7 +361,10 @@ __device__ __forceinline__ void quad_diffusion_edge(const QuadStageArgs& a, cons
     double* __restrict__ face = a.face;
     const long long nE = (long long)nx * (ny + 1) + (long long)(nx + 1) * ny;
     const size_t N = (size_t)nx * ny;
+    MP_CHECK_INDEX(status, e, nE);
     const QuadEdge g = quad_edge(q, nx, ny, gj0, gny, e);
+    MP_CHECK_INDEX(status, g.L, N);
+    if (!g.boundary) MP_CHECK_INDEX(status, g.R, N);
     const int type = g.boundary ? ph.wall_type[g.wall] : 1;
     if (g.boundary && type == 0) return;
     double len;
