@@ -31,7 +31,9 @@ entries (a few ulp), are up to 7e-12 (theta_H), 1e-11 (theta_C) and 5e-12
 double instead of long double intermediates moves theta by up to 8e-13. The
 GPU's FP64 evaluation is another such rounding. These four are held to
 1e-12 plus twice the distance between the two oracles measured in the same
-run (the per-cell-table convention's own spread).
+run (the per-cell-table convention's own spread), and, cell by cell, the
+cells above 1e-12 must be few (at most 0.1 %) and, 95 % of them or more,
+cells where the two conventions of the reference differ by more than 1e-14.
 
 The reference build needs about 23 KB of host memory per cell; where the
 host has less free memory, the per-cell-table oracle is the restated one
@@ -50,6 +52,10 @@ RTOL = 1e-12
 
 def rel(a, b):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-3 * max(np.max(np.abs(b)), 1e-300))))
+
+
+def per_cell(a, b):
+    return np.abs(a - b) / np.maximum(np.abs(b), 1e-3 * max(np.max(np.abs(b)), 1e-300))
 
 
 def rel_inf(a, b):
@@ -140,3 +146,17 @@ def test_headline_workload_against_the_oracles(cuda_lib):
         for k, v in e.items():
             bound = RTOL if k not in fractions else 2 * gap[k] + RTOL
             assert v <= bound, (k, v, bound)
+    # Cell by cell: the few cells where the headline path moves a ratio by
+    # more than 1e-12 (measured: 0.02-0.08 % of the cells) are, all but a
+    # handful, cells where the reference's own value moves with the rounding
+    # of its stencil tables (the two conventions differ there by > 1e-14).
+    pick = {"thetaH": lambda r: r["th"][0], "thetaC": lambda r: r["th"][1],
+            "phi": lambda r: r["rhs"]["phi"], "phi1": lambda r: r["st"][3]}
+    for k in fractions:
+        gv, uv, cv = pick[k](g), pick[k](o_uni), pick[k](o_cell)
+        e_g = per_cell(gv, uv)
+        big = e_g > RTOL
+        sensitive = per_cell(uv, cv)[big] > 1e-14
+        print(f"{k}: {int(big.sum())} cells above 1e-12, {int(sensitive.sum())} of them table-sensitive")
+        assert big.mean() <= 1e-3, (k, big.mean())
+        assert sensitive.mean() >= 0.95 if big.any() else True, (k, sensitive.mean())
