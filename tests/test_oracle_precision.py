@@ -26,9 +26,12 @@ def rel_inf(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-def run(lib, w):
-    o = po.TransportOracle(sy.material_s(), w, lib=lib, integrator=3, threads=0, uniform_tables=True)
-    o.set_face_velocity(*sy.face_velocity(w))
+def run(lib, w, **kw):
+    o = po.TransportOracle(sy.material_s(), w, lib=lib, integrator=3, threads=0, uniform_tables=True, **kw)
+    if kw.get("mesh_family"):
+        o.set_face_velocity(*sy.face_velocity_quads(w, o.vertices()))
+    else:
+        o.set_face_velocity(*sy.face_velocity(w))
     o.set_state(*sy.initial_state(w))
     code, a, b = o.limiter()
     assert code == 0
@@ -41,18 +44,19 @@ def run(lib, w):
     return (a, b), r, reps[0], st
 
 
-@pytest.mark.parametrize("nx,ny", [(20, 20), (80, 160)])
-def test_fp64_intermediates_move_only_the_ratios(nx, ny):
+@pytest.mark.parametrize("nx,ny,family", [(20, 20, 0), (80, 160, 0), (40, 60, 1)])
+def test_fp64_intermediates_move_only_the_ratios(nx, ny, family):
     w = sy.Workload(nx=nx, ny=ny)
-    th_l, r_l, rep_l, st_l = run(po.restated(), w)
-    th_d, r_d, rep_d, st_d = run(po.restated_fp64(), w)
+    kw = dict(mesh_family=1, perturbation=0.2, mesh_seed=11) if family else {}
+    th_l, r_l, rep_l, st_l = run(po.restated(), w, **kw)
+    th_d, r_d, rep_d, st_d = run(po.restated_fp64(), w, **kw)
     tight = {"T": rel(r_d["T"], r_l["T"]), "rate": rel(r_d["rate"], r_l["rate"]),
              "rhsH": rel_inf(r_d["rhsH"], r_l["rhsH"]), "rhsC": rel_inf(r_d["rhsC"], r_l["rhsC"]),
              "dt": abs(rep_d["dt"] - rep_l["dt"]) / rep_l["dt"],
              "H": rel(st_d[0], st_l[0]), "C": rel(st_d[1], st_l[1]), "T1": rel(st_d[2], st_l[2])}
     ratios = {"thetaH": rel(th_d[0], th_l[0]), "thetaC": rel(th_d[1], th_l[1]),
               "phi": rel(r_d["phi"], r_l["phi"]), "phi1": rel(st_d[3], st_l[3])}
-    print(f"{nx}x{ny} double vs long double intermediates:",
+    print(f"{nx}x{ny} (family {family}) double vs long double intermediates:",
           {k: f"{v:.2e}" for k, v in {**tight, **ratios}.items()})
     assert rep_d["retries"] == rep_l["retries"]
     assert all(v <= 1e-13 for v in tight.values()), tight
